@@ -1,0 +1,118 @@
+"""Seeded synthetic inputs for the level-set and droplet workloads.
+
+The reference ships no data sets; its drivers build fields analytically
+(tests/LargeTests/test_levelset2d_large.cpp:3-60, test_mac2d_large.cpp:
+377-470).  These generators build the same kinds of fields from a seed with
+numpy's PCG64 generator, in the padded reference layout
+idx(i,j) = j + (ny+6)*i (arrays of shape (nx+6, ny+6)).
+
+* ``perturbed_circle``: signed distance to a circle of radius 0.15 centred at
+  (0.5, 0.75) whose radius carries four seeded Fourier modes m = 2..5 with
+  sum |a_m| <= 0.01, in a rigid-rotation velocity u = -2 pi (y - 0.5),
+  v = 2 pi (x - 0.5) (level-set advection + reinitialisation workload).
+* ``droplet``: one heavy droplet of seeded radius in [0.1, 0.2] whose centre
+  is at least 0.25 from the walls, fluid at rest, walls all round
+  (two-phase step workload).
+* ``droplet_batch``: many droplets of uneven grid sizes for batched runs.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+NB = 3
+
+
+@dataclass
+class Case:
+    nx: int
+    ny: int
+    dx: float
+    dy: float
+    ls: np.ndarray
+    u: np.ndarray
+    v: np.ndarray
+    dt: float = 0.0
+    steps: int = 0
+    bc_u: tuple = ("dirichlet",) * 4
+    bc_v: tuple = ("dirichlet",) * 4
+    bc_p: tuple = ("neumann",) * 4
+    fluid: dict = field(default_factory=dict)
+    meta: dict = field(default_factory=dict)
+
+
+def _centres(nx, ny, dx, dy):
+    x = (np.arange(nx + 2 * NB) - NB + 0.5) * dx
+    y = (np.arange(ny + 2 * NB) - NB + 0.5) * dy
+    return np.meshgrid(x, y, indexing="ij")
+
+
+def perturbed_circle(n: int = 128, seed: int = 0, cfl: float = 0.5, revolutions: float = 1.0) -> Case:
+    """Level-set workload on [0,1]^2 with n x n cells (Neumann pressure-grid
+    boundaries, as the reference's level-set drivers use)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    dx = dy = 1.0 / n
+    a = rng.uniform(-0.01, 0.01, size=4)
+    s = np.abs(a).sum()
+    if s > 0.01:
+        a *= 0.01 / s
+    psi = rng.uniform(0.0, 2.0 * math.pi, size=4)
+    X, Y = _centres(n, n, dx, dy)
+    th = np.arctan2(Y - 0.75, X - 0.5)
+    R = 0.15 + sum(a[k] * np.cos((k + 2) * th + psi[k]) for k in range(4))
+    ls = R - np.sqrt((X - 0.5) ** 2 + (Y - 0.75) ** 2)
+    # u on west faces (x = (i-3) dx, y centred), v on south faces.
+    xf = (np.arange(n + 2 * NB) - NB) * dx
+    yf = (np.arange(n + 2 * NB) - NB) * dy
+    _, Yc = np.meshgrid(xf, (np.arange(n + 2 * NB) - NB + 0.5) * dy, indexing="ij")
+    Xc, _ = np.meshgrid((np.arange(n + 2 * NB) - NB + 0.5) * dx, yf, indexing="ij")
+    u = -2.0 * math.pi * (Yc - 0.5)
+    v = 2.0 * math.pi * (Xc - 0.5)
+    # dt from the fastest cell-centre speed, rounded to a whole number of
+    # steps per revolution (period T = 1).
+    sl = slice(NB, -NB)
+    speed = np.sqrt((2 * math.pi * (Y[sl, sl] - 0.5)) ** 2 + (2 * math.pi * (X[sl, sl] - 0.5)) ** 2).max()
+    steps = int(math.ceil(revolutions / (cfl * dx / speed)))
+    dt = revolutions / steps
+    return Case(n, n, dx, dy, np.ascontiguousarray(ls), np.ascontiguousarray(u), np.ascontiguousarray(v),
+                dt=dt, steps=steps, bc_u=("neumann",) * 4, bc_v=("neumann",) * 4, bc_p=("neumann",) * 4,
+                meta=dict(seed=seed, a=a.tolist(), psi=psi.tolist()))
+
+
+def droplet(n: int = 256, seed: int = 0, rho_ratio: float = 1000.0, mu_ratio: float = 100.0,
+            radius=(0.1, 0.2), sigma: float = 0.0728, g: float = 9.8, ny: int | None = None) -> Case:
+    """Two-phase droplet on [0,1] x [0, ny/n] with no-slip walls: U/V
+    Dirichlet 0, pressure Neumann (the reference's MAC drivers, e.g.
+    test_mac2d_large.cpp:423-425).  phi > 0 is the heavy fluid (droplet)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ny = n if ny is None else ny
+    dx = dy = 1.0 / n
+    lx, ly = 1.0, ny * dy
+    r = rng.uniform(*radius)
+    cx = rng.uniform(0.25, lx - 0.25)
+    cy = rng.uniform(0.25, ly - 0.25) if ly > 0.5 else 0.5 * ly
+    X, Y = _centres(n, ny, dx, dy)
+    ls = r - np.sqrt((X - cx) ** 2 + (Y - cy) ** 2)
+    u = np.zeros_like(ls)
+    v = np.zeros_like(ls)
+    fluid = dict(rho_h=1000.0, rho_l=1000.0 / rho_ratio, mu_h=1.0e-3, mu_l=1.0e-3 / mu_ratio,
+                 sigma=sigma, g=g, g_axis=1, fix_gravity=0, time_order=2, cfl=0.5)
+    return Case(n, ny, dx, dy, np.ascontiguousarray(ls), u, v, bc_u=("dirichlet",) * 4,
+                bc_v=("dirichlet",) * 4, bc_p=("neumann",) * 4, fluid=fluid,
+                meta=dict(seed=seed, radius=r, centre=(cx, cy)))
+
+
+def droplet_batch(count: int = 256, seed: int = 0, sides=tuple(range(64, 513, 32))) -> list:
+    """Uneven batch: per-droplet grid side from ``sides``, radius in
+    [0.08, 0.2], density ratio log-uniform in [1, 1000] and viscosity ratio
+    log-uniform in [1, 100]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for k in range(count):
+        n = int(rng.choice(sides))
+        rr = float(10 ** rng.uniform(0.0, 3.0))
+        mr = float(10 ** rng.uniform(0.0, 2.0))
+        out.append(droplet(n, seed=int(rng.integers(1 << 31)), rho_ratio=rr, mu_ratio=mr, radius=(0.08, 0.2)))
+    return out
