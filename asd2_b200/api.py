@@ -1,0 +1,309 @@
+"""Python host binding of the asd2g C ABI (include/asd2g.h) via ctypes.
+
+This mirrors what the reference's drivers do with LevelSetSolver2D /
+MACSolver2D / PoissonSolver2D (tests/LargeTests/*.cpp) on top of the B200
+library: fields are numpy float64 arrays of shape (nx+6, ny+6) in the
+reference layout idx(i,j) = j + (ny+6)*i.  There is no CPU fallback: loading
+fails with an error when libasd2g.so is missing, and every call raises
+``Asd2gError`` on a negative status.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libasd2g.so")
+
+BC_NAMES = ["periodic", "neumann", "dirichlet", "axisym", "wall", "inlet", "outlet", "pressure", "lsfree", "custom"]
+BC = {n: i for i, n in enumerate(BC_NAMES)}
+
+# fields (enum asd2g_field)
+LS, U, V, PS, P, KAPPA, H, HS, DIV, UHAT, VHAT, LSB, LS0, W0, W1, W2, W3 = range(17)
+FIELDS = dict(ls=LS, u=U, v=V, ps=PS, p=P, kappa=KAPPA, H=H, HS=HS, div=DIV, uhat=UHAT, vhat=VHAT, lsB=LSB,
+              ls0=LS0, w0=W0, w1=W1, w2=W2, w3=W3)
+# reinit modes
+REINIT_ORIGINAL, REINIT_SUSSMAN, REINIT_MINRK2, REINIT_FIRSTTIME, REINIT_MINRK2_SUSSMAN = range(5)
+# solvers
+PCG, PCG_REFERENCE, BICGSTAB, BICGSTAB_REFERENCE = range(4)
+NOT_CONVERGED = 1
+ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "unsupported",
+          -5: "non-finite value", -6: "Krylov breakdown"}
+
+
+class Asd2gError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"asd2g error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class _Params(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nbc", C.c_int32), ("precision", C.c_int32),
+                ("base_x", C.c_double), ("base_y", C.c_double), ("dx", C.c_double), ("dy", C.c_double),
+                ("bc_u", C.c_int32 * 4), ("bc_v", C.c_int32 * 4), ("bc_p", C.c_int32 * 4),
+                ("bcc_u", C.c_double * 4), ("bcc_v", C.c_double * 4), ("bcc_p", C.c_double * 4),
+                ("rho_h", C.c_double), ("rho_l", C.c_double), ("mu_h", C.c_double), ("mu_l", C.c_double),
+                ("sigma", C.c_double), ("gravity", C.c_double), ("g_axis", C.c_int32), ("fix_gravity", C.c_int32),
+                ("time_order", C.c_int32), ("reserved0", C.c_int32), ("cfl", C.c_double),
+                ("ls_max_atime", C.c_double)]
+
+
+EXPORTS = [
+    "asd2g_version", "asd2g_last_error", "asd2g_create", "asd2g_destroy", "asd2g_sync", "asd2g_field_ptr",
+    "asd2g_upload", "asd2g_download", "asd2g_copy_field", "asd2g_fill_field", "asd2g_apply_bc",
+    "asd2g_ls_advect", "asd2g_ls_weno_rhs", "asd2g_reinit", "asd2g_subcell_eno", "asd2g_eno",
+    "asd2g_sussman_constraint", "asd2g_heaviside_deriv", "asd2g_smoothed_sign", "asd2g_ls_step",
+    "asd2g_kappa", "asd2g_heaviside", "asd2g_convection", "asd2g_viscosity", "asd2g_momentum_rhs",
+    "asd2g_intermediate_vel", "asd2g_divergence", "asd2g_update_vel", "asd2g_update_dt",
+    "asd2g_assemble_gfm", "asd2g_get_system", "asd2g_solve_pressure", "asd2g_true_residual",
+    "asd2g_droplet_step",
+]
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load libasd2g.so (no fallback: raises if it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m asd2_b200.build`")
+    L = C.CDLL(path)
+    S = C.c_void_p
+    dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+    I, D = C.c_int, C.c_double
+    sig = {
+        "asd2g_version": ([], I), "asd2g_last_error": ([], C.c_char_p),
+        "asd2g_create": ([C.POINTER(_Params), C.c_void_p, C.POINTER(S)], I),
+        "asd2g_destroy": ([S], I), "asd2g_sync": ([S], I),
+        "asd2g_field_ptr": ([S, I, C.POINTER(C.c_void_p)], I),
+        "asd2g_upload": ([S, I, dp], I), "asd2g_download": ([S, I, dp], I),
+        "asd2g_copy_field": ([S, I, I], I), "asd2g_fill_field": ([S, I, D], I),
+        "asd2g_apply_bc": ([S, I, C.c_char], I),
+        "asd2g_ls_advect": ([S, D], I), "asd2g_ls_weno_rhs": ([S, I, I, I, I], I), "asd2g_reinit": ([S, I], I),
+        "asd2g_subcell_eno": ([S, I, I, I], I), "asd2g_eno": ([S, I, I, I], I),
+        "asd2g_sussman_constraint": ([S, I, I, I, I], I), "asd2g_heaviside_deriv": ([S, I, I], I),
+        "asd2g_smoothed_sign": ([S, I, I], I), "asd2g_ls_step": ([S, D, I], I),
+        "asd2g_kappa": ([S], I), "asd2g_heaviside": ([S], I), "asd2g_convection": ([S, I, I, I, I], I),
+        "asd2g_viscosity": ([S, I, I, I, I, I, I], I), "asd2g_momentum_rhs": ([S, I, I, I, I, I, I], I),
+        "asd2g_intermediate_vel": ([S, D, I], I), "asd2g_divergence": ([S, I, I, I], I),
+        "asd2g_update_vel": ([S, D], I), "asd2g_update_dt": ([S, C.POINTER(D)], I),
+        "asd2g_assemble_gfm": ([S, D, I], I),
+        "asd2g_get_system": ([S, dp, dp, dp, dp, dp, dp, C.POINTER(I)], I),
+        "asd2g_solve_pressure": ([S, I, D, I, D, C.POINTER(I), C.POINTER(D)], I),
+        "asd2g_true_residual": ([S, C.POINTER(D)], I),
+        "asd2g_droplet_step": ([S, C.POINTER(D), I, I, D, I, C.POINTER(I), C.POINTER(D)], I),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def _bcs(names):
+    return [BC[n.lower()] for n in names]
+
+
+@dataclass
+class Params:
+    nx: int
+    ny: int
+    dx: float
+    dy: float
+    bc_u: tuple = ("dirichlet",) * 4
+    bc_v: tuple = ("dirichlet",) * 4
+    bc_p: tuple = ("neumann",) * 4
+    bcc_u: tuple = (0.0,) * 4
+    bcc_v: tuple = (0.0,) * 4
+    bcc_p: tuple = (0.0,) * 4
+    rho_h: float = 1000.0
+    rho_l: float = 1.0
+    mu_h: float = 1.0e-3
+    mu_l: float = 1.0e-5
+    sigma: float = 0.0728
+    g: float = 9.8
+    g_axis: int = 1
+    fix_gravity: int = 0
+    time_order: int = 2
+    cfl: float = 0.5
+    ls_max_atime: float = 0.0
+    base_x: float = 0.0
+    base_y: float = 0.0
+    precision: int = 0
+
+    def c(self) -> _Params:
+        p = _Params()
+        p.nx, p.ny, p.nbc, p.precision = self.nx, self.ny, 3, self.precision
+        p.base_x, p.base_y, p.dx, p.dy = self.base_x, self.base_y, self.dx, self.dy
+        for k, (a, b, c) in enumerate(zip(_bcs(self.bc_u), _bcs(self.bc_v), _bcs(self.bc_p))):
+            p.bc_u[k], p.bc_v[k], p.bc_p[k] = a, b, c
+            p.bcc_u[k], p.bcc_v[k], p.bcc_p[k] = self.bcc_u[k], self.bcc_v[k], self.bcc_p[k]
+        p.rho_h, p.rho_l, p.mu_h, p.mu_l = self.rho_h, self.rho_l, self.mu_h, self.mu_l
+        p.sigma, p.gravity, p.g_axis, p.fix_gravity = self.sigma, self.g, self.g_axis, self.fix_gravity
+        p.time_order, p.cfl, p.ls_max_atime = self.time_order, self.cfl, self.ls_max_atime
+        return p
+
+    @classmethod
+    def from_case(cls, case, **kw):
+        fl = dict(case.fluid)
+        fl.pop("g", None)
+        g = case.fluid.get("g", 9.8)
+        return cls(case.nx, case.ny, case.dx, case.dy, bc_u=case.bc_u, bc_v=case.bc_v, bc_p=case.bc_p, g=g,
+                   **{k: v for k, v in fl.items() if k in cls.__dataclass_fields__}, **kw)
+
+
+class Session:
+    """One grid's device state on the B200 (an asd2g session)."""
+
+    def __init__(self, params: Params, stream: int | None = None):
+        self.L = load()
+        self.params = params
+        self.shape = (params.nx + 6, params.ny + 6)
+        h = C.c_void_p()
+        self._check(self.L.asd2g_create(C.byref(params.c()), C.c_void_p(stream) if stream else None, C.byref(h)))
+        self.h = h
+
+    # ---- plumbing ----
+    def _check(self, rc):
+        if rc < 0:
+            raise Asd2gError(rc, self.L.asd2g_last_error().decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.asd2g_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def sync(self):
+        self._check(self.L.asd2g_sync(self.h))
+
+    @staticmethod
+    def _f(f):
+        return FIELDS[f] if isinstance(f, str) else int(f)
+
+    def upload(self, f, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        assert a.shape == self.shape, (a.shape, self.shape)
+        self._check(self.L.asd2g_upload(self.h, self._f(f), a))
+
+    def download(self, f):
+        out = np.empty(self.shape)
+        self._check(self.L.asd2g_download(self.h, self._f(f), out))
+        return out
+
+    def ptr(self, f) -> int:
+        p = C.c_void_p()
+        self._check(self.L.asd2g_field_ptr(self.h, self._f(f), C.byref(p)))
+        return p.value
+
+    def copy(self, dst, src):
+        self._check(self.L.asd2g_copy_field(self.h, self._f(dst), self._f(src)))
+
+    def fill(self, f, value):
+        self._check(self.L.asd2g_fill_field(self.h, self._f(f), float(value)))
+
+    def apply_bc(self, f, kind):
+        self._check(self.L.asd2g_apply_bc(self.h, self._f(f), kind.upper().encode()))
+
+    # ---- level set ----
+    def ls_advect(self, dt):
+        self._check(self.L.asd2g_ls_advect(self.h, dt))
+
+    def ls_weno_rhs(self, ls="ls", uc="w0", vc="w1", out="w2"):
+        self._check(self.L.asd2g_ls_weno_rhs(self.h, self._f(ls), self._f(uc), self._f(vc), self._f(out)))
+
+    def reinit(self, mode):
+        self._check(self.L.asd2g_reinit(self.h, mode))
+
+    def ls_step(self, dt, mode):
+        self._check(self.L.asd2g_ls_step(self.h, dt, mode))
+
+    def subcell_eno(self, ls, ls0, out):
+        self._check(self.L.asd2g_subcell_eno(self.h, self._f(ls), self._f(ls0), self._f(out)))
+
+    def eno(self, ls, ls0, out):
+        self._check(self.L.asd2g_eno(self.h, self._f(ls), self._f(ls0), self._f(out)))
+
+    def sussman_constraint(self, ls, ls0, hd, out):
+        self._check(self.L.asd2g_sussman_constraint(self.h, self._f(ls), self._f(ls0), self._f(hd), self._f(out)))
+
+    def heaviside_deriv(self, ls, out):
+        self._check(self.L.asd2g_heaviside_deriv(self.h, self._f(ls), self._f(out)))
+
+    def smoothed_sign(self, ls, out):
+        self._check(self.L.asd2g_smoothed_sign(self.h, self._f(ls), self._f(out)))
+
+    # ---- momentum ----
+    def kappa(self):
+        self._check(self.L.asd2g_kappa(self.h))
+
+    def heaviside(self):
+        self._check(self.L.asd2g_heaviside(self.h))
+
+    def convection(self, u, v, cu, cv):
+        self._check(self.L.asd2g_convection(self.h, *(self._f(x) for x in (u, v, cu, cv))))
+
+    def viscosity(self, u, v, ls, h, du, dv):
+        self._check(self.L.asd2g_viscosity(self.h, *(self._f(x) for x in (u, v, ls, h, du, dv))))
+
+    def momentum_rhs(self, ls, u, v, h, fu, fv):
+        self._check(self.L.asd2g_momentum_rhs(self.h, *(self._f(x) for x in (ls, u, v, h, fu, fv))))
+
+    def intermediate_vel(self, dt, h="HS"):
+        self._check(self.L.asd2g_intermediate_vel(self.h, dt, self._f(h)))
+
+    def divergence(self, u="uhat", v="vhat", div="div"):
+        self._check(self.L.asd2g_divergence(self.h, self._f(u), self._f(v), self._f(div)))
+
+    def update_vel(self, dt):
+        self._check(self.L.asd2g_update_vel(self.h, dt))
+
+    def update_dt(self) -> float:
+        d = C.c_double()
+        self._check(self.L.asd2g_update_dt(self.h, C.byref(d)))
+        return d.value
+
+    # ---- pressure ----
+    def assemble_gfm(self, dt, recompute_kappa=True):
+        self._check(self.L.asd2g_assemble_gfm(self.h, dt, 1 if recompute_kappa else 0))
+
+    def get_system(self):
+        n = self.params.nx * self.params.ny
+        arrs = [np.zeros(n) for _ in range(6)]
+        pin = C.c_int()
+        self._check(self.L.asd2g_get_system(self.h, *arrs, C.byref(pin)))
+        return dict(diag=arrs[0], cw=arrs[1], ce=arrs[2], cs=arrs[3], cn=arrs[4], rhs=arrs[5], pinned=pin.value)
+
+    def solve_pressure(self, solver=PCG, tol=1e-10, maxit=100000, dt=1.0):
+        it, res = C.c_int(), C.c_double()
+        rc = self._check(self.L.asd2g_solve_pressure(self.h, solver, tol, maxit, dt, C.byref(it), C.byref(res)))
+        return dict(status=rc, iters=it.value, resid=res.value)
+
+    def true_residual(self) -> float:
+        d = C.c_double()
+        self._check(self.L.asd2g_true_residual(self.h, C.byref(d)))
+        return d.value
+
+    def droplet_step(self, dt, reinit_mode=REINIT_MINRK2, solver=PCG, tol=1e-10, maxit=200000):
+        d, it, res = C.c_double(dt), C.c_int(), C.c_double()
+        rc = self._check(self.L.asd2g_droplet_step(self.h, C.byref(d), reinit_mode, solver, tol, maxit,
+                                                   C.byref(it), C.byref(res)))
+        return dict(status=rc, dt_next=d.value, iters=it.value, resid=res.value)

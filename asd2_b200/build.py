@@ -1,0 +1,73 @@
+"""Build recipe for the asd2g shared library (sm_100a only).
+
+``python -m asd2_b200.build`` compiles every CUDA translation unit under
+csrc/ with nvcc for sm_100a into asd2_b200/libasd2g.so (in-tree, so the built
+library travels with the source tree).  The FP64 parity kernels are compiled
+with -fmad=false: no multiply is fused into an add, which keeps their results
+bit-identical to the reference's x86-64 build.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libasd2g.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# translation unit -> extra flags
+UNITS = {
+    "bc.cu": ["-fmad=false"],
+    "levelset.cu": ["-fmad=false"],
+    "momentum.cu": ["-fmad=false"],
+    "pressure.cu": ["-fmad=false"],
+    "api.cu": [],
+}
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return "nvcc"
+
+
+def _stale(out: str, deps: list) -> bool:
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(verbose: bool = False, ptxas_v: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    headers.append(os.path.join(ROOT, "include", "asd2g.h"))
+    objs = []
+    for unit, extra in UNITS.items():
+        src = os.path.join(CSRC, unit)
+        obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
+        objs.append(obj)
+        if not _stale(obj, [src, __file__] + headers):
+            continue
+        cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-rdc=false",
+               "-I", os.path.join(ROOT, "include"), "-I", CSRC, *extra, "-c", src, "-o", obj]
+        if ptxas_v:
+            cmd.insert(1, "-Xptxas=-v")
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    if _stale(LIB, objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, ptxas_v="-v" in sys.argv)

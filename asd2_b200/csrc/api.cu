@@ -1,0 +1,660 @@
+// C-ABI entry points (include/asd2g.h): sessions, fields and the step
+// operations, enqueued on the session's stream.
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "asd2g.h"
+#include "pressure.cuh"
+
+namespace asd2g {
+// levelset.cu
+void launch_center_vel(const Grid &g, const double *u, const double *v, double *tu, double *tv, cudaStream_t st);
+void launch_ls_stage(int stage, const Grid &g, const double *phi_in, const double *tu, const double *tv,
+                     const double *phi_n, double *out, const double *dt, cudaStream_t st);
+void launch_reinit(const Grid &g, int mode, double max_atime, double *ls, double *ls0, double *w1, double *w2,
+                   double *w3, cudaStream_t st);
+void launch_absgrad(const Grid &g, bool sub, const double *ls, const double *ls0, double *out, cudaStream_t st);
+void launch_sussman_only(const Grid &g, const double *ls, const double *ls0, const double *hd, double *out,
+                         cudaStream_t st);
+void launch_pointwise_ls(const Grid &g, int which, const double *a, double *out, cudaStream_t st);
+
+DivH make_divh(double h) {
+    DivH d;
+    d.h = h;
+    int e = 0;
+    const double m = std::frexp(h, &e);
+    d.pow2 = (m == 0.5) ? 1 : 0;
+    d.inv = d.pow2 ? std::ldexp(1.0, 1 - e) : 1.0 / h;
+    return d;
+}
+
+__global__ void k_set_scalar(double *p, double v) { *p = v; }
+__global__ void k_fill(double *a, int64_t n, double v) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        a[k] = v;
+}
+}  // namespace asd2g
+
+using namespace asd2g;
+
+namespace {
+thread_local char g_err[512] = "";
+
+int fail(int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int cuda_check(const char *what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(ASD2G_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return ASD2G_OK;
+}
+
+int kind_u(int side, int bc) {
+    switch (bc) {
+    case ASD2G_BC_PERIODIC: return K_PER;
+    case ASD2G_BC_NEUMANN: return K_NEU;
+    case ASD2G_BC_AXISYM: return side < 2 ? K_DIR : K_NEU;
+    case ASD2G_BC_WALL: case ASD2G_BC_DIRICHLET: case ASD2G_BC_INLET: return K_DIR;
+    case ASD2G_BC_OUTLET: return K_NEU;
+    default: return K_NONE;
+    }
+}
+int kind_v(int side, int bc) {
+    switch (bc) {
+    case ASD2G_BC_PERIODIC: return K_PER;
+    case ASD2G_BC_NEUMANN: return K_NEU;
+    case ASD2G_BC_AXISYM: return side < 2 ? K_NEU : K_DIR;
+    case ASD2G_BC_WALL: case ASD2G_BC_DIRICHLET: case ASD2G_BC_INLET: return K_DIR;
+    case ASD2G_BC_OUTLET: return K_NEU;
+    default: return K_NONE;
+    }
+}
+int kind_p(int bc) {
+    switch (bc) {
+    case ASD2G_BC_PERIODIC: return K_PER;
+    case ASD2G_BC_NEUMANN: case ASD2G_BC_AXISYM: case ASD2G_BC_WALL: return K_NEU;
+    case ASD2G_BC_DIRICHLET: case ASD2G_BC_INLET: case ASD2G_BC_OUTLET: case ASD2G_BC_PRESSURE: return K_DIR;
+    case ASD2G_BC_LSFREE: return K_LSF;
+    default: return K_NONE;
+    }
+}
+}  // namespace
+
+struct asd2g_session {
+    asd2g_params prm;
+    Grid g;
+    MomConst M;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    size_t G = 0, N = 0;
+    double *f[ASD2G_NFIELDS] = {};
+    double *tu = nullptr, *tv = nullptr, *w1 = nullptr, *w2 = nullptr, *w3 = nullptr;
+    double *ua = nullptr, *va = nullptr, *ub = nullptr, *vb = nullptr;
+    Sys sys{};
+    double *x = nullptr, *r = nullptr, *pa = nullptr, *pb = nullptr, *q = nullptr;
+    double *rt = nullptr, *sv = nullptr, *t3 = nullptr;
+    KState *ks = nullptr;
+    KState *ks_host = nullptr;
+    double *partial = nullptr;
+    unsigned *counter = nullptr;
+    double *dsc = nullptr;       // [0] dt of the step, [1] next dt, [2..3] residual sums, [4] counter
+    double *dsc_host = nullptr;  // pinned mirror
+    bool assembled = false;
+    cudaGraphExec_t chunk_exec[4] = {};
+    int chunk_len = 64;
+    std::vector<void *> allocs;
+};
+
+namespace {
+int dalloc(asd2g_session *s, double **p, size_t n) {
+    if (cudaMalloc(p, sizeof(double) * (n ? n : 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ASD2G_E_NOMEM, "cudaMalloc of %zu doubles failed", n);
+    }
+    s->allocs.push_back(*p);
+    return ASD2G_OK;
+}
+
+int set_dt(asd2g_session *s, double dt) {
+    k_set_scalar<<<1, 1, 0, s->st>>>(s->dsc, dt);
+    return cuda_check("set dt");
+}
+
+bool valid_field(int f) { return f >= 0 && f < ASD2G_NFIELDS; }
+
+int sync(asd2g_session *s) {
+    const cudaError_t e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) return fail(ASD2G_E_CUDA, "stream sync: %s", cudaGetErrorString(e));
+    return ASD2G_OK;
+}
+
+bool stream_capturing(asd2g_session *s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s->st, &cs);
+    return cs != cudaStreamCaptureStatusNone;
+}
+
+void enqueue_iters(asd2g_session *s, int solver, int count) {
+    const Grid &g = s->g;
+    for (int k = 0; k < count; k++) {
+        if (solver <= 1) {
+            if (k % 2 == 0) launch_pcg_iter(g, s->sys, s->x, s->r, s->pa, s->pb, s->q, s->ks, s->partial, s->st);
+            else launch_pcg_iter(g, s->sys, s->x, s->r, s->pb, s->pa, s->q, s->ks, s->partial, s->st);
+        } else {
+            launch_bicg_iter(g, s->sys, s->x, s->r, s->rt, s->pa, s->q, s->sv, s->t3, s->ks, s->partial, s->st);
+        }
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int asd2g_version(void) { return ASD2G_VERSION; }
+const char *asd2g_last_error(void) { return g_err; }
+
+int asd2g_create(const asd2g_params *p, void *stream, asd2g_session **out) {
+    if (!p || !out) return fail(ASD2G_E_ARG, "null argument");
+    *out = nullptr;
+    if (p->nbc != NB) return fail(ASD2G_E_ARG, "num_bc_grid must be 3 (WENO5 needs three ghost layers), got %d", p->nbc);
+    if (p->nx < 4 || p->ny < 4) return fail(ASD2G_E_ARG, "grid must be at least 4 x 4 cells, got %d x %d", p->nx, p->ny);
+    if ((int64_t)(p->nx + 6) * (p->ny + 6) > (int64_t)1 << 31)
+        return fail(ASD2G_E_ARG, "grid %d x %d too large", p->nx, p->ny);
+    if (p->precision != 0) return fail(ASD2G_E_UNSUPPORTED, "precision %d: only FP64 (0) is implemented", p->precision);
+    if (!(p->dx > 0.0) || !(p->dy > 0.0)) return fail(ASD2G_E_ARG, "dx, dy must be positive");
+    for (int k = 0; k < 4; k++)
+        if (p->bc_u[k] < 0 || p->bc_u[k] > 9 || p->bc_v[k] < 0 || p->bc_v[k] > 9 || p->bc_p[k] < 0 || p->bc_p[k] > 9)
+            return fail(ASD2G_E_ARG, "boundary kind out of range");
+    if (p->time_order < 0 || p->time_order > 2) return fail(ASD2G_E_ARG, "time_order must be 0, 1 or 2");
+    asd2g_session *s = new (std::nothrow) asd2g_session();
+    if (!s) return fail(ASD2G_E_NOMEM, "host allocation failed");
+    s->prm = *p;
+    Grid &g = s->g;
+    g.nx = p->nx;
+    g.ny = p->ny;
+    g.sx = p->nx + 2 * NB;
+    g.sy = p->ny + 2 * NB;
+    g.dx = p->dx;
+    g.dy = p->dy;
+    bool mirror = true, pinned = true;
+    for (int k = 0; k < 4; k++) {
+        g.ku[k] = kind_u(k, p->bc_u[k]);
+        g.kv[k] = kind_v(k, p->bc_v[k]);
+        g.kp[k] = kind_p(p->bc_p[k]);
+        g.bp[k] = p->bc_p[k];
+        g.cu[k] = p->bcc_u[k];
+        g.cv[k] = p->bcc_v[k];
+        g.cp[k] = p->bcc_p[k];
+        mirror &= (g.kp[k] == K_NEU || g.kp[k] == K_DIR);
+        pinned &= (p->bc_p[k] == ASD2G_BC_NEUMANN || p->bc_p[k] == ASD2G_BC_AXISYM || p->bc_p[k] == ASD2G_BC_WALL);
+    }
+    g.p_mirror = mirror ? 1 : 0;
+    g.pinned = pinned ? 1 : 0;
+    MomParams mp{p->rho_h, p->rho_l, p->mu_h, p->mu_l, p->sigma, p->gravity, p->cfl, p->g_axis, p->fix_gravity};
+    s->M = make_momconst(g, mp);
+    s->G = (size_t)g.sx * g.sy;
+    s->N = (size_t)g.nx * g.ny;
+    if (stream) s->st = (cudaStream_t)stream;
+    else {
+        if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
+            delete s;
+            return fail(ASD2G_E_CUDA, "cudaStreamCreate failed");
+        }
+        s->own_stream = true;
+    }
+    int rc = ASD2G_OK;
+    const size_t G = s->G, N = s->N;
+    for (int k = 0; k < ASD2G_NFIELDS && rc == ASD2G_OK; k++) rc = dalloc(s, &s->f[k], G);
+    double **gw[] = {&s->tu, &s->tv, &s->w1, &s->w2, &s->w3, &s->ua, &s->va, &s->ub, &s->vb};
+    for (double **pp : gw)
+        if (rc == ASD2G_OK) rc = dalloc(s, pp, G);
+    double **nw[] = {&s->sys.diag, &s->sys.cw, &s->sys.ce, &s->sys.cs, &s->sys.cn, &s->sys.minv, &s->sys.b,
+                     &s->x, &s->r, &s->pa, &s->pb, &s->q, &s->rt, &s->sv};
+    for (double **pp : nw)
+        if (rc == ASD2G_OK) rc = dalloc(s, pp, N);
+    if (rc == ASD2G_OK) rc = dalloc(s, &s->t3, 3 * N);
+    if (rc == ASD2G_OK) rc = dalloc(s, &s->partial, 3 * RED_BLOCKS_MAX + 2 * DT_BLOCKS);
+    if (rc == ASD2G_OK) rc = dalloc(s, &s->dsc, 8);
+    if (rc == ASD2G_OK) {
+        if (cudaMalloc(&s->ks, sizeof(KState)) != cudaSuccess) rc = fail(ASD2G_E_NOMEM, "KState allocation failed");
+        else s->allocs.push_back(s->ks);
+    }
+    if (rc == ASD2G_OK) {
+        if (cudaMalloc(&s->counter, sizeof(unsigned) * 4) != cudaSuccess) rc = fail(ASD2G_E_NOMEM, "counter allocation failed");
+        else s->allocs.push_back(s->counter);
+    }
+    if (rc == ASD2G_OK && cudaMallocHost(&s->ks_host, sizeof(KState)) != cudaSuccess) rc = fail(ASD2G_E_NOMEM, "pinned alloc");
+    if (rc == ASD2G_OK && cudaMallocHost(&s->dsc_host, sizeof(double) * 8) != cudaSuccess) rc = fail(ASD2G_E_NOMEM, "pinned alloc");
+    if (rc != ASD2G_OK) {
+        asd2g_destroy(s);
+        return rc;
+    }
+    s->sys.pinned = g.pinned;
+    // Fields and work arrays start at zero, like the reference's fresh vectors.
+    for (void *a : s->allocs) (void)a;
+    for (int k = 0; k < ASD2G_NFIELDS; k++) cudaMemsetAsync(s->f[k], 0, sizeof(double) * G, s->st);
+    for (double **pp : gw) cudaMemsetAsync(*pp, 0, sizeof(double) * G, s->st);
+    for (double **pp : nw) cudaMemsetAsync(*pp, 0, sizeof(double) * N, s->st);
+    cudaMemsetAsync(s->t3, 0, sizeof(double) * 3 * N, s->st);
+    cudaMemsetAsync(s->dsc, 0, sizeof(double) * 8, s->st);
+    cudaMemsetAsync(s->counter, 0, sizeof(unsigned) * 4, s->st);
+    cudaMemsetAsync(s->ks, 0, sizeof(KState), s->st);
+    rc = sync(s);
+    if (rc != ASD2G_OK) {
+        asd2g_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return ASD2G_OK;
+}
+
+int asd2g_destroy(asd2g_session *s) {
+    if (!s) return ASD2G_OK;
+    if (s->st) cudaStreamSynchronize(s->st);
+    for (auto &e : s->chunk_exec)
+        if (e) cudaGraphExecDestroy(e);
+    for (void *p : s->allocs) cudaFree(p);
+    if (s->ks_host) cudaFreeHost(s->ks_host);
+    if (s->dsc_host) cudaFreeHost(s->dsc_host);
+    if (s->own_stream && s->st) cudaStreamDestroy(s->st);
+    delete s;
+    return ASD2G_OK;
+}
+
+int asd2g_sync(asd2g_session *s) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    return sync(s);
+}
+
+int asd2g_field_ptr(asd2g_session *s, int field, double **dptr) {
+    if (!s || !dptr || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field or null argument");
+    *dptr = s->f[field];
+    return ASD2G_OK;
+}
+
+int asd2g_upload(asd2g_session *s, int field, const double *host) {
+    if (!s || !host || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field or null argument");
+    if (cudaMemcpyAsync(s->f[field], host, sizeof(double) * s->G, cudaMemcpyHostToDevice, s->st) != cudaSuccess)
+        return cuda_check("upload");
+    return sync(s);
+}
+
+int asd2g_download(asd2g_session *s, int field, double *host) {
+    if (!s || !host || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field or null argument");
+    if (cudaMemcpyAsync(host, s->f[field], sizeof(double) * s->G, cudaMemcpyDeviceToHost, s->st) != cudaSuccess)
+        return cuda_check("download");
+    return sync(s);
+}
+
+int asd2g_copy_field(asd2g_session *s, int dst, int src) {
+    if (!s || !valid_field(dst) || !valid_field(src)) return fail(ASD2G_E_ARG, "bad field");
+    if (dst == src) return ASD2G_OK;
+    cudaMemcpyAsync(s->f[dst], s->f[src], sizeof(double) * s->G, cudaMemcpyDeviceToDevice, s->st);
+    return cuda_check("copy_field");
+}
+
+int asd2g_fill_field(asd2g_session *s, int field, double value) {
+    if (!s || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field");
+    k_fill<<<(int)((s->G + 255) / 256), 256, 0, s->st>>>(s->f[field], (int64_t)s->G, value);
+    return cuda_check("fill_field");
+}
+
+int asd2g_apply_bc(asd2g_session *s, int field, char kind) {
+    if (!s || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field");
+    if (kind == 'U' || kind == 'u') launch_fill_uv(s->g, s->f[field], nullptr, s->st);
+    else if (kind == 'V' || kind == 'v') launch_fill_uv(s->g, nullptr, s->f[field], s->st);
+    else if (kind == 'P' || kind == 'p') launch_fill_p(s->g, s->f[field], s->st);
+    else return fail(ASD2G_E_ARG, "grid kind must be U, V or P");
+    return cuda_check("apply_bc");
+}
+
+// ------------------------------------------------------------ level set --
+int asd2g_ls_advect(asd2g_session *s, double dt) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    int rc = set_dt(s, dt);
+    if (rc) return rc;
+    const Grid &g = s->g;
+    double *ls = s->f[ASD2G_LS];
+    launch_center_vel(g, s->f[ASD2G_U], s->f[ASD2G_V], s->tu, s->tv, s->st);
+    launch_fill_p(g, ls, s->st);  // HJWENO5_LS_2D fills the input's ghosts first (levelset2d.cpp:99)
+    launch_ls_stage(1, g, ls, s->tu, s->tv, ls, s->w1, s->dsc, s->st);
+    launch_ls_stage(2, g, s->w1, s->tu, s->tv, ls, s->w2, s->dsc, s->st);
+    launch_ls_stage(3, g, s->w2, s->tu, s->tv, ls, ls, s->dsc, s->st);
+    return cuda_check("ls_advect");
+}
+
+int asd2g_ls_weno_rhs(asd2g_session *s, int ls, int uc, int vc, int out) {
+    if (!s || !valid_field(ls) || !valid_field(uc) || !valid_field(vc) || !valid_field(out))
+        return fail(ASD2G_E_ARG, "bad field");
+    if (out == ls || out == uc || out == vc) return fail(ASD2G_E_ARG, "out must differ from the inputs");
+    launch_fill_p(s->g, s->f[ls], s->st);
+    cudaMemsetAsync(s->f[out], 0, sizeof(double) * s->G, s->st);
+    launch_ls_stage(0, s->g, s->f[ls], s->f[uc], s->f[vc], s->f[ls], s->f[out], s->dsc, s->st);
+    return cuda_check("ls_weno_rhs");
+}
+
+int asd2g_reinit(asd2g_session *s, int mode) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    if (mode < 0 || mode > 4) return fail(ASD2G_E_ARG, "reinit mode %d out of range", mode);
+    launch_reinit(s->g, mode, s->prm.ls_max_atime, s->f[ASD2G_LS], s->f[ASD2G_LS0], s->w1, s->w2, s->w3, s->st);
+    return cuda_check("reinit");
+}
+
+int asd2g_subcell_eno(asd2g_session *s, int ls, int ls0, int out) {
+    if (!s || !valid_field(ls) || !valid_field(ls0) || !valid_field(out) || out == ls || out == ls0)
+        return fail(ASD2G_E_ARG, "bad field");
+    launch_absgrad(s->g, true, s->f[ls], s->f[ls0], s->f[out], s->st);
+    return cuda_check("subcell_eno");
+}
+
+int asd2g_eno(asd2g_session *s, int ls, int ls0, int out) {
+    if (!s || !valid_field(ls) || !valid_field(ls0) || !valid_field(out) || out == ls || out == ls0)
+        return fail(ASD2G_E_ARG, "bad field");
+    launch_absgrad(s->g, false, s->f[ls], s->f[ls0], s->f[out], s->st);
+    return cuda_check("eno");
+}
+
+int asd2g_sussman_constraint(asd2g_session *s, int ls, int ls0, int hd, int out) {
+    if (!s || !valid_field(ls) || !valid_field(ls0) || !valid_field(hd) || !valid_field(out) || out == ls ||
+        out == ls0 || out == hd)
+        return fail(ASD2G_E_ARG, "bad field");
+    launch_sussman_only(s->g, s->f[ls], s->f[ls0], s->f[hd], s->f[out], s->st);
+    return cuda_check("sussman_constraint");
+}
+
+int asd2g_heaviside_deriv(asd2g_session *s, int ls, int out) {
+    if (!s || !valid_field(ls) || !valid_field(out)) return fail(ASD2G_E_ARG, "bad field");
+    launch_pointwise_ls(s->g, 0, s->f[ls], s->f[out], s->st);
+    return cuda_check("heaviside_deriv");
+}
+
+int asd2g_smoothed_sign(asd2g_session *s, int ls, int out) {
+    if (!s || !valid_field(ls) || !valid_field(out)) return fail(ASD2G_E_ARG, "bad field");
+    launch_pointwise_ls(s->g, 1, s->f[ls], s->f[out], s->st);
+    return cuda_check("smoothed_sign");
+}
+
+int asd2g_ls_step(asd2g_session *s, double dt, int reinit_mode) {
+    int rc = asd2g_ls_advect(s, dt);
+    if (rc) return rc;
+    return asd2g_reinit(s, reinit_mode);
+}
+
+// -------------------------------------------------------------- momentum --
+int asd2g_kappa(asd2g_session *s) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    launch_kappa(s->g, s->f[ASD2G_LS], s->f[ASD2G_KAPPA], s->st);
+    return cuda_check("kappa");
+}
+
+int asd2g_heaviside(asd2g_session *s) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    launch_heaviside(s->g, s->f[ASD2G_LS], s->f[ASD2G_H], s->f[ASD2G_HS], s->st);
+    return cuda_check("heaviside");
+}
+
+static int mom_single(asd2g_session *s, int kind, int ls, int u, int v, int h, int fu, int fv) {
+    if (!s || !valid_field(u) || !valid_field(v) || !valid_field(fu) || !valid_field(fv) || fu == fv ||
+        fu == u || fu == v || fv == u || fv == v)
+        return fail(ASD2G_E_ARG, "bad field");
+    const double *lsp = valid_field(ls) ? s->f[ls] : s->f[ASD2G_LS];
+    const double *hp = valid_field(h) ? s->f[h] : s->f[ASD2G_HS];
+    cudaMemsetAsync(s->f[fu], 0, sizeof(double) * s->G, s->st);
+    cudaMemsetAsync(s->f[fv], 0, sizeof(double) * s->G, s->st);
+    launch_mom_stage(kind, s->g, s->M, lsp, hp, s->f[u], s->f[v], nullptr, nullptr, s->f[fu], s->f[fv], s->dsc, s->st);
+    return cuda_check("momentum term");
+}
+
+int asd2g_convection(asd2g_session *s, int u, int v, int cu, int cv) { return mom_single(s, 5, -1, u, v, -1, cu, cv); }
+int asd2g_viscosity(asd2g_session *s, int u, int v, int ls, int h, int du, int dv) {
+    return mom_single(s, 6, ls, u, v, h, du, dv);
+}
+int asd2g_momentum_rhs(asd2g_session *s, int ls, int u, int v, int h, int fu, int fv) {
+    return mom_single(s, 4, ls, u, v, h, fu, fv);
+}
+
+static int intermediate(asd2g_session *s, int h) {
+    const Grid &g = s->g;
+    const MomConst &M = s->M;
+    const double *ls = s->f[ASD2G_LS], *H = s->f[h], *u = s->f[ASD2G_U], *v = s->f[ASD2G_V];
+    double *uh = s->f[ASD2G_UHAT], *vh = s->f[ASD2G_VHAT];
+    const int order = s->prm.time_order;
+    if (order == 0) {
+        launch_mom_stage(0, g, M, ls, H, u, v, nullptr, nullptr, uh, vh, s->dsc, s->st);
+    } else if (order == 1) {
+        launch_mom_stage(0, g, M, ls, H, u, v, nullptr, nullptr, s->ua, s->va, s->dsc, s->st);
+        launch_fill_uv(g, s->ua, s->va, s->st);
+        launch_mom_stage(3, g, M, ls, H, s->ua, s->va, u, v, uh, vh, s->dsc, s->st);
+    } else {
+        launch_mom_stage(0, g, M, ls, H, u, v, nullptr, nullptr, s->ua, s->va, s->dsc, s->st);
+        launch_fill_uv(g, s->ua, s->va, s->st);
+        launch_mom_stage(1, g, M, ls, H, s->ua, s->va, u, v, s->ub, s->vb, s->dsc, s->st);
+        launch_fill_uv(g, s->ub, s->vb, s->st);
+        launch_mom_stage(2, g, M, ls, H, s->ub, s->vb, u, v, uh, vh, s->dsc, s->st);
+    }
+    return cuda_check("intermediate_vel");
+}
+
+int asd2g_intermediate_vel(asd2g_session *s, double dt, int h) {
+    if (!s || !valid_field(h)) return fail(ASD2G_E_ARG, "bad field");
+    int rc = set_dt(s, dt);
+    if (rc) return rc;
+    return intermediate(s, h);
+}
+
+int asd2g_divergence(asd2g_session *s, int u, int v, int div) {
+    if (!s || !valid_field(u) || !valid_field(v) || !valid_field(div) || div == u || div == v)
+        return fail(ASD2G_E_ARG, "bad field");
+    cudaMemsetAsync(s->f[div], 0, sizeof(double) * s->G, s->st);
+    launch_divergence(s->g, s->f[u], s->f[v], s->f[div], s->st);
+    return cuda_check("divergence");
+}
+
+int asd2g_update_vel(asd2g_session *s, double dt) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    int rc = set_dt(s, dt);
+    if (rc) return rc;
+    launch_update_vel(s->g, s->M, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->f[ASD2G_PS], s->f[ASD2G_LS], s->f[ASD2G_H],
+                      s->f[ASD2G_KAPPA], s->f[ASD2G_U], s->f[ASD2G_V], s->dsc, s->st);
+    return cuda_check("update_vel");
+}
+
+int asd2g_update_dt(asd2g_session *s, double *dt) {
+    if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
+    launch_update_dt(s->g, s->M, s->f[ASD2G_U], s->f[ASD2G_V], s->partial, s->counter, s->dsc + 1, s->st);
+    cudaMemcpyAsync(s->dsc_host, s->dsc, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
+    int rc = sync(s);
+    if (rc) return rc;
+    *dt = s->dsc_host[1];
+    return ASD2G_OK;
+}
+
+// -------------------------------------------------------------- pressure --
+static int p_supported(asd2g_session *s) {
+    for (int k = 0; k < 4; k++) {
+        const int b = s->prm.bc_p[k];
+        if (b == ASD2G_BC_PERIODIC || b == ASD2G_BC_AXISYM || b == ASD2G_BC_LSFREE || b == ASD2G_BC_CUSTOM)
+            return fail(ASD2G_E_UNSUPPORTED,
+                        "pressure boundary kind %d on side %d: the GFM assembly supports Neumann, Dirichlet, inlet, "
+                        "outlet, pressure and wall sides only",
+                        b, k);
+    }
+    return ASD2G_OK;
+}
+
+static int assemble(asd2g_session *s, int recompute_kappa) {
+    int rc = p_supported(s);
+    if (rc) return rc;
+    const Grid &g = s->g;
+    if (recompute_kappa) {
+        launch_kappa(g, s->f[ASD2G_LS], s->f[ASD2G_KAPPA], s->st);
+        launch_fill_p(g, s->f[ASD2G_KAPPA], s->st);
+    }
+    launch_assemble(g, s->M, s->f[ASD2G_LS], s->f[ASD2G_KAPPA], s->f[ASD2G_H], s->f[ASD2G_DIV], s->dsc, s->sys, s->st);
+    s->assembled = true;
+    return cuda_check("assemble_gfm");
+}
+
+int asd2g_assemble_gfm(asd2g_session *s, double dt, int recompute_kappa) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    int rc = set_dt(s, dt);
+    if (rc) return rc;
+    return assemble(s, recompute_kappa);
+}
+
+int asd2g_get_system(asd2g_session *s, double *diag, double *cw, double *ce, double *cs, double *cn, double *rhs,
+                     int *pinned) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    if (!s->assembled) return fail(ASD2G_E_ARG, "no system assembled");
+    const int nx = s->g.nx, ny = s->g.ny;
+    const size_t N = s->N;
+    std::vector<double> tmp(N);
+    double *outs[6] = {diag, cw, ce, cs, cn, rhs};
+    double *srcs[6] = {s->sys.diag, s->sys.cw, s->sys.ce, s->sys.cs, s->sys.cn, s->sys.b};
+    for (int a = 0; a < 6; a++) {
+        if (!outs[a]) continue;
+        cudaMemcpyAsync(tmp.data(), srcs[a], sizeof(double) * N, cudaMemcpyDeviceToHost, s->st);
+        int rc = sync(s);
+        if (rc) return rc;
+        for (int i = 0; i < nx; i++)
+            for (int j = 0; j < ny; j++) outs[a][i + (size_t)nx * j] = tmp[j + (size_t)ny * i];
+    }
+    if (pinned) *pinned = s->sys.pinned;
+    return ASD2G_OK;
+}
+
+static int capture_chunk(asd2g_session *s, int solver) {
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return cuda_check("capture begin");
+    enqueue_iters(s, solver, s->chunk_len);
+    if (cudaStreamEndCapture(s->st, &graph) != cudaSuccess) return cuda_check("capture end");
+    cudaGraphExec_t ex = nullptr;
+    if (cudaGraphInstantiate(&ex, graph, 0) != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return cuda_check("graph instantiate");
+    }
+    cudaGraphDestroy(graph);
+    s->chunk_exec[solver] = ex;
+    return ASD2G_OK;
+}
+
+static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters, double *resid) {
+    const Grid &g = s->g;
+    const int mode = solver;  // 0 PCG, 1 PCG (reference), 2 BiCGStab, 3 BiCGStab (reference)
+    const double reg = solver == 1 ? 1.0e-12 : 0.0;  // err_tol^2 in alpha (poisson2d.cpp:354)
+    launch_set_kstate(s->ks, tol, maxit, mode, reg, s->st);
+    if (solver <= 1) launch_pcg_init(g, s->sys, s->x, s->r, s->pa, s->ks, s->partial, s->st);
+    else launch_bicg_init(g, s->sys, s->x, s->r, s->rt, s->pa, s->q, s->ks, s->partial, s->st);
+    int rc = cuda_check("solver init");
+    if (rc) return rc;
+    const int chunk = s->chunk_len;
+    if (stream_capturing(s)) {
+        // Inside a caller's capture: enqueue maxit iterations (each returns at
+        // entry once converged); no host polling is possible.
+        enqueue_iters(s, solver, maxit + (maxit & 1));
+        if (iters) *iters = -1;
+        if (resid) *resid = -1.0;
+        return cuda_check("solver enqueue");
+    }
+    if (!s->chunk_exec[solver]) {
+        rc = capture_chunk(s, solver);
+        if (rc) return rc;
+    }
+    int launched = 0;
+    for (;;) {
+        if (cudaGraphLaunch(s->chunk_exec[solver], s->st) != cudaSuccess) return cuda_check("graph launch");
+        launched += chunk;
+        cudaMemcpyAsync(s->ks_host, s->ks, sizeof(KState), cudaMemcpyDeviceToHost, s->st);
+        rc = sync(s);
+        if (rc) return rc;
+        if (s->ks_host->done || launched >= maxit + chunk) break;
+    }
+    const KState &k = *s->ks_host;
+    if (iters) *iters = k.it;
+    if (resid) *resid = k.res;
+    if (k.status == -5) return fail(ASD2G_E_NONFINITE, "non-finite residual at iteration %d", k.it);
+    if (k.status == -6) return fail(ASD2G_E_BREAKDOWN, "Krylov breakdown at iteration %d", k.it);
+    const bool conv = solver == 0 ? !(k.res > tol) : (k.res <= tol);
+    return conv ? ASD2G_OK : ASD2G_NOT_CONVERGED;
+}
+
+int asd2g_solve_pressure(asd2g_session *s, int solver, double tol, int maxit, double dt, int *iters,
+                         double *rel_resid) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    if (solver < 0 || solver > 3) return fail(ASD2G_E_ARG, "solver %d out of range", solver);
+    if (!s->assembled) return fail(ASD2G_E_ARG, "assemble the system first");
+    if (maxit < 0) return fail(ASD2G_E_ARG, "maxit must be >= 0");
+    int rc = set_dt(s, dt);
+    if (rc) return rc;
+    const int st = solve(s, solver, tol, maxit, iters, rel_resid);
+    if (st < 0) return st;
+    launch_scatter_ps(s->g, s->x, s->f[ASD2G_PS], s->f[ASD2G_P], s->dsc, s->st);
+    rc = cuda_check("scatter ps");
+    return rc ? rc : st;
+}
+
+int asd2g_true_residual(asd2g_session *s, double *rel) {
+    if (!s || !rel) return fail(ASD2G_E_ARG, "null argument");
+    if (!s->assembled) return fail(ASD2G_E_ARG, "no system assembled");
+    launch_true_residual(s->g, s->sys, s->f[ASD2G_PS], s->partial, s->dsc + 2, s->st);
+    cudaMemcpyAsync(s->dsc_host, s->dsc, sizeof(double) * 4, cudaMemcpyDeviceToHost, s->st);
+    int rc = sync(s);
+    if (rc) return rc;
+    double bb = s->dsc_host[3];
+    if (bb == 0.0) bb = 1.0;
+    *rel = std::sqrt(s->dsc_host[2]) / std::sqrt(bb);
+    return ASD2G_OK;
+}
+
+// ------------------------------------------------------------------ step --
+int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver, double tol, int maxit, int *iters,
+                       double *rel_resid) {
+    if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
+    int rc = p_supported(s);
+    if (rc) return rc;
+    const Grid &g = s->g;
+    rc = set_dt(s, *dt);
+    if (rc) return rc;
+    cudaMemcpyAsync(s->f[ASD2G_LSB], s->f[ASD2G_LS], sizeof(double) * s->G, cudaMemcpyDeviceToDevice, s->st);
+    // Solve_LevelSet_2D (dt from the device scalar)
+    double *ls = s->f[ASD2G_LS];
+    launch_center_vel(g, s->f[ASD2G_U], s->f[ASD2G_V], s->tu, s->tv, s->st);
+    launch_fill_p(g, ls, s->st);
+    launch_ls_stage(1, g, ls, s->tu, s->tv, ls, s->w1, s->dsc, s->st);
+    launch_ls_stage(2, g, s->w1, s->tu, s->tv, ls, s->w2, s->dsc, s->st);
+    launch_ls_stage(3, g, s->w2, s->tu, s->tv, ls, ls, s->dsc, s->st);
+    launch_reinit(g, reinit_mode, s->prm.ls_max_atime, ls, s->f[ASD2G_LS0], s->w1, s->w2, s->w3, s->st);
+    launch_kappa(g, ls, s->f[ASD2G_KAPPA], s->st);
+    launch_heaviside(g, ls, s->f[ASD2G_H], s->f[ASD2G_HS], s->st);
+    rc = intermediate(s, ASD2G_HS);
+    if (rc) return rc;
+    launch_fill_uv(g, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->st);
+    cudaMemsetAsync(s->f[ASD2G_DIV], 0, sizeof(double) * s->G, s->st);
+    launch_divergence(g, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->f[ASD2G_DIV], s->st);
+    // SolvePoisson recomputes kappa when kWe = rhoH / sigma is finite and nonzero (mac2d.cpp:1307).
+    const double we = s->prm.rho_h / s->prm.sigma;
+    rc = assemble(s, (we != 0.0 && std::isfinite(we)) ? 1 : 0);
+    if (rc) return rc;
+    const int st = solve(s, solver, tol, maxit, iters, rel_resid);
+    if (st < 0) return st;
+    launch_scatter_ps(g, s->x, s->f[ASD2G_PS], s->f[ASD2G_P], s->dsc, s->st);
+    launch_update_vel(g, s->M, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->f[ASD2G_PS], ls, s->f[ASD2G_H],
+                      s->f[ASD2G_KAPPA], s->f[ASD2G_U], s->f[ASD2G_V], s->dsc, s->st);
+    launch_update_dt(g, s->M, s->f[ASD2G_U], s->f[ASD2G_V], s->partial, s->counter, s->dsc + 1, s->st);
+    cudaMemcpyAsync(s->dsc_host, s->dsc, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
+    rc = sync(s);
+    if (rc) return rc;
+    rc = cuda_check("droplet_step");
+    if (rc) return rc;
+    *dt = s->dsc_host[1];
+    return st;
+}
+
+}  // extern "C"

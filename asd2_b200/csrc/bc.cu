@@ -1,0 +1,247 @@
+// Ghost-cell fill for the staggered U, V and P grids.
+// BoundaryCondition2D::ApplyBC_{U,V,P}_2D (bc2d.cpp:123-128, :239-244,
+// :346-353) applies the W, E, S and N sides in that order, and later sides
+// read cells earlier sides wrote (e.g. the U-grid W side writes the whole
+// column i = 3, which a Dirichlet S side then overwrites in rows 0..2).  The
+// U/V fill therefore runs in one CTA with a barrier between sides.  The P fill
+// touches disjoint strips that only read interior cells for Neumann and
+// Dirichlet sides, so those run fully parallel; periodic and extrapolating
+// sides run side by side in order.
+#include "internal.cuh"
+
+namespace asd2g {
+
+// ---------------------------------------------------------------- U grid --
+// side: 0 W, 1 E, 2 S, 3 N.  Work is split over [tid, n) with stride.
+__device__ void fill_u_side(const Grid &g, double *a, int side, int tid, int nth) {
+    const int nx = g.nx, ny = g.ny, k = g.ku[side];
+    const double c = g.cu[side];
+    if (k == K_NONE || k == K_LSF) return;
+    if (side == 0) {
+        if (k == K_PER) {  // bc2d.cpp:575-579 (i = 0..3)
+            const int cnt = (NB + 1) * ny;
+            for (int t = tid; t < cnt; t += nth) {
+                const int i = t / ny, j = NB + t % ny;
+                a[IX(g, i, j)] = a[IX(g, nx - 1 + i, j)];
+            }
+        } else if (k == K_NEU) {  // :599-606
+            const int m = ny + 2 * NB, cnt2 = NB * (ny + 1);
+            for (int t = tid; t < m + cnt2; t += nth) {
+                if (t < m) a[IX(g, NB, t)] = a[IX(g, NB + 1, t)];
+                else {
+                    const int q = t - m, i = q / (ny + 1), j = NB + q % (ny + 1);
+                    a[IX(g, i, j)] = a[IX(g, 2 * NB - i, j)];
+                }
+            }
+        } else {  // K_DIR :631-640
+            const int m = ny + 2 * NB, cnt2 = NB * ny;
+            for (int t = tid; t < m + cnt2; t += nth) {
+                if (t < m) a[IX(g, NB, t)] = c;
+                else {
+                    const int q = t - m, i = q / ny, j = NB + q % ny;
+                    a[IX(g, i, j)] = -a[IX(g, 2 * NB - i, j)] + 2.0 * c;
+                }
+            }
+        }
+    } else if (side == 1) {
+        if (k == K_PER) {  // :581-585
+            for (int t = tid; t < NB * ny; t += nth) {
+                const int i = t / ny, j = NB + t % ny;
+                a[IX(g, nx + i + NB, j)] = a[IX(g, i + NB, j)];
+            }
+        } else if (k == K_NEU) {  // :608-615
+            const int m = ny + 2 * NB, cnt2 = (NB - 1) * (ny + 1);
+            for (int t = tid; t < m + cnt2; t += nth) {
+                if (t < m) a[IX(g, nx + NB, t)] = a[IX(g, nx + NB - 1, t)];
+                else {
+                    const int q = t - m, i = 1 + q / (ny + 1), j = NB + q % (ny + 1);
+                    a[IX(g, nx + 2 * NB - i, j)] = a[IX(g, nx + i, j)];
+                }
+            }
+        } else {  // :642-650
+            const int m = ny + 2 * NB, cnt2 = (NB - 1) * ny;
+            for (int t = tid; t < m + cnt2; t += nth) {
+                if (t < m) a[IX(g, nx + NB, t)] = c;
+                else {
+                    const int q = t - m, i = 1 + q / ny, j = NB + q % ny;
+                    a[IX(g, nx + 2 * NB - i, j)] = -a[IX(g, nx + i, j)] + 2.0 * c;
+                }
+            }
+        }
+    } else {
+        const bool north = side == 3;
+        if (k == K_PER || k == K_NEU) {  // :587-597, :617-627 (i = 4..nx+2)
+            const int ni = nx - 1;
+            for (int t = tid; t < ni * NB; t += nth) {
+                const int i = NB + 1 + t / NB, j = t % NB;
+                if (!north) a[IX(g, i, j)] = k == K_PER ? a[IX(g, i, ny + j)] : a[IX(g, i, 2 * NB - j - 1)];
+                else if (k == K_PER) a[IX(g, i, ny + j + NB)] = a[IX(g, i, j + NB)];
+                else a[IX(g, i, ny + 2 * NB - j - 1)] = a[IX(g, i, ny + j)];
+            }
+        } else {  // K_DIR :652-664 (i = 3..nx+2)
+            for (int t = tid; t < nx * NB; t += nth) {
+                const int i = NB + t / NB, j = t % NB;
+                if (!north) a[IX(g, i, j)] = -a[IX(g, i, 2 * NB - j - 1)] + 2.0 * c;
+                else a[IX(g, i, ny + 2 * NB - j - 1)] = -a[IX(g, i, ny + j)] + 2.0 * c;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- V grid --
+__device__ void fill_v_side(const Grid &g, double *a, int side, int tid, int nth) {
+    const int nx = g.nx, ny = g.ny, k = g.kv[side];
+    const double c = g.cv[side];
+    if (k == K_NONE || k == K_LSF) return;
+    if (side == 0 || side == 1) {  // :666-676, :690-700, :730-742 (j = 4..ny+2)
+        const bool east = side == 1;
+        const int nj = ny - 1;
+        for (int t = tid; t < NB * nj; t += nth) {
+            const int i = t / nj, j = NB + 1 + t % nj;
+            if (!east) {
+                if (k == K_PER) a[IX(g, i, j)] = a[IX(g, nx + i, j)];
+                else if (k == K_NEU) a[IX(g, i, j)] = a[IX(g, 2 * NB - i - 1, j)];
+                else a[IX(g, i, j)] = -a[IX(g, 2 * NB - i - 1, j)] + 2.0 * c;
+            } else {
+                if (k == K_PER) a[IX(g, nx + i + NB, j)] = a[IX(g, i + NB, j)];
+                else if (k == K_NEU) a[IX(g, nx + 2 * NB - i - 1, j)] = a[IX(g, nx + i, j)];
+                else a[IX(g, nx + 2 * NB - i - 1, j)] = -a[IX(g, nx + i, j)] + 2.0 * c;
+            }
+        }
+    } else if (side == 2) {
+        if (k == K_PER) {  // :678-682 (j = 0..3)
+            for (int t = tid; t < nx * (NB + 1); t += nth) {
+                const int i = NB + t / (NB + 1), j = t % (NB + 1);
+                a[IX(g, i, j)] = a[IX(g, i, ny - 1 + j)];
+            }
+        } else {  // :702-709 Neumann, :744-752 Dirichlet
+            const int m = nx + 2 * NB;
+            for (int t = tid; t < m + nx * NB; t += nth) {
+                if (t < m) a[IX(g, t, NB)] = k == K_NEU ? a[IX(g, t, NB + 1)] : c;
+                else {
+                    const int q = t - m, i = NB + q / NB, j = q % NB;
+                    a[IX(g, i, j)] = k == K_NEU ? a[IX(g, i, 2 * NB - j)] : -a[IX(g, i, 2 * NB - j)] + 2.0 * c;
+                }
+            }
+        }
+    } else {
+        if (k == K_PER) {  // :684-688
+            for (int t = tid; t < nx * NB; t += nth) {
+                const int i = NB + t / NB, j = t % NB;
+                a[IX(g, i, ny + j + NB)] = a[IX(g, i, j + NB)];
+            }
+        } else {  // :711-718, :754-762
+            const int m = nx + 2 * NB;
+            for (int t = tid; t < m + nx * (NB - 1); t += nth) {
+                if (t < m) a[IX(g, t, ny + NB)] = k == K_NEU ? a[IX(g, t, ny + NB - 1)] : c;
+                else {
+                    const int q = t - m, i = NB + q / (NB - 1), j = 1 + q % (NB - 1);
+                    a[IX(g, i, ny + 2 * NB - j)] =
+                        k == K_NEU ? a[IX(g, i, ny + j)] : -a[IX(g, i, ny + j)] + 2.0 * c;
+                }
+            }
+        }
+    }
+}
+
+// One CTA fills U and/or V (either pointer may be null), side by side.
+__global__ void __launch_bounds__(1024) k_fill_uv(Grid g, double *u, double *v) {
+    for (int side = 0; side < 4; side++) {
+        if (u) fill_u_side(g, u, side, threadIdx.x, blockDim.x);
+        if (v) fill_v_side(g, v, side, threadIdx.x, blockDim.x);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- P grid --
+__device__ __forceinline__ void fill_p_cell(const Grid &g, double *a, int side, int layer, int s) {
+    // layer t = 0..2 is the ghost distance index the reference loops use;
+    // s is the position along the side (interior j for W/E, interior i for S/N).
+    const int nx = g.nx, ny = g.ny, k = g.kp[side];
+    const double c = g.cp[side];
+    if (side == 0) {
+        const int j = s, i = layer;
+        if (k == K_PER) a[IX(g, i, j)] = a[IX(g, nx + i, j)];
+        else if (k == K_NEU) a[IX(g, i, j)] = a[IX(g, 2 * NB - i - 1, j)];
+        else if (k == K_DIR) a[IX(g, i, j)] = -a[IX(g, 2 * NB - i - 1, j)] + 2.0 * c;
+    } else if (side == 1) {
+        const int j = s, i = layer;
+        if (k == K_PER) a[IX(g, nx + i, j)] = a[IX(g, i + NB, j)];  // writes interior columns (bc2d.cpp:770-774)
+        else if (k == K_NEU) a[IX(g, nx + 2 * NB - i - 1, j)] = a[IX(g, nx + i, j)];
+        else if (k == K_DIR) a[IX(g, nx + 2 * NB - i - 1, j)] = -a[IX(g, nx + i, j)] + 2.0 * c;
+    } else if (side == 2) {
+        const int i = s, j = layer;
+        if (k == K_PER) a[IX(g, i, j)] = a[IX(g, i, ny + j)];
+        else if (k == K_NEU) a[IX(g, i, j)] = a[IX(g, i, 2 * NB - j - 1)];
+        else if (k == K_DIR) a[IX(g, i, j)] = -a[IX(g, i, 2 * NB - j - 1)] + 2.0 * c;
+    } else {
+        const int i = s, j = layer;
+        if (k == K_PER) a[IX(g, i, ny + j + NB)] = a[IX(g, i, j + NB)];
+        else if (k == K_NEU) a[IX(g, i, ny + 2 * NB - j - 1)] = a[IX(g, i, ny + j)];
+        else if (k == K_DIR) a[IX(g, i, ny + 2 * NB - j - 1)] = -a[IX(g, i, ny + j)] + 2.0 * c;
+    }
+}
+
+// LS free boundary: linear extrapolation outward (bc2d.cpp:863-900), the
+// three layers in the reference's order by one thread per line.
+__device__ __forceinline__ void fill_p_lsfree(const Grid &g, double *a, int side, int s) {
+    const int nx = g.nx, ny = g.ny;
+    const double dx = g.dx, dy = g.dy;
+    if (side == 0) {
+        const int j = s;
+        for (int i = NB - 1; i >= 0; i--)
+            a[IX(g, i, j)] = a[IX(g, i + 1, j)] + dx * (a[IX(g, i + 1, j)] - a[IX(g, i + 2, j)]) / dx;
+    } else if (side == 1) {
+        const int j = s;
+        for (int i = 0; i < NB; i++)
+            a[IX(g, nx + NB + i, j)] =
+                a[IX(g, nx + NB + i - 1, j)] + dx * (a[IX(g, nx + NB + i - 1, j)] - a[IX(g, nx + NB + i - 2, j)]) / dx;
+    } else if (side == 2) {
+        const int i = s;
+        for (int j = NB - 1; j >= 0; j--)
+            a[IX(g, i, j)] = a[IX(g, i, j + 1)] + dy * (a[IX(g, i, j + 1)] - a[IX(g, i, j + 2)]) / dy;
+    } else {
+        const int i = s;
+        for (int j = 0; j < NB; j++)
+            a[IX(g, i, ny + NB + j)] =
+                a[IX(g, i, ny + NB + j - 1)] + dy * (a[IX(g, i, ny + NB + j - 1)] - a[IX(g, i, ny + NB + j - 2)]) / dy;
+    }
+}
+
+// side_mask selects the sides handled by this launch.
+__global__ void k_fill_p(Grid g, double *a, int side_mask) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nwe = NB * g.ny, nsn = NB * g.nx;
+    int side, rem;
+    if (t < nwe) { side = 0; rem = t; }
+    else if (t < 2 * nwe) { side = 1; rem = t - nwe; }
+    else if (t < 2 * nwe + nsn) { side = 2; rem = t - 2 * nwe; }
+    else if (t < 2 * nwe + 2 * nsn) { side = 3; rem = t - 2 * nwe - nsn; }
+    else return;
+    if (!((side_mask >> side) & 1)) return;
+    const int along = side < 2 ? g.ny : g.nx;
+    const int layer = rem / along, s = NB + rem % along;
+    if (g.kp[side] == K_LSF) {
+        if (layer == 0) fill_p_lsfree(g, a, side, s);
+    } else {
+        fill_p_cell(g, a, side, layer, s);
+    }
+}
+
+void launch_fill_uv(const Grid &g, double *u, double *v, cudaStream_t st) {
+    k_fill_uv<<<1, 1024, 0, st>>>(g, u, v);
+}
+
+void launch_fill_p(const Grid &g, double *a, cudaStream_t st) {
+    const int n = 2 * NB * g.ny + 2 * NB * g.nx;
+    const int blocks = (n + 255) / 256;
+    bool seq = false;
+    for (int s = 0; s < 4; s++) seq |= (g.kp[s] == K_PER || g.kp[s] == K_LSF);
+    if (!seq) {
+        k_fill_p<<<blocks, 256, 0, st>>>(g, a, 0xF);
+    } else {
+        for (int s = 0; s < 4; s++) k_fill_p<<<blocks, 256, 0, st>>>(g, a, 1 << s);
+    }
+}
+
+}  // namespace asd2g

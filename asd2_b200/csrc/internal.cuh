@@ -1,0 +1,24 @@
+// Declarations shared by the asd2g translation units (not part of the ABI).
+#pragma once
+#include <cstdio>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace asd2g {
+
+// Division by a grid spacing.  When h is a power of two, x / h and
+// x * (1/h) are the same IEEE result, so the multiply is used; otherwise the
+// division is kept.  Either way the result equals the reference's x / h.
+struct DivH {
+    double h, inv;
+    int pow2;
+    __device__ __forceinline__ double operator()(double x) const { return pow2 ? x * inv : x / h; }
+};
+DivH make_divh(double h);
+
+// bc.cu
+void launch_fill_uv(const Grid &g, double *u, double *v, cudaStream_t st);
+void launch_fill_p(const Grid &g, double *a, cudaStream_t st);
+
+}  // namespace asd2g

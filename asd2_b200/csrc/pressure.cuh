@@ -1,0 +1,47 @@
+// GFM Poisson system and Krylov solvers (declarations shared with api.cu).
+#pragma once
+#include "momentum.cuh"
+
+namespace asd2g {
+
+// Matrix-free system over the nx*ny interior cells in the compact layout
+// k = j' + ny*i' (j' = j-3, i' = i-3; y fastest like the padded fields):
+//   (A x)_k = diag_k x_k - cw_k x_W - ce_k x_E - cs_k x_S - cn_k x_N
+// cw_k equals ce of the west neighbour and cs_k cn of the south neighbour
+// bit for bit (the face rule is symmetric), so the solvers read ce/cn only.
+struct Sys {
+    double *diag, *cw, *ce, *cs, *cn, *minv, *b;
+    int pinned;
+};
+
+// Scalars of one Krylov solve, kept on the device so that iterations can be
+// enqueued (and graph-captured) without host round trips.
+struct KState {
+    double rho, alpha, beta, bn, res, tol, reg;
+    double omega, rho1, rho2, rtv, snorm;
+    int it, maxit, done, status, mode;
+    unsigned counter;
+};
+
+constexpr int RED_BLOCKS_MAX = 1184;  // 8 x 148 SMs
+inline int red_blocks(int64_t n) {
+    int64_t b = (n + 255) / 256;
+    return (int)(b < 1 ? 1 : (b > RED_BLOCKS_MAX ? RED_BLOCKS_MAX : b));
+}
+
+void launch_assemble(const Grid &g, const MomConst &M, const double *ls, const double *kappa, const double *H,
+                     const double *div, const double *dtp, const Sys &S, cudaStream_t st);
+void launch_pcg_init(const Grid &g, const Sys &S, double *x, double *r, double *p, KState *ks, double *partial,
+                     cudaStream_t st);
+void launch_pcg_iter(const Grid &g, const Sys &S, double *x, double *r, const double *p_old, double *p_new,
+                     double *q, KState *ks, double *partial, cudaStream_t st);
+void launch_bicg_init(const Grid &g, const Sys &S, double *x, double *r, double *rt, double *p, double *v,
+                      KState *ks, double *partial, cudaStream_t st);
+void launch_bicg_iter(const Grid &g, const Sys &S, double *x, double *r, const double *rt, double *p, double *v,
+                      double *s, double *t, KState *ks, double *partial, cudaStream_t st);
+void launch_scatter_ps(const Grid &g, const double *x, double *ps, double *p, const double *dtp, cudaStream_t st);
+void launch_true_residual(const Grid &g, const Sys &S, const double *ps, double *partial, double *out2,
+                          cudaStream_t st);
+void launch_set_kstate(KState *ks, double tol, int maxit, int mode, double reg, cudaStream_t st);
+
+}  // namespace asd2g

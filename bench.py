@@ -1,0 +1,410 @@
+#!/usr/bin/env python
+"""Benchmark: GFM Poisson solves/s at relative residual 1e-8 on the 256^2
+two-phase droplet workload (plus level-set Mcells/s on the 128^2 level-set
+workload), one JSON line on stdout.
+
+A step is one complete GFM pressure solve: curvature + GFM assembly from the
+level set, H and divergence, then Jacobi-PCG in FP64 to a true relative
+residual <= 1e-8, then ps/p written back.  The system is the one a 256^2
+droplet (density ratio 1000, viscosity ratio 100, sigma 0.0728, no-slip
+walls) produces after a few steps of the full two-phase step from rest.
+Inputs are resident in HBM when the timed region starts; L2 is flushed
+(256 MB write) between timed steps because the working set fits in L2.
+
+e2e: the same solves through the C ABI with host buffers: upload ls, H and
+div from pinned host memory, assemble, solve, download ps -- all inside the
+timed region.
+
+Multi-GPU: the path does not shard (one pressure system per droplet); N
+ranks run N independent replicas, value = total solves/s over all ranks with
+the time taken as the max over ranks.
+
+--impl reference: the CPU implementation of the same solve on the host's
+cores (the C restatement of the reference, one single-threaded process per
+core on the same system, since the reference's own all-Neumann solve is
+mis-indexed and cannot converge -- see DESIGN.md).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+TOL = 1e-8
+N_GRID = 256
+LS_GRID = 128
+PREP_STEPS = 3
+BYTES_PER_UNKNOWN_ITER = 112  # 14 FP64 streams per PCG iteration (two fused sweeps)
+
+
+def metric_name():
+    with open(os.path.join(ROOT, "BASELINE.json")) as f:
+        return json.load(f)["metric"]
+
+
+# ---------------------------------------------------------------- clocks --
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=6)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------- workloads --
+def droplet_params(case):
+    from asd2_b200 import api
+    return api.Params.from_case(case)
+
+
+def prepare_state(n, seed, stream):
+    """Run a few full droplet steps from rest and return the session and the
+    snapshot (ls, H, div, dt) that defines the benchmark's GFM system."""
+    from asd2_b200 import api
+    from asd2_b200 import workloads as W
+    c = W.droplet(n, seed=seed)
+    s = api.Session(droplet_params(c), stream=stream)
+    s.upload("ls", c.ls)
+    s.upload("u", c.u)
+    s.upload("v", c.v)
+    s.apply_bc("ls", "P")
+    dt = s.update_dt()
+    for _ in range(PREP_STEPS):
+        r = s.droplet_step(dt, tol=1e-10, maxit=500000)
+        dt = r["dt_next"]
+    # the step's pressure system: kappa/H/div/ls as left by the last step
+    snap = {k: s.download(k) for k in ("ls", "H", "div", "kappa")}
+    return c, s, snap, dt
+
+
+def run_ours(args):
+    import torch
+    from asd2_b200 import api
+    from asd2_b200 import workloads as W
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+
+    c, s, snap, dt = prepare_state(args.n, args.seed + rank, sh)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def solve_once():
+        s.assemble_gfm(dt, recompute_kappa=True)
+        return s.solve_pressure(api.PCG, tol=TOL, maxit=500000, dt=dt)
+
+    # warm-up
+    for _ in range(args.warmup):
+        r = solve_once()
+    s.sync()
+    # timed: device-resident inputs, L2 flushed between steps
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    times, iters = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            r = solve_once()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+            iters.append(r["iters"])
+            assert r["status"] == 0, r
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    true_res = s.true_residual()
+    t_total = float(sum(times))
+    if dist:
+        t = torch.tensor([t_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_total = float(t.item())
+    value = world * args.steps / t_total
+
+    # assembly alone (to split the iteration time out of the solve time)
+    ta = []
+    for _ in range(max(3, args.steps)):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        s.assemble_gfm(dt, recompute_kappa=True)
+        e1.record(stream)
+        e1.synchronize()
+        ta.append(e0.elapsed_time(e1) / 1e3)
+    t_asm = float(np.median(ta))
+    it_mean = float(np.mean(iters))
+    t_iter = max((t_total / args.steps - t_asm) / it_mean, 1e-12)
+    N = args.n * args.n
+    achieved = BYTES_PER_UNKNOWN_ITER * N / t_iter / 1e9
+
+    # e2e through host buffers (pinned), copies inside the timed region
+    G = (args.n + 6) ** 2
+    pin = {k: torch.from_numpy(snap[k]).pin_memory() for k in ("ls", "H", "div")}
+    out = torch.empty((args.n + 6, args.n + 6), dtype=torch.float64).pin_memory()
+    host = {k: v.numpy() for k, v in pin.items()}
+    e2e_t = []
+    for k in range(args.warmup + args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        for f in ("ls", "H", "div"):
+            s.upload(f, host[f])
+        s.assemble_gfm(dt, recompute_kappa=True)
+        r = s.solve_pressure(api.PCG, tol=TOL, maxit=500000, dt=dt)
+        s.L.asd2g_download(s.h, api.PS, out.numpy())
+        e1.record(stream)
+        e1.synchronize()
+        if k >= args.warmup:
+            e2e_t.append(e0.elapsed_time(e1) / 1e3)
+    e2e_total = float(sum(e2e_t))
+    if dist:
+        t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * args.steps / e2e_total
+
+    # level-set Mcells/s on the 128^2 perturbed-circle workload
+    lc = W.perturbed_circle(LS_GRID, seed=args.seed)
+    ls_s = api.Session(api.Params(lc.nx, lc.ny, lc.dx, lc.dy, bc_u=lc.bc_u, bc_v=lc.bc_v, bc_p=lc.bc_p), stream=sh)
+    ls_s.upload("ls", lc.ls)
+    ls_s.upload("u", lc.u)
+    ls_s.upload("v", lc.v)
+    for _ in range(3):
+        ls_s.ls_step(lc.dt, api.REINIT_MINRK2_SUSSMAN)
+    ls_s.sync()
+    nls = 200
+    with torch.cuda.stream(stream):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+    for _ in range(nls):
+        ls_s.ls_step(lc.dt, api.REINIT_MINRK2_SUSSMAN)
+    e1.record(stream)
+    e1.synchronize()
+    t_ls = e0.elapsed_time(e1) / 1e3 / nls
+    ls_mcells = lc.nx * lc.ny / t_ls / 1e6
+    ls_s.close()
+
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    chunks = [math.ceil(i / 64) for i in iters]
+    launches = int(sum(4 + 2 + 128 * ch + 3 for ch in chunks))
+
+    line = {
+        "metric": metric_name(),
+        "value": value,
+        "unit": "GFM Poisson solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * t_total / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"GFM pressure solve of a {args.n}x{args.n} two-phase droplet (rho ratio 1000, "
+                               f"mu ratio 100, sigma 0.0728, no-slip walls) after {PREP_STEPS} full steps; "
+                               f"FP64 Jacobi-PCG to true rel. residual {TOL:g}",
+                   "grid": [args.n, args.n], "solver": "FP64 Jacobi-PCG (matrix-free, fused sweeps)",
+                   "tol": TOL, "l2": "flushed (256 MB write) between timed steps",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "solver_iters_mean": it_mean,
+        "true_rel_residual": true_res,
+        "ls_mcells_per_s": ls_mcells,
+        "ls_config": {"workload": f"{LS_GRID}x{LS_GRID} perturbed circle, WENO5/TVD-RK3 + 5 MinRK2 subcell "
+                                  "pseudo-steps with the Sussman constraint, FP64", "ms_per_step": t_ls * 1e3},
+        "roofline": {"bound": "hbm", "kernel": "pcg iteration (k_pcg_a + k_pcg_b)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "bytes_per_unknown_iter": BYTES_PER_UNKNOWN_ITER,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback",
+                     "note": "working set is L2-resident at 256^2; iteration time from CUDA events "
+                             "(solve minus assembly) / iterations"},
+        "e2e": {"value": e2e_value, "unit": "GFM Poisson solves/s",
+                "h2d_bytes_per_step": 3 * G * 8, "d2h_bytes_per_step": G * 8},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(snap, c, dt, args)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------------- CPU baseline --
+def _cpu_worker(payload):
+    sys.path.insert(0, ROOT)
+    from oracle.pyoracle import FluidSpec, GridSpec, Oracle
+    g = GridSpec(**payload["grid"])
+    f = FluidSpec(**payload["fluid"])
+    O = Oracle()
+    budget = payload["budget_s"]
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        kap = payload["kappa"].copy()
+        sysd = O.gfm_assemble(g, f, payload["dt"], payload["ls"], kap, payload["H"], payload["div"],
+                              recompute_kappa=True)
+        _, it, _, tres = O.pcg(g, sysd, tol=TOL, maxit=500000)
+        n += 1
+        if time.perf_counter() - t0 > budget or n >= payload["max_solves"]:
+            break
+    return n, time.perf_counter() - t0, it, tres
+
+
+def cpu_baseline(snap, case, dt, args, procs=1, budget_s=None):
+    """The C restatement of the reference's solve (single-threaded, fixed
+    summation order) on a bounded sample of the same workload."""
+    import multiprocessing as mp
+    budget = budget_s if budget_s is not None else args.cpu_budget
+    payload = dict(grid=dict(nx=case.nx, ny=case.ny, dx=case.dx, dy=case.dy, bc_u=case.bc_u, bc_v=case.bc_v,
+                             bc_p=case.bc_p),
+                   fluid={k: v for k, v in case.fluid.items()}, dt=dt, budget_s=budget, max_solves=10 ** 6,
+                   **{k: snap[k] for k in ("ls", "H", "div", "kappa")})
+    if procs == 1:
+        n, t, it, tres = _cpu_worker(payload)
+        total, tmax = n, t
+    else:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(procs) as pool:
+            res = pool.map(_cpu_worker, [payload] * procs)
+        total = sum(r[0] for r in res)
+        tmax = max(r[1] for r in res)
+        it, tres = res[0][2], res[0][3]
+    return {"value": total / tmax, "unit": "GFM Poisson solves/s", "cores": procs, "kind": "port",
+            "sample": f"{total} solves of the same {case.nx}x{case.ny} GFM system ({it} PCG iterations each, "
+                      f"true rel. residual {tres:.1e}) in {tmax:.1f} s, oracle/asd2_oracle.c built -O2"}
+
+
+def run_reference(args):
+    """Reference arm: CPU implementation of the same solves on all host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    # Inputs: the same GFM system, generated on the CPU by the restatement's
+    # own droplet steps (no GPU is needed for this arm).
+    from asd2_b200 import workloads as W
+    from oracle.pyoracle import FluidSpec, GridSpec, Oracle
+    c = W.droplet(args.n, seed=args.seed)
+    g = GridSpec(c.nx, c.ny, c.dx, c.dy, bc_u=c.bc_u, bc_v=c.bc_v, bc_p=c.bc_p)
+    f = FluidSpec(**c.fluid)
+    O = Oracle()
+    st = dict(ls=c.ls.copy(), u=c.u.copy(), v=c.v.copy(), kappa=g.zeros())
+    O.bc(g, "p", st["ls"])
+    st["dt"] = O.update_dt(g, f, st["u"], st["v"])
+    for _ in range(PREP_STEPS):
+        info = O.droplet_step(g, f, st, tol=1e-10)
+    snap = dict(ls=st["ls"], H=info["H"], div=info["div"], kappa=st["kappa"])
+    cores = os.cpu_count() or 1
+    per_step = max(args.cpu_budget / max(args.steps, 1), 1.0)
+    vals = []
+    for k in range(args.warmup + args.steps):
+        cb = cpu_baseline(snap, c, st["dt_used"], args, procs=cores, budget_s=per_step)
+        if k >= args.warmup:
+            vals.append(cb["value"])
+    value = float(np.mean(vals))
+    line = {"impl": "reference", "metric": metric_name(), "value": value, "unit": "GFM Poisson solves/s",
+            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"GFM pressure solve of a {args.n}x{args.n} two-phase droplet after "
+                                   f"{PREP_STEPS} full steps; Jacobi-PCG to true rel. residual {TOL:g}",
+                       "grid": [args.n, args.n]},
+            "cpu_baseline": {"value": value, "unit": "GFM Poisson solves/s", "cores": cores, "kind": "port",
+                             "sample": cb["sample"] + f"; {cores} processes"},
+            "e2e": {"value": value, "unit": "GFM Poisson solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_GRID)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,200 @@
+/* asd2g: B200 (sm_100a) implementation of the 2D two-phase droplet step of
+ * appleparan/ASD2, behind a C ABI.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, returns an
+ * int status (0 ok, > 0 not converged, < 0 error; see ASD2G_E*) and never
+ * throws.  A session owns one grid's device fields; all work is enqueued on
+ * the session's CUDA stream.  Fields use the reference layout: a padded
+ * (nx+6) x (ny+6) array of doubles, idx(i,j) = j + (ny+6)*i, three ghost
+ * layers, u on west faces and v on south faces (levelset2d.cpp:1048-1050).
+ *
+ * Reference interfaces replaced (appleparan/ASD2, file:line):
+ *   LevelSetSolver2D   include/levelset2d.h:17-87
+ *   MACSolver2D        include/mac2d.h:31-168
+ *   PoissonSolver2D    include/poisson2d.h:31-61
+ *   BoundaryCondition2D include/bc2d.h:20-127
+ * The C++ classes with those exact signatures live in asd2_b200/dropin/ and
+ * are implemented on top of these functions.
+ */
+#ifndef ASD2G_H_INCLUDED
+#define ASD2G_H_INCLUDED
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ASD2G_VERSION 1
+
+/* ---- status codes ---- */
+#define ASD2G_OK 0
+#define ASD2G_NOT_CONVERGED 1     /* iterative solve hit maxit */
+#define ASD2G_E_ARG (-1)          /* invalid argument (size, enum, null) */
+#define ASD2G_E_CUDA (-2)         /* CUDA runtime error */
+#define ASD2G_E_NOMEM (-3)        /* device allocation failed */
+#define ASD2G_E_UNSUPPORTED (-4)  /* configuration outside the implemented path */
+#define ASD2G_E_NONFINITE (-5)    /* NaN/Inf detected (the reference exit(1)s) */
+#define ASD2G_E_BREAKDOWN (-6)    /* Krylov breakdown (zero denominator) */
+
+/* ---- boundary kinds: same values as enum class BC2D (include/common.h:4) ---- */
+enum asd2g_bc {
+    ASD2G_BC_PERIODIC = 0, ASD2G_BC_NEUMANN, ASD2G_BC_DIRICHLET, ASD2G_BC_AXISYM, ASD2G_BC_WALL,
+    ASD2G_BC_INLET, ASD2G_BC_OUTLET, ASD2G_BC_PRESSURE, ASD2G_BC_LSFREE, ASD2G_BC_CUSTOM
+};
+
+/* ---- device fields of a session ---- */
+enum asd2g_field {
+    ASD2G_LS = 0,   /* level set phi (cell centres; > 0 heavy fluid) */
+    ASD2G_U,        /* u on west faces */
+    ASD2G_V,        /* v on south faces */
+    ASD2G_PS,       /* pseudo pressure ps = p * dt (cell centres) */
+    ASD2G_P,        /* pressure p = ps / dt */
+    ASD2G_KAPPA,    /* curvature */
+    ASD2G_H,        /* sharp Heaviside of phi */
+    ASD2G_HS,       /* smoothed Heaviside of phi */
+    ASD2G_DIV,      /* divergence of (uhat, vhat) */
+    ASD2G_UHAT,     /* intermediate velocity */
+    ASD2G_VHAT,
+    ASD2G_LSB,      /* phi at the start of the step */
+    ASD2G_LS0,      /* phi at the start of reinitialisation (lsInit) */
+    ASD2G_W0,       /* general work arrays (padded) usable by callers */
+    ASD2G_W1,
+    ASD2G_W2,
+    ASD2G_W3,
+    ASD2G_NFIELDS
+};
+
+/* ---- reinitialisation modes ---- */
+enum asd2g_reinit {
+    ASD2G_REINIT_ORIGINAL = 0,      /* Reinit_Original_2D        levelset2d.cpp:264 */
+    ASD2G_REINIT_SUSSMAN = 1,       /* Reinit_Sussman_2D         levelset2d.cpp:318 */
+    ASD2G_REINIT_MINRK2 = 2,        /* Reinit_MinRK2_2D          levelset2d.cpp:433 */
+    ASD2G_REINIT_FIRSTTIME = 3,     /* FirstTimeOnlyReinit_Sussman_2D levelset2d.cpp:377 */
+    ASD2G_REINIT_MINRK2_SUSSMAN = 4 /* MinRK2 subcell steps + Sussman constraint after each */
+};
+
+/* ---- pressure solvers ---- */
+enum asd2g_solver {
+    ASD2G_SOLVER_PCG = 0,          /* Jacobi-PCG, textbook recurrence            */
+    ASD2G_SOLVER_PCG_REFERENCE = 1,/* the reference iteration, poisson2d.cpp:285  */
+    ASD2G_SOLVER_BICGSTAB = 2,     /* right-Jacobi BiCGStab (rho_2 carried)       */
+    ASD2G_SOLVER_BICGSTAB_REFERENCE = 3 /* poisson2d.cpp:403 as written (rho_2 = 1) */
+};
+
+typedef struct asd2g_params {
+    int32_t nx, ny;          /* interior cells (>= 4 each) */
+    int32_t nbc;             /* ghost layers: must be 3 (WENO5) */
+    int32_t precision;       /* 0: FP64 throughout (the drop-in) */
+    double base_x, base_y;   /* lower-left corner (only for bookkeeping) */
+    double dx, dy;           /* cell sizes */
+    int32_t bc_u[4], bc_v[4], bc_p[4];      /* asd2g_bc per side, order W, E, S, N */
+    double bcc_u[4], bcc_v[4], bcc_p[4];    /* Dirichlet constants per side */
+    double rho_h, rho_l, mu_h, mu_l;        /* heavy (phi > 0) and light fluid */
+    double sigma, gravity;                  /* surface tension, gravity constant */
+    int32_t g_axis;          /* GAXISENUM2D: 0 X, 1 Y */
+    int32_t fix_gravity;     /* 0: reproduce mac2d.cpp:294 (V takes AddGravityFU) */
+    int32_t time_order;      /* TIMEORDERENUM: 0 Euler, 1 RK2, 2 RK3 */
+    int32_t reserved0;
+    double cfl;
+    double ls_max_atime;     /* reinit pseudo-time; <= 0: 1.5*kThickness (levelset2d.cpp:10) */
+} asd2g_params;
+
+typedef struct asd2g_session asd2g_session;
+
+/* Version of this ABI (ASD2G_VERSION). */
+int asd2g_version(void);
+/* Human-readable text for the last error on this thread. */
+const char *asd2g_last_error(void);
+
+/* Create a session on the current CUDA device.  stream: a cudaStream_t, or
+ * NULL for a stream owned by the session.  Replaces the constructors
+ * LevelSetSolver2D(...) levelset2d.h:19-22, MACSolver2D(...) mac2d.h:75-84,
+ * PoissonSolver2D(nx, ny, nbc) poisson2d.h:33. */
+int asd2g_create(const asd2g_params *params, void *stream, asd2g_session **out);
+int asd2g_destroy(asd2g_session *s);
+int asd2g_sync(asd2g_session *s);
+
+/* Device pointer of a field ((nx+6)*(ny+6) doubles). */
+int asd2g_field_ptr(asd2g_session *s, int field, double **dptr);
+/* Host <-> device copies of a whole padded field (synchronous). */
+int asd2g_upload(asd2g_session *s, int field, const double *host);
+int asd2g_download(asd2g_session *s, int field, double *host);
+int asd2g_copy_field(asd2g_session *s, int dst, int src);
+int asd2g_fill_field(asd2g_session *s, int field, double value);
+
+/* Ghost fill of one field as a U, V or P grid (kind 'U', 'V', 'P').
+ * BoundaryCondition2D::ApplyBC_{U,V,P}_2D, bc2d.cpp:123,239,346. */
+int asd2g_apply_bc(asd2g_session *s, int field, char kind);
+
+/* ---- level set (levelset2d.cpp) ---- */
+/* Solve_LevelSet_2D(LS, U, V, dt): TVD-RK3 + HJ-WENO5, levelset2d.cpp:43. */
+int asd2g_ls_advect(asd2g_session *s, double dt);
+/* HJWENO5_LS_2D(ls, uc, vc) -> out (cell-centred velocities), :88.  Applies
+ * the P boundary to ls first, as the reference does. */
+int asd2g_ls_weno_rhs(asd2g_session *s, int ls, int uc, int vc, int out);
+/* Reinitialise LS in place (asd2g_reinit mode). */
+int asd2g_reinit(asd2g_session *s, int mode);
+/* Building blocks: SubcellENO_Min_DerivAbsLS_2D :616, ENO_DerivAbsLS_2D :560,
+ * GetSussmanReinitConstraint :787, UpdateHeavisideFuncDeriv :27,
+ * GetSmoothedSignFunc :914.  All write every cell of out the reference writes
+ * and zero the rest (fresh-vector semantics). */
+int asd2g_subcell_eno(asd2g_session *s, int ls, int ls0, int out);
+int asd2g_eno(asd2g_session *s, int ls, int ls0, int out);
+int asd2g_sussman_constraint(asd2g_session *s, int ls, int ls0, int hd, int out);
+int asd2g_heaviside_deriv(asd2g_session *s, int ls, int out);
+int asd2g_smoothed_sign(asd2g_session *s, int ls, int out);
+/* Level-set step: advect (dt) then reinitialise (mode). */
+int asd2g_ls_step(asd2g_session *s, double dt, int reinit_mode);
+
+/* ---- MAC momentum (mac2d.cpp) ---- */
+/* UpdateKappa(LS) -> KAPPA interior, mac2d.cpp:221. */
+int asd2g_kappa(asd2g_session *s);
+/* UpdateHeavisideFunc / UpdateSmoothHeavisideFunc(LS) -> H, HS, :87, :103. */
+int asd2g_heaviside(asd2g_session *s);
+/* AddConvectionFU/FV(u, v) -> cu, cv (:308, :389). */
+int asd2g_convection(asd2g_session *s, int u, int v, int cu, int cv);
+/* AddViscosityFU/FV(u, v, ls, h) -> du, dv (:570, :811). */
+int asd2g_viscosity(asd2g_session *s, int u, int v, int ls, int h, int du, int dv);
+/* UpdateFU/FV(ls, u, v, h) -> fu, fv (:254, :281). */
+int asd2g_momentum_rhs(asd2g_session *s, int ls, int u, int v, int h, int fu, int fv);
+/* GetIntermediateVel(LS, U, V, UHAT, VHAT, h) with time step dt, :1081.
+ * Writes the interior faces of UHAT and VHAT only, as the reference does. */
+int asd2g_intermediate_vel(asd2g_session *s, double dt, int h);
+/* GetDivergence(u, v) -> div, :1729. */
+int asd2g_divergence(asd2g_session *s, int u, int v, int div);
+/* UpdateVel(U, V, UHAT, VHAT, PS, LS, H) with KAPPA, :1740; then the U/V
+ * boundary fill the reference applies at its end. */
+int asd2g_update_vel(asd2g_session *s, double dt);
+/* UpdateDt(U, V), :1851. */
+int asd2g_update_dt(asd2g_session *s, double *dt);
+
+/* ---- GFM pressure (mac2d.cpp:1249-1727, poisson2d.cpp) ---- */
+/* Assemble the matrix-free GFM system from LS, KAPPA, H, DIV with time step
+ * dt.  recompute_kappa: recompute KAPPA from LS and fill its P ghosts first
+ * (what SolvePoisson does when kWe is finite and nonzero, :1307-1310). */
+int asd2g_assemble_gfm(asd2g_session *s, double dt, int recompute_kappa);
+/* Copy the assembled system to the host in the reference's natural order
+ * k = i + nx*j: diagonal, west/east/south/north coupling magnitudes (the
+ * off-diagonal entries are their negatives) and right-hand side.  Any pointer
+ * may be NULL.  *pinned = 1 when cell 0 is held at 0 (all-Neumann pressure). */
+int asd2g_get_system(asd2g_session *s, double *diag, double *cw, double *ce, double *cs, double *cn,
+                     double *rhs, int *pinned);
+/* Solve the assembled system into PS (interior; P ghosts filled), and set
+ * P = PS / dt.  tol is on ||b - A x|| / ||b||.  Returns ASD2G_NOT_CONVERGED
+ * when maxit is reached.  iters and rel_resid (recurrence) may be NULL. */
+int asd2g_solve_pressure(asd2g_session *s, int solver, double tol, int maxit, double dt, int *iters,
+                         double *rel_resid);
+/* ||b - A x|| / ||b|| of the current PS against the assembled system, in FP64. */
+int asd2g_true_residual(asd2g_session *s, double *rel);
+
+/* ---- whole step (test_mac2d_large.cpp:496-552) ----
+ * lsB = LS; advect; reinit (reinit_mode); kappa; H, HS; intermediate velocity
+ * with HS; U/V fill; divergence; GFM assembly; pressure solve; projection;
+ * new dt.  *dt is read as the step's dt and receives the next one. */
+int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver, double tol, int maxit,
+                       int *iters, double *rel_resid);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

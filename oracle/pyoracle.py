@@ -315,6 +315,7 @@ class Oracle:
         p[3:-3, 3:-3] = ps[3:-3, 3:-3] / dt
         st["p"] = p
         self.update_vel(g, f, dt, u, v, uh, vh, ps, ls, H, st["kappa"])
+        st["dt_used"] = dt
         st["dt"] = self.update_dt(g, f, u, v)
         st["lsB"] = lsB
         return dict(iters=it, resid=res, true_resid=tres, sys=sysd, div=div, H=H, HS=HS, uhat=uh, vhat=vh)

@@ -1,0 +1,69 @@
+"""Shared test helpers: golden fixtures and grid/parameter conversions."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+from oracle.pyoracle import FluidSpec, GridSpec
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_golden.npz")
+GRIDS = {"A": (24, 20, 1.0 / 24, 1.0 / 20), "B": (32, 16, 1.0 / 32, 1.0 / 32)}
+
+_gold = None
+
+
+def golden():
+    global _gold
+    if _gold is None:
+        _gold = dict(np.load(GOLDEN))
+    return _gold
+
+
+def ls_grid(name) -> GridSpec:
+    nx, ny, dx, dy = GRIDS[name]
+    return GridSpec(nx, ny, dx, dy, bc_u=("neumann",) * 4, bc_v=("neumann",) * 4, bc_p=("neumann",) * 4)
+
+
+def mac_grid(name) -> GridSpec:
+    nx, ny, dx, dy = GRIDS[name]
+    return GridSpec(nx, ny, dx, dy)
+
+
+def params_for(g: GridSpec, f: FluidSpec | None = None, **kw):
+    from asd2_b200.api import Params
+    f = f or FluidSpec()
+    return Params(g.nx, g.ny, g.dx, g.dy, bc_u=g.bc_u, bc_v=g.bc_v, bc_p=g.bc_p, bcc_u=g.cu, bcc_v=g.cv,
+                  bcc_p=g.cp, rho_h=f.rho_h, rho_l=f.rho_l, mu_h=f.mu_h, mu_l=f.mu_l, sigma=f.sigma, g=f.g,
+                  g_axis=f.g_axis, fix_gravity=f.fix_gravity, time_order=f.time_order, cfl=f.cfl, **kw)
+
+
+def grid_from_case(c) -> GridSpec:
+    return GridSpec(c.nx, c.ny, c.dx, c.dy, bc_u=c.bc_u, bc_v=c.bc_v, bc_p=c.bc_p)
+
+
+def fluid_from_case(c) -> FluidSpec:
+    return FluidSpec(**c.fluid) if c.fluid else FluidSpec()
+
+
+def interior(a):
+    return a[3:-3, 3:-3]
+
+
+def assert_bitexact(a, b, what=""):
+    a, b = np.asarray(a), np.asarray(b)
+    if not np.array_equal(a, b):
+        d = np.abs(a - b)
+        idx = np.unravel_index(np.argmax(d), d.shape)
+        raise AssertionError(f"{what}: not bit-identical; max |diff| {d.max():.3e} at {idx} "
+                             f"({a[idx]!r} vs {b[idx]!r}); {np.count_nonzero(a != b)} cells differ")
+
+
+def assert_close(a, b, rtol, atol=0.0, what=""):
+    a, b = np.asarray(a), np.asarray(b)
+    d = np.abs(a - b)
+    lim = atol + rtol * np.abs(b)
+    if not np.all(d <= lim):
+        idx = np.unravel_index(np.argmax(d - lim), d.shape)
+        raise AssertionError(f"{what}: max |diff| {d.max():.3e} exceeds tolerance at {idx} "
+                             f"({a[idx]!r} vs {b[idx]!r})")

@@ -1,0 +1,58 @@
+"""CPU: the C-ABI library loads and exports every entry point that
+include/*.h declares (no compute call: there is no GPU here)."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+from asd2_b200 import api
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\*?\s*(asd2g_[a-z0-9_]+)\s*\(", src, re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    assert "asd2g_create" in names and "asd2g_droplet_step" in names
+    assert len(names) >= 30
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(api.LIB_PATH)
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_the_header():
+    assert set(declared_symbols()) <= set(api.EXPORTS)
+
+
+def test_version():
+    assert api.load().asd2g_version() == 1
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    api_mod = api
+    with pytest.raises(ImportError):
+        api_mod._lib_saved = api_mod._lib
+        try:
+            api_mod._lib = None
+            api_mod.load(str(tmp_path / "nope.so"))
+        finally:
+            api_mod._lib = api_mod._lib_saved
+
+
+def test_params_struct_matches_header():
+    # asd2g_params: 4 int32, 4 double, 12 int32, 12 double, 6 double, 4 int32, 2 double
+    assert ctypes.sizeof(api._Params) == 4 * 4 + 4 * 8 + 12 * 4 + 12 * 8 + 6 * 8 + 4 * 4 + 2 * 8
