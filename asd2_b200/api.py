@@ -59,7 +59,7 @@ EXPORTS = [
     "asd2g_kappa", "asd2g_heaviside", "asd2g_convection", "asd2g_viscosity", "asd2g_momentum_rhs",
     "asd2g_intermediate_vel", "asd2g_divergence", "asd2g_update_vel", "asd2g_update_dt",
     "asd2g_assemble_gfm", "asd2g_get_system", "asd2g_solve_pressure", "asd2g_true_residual",
-    "asd2g_droplet_step",
+    "asd2g_droplet_step", "asd2g_pcg_solve_static",
 ]
 
 _lib = None
@@ -97,6 +97,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_solve_pressure": ([S, I, D, I, D, C.POINTER(I), C.POINTER(D)], I),
         "asd2g_true_residual": ([S, C.POINTER(D)], I),
         "asd2g_droplet_step": ([S, C.POINTER(D), I, I, D, I, C.POINTER(I), C.POINTER(D)], I),
+        "asd2g_pcg_solve_static": ([I, I, I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, D, I,
+                                    C.c_void_p, C.POINTER(I), C.POINTER(D)], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

@@ -26,6 +26,7 @@ UNITS = {
     "momentum.cu": ["-fmad=false"],
     "pressure.cu": ["-fmad=false"],
     "api.cu": [],
+    "pcg_static.cu": ["-fmad=false"],
 }
 
 

@@ -88,6 +88,8 @@ int kind_p(int bc) {
 }
 }  // namespace
 
+void asd2g::asd2g_set_error_text(const char *msg) { snprintf(g_err, sizeof(g_err), "%s", msg ? msg : ""); }
+
 struct asd2g_session {
     asd2g_params prm;
     Grid g;

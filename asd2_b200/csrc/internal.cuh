@@ -17,6 +17,9 @@ struct DivH {
 };
 DivH make_divh(double h);
 
+// api.cu: set the thread's last-error text (read by asd2g_last_error)
+void asd2g_set_error_text(const char *msg);
+
 // bc.cu
 void launch_fill_uv(const Grid &g, double *u, double *v, cudaStream_t st);
 void launch_fill_p(const Grid &g, double *a, cudaStream_t st);

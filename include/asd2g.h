@@ -194,6 +194,31 @@ int asd2g_true_residual(asd2g_session *s, double *rel);
 int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver, double tol, int maxit,
                        int *iters, double *rel_resid);
 
+/* ---- allocation-free solve (no counterpart in the reference) ----
+ * Jacobi-PCG (textbook recurrence, FP64) on a system the caller has already
+ * assembled, for callers that cannot call cudaMalloc: a host that owns all
+ * device memory through its own pool and hands out only pre-registered
+ * buffers, a latency-critical loop where cudaMalloc/cudaFree would implicitly
+ * synchronise the device, or a process that has reserved the whole GPU.  It
+ * allocates nothing: its work space is a fixed file-scope device array of
+ * ASD2G_STATIC_MAX_UNKNOWNS unknowns (about 10 MiB, held on every GPU that
+ * loads the library until exit); larger systems are rejected with
+ * ASD2G_E_ARG.  The system is given in the compact interior layout
+ * k = j + ny*i (0-based interior indices, y fastest), as device arrays of
+ * nx*ny doubles: diag, and the east/north couplings ce, cn (the matrix
+ * entries are -ce and -cn; west/south couplings are the neighbours' ce/cn).
+ * pinned = 1 holds cell 0 at 0 (b[0] must then be 0).  x receives the
+ * solution.  All work runs on `stream` (a cudaStream_t, NULL = legacy
+ * stream) and the call returns when the solve has finished.
+ * The first call on a device looks up the array's address (with that device
+ * current) and caches it; make that first call before any stream capture.
+ * Every call shares the array, which keeps the last call's contents; each
+ * call resets what it reads first, and calls that overlap on the GPU race. */
+#define ASD2G_STATIC_MAX_UNKNOWNS (512 * 512)
+int asd2g_pcg_solve_static(int nx, int ny, int pinned, const double *diag, const double *ce, const double *cn,
+                           const double *b, double *x, double tol, int maxit, void *stream, int *iters,
+                           double *rel_resid);
+
 #ifdef __cplusplus
 }
 #endif
