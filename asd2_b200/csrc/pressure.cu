@@ -15,38 +15,58 @@
 namespace asd2g {
 
 // ---------------------------------------------------------------- reduce --
-// Sum NV per-thread values over the grid.  Returns true on thread 0 of the
-// last block, with the grid totals in tot.
+// Block-wide sum of NV values per thread; thread 0 receives the totals.
+// Fixed order (warp shuffles, then warps in index order): deterministic.
 template <int NV>
-__device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *partial, unsigned *counter, double (&tot)[NV]) {
-    __shared__ double sh[NV][32];
-    __shared__ bool last;
+__device__ __forceinline__ void block_sum(double (&v)[NV], double (&sh)[NV][32]) {
 #pragma unroll
     for (int q = 0; q < NV; q++)
         for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __syncthreads();  // sh may still be read from a previous use
     if (lane == 0)
 #pragma unroll
         for (int q = 0; q < NV; q++) sh[q][wid] = v[q];
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (wid == 0) {
 #pragma unroll
         for (int q = 0; q < NV; q++) {
-            double s = 0.0;
-            for (int w = 0; w < nw; w++) s += sh[q][w];
-            partial[NV * blockIdx.x + q] = s;
+            double s = lane < nw ? sh[q][lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+            v[q] = s;
         }
+    }
+}
+
+// Sum NV per-thread values over the grid.  Every block writes its partial;
+// the last block to take a ticket sums the partials with all its threads
+// (strided, then block_sum), so the result does not depend on which block
+// finishes last.  Returns true on thread 0 of the last block, with the
+// totals in tot.
+template <int NV>
+__device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *partial, unsigned *counter, double (&tot)[NV]) {
+    __shared__ double sh[NV][32];
+    __shared__ bool last;
+    block_sum<NV>(v, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; q++) partial[NV * blockIdx.x + q] = v[q];
         __threadfence();
         last = atomicAdd(counter, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (!(last && threadIdx.x == 0)) return false;
+    if (!last) return false;
     __threadfence();
+    double a[NV];
 #pragma unroll
-    for (int q = 0; q < NV; q++) tot[q] = 0.0;
-    for (unsigned b = 0; b < gridDim.x; b++)
+    for (int q = 0; q < NV; q++) a[q] = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
 #pragma unroll
-        for (int q = 0; q < NV; q++) tot[q] += ((volatile double *)partial)[NV * b + q];
+        for (int q = 0; q < NV; q++) a[q] += __ldcg(partial + NV * b + q);
+    block_sum<NV>(a, sh);
+    if (threadIdx.x != 0) return false;
+#pragma unroll
+    for (int q = 0; q < NV; q++) tot[q] = a[q];
     *counter = 0u;
     return true;
 }
