@@ -30,6 +30,7 @@ REINIT_ORIGINAL, REINIT_SUSSMAN, REINIT_MINRK2, REINIT_FIRSTTIME, REINIT_MINRK2_
 # solvers
 PCG, PCG_REFERENCE, BICGSTAB, BICGSTAB_REFERENCE = range(4)
 NOT_CONVERGED = 1
+FLAG_NO_CLUSTER_PCG = 1
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "unsupported",
           -5: "non-finite value", -6: "Krylov breakdown"}
 
@@ -47,7 +48,7 @@ class _Params(C.Structure):
                 ("bcc_u", C.c_double * 4), ("bcc_v", C.c_double * 4), ("bcc_p", C.c_double * 4),
                 ("rho_h", C.c_double), ("rho_l", C.c_double), ("mu_h", C.c_double), ("mu_l", C.c_double),
                 ("sigma", C.c_double), ("gravity", C.c_double), ("g_axis", C.c_int32), ("fix_gravity", C.c_int32),
-                ("time_order", C.c_int32), ("reserved0", C.c_int32), ("cfl", C.c_double),
+                ("time_order", C.c_int32), ("solver_flags", C.c_int32), ("cfl", C.c_double),
                 ("ls_max_atime", C.c_double)]
 
 
@@ -138,6 +139,7 @@ class Params:
     base_x: float = 0.0
     base_y: float = 0.0
     precision: int = 0
+    solver_flags: int = 0
 
     def c(self) -> _Params:
         p = _Params()
@@ -149,6 +151,7 @@ class Params:
         p.rho_h, p.rho_l, p.mu_h, p.mu_l = self.rho_h, self.rho_l, self.mu_h, self.mu_l
         p.sigma, p.gravity, p.g_axis, p.fix_gravity = self.sigma, self.g, self.g_axis, self.fix_gravity
         p.time_order, p.cfl, p.ls_max_atime = self.time_order, self.cfl, self.ls_max_atime
+        p.solver_flags = self.solver_flags
         return p
 
     @classmethod

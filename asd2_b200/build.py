@@ -27,6 +27,7 @@ UNITS = {
     "pressure.cu": ["-fmad=false"],
     "api.cu": [],
     "pcg_static.cu": ["-fmad=false"],
+    "pcg_cluster.cu": ["-fmad=false"],
 }
 
 

@@ -552,6 +552,24 @@ static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters
     const int mode = solver;  // 0 PCG, 1 PCG (reference), 2 BiCGStab, 3 BiCGStab (reference)
     const double reg = solver == 1 ? 1.0e-12 : 0.0;  // err_tol^2 in alpha (poisson2d.cpp:354)
     launch_set_kstate(s->ks, tol, maxit, mode, reg, s->st);
+    if (solver == 0 && !(s->prm.solver_flags & ASD2G_FLAG_NO_CLUSTER_PCG) &&
+        launch_pcg_cluster(g.nx, g.ny, s->sys, s->x, s->ks, tol, maxit, s->st)) {
+        // one launch ran the whole solve
+        if (stream_capturing(s)) {
+            if (iters) *iters = -1;
+            if (resid) *resid = -1.0;
+            return cuda_check("cluster pcg");
+        }
+        cudaMemcpyAsync(s->ks_host, s->ks, sizeof(KState), cudaMemcpyDeviceToHost, s->st);
+        int rc2 = sync(s);
+        if (rc2) return rc2;
+        const KState &k = *s->ks_host;
+        if (iters) *iters = k.it;
+        if (resid) *resid = k.res;
+        if (k.status == -5) return fail(ASD2G_E_NONFINITE, "non-finite residual at iteration %d", k.it);
+        if (k.status == -6) return fail(ASD2G_E_BREAKDOWN, "Krylov breakdown at iteration %d", k.it);
+        return !(k.res > tol) ? ASD2G_OK : ASD2G_NOT_CONVERGED;
+    }
     if (solver <= 1) launch_pcg_init(g, s->sys, s->x, s->r, s->pa, s->ks, s->partial, s->st);
     else launch_bicg_init(g, s->sys, s->x, s->r, s->rt, s->pa, s->q, s->ks, s->partial, s->st);
     int rc = cuda_check("solver init");

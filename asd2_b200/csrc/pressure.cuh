@@ -43,5 +43,10 @@ void launch_scatter_ps(const Grid &g, const double *x, double *ps, double *p, co
 void launch_true_residual(const Grid &g, const Sys &S, const double *ps, double *partial, double *out2,
                           cudaStream_t st);
 void launch_set_kstate(KState *ks, double tol, int maxit, int mode, double reg, cudaStream_t st);
+// pcg_cluster.cu: whole textbook PCG solve in one thread-block cluster;
+// false when the system does not fit one cluster or cannot be scheduled.
+int pcg_cluster_size(int nx, int ny);
+bool launch_pcg_cluster(int nx, int ny, const Sys &S, double *x, KState *ks, double tol, int maxit,
+                        cudaStream_t st);
 
 }  // namespace asd2g

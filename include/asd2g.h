@@ -81,6 +81,9 @@ enum asd2g_solver {
     ASD2G_SOLVER_BICGSTAB_REFERENCE = 3 /* poisson2d.cpp:403 as written (rho_2 = 1) */
 };
 
+/* solver_flags bits */
+#define ASD2G_FLAG_NO_CLUSTER_PCG 1 /* Jacobi-PCG always as per-iteration kernels (no cluster solver) */
+
 typedef struct asd2g_params {
     int32_t nx, ny;          /* interior cells (>= 4 each) */
     int32_t nbc;             /* ghost layers: must be 3 (WENO5) */
@@ -94,7 +97,7 @@ typedef struct asd2g_params {
     int32_t g_axis;          /* GAXISENUM2D: 0 X, 1 Y */
     int32_t fix_gravity;     /* 0: reproduce mac2d.cpp:294 (V takes AddGravityFU) */
     int32_t time_order;      /* TIMEORDERENUM: 0 Euler, 1 RK2, 2 RK3 */
-    int32_t reserved0;
+    int32_t solver_flags;    /* ASD2G_FLAG_* bits (0 = defaults) */
     double cfl;
     double ls_max_atime;     /* reinit pseudo-time; <= 0: 1.5*kThickness (levelset2d.cpp:10) */
 } asd2g_params;

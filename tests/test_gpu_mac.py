@@ -111,14 +111,16 @@ def _pressure_case(n=48, seed=2, bc_p=("neumann",) * 4, cp=(0.0,) * 4):
 
 
 @pytest.mark.parametrize("bc", ["neumann", "dirichlet"])
-@pytest.mark.parametrize("solver", [api.PCG, api.BICGSTAB])
-def test_pressure_solve(bc, solver):
+@pytest.mark.parametrize("solver,flags", [(api.PCG, 0), (api.PCG, api.FLAG_NO_CLUSTER_PCG), (api.BICGSTAB, 0)])
+def test_pressure_solve(bc, solver, flags):
+    """PCG runs as one cluster-resident launch by default and as per-iteration
+    kernels with FLAG_NO_CLUSTER_PCG; both must match the restatement."""
     g, f, ls, H, div = _pressure_case(bc_p=(bc,) * 4, cp=(0.0, 0.5, 0.0, 1.0) if bc == "dirichlet" else (0.0,) * 4)
     dt = 1e-3
     kap = O.kappa(g, ls)
     sysd = O.gfm_assemble(g, f, dt, ls, kap, H, div, recompute_kappa=True)
     x_ref, it_ref, _, tres_ref = O.pcg(g, sysd, tol=1e-12, maxit=100000)
-    with api.Session(params_for(g, f)) as s:
+    with api.Session(params_for(g, f, solver_flags=flags)) as s:
         s.upload("ls", ls)
         s.upload("H", H)
         s.upload("div", div)
