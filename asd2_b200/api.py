@@ -28,7 +28,7 @@ FIELDS = dict(ls=LS, u=U, v=V, ps=PS, p=P, kappa=KAPPA, H=H, HS=HS, div=DIV, uha
 # reinit modes
 REINIT_ORIGINAL, REINIT_SUSSMAN, REINIT_MINRK2, REINIT_FIRSTTIME, REINIT_MINRK2_SUSSMAN = range(5)
 # solvers
-PCG, PCG_REFERENCE, BICGSTAB, BICGSTAB_REFERENCE = range(4)
+PCG, PCG_REFERENCE, BICGSTAB, BICGSTAB_REFERENCE, MGPCG = range(5)
 NOT_CONVERGED = 1
 FLAG_NO_CLUSTER_PCG = 1
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "unsupported",

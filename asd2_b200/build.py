@@ -28,6 +28,7 @@ UNITS = {
     "api.cu": [],
     "pcg_static.cu": ["-fmad=false"],
     "pcg_cluster.cu": ["-fmad=false"],
+    "mg.cu": [],
 }
 
 

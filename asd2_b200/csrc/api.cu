@@ -7,7 +7,7 @@
 #include <vector>
 
 #include "asd2g.h"
-#include "pressure.cuh"
+#include "mg.cuh"
 
 namespace asd2g {
 // levelset.cu
@@ -110,7 +110,11 @@ struct asd2g_session {
     double *dsc = nullptr;       // [0] dt of the step, [1] next dt, [2..3] residual sums, [4] counter
     double *dsc_host = nullptr;  // pinned mirror
     bool assembled = false;
-    cudaGraphExec_t chunk_exec[4] = {};
+    cudaGraphExec_t chunk_exec[5] = {};
+    // multigrid preconditioner (allocated on first use)
+    MgLevel lv[MG_MAX_LEVELS] = {};
+    int nlev = 0;
+    double *coarse_inv = nullptr, *z = nullptr;
     int chunk_len = 64;
     std::vector<void *> allocs;
 };
@@ -122,6 +126,33 @@ int dalloc(asd2g_session *s, double **p, size_t n) {
         return fail(ASD2G_E_NOMEM, "cudaMalloc of %zu doubles failed", n);
     }
     s->allocs.push_back(*p);
+    return ASD2G_OK;
+}
+
+int mg_alloc(asd2g_session *s) {
+    if (s->nlev) return ASD2G_OK;
+    int dims[2 * MG_MAX_LEVELS];
+    const int n = mg_levels_for(s->g.nx, s->g.ny, dims, MG_MAX_LEVELS);
+    if (n < 2) return fail(ASD2G_E_UNSUPPORTED, "grid too small for the multigrid preconditioner");
+    for (int l = 0; l < n; l++) {
+        MgLevel &L = s->lv[l];
+        L.nx = dims[2 * l];
+        L.ny = dims[2 * l + 1];
+        const size_t m = (size_t)L.nx * L.ny;
+        float **arrs[] = {&L.diag, &L.ce, &L.cn, &L.f, &L.e};
+        for (float **a : arrs) {
+            if (cudaMalloc(a, sizeof(float) * m) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(ASD2G_E_NOMEM, "multigrid level allocation failed");
+            }
+            s->allocs.push_back(*a);
+            cudaMemsetAsync(*a, 0, sizeof(float) * m, s->st);
+        }
+    }
+    int rc = dalloc(s, &s->coarse_inv, (size_t)MG_COARSE_CELLS * MG_COARSE_CELLS);
+    if (rc == ASD2G_OK) rc = dalloc(s, &s->z, s->N);
+    if (rc) return rc;
+    s->nlev = n;
     return ASD2G_OK;
 }
 
@@ -147,7 +178,14 @@ bool stream_capturing(asd2g_session *s) {
 void enqueue_iters(asd2g_session *s, int solver, int count) {
     const Grid &g = s->g;
     for (int k = 0; k < count; k++) {
-        if (solver <= 1) {
+        if (solver == ASD2G_SOLVER_MGPCG) {
+            if (k % 2 == 0)
+                launch_fcg_iter(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->pa, s->pb, s->q,
+                                s->z, s->ks, s->partial, s->st);
+            else
+                launch_fcg_iter(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->pb, s->pa, s->q,
+                                s->z, s->ks, s->partial, s->st);
+        } else if (solver <= 1) {
             if (k % 2 == 0) launch_pcg_iter(g, s->sys, s->x, s->r, s->pa, s->pb, s->q, s->ks, s->partial, s->st);
             else launch_pcg_iter(g, s->sys, s->x, s->r, s->pb, s->pa, s->q, s->ks, s->partial, s->st);
         } else {
@@ -535,7 +573,7 @@ int asd2g_get_system(asd2g_session *s, double *diag, double *cw, double *ce, dou
 static int capture_chunk(asd2g_session *s, int solver) {
     cudaGraph_t graph = nullptr;
     if (cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return cuda_check("capture begin");
-    enqueue_iters(s, solver, s->chunk_len);
+    enqueue_iters(s, solver, solver == ASD2G_SOLVER_MGPCG ? 8 : s->chunk_len);
     if (cudaStreamEndCapture(s->st, &graph) != cudaSuccess) return cuda_check("capture end");
     cudaGraphExec_t ex = nullptr;
     if (cudaGraphInstantiate(&ex, graph, 0) != cudaSuccess) {
@@ -549,7 +587,7 @@ static int capture_chunk(asd2g_session *s, int solver) {
 
 static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters, double *resid) {
     const Grid &g = s->g;
-    const int mode = solver;  // 0 PCG, 1 PCG (reference), 2 BiCGStab, 3 BiCGStab (reference)
+    const int mode = solver;  // 0 PCG, 1 PCG (reference), 2 BiCGStab, 3 BiCGStab (reference), 4 MG-FCG
     const double reg = solver == 1 ? 1.0e-12 : 0.0;  // err_tol^2 in alpha (poisson2d.cpp:354)
     launch_set_kstate(s->ks, tol, maxit, mode, reg, s->st);
     if (solver == 0 && !(s->prm.solver_flags & ASD2G_FLAG_NO_CLUSTER_PCG) &&
@@ -570,11 +608,17 @@ static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters
         if (k.status == -6) return fail(ASD2G_E_BREAKDOWN, "Krylov breakdown at iteration %d", k.it);
         return !(k.res > tol) ? ASD2G_OK : ASD2G_NOT_CONVERGED;
     }
-    if (solver <= 1) launch_pcg_init(g, s->sys, s->x, s->r, s->pa, s->ks, s->partial, s->st);
+    if (solver == ASD2G_SOLVER_MGPCG) {
+        int rc0 = mg_alloc(s);
+        if (rc0) return rc0;
+        launch_mg_setup(s->sys, s->lv, s->nlev, s->coarse_inv, s->st);
+        launch_fcg_init(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->pa, s->q, s->z, s->ks,
+                        s->partial, s->st);
+    } else if (solver <= 1) launch_pcg_init(g, s->sys, s->x, s->r, s->pa, s->ks, s->partial, s->st);
     else launch_bicg_init(g, s->sys, s->x, s->r, s->rt, s->pa, s->q, s->ks, s->partial, s->st);
     int rc = cuda_check("solver init");
     if (rc) return rc;
-    const int chunk = s->chunk_len;
+    const int chunk = solver == ASD2G_SOLVER_MGPCG ? 8 : s->chunk_len;
     if (stream_capturing(s)) {
         // Inside a caller's capture: enqueue maxit iterations (each returns at
         // entry once converged); no host polling is possible.
@@ -601,14 +645,14 @@ static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters
     if (resid) *resid = k.res;
     if (k.status == -5) return fail(ASD2G_E_NONFINITE, "non-finite residual at iteration %d", k.it);
     if (k.status == -6) return fail(ASD2G_E_BREAKDOWN, "Krylov breakdown at iteration %d", k.it);
-    const bool conv = solver == 0 ? !(k.res > tol) : (k.res <= tol);
+    const bool conv = (solver == 0 || solver == ASD2G_SOLVER_MGPCG) ? !(k.res > tol) : (k.res <= tol);
     return conv ? ASD2G_OK : ASD2G_NOT_CONVERGED;
 }
 
 int asd2g_solve_pressure(asd2g_session *s, int solver, double tol, int maxit, double dt, int *iters,
                          double *rel_resid) {
     if (!s) return fail(ASD2G_E_ARG, "null session");
-    if (solver < 0 || solver > 3) return fail(ASD2G_E_ARG, "solver %d out of range", solver);
+    if (solver < 0 || solver > 4) return fail(ASD2G_E_ARG, "solver %d out of range", solver);
     if (!s->assembled) return fail(ASD2G_E_ARG, "assemble the system first");
     if (maxit < 0) return fail(ASD2G_E_ARG, "maxit must be >= 0");
     int rc = set_dt(s, dt);

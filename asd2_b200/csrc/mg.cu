@@ -1,0 +1,503 @@
+// Mixed-precision multigrid-preconditioned flexible CG for the GFM system.
+//
+// Outer solver: flexible CG (Polak-Ribiere beta) in FP64 on the assembled
+// system (x, r, p, q FP64; the residual that decides convergence is the FP64
+// recurrence residual, checked against the true FP64 residual by the host).
+// Preconditioner: one symmetric V(1,1)-cycle in FP32 of cell-centred
+// geometric multigrid:
+//   * coarse operators by Galerkin aggregation of 2x2 cells (piecewise-
+//     constant prolongation P, restriction R = P^T): coarse face couplings are
+//     the sums of the fine couplings across the coarse face, the coarse
+//     diagonal the aggregate's row sums; 5-point, SPD, and exact across the
+//     density jumps (no coefficient averaging);
+//   * red-black Gauss-Seidel smoothing, red then black before restriction and
+//     black then red after prolongation (the adjoint), so the cycle is
+//     symmetric; the prolonged correction is over-relaxed by omega = 1.9,
+//     which compensates the piecewise-constant coarse space;
+//   * the coarsest level (<= 64 cells) is solved exactly with its dense
+//     inverse, formed once per assembly.
+// Each level costs two kernels: "pre" = red sweep + black sweep + residual +
+// restriction, "post" = prolongation + black sweep + red sweep.  A 16 x 32
+// tile loads a two-cell halo into shared memory and recomputes the halo's
+// red/black values itself, so one kernel produces exactly the result of the
+// separate sweeps (no grid-wide barrier between them).  The level-0 "post"
+// kernel also converts z to FP64 and forms the two FCG dot products.
+#include "lsmath.cuh"
+#include "mg.cuh"
+
+namespace asd2g {
+
+namespace {
+
+constexpr int MT_I = 16, MT_J = 32;  // tile (rows i, columns j), must be even
+constexpr int MG_COARSE_MAX = 64;   // cells on the coarsest level
+constexpr int HI = MT_I + 4, HJ = MT_J + 4;
+
+// block sum and grid reduction (same fixed-order scheme as pressure.cu)
+template <int NV>
+__device__ __forceinline__ void mg_block_sum(double (&v)[NV], double (&sh)[NV][32]) {
+#pragma unroll
+    for (int q = 0; q < NV; q++)
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int lane = tid & 31, wid = tid >> 5, nw = (blockDim.x * blockDim.y) >> 5;
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NV; q++) sh[q][wid] = v[q];
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; q++) {
+            double s = lane < nw ? sh[q][lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+            v[q] = s;
+        }
+    }
+}
+
+template <int NV>
+__device__ __forceinline__ bool mg_grid_reduce(double (&v)[NV], double *partial, unsigned *counter,
+                                               double (&tot)[NV]) {
+    __shared__ double sh[NV][32];
+    __shared__ bool last;
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const unsigned bid = blockIdx.x + gridDim.x * blockIdx.y, nb = gridDim.x * gridDim.y;
+    mg_block_sum<NV>(v, sh);
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; q++) partial[NV * bid + q] = v[q];
+        __threadfence();
+        last = atomicAdd(counter, 1u) == nb - 1;
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    double a[NV];
+#pragma unroll
+    for (int q = 0; q < NV; q++) a[q] = 0.0;
+    for (unsigned b = tid; b < nb; b += blockDim.x * blockDim.y)
+#pragma unroll
+        for (int q = 0; q < NV; q++) a[q] += __ldcg(partial + NV * b + q);
+    mg_block_sum<NV>(a, sh);
+    if (tid != 0) return false;
+#pragma unroll
+    for (int q = 0; q < NV; q++) tot[q] = a[q];
+    *counter = 0u;
+    return true;
+}
+
+__device__ __forceinline__ int64_t LK(const MgLevel &L, int i, int j) { return (int64_t)j + (int64_t)L.ny * i; }
+
+// ------------------------------------------------------------- set-up --
+// Level 0 in FP32 from the assembled FP64 system; the pinned cell keeps its
+// diagonal and loses its couplings (its rhs is always 0, so it stays 0).
+__global__ void k_mg_l0(int nx, int ny, Sys S, MgLevel L) {
+    const int64_t n = (int64_t)nx * ny;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(k / ny), j = (int)(k % ny);
+        const bool pin0 = S.pinned && k == 0;
+        L.diag[k] = (float)S.diag[k];
+        L.ce[k] = (i < nx - 1 && !pin0) ? (float)S.ce[k] : 0.0f;
+        L.cn[k] = (j < ny - 1 && !pin0) ? (float)S.cn[k] : 0.0f;
+    }
+}
+
+// Galerkin aggregation R A P with piecewise-constant P (2x2 aggregates; the
+// last aggregate of an odd dimension has one cell in that direction).
+__global__ void k_mg_coarsen(MgLevel F, MgLevel C) {
+    const int64_t n = (int64_t)C.nx * C.ny;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int I = (int)(k / C.ny), J = (int)(k % C.ny);
+        const int i0 = 2 * I, j0 = 2 * J;
+        const bool hi = i0 + 1 < F.nx, hj = j0 + 1 < F.ny;
+        float d = F.diag[LK(F, i0, j0)];
+        if (hi) d += F.diag[LK(F, i0 + 1, j0)];
+        if (hj) d += F.diag[LK(F, i0, j0 + 1)];
+        if (hi && hj) d += F.diag[LK(F, i0 + 1, j0 + 1)];
+        float inner = 0.0f;
+        if (hi) inner += F.ce[LK(F, i0, j0)];
+        if (hi && hj) inner += F.ce[LK(F, i0, j0 + 1)];
+        if (hj) inner += F.cn[LK(F, i0, j0)];
+        if (hi && hj) inner += F.cn[LK(F, i0 + 1, j0)];
+        C.diag[k] = d - 2.0f * inner;
+        const int ie = hi ? i0 + 1 : i0, je = hj ? j0 + 1 : j0;
+        float ce = F.ce[LK(F, ie, j0)];
+        if (hj) ce += F.ce[LK(F, ie, j0 + 1)];
+        float cn = F.cn[LK(F, i0, je)];
+        if (hi) cn += F.cn[LK(F, i0 + 1, je)];
+        C.ce[k] = ce;
+        C.cn[k] = cn;
+    }
+}
+
+// ---------------------------------------------------------- tile loads --
+struct Tile {
+    float e[HI][HJ], f[HI][HJ], d[HI][HJ], ce[HI][HJ], cn[HI][HJ];
+};
+
+// Load f, d, ce, cn on the tile + 2-cell halo (out of domain: f 0, d 1,
+// couplings 0).  Level 0 reads f from the FP64 residual.
+template <bool L0>
+__device__ __forceinline__ void load_tile(Tile &T, const MgLevel &L, const double *__restrict__ r64, int i0, int j0) {
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
+    for (int t = tid; t < HI * HJ; t += nt) {
+        const int a = t / HJ, b = t % HJ;
+        const int i = i0 - 2 + a, j = j0 - 2 + b;
+        float f = 0.0f, d = 1.0f, ce = 0.0f, cn = 0.0f;
+        if (i >= 0 && i < L.nx && j >= 0 && j < L.ny) {
+            const int64_t k = LK(L, i, j);
+            f = L0 ? (float)r64[k] : L.f[k];
+            d = L.diag[k];
+            ce = L.ce[k];
+            cn = L.cn[k];
+        }
+        T.f[a][b] = f;
+        T.d[a][b] = d;
+        T.ce[a][b] = ce;
+        T.cn[a][b] = cn;
+    }
+}
+
+// Gauss-Seidel update of local cell (a, b) from its four neighbours.
+__device__ __forceinline__ float gs_cell(const Tile &T, int a, int b) {
+    const float s = T.f[a][b] + T.ce[a - 1][b] * T.e[a - 1][b] + T.ce[a][b] * T.e[a + 1][b] +
+                    T.cn[a][b - 1] * T.e[a][b - 1] + T.cn[a][b] * T.e[a][b + 1];
+    return s / T.d[a][b];
+}
+
+// ------------------------------------------------------------ pre pass --
+// From e = 0: red sweep on tile+2, black on tile+1, residual on the tile,
+// restriction (2x2 sums) into the next level's f.  Stores e (tile).
+template <bool L0>
+__global__ void __launch_bounds__(256) k_mg_pre(MgLevel L, MgLevel C, const double *__restrict__ r64,
+                                                const KState *ks) {
+    if (ks->done) return;
+    __shared__ Tile T;
+    __shared__ float res[MT_I][MT_J];
+    const int i0 = blockIdx.y * MT_I, j0 = blockIdx.x * MT_J;
+    load_tile<L0>(T, L, r64, i0, j0);
+    __syncthreads();
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
+    // red (i+j even) on tile+2 from zero: e = f / d; black cells start at 0
+    for (int t = tid; t < HI * HJ; t += nt) {
+        const int a = t / HJ, b = t % HJ;
+        const int i = i0 - 2 + a, j = j0 - 2 + b;
+        T.e[a][b] = (((i + j) & 1) == 0) ? T.f[a][b] / T.d[a][b] : 0.0f;
+    }
+    __syncthreads();
+    // black on tile+1
+    for (int t = tid; t < (HI - 2) * (HJ - 2); t += nt) {
+        const int a = 1 + t / (HJ - 2), b = 1 + t % (HJ - 2);
+        const int i = i0 - 2 + a, j = j0 - 2 + b;
+        if (((i + j) & 1) == 1) T.e[a][b] = gs_cell(T, a, b);
+    }
+    __syncthreads();
+    // residual on the tile; store e
+    for (int t = tid; t < MT_I * MT_J; t += nt) {
+        const int a = 2 + t / MT_J, b = 2 + t % MT_J;
+        const int i = i0 + t / MT_J, j = j0 + t % MT_J;
+        float rr = 0.0f;
+        if (i < L.nx && j < L.ny) {
+            const float Ae = T.d[a][b] * T.e[a][b] - T.ce[a - 1][b] * T.e[a - 1][b] - T.ce[a][b] * T.e[a + 1][b] -
+                             T.cn[a][b - 1] * T.e[a][b - 1] - T.cn[a][b] * T.e[a][b + 1];
+            rr = T.f[a][b] - Ae;
+            L.e[LK(L, i, j)] = T.e[a][b];
+        }
+        res[t / MT_J][t % MT_J] = rr;
+    }
+    __syncthreads();
+    // restriction: coarse cells of this tile
+    for (int t = tid; t < (MT_I / 2) * (MT_J / 2); t += nt) {
+        const int ci = t / (MT_J / 2), cj = t % (MT_J / 2);
+        const int I = i0 / 2 + ci, J = j0 / 2 + cj;
+        if (I < C.nx && J < C.ny)
+            C.f[LK(C, I, J)] = res[2 * ci][2 * cj] + res[2 * ci + 1][2 * cj] + res[2 * ci][2 * cj + 1] +
+                               res[2 * ci + 1][2 * cj + 1];
+    }
+}
+
+// ----------------------------------------------------------- post pass --
+// e += omega * P e_coarse on tile+2, black sweep on tile+1, red sweep on the
+// tile; stores e.  Level 0 instead writes z = (double) e (0 at the pinned
+// cell) and reduces z.r and z.q into the FCG beta.
+template <bool L0>
+__global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float omega, const double *__restrict__ r64,
+                                                 const double *__restrict__ q64, double *__restrict__ z64, int pinned,
+                                                 KState *ks, double *partial) {
+    if (ks->done) return;
+    __shared__ Tile T;
+    __shared__ float ec[MT_I / 2 + 2][MT_J / 2 + 2];
+    const int i0 = blockIdx.y * MT_I, j0 = blockIdx.x * MT_J;
+    load_tile<L0>(T, L, r64, i0, j0);
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
+    const int I0 = i0 / 2 - 1, J0 = j0 / 2 - 1;
+    for (int t = tid; t < (MT_I / 2 + 2) * (MT_J / 2 + 2); t += nt) {
+        const int a = t / (MT_J / 2 + 2), b = t % (MT_J / 2 + 2);
+        const int I = I0 + a, J = J0 + b;
+        ec[a][b] = (I >= 0 && I < C.nx && J >= 0 && J < C.ny) ? C.e[LK(C, I, J)] : 0.0f;
+    }
+    __syncthreads();
+    for (int t = tid; t < HI * HJ; t += nt) {
+        const int a = t / HJ, b = t % HJ;
+        const int i = i0 - 2 + a, j = j0 - 2 + b;
+        float e = 0.0f;
+        if (i >= 0 && i < L.nx && j >= 0 && j < L.ny) e = L.e[LK(L, i, j)] + omega * ec[(i >> 1) - I0][(j >> 1) - J0];
+        T.e[a][b] = e;
+    }
+    __syncthreads();
+    for (int t = tid; t < (HI - 2) * (HJ - 2); t += nt) {
+        const int a = 1 + t / (HJ - 2), b = 1 + t % (HJ - 2);
+        const int i = i0 - 2 + a, j = j0 - 2 + b;
+        if (((i + j) & 1) == 1 && i >= 0 && i < L.nx && j >= 0 && j < L.ny) T.e[a][b] = gs_cell(T, a, b);
+    }
+    __syncthreads();
+    double acc[2] = {0.0, 0.0};
+    for (int t = tid; t < MT_I * MT_J; t += nt) {
+        const int a = 2 + t / MT_J, b = 2 + t % MT_J;
+        const int i = i0 + t / MT_J, j = j0 + t % MT_J;
+        if (i < L.nx && j < L.ny) {
+            float e = T.e[a][b];
+            if (((i + j) & 1) == 0) e = gs_cell(T, a, b);
+            const int64_t k = LK(L, i, j);
+            if (L0) {
+                const double z = (pinned && k == 0) ? 0.0 : (double)e;
+                z64[k] = z;
+                acc[0] += z * r64[k];
+                acc[1] += z * q64[k];
+            } else {
+                L.e[k] = e;
+            }
+        }
+    }
+    if (L0) {
+        double tot[2];
+        if (mg_grid_reduce<2>(acc, partial, &ks->counter, tot)) {
+            // flexible CG: beta = z_{k+1}.(r_{k+1} - r_k) / (z_k.r_k), r_{k+1} - r_k = -alpha q_k
+            if (ks->it == 0) ks->beta = 0.0;
+            else ks->beta = -ks->alpha * tot[1] / ks->rho;
+            ks->rho = tot[0];
+            if (!(tot[0] > 0.0) && ks->it == 0 && ks->res > ks->tol) {
+                ks->status = -6;
+                ks->done = 1;
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------- coarsest --
+// The coarsest level (<= MG_COARSE_MAX cells) is solved exactly: its dense
+// inverse is formed once per assembly (Gauss-Jordan in FP64 in one CTA; the
+// aggregated operator is SPD, so no pivoting is needed) and each V-cycle
+// applies it as one small matrix-vector product.
+__global__ void __launch_bounds__(MG_COARSE_MAX) k_mg_coarse_invert(MgLevel L, double *inv) {
+    extern __shared__ double sm[];
+    constexpr int W = MG_COARSE_MAX + 1;
+    double *A = sm, *B = sm + MG_COARSE_MAX * W, *col = sm + 2 * MG_COARSE_MAX * W;
+    const int n = L.nx * L.ny, ny = L.ny, t = threadIdx.x;
+    for (int r = 0; r < n; r++)
+        if (t < n) {
+            A[r * W + t] = 0.0;
+            B[r * W + t] = (r == t) ? 1.0 : 0.0;
+        }
+    __syncthreads();
+    if (t < n) {
+        const int i = t / ny, j = t % ny;
+        A[t * W + t] = L.diag[t];
+        if (i < L.nx - 1) A[t * W + t + ny] = A[(t + ny) * W + t] = -(double)L.ce[t];
+        if (j < ny - 1) A[t * W + t + 1] = A[(t + 1) * W + t] = -(double)L.cn[t];
+    }
+    __syncthreads();
+    // Gauss-Jordan; thread t owns column t of A and B
+    for (int c = 0; c < n; c++) {
+        const double piv = A[c * W + c];
+        __syncthreads();
+        if (t < n) {
+            A[c * W + t] /= piv;
+            B[c * W + t] /= piv;
+        }
+        __syncthreads();
+        if (t < n) col[t] = A[t * W + c];
+        __syncthreads();
+        if (t < n)
+            for (int r = 0; r < n; r++) {
+                if (r == c) continue;
+                A[r * W + t] -= col[r] * A[c * W + t];
+                B[r * W + t] -= col[r] * B[c * W + t];
+            }
+        __syncthreads();
+    }
+    for (int r = 0; r < n; r++)
+        if (t < n) inv[r * MG_COARSE_MAX + t] = B[r * W + t];
+}
+
+__global__ void __launch_bounds__(MG_COARSE_MAX) k_mg_coarse(MgLevel L, const double *__restrict__ inv,
+                                                             const KState *ks) {
+    if (ks->done) return;
+    __shared__ float f[MG_COARSE_MAX];
+    const int n = L.nx * L.ny, t = threadIdx.x;
+    if (t < n) f[t] = L.f[t];
+    __syncthreads();
+    if (t < n) {
+        double s = 0.0;
+        for (int c = 0; c < n; c++) s += inv[t * MG_COARSE_MAX + c] * (double)f[c];
+        L.e[t] = (float)s;
+    }
+}
+
+// ------------------------------------------------------------ FCG FP64 --
+// p = z + beta p_old (cell and neighbours), q = A p, partial p.q -> alpha
+__global__ void __launch_bounds__(256) k_fcg_a(int nx, int ny, Sys S, const double *__restrict__ z,
+                                               const double *__restrict__ p_old, double *__restrict__ p_new,
+                                               double *__restrict__ q, KState *ks, double *partial) {
+    if (ks->done) return;
+    const double beta = ks->beta;
+    const int64_t n = (int64_t)nx * ny;
+    double v[1] = {0.0};
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int ii = (int)(k / ny), jj = (int)(k % ny);
+        auto pv = [&](int64_t m) { return z[m] + beta * p_old[m]; };
+        const double pc = pv(k);
+        double y = 0.0;
+        if (!(S.pinned && k == 0)) {
+            if (jj > 0) y += -S.cn[k - 1] * pv(k - 1);
+            if (ii > 0) y += -S.ce[k - ny] * pv(k - ny);
+            y += S.diag[k] * pc;
+            if (ii < nx - 1) y += -S.ce[k] * pv(k + ny);
+            if (jj < ny - 1) y += -S.cn[k] * pv(k + 1);
+        }
+        p_new[k] = pc;
+        q[k] = y;
+        v[0] += pc * y;
+    }
+    double tot[1];
+    if (mg_grid_reduce<1>(v, partial, &ks->counter, tot)) {
+        if (!(tot[0] != 0.0) || !isfinite(tot[0])) {
+            ks->status = -6;
+            ks->done = 1;
+        } else {
+            ks->alpha = ks->rho / tot[0];
+        }
+    }
+}
+
+// x += alpha p, r -= alpha q, ||r|| -> convergence
+__global__ void __launch_bounds__(256) k_fcg_b(int64_t n, double *__restrict__ x, double *__restrict__ r,
+                                               const double *__restrict__ p, const double *__restrict__ q, KState *ks,
+                                               double *partial) {
+    if (ks->done) return;
+    const double alpha = ks->alpha;
+    double v[1] = {0.0};
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        x[k] += alpha * p[k];
+        const double rk = r[k] - alpha * q[k];
+        r[k] = rk;
+        v[0] += rk * rk;
+    }
+    double tot[1];
+    if (mg_grid_reduce<1>(v, partial, &ks->counter, tot)) {
+        const int it = ks->it + 1;
+        ks->it = it;
+        ks->res = sqrt(tot[0]) / ks->bn;
+        if (!isfinite(ks->res)) {
+            ks->status = -5;
+            ks->done = 1;
+        } else if (!(ks->res > ks->tol) || it >= ks->maxit) {
+            ks->done = 1;
+        }
+    }
+}
+
+// r = b, x = 0, p = 0, ||b||; the first V-cycle follows.
+__global__ void k_fcg_init(int64_t n, Sys S, double *__restrict__ x, double *__restrict__ r, double *__restrict__ p,
+                           KState *ks, double *partial) {
+    double v[1] = {0.0};
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const double bk = S.b[k];
+        x[k] = 0.0;
+        r[k] = bk;
+        p[k] = 0.0;
+        v[0] += bk * bk;
+    }
+    double tot[1];
+    if (mg_grid_reduce<1>(v, partial, &ks->counter, tot)) {
+        double bn = sqrt(tot[0]);
+        if (bn == 0.0) bn = 1.0;
+        ks->bn = bn;
+        ks->res = sqrt(tot[0]) / bn;
+        ks->it = 0;
+        ks->status = 0;
+        ks->alpha = 0.0;
+        ks->done = (!(ks->res > ks->tol) || ks->maxit <= 0) ? 1 : 0;
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host --
+int mg_levels_for(int nx, int ny, int *dims, int max_levels) {
+    int n = 0, a = nx, b = ny;
+    for (;;) {
+        dims[2 * n] = a;
+        dims[2 * n + 1] = b;
+        n++;
+        if ((int64_t)a * b <= MG_COARSE_MAX || n == max_levels) break;
+        a = (a + 1) / 2;
+        b = (b + 1) / 2;
+    }
+    return ((int64_t)a * b <= MG_COARSE_MAX) ? n : 0;
+}
+
+void launch_mg_setup(const Sys &S, MgLevel *lv, int nlev, double *coarse_inv, cudaStream_t st) {
+    const int64_t n0 = (int64_t)lv[0].nx * lv[0].ny;
+    k_mg_l0<<<red_blocks(n0), 256, 0, st>>>(lv[0].nx, lv[0].ny, S, lv[0]);
+    for (int l = 1; l < nlev; l++) {
+        const int64_t n = (int64_t)lv[l].nx * lv[l].ny;
+        k_mg_coarsen<<<red_blocks(n), 256, 0, st>>>(lv[l - 1], lv[l]);
+    }
+    const size_t smem = sizeof(double) * (2 * MG_COARSE_MAX * (MG_COARSE_MAX + 1) + MG_COARSE_MAX);
+    cudaFuncSetAttribute(k_mg_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_mg_coarse_invert<<<1, MG_COARSE_MAX, smem, st>>>(lv[nlev - 1], coarse_inv);
+}
+
+static dim3 tile_grid(const MgLevel &L) { return dim3((L.ny + MT_J - 1) / MT_J, (L.nx + MT_I - 1) / MT_I); }
+
+// One V-cycle: input r (FP64 level-0 rhs), output z (FP64), with the FCG
+// beta update folded into the level-0 post pass.
+static void enqueue_vcycle(MgLevel *lv, int nlev, const double *coarse_inv, const double *r, const double *q,
+                           double *z, int pinned, KState *ks, double *partial, cudaStream_t st) {
+    const dim3 blk(32, 8);
+    for (int l = 0; l < nlev - 1; l++) {
+        if (l == 0) k_mg_pre<true><<<tile_grid(lv[0]), blk, 0, st>>>(lv[0], lv[1], r, ks);
+        else k_mg_pre<false><<<tile_grid(lv[l]), blk, 0, st>>>(lv[l], lv[l + 1], nullptr, ks);
+    }
+    k_mg_coarse<<<1, MG_COARSE_MAX, 0, st>>>(lv[nlev - 1], coarse_inv, ks);
+    const float omega = 1.9f;
+    for (int l = nlev - 2; l >= 0; l--) {
+        if (l == 0)
+            k_mg_post<true><<<tile_grid(lv[0]), blk, 0, st>>>(lv[0], lv[1], omega, r, q, z, pinned, ks, partial);
+        else
+            k_mg_post<false><<<tile_grid(lv[l]), blk, 0, st>>>(lv[l], lv[l + 1], omega, nullptr, nullptr, nullptr, 0,
+                                                              ks, partial);
+    }
+}
+
+void launch_fcg_init(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, double *x,
+                     double *r, double *p, double *q, double *z, KState *ks, double *partial, cudaStream_t st) {
+    const int64_t n = (int64_t)nx * ny;
+    k_fcg_init<<<red_blocks(n), 256, 0, st>>>(n, S, x, r, p, ks, partial);
+    cudaMemsetAsync(q, 0, sizeof(double) * n, st);
+    enqueue_vcycle(lv, nlev, coarse_inv, r, q, z, S.pinned, ks, partial, st);
+}
+
+void launch_fcg_iter(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, double *x,
+                     double *r, const double *p_old, double *p_new, double *q, double *z, KState *ks,
+                     double *partial, cudaStream_t st) {
+    const int64_t n = (int64_t)nx * ny;
+    const int nb = red_blocks(n);
+    k_fcg_a<<<nb, 256, 0, st>>>(nx, ny, S, z, p_old, p_new, q, ks, partial);
+    k_fcg_b<<<nb, 256, 0, st>>>(n, x, r, p_new, q, ks, partial);
+    enqueue_vcycle(lv, nlev, coarse_inv, r, q, z, S.pinned, ks, partial, st);
+}
+
+}  // namespace asd2g

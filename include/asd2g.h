@@ -78,7 +78,8 @@ enum asd2g_solver {
     ASD2G_SOLVER_PCG = 0,          /* Jacobi-PCG, textbook recurrence            */
     ASD2G_SOLVER_PCG_REFERENCE = 1,/* the reference iteration, poisson2d.cpp:285  */
     ASD2G_SOLVER_BICGSTAB = 2,     /* right-Jacobi BiCGStab (rho_2 carried)       */
-    ASD2G_SOLVER_BICGSTAB_REFERENCE = 3 /* poisson2d.cpp:403 as written (rho_2 = 1) */
+    ASD2G_SOLVER_BICGSTAB_REFERENCE = 3, /* poisson2d.cpp:403 as written (rho_2 = 1) */
+    ASD2G_SOLVER_MGPCG = 4         /* FP64 flexible CG preconditioned by an FP32 multigrid V-cycle */
 };
 
 /* solver_flags bits */

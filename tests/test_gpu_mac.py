@@ -111,7 +111,8 @@ def _pressure_case(n=48, seed=2, bc_p=("neumann",) * 4, cp=(0.0,) * 4):
 
 
 @pytest.mark.parametrize("bc", ["neumann", "dirichlet"])
-@pytest.mark.parametrize("solver,flags", [(api.PCG, 0), (api.PCG, api.FLAG_NO_CLUSTER_PCG), (api.BICGSTAB, 0)])
+@pytest.mark.parametrize("solver,flags", [(api.PCG, 0), (api.PCG, api.FLAG_NO_CLUSTER_PCG), (api.BICGSTAB, 0),
+                                          (api.MGPCG, 0)])
 def test_pressure_solve(bc, solver, flags):
     """PCG runs as one cluster-resident launch by default and as per-iteration
     kernels with FLAG_NO_CLUSTER_PCG; both must match the restatement."""
@@ -139,6 +140,8 @@ def test_pressure_solve(bc, solver, flags):
     assert_close(interior(p), interior(ps) / dt, 1e-15, 0.0, "p = ps / dt")
     if solver == api.PCG:  # same recurrence: iteration counts agree closely
         assert abs(r["iters"] - it_ref) <= max(3, it_ref // 50)
+    if solver == api.MGPCG:  # multigrid-preconditioned: a small fraction of Jacobi's iterations
+        assert r["iters"] < max(40, it_ref // 10), (r["iters"], it_ref)
 
 
 def test_reference_cg_iterates():
