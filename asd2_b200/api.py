@@ -49,7 +49,8 @@ class _Params(C.Structure):
                 ("rho_h", C.c_double), ("rho_l", C.c_double), ("mu_h", C.c_double), ("mu_l", C.c_double),
                 ("sigma", C.c_double), ("gravity", C.c_double), ("g_axis", C.c_int32), ("fix_gravity", C.c_int32),
                 ("time_order", C.c_int32), ("solver_flags", C.c_int32), ("cfl", C.c_double),
-                ("ls_max_atime", C.c_double)]
+                ("ls_max_atime", C.c_double), ("numbers_given", C.c_int32), ("reserved1", C.c_int32),
+                ("re", C.c_double), ("we", C.c_double), ("fr", C.c_double)]
 
 
 EXPORTS = [
@@ -60,7 +61,8 @@ EXPORTS = [
     "asd2g_kappa", "asd2g_heaviside", "asd2g_convection", "asd2g_viscosity", "asd2g_momentum_rhs",
     "asd2g_intermediate_vel", "asd2g_divergence", "asd2g_update_vel", "asd2g_update_dt",
     "asd2g_assemble_gfm", "asd2g_get_system", "asd2g_solve_pressure", "asd2g_true_residual",
-    "asd2g_droplet_step", "asd2g_pcg_solve_static",
+    "asd2g_droplet_step", "asd2g_pcg_solve_static", "asd2g_weno5_line", "asd2g_weno_absgrad",
+    "asd2g_apply_bc_side", "asd2g_update_ntk", "asd2g_csr_solve",
 ]
 
 _lib = None
@@ -76,6 +78,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L = C.CDLL(path)
     S = C.c_void_p
     dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+    ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
     I, D = C.c_int, C.c_double
     sig = {
         "asd2g_version": ([], I), "asd2g_last_error": ([], C.c_char_p),
@@ -100,6 +103,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_droplet_step": ([S, C.POINTER(D), I, I, D, I, C.POINTER(I), C.POINTER(D)], I),
         "asd2g_pcg_solve_static": ([I, I, I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, D, I,
                                     C.c_void_p, C.POINTER(I), C.POINTER(D)], I),
+        "asd2g_weno5_line": ([S, dp, dp, dp, D, I], I), "asd2g_weno_absgrad": ([S, I, I, I], I),
+        "asd2g_apply_bc_side": ([S, I, C.c_char, I, I], I), "asd2g_update_ntk": ([S, I, I, I], I),
+        "asd2g_csr_solve": ([S, I, I, ip, ip, dp, dp, dp, dp, D, I, C.POINTER(I), C.POINTER(D)], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -240,6 +246,29 @@ class Session:
 
     def ls_step(self, dt, mode):
         self._check(self.L.asd2g_ls_step(self.h, dt, mode))
+
+    def weno5_line(self, F, d, n):
+        FP, FM = np.zeros(n + 6), np.zeros(n + 6)
+        self._check(self.L.asd2g_weno5_line(self.h, np.ascontiguousarray(F, dtype=np.float64), FP, FM, d, n))
+        return FP, FM
+
+    def weno_absgrad(self, ls, ls0, out):
+        self._check(self.L.asd2g_weno_absgrad(self.h, self._f(ls), self._f(ls0), self._f(out)))
+
+    def apply_bc_side(self, f, kind, side, fill=-1):
+        self._check(self.L.asd2g_apply_bc_side(self.h, self._f(f), kind.upper().encode(), side, fill))
+
+    def update_ntk(self, ls, nxf, nyf):
+        self._check(self.L.asd2g_update_ntk(self.h, self._f(ls), self._f(nxf), self._f(nyf)))
+
+    def csr_solve(self, solver, a, ia, ja, diag, b, tol=1e-6, maxit=100000):
+        x = np.zeros(len(ia) - 1)
+        it, res = C.c_int(), C.c_double()
+        rc = self._check(self.L.asd2g_csr_solve(self.h, solver, len(ia) - 1, np.ascontiguousarray(ia, np.int32),
+                                                np.ascontiguousarray(ja, np.int32), np.ascontiguousarray(a, float),
+                                                np.ascontiguousarray(diag, float), np.ascontiguousarray(b, float), x,
+                                                tol, maxit, C.byref(it), C.byref(res)))
+        return x, dict(status=rc, iters=it.value, resid=res.value)
 
     def subcell_eno(self, ls, ls0, out):
         self._check(self.L.asd2g_subcell_eno(self.h, self._f(ls), self._f(ls0), self._f(out)))

@@ -17,6 +17,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libasd2g.so")
+DROPIN = os.path.join(HERE, "dropin")
+DROPIN_LIB = os.path.join(HERE, "libasd2_dropin.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # translation unit -> extra flags
@@ -46,6 +48,29 @@ def _stale(out: str, deps: list) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def gxx() -> str:
+    for cand in (os.environ.get("ASD2_CXX"), "/usr/bin/g++", "g++"):
+        if cand and (not os.path.isabs(cand) or os.path.exists(cand)):
+            return cand
+    return "g++"
+
+
+def build_dropin(verbose: bool = False) -> str:
+    """The C++ classes with the reference's interfaces, linked against libasd2g.so."""
+    srcs = sorted(os.path.join(DROPIN, f) for f in os.listdir(DROPIN) if f.endswith(".cpp"))
+    hdrs = [os.path.join(DROPIN, f) for f in os.listdir(DROPIN) if f.endswith(".h")]
+    hdrs.append(os.path.join(ROOT, "include", "asd2g.h"))
+    if not _stale(DROPIN_LIB, srcs + hdrs + [LIB, __file__]):
+        return DROPIN_LIB
+    cmd = [gxx(), "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall", "-Wno-unused-function",
+           "-I", os.path.join(ROOT, "include"), "-I", DROPIN, *srcs, "-o", DROPIN_LIB,
+           "-L", HERE, "-lasd2g", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return DROPIN_LIB
+
+
 def build(verbose: bool = False, ptxas_v: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
@@ -69,6 +94,7 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> str:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+    build_dropin(verbose)
     return LIB
 
 

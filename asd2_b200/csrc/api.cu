@@ -20,6 +20,8 @@ void launch_absgrad(const Grid &g, bool sub, const double *ls, const double *ls0
 void launch_sussman_only(const Grid &g, const double *ls, const double *ls0, const double *hd, double *out,
                          cudaStream_t st);
 void launch_pointwise_ls(const Grid &g, int which, const double *a, double *out, cudaStream_t st);
+void launch_weno_line(const double *F, double *FP, double *FM, double d, int n, cudaStream_t st);
+void launch_weno_absgrad(const Grid &g, const double *ls, const double *ls0, double *out, cudaStream_t st);
 
 DivH make_divh(double h) {
     DivH d;
@@ -237,7 +239,8 @@ int asd2g_create(const asd2g_params *p, void *stream, asd2g_session **out) {
     }
     g.p_mirror = mirror ? 1 : 0;
     g.pinned = pinned ? 1 : 0;
-    MomParams mp{p->rho_h, p->rho_l, p->mu_h, p->mu_l, p->sigma, p->gravity, p->cfl, p->g_axis, p->fix_gravity};
+    MomParams mp{p->rho_h, p->rho_l, p->mu_h, p->mu_l, p->sigma, p->gravity, p->cfl, p->g_axis, p->fix_gravity,
+                 p->numbers_given, p->re, p->we, p->fr};
     s->M = make_momconst(g, mp);
     s->G = (size_t)g.sx * g.sy;
     s->N = (size_t)g.nx * g.ny;
@@ -346,6 +349,24 @@ int asd2g_fill_field(asd2g_session *s, int field, double value) {
     return cuda_check("fill_field");
 }
 
+int asd2g_apply_bc_side(asd2g_session *s, int field, char kind, int side, int fill) {
+    if (!s || !valid_field(field) || side < 0 || side > 3) return fail(ASD2G_E_ARG, "bad field or side");
+    int gk;
+    if (kind == 'U' || kind == 'u') gk = 0;
+    else if (kind == 'V' || kind == 'v') gk = 1;
+    else if (kind == 'P' || kind == 'p') gk = 2;
+    else return fail(ASD2G_E_ARG, "grid kind must be U, V or P");
+    int k;
+    if (fill == ASD2G_FILL_CONFIGURED) k = gk == 0 ? s->g.ku[side] : gk == 1 ? s->g.kv[side] : s->g.kp[side];
+    else if (fill == ASD2G_FILL_PERIODIC) k = K_PER;
+    else if (fill == ASD2G_FILL_NEUMANN) k = K_NEU;
+    else if (fill == ASD2G_FILL_DIRICHLET) k = K_DIR;
+    else if (fill == ASD2G_FILL_LSFREE && gk == 2) k = K_LSF;
+    else return fail(ASD2G_E_ARG, "fill rule %d not defined for this grid", fill);
+    launch_fill_side(s->g, s->f[field], gk, side, k, s->st);
+    return cuda_check("apply_bc_side");
+}
+
 int asd2g_apply_bc(asd2g_session *s, int field, char kind) {
     if (!s || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field");
     if (kind == 'U' || kind == 'u') launch_fill_uv(s->g, s->f[field], nullptr, s->st);
@@ -425,6 +446,27 @@ int asd2g_ls_step(asd2g_session *s, double dt, int reinit_mode) {
     int rc = asd2g_ls_advect(s, dt);
     if (rc) return rc;
     return asd2g_reinit(s, reinit_mode);
+}
+
+int asd2g_weno5_line(asd2g_session *s, const double *F, double *FP, double *FM, double d, int n) {
+    if (!s || !F || !FP || !FM || n < 1 || (size_t)(n + 2 * NB) > s->G || !(d > 0.0))
+        return fail(ASD2G_E_ARG, "weno5_line: bad arguments");
+    const size_t m = (size_t)n + 2 * NB;
+    cudaMemcpyAsync(s->f[ASD2G_W0], F, sizeof(double) * m, cudaMemcpyHostToDevice, s->st);
+    cudaMemsetAsync(s->f[ASD2G_W1], 0, sizeof(double) * m, s->st);
+    cudaMemsetAsync(s->f[ASD2G_W2], 0, sizeof(double) * m, s->st);
+    launch_weno_line(s->f[ASD2G_W0], s->f[ASD2G_W1], s->f[ASD2G_W2], d, n, s->st);
+    cudaMemcpyAsync(FP, s->f[ASD2G_W1], sizeof(double) * m, cudaMemcpyDeviceToHost, s->st);
+    cudaMemcpyAsync(FM, s->f[ASD2G_W2], sizeof(double) * m, cudaMemcpyDeviceToHost, s->st);
+    int rc = cuda_check("weno5_line");
+    return rc ? rc : sync(s);
+}
+
+int asd2g_weno_absgrad(asd2g_session *s, int ls, int ls0, int out) {
+    if (!s || !valid_field(ls) || !valid_field(ls0) || !valid_field(out) || out == ls || out == ls0)
+        return fail(ASD2G_E_ARG, "bad field");
+    launch_weno_absgrad(s->g, s->f[ls], s->f[ls0], s->f[out], s->st);
+    return cuda_check("weno_absgrad");
 }
 
 // -------------------------------------------------------------- momentum --
@@ -514,6 +556,14 @@ int asd2g_update_dt(asd2g_session *s, double *dt) {
     if (rc) return rc;
     *dt = s->dsc_host[1];
     return ASD2G_OK;
+}
+
+int asd2g_update_ntk(asd2g_session *s, int ls, int nxf, int nyf) {
+    if (!s || !valid_field(ls) || !valid_field(nxf) || !valid_field(nyf) || nxf == nyf || nxf == ls || nyf == ls)
+        return fail(ASD2G_E_ARG, "bad field");
+    launch_absgrad(s->g, false, s->f[ls], s->f[ls], s->w1, s->st);  // ENO_DerivAbsLS_2D(ls, ls)
+    launch_ntk(s->g, s->f[ls], s->w1, s->f[nxf], s->f[nyf], s->st);
+    return cuda_check("update_ntk");
 }
 
 // -------------------------------------------------------------- pressure --
@@ -677,6 +727,74 @@ int asd2g_true_residual(asd2g_session *s, double *rel) {
     return ASD2G_OK;
 }
 
+int asd2g_csr_solve(asd2g_session *s, int solver, int rows, const int *ia, const int *ja, const double *a,
+                    const double *diag, const double *b, double *x, double tol, int maxit, int *iters,
+                    double *rel_resid) {
+    if (!s || !ia || !ja || !a || !diag || !b || !x) return fail(ASD2G_E_ARG, "null argument");
+    if (rows < 1 || (size_t)rows > s->N) return fail(ASD2G_E_ARG, "rows must be in [1, nx*ny]");
+    if (solver < 0 || solver > 3) return fail(ASD2G_E_ARG, "solver %d not available for CSR input", solver);
+    if (maxit < 0) return fail(ASD2G_E_ARG, "maxit must be >= 0");
+    const int nnz = ia[rows];
+    if (nnz < 0 || ia[0] != 0) return fail(ASD2G_E_ARG, "bad CSR row pointer");
+    std::vector<double> minv(rows);
+    for (int r = 0; r < rows; r++) minv[r] = 1.0 / diag[r];  // InvertMatrixDiagonal, poisson2d.cpp:577-585
+    int *dia = nullptr, *dja = nullptr;
+    double *da = nullptr, *dminv = nullptr, *db = nullptr;
+    bool ok = cudaMalloc(&dia, sizeof(int) * (rows + 1)) == cudaSuccess &&
+              cudaMalloc(&dja, sizeof(int) * (nnz ? nnz : 1)) == cudaSuccess &&
+              cudaMalloc(&da, sizeof(double) * (nnz ? nnz : 1)) == cudaSuccess &&
+              cudaMalloc(&dminv, sizeof(double) * rows) == cudaSuccess && cudaMalloc(&db, sizeof(double) * rows) == cudaSuccess;
+    int rc = ASD2G_OK;
+    if (!ok) {
+        cudaGetLastError();
+        rc = fail(ASD2G_E_NOMEM, "CSR buffers");
+    }
+    KState k{};
+    if (rc == ASD2G_OK) {
+        cudaMemcpyAsync(dia, ia, sizeof(int) * (rows + 1), cudaMemcpyHostToDevice, s->st);
+        cudaMemcpyAsync(dja, ja, sizeof(int) * nnz, cudaMemcpyHostToDevice, s->st);
+        cudaMemcpyAsync(da, a, sizeof(double) * nnz, cudaMemcpyHostToDevice, s->st);
+        cudaMemcpyAsync(dminv, minv.data(), sizeof(double) * rows, cudaMemcpyHostToDevice, s->st);
+        cudaMemcpyAsync(db, b, sizeof(double) * rows, cudaMemcpyHostToDevice, s->st);
+        Sys S{};
+        S.minv = dminv;
+        S.b = db;
+        const double reg = solver == 1 ? 1.0e-12 : 0.0;
+        launch_set_kstate(s->ks, tol, maxit, solver, reg, s->st);
+        if (solver <= 1) launch_pcg_init_n(rows, S, s->x, s->r, s->pa, s->ks, s->partial, s->st);
+        else launch_bicg_init_n(rows, S, s->x, s->r, s->rt, s->pa, s->q, s->ks, s->partial, s->st);
+        for (int done = 0, launched = 0; !done; launched += 64) {
+            for (int it = 0; it < 64; it++) {
+                if (solver <= 1)
+                    launch_csr_pcg_iter(dia, dja, da, rows, S, s->x, s->r, s->pa, s->q, s->ks, s->partial, s->st);
+                else
+                    launch_csr_bicg_iter(dia, dja, da, rows, S, s->x, s->r, s->rt, s->pa, s->q, s->sv, s->t3, s->ks,
+                                         s->partial, s->st);
+            }
+            cudaMemcpyAsync(&k, s->ks, sizeof(KState), cudaMemcpyDeviceToHost, s->st);
+            rc = sync(s);
+            if (rc) break;
+            done = k.done || launched + 64 >= maxit + 64;
+        }
+        if (rc == ASD2G_OK) {
+            cudaMemcpyAsync(x, s->x, sizeof(double) * rows, cudaMemcpyDeviceToHost, s->st);
+            rc = sync(s);
+        }
+    }
+    cudaFree(dia);
+    cudaFree(dja);
+    cudaFree(da);
+    cudaFree(dminv);
+    cudaFree(db);
+    if (rc) return rc;
+    if (iters) *iters = k.it;
+    if (rel_resid) *rel_resid = k.res;
+    if (k.status == -5) return fail(ASD2G_E_NONFINITE, "non-finite residual at iteration %d", k.it);
+    if (k.status == -6) return fail(ASD2G_E_BREAKDOWN, "Krylov breakdown at iteration %d", k.it);
+    const bool conv = solver == 0 ? !(k.res > tol) : (k.res <= tol);
+    return conv ? ASD2G_OK : ASD2G_NOT_CONVERGED;
+}
+
 // ------------------------------------------------------------------ step --
 int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver, double tol, int maxit, int *iters,
                        double *rel_resid) {
@@ -702,8 +820,8 @@ int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver
     launch_fill_uv(g, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->st);
     cudaMemsetAsync(s->f[ASD2G_DIV], 0, sizeof(double) * s->G, s->st);
     launch_divergence(g, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->f[ASD2G_DIV], s->st);
-    // SolvePoisson recomputes kappa when kWe = rhoH / sigma is finite and nonzero (mac2d.cpp:1307).
-    const double we = s->prm.rho_h / s->prm.sigma;
+    // SolvePoisson recomputes kappa when kWe is finite and nonzero (mac2d.cpp:1307).
+    const double we = s->prm.numbers_given ? s->prm.we : s->prm.rho_h / s->prm.sigma;
     rc = assemble(s, (we != 0.0 && std::isfinite(we)) ? 1 : 0);
     if (rc) return rc;
     const int st = solve(s, solver, tol, maxit, iters, rel_resid);

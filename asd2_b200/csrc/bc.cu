@@ -228,6 +228,22 @@ __global__ void k_fill_p(Grid g, double *a, int side_mask) {
     }
 }
 
+// One side of one grid with an explicit fill kind (the per-side methods
+// BC_UW, BC_NeumannUW, ... of bc2d.cpp).  grid_kind: 0 U, 1 V, 2 P.
+void launch_fill_side(const Grid &g0, double *a, int grid_kind, int side, int kind, cudaStream_t st) {
+    Grid g = g0;
+    for (int s = 0; s < 4; s++) g.ku[s] = g.kv[s] = g.kp[s] = K_NONE;
+    if (grid_kind == 0) g.ku[side] = kind;
+    else if (grid_kind == 1) g.kv[side] = kind;
+    else g.kp[side] = kind;
+    if (grid_kind == 0) k_fill_uv<<<1, 1024, 0, st>>>(g, a, nullptr);
+    else if (grid_kind == 1) k_fill_uv<<<1, 1024, 0, st>>>(g, nullptr, a);
+    else {
+        const int n = 2 * NB * g.ny + 2 * NB * g.nx;
+        k_fill_p<<<(n + 255) / 256, 256, 0, st>>>(g, a, 1 << side);
+    }
+}
+
 void launch_fill_uv(const Grid &g, double *u, double *v, cudaStream_t st) {
     k_fill_uv<<<1, 1024, 0, st>>>(g, u, v);
 }

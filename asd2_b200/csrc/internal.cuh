@@ -23,5 +23,6 @@ void asd2g_set_error_text(const char *msg);
 // bc.cu
 void launch_fill_uv(const Grid &g, double *u, double *v, cudaStream_t st);
 void launch_fill_p(const Grid &g, double *a, cudaStream_t st);
+void launch_fill_side(const Grid &g, double *a, int grid_kind, int side, int kind, cudaStream_t st);
 
 }  // namespace asd2g

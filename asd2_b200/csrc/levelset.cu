@@ -186,6 +186,37 @@ __global__ void k_pointwise_ls(int64_t n, int which, double eps, const double *_
 }
 
 // ------------------------------------------------------------------------
+// UnitHJWENO5 on one line F[0 .. n+5] (levelset2d.cpp:159-262): FP, FM at
+// points 3 .. n+2.
+__global__ void k_weno_line(const double *__restrict__ F, double *__restrict__ FP, double *__restrict__ FM, DivH dv,
+                            int n) {
+    const int i = NB + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n + NB) return;
+    double D[6], fp, fm;
+#pragma unroll
+    for (int k = 0; k < 6; k++) D[k] = F[i - 2 + k] - F[i - 3 + k];
+    weno5_point(D, dv, fp, fm);
+    FP[i] = fp;
+    FM[i] = fm;
+}
+
+// HJWENO5_DerivAbsLS_2D (levelset2d.cpp:488-558): WENO5 one-sided derivatives
+// of phi itself along each line, Godunov |grad phi| with the sign of phi0.
+__global__ void k_weno_absgrad(Grid g, DivH ddx, DivH ddy, const double *__restrict__ ls,
+                               const double *__restrict__ ls0, double *__restrict__ out) {
+    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
+    if (i >= g.nx + NB || j >= g.ny + NB) return;
+    double D[6], pX, mX, pY, mY;
+#pragma unroll
+    for (int k = 0; k < 6; k++) D[k] = ls[IX(g, i - 2 + k, j)] - ls[IX(g, i - 3 + k, j)];
+    weno5_point(D, ddx, pX, mX);
+#pragma unroll
+    for (int k = 0; k < 6; k++) D[k] = ls[IX(g, i, j - 2 + k)] - ls[IX(g, i, j - 3 + k)];
+    weno5_point(D, ddy, pY, mY);
+    out[IX(g, i, j)] = godunov(ls0[IX(g, i, j)], pX, mX, pY, mY);
+}
+
+// ------------------------------------------------------------------------
 // Host launchers
 LsConst make_lsconst(const Grid &g) {
     LsConst K;
@@ -332,6 +363,15 @@ void launch_sussman_only(const Grid &g, const double *ls, const double *ls0, con
     const LsConst K = make_lsconst(g);
     cudaMemsetAsync(out, 0, sizeof(double) * (size_t)g.sx * g.sy, st);
     k_sussman_only<<<cell_grid(g), dim3(TJ, TI), 0, st>>>(g, K, ls, ls0, hd, out);
+}
+
+void launch_weno_line(const double *F, double *FP, double *FM, double d, int n, cudaStream_t st) {
+    k_weno_line<<<(n + 127) / 128, 128, 0, st>>>(F, FP, FM, make_divh(d), n);
+}
+
+void launch_weno_absgrad(const Grid &g, const double *ls, const double *ls0, double *out, cudaStream_t st) {
+    cudaMemsetAsync(out, 0, sizeof(double) * (size_t)g.sx * g.sy, st);
+    k_weno_absgrad<<<cell_grid(g), dim3(TJ, TI), 0, st>>>(g, make_divh(g.dx), make_divh(g.dy), ls, ls0, out);
 }
 
 void launch_pointwise_ls(const Grid &g, int which, const double *a, double *out, cudaStream_t st) {

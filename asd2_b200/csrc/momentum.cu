@@ -334,6 +334,27 @@ __global__ void k_update_dt(Grid g, MomConst M, const double *__restrict__ u, co
     }
 }
 
+// ------------------------------------------------------------- UpdateNTK --
+// MACSolver2D::UpdateNTK (mac2d.cpp:124-219) as far as the reference goes:
+// Q = |1 - |grad phi|_ENO(phi, phi)|; where Q <= 1e-4 the unit normal from
+// central differences is written; elsewhere (its curve-fitting branch is
+// empty) nothing is written.  absg holds ENO_DerivAbsLS_2D(phi, phi).
+__global__ void k_ntk(Grid g, DivH d2x, DivH d2y, const double *__restrict__ ls, const double *__restrict__ absg,
+                      double *__restrict__ nxo, double *__restrict__ nyo) {
+    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
+    if (i >= g.nx + NB || j >= g.ny + NB) return;
+    const double Q = fabs(1.0 - absg[IX(g, i, j)]);
+    if (Q > 0.0001) return;
+    const double gx = d2x(ls[IX(g, i + 1, j)] - ls[IX(g, i - 1, j)]);
+    const double gy = d2y(ls[IX(g, i, j + 1)] - ls[IX(g, i, j - 1)]);
+    nxo[IX(g, i, j)] = 1.0 / sqrt(gx * gx + gy * gy + 1.0e-100) * gx;
+    nyo[IX(g, i, j)] = 1.0 / sqrt(gx * gx + gy * gy + 1.0e-100) * gy;
+}
+
+void launch_ntk(const Grid &g, const double *ls, const double *absg, double *nxo, double *nyo, cudaStream_t st) {
+    k_ntk<<<cell_grid(g), dim3(TJ, TI), 0, st>>>(g, make_divh(2.0 * g.dx), make_divh(2.0 * g.dy), ls, absg, nxo, nyo);
+}
+
 // ------------------------------------------------------------------ host --
 MomConst make_momconst(const Grid &g, const MomParams &p) {
     MomConst M;
@@ -346,11 +367,12 @@ MomConst make_momconst(const Grid &g, const MomParams &p) {
     M.sigma = p.sigma;
     M.g = p.g;
     M.cfl = p.cfl;
-    // kRe = rhoH L U / muH with L = U = 1 (mac2d.cpp:33); no viscosity when kRe <= 0 (:598).
-    const double re = p.rho_h / p.mu_h;
+    // kRe = rhoH L U / muH with L = U = 1 (mac2d.cpp:33) unless given; no
+    // viscosity when kRe <= 0 (:598).
+    const double re = p.numbers_given ? p.re : p.rho_h / p.mu_h;
     M.visc = !(re <= 0.0);
-    // Gravity (AddGravityFU/FV :1043-1079): kG = g, kFr = 1/g (L = U = 1).
-    const double fr = 1.0 / p.g;
+    // Gravity (AddGravityFU/FV :1043-1079): kG = g, kFr = U^2 / (g L) (:35).
+    const double fr = p.numbers_given ? p.fr : 1.0 / p.g;
     auto on = [&](int axis) { return (fr != 0 || p.g != 0.0) && !std::isnan(fr) && !std::isinf(fr) && p.g_axis == axis; };
     M.gu = on(0) ? -p.g : 0.0;
     if (p.fix_gravity) {

@@ -9,6 +9,8 @@ namespace asd2g {
 struct MomParams {
     double rho_h, rho_l, mu_h, mu_l, sigma, g, cfl;
     int g_axis, fix_gravity;
+    int numbers_given;
+    double re, we, fr;
 };
 
 struct MomConst {
@@ -33,6 +35,7 @@ void launch_divergence(const Grid &g, const double *u, const double *v, double *
 void launch_update_vel(const Grid &g, const MomConst &M, const double *us, const double *vs, const double *ps,
                        const double *ls, const double *H, const double *kappa, double *u, double *v,
                        const double *dtp, cudaStream_t st);
+void launch_ntk(const Grid &g, const double *ls, const double *absg, double *nxo, double *nyo, cudaStream_t st);
 void launch_update_dt(const Grid &g, const MomConst &M, const double *u, const double *v, double *partial,
                       unsigned *counter, double *dt_out, cudaStream_t st);
 

@@ -412,6 +412,78 @@ __global__ void k_bicg_x(int64_t n, double *__restrict__ x, double *__restrict__
     }
 }
 
+// ------------------------------------------------------------------ CSR --
+// PoissonSolver2D's CSR interface (poisson2d.cpp:230-575): a general CSR
+// matrix from the caller, one thread per row.  Column indices outside
+// [0, rows) are skipped (the reference's pinned all-Neumann matrix carries
+// such entries, with value 0, which MKL would read out of bounds).
+struct Csr {
+    const int *ia, *ja;
+    const double *a;
+    int rows;
+};
+__device__ __forceinline__ double csr_row(const Csr &A, int r, const double *__restrict__ x) {
+    double s = 0.0;
+    for (int k = A.ia[r]; k < A.ia[r + 1]; k++) {
+        const int c = A.ja[k];
+        if (c < 0 || c >= A.rows) continue;
+        s += A.a[k] * x[c];
+    }
+    return s;
+}
+
+// p = Minv r + beta p (PCG direction update)
+__global__ void k_csr_pcg_p(int64_t n, Sys S, const double *__restrict__ r, double *__restrict__ p, const KState *ks) {
+    if (ks->done) return;
+    const double beta = ks->beta;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        p[k] = S.minv[k] * r[k] + beta * p[k];
+}
+
+// q = A p, p.q -> alpha
+__global__ void __launch_bounds__(256) k_csr_pcg_q(Csr A, const double *__restrict__ p, double *__restrict__ q,
+                                                   KState *ks, double *partial) {
+    if (ks->done) return;
+    double v[1] = {0.0};
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.rows; r += gridDim.x * blockDim.x) {
+        const double y = csr_row(A, r, p);
+        q[r] = y;
+        v[0] += p[r] * y;
+    }
+    double tot[1];
+    if (grid_reduce<1>(v, partial, &ks->counter, tot)) {
+        const double den = tot[0] + ks->reg;
+        if (!(den != 0.0) || !isfinite(den)) {
+            ks->status = -6;
+            ks->done = 1;
+        } else {
+            ks->alpha = ks->rho / den;
+        }
+    }
+}
+
+// y = A xin and dots (BiCGStab), as k_bicg_spmv with a CSR operator
+template <int NV>
+__global__ void __launch_bounds__(256) k_csr_bicg_spmv(Csr A, const double *__restrict__ xin, double *__restrict__ y,
+                                                       const double *__restrict__ w, KState *ks, double *partial,
+                                                       int which) {
+    if (ks->done) return;
+    double a[NV];
+#pragma unroll
+    for (int q = 0; q < NV; q++) a[q] = 0.0;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.rows; r += gridDim.x * blockDim.x) {
+        const double s = csr_row(A, r, xin);
+        y[r] = s;
+        if (NV == 1) a[0] += w[r] * s;
+        else { a[0] += s * w[r]; a[NV - 1] += s * s; }
+    }
+    double tot[NV];
+    if (grid_reduce<NV>(a, partial, &ks->counter, tot)) {
+        if (which == 0) ks->alpha = ks->rho1 / tot[0];
+        else ks->omega = tot[0] / tot[NV - 1];
+    }
+}
+
 // ---------------------------------------------------------- scatter / res --
 // PS = 0 everywhere, interior = x, then (host) P fill, then P = PS / dt.
 __global__ void k_scatter_ps(Grid g, const double *__restrict__ x, double *__restrict__ ps) {
@@ -506,6 +578,39 @@ void launch_bicg_iter(const Grid &g, const Sys &S, double *x, double *r, const d
     k_bicg_shat<<<nb, 256, 0, st>>>(n, S, s, shat, ks, x, phat);
     k_bicg_spmv<2><<<nb, 256, 0, st>>>(g.nx, g.ny, S, shat, t, s, ks, partial, 1);
     k_bicg_x<<<nb, 256, 0, st>>>(n, x, r, rt, phat, shat, s, t, ks, partial);
+}
+
+void launch_csr_pcg_iter(const int *ia, const int *ja, const double *a, int rows, const Sys &S, double *x,
+                         double *r, double *p, double *q, KState *ks, double *partial, cudaStream_t st) {
+    const Csr A{ia, ja, a, rows};
+    const int nb = red_blocks(rows);
+    k_csr_pcg_p<<<nb, 256, 0, st>>>(rows, S, r, p, ks);
+    k_csr_pcg_q<<<nb, 256, 0, st>>>(A, p, q, ks, partial);
+    k_pcg_b<<<nb, 256, 0, st>>>(rows, S, x, r, p, q, ks, partial);
+}
+
+void launch_csr_bicg_iter(const int *ia, const int *ja, const double *a, int rows, const Sys &S, double *x, double *r,
+                          const double *rt, double *p, double *v, double *s, double *t, KState *ks, double *partial,
+                          cudaStream_t st) {
+    const Csr A{ia, ja, a, rows};
+    const int64_t n = rows;
+    const int nb = red_blocks(n);
+    double *phat = t + n, *shat = t + 2 * n;
+    k_bicg_p<<<nb, 256, 0, st>>>(n, S, r, p, v, phat, ks);
+    k_csr_bicg_spmv<1><<<nb, 256, 0, st>>>(A, phat, v, rt, ks, partial, 0);
+    k_bicg_s<<<nb, 256, 0, st>>>(n, r, v, s, ks, partial);
+    k_bicg_shat<<<nb, 256, 0, st>>>(n, S, s, shat, ks, x, phat);
+    k_csr_bicg_spmv<2><<<nb, 256, 0, st>>>(A, shat, t, s, ks, partial, 1);
+    k_bicg_x<<<nb, 256, 0, st>>>(n, x, r, rt, phat, shat, s, t, ks, partial);
+}
+
+void launch_pcg_init_n(int64_t n, const Sys &S, double *x, double *r, double *p, KState *ks, double *partial,
+                       cudaStream_t st) {
+    k_pcg_init<<<red_blocks(n), 256, 0, st>>>(n, S, x, r, p, ks, partial);
+}
+void launch_bicg_init_n(int64_t n, const Sys &S, double *x, double *r, double *rt, double *p, double *v, KState *ks,
+                        double *partial, cudaStream_t st) {
+    k_bicg_init<<<red_blocks(n), 256, 0, st>>>(n, S, x, r, rt, p, v, ks, partial);
 }
 
 void launch_scatter_ps(const Grid &g, const double *x, double *ps, double *p, const double *dtp, cudaStream_t st) {

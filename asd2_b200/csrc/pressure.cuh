@@ -43,6 +43,16 @@ void launch_scatter_ps(const Grid &g, const double *x, double *ps, double *p, co
 void launch_true_residual(const Grid &g, const Sys &S, const double *ps, double *partial, double *out2,
                           cudaStream_t st);
 void launch_set_kstate(KState *ks, double tol, int maxit, int mode, double reg, cudaStream_t st);
+// CSR-operator variants (PoissonSolver2D's CSR interface); Sys carries b and minv only.
+void launch_pcg_init_n(int64_t n, const Sys &S, double *x, double *r, double *p, KState *ks, double *partial,
+                       cudaStream_t st);
+void launch_bicg_init_n(int64_t n, const Sys &S, double *x, double *r, double *rt, double *p, double *v, KState *ks,
+                        double *partial, cudaStream_t st);
+void launch_csr_pcg_iter(const int *ia, const int *ja, const double *a, int rows, const Sys &S, double *x,
+                         double *r, double *p, double *q, KState *ks, double *partial, cudaStream_t st);
+void launch_csr_bicg_iter(const int *ia, const int *ja, const double *a, int rows, const Sys &S, double *x, double *r,
+                          const double *rt, double *p, double *v, double *s, double *t, KState *ks, double *partial,
+                          cudaStream_t st);
 // pcg_cluster.cu: whole textbook PCG solve in one thread-block cluster;
 // false when the system does not fit one cluster or cannot be scheduled.
 int pcg_cluster_size(int nx, int ny);

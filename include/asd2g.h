@@ -101,6 +101,12 @@ typedef struct asd2g_params {
     int32_t solver_flags;    /* ASD2G_FLAG_* bits (0 = defaults) */
     double cfl;
     double ls_max_atime;     /* reinit pseudo-time; <= 0: 1.5*kThickness (levelset2d.cpp:10) */
+    int32_t numbers_given;   /* 1: use re/we/fr below; 0: kRe = rho_h/mu_h, kWe = rho_h/sigma,
+                                kFr = 1/gravity (the second MACSolver2D constructor with L = U = 1) */
+    int32_t reserved1;
+    double re, we, fr;       /* kRe, kWe, kFr of MACSolver2D (mac2d.h:37): viscosity is skipped when
+                                kRe <= 0, the curvature is recomputed in the solve when kWe is finite and
+                                nonzero, gravity needs kFr finite (mac2d.cpp:598, :1307, :1047) */
 } asd2g_params;
 
 typedef struct asd2g_session asd2g_session;
@@ -129,6 +135,16 @@ int asd2g_fill_field(asd2g_session *s, int field, double value);
 /* Ghost fill of one field as a U, V or P grid (kind 'U', 'V', 'P').
  * BoundaryCondition2D::ApplyBC_{U,V,P}_2D, bc2d.cpp:123,239,346. */
 int asd2g_apply_bc(asd2g_session *s, int field, char kind);
+/* One side (0 W, 1 E, 2 S, 3 N) of that fill.  fill = ASD2G_FILL_CONFIGURED
+ * applies the session's boundary kind for that side (BC_UW ... BC_PN,
+ * bc2d.cpp:355-573); the other values force one rule (BC_PeriodicUW,
+ * BC_NeumannUW, BC_DirichletUW, BC_LSFreeBoundaryPW, ... :575-934) with the
+ * session's Dirichlet constant for that side. */
+enum asd2g_fill {
+    ASD2G_FILL_CONFIGURED = -1, ASD2G_FILL_PERIODIC = 1, ASD2G_FILL_NEUMANN = 2, ASD2G_FILL_DIRICHLET = 3,
+    ASD2G_FILL_LSFREE = 4
+};
+int asd2g_apply_bc_side(asd2g_session *s, int field, char kind, int side, int fill);
 
 /* ---- level set (levelset2d.cpp) ---- */
 /* Solve_LevelSet_2D(LS, U, V, dt): TVD-RK3 + HJ-WENO5, levelset2d.cpp:43. */
@@ -149,6 +165,12 @@ int asd2g_heaviside_deriv(asd2g_session *s, int ls, int out);
 int asd2g_smoothed_sign(asd2g_session *s, int ls, int out);
 /* Level-set step: advect (dt) then reinitialise (mode). */
 int asd2g_ls_step(asd2g_session *s, double dt, int reinit_mode);
+/* UnitHJWENO5(F, FP, FM, d, n), levelset2d.cpp:159 / mac2d.cpp:465: WENO5
+ * one-sided derivatives of the line F[0 .. n+5] (host arrays), written to
+ * FP[3 .. n+2] and FM[3 .. n+2].  n + 6 must not exceed (nx+6)*(ny+6). */
+int asd2g_weno5_line(asd2g_session *s, const double *F, double *FP, double *FM, double d, int n);
+/* HJWENO5_DerivAbsLS_2D(ls, ls0) -> out, levelset2d.cpp:488. */
+int asd2g_weno_absgrad(asd2g_session *s, int ls, int ls0, int out);
 
 /* ---- MAC momentum (mac2d.cpp) ---- */
 /* UpdateKappa(LS) -> KAPPA interior, mac2d.cpp:221. */
@@ -171,6 +193,10 @@ int asd2g_divergence(asd2g_session *s, int u, int v, int div);
 int asd2g_update_vel(asd2g_session *s, double dt);
 /* UpdateDt(U, V), :1851. */
 int asd2g_update_dt(asd2g_session *s, double *dt);
+/* UpdateNTK (mac2d.cpp:124-219) as far as the reference implements it: the
+ * unit normal (central differences) at cells where |1 - |grad phi|| <= 1e-4
+ * (ENO gradient), written into fields nxf and nyf; other cells untouched. */
+int asd2g_update_ntk(asd2g_session *s, int ls, int nxf, int nyf);
 
 /* ---- GFM pressure (mac2d.cpp:1249-1727, poisson2d.cpp) ---- */
 /* Assemble the matrix-free GFM system from LS, KAPPA, H, DIV with time step
@@ -190,6 +216,15 @@ int asd2g_solve_pressure(asd2g_session *s, int solver, double tol, int maxit, do
                          double *rel_resid);
 /* ||b - A x|| / ||b|| of the current PS against the assembled system, in FP64. */
 int asd2g_true_residual(asd2g_session *s, double *rel);
+/* PoissonSolver2D's CSR interface (poisson2d.cpp:230-575): solve A x = b for
+ * a caller-assembled CSR matrix (0-based, host arrays: ia[rows+1], ja/a[nnz])
+ * with the Jacobi preconditioner diag (one value per row), from x = 0.
+ * solver: ASD2G_SOLVER_PCG, _PCG_REFERENCE, _BICGSTAB or _BICGSTAB_REFERENCE.
+ * Column indices outside [0, rows) are skipped.  rows must not exceed nx*ny
+ * of the session.  x (host, rows values) receives the solution. */
+int asd2g_csr_solve(asd2g_session *s, int solver, int rows, const int *ia, const int *ja, const double *a,
+                    const double *diag, const double *b, double *x, double tol, int maxit, int *iters,
+                    double *rel_resid);
 
 /* ---- whole step (test_mac2d_large.cpp:496-552) ----
  * lsB = LS; advect; reinit (reinit_mode); kappa; H, HS; intermediate velocity

@@ -286,9 +286,11 @@ class Oracle:
         return m
 
     # ---- composed droplet step (tests/LargeTests/test_mac2d_large.cpp:496-552) ----
-    def droplet_step(self, g, f, st, tol=1e-10, maxit=200000, reinit_mode=2):
+    def droplet_step(self, g, f, st, tol=1e-10, maxit=200000, reinit_mode=2, pcg_mode=0, bicgstab_mode=None):
         """One full two-phase step in the driver's order, with the pressure
-        system solved by the fixed-order FP64 PCG to ``tol``.  ``st`` is a dict
+        system solved by the fixed-order FP64 PCG to ``tol`` (``pcg_mode`` 1:
+        the reference's own CG iteration; ``bicgstab_mode`` not None: BiCGStab
+        in that mode instead of CG).  ``st`` is a dict
         with ls, u, v, ps, p, kappa (padded) and dt; it is updated in place and
         the Poisson statistics are returned."""
         ls, u, v = st["ls"], st["u"], st["v"]
@@ -306,7 +308,10 @@ class Oracle:
         self.bc(g, "v", vh)
         div = self.divergence(g, uh, vh)
         sysd = self.gfm_assemble(g, f, dt, ls, st["kappa"], H, div, recompute_kappa=f.sigma != 0.0)
-        x, it, res, tres = self.pcg(g, sysd, tol=tol, maxit=maxit)
+        if bicgstab_mode is None:
+            x, it, res, tres = self.pcg(g, sysd, tol=tol, maxit=maxit, mode=pcg_mode)
+        else:
+            x, it, res, tres = self.bicgstab(g, sysd, tol=tol, maxit=maxit, mode=bicgstab_mode)
         ps = g.zeros()
         self.scatter(g, x, ps)
         self.bc(g, "p", ps)

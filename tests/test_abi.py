@@ -54,5 +54,5 @@ def test_missing_library_fails_loudly(tmp_path):
 
 
 def test_params_struct_matches_header():
-    # asd2g_params: 4 int32, 4 double, 12 int32, 12 double, 6 double, 4 int32, 2 double
-    assert ctypes.sizeof(api._Params) == 4 * 4 + 4 * 8 + 12 * 4 + 12 * 8 + 6 * 8 + 4 * 4 + 2 * 8
+    # asd2g_params: 4 int32, 4 double, 12 int32, 12 double, 6 double, 4 int32, 2 double, 2 int32, 3 double
+    assert ctypes.sizeof(api._Params) == 4 * 4 + 4 * 8 + 12 * 4 + 12 * 8 + 6 * 8 + 4 * 4 + 2 * 8 + 2 * 4 + 3 * 8
