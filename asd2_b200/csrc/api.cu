@@ -117,6 +117,8 @@ struct asd2g_session {
     MgLevel lv[MG_MAX_LEVELS] = {};
     int nlev = 0;
     double *coarse_inv = nullptr, *z = nullptr;
+    double *mg_partial = nullptr;  // per-tile partial sums of the V-cycle's fused dots
+    int64_t mg_partial_n = 0;
     int chunk_len = 64;
     std::vector<void *> allocs;
 };
@@ -141,7 +143,7 @@ int mg_alloc(asd2g_session *s) {
         L.nx = dims[2 * l];
         L.ny = dims[2 * l + 1];
         const size_t m = (size_t)L.nx * L.ny;
-        float **arrs[] = {&L.diag, &L.ce, &L.cn, &L.f, &L.e};
+        float **arrs[] = {&L.diag, &L.ce, &L.cn, &L.f, &L.e, &L.ep};
         for (float **a : arrs) {
             if (cudaMalloc(a, sizeof(float) * m) != cudaSuccess) {
                 cudaGetLastError();
@@ -153,7 +155,10 @@ int mg_alloc(asd2g_session *s) {
     }
     int rc = dalloc(s, &s->coarse_inv, (size_t)MG_COARSE_CELLS * MG_COARSE_CELLS);
     if (rc == ASD2G_OK) rc = dalloc(s, &s->z, s->N);
+    const int64_t np = mg_partial_len(s->g.nx, s->g.ny);
+    if (rc == ASD2G_OK) rc = dalloc(s, &s->mg_partial, (size_t)np);
     if (rc) return rc;
+    s->mg_partial_n = np;
     s->nlev = n;
     return ASD2G_OK;
 }
@@ -177,16 +182,21 @@ bool stream_capturing(asd2g_session *s) {
     return cs != cudaStreamCaptureStatusNone;
 }
 
-void enqueue_iters(asd2g_session *s, int solver, int count) {
+// false if a multigrid launch was refused (partial-sum buffer too small).
+bool enqueue_iters(asd2g_session *s, int solver, int count) {
     const Grid &g = s->g;
     for (int k = 0; k < count; k++) {
         if (solver == ASD2G_SOLVER_MGPCG) {
-            if (k % 2 == 0)
-                launch_fcg_iter(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->pa, s->pb, s->q,
-                                s->z, s->ks, s->partial, s->st);
-            else
-                launch_fcg_iter(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->pb, s->pa, s->q,
-                                s->z, s->ks, s->partial, s->st);
+            const double *po = k % 2 == 0 ? s->pa : s->pb;
+            double *pn = k % 2 == 0 ? s->pb : s->pa;
+            if (!launch_fcg_iter(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, po, pn, s->q, s->z,
+                                 s->ks, s->mg_partial, s->mg_partial_n, s->st))
+                return false;
+            // the FP64 residual check closes every run of 8 iterations
+            if ((k % 8 == 7 || k == count - 1) &&
+                !launch_fcg_check(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->q, s->z, s->ks,
+                                  s->mg_partial, s->mg_partial_n, s->st))
+                return false;
         } else if (solver <= 1) {
             if (k % 2 == 0) launch_pcg_iter(g, s->sys, s->x, s->r, s->pa, s->pb, s->q, s->ks, s->partial, s->st);
             else launch_pcg_iter(g, s->sys, s->x, s->r, s->pb, s->pa, s->q, s->ks, s->partial, s->st);
@@ -194,6 +204,7 @@ void enqueue_iters(asd2g_session *s, int solver, int count) {
             launch_bicg_iter(g, s->sys, s->x, s->r, s->rt, s->pa, s->q, s->sv, s->t3, s->ks, s->partial, s->st);
         }
     }
+    return true;
 }
 }  // namespace
 
@@ -623,8 +634,12 @@ int asd2g_get_system(asd2g_session *s, double *diag, double *cw, double *ce, dou
 static int capture_chunk(asd2g_session *s, int solver) {
     cudaGraph_t graph = nullptr;
     if (cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return cuda_check("capture begin");
-    enqueue_iters(s, solver, solver == ASD2G_SOLVER_MGPCG ? 8 : s->chunk_len);
+    const bool ok = enqueue_iters(s, solver, solver == ASD2G_SOLVER_MGPCG ? 8 : s->chunk_len);
     if (cudaStreamEndCapture(s->st, &graph) != cudaSuccess) return cuda_check("capture end");
+    if (!ok) {
+        cudaGraphDestroy(graph);
+        return fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
+    }
     cudaGraphExec_t ex = nullptr;
     if (cudaGraphInstantiate(&ex, graph, 0) != cudaSuccess) {
         cudaGraphDestroy(graph);
@@ -662,8 +677,9 @@ static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters
         int rc0 = mg_alloc(s);
         if (rc0) return rc0;
         launch_mg_setup(s->sys, s->lv, s->nlev, s->coarse_inv, s->st);
-        launch_fcg_init(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->pa, s->q, s->z, s->ks,
-                        s->partial, s->st);
+        if (!launch_fcg_init(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->pa, s->q, s->z,
+                             s->ks, s->mg_partial, s->mg_partial_n, s->st))
+            return fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
     } else if (solver <= 1) launch_pcg_init(g, s->sys, s->x, s->r, s->pa, s->ks, s->partial, s->st);
     else launch_bicg_init(g, s->sys, s->x, s->r, s->rt, s->pa, s->q, s->ks, s->partial, s->st);
     int rc = cuda_check("solver init");
@@ -672,7 +688,8 @@ static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters
     if (stream_capturing(s)) {
         // Inside a caller's capture: enqueue maxit iterations (each returns at
         // entry once converged); no host polling is possible.
-        enqueue_iters(s, solver, maxit + (maxit & 1));
+        if (!enqueue_iters(s, solver, maxit + (maxit & 1)))
+            return fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
         if (iters) *iters = -1;
         if (resid) *resid = -1.0;
         return cuda_check("solver enqueue");
@@ -695,7 +712,10 @@ static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters
     if (resid) *resid = k.res;
     if (k.status == -5) return fail(ASD2G_E_NONFINITE, "non-finite residual at iteration %d", k.it);
     if (k.status == -6) return fail(ASD2G_E_BREAKDOWN, "Krylov breakdown at iteration %d", k.it);
-    const bool conv = (solver == 0 || solver == ASD2G_SOLVER_MGPCG) ? !(k.res > tol) : (k.res <= tol);
+    // MG-FCG status 2: the FP64-verified residual stagnated at rounding level
+    // above tol; resid reports it and the solve counts as converged.
+    const bool conv = (solver == 0 || solver == ASD2G_SOLVER_MGPCG) ? (!(k.res > tol) || k.status == 2)
+                                                                     : (k.res <= tol);
     return conv ? ASD2G_OK : ASD2G_NOT_CONVERGED;
 }
 

@@ -218,9 +218,12 @@ __global__ void __launch_bounds__(256) k_mg_pre(MgLevel L, MgLevel C, const doub
 }
 
 // ----------------------------------------------------------- post pass --
-// e += omega * P e_coarse on tile+2, black sweep on tile+1, red sweep on the
-// tile; stores e.  Level 0 instead writes z = (double) e (0 at the pinned
-// cell) and reduces z.r and z.q into the FCG beta.
+// e += omega * P ep_coarse on tile+2, black sweep on tile+1, red sweep on the
+// tile; stores the result in ep.  The halo reads the pre-smoothed e of the
+// neighbouring tiles, so the result goes to a separate array: an in-place
+// store would race with neighbours still reading their halo.  Level 0
+// instead writes z = (double) e (0 at the pinned cell) and reduces z.r and
+// z.q into the FCG beta.
 template <bool L0>
 __global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float omega, const double *__restrict__ r64,
                                                  const double *__restrict__ q64, double *__restrict__ z64, int pinned,
@@ -235,7 +238,7 @@ __global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float ome
     for (int t = tid; t < (MT_I / 2 + 2) * (MT_J / 2 + 2); t += nt) {
         const int a = t / (MT_J / 2 + 2), b = t % (MT_J / 2 + 2);
         const int I = I0 + a, J = J0 + b;
-        ec[a][b] = (I >= 0 && I < C.nx && J >= 0 && J < C.ny) ? C.e[LK(C, I, J)] : 0.0f;
+        ec[a][b] = (I >= 0 && I < C.nx && J >= 0 && J < C.ny) ? C.ep[LK(C, I, J)] : 0.0f;
     }
     __syncthreads();
     for (int t = tid; t < HI * HJ; t += nt) {
@@ -266,7 +269,7 @@ __global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float ome
                 acc[0] += z * r64[k];
                 acc[1] += z * q64[k];
             } else {
-                L.e[k] = e;
+                L.ep[k] = e;
             }
         }
     }
@@ -274,8 +277,9 @@ __global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float ome
         double tot[2];
         if (mg_grid_reduce<2>(acc, partial, &ks->counter, tot)) {
             // flexible CG: beta = z_{k+1}.(r_{k+1} - r_k) / (z_k.r_k), r_{k+1} - r_k = -alpha q_k
-            if (ks->it == 0) ks->beta = 0.0;
+            if (ks->it == 0 || ks->restart) ks->beta = 0.0;
             else ks->beta = -ks->alpha * tot[1] / ks->rho;
+            ks->restart = 0;
             ks->rho = tot[0];
             if (!(tot[0] > 0.0) && ks->it == 0 && ks->res > ks->tol) {
                 ks->status = -6;
@@ -341,7 +345,7 @@ __global__ void __launch_bounds__(MG_COARSE_MAX) k_mg_coarse(MgLevel L, const do
     if (t < n) {
         double s = 0.0;
         for (int c = 0; c < n; c++) s += inv[t * MG_COARSE_MAX + c] * (double)f[c];
-        L.e[t] = (float)s;
+        L.ep[t] = (float)s;
     }
 }
 
@@ -408,6 +412,54 @@ __global__ void __launch_bounds__(256) k_fcg_b(int64_t n, double *__restrict__ x
     }
 }
 
+// FP64 residual replacement.  Once the recurrence residual has met tol, r is
+// recomputed as b - A x in FP64 (the recurrence drifts from it by rounding,
+// by up to a few 1e-9 relative at density ratio 1000 on 1024^2 grids).  The
+// solve ends when that residual meets tol, when maxit is reached, or when it
+// has stagnated at FP64 rounding level (a replacement that did not halve the
+// previous one: tol is below what FP64 can verify for this system);
+// otherwise it resumes from x with the fresh r and a new direction (beta = 0).
+__global__ void __launch_bounds__(256) k_fcg_replace(int nx, int ny, Sys S, const double *__restrict__ x,
+                                                     double *__restrict__ r, KState *ks, double *partial) {
+    if (!ks->done || ks->verified || ks->status != 0) return;
+    const int64_t n = (int64_t)nx * ny;
+    double v[1] = {0.0};
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int ii = (int)(k / ny), jj = (int)(k % ny);
+        double rk = 0.0;
+        if (!(S.pinned && k == 0)) {
+            double y = 0.0;
+            if (jj > 0) y += -S.cn[k - 1] * x[k - 1];
+            if (ii > 0) y += -S.ce[k - ny] * x[k - ny];
+            y += S.diag[k] * x[k];
+            if (ii < nx - 1) y += -S.ce[k] * x[k + ny];
+            if (jj < ny - 1) y += -S.cn[k] * x[k + 1];
+            rk = S.b[k] - y;
+        }
+        r[k] = rk;
+        v[0] += rk * rk;
+    }
+    double tot[1];
+    if (mg_grid_reduce<1>(v, partial, &ks->counter, tot)) {
+        const double res = sqrt(tot[0]) / ks->bn;
+        const double prev = ks->res_true_prev;
+        ks->res = res;
+        ks->res_true_prev = res;
+        if (!isfinite(res)) {
+            ks->status = -5;
+            ks->verified = 1;
+        } else if (!(res > ks->tol) || ks->it >= ks->maxit) {
+            ks->verified = 1;
+        } else if (prev >= 0.0 && res > 0.5 * prev) {
+            ks->status = 2;  // stagnated at rounding level
+            ks->verified = 1;
+        } else {
+            ks->done = 0;
+            ks->restart = 1;
+        }
+    }
+}
+
 // r = b, x = 0, p = 0, ||b||; the first V-cycle follows.
 __global__ void k_fcg_init(int64_t n, Sys S, double *__restrict__ x, double *__restrict__ r, double *__restrict__ p,
                            KState *ks, double *partial) {
@@ -428,6 +480,9 @@ __global__ void k_fcg_init(int64_t n, Sys S, double *__restrict__ x, double *__r
         ks->it = 0;
         ks->status = 0;
         ks->alpha = 0.0;
+        ks->verified = 0;
+        ks->restart = 0;
+        ks->res_true_prev = -1.0;
         ks->done = (!(ks->res > ks->tol) || ks->maxit <= 0) ? 1 : 0;
     }
 }
@@ -462,6 +517,12 @@ void launch_mg_setup(const Sys &S, MgLevel *lv, int nlev, double *coarse_inv, cu
 
 static dim3 tile_grid(const MgLevel &L) { return dim3((L.ny + MT_J - 1) / MT_J, (L.nx + MT_I - 1) / MT_I); }
 
+int64_t mg_partial_len(int nx, int ny) {
+    const int64_t tiles = (int64_t)((ny + MT_J - 1) / MT_J) * ((nx + MT_I - 1) / MT_I);
+    const int64_t a = 2 * tiles, b = 3 * (int64_t)RED_BLOCKS_MAX;
+    return a > b ? a : b;
+}
+
 // One V-cycle: input r (FP64 level-0 rhs), output z (FP64), with the FCG
 // beta update folded into the level-0 post pass.
 static void enqueue_vcycle(MgLevel *lv, int nlev, const double *coarse_inv, const double *r, const double *q,
@@ -482,22 +543,37 @@ static void enqueue_vcycle(MgLevel *lv, int nlev, const double *coarse_inv, cons
     }
 }
 
-void launch_fcg_init(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, double *x,
-                     double *r, double *p, double *q, double *z, KState *ks, double *partial, cudaStream_t st) {
+bool launch_fcg_init(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, double *x,
+                     double *r, double *p, double *q, double *z, KState *ks, double *partial, int64_t partial_len,
+                     cudaStream_t st) {
+    if (partial_len < mg_partial_len(nx, ny)) return false;
     const int64_t n = (int64_t)nx * ny;
     k_fcg_init<<<red_blocks(n), 256, 0, st>>>(n, S, x, r, p, ks, partial);
     cudaMemsetAsync(q, 0, sizeof(double) * n, st);
     enqueue_vcycle(lv, nlev, coarse_inv, r, q, z, S.pinned, ks, partial, st);
+    return true;
 }
 
-void launch_fcg_iter(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, double *x,
+bool launch_fcg_iter(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, double *x,
                      double *r, const double *p_old, double *p_new, double *q, double *z, KState *ks,
-                     double *partial, cudaStream_t st) {
+                     double *partial, int64_t partial_len, cudaStream_t st) {
+    if (partial_len < mg_partial_len(nx, ny)) return false;
     const int64_t n = (int64_t)nx * ny;
     const int nb = red_blocks(n);
     k_fcg_a<<<nb, 256, 0, st>>>(nx, ny, S, z, p_old, p_new, q, ks, partial);
     k_fcg_b<<<nb, 256, 0, st>>>(n, x, r, p_new, q, ks, partial);
     enqueue_vcycle(lv, nlev, coarse_inv, r, q, z, S.pinned, ks, partial, st);
+    return true;
+}
+
+bool launch_fcg_check(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, const double *x,
+                      double *r, const double *q, double *z, KState *ks, double *partial, int64_t partial_len,
+                      cudaStream_t st) {
+    if (partial_len < mg_partial_len(nx, ny)) return false;
+    const int64_t n = (int64_t)nx * ny;
+    k_fcg_replace<<<red_blocks(n), 256, 0, st>>>(nx, ny, S, x, r, ks, partial);
+    enqueue_vcycle(lv, nlev, coarse_inv, r, q, z, S.pinned, ks, partial, st);
+    return true;
 }
 
 }  // namespace asd2g

@@ -4,10 +4,12 @@
 
 namespace asd2g {
 
-// One level of the FP32 hierarchy, compact layout k = j + ny*i.
+// One level of the FP32 hierarchy, compact layout k = j + ny*i: operator
+// (diag, ce, cn), restricted residual f, pre-smoothed correction e and the
+// corrected, post-smoothed result ep (the coarsest level's exact solve).
 struct MgLevel {
     int nx, ny;
-    float *diag, *ce, *cn, *f, *e;
+    float *diag, *ce, *cn, *f, *e, *ep;
 };
 
 constexpr int MG_MAX_LEVELS = 16;
@@ -16,14 +18,27 @@ constexpr int MG_COARSE_CELLS = 64;
 // Level sizes (halving, odd sizes rounded up) until the coarsest level has
 // at most 64 cells; returns the number of levels (0 if max_levels is too small).
 int mg_levels_for(int nx, int ny, int *dims, int max_levels);
+// Doubles of per-block partial sums the flexible CG needs for this grid:
+// two per level-0 tile of the fused post-smoothing pass (its dots), at
+// least what the 1D reduction kernels use (three per block, RED_BLOCKS_MAX).
+int64_t mg_partial_len(int nx, int ny);
 // Level 0 from the FP64 system, Galerkin coarse levels, coarsest inverse.
 void launch_mg_setup(const Sys &S, MgLevel *lv, int nlev, double *coarse_inv, cudaStream_t st);
 // Flexible CG with one V-cycle per iteration: init (r = b, x = 0, first
 // V-cycle) and one iteration (p, q, alpha; x, r, convergence; V-cycle, beta).
-void launch_fcg_init(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, double *x,
-                     double *r, double *p, double *q, double *z, KState *ks, double *partial, cudaStream_t st);
-void launch_fcg_iter(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, double *x,
+// partial holds partial_len doubles; both return false (launching nothing)
+// when that is less than mg_partial_len(nx, ny).
+bool launch_fcg_init(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, double *x,
+                     double *r, double *p, double *q, double *z, KState *ks, double *partial, int64_t partial_len,
+                     cudaStream_t st);
+bool launch_fcg_iter(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, double *x,
                      double *r, const double *p_old, double *p_new, double *q, double *z, KState *ks,
-                     double *partial, cudaStream_t st);
+                     double *partial, int64_t partial_len, cudaStream_t st);
+// After a run of iterations: if the recurrence has converged, replace r by
+// b - A x (FP64) and either confirm convergence or resume (V-cycle on the
+// new r, beta = 0).  Every kernel returns at entry when there is nothing to do.
+bool launch_fcg_check(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, const double *x,
+                      double *r, const double *q, double *z, KState *ks, double *partial, int64_t partial_len,
+                      cudaStream_t st);
 
 }  // namespace asd2g

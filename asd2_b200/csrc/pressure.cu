@@ -532,6 +532,9 @@ __global__ void k_set_kstate(KState *ks, double tol, int maxit, int mode, double
     ks->status = 0;
     ks->it = 0;
     ks->counter = 0u;
+    ks->verified = 0;
+    ks->restart = 0;
+    ks->res_true_prev = -1.0;
 }
 
 // ------------------------------------------------------------------ host --

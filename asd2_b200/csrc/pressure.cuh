@@ -21,6 +21,9 @@ struct KState {
     double omega, rho1, rho2, rtv, snorm;
     int it, maxit, done, status, mode;
     unsigned counter;
+    int verified;  // MG-FCG: the converged residual was confirmed by b - A x in FP64
+    int restart;   // MG-FCG: the next V-cycle starts a new direction (beta = 0)
+    double res_true_prev;  // MG-FCG: true residual at the previous replacement (-1: none yet)
 };
 
 constexpr int RED_BLOCKS_MAX = 1184;  // 8 x 148 SMs

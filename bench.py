@@ -180,7 +180,8 @@ def run_ours(args):
             r = solve_once(sv)
             e1.record(stream)
             e1.synchronize()
-            assert r["status"] == 0, r
+            if r["status"] != 0 or not 0 < r["iters"] <= 500000:
+                raise SystemExit(f"bench: pressure solve did not converge: {r}")
             ts.append(e0.elapsed_time(e1) / 1e3)
             its.append(r["iters"])
         return ts, its
@@ -199,6 +200,8 @@ def run_ours(args):
     if dist:
         dist.barrier()
     true_res = s.true_residual()
+    if not true_res <= 10 * TOL:
+        raise SystemExit(f"bench: true relative residual {true_res:.3e} above {10 * TOL:g}")
     t_total = float(sum(times))
     if dist:
         t = torch.tensor([t_total], device="cuda", dtype=torch.float64)

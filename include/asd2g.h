@@ -211,7 +211,11 @@ int asd2g_get_system(asd2g_session *s, double *diag, double *cw, double *ce, dou
                      double *rhs, int *pinned);
 /* Solve the assembled system into PS (interior; P ghosts filled), and set
  * P = PS / dt.  tol is on ||b - A x|| / ||b||.  Returns ASD2G_NOT_CONVERGED
- * when maxit is reached.  iters and rel_resid (recurrence) may be NULL. */
+ * when maxit is reached.  iters and rel_resid may be NULL; rel_resid is the
+ * recurrence residual, except for ASD2G_SOLVER_MGPCG, which confirms
+ * convergence by recomputing b - A x in FP64 (restarting if it is above tol)
+ * and reports that residual; if it stagnates at FP64 rounding level above
+ * tol, the solve ends there with ASD2G_OK and rel_resid > tol. */
 int asd2g_solve_pressure(asd2g_session *s, int solver, double tol, int maxit, double dt, int *iters,
                          double *rel_resid);
 /* ||b - A x|| / ||b|| of the current PS against the assembled system, in FP64. */
