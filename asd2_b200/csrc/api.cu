@@ -159,6 +159,7 @@ int mg_alloc(asd2g_session *s) {
     if (rc == ASD2G_OK) rc = dalloc(s, &s->mg_partial, (size_t)np);
     if (rc) return rc;
     s->mg_partial_n = np;
+    if (!mg_cta_prepare(s->lv, n)) return fail(ASD2G_E_UNSUPPORTED, "multigrid coarse cycle does not fit a CTA");
     s->nlev = n;
     return ASD2G_OK;
 }

@@ -294,59 +294,186 @@ __global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float ome
 // inverse is formed once per assembly (Gauss-Jordan in FP64 in one CTA; the
 // aggregated operator is SPD, so no pivoting is needed) and each V-cycle
 // applies it as one small matrix-vector product.
-__global__ void __launch_bounds__(MG_COARSE_MAX) k_mg_coarse_invert(MgLevel L, double *inv) {
+// Augmented [A | I] of n x 2n doubles, row stride 2 * MG_COARSE_MAX; 32 x 32
+// threads (ty: rows, tx: columns) eliminate each pivot step in parallel.
+constexpr int MG_INV_THREADS = 1024;
+__global__ void __launch_bounds__(MG_INV_THREADS) k_mg_coarse_invert(MgLevel L, double *inv) {
     extern __shared__ double sm[];
-    constexpr int W = MG_COARSE_MAX + 1;
-    double *A = sm, *B = sm + MG_COARSE_MAX * W, *col = sm + 2 * MG_COARSE_MAX * W;
-    const int n = L.nx * L.ny, ny = L.ny, t = threadIdx.x;
-    for (int r = 0; r < n; r++)
-        if (t < n) {
-            A[r * W + t] = 0.0;
-            B[r * W + t] = (r == t) ? 1.0 : 0.0;
-        }
+    constexpr int W = 2 * MG_COARSE_MAX;
+    double *M = sm, *col = sm + MG_COARSE_MAX * W;
+    const int n = L.nx * L.ny, ny = L.ny, tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+    for (int r = ty; r < n; r += 32)
+        for (int c = tx; c < 2 * n; c += 32) M[r * W + c] = (c == n + r) ? 1.0 : 0.0;
     __syncthreads();
-    if (t < n) {
-        const int i = t / ny, j = t % ny;
-        A[t * W + t] = L.diag[t];
-        if (i < L.nx - 1) A[t * W + t + ny] = A[(t + ny) * W + t] = -(double)L.ce[t];
-        if (j < ny - 1) A[t * W + t + 1] = A[(t + 1) * W + t] = -(double)L.cn[t];
+    if (tid < n) {
+        const int t = tid, i = t / ny, j = t % ny;
+        M[t * W + t] = L.diag[t];
+        if (i < L.nx - 1) M[t * W + t + ny] = M[(t + ny) * W + t] = -(double)L.ce[t];
+        if (j < ny - 1) M[t * W + t + 1] = M[(t + 1) * W + t] = -(double)L.cn[t];
     }
     __syncthreads();
-    // Gauss-Jordan; thread t owns column t of A and B
     for (int c = 0; c < n; c++) {
-        const double piv = A[c * W + c];
+        const double rpiv = 1.0 / M[c * W + c];
+        if (tid < n) col[tid] = M[tid * W + c];
         __syncthreads();
-        if (t < n) {
-            A[c * W + t] /= piv;
-            B[c * W + t] /= piv;
+        if (tid < 2 * n) M[c * W + tid] *= rpiv;
+        __syncthreads();
+        for (int r = ty; r < n; r += 32) {
+            if (r == c) continue;
+            const double f = col[r];
+            for (int t = tx; t < 2 * n; t += 32) M[r * W + t] -= f * M[c * W + t];
         }
         __syncthreads();
-        if (t < n) col[t] = A[t * W + c];
+    }
+    for (int r = ty; r < n; r += 32)
+        for (int c = tx; c < n; c += 32) inv[r * MG_COARSE_MAX + c] = M[r * W + n + c];
+}
+
+// ------------------------------------------------------ coarse V-cycle --
+// Levels s .. nlev-1 (level s has at most MG_CTA_CELLS cells) in ONE CTA:
+// every level's operator, restricted residual and correction live in shared
+// memory, the sweeps are separated by __syncthreads instead of kernel
+// boundaries, and the coarsest level is solved with its dense inverse.  Same
+// sweeps as the tile kernels (red from zero, black; residual, 2x2
+// restriction; descend; coarsest; prolongation with omega, black, red), so
+// the preconditioner is the same.  Reads lv[s].f, writes lv[s].ep.
+constexpr int MG_CTA_CELLS = 4096;
+constexpr int MG_CTA_THREADS = 1024;
+
+struct MgHier {
+    MgLevel l[MG_MAX_LEVELS];
+};
+
+__host__ __device__ inline size_t mg_cta_smem(const MgHier &H, int s, int nlev) {
+    size_t n = 0;
+    for (int l = s; l < nlev; l++) n += 5 * (size_t)H.l[l].nx * H.l[l].ny;
+    return n * sizeof(float);
+}
+
+__global__ void __launch_bounds__(MG_CTA_THREADS) k_mg_cta_cycle(MgHier H, int s, int nlev,
+                                                                const double *__restrict__ inv, float omega,
+                                                                const KState *ks) {
+    if (ks->done) return;
+    extern __shared__ float smf[];
+    // 32 x 32 threads: ty walks rows i, tx columns j (no integer division)
+    const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+    size_t off[MG_MAX_LEVELS];
+    {
+        size_t o = 0;
+        for (int l = s; l < nlev; l++) {
+            off[l] = o;
+            o += 5 * (size_t)H.l[l].nx * H.l[l].ny;
+        }
+    }
+    for (int l = s; l < nlev; l++) {
+        const MgLevel &L = H.l[l];
+        const int n = L.nx * L.ny;
+        float *D = smf + off[l], *CE = D + n, *CN = CE + n, *F = CN + n;
+        for (int k = tid; k < n; k += MG_CTA_THREADS) {
+            D[k] = L.diag[k];
+            CE[k] = L.ce[k];
+            CN[k] = L.cn[k];
+            if (l == s) F[k] = L.f[k];
+        }
+    }
+    __syncthreads();
+    for (int l = s; l < nlev - 1; l++) {
+        const int nx = H.l[l].nx, ny = H.l[l].ny, n = nx * ny;
+        const float *D = smf + off[l], *CE = D + n, *CN = CE + n, *F = CN + n;
+        float *E = smf + off[l] + 4 * (size_t)n;
+        // red from zero (e = f / d) and black from those red values, in one
+        // pass: a black cell evaluates its red neighbours' f / d itself
+        for (int i = ty; i < nx; i += 32)
+            for (int j = tx; j < ny; j += 32) {
+                const int k = j + ny * i;
+                if (((i + j) & 1) == 0) {
+                    E[k] = F[k] / D[k];
+                } else {
+                    float acc = F[k];
+                    if (i > 0) acc += CE[k - ny] * (F[k - ny] / D[k - ny]);
+                    if (i < nx - 1) acc += CE[k] * (F[k + ny] / D[k + ny]);
+                    if (j > 0) acc += CN[k - 1] * (F[k - 1] / D[k - 1]);
+                    if (j < ny - 1) acc += CN[k] * (F[k + 1] / D[k + 1]);
+                    E[k] = acc / D[k];
+                }
+            }
         __syncthreads();
-        if (t < n)
-            for (int r = 0; r < n; r++) {
-                if (r == c) continue;
-                A[r * W + t] -= col[r] * A[c * W + t];
-                B[r * W + t] -= col[r] * B[c * W + t];
+        const int cnx = H.l[l + 1].nx, cny = H.l[l + 1].ny;
+        float *Fc = smf + off[l + 1] + 3 * (size_t)cnx * cny;
+        for (int I = ty; I < cnx; I += 32)
+            for (int J = tx; J < cny; J += 32) {
+                float sum = 0.0f;
+#pragma unroll
+                for (int a = 0; a < 2; a++)
+#pragma unroll
+                    for (int b = 0; b < 2; b++) {
+                        const int i = 2 * I + a, j = 2 * J + b;
+                        if (i >= nx || j >= ny) continue;
+                        const int k = j + ny * i;
+                        float Ae = D[k] * E[k];
+                        if (i > 0) Ae -= CE[k - ny] * E[k - ny];
+                        if (i < nx - 1) Ae -= CE[k] * E[k + ny];
+                        if (j > 0) Ae -= CN[k - 1] * E[k - 1];
+                        if (j < ny - 1) Ae -= CN[k] * E[k + 1];
+                        sum += F[k] - Ae;
+                    }
+                Fc[J + cny * I] = sum;
             }
         __syncthreads();
     }
-    for (int r = 0; r < n; r++)
-        if (t < n) inv[r * MG_COARSE_MAX + t] = B[r * W + t];
-}
-
-__global__ void __launch_bounds__(MG_COARSE_MAX) k_mg_coarse(MgLevel L, const double *__restrict__ inv,
-                                                             const KState *ks) {
-    if (ks->done) return;
-    __shared__ float f[MG_COARSE_MAX];
-    const int n = L.nx * L.ny, t = threadIdx.x;
-    if (t < n) f[t] = L.f[t];
-    __syncthreads();
-    if (t < n) {
-        double s = 0.0;
-        for (int c = 0; c < n; c++) s += inv[t * MG_COARSE_MAX + c] * (double)f[c];
-        L.ep[t] = (float)s;
+    {
+        // e = inv f on the coarsest level (<= 64 cells): 16 lanes per row
+        const int l = nlev - 1, n = H.l[l].nx * H.l[l].ny;
+        const float *F = smf + off[l] + 3 * (size_t)n;
+        float *E = smf + off[l] + 4 * (size_t)n;
+        const int row = tid >> 4, c = tid & 15;
+        double acc = 0.0;
+        if (row < n)
+#pragma unroll
+            for (int q = 0; q < MG_COARSE_MAX / 16; q++)
+                if (c + 16 * q < n) acc += inv[row * MG_COARSE_MAX + c + 16 * q] * (double)F[c + 16 * q];
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, 16);
+        if (row < n && c == 0) E[row] = (float)acc;
+        __syncthreads();
     }
+    for (int l = nlev - 2; l >= s; l--) {
+        const int nx = H.l[l].nx, ny = H.l[l].ny, n = nx * ny;
+        const int cny = H.l[l + 1].ny, cn = H.l[l + 1].nx * cny;
+        const float *D = smf + off[l], *CE = D + n, *CN = CE + n, *F = CN + n;
+        float *E = smf + off[l] + 4 * (size_t)n;
+        const float *Ec = smf + off[l + 1] + 4 * (size_t)cn;
+        // prolongation fused into the black sweep: a black cell reads its red
+        // neighbours as e + omega * e_coarse (its own old value is not used)
+        auto pe = [&](int k, int i, int j) { return E[k] + omega * Ec[(j >> 1) + cny * (i >> 1)]; };
+        for (int i = ty; i < nx; i += 32)
+            for (int j = 2 * tx + ((i + 1) & 1); j < ny; j += 64) {
+                // black cells: lane tx takes j = 2 tx + ((i + 1) & 1) + 64 m
+                const int k = j + ny * i;
+                float acc = F[k];
+                if (i > 0) acc += CE[k - ny] * pe(k - ny, i - 1, j);
+                if (i < nx - 1) acc += CE[k] * pe(k + ny, i + 1, j);
+                if (j > 0) acc += CN[k - 1] * pe(k - 1, i, j - 1);
+                if (j < ny - 1) acc += CN[k] * pe(k + 1, i, j + 1);
+                E[k] = acc / D[k];
+            }
+        __syncthreads();
+        for (int i = ty; i < nx; i += 32)
+            for (int j = 2 * tx + (i & 1); j < ny; j += 64) {
+                // red cells from the new black values
+                const int k = j + ny * i;
+                float acc = F[k];
+                if (i > 0) acc += CE[k - ny] * E[k - ny];
+                if (i < nx - 1) acc += CE[k] * E[k + ny];
+                if (j > 0) acc += CN[k - 1] * E[k - 1];
+                if (j < ny - 1) acc += CN[k] * E[k + 1];
+                E[k] = acc / D[k];
+            }
+        __syncthreads();
+    }
+    const int n = H.l[s].nx * H.l[s].ny;
+    const float *E = smf + off[s] + 4 * (size_t)n;
+    for (int k = tid; k < n; k += MG_CTA_THREADS) H.l[s].ep[k] = E[k];
 }
 
 // ------------------------------------------------------------ FCG FP64 --
@@ -510,9 +637,9 @@ void launch_mg_setup(const Sys &S, MgLevel *lv, int nlev, double *coarse_inv, cu
         const int64_t n = (int64_t)lv[l].nx * lv[l].ny;
         k_mg_coarsen<<<red_blocks(n), 256, 0, st>>>(lv[l - 1], lv[l]);
     }
-    const size_t smem = sizeof(double) * (2 * MG_COARSE_MAX * (MG_COARSE_MAX + 1) + MG_COARSE_MAX);
+    const size_t smem = sizeof(double) * (MG_COARSE_MAX * 2 * MG_COARSE_MAX + MG_COARSE_MAX);
     cudaFuncSetAttribute(k_mg_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_mg_coarse_invert<<<1, MG_COARSE_MAX, smem, st>>>(lv[nlev - 1], coarse_inv);
+    k_mg_coarse_invert<<<1, MG_INV_THREADS, smem, st>>>(lv[nlev - 1], coarse_inv);
 }
 
 static dim3 tile_grid(const MgLevel &L) { return dim3((L.ny + MT_J - 1) / MT_J, (L.nx + MT_I - 1) / MT_I); }
@@ -523,18 +650,44 @@ int64_t mg_partial_len(int nx, int ny) {
     return a > b ? a : b;
 }
 
+// First level handled by the single-CTA coarse cycle: the first level
+// after level 0 with at most MG_CTA_CELLS cells.
+static int mg_cta_level(const MgLevel *lv, int nlev) {
+    int s = 1;
+    while (s < nlev - 1 && (int64_t)lv[s].nx * lv[s].ny > MG_CTA_CELLS) s++;
+    return s;
+}
+
+// Shared memory of the coarse cycle: level s has at most 4096 cells and each
+// coarser level at most half of the previous one plus one (a one-cell-wide
+// level halves in one direction only), so 5 floats x 8192 cells = 160 KiB
+// bounds every hierarchy; the kernel attribute is set to that bound (it is
+// process-wide, so it must cover every session's hierarchy).
+constexpr size_t MG_CTA_SMEM_BOUND = 5 * sizeof(float) * 2 * (size_t)MG_CTA_CELLS;
+bool mg_cta_prepare(const MgLevel *lv, int nlev) {
+    MgHier H{};
+    for (int l = 0; l < nlev; l++) H.l[l] = lv[l];
+    if (mg_cta_smem(H, mg_cta_level(lv, nlev), nlev) > MG_CTA_SMEM_BOUND) return false;
+    return cudaFuncSetAttribute(k_mg_cta_cycle, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)MG_CTA_SMEM_BOUND) == cudaSuccess;
+}
+
 // One V-cycle: input r (FP64 level-0 rhs), output z (FP64), with the FCG
-// beta update folded into the level-0 post pass.
+// beta update folded into the level-0 post pass.  Levels 0 .. s-1 run as
+// tile kernels over the whole GPU, levels s .. nlev-1 in one CTA.
 static void enqueue_vcycle(MgLevel *lv, int nlev, const double *coarse_inv, const double *r, const double *q,
                            double *z, int pinned, KState *ks, double *partial, cudaStream_t st) {
     const dim3 blk(32, 8);
-    for (int l = 0; l < nlev - 1; l++) {
+    const int s = mg_cta_level(lv, nlev);
+    for (int l = 0; l < s; l++) {
         if (l == 0) k_mg_pre<true><<<tile_grid(lv[0]), blk, 0, st>>>(lv[0], lv[1], r, ks);
         else k_mg_pre<false><<<tile_grid(lv[l]), blk, 0, st>>>(lv[l], lv[l + 1], nullptr, ks);
     }
-    k_mg_coarse<<<1, MG_COARSE_MAX, 0, st>>>(lv[nlev - 1], coarse_inv, ks);
+    MgHier H{};
+    for (int l = 0; l < nlev; l++) H.l[l] = lv[l];
     const float omega = 1.9f;
-    for (int l = nlev - 2; l >= 0; l--) {
+    k_mg_cta_cycle<<<1, MG_CTA_THREADS, mg_cta_smem(H, s, nlev), st>>>(H, s, nlev, coarse_inv, omega, ks);
+    for (int l = s - 1; l >= 0; l--) {
         if (l == 0)
             k_mg_post<true><<<tile_grid(lv[0]), blk, 0, st>>>(lv[0], lv[1], omega, r, q, z, pinned, ks, partial);
         else

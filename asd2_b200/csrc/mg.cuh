@@ -22,6 +22,9 @@ int mg_levels_for(int nx, int ny, int *dims, int max_levels);
 // two per level-0 tile of the fused post-smoothing pass (its dots), at
 // least what the 1D reduction kernels use (three per block, RED_BLOCKS_MAX).
 int64_t mg_partial_len(int nx, int ny);
+// Sets up the single-CTA coarse cycle for this hierarchy (its shared memory);
+// false if it does not fit (not reachable with <= 4096-cell CTA levels).
+bool mg_cta_prepare(const MgLevel *lv, int nlev);
 // Level 0 from the FP64 system, Galerkin coarse levels, coarsest inverse.
 void launch_mg_setup(const Sys &S, MgLevel *lv, int nlev, double *coarse_inv, cudaStream_t st);
 // Flexible CG with one V-cycle per iteration: init (r = b, x = 0, first
