@@ -31,6 +31,7 @@ REINIT_ORIGINAL, REINIT_SUSSMAN, REINIT_MINRK2, REINIT_FIRSTTIME, REINIT_MINRK2_
 PCG, PCG_REFERENCE, BICGSTAB, BICGSTAB_REFERENCE, MGPCG = range(5)
 NOT_CONVERGED = 1
 FLAG_NO_CLUSTER_PCG = 1
+PRECISION_FP64, PRECISION_MIXED = 0, 1
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "unsupported",
           -5: "non-finite value", -6: "Krylov breakdown"}
 
@@ -62,7 +63,7 @@ EXPORTS = [
     "asd2g_intermediate_vel", "asd2g_divergence", "asd2g_update_vel", "asd2g_update_dt",
     "asd2g_assemble_gfm", "asd2g_get_system", "asd2g_solve_pressure", "asd2g_true_residual",
     "asd2g_droplet_step", "asd2g_pcg_solve_static", "asd2g_weno5_line", "asd2g_weno_absgrad",
-    "asd2g_apply_bc_side", "asd2g_update_ntk", "asd2g_csr_solve",
+    "asd2g_apply_bc_side", "asd2g_update_ntk", "asd2g_csr_solve", "asd2g_volume", "asd2g_last_volume",
 ]
 
 _lib = None
@@ -106,6 +107,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_weno5_line": ([S, dp, dp, dp, D, I], I), "asd2g_weno_absgrad": ([S, I, I, I], I),
         "asd2g_apply_bc_side": ([S, I, C.c_char, I, I], I), "asd2g_update_ntk": ([S, I, I, I], I),
         "asd2g_csr_solve": ([S, I, I, ip, ip, dp, dp, dp, dp, D, I, C.POINTER(I), C.POINTER(D)], I),
+        "asd2g_volume": ([S, C.POINTER(D), C.POINTER(D)], I),
+        "asd2g_last_volume": ([S, C.POINTER(D), C.POINTER(D)], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -341,3 +344,14 @@ class Session:
         rc = self._check(self.L.asd2g_droplet_step(self.h, C.byref(d), reinit_mode, solver, tol, maxit,
                                                    C.byref(it), C.byref(res)))
         return dict(status=rc, dt_next=d.value, iters=it.value, resid=res.value)
+
+    def volume(self):
+        """FP64 (sum H dx dy, sum HS dx dy) of the current level set."""
+        a, b = C.c_double(), C.c_double()
+        self._check(self.L.asd2g_volume(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def last_volume(self):
+        a, b = C.c_double(), C.c_double()
+        self._check(self.L.asd2g_last_volume(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value

@@ -31,6 +31,7 @@ UNITS = {
     "pcg_static.cu": ["-fmad=false"],
     "pcg_cluster.cu": ["-fmad=false"],
     "mg.cu": [],
+    "levelset32.cu": [],
 }
 
 

@@ -8,6 +8,7 @@
 
 #include "asd2g.h"
 #include "mg.cuh"
+#include "ls32.cuh"
 
 namespace asd2g {
 // levelset.cu
@@ -30,6 +31,16 @@ DivH make_divh(double h) {
     const double m = std::frexp(h, &e);
     d.pow2 = (m == 0.5) ? 1 : 0;
     d.inv = d.pow2 ? std::ldexp(1.0, 1 - e) : 1.0 / h;
+    return d;
+}
+
+DivHT<float> make_divh_f(double h) {
+    DivHT<float> d;
+    d.h = (float)h;
+    int e = 0;
+    const float m = std::frexp(d.h, &e);
+    d.pow2 = (m == 0.5f) ? 1 : 0;
+    d.inv = d.pow2 ? std::ldexp(1.0f, 1 - e) : 1.0f / d.h;
     return d;
 }
 
@@ -118,6 +129,8 @@ struct asd2g_session {
     int nlev = 0;
     double *coarse_inv = nullptr, *z = nullptr;
     double *mg_partial = nullptr;  // per-tile partial sums of the V-cycle's fused dots
+    Ls32Work w32{};                // FP32 level-set work arrays (precision = mixed)
+    double last_volume[2] = {0.0, 0.0};  // volume check of the last droplet step (sharp, smoothed)
     int64_t mg_partial_n = 0;
     int chunk_len = 64;
     std::vector<void *> allocs;
@@ -221,7 +234,8 @@ int asd2g_create(const asd2g_params *p, void *stream, asd2g_session **out) {
     if (p->nx < 4 || p->ny < 4) return fail(ASD2G_E_ARG, "grid must be at least 4 x 4 cells, got %d x %d", p->nx, p->ny);
     if ((int64_t)(p->nx + 6) * (p->ny + 6) > (int64_t)1 << 31)
         return fail(ASD2G_E_ARG, "grid %d x %d too large", p->nx, p->ny);
-    if (p->precision != 0) return fail(ASD2G_E_UNSUPPORTED, "precision %d: only FP64 (0) is implemented", p->precision);
+    if (p->precision != ASD2G_PRECISION_FP64 && p->precision != ASD2G_PRECISION_MIXED)
+        return fail(ASD2G_E_ARG, "precision %d: expected ASD2G_PRECISION_FP64 or _MIXED", p->precision);
     if (!(p->dx > 0.0) || !(p->dy > 0.0)) return fail(ASD2G_E_ARG, "dx, dy must be positive");
     for (int k = 0; k < 4; k++)
         if (p->bc_u[k] < 0 || p->bc_u[k] > 9 || p->bc_v[k] < 0 || p->bc_v[k] > 9 || p->bc_p[k] < 0 || p->bc_p[k] > 9)
@@ -251,6 +265,10 @@ int asd2g_create(const asd2g_params *p, void *stream, asd2g_session **out) {
     }
     g.p_mirror = mirror ? 1 : 0;
     g.pinned = pinned ? 1 : 0;
+    if (p->precision == ASD2G_PRECISION_MIXED && !g.p_mirror) {
+        delete s;
+        return fail(ASD2G_E_UNSUPPORTED, "mixed precision needs Neumann or Dirichlet pressure on all four sides");
+    }
     MomParams mp{p->rho_h, p->rho_l, p->mu_h, p->mu_l, p->sigma, p->gravity, p->cfl, p->g_axis, p->fix_gravity,
                  p->numbers_given, p->re, p->we, p->fr};
     s->M = make_momconst(g, mp);
@@ -275,6 +293,19 @@ int asd2g_create(const asd2g_params *p, void *stream, asd2g_session **out) {
     for (double **pp : nw)
         if (rc == ASD2G_OK) rc = dalloc(s, pp, N);
     if (rc == ASD2G_OK) rc = dalloc(s, &s->t3, 3 * N);
+    if (rc == ASD2G_OK && p->precision == ASD2G_PRECISION_MIXED) {
+        float **fw[LS32_ARRAYS] = {&s->w32.phi, &s->w32.ls0, &s->w32.a, &s->w32.b, &s->w32.tu, &s->w32.tv};
+        for (float **pp : fw) {
+            if (rc != ASD2G_OK) break;
+            if (cudaMalloc(pp, sizeof(float) * G) != cudaSuccess) {
+                cudaGetLastError();
+                rc = fail(ASD2G_E_NOMEM, "FP32 work allocation failed");
+            } else {
+                s->allocs.push_back(*pp);
+                cudaMemsetAsync(*pp, 0, sizeof(float) * G, s->st);
+            }
+        }
+    }
     if (rc == ASD2G_OK) rc = dalloc(s, &s->partial, 3 * RED_BLOCKS_MAX + 2 * DT_BLOCKS);
     if (rc == ASD2G_OK) rc = dalloc(s, &s->dsc, 8);
     if (rc == ASD2G_OK) {
@@ -455,9 +486,39 @@ int asd2g_smoothed_sign(asd2g_session *s, int ls, int out) {
 }
 
 int asd2g_ls_step(asd2g_session *s, double dt, int reinit_mode) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    if (s->prm.precision == ASD2G_PRECISION_MIXED) {
+        if (!ls32_supported(s->g, reinit_mode))
+            return fail(ASD2G_E_UNSUPPORTED, "mixed precision implements reinit modes 0, 2 and 4, not %d", reinit_mode);
+        int rc = set_dt(s, dt);
+        if (rc) return rc;
+        launch_fill_p(s->g, s->f[ASD2G_LS], s->st);
+        launch_ls_step32(s->g, reinit_mode, s->prm.ls_max_atime, s->f[ASD2G_U], s->f[ASD2G_V], s->dsc,
+                         s->f[ASD2G_LS], s->w32, s->st);
+        return cuda_check("ls_step (mixed)");
+    }
     int rc = asd2g_ls_advect(s, dt);
     if (rc) return rc;
     return asd2g_reinit(s, reinit_mode);
+}
+
+int asd2g_last_volume(asd2g_session *s, double *sharp, double *smooth) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    if (sharp) *sharp = s->last_volume[0];
+    if (smooth) *smooth = s->last_volume[1];
+    return ASD2G_OK;
+}
+
+int asd2g_volume(asd2g_session *s, double *sharp, double *smooth) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    launch_heaviside(s->g, s->f[ASD2G_LS], s->f[ASD2G_H], s->f[ASD2G_HS], s->st);
+    launch_volume(s->g, s->f[ASD2G_H], s->f[ASD2G_HS], s->partial, s->counter + 1, s->dsc + 5, s->st);
+    cudaMemcpyAsync(s->dsc_host + 5, s->dsc + 5, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
+    int rc = sync(s);
+    if (rc) return rc;
+    if (sharp) *sharp = s->dsc_host[5];
+    if (smooth) *smooth = s->dsc_host[6];
+    return cuda_check("volume");
 }
 
 int asd2g_weno5_line(asd2g_session *s, const double *F, double *FP, double *FM, double d, int n) {
@@ -826,16 +887,27 @@ int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver
     rc = set_dt(s, *dt);
     if (rc) return rc;
     cudaMemcpyAsync(s->f[ASD2G_LSB], s->f[ASD2G_LS], sizeof(double) * s->G, cudaMemcpyDeviceToDevice, s->st);
-    // Solve_LevelSet_2D (dt from the device scalar)
+    // Solve_LevelSet_2D (dt from the device scalar) and the reinitialisation
     double *ls = s->f[ASD2G_LS];
-    launch_center_vel(g, s->f[ASD2G_U], s->f[ASD2G_V], s->tu, s->tv, s->st);
-    launch_fill_p(g, ls, s->st);
-    launch_ls_stage(1, g, ls, s->tu, s->tv, ls, s->w1, s->dsc, s->st);
-    launch_ls_stage(2, g, s->w1, s->tu, s->tv, ls, s->w2, s->dsc, s->st);
-    launch_ls_stage(3, g, s->w2, s->tu, s->tv, ls, ls, s->dsc, s->st);
-    launch_reinit(g, reinit_mode, s->prm.ls_max_atime, ls, s->f[ASD2G_LS0], s->w1, s->w2, s->w3, s->st);
+    const bool mixed = s->prm.precision == ASD2G_PRECISION_MIXED;
+    if (mixed) {
+        if (!ls32_supported(g, reinit_mode))
+            return fail(ASD2G_E_UNSUPPORTED, "mixed precision implements reinit modes 0, 2 and 4, not %d", reinit_mode);
+        launch_fill_p(g, ls, s->st);
+        launch_ls_step32(g, reinit_mode, s->prm.ls_max_atime, s->f[ASD2G_U], s->f[ASD2G_V], s->dsc, ls, s->w32,
+                         s->st);
+    } else {
+        launch_center_vel(g, s->f[ASD2G_U], s->f[ASD2G_V], s->tu, s->tv, s->st);
+        launch_fill_p(g, ls, s->st);
+        launch_ls_stage(1, g, ls, s->tu, s->tv, ls, s->w1, s->dsc, s->st);
+        launch_ls_stage(2, g, s->w1, s->tu, s->tv, ls, s->w2, s->dsc, s->st);
+        launch_ls_stage(3, g, s->w2, s->tu, s->tv, ls, ls, s->dsc, s->st);
+        launch_reinit(g, reinit_mode, s->prm.ls_max_atime, ls, s->f[ASD2G_LS0], s->w1, s->w2, s->w3, s->st);
+    }
     launch_kappa(g, ls, s->f[ASD2G_KAPPA], s->st);
     launch_heaviside(g, ls, s->f[ASD2G_H], s->f[ASD2G_HS], s->st);
+    // FP64 volume check of the new level set (read by asd2g_last_volume)
+    launch_volume(g, s->f[ASD2G_H], s->f[ASD2G_HS], s->partial, s->counter + 1, s->dsc + 5, s->st);
     rc = intermediate(s, ASD2G_HS);
     if (rc) return rc;
     launch_fill_uv(g, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->st);
@@ -851,12 +923,14 @@ int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver
     launch_update_vel(g, s->M, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->f[ASD2G_PS], ls, s->f[ASD2G_H],
                       s->f[ASD2G_KAPPA], s->f[ASD2G_U], s->f[ASD2G_V], s->dsc, s->st);
     launch_update_dt(g, s->M, s->f[ASD2G_U], s->f[ASD2G_V], s->partial, s->counter, s->dsc + 1, s->st);
-    cudaMemcpyAsync(s->dsc_host, s->dsc, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
+    cudaMemcpyAsync(s->dsc_host, s->dsc, sizeof(double) * 7, cudaMemcpyDeviceToHost, s->st);
     rc = sync(s);
     if (rc) return rc;
     rc = cuda_check("droplet_step");
     if (rc) return rc;
     *dt = s->dsc_host[1];
+    s->last_volume[0] = s->dsc_host[5];
+    s->last_volume[1] = s->dsc_host[6];
     return st;
 }
 

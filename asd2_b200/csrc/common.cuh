@@ -31,27 +31,28 @@ __host__ __device__ __forceinline__ int64_t IX(const Grid &g, int i, int j) { re
 // (bc2d.cpp:788-810 Neumann, :835-861 Dirichlet) derives from this cell.
 // Valid only when g.p_mirror is set; corners are never touched, as in the
 // reference.
-__device__ __forceinline__ void p_mirror_store(const Grid &g, double *a, int i, int j, double val) {
+template <typename T>
+__device__ __forceinline__ void p_mirror_store(const Grid &g, T *a, int i, int j, T val) {
     const int nx = g.nx, ny = g.ny;
     // W: a[t] = a[5-t]        (t = 0..2)  <- interior i = 3..5
     if (i <= 2 * NB - 1) {
         const int t = 2 * NB - 1 - i;
-        a[IX(g, t, j)] = g.kp[0] == K_NEU ? val : -val + 2.0 * g.cp[0];
+        a[IX(g, t, j)] = g.kp[0] == K_NEU ? val : -val + T(2.0) * T(g.cp[0]);
     }
     // E: a[nx+5-t] = a[nx+t]  (t = 0..2)  <- interior i = nx..nx+2
     if (i >= nx) {
         const int t = i - nx;
-        a[IX(g, nx + 2 * NB - t - 1, j)] = g.kp[1] == K_NEU ? val : -val + 2.0 * g.cp[1];
+        a[IX(g, nx + 2 * NB - t - 1, j)] = g.kp[1] == K_NEU ? val : -val + T(2.0) * T(g.cp[1]);
     }
     // S: a[.,t] = a[.,5-t]
     if (j <= 2 * NB - 1) {
         const int t = 2 * NB - 1 - j;
-        a[IX(g, i, t)] = g.kp[2] == K_NEU ? val : -val + 2.0 * g.cp[2];
+        a[IX(g, i, t)] = g.kp[2] == K_NEU ? val : -val + T(2.0) * T(g.cp[2]);
     }
     // N: a[., ny+5-t] = a[., ny+t]
     if (j >= ny) {
         const int t = j - ny;
-        a[IX(g, i, ny + 2 * NB - t - 1)] = g.kp[3] == K_NEU ? val : -val + 2.0 * g.cp[3];
+        a[IX(g, i, ny + 2 * NB - t - 1)] = g.kp[3] == K_NEU ? val : -val + T(2.0) * T(g.cp[3]);
     }
 }
 

@@ -10,12 +10,15 @@ namespace asd2g {
 // Division by a grid spacing.  When h is a power of two, x / h and
 // x * (1/h) are the same IEEE result, so the multiply is used; otherwise the
 // division is kept.  Either way the result equals the reference's x / h.
-struct DivH {
-    double h, inv;
+template <typename T>
+struct DivHT {
+    T h, inv;
     int pow2;
-    __device__ __forceinline__ double operator()(double x) const { return pow2 ? x * inv : x / h; }
+    __device__ __forceinline__ T operator()(T x) const { return pow2 ? x * inv : x / h; }
 };
+using DivH = DivHT<double>;
 DivH make_divh(double h);
+DivHT<float> make_divh_f(double h);
 
 // api.cu: set the thread's last-error text (read by asd2g_last_error)
 void asd2g_set_error_text(const char *msg);

@@ -1,153 +1,9 @@
-// Level-set kernels: HJ-WENO5 + TVD-RK3 advection (Solve_LevelSet_2D,
-// levelset2d.cpp:43-157) and the reinitialisation passes (:264-486, :560-893).
-//
-// Each kernel computes final interior values and, when the pressure-grid
-// boundary is Neumann/Dirichlet on all sides, also writes the ghost mirrors
-// of the cells it owns (p_mirror_store), which is what the reference's
-// ApplyBC_P_2D after the loop would produce.  Otherwise the host runs the
-// P fill after the kernel.
-#include "lsmath.cuh"
+// Level-set kernels in FP64 (the bit-exact path, built with -fmad=false):
+// the templated stencils of levelset_impl.cuh instantiated for double, the
+// reinitialisation driver and the building-block kernels of the ABI.
+#include "levelset_impl.cuh"
 
 namespace asd2g {
-
-// ------------------------------------------------------------------------
-// Velocity centring (levelset2d.cpp:50-54).
-__global__ void k_center_vel(Grid g, const double *__restrict__ u, const double *__restrict__ v,
-                             double *__restrict__ tu, double *__restrict__ tv) {
-    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
-    if (i >= g.nx + NB || j >= g.ny + NB) return;
-    const double a = (u[IX(g, i, j)] + u[IX(g, i + 1, j)]) * 0.5;
-    const double b = (v[IX(g, i, j)] + v[IX(g, i, j + 1)]) * 0.5;
-    tu[IX(g, i, j)] = a;
-    tv[IX(g, i, j)] = b;
-    if (g.p_mirror) {
-        p_mirror_store(g, tu, i, j, a);
-        p_mirror_store(g, tv, i, j, b);
-    }
-}
-
-// ------------------------------------------------------------------------
-// One TVD-RK3 stage.  L = HJWENO5_LS_2D(phi_in, tu, tv) at each interior
-// cell, then
-//   STAGE 1: out = phi_n - dt L                                      (:68)
-//   STAGE 2: out = 0.75 phi_n + 0.25 phi_in - 0.25 dt L              (:75)
-//   STAGE 3: out = 1/3 phi_n + 2/3 phi_in - 2/3 dt L                 (:82)
-//   STAGE 0: out = L (HJWENO5_LS_2D itself)
-// The fluxes F = phi*u (x) and phi*v (y) of a 8 x 32 cell tile plus its
-// three-cell halo along each axis are staged in shared memory; every cell
-// then differences its own 7-point windows, so each interior value is
-// computed exactly as the reference's per-row/per-column sweep computes it.
-// out may alias phi_n (stage 3 writes phi in place): each thread reads
-// phi_n only at its own cell before writing it.
-template <int STAGE>
-__global__ void __launch_bounds__(TJ *TI) k_ls_stage(Grid g, DivH ddx, DivH ddy, const double *__restrict__ phi_in,
-                                                       const double *__restrict__ tu, const double *__restrict__ tv,
-                                                       const double *phi_n, double *out,
-                                                       const double *__restrict__ dtp) {
-    __shared__ double sFx[TI + 2 * NB][TJ];      // rows i0-3 .. i0+TI+2, cols j0 .. j0+TJ-1
-    __shared__ double sFy[TI][TJ + 2 * NB + 1];  // rows i0 .. i0+TI-1, cols j0-3 .. j0+TJ+2
-    const int j0 = NB + blockIdx.x * TJ, i0 = NB + blockIdx.y * TI;
-    const int tid = threadIdx.y * TJ + threadIdx.x;
-    for (int t = tid; t < (TI + 2 * NB) * TJ; t += TJ * TI) {
-        const int r = t / TJ, c = t % TJ;
-        const int i = i0 - NB + r, j = j0 + c;
-        double f = 0.0;
-        if (i < g.sx && j < g.ny + NB) f = phi_in[IX(g, i, j)] * tu[IX(g, i, j)];
-        sFx[r][c] = f;
-    }
-    for (int t = tid; t < TI * (TJ + 2 * NB); t += TJ * TI) {
-        const int r = t / (TJ + 2 * NB), c = t % (TJ + 2 * NB);
-        const int i = i0 + r, j = j0 - NB + c;
-        double f = 0.0;
-        if (i < g.nx + NB && j < g.sy) f = phi_in[IX(g, i, j)] * tv[IX(g, i, j)];
-        sFy[r][c] = f;
-    }
-    __syncthreads();
-    const int ti = threadIdx.y, tj = threadIdx.x;
-    const int i = i0 + ti, j = j0 + tj;
-    if (i >= g.nx + NB || j >= g.ny + NB) return;
-    double D[6], xp, xm, yp, ym;
-#pragma unroll
-    for (int k = 0; k < 6; k++) D[k] = sFx[ti + k + 1][tj] - sFx[ti + k][tj];
-    weno5_point(D, ddx, xp, xm);
-#pragma unroll
-    for (int k = 0; k < 6; k++) D[k] = sFy[ti][tj + k + 1] - sFy[ti][tj + k];
-    weno5_point(D, ddy, yp, ym);
-    const int64_t c = IX(g, i, j);
-    const double L = weno_blend(xp, xm, yp, ym, tu[c], tv[c]);
-    const double dt = STAGE == 0 ? 0.0 : *dtp;
-    double val;
-    if (STAGE == 0) val = L;
-    else if (STAGE == 1) val = phi_n[c] - dt * L;
-    else if (STAGE == 2) val = 0.75 * phi_n[c] + 0.25 * phi_in[c] - 0.25 * dt * L;
-    else val = 1.0 / 3.0 * phi_n[c] + 2.0 / 3.0 * phi_in[c] - 2.0 / 3.0 * dt * L;
-    out[c] = val;
-    if (STAGE != 0 && g.p_mirror) p_mirror_store(g, out, i, j, val);
-}
-
-// ------------------------------------------------------------------------
-// Reinitialisation passes.  Every pass reads its stencil input from buffers
-// other than the one it writes, except for the cell-local reads of `base`,
-// so in-place use of `out == base` is safe.
-enum { RM_ORIG = 0, RM_SUSS = 1, RM_MINRK2 = 2, RM_FIRST = 3, RM_MINRK2_SUSS = 4 };
-
-__device__ __forceinline__ double reinit_sign(int mode, double l0, double eps) {
-    // MinRK2 uses the smoothed sign of phi0 (levelset2d.cpp:445,456); the
-    // other modes use sign(phi0) (:284).
-    return (mode == RM_MINRK2 || mode == RM_MINRK2_SUSS) ? smoothed_sign(l0, eps) : (double)isgn(l0);
-}
-
-// Pass A: out = src - adt * S * (|grad src| - 1)   (LS1 of every mode)
-template <int MODE>
-__global__ void k_reinit_a(Grid g, LsConst K, const double *__restrict__ src, const double *__restrict__ ls0,
-                           double *__restrict__ out, int mirror) {
-    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
-    if (i >= g.nx + NB || j >= g.ny + NB) return;
-    constexpr bool SUB = (MODE == RM_MINRK2 || MODE == RM_MINRK2_SUSS);
-    const int64_t c = IX(g, i, j);
-    const double a = absgrad<SUB>(g, K, src, ls0, i, j);
-    const double S = reinit_sign(MODE, ls0[c], K.eps);
-    double val;
-    if (SUB) val = src[c] - K.adt * S * (a - 1.0);
-    else val = src[c] - K.adt * (double)isgn(ls0[c]) * (a - 1.0);
-    out[c] = val;
-    if (mirror) p_mirror_store(g, out, i, j, val);
-}
-
-// Pass B: LS2 = step_base - adt * S * (|grad ls1| - 1); out = 0.5 * (base + LS2)
-// step_base is ls1 itself except for the first-time mode, which steps from
-// phi again (levelset2d.cpp:413-416).
-template <int MODE>
-__global__ void k_reinit_b(Grid g, LsConst K, const double *__restrict__ ls1, const double *__restrict__ ls0,
-                           const double *base, double *out, int mirror) {
-    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
-    if (i >= g.nx + NB || j >= g.ny + NB) return;
-    constexpr bool SUB = (MODE == RM_MINRK2 || MODE == RM_MINRK2_SUSS);
-    const int64_t c = IX(g, i, j);
-    const double a = absgrad<SUB>(g, K, ls1, ls0, i, j);
-    const double b = base[c];
-    double ls2;
-    if (SUB) ls2 = ls1[c] - K.adt * reinit_sign(MODE, ls0[c], K.eps) * (a - 1.0);
-    else if (MODE == RM_FIRST) ls2 = b - K.adt * (double)isgn(ls0[c]) * (a - 1.0);
-    else ls2 = ls1[c] - K.adt * (double)isgn(ls0[c]) * (a - 1.0);
-    const double val = 0.5 * (b + ls2);
-    out[c] = val;
-    if (mirror) p_mirror_store(g, out, i, j, val);
-}
-
-// Pass C (Sussman constraint, :787-893): out = base + constraint(tmp, ls0)
-// with hd = UpdateHeavisideFuncDeriv(tmp).  Sussman mode: base = phi
-// (levelset2d.cpp:368-372); MinRK2+Sussman: base = tmp.
-__global__ void k_reinit_c(Grid g, LsConst K, const double *__restrict__ tmp, const double *__restrict__ ls0,
-                           const double *base, double *out, int mirror) {
-    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
-    if (i >= g.nx + NB || j >= g.ny + NB) return;
-    const int64_t c = IX(g, i, j);
-    const double hd = heaviside_deriv(tmp[c], K.eps);
-    const double val = base[c] + sussman_constraint(g, K, tmp, ls0, hd, i, j);
-    out[c] = val;
-    if (mirror) p_mirror_store(g, out, i, j, val);
-}
 
 // First-time mode normalisation (levelset2d.cpp:388-395): phi0 / |grad phi0|
 // where positive, written to a separate buffer.
@@ -233,7 +89,7 @@ LsConst make_lsconst(const Grid &g) {
 }
 
 void launch_center_vel(const Grid &g, const double *u, const double *v, double *tu, double *tv, cudaStream_t st) {
-    k_center_vel<<<cell_grid(g), dim3(TJ, TI), 0, st>>>(g, u, v, tu, tv);
+    k_center_vel<double><<<cell_grid(g), dim3(TJ, TI), 0, st>>>(g, u, v, tu, tv);
     if (!g.p_mirror) {
         launch_fill_p(g, tu, st);
         launch_fill_p(g, tv, st);
@@ -245,10 +101,10 @@ void launch_ls_stage(int stage, const Grid &g, const double *phi_in, const doubl
     const DivH ddx = make_divh(g.dx), ddy = make_divh(g.dy);
     const dim3 grd = cell_grid(g), blk(TJ, TI);
     switch (stage) {
-    case 0: k_ls_stage<0><<<grd, blk, 0, st>>>(g, ddx, ddy, phi_in, tu, tv, phi_n, out, dt); break;
-    case 1: k_ls_stage<1><<<grd, blk, 0, st>>>(g, ddx, ddy, phi_in, tu, tv, phi_n, out, dt); break;
-    case 2: k_ls_stage<2><<<grd, blk, 0, st>>>(g, ddx, ddy, phi_in, tu, tv, phi_n, out, dt); break;
-    default: k_ls_stage<3><<<grd, blk, 0, st>>>(g, ddx, ddy, phi_in, tu, tv, phi_n, out, dt); break;
+    case 0: k_ls_stage<0, double><<<grd, blk, 0, st>>>(g, ddx, ddy, phi_in, tu, tv, phi_n, out, dt); break;
+    case 1: k_ls_stage<1, double><<<grd, blk, 0, st>>>(g, ddx, ddy, phi_in, tu, tv, phi_n, out, dt); break;
+    case 2: k_ls_stage<2, double><<<grd, blk, 0, st>>>(g, ddx, ddy, phi_in, tu, tv, phi_n, out, dt); break;
+    default: k_ls_stage<3, double><<<grd, blk, 0, st>>>(g, ddx, ddy, phi_in, tu, tv, phi_n, out, dt); break;
     }
     if (stage != 0 && !g.p_mirror) launch_fill_p(g, out, st);
 }
@@ -256,18 +112,18 @@ void launch_ls_stage(int stage, const Grid &g, const double *phi_in, const doubl
 template <int MODE>
 static void reinit_a(const Grid &g, const LsConst &K, const double *src, const double *ls0, double *out, bool bc,
                      cudaStream_t st) {
-    k_reinit_a<MODE><<<cell_grid(g), dim3(TJ, TI), 0, st>>>(g, K, src, ls0, out, bc && g.p_mirror);
+    k_reinit_a<MODE, double><<<cell_grid(g), dim3(TJ, TI), 0, st>>>(g, K, src, ls0, out, bc && g.p_mirror);
     if (bc && !g.p_mirror) launch_fill_p(g, out, st);
 }
 template <int MODE>
 static void reinit_b(const Grid &g, const LsConst &K, const double *ls1, const double *ls0, const double *base,
                      double *out, bool bc, cudaStream_t st) {
-    k_reinit_b<MODE><<<cell_grid(g), dim3(TJ, TI), 0, st>>>(g, K, ls1, ls0, base, out, bc && g.p_mirror);
+    k_reinit_b<MODE, double><<<cell_grid(g), dim3(TJ, TI), 0, st>>>(g, K, ls1, ls0, base, out, bc && g.p_mirror);
     if (bc && !g.p_mirror) launch_fill_p(g, out, st);
 }
 static void reinit_c(const Grid &g, const LsConst &K, const double *tmp, const double *ls0, const double *base,
                      double *out, cudaStream_t st) {
-    k_reinit_c<<<cell_grid(g), dim3(TJ, TI), 0, st>>>(g, K, tmp, ls0, base, out, g.p_mirror);
+    k_reinit_c<double><<<cell_grid(g), dim3(TJ, TI), 0, st>>>(g, K, tmp, ls0, base, out, g.p_mirror);
     if (!g.p_mirror) launch_fill_p(g, out, st);
 }
 

@@ -144,6 +144,99 @@ def prepare_state(n, seed, stream):
     return c, s, snap, dt
 
 
+LS_MIXED_GRID = 2048       # above L2 for the FP32 level-set working set (6 FP32 + 1 FP64 padded arrays)
+LS_MIXED_BYTES = 244       # 55 FP32 streams (220 B) + FP64 -> FP32 -> FP64 conversion of phi (24 B), per cell
+LS_FP64_BYTES = 440        # 55 FP64 streams per cell
+CFG3_GRID, CFG3_STEPS = 1024, 50
+
+
+def level_set_rates(sh, stream, flush, peak):
+    """Level-set step (WENO5/TVD-RK3 + 5 MinRK2 pseudo-steps with the Sussman
+    constraint) at LS_MIXED_GRID in FP32 (mixed session) and FP64: Mcells/s,
+    and algorithmic GB/s against the HBM peak.  L2 is flushed before each
+    timed step; each step is timed alone with CUDA events on the session's
+    stream."""
+    import torch
+    from asd2_b200 import api
+    from asd2_b200 import workloads as W
+    lc = W.perturbed_circle(LS_MIXED_GRID, seed=0)
+    out = {}
+    for prec, bytes_cell, name in ((api.PRECISION_MIXED, LS_MIXED_BYTES, "fp32"), (api.PRECISION_FP64,
+                                                                                 LS_FP64_BYTES, "fp64")):
+        p = api.Params(lc.nx, lc.ny, lc.dx, lc.dy, bc_u=lc.bc_u, bc_v=lc.bc_v, bc_p=lc.bc_p, precision=prec)
+        ss = api.Session(p, stream=sh)
+        ss.upload("ls", lc.ls)
+        ss.upload("u", lc.u)
+        ss.upload("v", lc.v)
+        for _ in range(3):
+            ss.ls_step(lc.dt, api.REINIT_MINRK2_SUSSMAN)
+        ts = []
+        for _ in range(10 if prec == api.PRECISION_MIXED else 4):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            ss.ls_step(lc.dt, api.REINIT_MINRK2_SUSSMAN)
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        ss.close()
+        t = float(np.median(ts))
+        cells = lc.nx * lc.ny
+        gbs = bytes_cell * cells / t / 1e9
+        out[name] = {"mcells_per_s": cells / t / 1e6, "ms_per_step": t * 1e3, "achieved_gbs": gbs,
+                     "frac_of_measured_hbm": gbs / peak, "bytes_per_cell": bytes_cell}
+    out["grid"] = [LS_MIXED_GRID, LS_MIXED_GRID]
+    out["l2"] = "flushed (256 MB write) before each timed step"
+    return out
+
+
+def mixed_precision_errors(sh):
+    """The 1024^2 two-phase droplet for 50 steps in FP64 (Jacobi-PCG) and in
+    mixed precision (FP32 level set, MG-FCG with an FP32 V-cycle): relative
+    max and L2 errors of phi and p against the FP64 run, volume check, and the
+    wall time of each run (device synchronised)."""
+    from asd2_b200 import api
+    from asd2_b200 import workloads as W
+    c = W.droplet(CFG3_GRID, seed=0)
+    res = {}
+    for prec, solver in ((api.PRECISION_FP64, api.PCG), (api.PRECISION_MIXED, api.MGPCG)):
+        ss = api.Session(api.Params.from_case(c, precision=prec), stream=sh)
+        ss.upload("ls", c.ls)
+        ss.upload("u", c.u)
+        ss.upload("v", c.v)
+        ss.apply_bc("ls", "P")
+        dt = ss.update_dt()
+        vol0 = ss.volume()
+        ss.sync()
+        t0 = time.perf_counter()
+        its = 0
+        for _ in range(CFG3_STEPS):
+            r = ss.droplet_step(dt, reinit_mode=api.REINIT_MINRK2, solver=solver, tol=1e-10, maxit=500000)
+            if r["status"] != 0:
+                raise SystemExit(f"bench: droplet step failed: {r}")
+            dt = r["dt_next"]
+            its += r["iters"]
+        ss.sync()
+        el = time.perf_counter() - t0
+        res[prec] = dict(ls=ss.download("ls")[3:-3, 3:-3], p=ss.download("p")[3:-3, 3:-3], t=el, its=its,
+                         vol0=vol0, vol=ss.last_volume())
+        ss.close()
+    a, b = res[api.PRECISION_MIXED], res[api.PRECISION_FP64]
+    err = {}
+    for k in ("ls", "p"):
+        d = a[k] - b[k]
+        err[k] = {"rel_max": float(np.abs(d).max() / np.abs(b[k]).max()),
+                  "rel_l2": float(np.sqrt((d ** 2).mean() / (b[k] ** 2).mean()))}
+    return {"workload": f"{CFG3_GRID}x{CFG3_GRID} droplet (rho ratio 1000, mu ratio 100), {CFG3_STEPS} full steps, "
+                        "pressure to rel. residual 1e-10",
+            "error_vs_fp64": err,
+            "volume_rel_change": {"fp64": (b["vol"][1] - b["vol0"][1]) / b["vol0"][1],
+                                  "mixed": (a["vol"][1] - a["vol0"][1]) / a["vol0"][1]},
+            "seconds": {"fp64": b["t"], "mixed": a["t"]},
+            "pressure_iterations": {"fp64_jacobi_pcg": b["its"], "mixed_mg_fcg": a["its"]}}
+
+
 def run_ours(args):
     import torch
     from asd2_b200 import api
@@ -286,6 +379,8 @@ def run_ours(args):
     except Exception:
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
+    ls_rates = level_set_rates(sh, stream, flush, peak) if not args.no_extra else None
+    mixed = mixed_precision_errors(sh) if not args.no_extra else None
     nlev = len(_mg_levels(args.n, args.n))
     per_iter = 2 + 2 * (nlev - 1) + 1
     launches = int(sum(4 + (1 + nlev) + (1 + per_iter - 2) + 8 * per_iter * math.ceil(i / 8) + 3 for i in iters))
@@ -325,6 +420,8 @@ def run_ours(args):
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback",
                      "note": "working set is L2-resident at 256^2; iteration time from CUDA events "
                              "(solve minus assembly) / iterations"},
+        "ls_large": ls_rates,
+        "mixed_precision_1024": mixed,
         "e2e": {"value": e2e_value, "unit": "GFM Poisson solves/s",
                 "h2d_bytes_per_step": 3 * G * 8, "d2h_bytes_per_step": G * 8},
         "gpu_launches": launches,
@@ -435,6 +532,7 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the 2048^2 level-set and 1024^2 mixed-precision reports")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -85,10 +85,18 @@ enum asd2g_solver {
 /* solver_flags bits */
 #define ASD2G_FLAG_NO_CLUSTER_PCG 1 /* Jacobi-PCG always as per-iteration kernels (no cluster solver) */
 
+/* precision (no reference counterpart: the reference is FP64 throughout) */
+#define ASD2G_PRECISION_FP64 0  /* every field and kernel in FP64 (the drop-in) */
+#define ASD2G_PRECISION_MIXED 1 /* level-set advection + reinitialisation in FP32 (FP64 fields stay
+                                   the interface); momentum, GFM assembly and projection in FP64;
+                                   pressure with ASD2G_SOLVER_MGPCG is FP32 inside, FP64 outside.
+                                   Needs Neumann/Dirichlet pressure on all sides and reinit mode
+                                   0, 2 or 4. */
+
 typedef struct asd2g_params {
     int32_t nx, ny;          /* interior cells (>= 4 each) */
     int32_t nbc;             /* ghost layers: must be 3 (WENO5) */
-    int32_t precision;       /* 0: FP64 throughout (the drop-in) */
+    int32_t precision;       /* ASD2G_PRECISION_FP64 (the drop-in) or ASD2G_PRECISION_MIXED */
     double base_x, base_y;   /* lower-left corner (only for bookkeeping) */
     double dx, dy;           /* cell sizes */
     int32_t bc_u[4], bc_v[4], bc_p[4];      /* asd2g_bc per side, order W, E, S, N */
@@ -163,8 +171,16 @@ int asd2g_eno(asd2g_session *s, int ls, int ls0, int out);
 int asd2g_sussman_constraint(asd2g_session *s, int ls, int ls0, int hd, int out);
 int asd2g_heaviside_deriv(asd2g_session *s, int ls, int out);
 int asd2g_smoothed_sign(asd2g_session *s, int ls, int out);
-/* Level-set step: advect (dt) then reinitialise (mode). */
+/* Level-set step: advect (dt) then reinitialise (mode).  In a mixed-precision
+ * session both run in FP32 on an FP32 copy of LS (LS is read and written in
+ * FP64, ghosts included). */
 int asd2g_ls_step(asd2g_session *s, double dt, int reinit_mode);
+/* FP64 volume check (no reference counterpart; the reference's tests print
+ * the area of phi >= 0, test_levelset2d_large.cpp:106-130): recomputes H and
+ * HS from LS and returns sum(H) dx dy and sum(HS) dx dy over the interior. */
+int asd2g_volume(asd2g_session *s, double *sharp, double *smooth);
+/* The same two integrals for the level set of the last asd2g_droplet_step. */
+int asd2g_last_volume(asd2g_session *s, double *sharp, double *smooth);
 /* UnitHJWENO5(F, FP, FM, d, n), levelset2d.cpp:159 / mac2d.cpp:465: WENO5
  * one-sided derivatives of the line F[0 .. n+5] (host arrays), written to
  * FP[3 .. n+2] and FM[3 .. n+2].  n + 6 must not exceed (nx+6)*(ny+6). */

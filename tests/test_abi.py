@@ -56,3 +56,17 @@ def test_missing_library_fails_loudly(tmp_path):
 def test_params_struct_matches_header():
     # asd2g_params: 4 int32, 4 double, 12 int32, 12 double, 6 double, 4 int32, 2 double, 2 int32, 3 double
     assert ctypes.sizeof(api._Params) == 4 * 4 + 4 * 8 + 12 * 4 + 12 * 8 + 6 * 8 + 4 * 4 + 2 * 8 + 2 * 4 + 3 * 8
+
+
+def test_mixed_precision_needs_producer_side_pressure_fill():
+    """The FP32 level-set kernels write their own ghost mirrors, so a mixed
+    session with periodic pressure sides is refused when it is created
+    (before any device work)."""
+    p = api.Params(32, 32, 1 / 32, 1 / 32, bc_p=("periodic",) * 4, precision=api.PRECISION_MIXED)
+    with pytest.raises(api.Asd2gError) as e:
+        api.Session(p)
+    assert e.value.code == -4
+    p = api.Params(32, 32, 1 / 32, 1 / 32, precision=7)
+    with pytest.raises(api.Asd2gError) as e:
+        api.Session(p)
+    assert e.value.code == -1
