@@ -4,7 +4,8 @@
 csrc/ with nvcc for sm_100a into asd2_b200/libasd2g.so (in-tree, so the built
 library travels with the source tree).  The FP64 parity kernels are compiled
 with -fmad=false: no multiply is fused into an add, which keeps their results
-bit-identical to the reference's x86-64 build.
+bit-identical to the reference's x86-64 build.  The FP32 level-set unit
+(levelset32.cu, the mixed-precision path) is built with fused multiply-adds.
 """
 from __future__ import annotations
 

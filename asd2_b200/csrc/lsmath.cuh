@@ -31,6 +31,27 @@ template <typename T> __device__ __forceinline__ T minmod(T a, T b) {
     return quiet_nan<T>();
 }
 
+// Jiang-Peng weights (0.1, 0.6, 0.3) / (eps + IS)^2, normalised.  FP64: the
+// reference's divisions as written.  FP32 (not bit-exact by design): the
+// fast single-precision divide for the three alphas and one reciprocal of
+// their sum -- the weights are a smoothness heuristic, and these divisions
+// were a third of the FP32 stencil's instructions.
+template <typename T> __device__ __forceinline__ void weno_weights(T is0, T is1, T is2, T eps, T &w0, T &w1, T &w2) {
+    if constexpr (sizeof(T) == sizeof(float)) {
+        const float a0 = __fdividef(0.1f, sq(eps + is0)), a1 = __fdividef(0.6f, sq(eps + is1)),
+                    a2 = __fdividef(0.3f, sq(eps + is2));
+        const float r = __fdividef(1.0f, a0 + a1 + a2);
+        w0 = a0 * r;
+        w1 = a1 * r;
+        w2 = a2 * r;
+    } else {
+        const T a0 = T(0.1) / sq(eps + is0), a1 = T(0.6) / sq(eps + is1), a2 = T(0.3) / sq(eps + is2);
+        w0 = a0 / (a0 + a1 + a2);
+        w1 = a1 / (a0 + a1 + a2);
+        w2 = a2 / (a0 + a1 + a2);
+    }
+}
+
 // UnitHJWENO5 at one point (levelset2d.cpp:159-262).  D[k] = DFPlus[i-3+k],
 // k = 0..5.  dv divides by the spacing d.
 template <typename T>
@@ -42,8 +63,8 @@ __device__ __forceinline__ void weno5_point(const T D[6], const DivHT<T> &dv, T 
         const T is0 = T(13.0 / 12.0) * sq(dv(d3 - T(2.0) * d2 + d1)) + T(1.0 / 4.0) * sq(dv(d3 - T(4.0) * d2 + T(3.0) * d1));
         const T is1 = T(13.0 / 12.0) * sq(dv(d2 - T(2.0) * d1 + d0)) + T(1.0 / 4.0) * sq(dv(d2 - d0));
         const T is2 = T(13.0 / 12.0) * sq(dv(d1 - T(2.0) * d0 + p1)) + T(1.0 / 4.0) * sq(dv(T(3.0) * d1 - T(4.0) * d0 + p1));
-        const T a0 = T(0.1) / sq(eps + is0), a1 = T(0.6) / sq(eps + is1), a2 = T(0.3) / sq(eps + is2);
-        const T w0 = a0 / (a0 + a1 + a2), w1 = a1 / (a0 + a1 + a2), w2 = a2 / (a0 + a1 + a2);
+        T w0, w1, w2;
+        weno_weights(is0, is1, is2, eps, w0, w1, w2);
         FM = dv(w0 * (T(1.0 / 3.0) * d3 - T(7.0 / 6.0) * d2 + T(11.0 / 6.0) * d1)) +
              dv(w1 * (T(-1.0 / 6.0) * d2 + T(5.0 / 6.0) * d1 + T(1.0 / 3.0) * d0)) +
              dv(w2 * (T(1.0 / 3.0) * d1 + T(5.0 / 6.0) * d0 - T(1.0 / 6.0) * p1));
@@ -54,8 +75,8 @@ __device__ __forceinline__ void weno5_point(const T D[6], const DivHT<T> &dv, T 
         const T is0 = T(13.0 / 12.0) * sq(dv(p2 - T(2.0) * p1 + d0)) + T(1.0 / 4.0) * sq(dv(p2 - T(4.0) * p1 + T(3.0) * d0));
         const T is1 = T(13.0 / 12.0) * sq(dv(p1 - T(2.0) * d0 + m1)) + T(1.0 / 4.0) * sq(dv(p1 - m1));
         const T is2 = T(13.0 / 12.0) * sq(dv(d0 - T(2.0) * m1 + m2)) + T(1.0 / 4.0) * sq(dv(T(3.0) * d0 - T(4.0) * m1 + m2));
-        const T a0 = T(0.1) / sq(eps + is0), a1 = T(0.6) / sq(eps + is1), a2 = T(0.3) / sq(eps + is2);
-        const T w0 = a0 / (a0 + a1 + a2), w1 = a1 / (a0 + a1 + a2), w2 = a2 / (a0 + a1 + a2);
+        T w0, w1, w2;
+        weno_weights(is0, is1, is2, eps, w0, w1, w2);
         FP = dv(w0 * (T(1.0 / 3.0) * p2 - T(7.0 / 6.0) * p1 + T(11.0 / 6.0) * d0)) +
              dv(w1 * (T(-1.0 / 6.0) * p1 + T(5.0 / 6.0) * d0 + T(1.0 / 3.0) * m1)) +
              dv(w2 * (T(1.0 / 3.0) * d0 + T(5.0 / 6.0) * m1 - T(1.0 / 6.0) * m2));

@@ -533,11 +533,33 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the 2048^2 level-set and 1024^2 mixed-precision reports")
+    ap.add_argument("--section", default=None, choices=["ls_large", "mixed_1024"],
+                    help="run only this report (its JSON object on stdout), e.g. to profile it")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.section:
+        run_section(args.section)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
+
+
+def run_section(name):
+    import torch
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    if name == "ls_large":
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        peak = 6650.0
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                peak = json.load(f).get("hbm_gbs", peak)
+        except Exception:
+            pass
+        out = level_set_rates(stream.cuda_stream, stream, flush, peak)
+    else:
+        out = mixed_precision_errors(stream.cuda_stream)
+    print(json.dumps({"section": name, **out}), flush=True)
 
 
 if __name__ == "__main__":
