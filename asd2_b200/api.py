@@ -64,6 +64,8 @@ EXPORTS = [
     "asd2g_assemble_gfm", "asd2g_get_system", "asd2g_solve_pressure", "asd2g_true_residual",
     "asd2g_droplet_step", "asd2g_pcg_solve_static", "asd2g_weno5_line", "asd2g_weno_absgrad",
     "asd2g_apply_bc_side", "asd2g_update_ntk", "asd2g_csr_solve", "asd2g_volume", "asd2g_last_volume",
+    "asd2g_batch_create", "asd2g_batch_destroy", "asd2g_batch_upload", "asd2g_batch_download",
+    "asd2g_batch_field_ptr", "asd2g_batch_offset", "asd2g_batch_assemble", "asd2g_batch_solve", "asd2g_batch_sync",
 ]
 
 _lib = None
@@ -109,6 +111,13 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_csr_solve": ([S, I, I, ip, ip, dp, dp, dp, dp, D, I, C.POINTER(I), C.POINTER(D)], I),
         "asd2g_volume": ([S, C.POINTER(D), C.POINTER(D)], I),
         "asd2g_last_volume": ([S, C.POINTER(D), C.POINTER(D)], I),
+        "asd2g_batch_create": ([C.POINTER(_Params), I, C.c_void_p, C.POINTER(S)], I),
+        "asd2g_batch_destroy": ([S], I), "asd2g_batch_sync": ([S], I),
+        "asd2g_batch_upload": ([S, I, I, dp], I), "asd2g_batch_download": ([S, I, I, dp], I),
+        "asd2g_batch_field_ptr": ([S, I, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)], I),
+        "asd2g_batch_offset": ([S, I, C.POINTER(C.c_size_t)], I),
+        "asd2g_batch_assemble": ([S, dp], I),
+        "asd2g_batch_solve": ([S, D, I, ip, dp], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -355,3 +364,64 @@ class Session:
         a, b = C.c_double(), C.c_double()
         self._check(self.L.asd2g_last_volume(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+
+class Batch:
+    """Many GFM pressure systems of uneven sizes solved together
+    (asd2g_batch_*): one kernel launch per phase for the whole batch."""
+
+    def __init__(self, params: list, stream: int | None = None):
+        self.L = load()
+        self.params = list(params)
+        arr = (_Params * len(self.params))(*[p.c() for p in self.params])
+        h = C.c_void_p()
+        self._check(self.L.asd2g_batch_create(arr, len(self.params), C.c_void_p(stream) if stream else None,
+                                              C.byref(h)))
+        self.h = h
+
+    def _check(self, rc):
+        if rc < 0:
+            raise Asd2gError(rc, self.L.asd2g_last_error().decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.asd2g_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload(self, inst, field, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        p = self.params[inst]
+        assert a.size == (p.nx + 6) * (p.ny + 6)
+        self._check(self.L.asd2g_batch_upload(self.h, inst, Session._f(field), a.ravel()))
+
+    def download(self, inst, field):
+        p = self.params[inst]
+        out = np.zeros((p.nx + 6, p.ny + 6))
+        self._check(self.L.asd2g_batch_download(self.h, inst, Session._f(field), out.ravel()))
+        return out
+
+    def assemble(self, dts):
+        self._check(self.L.asd2g_batch_assemble(self.h, np.ascontiguousarray(dts, dtype=np.float64)))
+
+    def solve(self, tol=1e-8, maxit=10000):
+        n = len(self.params)
+        it, res = np.zeros(n, np.int32), np.zeros(n)
+        rc = self._check(self.L.asd2g_batch_solve(self.h, tol, maxit, it, res))
+        return dict(status=rc, iters=it, resid=res)
+
+    def sync(self):
+        self._check(self.L.asd2g_batch_sync(self.h))
+

@@ -33,6 +33,7 @@ UNITS = {
     "pcg_cluster.cu": ["-fmad=false"],
     "mg.cu": [],
     "levelset32.cu": [],
+    "batch.cu": [],
 }
 
 

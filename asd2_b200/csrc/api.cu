@@ -99,6 +99,49 @@ int kind_p(int bc) {
     default: return K_NONE;
     }
 }
+
+// Validates p and derives the device-side grid and momentum constants of one
+// session (or one batch instance).
+int grid_from_params(const asd2g_params *p, Grid &g, MomConst &M) {
+    if (p->nbc != NB) return fail(ASD2G_E_ARG, "num_bc_grid must be 3 (WENO5 needs three ghost layers), got %d", p->nbc);
+    if (p->nx < 4 || p->ny < 4) return fail(ASD2G_E_ARG, "grid must be at least 4 x 4 cells, got %d x %d", p->nx, p->ny);
+    if ((int64_t)(p->nx + 6) * (p->ny + 6) > (int64_t)1 << 31)
+        return fail(ASD2G_E_ARG, "grid %d x %d too large", p->nx, p->ny);
+    if (p->precision != ASD2G_PRECISION_FP64 && p->precision != ASD2G_PRECISION_MIXED)
+        return fail(ASD2G_E_ARG, "precision %d: expected ASD2G_PRECISION_FP64 or _MIXED", p->precision);
+    if (!(p->dx > 0.0) || !(p->dy > 0.0)) return fail(ASD2G_E_ARG, "dx, dy must be positive");
+    for (int k = 0; k < 4; k++)
+        if (p->bc_u[k] < 0 || p->bc_u[k] > 9 || p->bc_v[k] < 0 || p->bc_v[k] > 9 || p->bc_p[k] < 0 || p->bc_p[k] > 9)
+            return fail(ASD2G_E_ARG, "boundary kind out of range");
+    if (p->time_order < 0 || p->time_order > 2) return fail(ASD2G_E_ARG, "time_order must be 0, 1 or 2");
+    g = Grid{};
+    g.nx = p->nx;
+    g.ny = p->ny;
+    g.sx = p->nx + 2 * NB;
+    g.sy = p->ny + 2 * NB;
+    g.dx = p->dx;
+    g.dy = p->dy;
+    bool mirror = true, pinned = true;
+    for (int k = 0; k < 4; k++) {
+        g.ku[k] = kind_u(k, p->bc_u[k]);
+        g.kv[k] = kind_v(k, p->bc_v[k]);
+        g.kp[k] = kind_p(p->bc_p[k]);
+        g.bp[k] = p->bc_p[k];
+        g.cu[k] = p->bcc_u[k];
+        g.cv[k] = p->bcc_v[k];
+        g.cp[k] = p->bcc_p[k];
+        mirror &= (g.kp[k] == K_NEU || g.kp[k] == K_DIR);
+        pinned &= (p->bc_p[k] == ASD2G_BC_NEUMANN || p->bc_p[k] == ASD2G_BC_AXISYM || p->bc_p[k] == ASD2G_BC_WALL);
+    }
+    g.p_mirror = mirror ? 1 : 0;
+    g.pinned = pinned ? 1 : 0;
+    if (p->precision == ASD2G_PRECISION_MIXED && !g.p_mirror)
+        return fail(ASD2G_E_UNSUPPORTED, "mixed precision needs Neumann or Dirichlet pressure on all four sides");
+    MomParams mp{p->rho_h, p->rho_l, p->mu_h, p->mu_l, p->sigma, p->gravity, p->cfl, p->g_axis, p->fix_gravity,
+                 p->numbers_given, p->re, p->we, p->fr};
+    M = make_momconst(g, mp);
+    return ASD2G_OK;
+}
 }  // namespace
 
 void asd2g::asd2g_set_error_text(const char *msg) { snprintf(g_err, sizeof(g_err), "%s", msg ? msg : ""); }
@@ -230,48 +273,16 @@ const char *asd2g_last_error(void) { return g_err; }
 int asd2g_create(const asd2g_params *p, void *stream, asd2g_session **out) {
     if (!p || !out) return fail(ASD2G_E_ARG, "null argument");
     *out = nullptr;
-    if (p->nbc != NB) return fail(ASD2G_E_ARG, "num_bc_grid must be 3 (WENO5 needs three ghost layers), got %d", p->nbc);
-    if (p->nx < 4 || p->ny < 4) return fail(ASD2G_E_ARG, "grid must be at least 4 x 4 cells, got %d x %d", p->nx, p->ny);
-    if ((int64_t)(p->nx + 6) * (p->ny + 6) > (int64_t)1 << 31)
-        return fail(ASD2G_E_ARG, "grid %d x %d too large", p->nx, p->ny);
-    if (p->precision != ASD2G_PRECISION_FP64 && p->precision != ASD2G_PRECISION_MIXED)
-        return fail(ASD2G_E_ARG, "precision %d: expected ASD2G_PRECISION_FP64 or _MIXED", p->precision);
-    if (!(p->dx > 0.0) || !(p->dy > 0.0)) return fail(ASD2G_E_ARG, "dx, dy must be positive");
-    for (int k = 0; k < 4; k++)
-        if (p->bc_u[k] < 0 || p->bc_u[k] > 9 || p->bc_v[k] < 0 || p->bc_v[k] > 9 || p->bc_p[k] < 0 || p->bc_p[k] > 9)
-            return fail(ASD2G_E_ARG, "boundary kind out of range");
-    if (p->time_order < 0 || p->time_order > 2) return fail(ASD2G_E_ARG, "time_order must be 0, 1 or 2");
+    Grid g0{};
+    MomConst M0{};
+    int rc0 = grid_from_params(p, g0, M0);
+    if (rc0) return rc0;
     asd2g_session *s = new (std::nothrow) asd2g_session();
     if (!s) return fail(ASD2G_E_NOMEM, "host allocation failed");
     s->prm = *p;
+    s->g = g0;
+    s->M = M0;
     Grid &g = s->g;
-    g.nx = p->nx;
-    g.ny = p->ny;
-    g.sx = p->nx + 2 * NB;
-    g.sy = p->ny + 2 * NB;
-    g.dx = p->dx;
-    g.dy = p->dy;
-    bool mirror = true, pinned = true;
-    for (int k = 0; k < 4; k++) {
-        g.ku[k] = kind_u(k, p->bc_u[k]);
-        g.kv[k] = kind_v(k, p->bc_v[k]);
-        g.kp[k] = kind_p(p->bc_p[k]);
-        g.bp[k] = p->bc_p[k];
-        g.cu[k] = p->bcc_u[k];
-        g.cv[k] = p->bcc_v[k];
-        g.cp[k] = p->bcc_p[k];
-        mirror &= (g.kp[k] == K_NEU || g.kp[k] == K_DIR);
-        pinned &= (p->bc_p[k] == ASD2G_BC_NEUMANN || p->bc_p[k] == ASD2G_BC_AXISYM || p->bc_p[k] == ASD2G_BC_WALL);
-    }
-    g.p_mirror = mirror ? 1 : 0;
-    g.pinned = pinned ? 1 : 0;
-    if (p->precision == ASD2G_PRECISION_MIXED && !g.p_mirror) {
-        delete s;
-        return fail(ASD2G_E_UNSUPPORTED, "mixed precision needs Neumann or Dirichlet pressure on all four sides");
-    }
-    MomParams mp{p->rho_h, p->rho_l, p->mu_h, p->mu_l, p->sigma, p->gravity, p->cfl, p->g_axis, p->fix_gravity,
-                 p->numbers_given, p->re, p->we, p->fr};
-    s->M = make_momconst(g, mp);
     s->G = (size_t)g.sx * g.sy;
     s->N = (size_t)g.nx * g.ny;
     if (stream) s->st = (cudaStream_t)stream;
@@ -935,3 +946,9 @@ int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver
 }
 
 }  // extern "C"
+
+// Entry points of the ABI layer's helpers for the other host unit (batch.cu).
+namespace asd2g {
+int api_fail(int code, const char *msg) { return fail(code, "%s", msg); }
+int api_grid_from_params(const asd2g_params *p, Grid &g, MomConst &M) { return grid_from_params(p, g, M); }
+}  // namespace asd2g

@@ -1,0 +1,365 @@
+// Batched GFM pressure solves (no reference counterpart: the reference solves
+// one droplet per process).  A batch holds many droplet instances of uneven
+// grid sizes; each phase -- assembly, multigrid set-up, every flexible-CG
+// kernel, every V-cycle pass, the scatter -- is ONE kernel launch for the
+// whole batch over device work lists of (instance, tile) or (instance, chunk)
+// entries.  Each instance keeps its own solver scalars and stops on its own;
+// chunks of iterations are captured once in a CUDA graph and replayed until
+// every instance has converged.
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "asd2g.h"
+#include "batch.cuh"
+
+namespace asd2g {
+int api_fail(int code, const char *msg);
+int api_grid_from_params(const asd2g_params *p, Grid &g, MomConst &M);
+}  // namespace asd2g
+
+using namespace asd2g;
+
+struct asd2g_batch {
+    int count = 0;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    std::vector<asd2g_params> prm;
+    std::vector<BInst> hinst;
+    BInst *dinst = nullptr;
+    std::vector<size_t> goff;  // padded-field offset of each instance
+    size_t gtot = 0;
+    double *pad = nullptr;     // 6 padded fields x gtot: LS, KAPPA, H, DIV, PS, P
+    BTile *cell_tiles = nullptr;
+    int ncell_tiles = 0;
+    BatchPlan plan{};
+    KState *ks = nullptr;
+    KState *ks_host = nullptr;
+    cudaGraphExec_t chunk_exec = nullptr;
+    std::vector<void *> allocs;
+};
+
+namespace {
+
+constexpr int FCG_CHUNK_ITERS = 8;
+constexpr int PAD_FIELDS = 6;
+
+int pad_slot(int field) {
+    switch (field) {
+    case ASD2G_LS: return 0;
+    case ASD2G_KAPPA: return 1;
+    case ASD2G_H: return 2;
+    case ASD2G_DIV: return 3;
+    case ASD2G_PS: return 4;
+    case ASD2G_P: return 5;
+    default: return -1;
+    }
+}
+
+template <typename T> int balloc(asd2g_batch *b, T **p, size_t n) {
+    if (cudaMalloc(p, sizeof(T) * (n ? n : 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return api_fail(ASD2G_E_NOMEM, "batch device allocation failed");
+    }
+    b->allocs.push_back(*p);
+    return ASD2G_OK;
+}
+
+template <typename T> int upload_list(asd2g_batch *b, const std::vector<T> &v, const T **out) {
+    T *d = nullptr;
+    int rc = balloc(b, &d, v.size());
+    if (rc) return rc;
+    if (!v.empty()) cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, b->st);
+    *out = d;
+    return ASD2G_OK;
+}
+
+int check(const char *what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return ASD2G_OK;
+    char msg[256];
+    snprintf(msg, sizeof(msg), "%s: %s", what, cudaGetErrorString(e));
+    return api_fail(ASD2G_E_CUDA, msg);
+}
+
+void release(asd2g_batch *b) {
+    if (b->chunk_exec) cudaGraphExecDestroy(b->chunk_exec);
+    for (void *p : b->allocs) cudaFree(p);
+    if (b->ks_host) cudaFreeHost(b->ks_host);
+    if (b->own_stream && b->st) cudaStreamDestroy(b->st);
+    delete b;
+}
+
+int build(asd2g_batch *b) {
+    const int count = b->count;
+    b->hinst.assign(count, BInst{});
+    b->goff.assign(count, 0);
+    std::vector<size_t> noff(count), poff(count);
+    size_t ntot = 0, ptot = 0;
+    std::vector<int> dims(2 * MG_MAX_LEVELS * (size_t)count);
+    std::vector<size_t> mg_cells(MG_MAX_LEVELS, 0);
+    for (int i = 0; i < count; i++) {
+        BInst &I = b->hinst[i];
+        int rc = api_grid_from_params(&b->prm[i], I.g, I.M);
+        if (rc) return rc;
+        if (!I.g.p_mirror)
+            return api_fail(ASD2G_E_UNSUPPORTED, "batch instances need Neumann or Dirichlet pressure on all sides");
+        I.dxx = make_divh(I.g.dx * I.g.dx);
+        I.dyy = make_divh(I.g.dy * I.g.dy);
+        I.n = (int64_t)I.g.nx * I.g.ny;
+        I.chunks = (int)((I.n + FCG_CHUNK - 1) / FCG_CHUNK);
+        I.tiles0 = batch_tiles0(I.g.nx, I.g.ny);
+        I.nlev = mg_levels_for(I.g.nx, I.g.ny, &dims[2 * MG_MAX_LEVELS * (size_t)i], MG_MAX_LEVELS);
+        if (I.nlev < 2) return api_fail(ASD2G_E_UNSUPPORTED, "instance too small for the multigrid preconditioner");
+        b->goff[i] = b->gtot;
+        b->gtot += (size_t)I.g.sx * I.g.sy;
+        noff[i] = ntot;
+        ntot += (size_t)I.n;
+        poff[i] = ptot;
+        ptot += (size_t)batch_partial_len(I.g.nx, I.g.ny);
+        for (int l = 0; l < I.nlev; l++)
+            mg_cells[l] += (size_t)dims[2 * MG_MAX_LEVELS * (size_t)i + 2 * l] * dims[2 * MG_MAX_LEVELS * (size_t)i + 2 * l + 1];
+    }
+    // arenas
+    int rc = balloc(b, &b->pad, PAD_FIELDS * b->gtot);
+    double *vec = nullptr, *partial = nullptr, *inv = nullptr;
+    constexpr int NVEC = 13;  // diag cw ce cs cn minv b | x r pa pb q z
+    if (!rc) rc = balloc(b, &vec, NVEC * ntot);
+    if (!rc) rc = balloc(b, &partial, ptot);
+    if (!rc) rc = balloc(b, &inv, (size_t)count * MG_COARSE_CELLS * MG_COARSE_CELLS);
+    if (!rc) rc = balloc(b, &b->ks, (size_t)count);
+    std::vector<float *> mg_base(MG_MAX_LEVELS, nullptr);
+    for (int l = 0; l < MG_MAX_LEVELS && !rc; l++)
+        if (mg_cells[l]) rc = balloc(b, &mg_base[l], 6 * mg_cells[l]);
+    if (rc) return rc;
+    if (cudaMallocHost(&b->ks_host, sizeof(KState) * count) != cudaSuccess)
+        return api_fail(ASD2G_E_NOMEM, "pinned allocation failed");
+    cudaMemsetAsync(b->pad, 0, sizeof(double) * PAD_FIELDS * b->gtot, b->st);
+    cudaMemsetAsync(vec, 0, sizeof(double) * NVEC * ntot, b->st);
+    std::vector<size_t> mg_used(MG_MAX_LEVELS, 0);
+    for (int i = 0; i < count; i++) {
+        BInst &I = b->hinst[i];
+        const size_t go = b->goff[i], G = b->gtot;
+        I.ls = b->pad + 0 * G + go;
+        I.kappa = b->pad + 1 * G + go;
+        I.H = b->pad + 2 * G + go;
+        I.div = b->pad + 3 * G + go;
+        I.ps = b->pad + 4 * G + go;
+        I.p = b->pad + 5 * G + go;
+        double *v = vec + noff[i];
+        double **slots[NVEC] = {&I.S.diag, &I.S.cw, &I.S.ce, &I.S.cs, &I.S.cn, &I.S.minv, &I.S.b,
+                                &I.x, &I.r, &I.pa, &I.pb, &I.q, &I.z};
+        for (int k = 0; k < NVEC; k++) *slots[k] = v + (size_t)k * ntot;
+        I.S.pinned = I.g.pinned;
+        I.ks = b->ks + i;
+        I.partial = partial + poff[i];
+        I.coarse_inv = inv + (size_t)i * MG_COARSE_CELLS * MG_COARSE_CELLS;
+        I.dt = 1.0;
+        const int *d = &dims[2 * MG_MAX_LEVELS * (size_t)i];
+        for (int l = 0; l < I.nlev; l++) {
+            MgLevel &L = I.lv[l];
+            L.nx = d[2 * l];
+            L.ny = d[2 * l + 1];
+            const size_t m = (size_t)L.nx * L.ny, tot = mg_cells[l];
+            float *base = mg_base[l] + mg_used[l];
+            L.diag = base;
+            L.ce = base + tot;
+            L.cn = base + 2 * tot;
+            L.f = base + 3 * tot;
+            L.e = base + 4 * tot;
+            L.ep = base + 5 * tot;
+            mg_used[l] += m;
+        }
+        I.s_cta = mg_cta_first_level(I.lv, I.nlev);
+    }
+    for (int l = 0; l < MG_MAX_LEVELS; l++)
+        if (mg_cells[l]) cudaMemsetAsync(mg_base[l], 0, sizeof(float) * 6 * mg_cells[l], b->st);
+    // work lists
+    std::vector<BTile> cells;
+    std::vector<BChunk> chunks;
+    std::vector<std::vector<BChunk>> lvl(MG_MAX_LEVELS);
+    std::vector<std::vector<BTile>> mgt(MG_MAX_LEVELS);
+    int max_s = 0, max_nlev = 0;
+    for (int i = 0; i < count; i++) {
+        const BInst &I = b->hinst[i];
+        const int gx = (I.g.ny + TJ - 1) / TJ, gy = (I.g.nx + TI - 1) / TI;
+        for (int by = 0; by < gy; by++)
+            for (int bx = 0; bx < gx; bx++) cells.push_back({i, bx, by});
+        for (int c = 0; c < I.chunks; c++) chunks.push_back({i, c});
+        for (int l = 1; l < I.nlev; l++) {
+            const int64_t m = (int64_t)I.lv[l].nx * I.lv[l].ny;
+            for (int c = 0; c < (int)((m + FCG_CHUNK - 1) / FCG_CHUNK); c++) lvl[l].push_back({i, c});
+        }
+        for (int l = 0; l < I.s_cta; l++) {
+            const int tx = (I.lv[l].ny + 31) / 32, ty = (I.lv[l].nx + 15) / 16;
+            for (int by = 0; by < ty; by++)
+                for (int bx = 0; bx < tx; bx++) mgt[l].push_back({i, bx, by});
+        }
+        max_s = I.s_cta > max_s ? I.s_cta : max_s;
+        max_nlev = I.nlev > max_nlev ? I.nlev : max_nlev;
+    }
+    BatchPlan &P = b->plan;
+    rc = balloc(b, &b->dinst, (size_t)count);
+    if (rc) return rc;
+    cudaMemcpyAsync(b->dinst, b->hinst.data(), sizeof(BInst) * count, cudaMemcpyHostToDevice, b->st);
+    P.insts = b->dinst;
+    P.count = count;
+    const BTile *ct = nullptr;
+    rc = upload_list(b, cells, &ct);
+    b->cell_tiles = const_cast<BTile *>(ct);
+    b->ncell_tiles = (int)cells.size();
+    if (!rc) rc = upload_list(b, chunks, &P.chunks);
+    P.nchunks = (int)chunks.size();
+    for (int l = 0; l < MG_MAX_LEVELS && !rc; l++) {
+        P.nlvl_chunks[l] = (int)lvl[l].size();
+        P.nmg_tiles[l] = (int)mgt[l].size();
+        if (!lvl[l].empty()) rc = upload_list(b, lvl[l], &P.lvl_chunks[l]);
+        if (!rc && !mgt[l].empty()) rc = upload_list(b, mgt[l], &P.mg_tiles[l]);
+    }
+    P.max_s = max_s;
+    P.max_nlev = max_nlev;
+    if (rc) return rc;
+    if (!batch_cta_prepare()) return api_fail(ASD2G_E_CUDA, "coarse-cycle shared memory attribute");
+    return check("batch set-up");
+}
+
+}  // namespace
+
+extern "C" {
+
+int asd2g_batch_create(const asd2g_params *params, int count, void *stream, asd2g_batch **out) {
+    if (!params || !out || count < 1) return api_fail(ASD2G_E_ARG, "batch_create: bad arguments");
+    *out = nullptr;
+    for (int i = 0; i < count; i++) {  // validate every instance before any device work
+        Grid g{};
+        MomConst M{};
+        const int rc = api_grid_from_params(&params[i], g, M);
+        if (rc) return rc;
+        if (!g.p_mirror)
+            return api_fail(ASD2G_E_UNSUPPORTED, "batch instances need Neumann or Dirichlet pressure on all sides");
+    }
+    asd2g_batch *b = new (std::nothrow) asd2g_batch();
+    if (!b) return api_fail(ASD2G_E_NOMEM, "host allocation failed");
+    b->count = count;
+    b->prm.assign(params, params + count);
+    if (stream) b->st = (cudaStream_t)stream;
+    else {
+        if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess) {
+            delete b;
+            return api_fail(ASD2G_E_CUDA, "cudaStreamCreate failed");
+        }
+        b->own_stream = true;
+    }
+    const int rc = build(b);
+    if (rc) {
+        release(b);
+        return rc;
+    }
+    *out = b;
+    return ASD2G_OK;
+}
+
+int asd2g_batch_destroy(asd2g_batch *b) {
+    if (!b) return ASD2G_OK;
+    cudaStreamSynchronize(b->st);
+    release(b);
+    return ASD2G_OK;
+}
+
+int asd2g_batch_upload(asd2g_batch *b, int inst, int field, const double *host) {
+    const int slot = pad_slot(field);
+    if (!b || !host || inst < 0 || inst >= b->count || slot < 0)
+        return api_fail(ASD2G_E_ARG, "batch_upload: bad instance or field (LS, KAPPA, H, DIV, PS, P)");
+    const Grid &g = b->hinst[inst].g;
+    double *dst = b->pad + (size_t)slot * b->gtot + b->goff[inst];
+    cudaMemcpyAsync(dst, host, sizeof(double) * (size_t)g.sx * g.sy, cudaMemcpyHostToDevice, b->st);
+    return check("batch_upload");
+}
+
+int asd2g_batch_download(asd2g_batch *b, int inst, int field, double *host) {
+    const int slot = pad_slot(field);
+    if (!b || !host || inst < 0 || inst >= b->count || slot < 0)
+        return api_fail(ASD2G_E_ARG, "batch_download: bad instance or field (LS, KAPPA, H, DIV, PS, P)");
+    const Grid &g = b->hinst[inst].g;
+    const double *src = b->pad + (size_t)slot * b->gtot + b->goff[inst];
+    cudaMemcpyAsync(host, src, sizeof(double) * (size_t)g.sx * g.sy, cudaMemcpyDeviceToHost, b->st);
+    if (cudaStreamSynchronize(b->st) != cudaSuccess) return check("batch_download");
+    return check("batch_download");
+}
+
+int asd2g_batch_field_ptr(asd2g_batch *b, int field, void **dptr, size_t *stride_doubles) {
+    const int slot = pad_slot(field);
+    if (!b || !dptr || slot < 0) return api_fail(ASD2G_E_ARG, "batch_field_ptr: bad field");
+    *dptr = b->pad + (size_t)slot * b->gtot;
+    if (stride_doubles) *stride_doubles = b->gtot;
+    return ASD2G_OK;
+}
+
+int asd2g_batch_offset(asd2g_batch *b, int inst, size_t *offset_doubles) {
+    if (!b || !offset_doubles || inst < 0 || inst >= b->count) return api_fail(ASD2G_E_ARG, "batch_offset: bad instance");
+    *offset_doubles = b->goff[inst];
+    return ASD2G_OK;
+}
+
+int asd2g_batch_assemble(asd2g_batch *b, const double *dt) {
+    if (!b || !dt) return api_fail(ASD2G_E_ARG, "batch_assemble: null argument");
+    for (int i = 0; i < b->count; i++) {
+        if (!(dt[i] > 0.0) || !std::isfinite(dt[i])) return api_fail(ASD2G_E_ARG, "batch_assemble: dt must be positive");
+        b->hinst[i].dt = dt[i];
+    }
+    cudaMemcpyAsync(b->dinst, b->hinst.data(), sizeof(BInst) * b->count, cudaMemcpyHostToDevice, b->st);
+    launch_batch_assemble(b->dinst, b->cell_tiles, b->ncell_tiles, b->st);
+    return check("batch_assemble");
+}
+
+int asd2g_batch_solve(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_resid) {
+    if (!b || !(tol > 0.0) || maxit < 1) return api_fail(ASD2G_E_ARG, "batch_solve: bad arguments");
+    const BatchPlan &P = b->plan;
+    launch_batch_set_kstate(P, tol, maxit, b->st);
+    launch_batch_mg_setup(P, b->st);
+    launch_batch_fcg_init(P, b->st);
+    int rc = check("batch solve set-up");
+    if (rc) return rc;
+    if (!b->chunk_exec) {
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return check("capture");
+        for (int k = 0; k < FCG_CHUNK_ITERS; k++) launch_batch_fcg_iter(P, k & 1, b->st);
+        launch_batch_fcg_check(P, b->st);
+        if (cudaStreamEndCapture(b->st, &graph) != cudaSuccess) return check("capture end");
+        const cudaError_t e = cudaGraphInstantiate(&b->chunk_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return check("graph instantiate");
+    }
+    bool all_done = false;
+    for (int launched = 0; !all_done && launched < maxit + 2 * FCG_CHUNK_ITERS; launched += FCG_CHUNK_ITERS) {
+        if (cudaGraphLaunch(b->chunk_exec, b->st) != cudaSuccess) return check("graph launch");
+        cudaMemcpyAsync(b->ks_host, b->ks, sizeof(KState) * b->count, cudaMemcpyDeviceToHost, b->st);
+        if (cudaStreamSynchronize(b->st) != cudaSuccess) return check("batch solve");
+        all_done = true;
+        for (int i = 0; i < b->count; i++)
+            if (!b->ks_host[i].done) all_done = false;
+    }
+    launch_batch_scatter(b->dinst, b->cell_tiles, b->ncell_tiles, b->st);
+    rc = check("batch scatter");
+    if (rc) return rc;
+    int status = ASD2G_OK;
+    for (int i = 0; i < b->count; i++) {
+        const KState &k = b->ks_host[i];
+        if (iters) iters[i] = k.it;
+        if (rel_resid) rel_resid[i] = k.res;
+        if (k.status == -5) status = api_fail(ASD2G_E_NONFINITE, "batch: non-finite residual");
+        else if (k.status == -6) status = api_fail(ASD2G_E_BREAKDOWN, "batch: Krylov breakdown");
+        else if (status == ASD2G_OK && !(!(k.res > tol) || k.status == 2)) status = ASD2G_NOT_CONVERGED;
+    }
+    if (cudaStreamSynchronize(b->st) != cudaSuccess) return check("batch solve");
+    return status;
+}
+
+int asd2g_batch_sync(asd2g_batch *b) {
+    if (!b) return api_fail(ASD2G_E_ARG, "null batch");
+    if (cudaStreamSynchronize(b->st) != cudaSuccess) return check("batch sync");
+    return ASD2G_OK;
+}
+
+}  // extern "C"

@@ -24,6 +24,8 @@
 // kernel also converts z to FP64 and forms the two FCG dot products.
 #include "lsmath.cuh"
 #include "mg.cuh"
+#include "asd2g.h"
+#include "batch.cuh"
 
 namespace asd2g {
 
@@ -56,13 +58,15 @@ __device__ __forceinline__ void mg_block_sum(double (&v)[NV], double (&sh)[NV][3
     }
 }
 
+// Sum NV values over the nb blocks (ids bid) that share partial and counter:
+// every block writes its block sum, the last one to arrive adds them in
+// block order (deterministic) and returns true with the totals in thread 0.
 template <int NV>
-__device__ __forceinline__ bool mg_grid_reduce(double (&v)[NV], double *partial, unsigned *counter,
-                                               double (&tot)[NV]) {
+__device__ __forceinline__ bool mg_reduce(double (&v)[NV], double *partial, unsigned *counter, unsigned bid,
+                                          unsigned nb, double (&tot)[NV]) {
     __shared__ double sh[NV][32];
     __shared__ bool last;
     const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-    const unsigned bid = blockIdx.x + gridDim.x * blockIdx.y, nb = gridDim.x * gridDim.y;
     mg_block_sum<NV>(v, sh);
     if (tid == 0) {
 #pragma unroll
@@ -87,48 +91,60 @@ __device__ __forceinline__ bool mg_grid_reduce(double (&v)[NV], double *partial,
     return true;
 }
 
+template <int NV>
+__device__ __forceinline__ bool mg_grid_reduce(double (&v)[NV], double *partial, unsigned *counter,
+                                               double (&tot)[NV]) {
+    return mg_reduce<NV>(v, partial, counter, blockIdx.x + gridDim.x * blockIdx.y, gridDim.x * gridDim.y, tot);
+}
+
 __device__ __forceinline__ int64_t LK(const MgLevel &L, int i, int j) { return (int64_t)j + (int64_t)L.ny * i; }
 
 // ------------------------------------------------------------- set-up --
 // Level 0 in FP32 from the assembled FP64 system; the pinned cell keeps its
 // diagonal and loses its couplings (its rhs is always 0, so it stays 0).
+__device__ __forceinline__ void mg_l0_cell(int nx, int ny, const Sys &S, const MgLevel &L, int64_t k) {
+    const int i = (int)(k / ny), j = (int)(k % ny);
+    const bool pin0 = S.pinned && k == 0;
+    L.diag[k] = (float)S.diag[k];
+    L.ce[k] = (i < nx - 1 && !pin0) ? (float)S.ce[k] : 0.0f;
+    L.cn[k] = (j < ny - 1 && !pin0) ? (float)S.cn[k] : 0.0f;
+}
+
 __global__ void k_mg_l0(int nx, int ny, Sys S, MgLevel L) {
     const int64_t n = (int64_t)nx * ny;
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(k / ny), j = (int)(k % ny);
-        const bool pin0 = S.pinned && k == 0;
-        L.diag[k] = (float)S.diag[k];
-        L.ce[k] = (i < nx - 1 && !pin0) ? (float)S.ce[k] : 0.0f;
-        L.cn[k] = (j < ny - 1 && !pin0) ? (float)S.cn[k] : 0.0f;
-    }
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        mg_l0_cell(nx, ny, S, L, k);
 }
 
 // Galerkin aggregation R A P with piecewise-constant P (2x2 aggregates; the
 // last aggregate of an odd dimension has one cell in that direction).
+__device__ __forceinline__ void mg_coarsen_cell(const MgLevel &F, const MgLevel &C, int64_t k) {
+    const int I = (int)(k / C.ny), J = (int)(k % C.ny);
+    const int i0 = 2 * I, j0 = 2 * J;
+    const bool hi = i0 + 1 < F.nx, hj = j0 + 1 < F.ny;
+    float d = F.diag[LK(F, i0, j0)];
+    if (hi) d += F.diag[LK(F, i0 + 1, j0)];
+    if (hj) d += F.diag[LK(F, i0, j0 + 1)];
+    if (hi && hj) d += F.diag[LK(F, i0 + 1, j0 + 1)];
+    float inner = 0.0f;
+    if (hi) inner += F.ce[LK(F, i0, j0)];
+    if (hi && hj) inner += F.ce[LK(F, i0, j0 + 1)];
+    if (hj) inner += F.cn[LK(F, i0, j0)];
+    if (hi && hj) inner += F.cn[LK(F, i0 + 1, j0)];
+    C.diag[k] = d - 2.0f * inner;
+    const int ie = hi ? i0 + 1 : i0, je = hj ? j0 + 1 : j0;
+    float ce = F.ce[LK(F, ie, j0)];
+    if (hj) ce += F.ce[LK(F, ie, j0 + 1)];
+    float cn = F.cn[LK(F, i0, je)];
+    if (hi) cn += F.cn[LK(F, i0 + 1, je)];
+    C.ce[k] = ce;
+    C.cn[k] = cn;
+}
+
 __global__ void k_mg_coarsen(MgLevel F, MgLevel C) {
     const int64_t n = (int64_t)C.nx * C.ny;
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        const int I = (int)(k / C.ny), J = (int)(k % C.ny);
-        const int i0 = 2 * I, j0 = 2 * J;
-        const bool hi = i0 + 1 < F.nx, hj = j0 + 1 < F.ny;
-        float d = F.diag[LK(F, i0, j0)];
-        if (hi) d += F.diag[LK(F, i0 + 1, j0)];
-        if (hj) d += F.diag[LK(F, i0, j0 + 1)];
-        if (hi && hj) d += F.diag[LK(F, i0 + 1, j0 + 1)];
-        float inner = 0.0f;
-        if (hi) inner += F.ce[LK(F, i0, j0)];
-        if (hi && hj) inner += F.ce[LK(F, i0, j0 + 1)];
-        if (hj) inner += F.cn[LK(F, i0, j0)];
-        if (hi && hj) inner += F.cn[LK(F, i0 + 1, j0)];
-        C.diag[k] = d - 2.0f * inner;
-        const int ie = hi ? i0 + 1 : i0, je = hj ? j0 + 1 : j0;
-        float ce = F.ce[LK(F, ie, j0)];
-        if (hj) ce += F.ce[LK(F, ie, j0 + 1)];
-        float cn = F.cn[LK(F, i0, je)];
-        if (hi) cn += F.cn[LK(F, i0 + 1, je)];
-        C.ce[k] = ce;
-        C.cn[k] = cn;
-    }
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        mg_coarsen_cell(F, C, k);
 }
 
 // ---------------------------------------------------------- tile loads --
@@ -170,12 +186,10 @@ __device__ __forceinline__ float gs_cell(const Tile &T, int a, int b) {
 // From e = 0: red sweep on tile+2, black on tile+1, residual on the tile,
 // restriction (2x2 sums) into the next level's f.  Stores e (tile).
 template <bool L0>
-__global__ void __launch_bounds__(256) k_mg_pre(MgLevel L, MgLevel C, const double *__restrict__ r64,
-                                                const KState *ks) {
-    if (ks->done) return;
+__device__ __forceinline__ void mg_pre_tile(const MgLevel &L, const MgLevel &C, const double *__restrict__ r64,
+                                            int i0, int j0) {
     __shared__ Tile T;
     __shared__ float res[MT_I][MT_J];
-    const int i0 = blockIdx.y * MT_I, j0 = blockIdx.x * MT_J;
     load_tile<L0>(T, L, r64, i0, j0);
     __syncthreads();
     const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
@@ -217,6 +231,13 @@ __global__ void __launch_bounds__(256) k_mg_pre(MgLevel L, MgLevel C, const doub
     }
 }
 
+template <bool L0>
+__global__ void __launch_bounds__(256) k_mg_pre(MgLevel L, MgLevel C, const double *__restrict__ r64,
+                                                const KState *ks) {
+    if (ks->done) return;
+    mg_pre_tile<L0>(L, C, r64, blockIdx.y * MT_I, blockIdx.x * MT_J);
+}
+
 // ----------------------------------------------------------- post pass --
 // e += omega * P ep_coarse on tile+2, black sweep on tile+1, red sweep on the
 // tile; stores the result in ep.  The halo reads the pre-smoothed e of the
@@ -225,13 +246,12 @@ __global__ void __launch_bounds__(256) k_mg_pre(MgLevel L, MgLevel C, const doub
 // instead writes z = (double) e (0 at the pinned cell) and reduces z.r and
 // z.q into the FCG beta.
 template <bool L0>
-__global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float omega, const double *__restrict__ r64,
-                                                 const double *__restrict__ q64, double *__restrict__ z64, int pinned,
-                                                 KState *ks, double *partial) {
-    if (ks->done) return;
+__device__ __forceinline__ void mg_post_tile(const MgLevel &L, const MgLevel &C, float omega,
+                                             const double *__restrict__ r64, const double *__restrict__ q64,
+                                             double *__restrict__ z64, int pinned, int i0, int j0,
+                                             double (&acc)[2]) {
     __shared__ Tile T;
     __shared__ float ec[MT_I / 2 + 2][MT_J / 2 + 2];
-    const int i0 = blockIdx.y * MT_I, j0 = blockIdx.x * MT_J;
     load_tile<L0>(T, L, r64, i0, j0);
     const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
     const int I0 = i0 / 2 - 1, J0 = j0 / 2 - 1;
@@ -255,7 +275,7 @@ __global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float ome
         if (((i + j) & 1) == 1 && i >= 0 && i < L.nx && j >= 0 && j < L.ny) T.e[a][b] = gs_cell(T, a, b);
     }
     __syncthreads();
-    double acc[2] = {0.0, 0.0};
+    acc[0] = acc[1] = 0.0;
     for (int t = tid; t < MT_I * MT_J; t += nt) {
         const int a = 2 + t / MT_J, b = 2 + t % MT_J;
         const int i = i0 + t / MT_J, j = j0 + t % MT_J;
@@ -273,19 +293,31 @@ __global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float ome
             }
         }
     }
+}
+
+// flexible CG: beta = z_{k+1}.(r_{k+1} - r_k) / (z_k.r_k), r_{k+1} - r_k = -alpha q_k
+// (tot = {z.r, z.q} of the new z; thread 0 of the last block).
+__device__ __forceinline__ void fcg_beta(KState *ks, const double (&tot)[2]) {
+    if (ks->it == 0 || ks->restart) ks->beta = 0.0;
+    else ks->beta = -ks->alpha * tot[1] / ks->rho;
+    ks->restart = 0;
+    ks->rho = tot[0];
+    if (!(tot[0] > 0.0) && ks->it == 0 && ks->res > ks->tol) {
+        ks->status = -6;
+        ks->done = 1;
+    }
+}
+
+template <bool L0>
+__global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float omega, const double *__restrict__ r64,
+                                                 const double *__restrict__ q64, double *__restrict__ z64, int pinned,
+                                                 KState *ks, double *partial) {
+    if (ks->done) return;
+    double acc[2];
+    mg_post_tile<L0>(L, C, omega, r64, q64, z64, pinned, blockIdx.y * MT_I, blockIdx.x * MT_J, acc);
     if (L0) {
         double tot[2];
-        if (mg_grid_reduce<2>(acc, partial, &ks->counter, tot)) {
-            // flexible CG: beta = z_{k+1}.(r_{k+1} - r_k) / (z_k.r_k), r_{k+1} - r_k = -alpha q_k
-            if (ks->it == 0 || ks->restart) ks->beta = 0.0;
-            else ks->beta = -ks->alpha * tot[1] / ks->rho;
-            ks->restart = 0;
-            ks->rho = tot[0];
-            if (!(tot[0] > 0.0) && ks->it == 0 && ks->res > ks->tol) {
-                ks->status = -6;
-                ks->done = 1;
-            }
-        }
+        if (mg_grid_reduce<2>(acc, partial, &ks->counter, tot)) fcg_beta(ks, tot);
     }
 }
 
@@ -297,7 +329,7 @@ __global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float ome
 // Augmented [A | I] of n x 2n doubles, row stride 2 * MG_COARSE_MAX; 32 x 32
 // threads (ty: rows, tx: columns) eliminate each pivot step in parallel.
 constexpr int MG_INV_THREADS = 1024;
-__global__ void __launch_bounds__(MG_INV_THREADS) k_mg_coarse_invert(MgLevel L, double *inv) {
+__device__ __forceinline__ void mg_invert_body(const MgLevel &L, double *inv) {
     extern __shared__ double sm[];
     constexpr int W = 2 * MG_COARSE_MAX;
     double *M = sm, *col = sm + MG_COARSE_MAX * W;
@@ -329,6 +361,8 @@ __global__ void __launch_bounds__(MG_INV_THREADS) k_mg_coarse_invert(MgLevel L, 
         for (int c = tx; c < n; c += 32) inv[r * MG_COARSE_MAX + c] = M[r * W + n + c];
 }
 
+__global__ void __launch_bounds__(MG_INV_THREADS) k_mg_coarse_invert(MgLevel L, double *inv) { mg_invert_body(L, inv); }
+
 // ------------------------------------------------------ coarse V-cycle --
 // Levels s .. nlev-1 (level s has at most MG_CTA_CELLS cells) in ONE CTA:
 // every level's operator, restricted residual and correction live in shared
@@ -350,10 +384,8 @@ __host__ __device__ inline size_t mg_cta_smem(const MgHier &H, int s, int nlev) 
     return n * sizeof(float);
 }
 
-__global__ void __launch_bounds__(MG_CTA_THREADS) k_mg_cta_cycle(MgHier H, int s, int nlev,
-                                                                const double *__restrict__ inv, float omega,
-                                                                const KState *ks) {
-    if (ks->done) return;
+__device__ __forceinline__ void mg_cta_body(const MgLevel *__restrict__ lv, int s, int nlev,
+                                            const double *__restrict__ inv, float omega) {
     extern __shared__ float smf[];
     // 32 x 32 threads: ty walks rows i, tx columns j (no integer division)
     const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
@@ -362,11 +394,11 @@ __global__ void __launch_bounds__(MG_CTA_THREADS) k_mg_cta_cycle(MgHier H, int s
         size_t o = 0;
         for (int l = s; l < nlev; l++) {
             off[l] = o;
-            o += 5 * (size_t)H.l[l].nx * H.l[l].ny;
+            o += 5 * (size_t)lv[l].nx * lv[l].ny;
         }
     }
     for (int l = s; l < nlev; l++) {
-        const MgLevel &L = H.l[l];
+        const MgLevel &L = lv[l];
         const int n = L.nx * L.ny;
         float *D = smf + off[l], *CE = D + n, *CN = CE + n, *F = CN + n;
         for (int k = tid; k < n; k += MG_CTA_THREADS) {
@@ -378,7 +410,7 @@ __global__ void __launch_bounds__(MG_CTA_THREADS) k_mg_cta_cycle(MgHier H, int s
     }
     __syncthreads();
     for (int l = s; l < nlev - 1; l++) {
-        const int nx = H.l[l].nx, ny = H.l[l].ny, n = nx * ny;
+        const int nx = lv[l].nx, ny = lv[l].ny, n = nx * ny;
         const float *D = smf + off[l], *CE = D + n, *CN = CE + n, *F = CN + n;
         float *E = smf + off[l] + 4 * (size_t)n;
         // red from zero (e = f / d) and black from those red values, in one
@@ -398,7 +430,7 @@ __global__ void __launch_bounds__(MG_CTA_THREADS) k_mg_cta_cycle(MgHier H, int s
                 }
             }
         __syncthreads();
-        const int cnx = H.l[l + 1].nx, cny = H.l[l + 1].ny;
+        const int cnx = lv[l + 1].nx, cny = lv[l + 1].ny;
         float *Fc = smf + off[l + 1] + 3 * (size_t)cnx * cny;
         for (int I = ty; I < cnx; I += 32)
             for (int J = tx; J < cny; J += 32) {
@@ -423,7 +455,7 @@ __global__ void __launch_bounds__(MG_CTA_THREADS) k_mg_cta_cycle(MgHier H, int s
     }
     {
         // e = inv f on the coarsest level (<= 64 cells): 16 lanes per row
-        const int l = nlev - 1, n = H.l[l].nx * H.l[l].ny;
+        const int l = nlev - 1, n = lv[l].nx * lv[l].ny;
         const float *F = smf + off[l] + 3 * (size_t)n;
         float *E = smf + off[l] + 4 * (size_t)n;
         const int row = tid >> 4, c = tid & 15;
@@ -438,8 +470,8 @@ __global__ void __launch_bounds__(MG_CTA_THREADS) k_mg_cta_cycle(MgHier H, int s
         __syncthreads();
     }
     for (int l = nlev - 2; l >= s; l--) {
-        const int nx = H.l[l].nx, ny = H.l[l].ny, n = nx * ny;
-        const int cny = H.l[l + 1].ny, cn = H.l[l + 1].nx * cny;
+        const int nx = lv[l].nx, ny = lv[l].ny, n = nx * ny;
+        const int cny = lv[l + 1].ny, cn = lv[l + 1].nx * cny;
         const float *D = smf + off[l], *CE = D + n, *CN = CE + n, *F = CN + n;
         float *E = smf + off[l] + 4 * (size_t)n;
         const float *Ec = smf + off[l + 1] + 4 * (size_t)cn;
@@ -471,9 +503,16 @@ __global__ void __launch_bounds__(MG_CTA_THREADS) k_mg_cta_cycle(MgHier H, int s
             }
         __syncthreads();
     }
-    const int n = H.l[s].nx * H.l[s].ny;
+    const int n = lv[s].nx * lv[s].ny;
     const float *E = smf + off[s] + 4 * (size_t)n;
-    for (int k = tid; k < n; k += MG_CTA_THREADS) H.l[s].ep[k] = E[k];
+    for (int k = tid; k < n; k += MG_CTA_THREADS) lv[s].ep[k] = E[k];
+}
+
+__global__ void __launch_bounds__(MG_CTA_THREADS) k_mg_cta_cycle(MgHier H, int s, int nlev,
+                                                                const double *__restrict__ inv, float omega,
+                                                                const KState *ks) {
+    if (ks->done) return;
+    mg_cta_body(H.l, s, nlev, inv, omega);
 }
 
 // ------------------------------------------------------------ FCG FP64 --
@@ -614,6 +653,240 @@ __global__ void k_fcg_init(int64_t n, Sys S, double *__restrict__ x, double *__r
     }
 }
 
+// ------------------------------------------------------------ batched --
+// The kernels below serve every instance of a batch in one launch: block b
+// takes work-list entry b, reads that instance's descriptor and returns at
+// entry once the instance has converged (every block of an instance sees the
+// same flag: it only changes in the last block of a reduction, after all of
+// them have arrived).  Per-instance sums use the instance's own partial slots
+// and KState ticket, with block ids local to the instance.
+
+__global__ void k_bmg_l0(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    const int64_t k0 = (int64_t)w.c * FCG_CHUNK;
+    for (int t = threadIdx.x; t < FCG_CHUNK; t += blockDim.x)
+        if (k0 + t < I.n) mg_l0_cell(I.g.nx, I.g.ny, I.S, I.lv[0], k0 + t);
+}
+
+__global__ void k_bmg_coarsen(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks, int l) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    const MgLevel &C = I.lv[l];
+    const int64_t k0 = (int64_t)w.c * FCG_CHUNK, n = (int64_t)C.nx * C.ny;
+    for (int t = threadIdx.x; t < FCG_CHUNK; t += blockDim.x)
+        if (k0 + t < n) mg_coarsen_cell(I.lv[l - 1], C, k0 + t);
+}
+
+__global__ void __launch_bounds__(MG_INV_THREADS) k_bmg_invert(const BInst *__restrict__ insts) {
+    const BInst &I = insts[blockIdx.x];
+    mg_invert_body(I.lv[I.nlev - 1], I.coarse_inv);
+}
+
+__global__ void k_bset_kstate(const BInst *__restrict__ insts, int count, double tol, int maxit) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= count) return;
+    KState *ks = insts[b].ks;
+    ks->tol = tol;
+    ks->maxit = maxit;
+    ks->mode = ASD2G_SOLVER_MGPCG;
+    ks->reg = 0.0;
+    ks->done = 0;
+    ks->status = 0;
+    ks->it = 0;
+    ks->counter = 0u;
+    ks->verified = 0;
+    ks->restart = 0;
+    ks->res_true_prev = -1.0;
+}
+
+__global__ void __launch_bounds__(256) k_bfcg_init(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    const int64_t k0 = (int64_t)w.c * FCG_CHUNK;
+    double v[1] = {0.0};
+    for (int t = threadIdx.x; t < FCG_CHUNK; t += blockDim.x) {
+        const int64_t k = k0 + t;
+        if (k >= I.n) break;
+        const double bk = I.S.b[k];
+        I.x[k] = 0.0;
+        I.r[k] = bk;
+        I.pa[k] = 0.0;
+        I.q[k] = 0.0;
+        v[0] += bk * bk;
+    }
+    double tot[1];
+    KState *ks = I.ks;
+    if (mg_reduce<1>(v, I.partial, &ks->counter, w.c, I.chunks, tot)) {
+        double bn = sqrt(tot[0]);
+        if (bn == 0.0) bn = 1.0;
+        ks->bn = bn;
+        ks->res = sqrt(tot[0]) / bn;
+        ks->it = 0;
+        ks->status = 0;
+        ks->alpha = 0.0;
+        ks->verified = 0;
+        ks->restart = 0;
+        ks->res_true_prev = -1.0;
+        ks->done = (!(ks->res > ks->tol) || ks->maxit <= 0) ? 1 : 0;
+    }
+}
+
+// (A x)_k of one instance's compact system (pinned row: 0)
+__device__ __forceinline__ double sys_apply(const Sys &S, int nx, int ny, const double *__restrict__ x, int64_t k) {
+    if (S.pinned && k == 0) return 0.0;
+    const int ii = (int)(k / ny), jj = (int)(k % ny);
+    double y = 0.0;
+    if (jj > 0) y += -S.cn[k - 1] * x[k - 1];
+    if (ii > 0) y += -S.ce[k - ny] * x[k - ny];
+    y += S.diag[k] * x[k];
+    if (ii < nx - 1) y += -S.ce[k] * x[k + ny];
+    if (jj < ny - 1) y += -S.cn[k] * x[k + 1];
+    return y;
+}
+
+__global__ void __launch_bounds__(256) k_bfcg_a(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks,
+                                                int parity) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    KState *ks = I.ks;
+    if (ks->done) return;
+    const double beta = ks->beta;
+    const double *p_old = parity ? I.pb : I.pa;
+    double *p_new = parity ? I.pa : I.pb;
+    const int nx = I.g.nx, ny = I.g.ny;
+    const int64_t k0 = (int64_t)w.c * FCG_CHUNK;
+    double v[1] = {0.0};
+    for (int t = threadIdx.x; t < FCG_CHUNK; t += blockDim.x) {
+        const int64_t k = k0 + t;
+        if (k >= I.n) break;
+        const int ii = (int)(k / ny), jj = (int)(k % ny);
+        auto pv = [&](int64_t m) { return I.z[m] + beta * p_old[m]; };
+        const double pc = pv(k);
+        double y = 0.0;
+        if (!(I.S.pinned && k == 0)) {
+            if (jj > 0) y += -I.S.cn[k - 1] * pv(k - 1);
+            if (ii > 0) y += -I.S.ce[k - ny] * pv(k - ny);
+            y += I.S.diag[k] * pc;
+            if (ii < nx - 1) y += -I.S.ce[k] * pv(k + ny);
+            if (jj < ny - 1) y += -I.S.cn[k] * pv(k + 1);
+        }
+        p_new[k] = pc;
+        I.q[k] = y;
+        v[0] += pc * y;
+    }
+    double tot[1];
+    if (mg_reduce<1>(v, I.partial, &ks->counter, w.c, I.chunks, tot)) {
+        if (!(tot[0] != 0.0) || !isfinite(tot[0])) {
+            ks->status = -6;
+            ks->done = 1;
+        } else {
+            ks->alpha = ks->rho / tot[0];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_bfcg_b(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks,
+                                                int parity) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    KState *ks = I.ks;
+    if (ks->done) return;
+    const double alpha = ks->alpha;
+    const double *p = parity ? I.pa : I.pb;
+    const int64_t k0 = (int64_t)w.c * FCG_CHUNK;
+    double v[1] = {0.0};
+    for (int t = threadIdx.x; t < FCG_CHUNK; t += blockDim.x) {
+        const int64_t k = k0 + t;
+        if (k >= I.n) break;
+        I.x[k] += alpha * p[k];
+        const double rk = I.r[k] - alpha * I.q[k];
+        I.r[k] = rk;
+        v[0] += rk * rk;
+    }
+    double tot[1];
+    if (mg_reduce<1>(v, I.partial, &ks->counter, w.c, I.chunks, tot)) {
+        const int it = ks->it + 1;
+        ks->it = it;
+        ks->res = sqrt(tot[0]) / ks->bn;
+        if (!isfinite(ks->res)) {
+            ks->status = -5;
+            ks->done = 1;
+        } else if (!(ks->res > ks->tol) || it >= ks->maxit) {
+            ks->done = 1;
+        }
+    }
+}
+
+// FP64 residual replacement with the single-system rules (k_fcg_replace).
+__global__ void __launch_bounds__(256) k_bfcg_replace(const BInst *__restrict__ insts,
+                                                      const BChunk *__restrict__ chunks) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    KState *ks = I.ks;
+    if (!ks->done || ks->verified || ks->status != 0) return;
+    const int64_t k0 = (int64_t)w.c * FCG_CHUNK;
+    double v[1] = {0.0};
+    for (int t = threadIdx.x; t < FCG_CHUNK; t += blockDim.x) {
+        const int64_t k = k0 + t;
+        if (k >= I.n) break;
+        const double rk = (I.S.pinned && k == 0) ? 0.0 : I.S.b[k] - sys_apply(I.S, I.g.nx, I.g.ny, I.x, k);
+        I.r[k] = rk;
+        v[0] += rk * rk;
+    }
+    double tot[1];
+    if (mg_reduce<1>(v, I.partial, &ks->counter, w.c, I.chunks, tot)) {
+        const double res = sqrt(tot[0]) / ks->bn;
+        const double prev = ks->res_true_prev;
+        ks->res = res;
+        ks->res_true_prev = res;
+        if (!isfinite(res)) {
+            ks->status = -5;
+            ks->verified = 1;
+        } else if (!(res > ks->tol) || ks->it >= ks->maxit) {
+            ks->verified = 1;
+        } else if (prev >= 0.0 && res > 0.5 * prev) {
+            ks->status = 2;
+            ks->verified = 1;
+        } else {
+            ks->done = 0;
+            ks->restart = 1;
+        }
+    }
+}
+
+template <bool L0>
+__global__ void __launch_bounds__(256) k_bmg_pre(const BInst *__restrict__ insts, const BTile *__restrict__ tiles,
+                                                 int l) {
+    const BTile w = tiles[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    if (I.ks->done) return;
+    mg_pre_tile<L0>(I.lv[l], I.lv[l + 1], L0 ? I.r : nullptr, w.by * MT_I, w.bx * MT_J);
+}
+
+__global__ void __launch_bounds__(MG_CTA_THREADS) k_bmg_cta(const BInst *__restrict__ insts, float omega) {
+    const BInst &I = insts[blockIdx.x];
+    if (I.ks->done) return;
+    mg_cta_body(I.lv, I.s_cta, I.nlev, I.coarse_inv, omega);
+}
+
+template <bool L0>
+__global__ void __launch_bounds__(256) k_bmg_post(const BInst *__restrict__ insts, const BTile *__restrict__ tiles,
+                                                  int l, float omega) {
+    const BTile w = tiles[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    KState *ks = I.ks;
+    if (ks->done) return;
+    double acc[2];
+    mg_post_tile<L0>(I.lv[l], I.lv[l + 1], omega, L0 ? I.r : nullptr, L0 ? I.q : nullptr, L0 ? I.z : nullptr,
+                     I.S.pinned, w.by * MT_I, w.bx * MT_J, acc);
+    if (L0) {
+        const int gx = (I.lv[0].ny + MT_J - 1) / MT_J;
+        double tot[2];
+        if (mg_reduce<2>(acc, I.partial, &ks->counter, w.bx + gx * w.by, I.tiles0, tot)) fcg_beta(ks, tot);
+    }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ host --
@@ -657,6 +930,8 @@ static int mg_cta_level(const MgLevel *lv, int nlev) {
     while (s < nlev - 1 && (int64_t)lv[s].nx * lv[s].ny > MG_CTA_CELLS) s++;
     return s;
 }
+
+int mg_cta_first_level(const MgLevel *lv, int nlev) { return mg_cta_level(lv, nlev); }
 
 // Shared memory of the coarse cycle: level s has at most 4096 cells and each
 // coarser level at most half of the previous one plus one (a one-cell-wide
@@ -726,6 +1001,69 @@ bool launch_fcg_check(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const
     const int64_t n = (int64_t)nx * ny;
     k_fcg_replace<<<red_blocks(n), 256, 0, st>>>(nx, ny, S, x, r, ks, partial);
     enqueue_vcycle(lv, nlev, coarse_inv, r, q, z, S.pinned, ks, partial, st);
+    return true;
+}
+
+// ---------------------------------------------------------- batched host --
+int batch_tiles0(int nx, int ny) { return ((ny + MT_J - 1) / MT_J) * ((nx + MT_I - 1) / MT_I); }
+
+int64_t batch_partial_len(int nx, int ny) {
+    const int64_t chunks = ((int64_t)nx * ny + FCG_CHUNK - 1) / FCG_CHUNK;
+    const int64_t a = 2 * (int64_t)batch_tiles0(nx, ny), b = 2 * chunks;
+    return a > b ? a : b;
+}
+
+bool batch_cta_prepare() {
+    const size_t inv = sizeof(double) * (MG_COARSE_MAX * 2 * MG_COARSE_MAX + MG_COARSE_MAX);
+    return cudaFuncSetAttribute(k_bmg_cta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MG_CTA_SMEM_BOUND) ==
+               cudaSuccess &&
+           cudaFuncSetAttribute(k_bmg_invert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv) == cudaSuccess;
+}
+
+void launch_batch_set_kstate(const BatchPlan &P, double tol, int maxit, cudaStream_t st) {
+    k_bset_kstate<<<(P.count + 127) / 128, 128, 0, st>>>(P.insts, P.count, tol, maxit);
+}
+
+void launch_batch_mg_setup(const BatchPlan &P, cudaStream_t st) {
+    k_bmg_l0<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks);
+    for (int l = 1; l < P.max_nlev; l++)
+        if (P.nlvl_chunks[l] > 0) k_bmg_coarsen<<<P.nlvl_chunks[l], 256, 0, st>>>(P.insts, P.lvl_chunks[l], l);
+    const size_t inv = sizeof(double) * (MG_COARSE_MAX * 2 * MG_COARSE_MAX + MG_COARSE_MAX);
+    k_bmg_invert<<<P.count, MG_INV_THREADS, inv, st>>>(P.insts);
+}
+
+static void batch_vcycle(const BatchPlan &P, cudaStream_t st) {
+    const dim3 blk(32, 8);
+    const float omega = 1.9f;
+    for (int l = 0; l < P.max_s; l++) {
+        if (P.nmg_tiles[l] == 0) continue;
+        if (l == 0) k_bmg_pre<true><<<P.nmg_tiles[0], blk, 0, st>>>(P.insts, P.mg_tiles[0], 0);
+        else k_bmg_pre<false><<<P.nmg_tiles[l], blk, 0, st>>>(P.insts, P.mg_tiles[l], l);
+    }
+    k_bmg_cta<<<P.count, MG_CTA_THREADS, MG_CTA_SMEM_BOUND, st>>>(P.insts, omega);
+    for (int l = P.max_s - 1; l >= 0; l--) {
+        if (P.nmg_tiles[l] == 0) continue;
+        if (l == 0) k_bmg_post<true><<<P.nmg_tiles[0], blk, 0, st>>>(P.insts, P.mg_tiles[0], 0, omega);
+        else k_bmg_post<false><<<P.nmg_tiles[l], blk, 0, st>>>(P.insts, P.mg_tiles[l], l, omega);
+    }
+}
+
+bool launch_batch_fcg_init(const BatchPlan &P, cudaStream_t st) {
+    k_bfcg_init<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks);
+    batch_vcycle(P, st);
+    return true;
+}
+
+bool launch_batch_fcg_iter(const BatchPlan &P, int parity, cudaStream_t st) {
+    k_bfcg_a<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks, parity);
+    k_bfcg_b<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks, parity);
+    batch_vcycle(P, st);
+    return true;
+}
+
+bool launch_batch_fcg_check(const BatchPlan &P, cudaStream_t st) {
+    k_bfcg_replace<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks);
+    batch_vcycle(P, st);
     return true;
 }
 

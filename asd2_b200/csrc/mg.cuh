@@ -22,6 +22,8 @@ int mg_levels_for(int nx, int ny, int *dims, int max_levels);
 // two per level-0 tile of the fused post-smoothing pass (its dots), at
 // least what the 1D reduction kernels use (three per block, RED_BLOCKS_MAX).
 int64_t mg_partial_len(int nx, int ny);
+// First level of the one-CTA coarse cycle for this hierarchy (at least 1).
+int mg_cta_first_level(const MgLevel *lv, int nlev);
 // Sets up the single-CTA coarse cycle for this hierarchy (its shared memory);
 // false if it does not fit (not reachable with <= 4096-cell CTA levels).
 bool mg_cta_prepare(const MgLevel *lv, int nlev);

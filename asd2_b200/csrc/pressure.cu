@@ -11,6 +11,7 @@
 // a CUDA graph) and the host only polls between chunks.
 #include "lsmath.cuh"
 #include "pressure.cuh"
+#include "batch.cuh"
 
 namespace asd2g {
 
@@ -91,12 +92,12 @@ __device__ __forceinline__ bool p_dir_like(int b) {
     return b == 2 /*DIRICHLET*/ || b == 5 /*INLET*/ || b == 6 /*OUTLET*/ || b == 7 /*PRESSURE*/ || b == 4 /*WALL*/;
 }
 
-__global__ void k_assemble(Grid g, MomConst M, DivH dxx, DivH dyy, const double *__restrict__ ls,
-                           const double *__restrict__ kappa, const double *__restrict__ H,
-                           const double *__restrict__ div, const double *__restrict__ dtp, Sys S) {
-    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
-    if (i >= g.nx + NB || j >= g.ny + NB) return;
-    const double dt = *dtp, rH = M.rho_h, rL = M.rho_l, sig = M.sigma;
+// One interior cell (i, j) of the GFM system (mac2d.cpp:1330-1607).
+__device__ __forceinline__ void assemble_cell(const Grid &g, const MomConst &M, const DivH &dxx, const DivH &dyy,
+                                              const double *__restrict__ ls, const double *__restrict__ kappa,
+                                              const double *__restrict__ H, const double *__restrict__ div,
+                                              double dt, const Sys &S, int i, int j) {
+    const double rH = M.rho_h, rL = M.rho_l, sig = M.sigma;
     const int64_t c = IX(g, i, j), cw = IX(g, i - 1, j), ce = IX(g, i + 1, j), cs = IX(g, i, j - 1),
                   cn = IX(g, i, j + 1);
     const double lsM = ls[c];
@@ -147,6 +148,37 @@ __global__ void k_assemble(Grid g, MomConst M, DivH dxx, DivH dyy, const double 
     S.cn[k] = -aN;
     S.b[k] = pin0 ? 0.0 : r;
     S.minv[k] = pin0 ? 0.0 : 1.0 / aC;  // InvertMatrixDiagonal, poisson2d.cpp:577-585
+}
+
+__global__ void k_assemble(Grid g, MomConst M, DivH dxx, DivH dyy, const double *__restrict__ ls,
+                           const double *__restrict__ kappa, const double *__restrict__ H,
+                           const double *__restrict__ div, const double *__restrict__ dtp, Sys S) {
+    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
+    if (i >= g.nx + NB || j >= g.ny + NB) return;
+    assemble_cell(g, M, dxx, dyy, ls, kappa, H, div, *dtp, S, i, j);
+}
+
+// Batched: block b assembles cell tile b of its instance (32 x 8 cells).
+__global__ void k_bassemble(const BInst *__restrict__ insts, const BTile *__restrict__ tiles) {
+    const BTile w = tiles[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    const int j = NB + w.bx * TJ + threadIdx.x, i = NB + w.by * TI + threadIdx.y;
+    if (i >= I.g.nx + NB || j >= I.g.ny + NB) return;
+    assemble_cell(I.g, I.M, I.dxx, I.dyy, I.ls, I.kappa, I.H, I.div, I.dt, I.S, i, j);
+}
+
+// Batched scatter: PS = x on the interior with its ghost mirrors (every
+// batch instance has Neumann/Dirichlet pressure sides), P = PS / dt.
+__global__ void k_bscatter(const BInst *__restrict__ insts, const BTile *__restrict__ tiles) {
+    const BTile w = tiles[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    const Grid &g = I.g;
+    const int j = NB + w.bx * TJ + threadIdx.x, i = NB + w.by * TI + threadIdx.y;
+    if (i >= g.nx + NB || j >= g.ny + NB) return;
+    const double v = I.x[(int64_t)(j - NB) + (int64_t)g.ny * (i - NB)];
+    I.ps[IX(g, i, j)] = v;
+    p_mirror_store(g, I.ps, i, j, v);
+    I.p[IX(g, i, j)] = v / I.dt;  // mac2d.cpp:1722-1724
 }
 
 // ------------------------------------------------------------------ SpMV --
@@ -628,6 +660,14 @@ void launch_true_residual(const Grid &g, const Sys &S, const double *ps, double 
     const int64_t n = (int64_t)g.nx * g.ny;
     unsigned *counter = reinterpret_cast<unsigned *>(out2 + 2);
     k_true_residual<<<red_blocks(n), 256, 0, st>>>(g, S, ps, partial, counter, out2);
+}
+
+void launch_batch_assemble(const BInst *insts, const BTile *tiles, int ntiles, cudaStream_t st) {
+    if (ntiles > 0) k_bassemble<<<ntiles, dim3(TJ, TI), 0, st>>>(insts, tiles);
+}
+
+void launch_batch_scatter(const BInst *insts, const BTile *tiles, int ntiles, cudaStream_t st) {
+    if (ntiles > 0) k_bscatter<<<ntiles, dim3(TJ, TI), 0, st>>>(insts, tiles);
 }
 
 }  // namespace asd2g

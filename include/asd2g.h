@@ -246,6 +246,31 @@ int asd2g_csr_solve(asd2g_session *s, int solver, int rows, const int *ia, const
                     const double *diag, const double *b, double *x, double tol, int maxit, int *iters,
                     double *rel_resid);
 
+/* ---- batched GFM pressure solves (no reference counterpart) ----
+ * Many independent droplets of uneven grid sizes: each phase of assembly and
+ * of the mixed-precision multigrid-preconditioned flexible CG is one kernel
+ * launch for the whole batch; every instance has its own solver scalars and
+ * stops on its own (same rules as ASD2G_SOLVER_MGPCG).  Instances need
+ * Neumann or Dirichlet pressure on all four sides. */
+typedef struct asd2g_batch asd2g_batch;
+/* params[0 .. count-1]: one per instance (grid, fluid, BCs as for a session). */
+int asd2g_batch_create(const asd2g_params *params, int count, void *stream, asd2g_batch **out);
+int asd2g_batch_destroy(asd2g_batch *b);
+/* Padded (nx+6)*(ny+6) arrays of instance inst: LS, KAPPA, H, DIV (inputs of
+ * the assembly), PS, P (outputs of the solve). */
+int asd2g_batch_upload(asd2g_batch *b, int inst, int field, const double *host);
+int asd2g_batch_download(asd2g_batch *b, int inst, int field, double *host);
+/* Device arena of a field (all instances, instance i at offset(i) doubles). */
+int asd2g_batch_field_ptr(asd2g_batch *b, int field, void **dptr, size_t *stride_doubles);
+int asd2g_batch_offset(asd2g_batch *b, int inst, size_t *offset_doubles);
+/* GFM assembly of every instance (KAPPA as uploaded), dt[count]. */
+int asd2g_batch_assemble(asd2g_batch *b, const double *dt);
+/* Solve every assembled system to the FP64-verified rel. residual tol; PS and
+ * P written (P = PS / dt).  iters[count], rel_resid[count] may be NULL.
+ * ASD2G_NOT_CONVERGED if any instance reached maxit. */
+int asd2g_batch_solve(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_resid);
+int asd2g_batch_sync(asd2g_batch *b);
+
 /* ---- whole step (test_mac2d_large.cpp:496-552) ----
  * lsB = LS; advect; reinit (reinit_mode); kappa; H, HS; intermediate velocity
  * with HS; U/V fill; divergence; GFM assembly; pressure solve; projection;

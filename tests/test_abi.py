@@ -70,3 +70,11 @@ def test_mixed_precision_needs_producer_side_pressure_fill():
     with pytest.raises(api.Asd2gError) as e:
         api.Session(p)
     assert e.value.code == -1
+
+
+def test_batch_refuses_periodic_pressure_before_device_work():
+    ok = api.Params(32, 32, 1 / 32, 1 / 32)
+    bad = api.Params(40, 24, 1 / 40, 1 / 40, bc_p=("periodic",) * 4)
+    with pytest.raises(api.Asd2gError) as e:
+        api.Batch([ok, bad])
+    assert e.value.code == -4
