@@ -237,6 +237,93 @@ def mixed_precision_errors(sh):
             "pressure_iterations": {"fp64_jacobi_pcg": b["its"], "mixed_mg_fcg": a["its"]}}
 
 
+BATCH_COUNT = 256
+
+
+def batched_solves(sh, stream, flush, count=BATCH_COUNT):
+    """The 256-droplet batch (grid side uniform in {64, 96, ..., 512}, radius
+    in [0.08, 0.2], density ratio log-uniform in [1, 1000], viscosity ratio
+    log-uniform in [1, 100]): each instance's GFM system is taken after one
+    full FP64 droplet step from rest.  Timed: the batched assembly + solve of
+    all systems to the FP64-verified rel. residual 1e-8 (one launch per
+    phase), against the same systems solved one after another by the FP64
+    Jacobi-PCG (the plain FP64 GPU CG) and by the single-system MG-FCG."""
+    import torch
+    from asd2_b200 import api
+    from asd2_b200 import workloads as W
+    cases = W.droplet_batch(count, seed=0)
+    states, t_cg, t_mg, its_cg, its_mg = [], 0.0, 0.0, [], []
+
+    def timed(fn):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return r, e0.elapsed_time(e1) / 1e3
+
+    for c in cases:
+        with api.Session(api.Params.from_case(c), stream=sh) as ss:
+            ss.upload("ls", c.ls)
+            ss.upload("u", c.u)
+            ss.upload("v", c.v)
+            ss.apply_bc("ls", "P")
+            dt = ss.update_dt()
+            r = ss.droplet_step(dt, solver=api.MGPCG, tol=1e-10, maxit=500000)
+            if r["status"] != 0:
+                raise SystemExit(f"bench: batch preparation step failed: {r}")
+            snap = {k: ss.download(k) for k in ("ls", "H", "kappa", "div")}
+            states.append((snap, dt))
+
+            def solve(sv):
+                ss.assemble_gfm(dt, recompute_kappa=False)
+                return ss.solve_pressure(sv, tol=TOL, maxit=500000, dt=dt)
+            solve(api.PCG)
+            rc, t = timed(lambda: solve(api.PCG))
+            if rc["status"] != 0:
+                raise SystemExit(f"bench: FP64 CG did not converge: {rc}")
+            t_cg += t
+            its_cg.append(rc["iters"])
+            solve(api.MGPCG)
+            rm, t = timed(lambda: solve(api.MGPCG))
+            t_mg += t
+            its_mg.append(rm["iters"])
+    b = api.Batch([api.Params.from_case(c) for c in cases], stream=sh)
+    for k, (snap, _) in enumerate(states):
+        for f in ("ls", "H", "kappa", "div"):
+            b.upload(k, f, snap[f])
+    dts = np.array([dt for _, dt in states])
+
+    def batch_once():
+        b.assemble(dts)
+        return b.solve(tol=TOL, maxit=10000)
+    for _ in range(2):
+        batch_once()
+    times, res = [], None
+    for _ in range(5):
+        res, t = timed(batch_once)
+        if res["status"] != 0:
+            raise SystemExit(f"bench: batched solve did not converge: {res['status']}")
+        times.append(t)
+    b.close()
+    t_b = float(np.median(times))
+    cells = int(sum(c.nx * c.ny for c in cases))
+    return {"workload": f"{count} droplets, grid side uniform in {{64, 96, ..., 512}} ({cells / 1e6:.1f} M unknowns), "
+                        "radius [0.08, 0.2], density ratio log-U[1, 1000], viscosity ratio log-U[1, 100]; "
+                        "each system after one full step from rest",
+            "value": count / t_b, "unit": "GFM Poisson solves/s", "ms_per_batch": t_b * 1e3,
+            "tol": TOL, "max_true_rel_residual": float(np.max(res["resid"])),
+            "iters": {"batched_max": int(np.max(res["iters"])), "batched_mean": float(np.mean(res["iters"])),
+                      "fp64_cg_mean": float(np.mean(its_cg)), "single_mg_mean": float(np.mean(its_mg))},
+            "fp64_cg_sequential": {"value": count / t_cg, "unit": "GFM Poisson solves/s",
+                                   "solver": "FP64 Jacobi-PCG per system, one system after another"},
+            "single_mg_sequential": {"value": count / t_mg, "unit": "GFM Poisson solves/s"},
+            "speedup_vs_fp64_cg": t_cg / t_b,
+            "l2": "flushed (256 MB write) before each timed batch / system"}
+
+
 def run_ours(args):
     import torch
     from asd2_b200 import api
@@ -380,6 +467,7 @@ def run_ours(args):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     ls_rates = level_set_rates(sh, stream, flush, peak) if not args.no_extra else None
+    batched = batched_solves(sh, stream, flush) if not args.no_extra else None
     mixed = mixed_precision_errors(sh) if not args.no_extra else None
     nlev = len(_mg_levels(args.n, args.n))
     per_iter = 2 + 2 * (nlev - 1) + 1
@@ -420,6 +508,7 @@ def run_ours(args):
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback",
                      "note": "working set is L2-resident at 256^2; iteration time from CUDA events "
                              "(solve minus assembly) / iterations"},
+        "batched_256": batched,
         "ls_large": ls_rates,
         "mixed_precision_1024": mixed,
         "e2e": {"value": e2e_value, "unit": "GFM Poisson solves/s",
@@ -533,7 +622,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the 2048^2 level-set and 1024^2 mixed-precision reports")
-    ap.add_argument("--section", default=None, choices=["ls_large", "mixed_1024"],
+    ap.add_argument("--section", default=None, choices=["ls_large", "mixed_1024", "batched"],
                     help="run only this report (its JSON object on stdout), e.g. to profile it")
     args = ap.parse_args()
     if args.section:
@@ -557,6 +646,9 @@ def run_section(name):
         except Exception:
             pass
         out = level_set_rates(stream.cuda_stream, stream, flush, peak)
+    elif name == "batched":
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        out = batched_solves(stream.cuda_stream, stream, flush)
     else:
         out = mixed_precision_errors(stream.cuda_stream)
     print(json.dumps({"section": name, **out}), flush=True)
