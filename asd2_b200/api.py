@@ -66,6 +66,7 @@ EXPORTS = [
     "asd2g_apply_bc_side", "asd2g_update_ntk", "asd2g_csr_solve", "asd2g_volume", "asd2g_last_volume",
     "asd2g_batch_create", "asd2g_batch_destroy", "asd2g_batch_upload", "asd2g_batch_download",
     "asd2g_batch_field_ptr", "asd2g_batch_offset", "asd2g_batch_assemble", "asd2g_batch_solve", "asd2g_batch_sync",
+    "asd2g_conv_wpack_bytes", "asd2g_conv_pack_weights", "asd2g_conv3x3_bf16",
 ]
 
 _lib = None
@@ -118,6 +119,10 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_batch_offset": ([S, I, C.POINTER(C.c_size_t)], I),
         "asd2g_batch_assemble": ([S, dp], I),
         "asd2g_batch_solve": ([S, D, I, ip, dp], I),
+        "asd2g_conv_wpack_bytes": ([I, I], C.c_size_t),
+        "asd2g_conv_pack_weights": ([C.c_void_p, I, I, I, I, C.c_void_p, C.c_void_p], I),
+        "asd2g_conv3x3_bf16": ([C.c_void_p, I, I, I, I, C.c_void_p, C.c_void_p, I, C.c_void_p, C.c_void_p, I,
+                                C.c_void_p, C.c_void_p], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

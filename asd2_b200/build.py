@@ -34,6 +34,7 @@ UNITS = {
     "mg.cu": [],
     "levelset32.cu": [],
     "batch.cu": [],
+    "unet.cu": [],
 }
 
 

@@ -1,0 +1,206 @@
+// Tensor-core building blocks of the learned preconditioner (U-Net): a 3x3
+// "same" convolution as an implicit GEMM on tcgen05 (BF16 activations and
+// weights, FP32 accumulation in tensor memory), and the weight packing it
+// reads.  No reference counterpart (the reference has no learned solver).
+//
+// Implicit GEMM: D[p][co] = sum over taps t and input channels ci of
+// X[p + off(t)][ci] * W[co][t][ci] for a tile of 128 consecutive output
+// pixels p of one image row (M = 128) and all output channels (N = Cout).
+// Activations are NHWC BF16 with Cin a multiple of 16.  For each chunk of 16
+// input channels the CTA stages in shared memory
+//   * the input patch (3 rows x 130 pixels) as two 8-channel half-planes of
+//     16-byte pixel rows -- the K-major canonical layout, so the A operand of
+//     tap (dy, dx) is the same buffer started dy * 130 + dx rows later;
+//   * the chunk's packed weights [tap][half][co][8] (the B operands);
+// then one thread issues the nine tcgen05.mma of the chunk and commits them
+// to an mbarrier.  The epilogue reads the accumulator from tensor memory
+// (warp w owns pixel rows 32w .. 32w+31), adds the bias, applies ReLU and
+// stores BF16 NHWC (and optionally channel 0 in FP32).
+#include <cuda_bf16.h>
+
+#include "asd2g.h"
+#include "internal.cuh"
+#include "tc05.cuh"
+
+namespace asd2g {
+namespace {
+
+constexpr int CT_PIX = 128;             // output pixels per tile
+constexpr int PATCH_W = CT_PIX + 2;     // patch row: one halo pixel each side
+constexpr int PATCH_PIX = 3 * PATCH_W;  // pixels per half-plane
+constexpr int PATCH_BYTES = 2 * PATCH_PIX * 16;
+constexpr int CONV_THREADS = 128;
+
+__host__ __device__ constexpr int conv_smem_bytes(int cout) { return PATCH_BYTES + 288 * cout + 16; }
+
+template <int COUT>
+__global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __nv_bfloat16 *__restrict__ in, int H, int W,
+                                                             int CIN, const uint4 *__restrict__ wpack,
+                                                             const float *__restrict__ bias,
+                                                             __nv_bfloat16 *__restrict__ out,
+                                                             float *__restrict__ out32, int relu, int *err) {
+    extern __shared__ __align__(128) uint8_t sm[];
+    uint4 *patch = reinterpret_cast<uint4 *>(sm);                // [2][PATCH_PIX]
+    uint4 *wsm = reinterpret_cast<uint4 *>(sm + PATCH_BYTES);    // [9][2][COUT]
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + PATCH_BYTES + 288 * COUT);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * CT_PIX, y = blockIdx.y, img = blockIdx.z;
+    const __nv_bfloat16 *inb = in + (size_t)img * H * W * CIN;
+    constexpr uint32_t NCOL = COUT < 32 ? 32 : COUT;
+    constexpr uint32_t IDESC = umma_idesc_bf16(128, COUT);
+    if (warp == 0) {
+        tmem_alloc(tslot, NCOL);
+        tmem_relinquish();
+    }
+    if (tid == 0) mbar_init(bar, 1);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const int nkc = CIN / 16;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int kc = 0; kc < nkc && ok; kc++) {
+        for (int t = tid; t < 2 * PATCH_PIX; t += CONV_THREADS) {
+            const int h = t / PATCH_PIX, q = t % PATCH_PIX, r = q / PATCH_W, c = q % PATCH_W;
+            const int yy = y - 1 + r, xx = x0 - 1 + c;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (yy >= 0 && yy < H && xx >= 0 && xx < W)
+                v = *reinterpret_cast<const uint4 *>(inb + ((size_t)yy * W + xx) * CIN + kc * 16 + h * 8);
+            patch[t] = v;
+        }
+        const uint4 *wk = wpack + (size_t)kc * 9 * 2 * COUT;
+        for (int t = tid; t < 9 * 2 * COUT; t += CONV_THREADS) wsm[t] = wk[t];
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t pa = smem_u32(patch), pw = smem_u32(wsm);
+            for (int tap = 0; tap < 9; tap++) {
+                const int dy = tap / 3, dx = tap % 3;
+                const uint64_t ad = umma_desc_k(pa + (uint32_t)(dy * PATCH_W + dx) * 16u, PATCH_PIX * 16u, 128u);
+                const uint64_t bd = umma_desc_k(pw + (uint32_t)tap * 2u * COUT * 16u, COUT * 16u, 128u);
+                umma_bf16(tmem, ad, bd, IDESC, (kc > 0 || tap > 0) ? 1u : 0u);
+            }
+            umma_commit(bar);
+        }
+        ok = mbar_wait(bar, phase, err, 1);
+        phase ^= 1u;
+        tc_fence_after();
+        __syncthreads();  // the next chunk overwrites shared memory only after every MMA has read it
+    }
+    if (ok) {
+        const int x = x0 + warp * 32 + lane;
+        const size_t pix = (size_t)img * H * W + (size_t)y * W + x;
+#pragma unroll
+        for (int c0 = 0; c0 < COUT; c0 += 16) {
+            uint32_t r[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
+            tmem_wait_ld();
+            if (x < W) {
+                float v[16];
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    v[i] = __uint_as_float(r[i]) + bias[c0 + i];
+                    if (relu) v[i] = fmaxf(v[i], 0.0f);
+                }
+                if (out) {
+                    uint32_t w[8];
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+                        w[i] = *reinterpret_cast<const uint32_t *>(&b2);
+                    }
+                    uint4 *o = reinterpret_cast<uint4 *>(out + pix * COUT + c0);
+                    o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                    o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                }
+                if (out32 && c0 == 0) out32[pix] = v[0];
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, NCOL);
+}
+
+// w[co][ci][3][3] (FP32, cout x cin real channels) -> wpack[kc][tap][half][co][8]
+// (BF16, padded to cout_pad x cin_pad with zeros).
+__global__ void k_pack_conv(const float *__restrict__ w, int cout, int cin, int cout_pad, int cin_pad,
+                            __nv_bfloat16 *__restrict__ wpack) {
+    const int64_t n = (int64_t)cin_pad * 9 * cout_pad;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        // e enumerates (kc, tap, half, co, j) with ci = kc*16 + half*8 + j
+        const int j = (int)(e % 8);
+        int64_t r = e / 8;
+        const int co = (int)(r % cout_pad);
+        r /= cout_pad;
+        const int half = (int)(r % 2);
+        r /= 2;
+        const int tap = (int)(r % 9);
+        const int kc = (int)(r / 9);
+        const int ci = kc * 16 + half * 8 + j;
+        float v = 0.0f;
+        if (co < cout && ci < cin) v = w[(((size_t)co * cin + ci) * 3 + tap / 3) * 3 + tap % 3];
+        wpack[e] = __float2bfloat16_rn(v);
+    }
+}
+
+template <int COUT> bool conv_prepare() {
+    static bool done = false;
+    if (!done)
+        done = cudaFuncSetAttribute(k_conv3x3_tc<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    conv_smem_bytes(COUT)) == cudaSuccess;
+    return done;
+}
+
+template <int COUT>
+int conv_launch(const void *in, int n, int h, int w, int cin, const void *wpack, const float *bias, void *out,
+                float *out32, int relu, int *err, cudaStream_t st) {
+    if (!conv_prepare<COUT>()) return ASD2G_E_CUDA;
+    const dim3 grid((w + CT_PIX - 1) / CT_PIX, h, n);
+    k_conv3x3_tc<COUT><<<grid, CONV_THREADS, conv_smem_bytes(COUT), st>>>(
+        (const __nv_bfloat16 *)in, h, w, cin, (const uint4 *)wpack, bias, (__nv_bfloat16 *)out, out32, relu, err);
+    return cudaGetLastError() == cudaSuccess ? ASD2G_OK : ASD2G_E_CUDA;
+}
+
+}  // namespace
+
+int conv3x3_tc(const void *in, int n, int h, int w, int cin, const void *wpack, const float *bias, int cout,
+               void *out, float *out32, int relu, int *err, cudaStream_t st) {
+    switch (cout) {
+    case 16: return conv_launch<16>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    case 32: return conv_launch<32>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    case 64: return conv_launch<64>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    case 128: return conv_launch<128>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    default: return ASD2G_E_ARG;
+    }
+}
+
+}  // namespace asd2g
+
+using namespace asd2g;
+
+extern "C" {
+
+size_t asd2g_conv_wpack_bytes(int cout_pad, int cin_pad) { return (size_t)cout_pad * cin_pad * 9 * 2; }
+
+int asd2g_conv_pack_weights(const float *w, int cout, int cin, int cout_pad, int cin_pad, void *wpack, void *stream) {
+    if (!w || !wpack || cout < 1 || cin < 1 || cout > cout_pad || cin > cin_pad || cin_pad % 16 ||
+        (cout_pad != 16 && cout_pad != 32 && cout_pad != 64 && cout_pad != 128))
+        return ASD2G_E_ARG;
+    const int64_t n = (int64_t)cin_pad * 9 * cout_pad;
+    k_pack_conv<<<(int)((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184), 256, 0, (cudaStream_t)stream>>>(
+        w, cout, cin, cout_pad, cin_pad, (__nv_bfloat16 *)wpack);
+    return cudaGetLastError() == cudaSuccess ? ASD2G_OK : ASD2G_E_CUDA;
+}
+
+int asd2g_conv3x3_bf16(const void *in, int n, int h, int w, int cin, const void *wpack, const float *bias, int cout,
+                       void *out, float *out32, int relu, int *err, void *stream) {
+    if (!in || !wpack || !bias || (!out && !out32) || n < 1 || h < 1 || w < 1 || cin < 16 || cin % 16)
+        return ASD2G_E_ARG;
+    return conv3x3_tc(in, n, h, w, cin, wpack, bias, cout, out, out32, relu, err, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -271,6 +271,18 @@ int asd2g_batch_assemble(asd2g_batch *b, const double *dt);
 int asd2g_batch_solve(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_resid);
 int asd2g_batch_sync(asd2g_batch *b);
 
+/* ---- learned preconditioner building blocks (no reference counterpart) ----
+ * 3x3 "same" convolution on the tcgen05 tensor cores: BF16 NHWC activations
+ * (cin a multiple of 16), BF16 packed weights, FP32 accumulation, FP32 bias,
+ * optional ReLU; out: BF16 NHWC with cout channels (16, 32, 64 or 128), out32:
+ * channel 0 in FP32 (either may be NULL).  All pointers are device memory;
+ * err (device int, may be NULL) is set if a tensor-core wait timed out. */
+size_t asd2g_conv_wpack_bytes(int cout_pad, int cin_pad);
+/* w[cout][cin][3][3] FP32 (device) -> packed BF16 weights, zero-padded. */
+int asd2g_conv_pack_weights(const float *w, int cout, int cin, int cout_pad, int cin_pad, void *wpack, void *stream);
+int asd2g_conv3x3_bf16(const void *in, int n, int h, int w, int cin, const void *wpack, const float *bias, int cout,
+                       void *out, float *out32, int relu, int *err, void *stream);
+
 /* ---- whole step (test_mac2d_large.cpp:496-552) ----
  * lsB = LS; advect; reinit (reinit_mode); kappa; H, HS; intermediate velocity
  * with HS; U/V fill; divergence; GFM assembly; pressure solve; projection;
