@@ -67,6 +67,9 @@ EXPORTS = [
     "asd2g_batch_create", "asd2g_batch_destroy", "asd2g_batch_upload", "asd2g_batch_download",
     "asd2g_batch_field_ptr", "asd2g_batch_offset", "asd2g_batch_assemble", "asd2g_batch_solve", "asd2g_batch_sync",
     "asd2g_conv_wpack_bytes", "asd2g_conv_pack_weights", "asd2g_conv3x3_bf16",
+    "asd2g_unet_create", "asd2g_unet_destroy", "asd2g_unet_nparams", "asd2g_unet_init", "asd2g_unet_set_params",
+    "asd2g_unet_get_params", "asd2g_unet_get_grads", "asd2g_unet_forward", "asd2g_unet_train_step",
+    "asd2g_unet_error_flag",
 ]
 
 _lib = None
@@ -83,6 +86,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     S = C.c_void_p
     dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
     ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+    fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
     I, D = C.c_int, C.c_double
     sig = {
         "asd2g_version": ([], I), "asd2g_last_error": ([], C.c_char_p),
@@ -123,6 +127,13 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_conv_pack_weights": ([C.c_void_p, I, I, I, I, C.c_void_p, C.c_void_p], I),
         "asd2g_conv3x3_bf16": ([C.c_void_p, I, I, I, I, C.c_void_p, C.c_void_p, I, C.c_void_p, C.c_void_p, I,
                                 C.c_void_p, C.c_void_p], I),
+        "asd2g_unet_create": ([I, I, I, C.c_void_p, C.POINTER(S)], I), "asd2g_unet_destroy": ([S], I),
+        "asd2g_unet_nparams": ([S], C.c_size_t), "asd2g_unet_init": ([S, C.c_ulonglong], I),
+        "asd2g_unet_set_params": ([S, fp], I), "asd2g_unet_get_params": ([S, fp], I),
+        "asd2g_unet_get_grads": ([S, fp], I),
+        "asd2g_unet_forward": ([S, I, I, I, C.c_void_p, C.c_void_p], I),
+        "asd2g_unet_train_step": ([S, I, I, I, C.c_void_p, C.c_void_p, C.c_float, C.POINTER(C.c_float)], I),
+        "asd2g_unet_error_flag": ([S, C.POINTER(I)], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -429,4 +440,84 @@ class Batch:
 
     def sync(self):
         self._check(self.L.asd2g_batch_sync(self.h))
+
+
+UNET_LAYERS = [(4, 16, 1), (16, 16, 1), (16, 32, 1), (32, 32, 1), (32, 64, 1), (64, 64, 1), (64, 128, 1),
+               (128, 128, 1), (192, 64, 1), (64, 64, 1), (96, 32, 1), (32, 32, 1), (48, 16, 1), (16, 16, 1),
+               (16, 1, 0)]
+
+
+class UNet:
+    """The learned preconditioner network (asd2g_unet_*).  Inputs and outputs
+    are device tensors (torch CUDA tensors or raw device pointers)."""
+
+    def __init__(self, max_batch, max_h, max_w, stream: int | None = None):
+        self.L = load()
+        h = C.c_void_p()
+        rc = self.L.asd2g_unet_create(max_batch, max_h, max_w, C.c_void_p(stream) if stream else None, C.byref(h))
+        self._check(rc)
+        self.h = h
+        self.n = int(self.L.asd2g_unet_nparams(self.h))
+
+    def _check(self, rc):
+        if rc < 0:
+            raise Asd2gError(rc, self.L.asd2g_last_error().decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.asd2g_unet_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _ptr(t):
+        return C.c_void_p(t if isinstance(t, int) else t.data_ptr())
+
+    def init(self, seed=0):
+        self._check(self.L.asd2g_unet_init(self.h, seed))
+
+    def params(self):
+        a = np.zeros(self.n, np.float32)
+        self._check(self.L.asd2g_unet_get_params(self.h, a))
+        return a
+
+    def set_params(self, a):
+        self._check(self.L.asd2g_unet_set_params(self.h, np.ascontiguousarray(a, dtype=np.float32)))
+
+    def grads(self):
+        a = np.zeros(self.n, np.float32)
+        self._check(self.L.asd2g_unet_get_grads(self.h, a))
+        return a
+
+    def forward(self, feats, out, B, H, W):
+        self._check(self.L.asd2g_unet_forward(self.h, B, H, W, self._ptr(feats), self._ptr(out)))
+
+    def train_step(self, feats, target, B, H, W, lr):
+        loss = C.c_float()
+        self._check(self.L.asd2g_unet_train_step(self.h, B, H, W, self._ptr(feats), self._ptr(target), lr,
+                                                 C.byref(loss)))
+        return loss.value
+
+    def error_flag(self):
+        f = C.c_int()
+        self._check(self.L.asd2g_unet_error_flag(self.h, C.byref(f)))
+        return f.value
+
+    @staticmethod
+    def layout():
+        """(w_offset, b_offset, cin, cout, relu) of each layer in the flat parameter vector."""
+        out, off = [], 0
+        for cin, cout, relu in UNET_LAYERS:
+            wo = off
+            off += cout * cin * 9
+            bo = off
+            off += (cout + 15) // 16 * 16
+            out.append((wo, bo, cin, cout, relu))
+        return out, off
 

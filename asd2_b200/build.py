@@ -35,6 +35,7 @@ UNITS = {
     "levelset32.cu": [],
     "batch.cu": [],
     "unet.cu": [],
+    "unet_net.cu": [],
 }
 
 

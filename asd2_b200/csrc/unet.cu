@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __nv_bfloat16
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int x0 = blockIdx.x * CT_PIX, y = blockIdx.y, img = blockIdx.z;
     const __nv_bfloat16 *inb = in + (size_t)img * H * W * CIN;
-    constexpr uint32_t NCOL = COUT < 32 ? 32 : COUT;
+    constexpr uint32_t NCOL = COUT <= 32 ? 32 : COUT <= 64 ? 64 : COUT <= 128 ? 128 : 256;  // power of two
     constexpr uint32_t IDESC = umma_idesc_bf16(128, COUT);
     if (warp == 0) {
         tmem_alloc(tslot, NCOL);
@@ -167,13 +167,18 @@ int conv_launch(const void *in, int n, int h, int w, int cin, const void *wpack,
 
 }  // namespace
 
+bool conv_cout_ok(int c) { return c == 16 || c == 32 || c == 48 || c == 64 || c == 96 || c == 128 || c == 192; }
+
 int conv3x3_tc(const void *in, int n, int h, int w, int cin, const void *wpack, const float *bias, int cout,
                void *out, float *out32, int relu, int *err, cudaStream_t st) {
     switch (cout) {
     case 16: return conv_launch<16>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
     case 32: return conv_launch<32>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    case 48: return conv_launch<48>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
     case 64: return conv_launch<64>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    case 96: return conv_launch<96>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
     case 128: return conv_launch<128>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    case 192: return conv_launch<192>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
     default: return ASD2G_E_ARG;
     }
 }
@@ -188,7 +193,7 @@ size_t asd2g_conv_wpack_bytes(int cout_pad, int cin_pad) { return (size_t)cout_p
 
 int asd2g_conv_pack_weights(const float *w, int cout, int cin, int cout_pad, int cin_pad, void *wpack, void *stream) {
     if (!w || !wpack || cout < 1 || cin < 1 || cout > cout_pad || cin > cin_pad || cin_pad % 16 ||
-        (cout_pad != 16 && cout_pad != 32 && cout_pad != 64 && cout_pad != 128))
+        !conv_cout_ok(cout_pad))
         return ASD2G_E_ARG;
     const int64_t n = (int64_t)cin_pad * 9 * cout_pad;
     k_pack_conv<<<(int)((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184), 256, 0, (cudaStream_t)stream>>>(

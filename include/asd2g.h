@@ -274,7 +274,8 @@ int asd2g_batch_sync(asd2g_batch *b);
 /* ---- learned preconditioner building blocks (no reference counterpart) ----
  * 3x3 "same" convolution on the tcgen05 tensor cores: BF16 NHWC activations
  * (cin a multiple of 16), BF16 packed weights, FP32 accumulation, FP32 bias,
- * optional ReLU; out: BF16 NHWC with cout channels (16, 32, 64 or 128), out32:
+ * optional ReLU; out: BF16 NHWC with cout channels (16, 32, 48, 64, 96, 128 or
+ * 192), out32:
  * channel 0 in FP32 (either may be NULL).  All pointers are device memory;
  * err (device int, may be NULL) is set if a tensor-core wait timed out. */
 size_t asd2g_conv_wpack_bytes(int cout_pad, int cin_pad);
@@ -282,6 +283,31 @@ size_t asd2g_conv_wpack_bytes(int cout_pad, int cin_pad);
 int asd2g_conv_pack_weights(const float *w, int cout, int cin, int cout_pad, int cin_pad, void *wpack, void *stream);
 int asd2g_conv3x3_bf16(const void *in, int n, int h, int w, int cin, const void *wpack, const float *bias, int cout,
                        void *out, float *out32, int relu, int *err, void *stream);
+
+/* ---- the learned preconditioner (no reference counterpart) ----
+ * A 4-level U-Net (16/32/64/128 channels, 15 3x3 convolutions, ReLU, 2x2
+ * average pooling, nearest upsampling + skip concatenation); forward and
+ * input-gradient convolutions on the tcgen05 tensor cores (BF16, FP32
+ * accumulation), weight gradients in FP32, Adam on FP32 master weights.
+ * Images: H x W, both multiples of 8, up to the sizes given at creation.
+ * feats: device FP32 [B][H][W][4] (vector / RMS, diag / s, ce / s, cn / s);
+ * out and target: device FP32 [B][H][W]. */
+typedef struct asd2g_unet asd2g_unet;
+int asd2g_unet_create(int max_batch, int max_h, int max_w, void *stream, asd2g_unet **out);
+int asd2g_unet_destroy(asd2g_unet *u);
+size_t asd2g_unet_nparams(asd2g_unet *u);
+int asd2g_unet_init(asd2g_unet *u, unsigned long long seed);
+/* FP32 host arrays of asd2g_unet_nparams() values (layer by layer: W[cout][cin][3][3], b[cout padded to 16]). */
+int asd2g_unet_set_params(asd2g_unet *u, const float *host);
+int asd2g_unet_get_params(asd2g_unet *u, float *host);
+/* Gradients of the last train step (same layout). */
+int asd2g_unet_get_grads(asd2g_unet *u, float *host);
+int asd2g_unet_forward(asd2g_unet *u, int B, int H, int W, const float *feats, float *out);
+/* One Adam step; *loss_mean = mean over the batch of |out - target|^2 / |target|^2 (may be NULL). */
+int asd2g_unet_train_step(asd2g_unet *u, int B, int H, int W, const float *feats, const float *target, float lr,
+                          float *loss_mean);
+/* 1 if a tensor-core wait of any launch so far timed out. */
+int asd2g_unet_error_flag(asd2g_unet *u, int *flag);
 
 /* ---- whole step (test_mac2d_large.cpp:496-552) ----
  * lsB = LS; advect; reinit (reinit_mode); kappa; H, HS; intermediate velocity

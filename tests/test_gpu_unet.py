@@ -7,6 +7,8 @@ the FP32 reference to 1e-5 relative to the output scale (only the summation
 order differs); the BF16 output to BF16 rounding (2^-8 relative)."""
 import ctypes as C
 
+import numpy as np
+
 import pytest
 import torch
 import torch.nn.functional as F
@@ -29,7 +31,8 @@ def pack_weights(L, w, cout_pad, cin_pad, stream):
 
 @pytest.mark.parametrize("n,h,w,cin,cout,relu", [(1, 8, 128, 16, 16, 0), (2, 20, 200, 16, 32, 1),
                                                  (1, 16, 64, 32, 64, 1), (1, 12, 40, 128, 128, 0),
-                                                 (1, 9, 300, 64, 16, 1)])
+                                                 (1, 9, 300, 64, 16, 1), (1, 8, 96, 16, 48, 0),
+                                                 (1, 8, 136, 32, 96, 1), (1, 6, 64, 48, 192, 0)])
 def test_conv3x3_tensor_core(n, h, w, cin, cout, relu):
     L = api.load()
     torch.manual_seed(1)
@@ -53,3 +56,107 @@ def test_conv3x3_tensor_core(n, h, w, cin, cout, relu):
     scale = ref.abs().max().item()
     assert (out32 - ref[..., 0]).abs().max().item() <= 1e-5 * scale
     assert (out.float() - ref).abs().max().item() <= 2 ** -7 * scale
+
+
+# ------------------------------------------------------------------ U-Net --
+def torch_unet(p, x):
+    """The same network in PyTorch FP32 (NCHW), from the flat parameter vector."""
+    lay, _ = api.UNet.layout()
+
+    def conv(i, t):
+        wo, bo, cin, cout, relu = lay[i]
+        w = torch.from_numpy(p[wo:wo + cout * cin * 9]).view(cout, cin, 3, 3).cuda()
+        b = torch.from_numpy(p[bo:bo + cout]).cuda()
+        y = F.conv2d(t, w, b, padding=1)
+        return torch.relu(y) if relu else y
+    t = x.permute(0, 3, 1, 2)
+    e = []
+    for lv in range(4):
+        ee = conv(2 * lv + 1, conv(2 * lv, t))
+        e.append(ee)
+        if lv < 3:
+            t = F.avg_pool2d(ee, 2)
+    low = e[3]
+    for lv in (2, 1, 0):
+        c = torch.cat([F.interpolate(low, scale_factor=2, mode="nearest"), e[lv]], 1)
+        li = 8 + 2 * (2 - lv)
+        low = conv(li + 1, conv(li, c))
+    return conv(14, low)[:, 0]
+
+
+def _unet_inputs(B, H, W, seed=0):
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    feats = torch.rand(B, H, W, 4, device="cuda", generator=g)
+    feats[..., 0] = torch.randn(B, H, W, device="cuda", generator=g)
+    return feats.contiguous()
+
+
+def test_unet_forward_matches_fp32_reference():
+    B, H, W = 2, 32, 64
+    net = api.UNet(B, H, W)
+    net.init(seed=3)
+    p = net.params()
+    feats = _unet_inputs(B, H, W)
+    out = torch.empty(B, H, W, device="cuda")
+    net.forward(feats, out, B, H, W)
+    torch.cuda.synchronize()
+    assert net.error_flag() == 0
+    ref = torch_unet(p, feats)
+    rel = ((out - ref).norm() / ref.norm()).item()
+    assert rel < 3e-2, rel  # BF16 activations through 15 layers
+
+
+def test_unet_gradients_match_autograd():
+    B, H, W = 2, 32, 32
+    net = api.UNet(B, H, W)
+    net.init(seed=5)
+    p = net.params()
+    feats = _unet_inputs(B, H, W, seed=1)
+    target = torch.randn(B, H, W, device="cuda")
+    net.train_step(feats, target, B, H, W, lr=0.0)  # gradients of this batch, weights unchanged
+    torch.cuda.synchronize()
+    g = net.grads()
+    assert net.error_flag() == 0
+    pt = torch.from_numpy(p).cuda().requires_grad_(True)
+
+    lay, _ = api.UNet.layout()
+
+    def conv(i, t):
+        wo, bo, cin, cout, relu = lay[i]
+        y = F.conv2d(t, pt[wo:wo + cout * cin * 9].view(cout, cin, 3, 3), pt[bo:bo + cout], padding=1)
+        return torch.relu(y) if relu else y
+    t = feats.permute(0, 3, 1, 2)
+    e = []
+    for lv in range(4):
+        ee = conv(2 * lv + 1, conv(2 * lv, t))
+        e.append(ee)
+        if lv < 3:
+            t = F.avg_pool2d(ee, 2)
+    low = e[3]
+    for lv in (2, 1, 0):
+        c = torch.cat([F.interpolate(low, scale_factor=2, mode="nearest"), e[lv]], 1)
+        li = 8 + 2 * (2 - lv)
+        low = conv(li + 1, conv(li, c))
+    out = conv(14, low)[:, 0]
+    loss = (((out - target) ** 2).sum((1, 2)) / (target ** 2).sum((1, 2))).mean()
+    loss.backward()
+    gref = pt.grad.cpu().numpy()
+    for i, (wo, bo, cin, cout, relu) in enumerate(lay):
+        a, r = g[wo:wo + cout * cin * 9], gref[wo:wo + cout * cin * 9]
+        cos = float((a * r).sum() / (np.linalg.norm(a) * np.linalg.norm(r) + 1e-30))
+        assert cos > 0.98, (i, cos)
+        assert 0.85 < np.linalg.norm(a) / np.linalg.norm(r) < 1.15, (i, np.linalg.norm(a) / np.linalg.norm(r))
+
+
+def test_unet_training_reduces_loss():
+    B, H, W = 4, 32, 32
+    net = api.UNet(B, H, W)
+    net.init(seed=7)
+    feats = _unet_inputs(B, H, W, seed=2)
+    target = F.avg_pool2d(feats[..., 0].unsqueeze(1), 3, 1, 1).squeeze(1).contiguous()  # a smooth map of the input
+    first = net.train_step(feats, target, B, H, W, lr=2e-3)
+    last = first
+    for _ in range(60):
+        last = net.train_step(feats, target, B, H, W, lr=2e-3)
+    assert net.error_flag() == 0
+    assert last < 0.5 * first, (first, last)
