@@ -28,7 +28,7 @@ FIELDS = dict(ls=LS, u=U, v=V, ps=PS, p=P, kappa=KAPPA, H=H, HS=HS, div=DIV, uha
 # reinit modes
 REINIT_ORIGINAL, REINIT_SUSSMAN, REINIT_MINRK2, REINIT_FIRSTTIME, REINIT_MINRK2_SUSSMAN = range(5)
 # solvers
-PCG, PCG_REFERENCE, BICGSTAB, BICGSTAB_REFERENCE, MGPCG = range(5)
+PCG, PCG_REFERENCE, BICGSTAB, BICGSTAB_REFERENCE, MGPCG, UNET = range(6)
 NOT_CONVERGED = 1
 FLAG_NO_CLUSTER_PCG = 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
@@ -69,7 +69,8 @@ EXPORTS = [
     "asd2g_conv_wpack_bytes", "asd2g_conv_pack_weights", "asd2g_conv3x3_bf16",
     "asd2g_unet_create", "asd2g_unet_destroy", "asd2g_unet_nparams", "asd2g_unet_init", "asd2g_unet_set_params",
     "asd2g_unet_get_params", "asd2g_unet_get_grads", "asd2g_unet_forward", "asd2g_unet_train_step",
-    "asd2g_unet_error_flag",
+    "asd2g_unet_error_flag", "asd2g_unet_set_stream", "asd2g_set_preconditioner_net", "asd2g_last_fallback",
+    "asd2g_pc_training_pair",
 ]
 
 _lib = None
@@ -133,7 +134,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_unet_get_grads": ([S, fp], I),
         "asd2g_unet_forward": ([S, I, I, I, C.c_void_p, C.c_void_p], I),
         "asd2g_unet_train_step": ([S, I, I, I, C.c_void_p, C.c_void_p, C.c_float, C.POINTER(C.c_float)], I),
-        "asd2g_unet_error_flag": ([S, C.POINTER(I)], I),
+        "asd2g_unet_error_flag": ([S, C.POINTER(I)], I), "asd2g_unet_set_stream": ([S, C.c_void_p], I),
+        "asd2g_set_preconditioner_net": ([S, S], I), "asd2g_last_fallback": ([S, C.POINTER(I)], I),
+        "asd2g_pc_training_pair": ([S, C.c_void_p, C.c_void_p], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -369,6 +372,20 @@ class Session:
         rc = self._check(self.L.asd2g_droplet_step(self.h, C.byref(d), reinit_mode, solver, tol, maxit,
                                                    C.byref(it), C.byref(res)))
         return dict(status=rc, dt_next=d.value, iters=it.value, resid=res.value)
+
+    def set_preconditioner_net(self, net):
+        self._check(self.L.asd2g_set_preconditioner_net(self.h, net.h if net is not None else None))
+        self._pc_net = net  # the session refers to it: keep it alive while attached
+
+    def last_fallback(self) -> int:
+        f = C.c_int()
+        self._check(self.L.asd2g_last_fallback(self.h, C.byref(f)))
+        return f.value
+
+    def training_pair(self, feats, target):
+        """Features and unit-RMS solution of the last solved system into device tensors."""
+        self._check(self.L.asd2g_pc_training_pair(self.h, C.c_void_p(feats.data_ptr()),
+                                                  C.c_void_p(target.data_ptr())))
 
     def volume(self):
         """FP64 (sum H dx dy, sum HS dx dy) of the current level set."""

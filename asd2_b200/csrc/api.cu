@@ -166,7 +166,11 @@ struct asd2g_session {
     double *dsc = nullptr;       // [0] dt of the step, [1] next dt, [2..3] residual sums, [4] counter
     double *dsc_host = nullptr;  // pinned mirror
     bool assembled = false;
-    cudaGraphExec_t chunk_exec[5] = {};
+    cudaGraphExec_t chunk_exec[6] = {};
+    // learned preconditioner (ASD2G_SOLVER_UNET): network, features, output, scale
+    asd2g_unet *pc_net = nullptr;
+    float *pc_feats = nullptr, *pc_out = nullptr, *pc_scal = nullptr;
+    int last_fallback = 0;
     // multigrid preconditioner (allocated on first use)
     MgLevel lv[MG_MAX_LEVELS] = {};
     int nlev = 0;
@@ -353,6 +357,7 @@ int asd2g_create(const asd2g_params *p, void *stream, asd2g_session **out) {
 }
 
 int asd2g_destroy(asd2g_session *s) {
+    if (s && s->pc_net) asd2g_unet_set_stream(s->pc_net, nullptr);  // it must not keep this session's stream
     if (!s) return ASD2G_OK;
     if (s->st) cudaStreamSynchronize(s->st);
     for (auto &e : s->chunk_exec)
@@ -792,15 +797,145 @@ static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters
     return conv ? ASD2G_OK : ASD2G_NOT_CONVERGED;
 }
 
+// ---- flexible CG preconditioned by the learned network (ASD2G_SOLVER_UNET) ----
+// One preconditioner application: features of r, the network, z and beta.
+static int pc_apply(asd2g_session *s) {
+    const Grid &g = s->g;
+    launch_pc_features(s->sys, g.nx, g.ny, s->r, s->ks, s->pc_scal, s->pc_feats, s->st);
+    const int rc = asd2g_unet_forward(s->pc_net, 1, g.nx, g.ny, s->pc_feats, s->pc_out);
+    if (rc) return rc;
+    launch_pc_apply(g.nx, g.ny, s->pc_out, s->pc_scal, s->r, s->q, s->z, s->sys.pinned, s->ks, s->partial, s->st);
+    return cuda_check("learned preconditioner");
+}
+
+constexpr int PC_CHUNK = 4;
+constexpr int PC_MAX_ITERS = 500;  // iterations of the learned phase before the Jacobi-PCG fallback
+
+static int pc_chunk(asd2g_session *s) {
+    const Grid &g = s->g;
+    for (int k = 0; k < PC_CHUNK; k++) {
+        const double *po = k % 2 == 0 ? s->pa : s->pb;
+        double *pn = k % 2 == 0 ? s->pb : s->pa;
+        launch_fcg_pc_ab(s->sys, g.nx, g.ny, s->x, s->r, po, pn, s->q, s->z, s->ks, s->partial, s->st);
+        const int rc = pc_apply(s);
+        if (rc) return rc;
+    }
+    launch_fcg_pc_replace(s->sys, g.nx, g.ny, s->x, s->r, s->ks, s->partial, s->st);
+    return pc_apply(s);
+}
+
+static int solve_learned(asd2g_session *s, double tol, int maxit, int *iters, double *resid) {
+    const Grid &g = s->g;
+    if (!s->pc_net) return fail(ASD2G_E_ARG, "no preconditioner network attached (asd2g_set_preconditioner_net)");
+    int rc = mg_alloc(s);  // the FCG vector z lives with the multigrid buffers
+    if (rc) return rc;
+    rc = asd2g_unet_set_stream(s->pc_net, s->st);
+    if (rc) return rc;
+    const int cap = maxit < PC_MAX_ITERS ? maxit : PC_MAX_ITERS;
+    launch_set_kstate(s->ks, tol, cap, ASD2G_SOLVER_MGPCG, 0.0, s->st);
+    launch_pc_setup(s->sys, g.nx, g.ny, s->pc_feats, s->pc_scal, s->partial, s->counter + 2, s->ks, s->st);
+    launch_fcg_pc_init(s->sys, g.nx, g.ny, s->x, s->r, s->pa, s->q, s->ks, s->partial, s->st);
+    rc = pc_apply(s);
+    if (rc) return rc;
+    if (!s->chunk_exec[ASD2G_SOLVER_UNET]) {
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return cuda_check("capture");
+        const int rc2 = pc_chunk(s);
+        if (cudaStreamEndCapture(s->st, &graph) != cudaSuccess) return cuda_check("capture end");
+        if (rc2) {
+            cudaGraphDestroy(graph);
+            return rc2;
+        }
+        const cudaError_t e = cudaGraphInstantiate(&s->chunk_exec[ASD2G_SOLVER_UNET], graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return cuda_check("graph instantiate");
+    }
+    for (int launched = 0;; launched += PC_CHUNK) {
+        if (cudaGraphLaunch(s->chunk_exec[ASD2G_SOLVER_UNET], s->st) != cudaSuccess) return cuda_check("graph launch");
+        cudaMemcpyAsync(s->ks_host, s->ks, sizeof(KState), cudaMemcpyDeviceToHost, s->st);
+        rc = sync(s);
+        if (rc) return rc;
+        if (s->ks_host->done || launched + PC_CHUNK >= cap) break;
+    }
+    const KState k = *s->ks_host;
+    int unet_flag = 0;
+    asd2g_unet_error_flag(s->pc_net, &unet_flag);
+    if ((k.status == 0 || k.status == 2) && !unet_flag && (!(k.res > tol) || k.status == 2)) {
+        s->last_fallback = 0;
+        if (iters) *iters = k.it;
+        if (resid) *resid = k.res;
+        return ASD2G_OK;
+    }
+    // Jacobi-PCG fallback, judged by the same FP64 residual.
+    s->last_fallback = 1;
+    int it2 = 0;
+    const int st = solve(s, ASD2G_SOLVER_PCG, tol, maxit, &it2, resid);
+    if (iters) *iters = k.it + it2;
+    return st;
+}
+
+int asd2g_set_preconditioner_net(asd2g_session *s, asd2g_unet *net) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    if (net && (s->g.nx % 8 || s->g.ny % 8))
+        return fail(ASD2G_E_UNSUPPORTED, "the learned preconditioner needs nx and ny multiples of 8");
+    if (s->pc_net && s->pc_net != net) asd2g_unet_set_stream(s->pc_net, nullptr);
+    s->pc_net = net;
+    if (net && !s->pc_feats) {
+        float **pp[] = {&s->pc_feats, &s->pc_out};
+        const size_t sizes[] = {4 * s->N, s->N};
+        for (int i = 0; i < 2; i++) {
+            if (cudaMalloc(pp[i], sizeof(float) * sizes[i]) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(ASD2G_E_NOMEM, "preconditioner buffers");
+            }
+            s->allocs.push_back(*pp[i]);
+        }
+    }
+    if (net && !s->pc_scal) {
+        if (cudaMalloc(&s->pc_scal, sizeof(float) * 4) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ASD2G_E_NOMEM, "preconditioner buffers");
+        }
+        s->allocs.push_back(s->pc_scal);
+    }
+    if (s->chunk_exec[ASD2G_SOLVER_UNET]) {  // the captured chunk holds the previous network's launches
+        cudaGraphExecDestroy(s->chunk_exec[ASD2G_SOLVER_UNET]);
+        s->chunk_exec[ASD2G_SOLVER_UNET] = nullptr;
+    }
+    return ASD2G_OK;
+}
+
+int asd2g_last_fallback(asd2g_session *s, int *used) {
+    if (!s || !used) return fail(ASD2G_E_ARG, "null argument");
+    *used = s->last_fallback;
+    return ASD2G_OK;
+}
+
+int asd2g_pc_training_pair(asd2g_session *s, void *feats, void *target) {
+    if (!s || !feats || !target) return fail(ASD2G_E_ARG, "null argument");
+    if (!s->assembled) return fail(ASD2G_E_ARG, "assemble and solve the system first");
+    if (!s->pc_scal) {
+        if (cudaMalloc(&s->pc_scal, sizeof(float) * 4) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ASD2G_E_NOMEM, "scale buffer");
+        }
+        s->allocs.push_back(s->pc_scal);
+    }
+    launch_pc_pair(s->sys, s->g.nx, s->g.ny, s->x, s->ks, s->pc_scal, s->partial, s->counter + 2, (float *)feats,
+                   (float *)target, s->st);
+    return cuda_check("training pair");
+}
+
 int asd2g_solve_pressure(asd2g_session *s, int solver, double tol, int maxit, double dt, int *iters,
                          double *rel_resid) {
     if (!s) return fail(ASD2G_E_ARG, "null session");
-    if (solver < 0 || solver > 4) return fail(ASD2G_E_ARG, "solver %d out of range", solver);
+    if (solver < 0 || solver > ASD2G_SOLVER_UNET) return fail(ASD2G_E_ARG, "solver %d out of range", solver);
     if (!s->assembled) return fail(ASD2G_E_ARG, "assemble the system first");
     if (maxit < 0) return fail(ASD2G_E_ARG, "maxit must be >= 0");
     int rc = set_dt(s, dt);
     if (rc) return rc;
-    const int st = solve(s, solver, tol, maxit, iters, rel_resid);
+    const int st = solver == ASD2G_SOLVER_UNET ? solve_learned(s, tol, maxit, iters, rel_resid)
+                                                : solve(s, solver, tol, maxit, iters, rel_resid);
     if (st < 0) return st;
     launch_scatter_ps(s->g, s->x, s->f[ASD2G_PS], s->f[ASD2G_P], s->dsc, s->st);
     rc = cuda_check("scatter ps");

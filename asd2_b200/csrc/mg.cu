@@ -887,6 +887,104 @@ __global__ void __launch_bounds__(256) k_bmg_post(const BInst *__restrict__ inst
     }
 }
 
+// ------------------------------------------------- learned preconditioner --
+// Flexible CG with the U-Net as preconditioner (the FCG kernels above, the
+// V-cycle replaced by: features of r -> network -> z).  scal[0] = s, the
+// largest diagonal entry (the coefficient scale), set once per assembly.
+
+__global__ void __launch_bounds__(256) k_pc_diag_max(int64_t n, const double *__restrict__ diag, double *partial,
+                                                     unsigned *counter, float *scal) {
+    double v = 0.0;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        v = fmax(v, fabs(diag[k]));
+    __shared__ double sm[256];
+    sm[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
+        __syncthreads();
+    }
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = sm[0];
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    double mx = 0.0;
+    for (unsigned b = 0; b < gridDim.x; b++) mx = fmax(mx, __ldcg(partial + b));
+    scal[0] = (float)(mx > 0.0 ? mx : 1.0);
+    *counter = 0u;
+}
+
+// feats [nx][ny][4]: channel 0 = r / rms(r) (rms from the solver scalars),
+// channels 1..3 = diag, ce, cn over s (written when consts != 0).
+__global__ void k_pc_features(int nx, int ny, Sys S, const double *__restrict__ r, const KState *ks,
+                              const float *__restrict__ scal, float *__restrict__ feats, int consts) {
+    if (ks->done && !consts) return;
+    const int64_t n = (int64_t)nx * ny;
+    const double rms = ks->res * ks->bn / sqrt((double)n);
+    const double inv = (rms > 0.0 && isfinite(rms)) ? 1.0 / rms : 0.0;
+    const float is = 1.0f / scal[0];
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        feats[4 * k] = (float)(r[k] * inv);
+        if (consts) {
+            feats[4 * k + 1] = (float)S.diag[k] * is;
+            feats[4 * k + 2] = (float)S.ce[k] * is;
+            feats[4 * k + 3] = (float)S.cn[k] * is;
+        }
+    }
+}
+
+// z = out * rms / s (FP64; 0 at the pinned cell), then the FCG beta from z.r, z.q.
+__global__ void __launch_bounds__(256) k_pc_apply(int64_t n, const float *__restrict__ out,
+                                                  const float *__restrict__ scal, const double *__restrict__ r,
+                                                  const double *__restrict__ q, double *__restrict__ z, int pinned,
+                                                  KState *ks, double *partial) {
+    if (ks->done) return;
+    const double rms = ks->res * ks->bn / sqrt((double)n), f = rms / (double)scal[0];
+    double acc[2] = {0.0, 0.0};
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const double zk = (pinned && k == 0) ? 0.0 : (double)out[k] * f;
+        z[k] = zk;
+        acc[0] += zk * r[k];
+        acc[1] += zk * q[k];
+    }
+    double tot[2];
+    if (mg_grid_reduce<2>(acc, partial, &ks->counter, tot)) fcg_beta(ks, tot);
+}
+
+// Training pair from an assembled system and its solution x: feats = (b /
+// rms(b), diag / s, ce / s, cn / s), target = x / rms(x).  Flexible CG is
+// invariant to a scalar factor on the preconditioner's output, so the
+// network learns the direction of A^-1 b.  rms(b) from the KState (bn = |b|
+// of the last solve), |x|^2 into scal[2].
+__global__ void __launch_bounds__(256) k_pc_sumsq(int64_t n, const double *__restrict__ x, double *partial,
+                                                  unsigned *counter, float *scal) {
+    double v[1] = {0.0};
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        v[0] += x[k] * x[k];
+    double tot[1];
+    if (mg_grid_reduce<1>(v, partial, counter, tot)) scal[2] = (float)tot[0];
+}
+
+__global__ void k_pc_pair(int nx, int ny, Sys S, const double *__restrict__ x, const KState *ks,
+                          const float *__restrict__ scal, float *__restrict__ feats, float *__restrict__ target) {
+    const int64_t n = (int64_t)nx * ny;
+    const double rms = ks->bn / sqrt((double)n), inv = rms > 0.0 ? 1.0 / rms : 0.0;
+    const double xr = sqrt((double)scal[2] / (double)n), xinv = xr > 0.0 ? 1.0 / xr : 0.0;
+    const float is = 1.0f / scal[0];
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        feats[4 * k] = (float)(S.b[k] * inv);
+        feats[4 * k + 1] = (float)S.diag[k] * is;
+        feats[4 * k + 2] = (float)S.ce[k] * is;
+        feats[4 * k + 3] = (float)S.cn[k] * is;
+        target[k] = (float)(x[k] * xinv);
+    }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ host --
@@ -1065,6 +1163,55 @@ bool launch_batch_fcg_check(const BatchPlan &P, cudaStream_t st) {
     k_bfcg_replace<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks);
     batch_vcycle(P, st);
     return true;
+}
+
+// ------------------------------------------------- learned preconditioner --
+void launch_pc_setup(const Sys &S, int nx, int ny, float *feats, float *scal, double *partial, unsigned *counter,
+                     const KState *ks, cudaStream_t st) {
+    const int64_t n = (int64_t)nx * ny;
+    const int nb = red_blocks(n);
+    k_pc_diag_max<<<nb, 256, 0, st>>>(n, S.diag, partial, counter, scal);
+    k_pc_features<<<nb, 256, 0, st>>>(nx, ny, S, S.b, ks, scal, feats, 1);
+}
+
+void launch_fcg_pc_init(const Sys &S, int nx, int ny, double *x, double *r, double *p, double *q, KState *ks,
+                        double *partial, cudaStream_t st) {
+    const int64_t n = (int64_t)nx * ny;
+    k_fcg_init<<<red_blocks(n), 256, 0, st>>>(n, S, x, r, p, ks, partial);
+    cudaMemsetAsync(q, 0, sizeof(double) * n, st);
+}
+
+void launch_pc_features(const Sys &S, int nx, int ny, const double *r, const KState *ks, const float *scal,
+                        float *feats, cudaStream_t st) {
+    k_pc_features<<<red_blocks((int64_t)nx * ny), 256, 0, st>>>(nx, ny, S, r, ks, scal, feats, 0);
+}
+
+void launch_pc_apply(int nx, int ny, const float *out, const float *scal, const double *r, const double *q, double *z,
+                     int pinned, KState *ks, double *partial, cudaStream_t st) {
+    const int64_t n = (int64_t)nx * ny;
+    k_pc_apply<<<red_blocks(n), 256, 0, st>>>(n, out, scal, r, q, z, pinned, ks, partial);
+}
+
+void launch_fcg_pc_ab(const Sys &S, int nx, int ny, double *x, double *r, const double *p_old, double *p_new,
+                      double *q, const double *z, KState *ks, double *partial, cudaStream_t st) {
+    const int64_t n = (int64_t)nx * ny;
+    const int nb = red_blocks(n);
+    k_fcg_a<<<nb, 256, 0, st>>>(nx, ny, S, z, p_old, p_new, q, ks, partial);
+    k_fcg_b<<<nb, 256, 0, st>>>(n, x, r, p_new, q, ks, partial);
+}
+
+void launch_fcg_pc_replace(const Sys &S, int nx, int ny, const double *x, double *r, KState *ks, double *partial,
+                           cudaStream_t st) {
+    k_fcg_replace<<<red_blocks((int64_t)nx * ny), 256, 0, st>>>(nx, ny, S, x, r, ks, partial);
+}
+
+void launch_pc_pair(const Sys &S, int nx, int ny, const double *x, const KState *ks, float *scal, double *partial,
+                    unsigned *counter, float *feats, float *target, cudaStream_t st) {
+    const int64_t n = (int64_t)nx * ny;
+    const int nb = red_blocks(n);
+    k_pc_diag_max<<<nb, 256, 0, st>>>(n, S.diag, partial, counter, scal);
+    k_pc_sumsq<<<nb, 256, 0, st>>>(n, x, partial, counter, scal);
+    k_pc_pair<<<nb, 256, 0, st>>>(nx, ny, S, x, ks, scal, feats, target);
 }
 
 }  // namespace asd2g

@@ -275,7 +275,9 @@ struct UnetLayer {
 };
 
 struct asd2g_unet {
-    cudaStream_t st = nullptr;
+    cudaStream_t st = nullptr;       // the stream launches go to
+    cudaStream_t own_st = nullptr;   // created here when none was given
+    cudaStream_t home_st = nullptr;  // the creation-time stream (given or own)
     bool own_stream = false;
     int max_b = 0, max_h = 0, max_w = 0;
     std::vector<UnetLayer> L;
@@ -420,7 +422,7 @@ int backward(asd2g_unet *u, int B, int H, int W) {
 void release(asd2g_unet *u) {
     for (void *p : u->allocs) cudaFree(p);
     if (u->loss_host) cudaFreeHost(u->loss_host);
-    if (u->own_stream && u->st) cudaStreamDestroy(u->st);
+    if (u->own_stream && u->own_st) cudaStreamDestroy(u->own_st);
     delete u;
 }
 
@@ -439,12 +441,14 @@ int asd2g_unet_create(int max_batch, int max_h, int max_w, void *stream, asd2g_u
     u->max_w = max_w;
     if (stream) u->st = (cudaStream_t)stream;
     else {
-        if (cudaStreamCreateWithFlags(&u->st, cudaStreamNonBlocking) != cudaSuccess) {
+        if (cudaStreamCreateWithFlags(&u->own_st, cudaStreamNonBlocking) != cudaSuccess) {
             delete u;
             return api_fail(ASD2G_E_CUDA, "cudaStreamCreate failed");
         }
+        u->st = u->own_st;
         u->own_stream = true;
     }
+    u->home_st = u->st;
     size_t off = 0;
     for (int i = 0; i < 15; i++) {
         UnetLayer l;
@@ -590,6 +594,13 @@ int asd2g_unet_train_step(asd2g_unet *u, int B, int H, int W, const float *feats
         *loss_mean = s / (float)B;
     }
     return cuda_ok("train_step");
+}
+
+// NULL returns the network to the stream it was created with.
+int asd2g_unet_set_stream(asd2g_unet *u, void *stream) {
+    if (!u) return api_fail(ASD2G_E_ARG, "null network");
+    u->st = stream ? (cudaStream_t)stream : u->home_st;
+    return ASD2G_OK;
 }
 
 int asd2g_unet_get_grads(asd2g_unet *u, float *host) {

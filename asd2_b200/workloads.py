@@ -116,3 +116,41 @@ def droplet_batch(count: int = 256, seed: int = 0, sides=tuple(range(64, 513, 32
         mr = float(10 ** rng.uniform(0.0, 2.0))
         out.append(droplet(n, seed=int(rng.integers(1 << 31)), rho_ratio=rr, mu_ratio=mr, radius=(0.08, 0.2)))
     return out
+
+
+def multi_droplet(n: int = 256, seed: int = 0, count: int = 3, rho_ratio: float = 1000.0, mu_ratio: float = 100.0,
+                  radius=(0.05, 0.15), sigma: float = 0.0728, g: float = 9.8) -> Case:
+    """Several droplets on [0,1]^2 (no-slip walls, Neumann pressure): phi is
+    the largest of the droplets' signed distances r_k - |x - c_k| (heavy
+    inside any droplet); centres at least a radius plus 0.05 from the walls."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    dx = dy = 1.0 / n
+    X, Y = _centres(n, n, dx, dy)
+    ls = np.full_like(X, -np.inf)
+    drops = []
+    for _ in range(count):
+        r = rng.uniform(*radius)
+        cx, cy = rng.uniform(r + 0.05, 0.95 - r, size=2)
+        ls = np.maximum(ls, r - np.sqrt((X - cx) ** 2 + (Y - cy) ** 2))
+        drops.append((r, cx, cy))
+    u = np.zeros_like(ls)
+    fluid = dict(rho_h=1000.0, rho_l=1000.0 / rho_ratio, mu_h=1.0e-3, mu_l=1.0e-3 / mu_ratio,
+                 sigma=sigma, g=g, g_axis=1, fix_gravity=0, time_order=2, cfl=0.5)
+    return Case(n, n, dx, dy, np.ascontiguousarray(ls), u, u.copy(), bc_u=("dirichlet",) * 4,
+                bc_v=("dirichlet",) * 4, bc_p=("neumann",) * 4, fluid=fluid, meta=dict(seed=seed, drops=drops))
+
+
+def smooth_field(n: int, ny: int, rng, modes: int = 6, amplitude: float = 10.0) -> np.ndarray:
+    """A random smooth padded (n+6) x (ny+6) field: a sum of Fourier modes
+    with random wave numbers up to 2*modes, amplitudes decaying with the
+    wave number."""
+    X = (np.arange(n + 6) - 2.5) / n
+    Y = (np.arange(ny + 6) - 2.5) / ny
+    f = np.zeros((n + 6, ny + 6))
+    for _ in range(modes):
+        kx, ky = rng.integers(1, 2 * modes + 1, size=2)
+        a = amplitude * rng.normal() / np.hypot(kx, ky)
+        px, py = rng.uniform(0, 2 * np.pi, size=2)
+        f += a * np.outer(np.cos(np.pi * kx * X + px), np.cos(np.pi * ky * Y + py))
+    return f
+

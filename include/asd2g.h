@@ -79,7 +79,9 @@ enum asd2g_solver {
     ASD2G_SOLVER_PCG_REFERENCE = 1,/* the reference iteration, poisson2d.cpp:285  */
     ASD2G_SOLVER_BICGSTAB = 2,     /* right-Jacobi BiCGStab (rho_2 carried)       */
     ASD2G_SOLVER_BICGSTAB_REFERENCE = 3, /* poisson2d.cpp:403 as written (rho_2 = 1) */
-    ASD2G_SOLVER_MGPCG = 4         /* FP64 flexible CG preconditioned by an FP32 multigrid V-cycle */
+    ASD2G_SOLVER_MGPCG = 4,        /* FP64 flexible CG preconditioned by an FP32 multigrid V-cycle */
+    ASD2G_SOLVER_UNET = 5          /* FP64 flexible CG preconditioned by the learned network
+                                      (asd2g_set_preconditioner_net), Jacobi-PCG fallback */
 };
 
 /* solver_flags bits */
@@ -308,6 +310,23 @@ int asd2g_unet_train_step(asd2g_unet *u, int B, int H, int W, const float *feats
                           float *loss_mean);
 /* 1 if a tensor-core wait of any launch so far timed out. */
 int asd2g_unet_error_flag(asd2g_unet *u, int *flag);
+/* Run the network's launches on this stream from now on (NULL: the stream it
+ * was created with). */
+int asd2g_unet_set_stream(asd2g_unet *u, void *stream);
+/* Attach (or detach with NULL) the network used by ASD2G_SOLVER_UNET: nx and
+ * ny multiples of 8 and within the network's maximum image size; keep the
+ * network alive while attached.  The solve is flexible CG in FP64 with z =
+ * network(r) (BF16 / FP32 inside), convergence verified on the FP64 residual
+ * as for ASD2G_SOLVER_MGPCG; if it does not converge within min(maxit, 500)
+ * iterations the system is solved again by Jacobi-PCG and
+ * asd2g_last_fallback reports 1. */
+int asd2g_set_preconditioner_net(asd2g_session *s, asd2g_unet *net);
+int asd2g_last_fallback(asd2g_session *s, int *used);
+/* Training pair of the network from the session's last assembled and solved
+ * system: feats (device FP32 [nx][ny][4]) = (b / rms(b), diag / s, ce / s,
+ * cn / s), target (device FP32 [nx][ny]) = x / rms(x), s = max diag (flexible
+ * CG is invariant to a scalar factor on the preconditioner's output). */
+int asd2g_pc_training_pair(asd2g_session *s, void *feats, void *target);
 
 /* ---- whole step (test_mac2d_large.cpp:496-552) ----
  * lsB = LS; advect; reinit (reinit_mode); kappa; H, HS; intermediate velocity
