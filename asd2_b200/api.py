@@ -69,6 +69,7 @@ EXPORTS = [
     "asd2g_conv_wpack_bytes", "asd2g_conv_pack_weights", "asd2g_conv3x3_bf16",
     "asd2g_unet_create", "asd2g_unet_destroy", "asd2g_unet_nparams", "asd2g_unet_init", "asd2g_unet_set_params",
     "asd2g_unet_get_params", "asd2g_unet_get_grads", "asd2g_unet_forward", "asd2g_unet_train_step",
+    "asd2g_unet_train_step_residual", "asd2g_unet_train_step_energy",
     "asd2g_unet_error_flag", "asd2g_unet_set_stream", "asd2g_set_preconditioner_net", "asd2g_last_fallback",
     "asd2g_pc_training_pair",
 ]
@@ -134,6 +135,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_unet_get_grads": ([S, fp], I),
         "asd2g_unet_forward": ([S, I, I, I, C.c_void_p, C.c_void_p], I),
         "asd2g_unet_train_step": ([S, I, I, I, C.c_void_p, C.c_void_p, C.c_float, C.POINTER(C.c_float)], I),
+        "asd2g_unet_train_step_residual": ([S, I, I, I, C.c_void_p, C.c_float, C.POINTER(C.c_float)], I),
+        "asd2g_unet_train_step_energy": ([S, I, I, I, C.c_void_p, C.c_void_p, C.c_float, C.POINTER(C.c_float)],
+                                         I),
         "asd2g_unet_error_flag": ([S, C.POINTER(I)], I), "asd2g_unet_set_stream": ([S, C.c_void_p], I),
         "asd2g_set_preconditioner_net": ([S, S], I), "asd2g_last_fallback": ([S, C.POINTER(I)], I),
         "asd2g_pc_training_pair": ([S, C.c_void_p, C.c_void_p], I),
@@ -519,6 +523,21 @@ class UNet:
         loss = C.c_float()
         self._check(self.L.asd2g_unet_train_step(self.h, B, H, W, self._ptr(feats), self._ptr(target), lr,
                                                  C.byref(loss)))
+        return loss.value
+
+    def train_step_residual(self, feats, B, H, W, lr):
+        """Adam step on the residual loss 1 - cos^2(A out, r) (r = feats[..., 0],
+        A the 5-point operator of feats[..., 1:4]); returns the mean loss."""
+        loss = C.c_float()
+        self._check(self.L.asd2g_unet_train_step_residual(self.h, B, H, W, self._ptr(feats), lr, C.byref(loss)))
+        return loss.value
+
+    def train_step_energy(self, feats, target, B, H, W, lr):
+        """Adam step on the energy loss 1 - (u'At)^2 / ((u'Au)(t'At)) (A the
+        5-point operator of feats[..., 1:4]); returns the mean loss."""
+        loss = C.c_float()
+        self._check(self.L.asd2g_unet_train_step_energy(self.h, B, H, W, self._ptr(feats), self._ptr(target), lr,
+                                                        C.byref(loss)))
         return loss.value
 
     def error_flag(self):

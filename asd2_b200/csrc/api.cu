@@ -797,45 +797,53 @@ static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters
     return conv ? ASD2G_OK : ASD2G_NOT_CONVERGED;
 }
 
-// ---- flexible CG preconditioned by the learned network (ASD2G_SOLVER_UNET) ----
-// One preconditioner application: features of r, the network, z and beta.
-static int pc_apply(asd2g_session *s) {
+// ---- flexible CG with the two-level learned preconditioner (ASD2G_SOLVER_UNET) ----
+// After each V-cycle (which leaves beta alone in this mode): r1 = r - A z_mg,
+// the network on r1's features, omega, z = z_mg + omega u and beta.
+static int pc_correct(asd2g_session *s) {
     const Grid &g = s->g;
-    launch_pc_features(s->sys, g.nx, g.ny, s->r, s->ks, s->pc_scal, s->pc_feats, s->st);
+    launch_pc_input(s->sys, g.nx, g.ny, s->r, s->z, s->rt, s->ks, s->pc_scal, s->pc_feats, s->mg_partial, s->st);
     const int rc = asd2g_unet_forward(s->pc_net, 1, g.nx, g.ny, s->pc_feats, s->pc_out);
     if (rc) return rc;
-    launch_pc_apply(g.nx, g.ny, s->pc_out, s->pc_scal, s->r, s->q, s->z, s->sys.pinned, s->ks, s->partial, s->st);
+    launch_pc_output(s->sys, g.nx, g.ny, s->pc_out, s->rt, s->r, s->q, s->z, s->ks, s->mg_partial, s->st);
     return cuda_check("learned preconditioner");
 }
 
-constexpr int PC_CHUNK = 4;
-constexpr int PC_MAX_ITERS = 500;  // iterations of the learned phase before the Jacobi-PCG fallback
+constexpr int PC_CHUNK = 8;          // iterations per captured chunk; the FP64 residual check closes it
+constexpr int PC_MAX_ITERS = 500;    // iterations of the learned phase before the Jacobi-PCG fallback
 
 static int pc_chunk(asd2g_session *s) {
     const Grid &g = s->g;
     for (int k = 0; k < PC_CHUNK; k++) {
         const double *po = k % 2 == 0 ? s->pa : s->pb;
         double *pn = k % 2 == 0 ? s->pb : s->pa;
-        launch_fcg_pc_ab(s->sys, g.nx, g.ny, s->x, s->r, po, pn, s->q, s->z, s->ks, s->partial, s->st);
-        const int rc = pc_apply(s);
+        if (!launch_fcg_iter(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, po, pn, s->q, s->z, s->ks,
+                             s->mg_partial, s->mg_partial_n, s->st))
+            return fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
+        const int rc = pc_correct(s);
         if (rc) return rc;
     }
-    launch_fcg_pc_replace(s->sys, g.nx, g.ny, s->x, s->r, s->ks, s->partial, s->st);
-    return pc_apply(s);
+    if (!launch_fcg_check(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->q, s->z, s->ks,
+                          s->mg_partial, s->mg_partial_n, s->st))
+        return fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
+    return pc_correct(s);
 }
 
 static int solve_learned(asd2g_session *s, double tol, int maxit, int *iters, double *resid) {
     const Grid &g = s->g;
     if (!s->pc_net) return fail(ASD2G_E_ARG, "no preconditioner network attached (asd2g_set_preconditioner_net)");
-    int rc = mg_alloc(s);  // the FCG vector z lives with the multigrid buffers
+    int rc = mg_alloc(s);
     if (rc) return rc;
     rc = asd2g_unet_set_stream(s->pc_net, s->st);
     if (rc) return rc;
     const int cap = maxit < PC_MAX_ITERS ? maxit : PC_MAX_ITERS;
-    launch_set_kstate(s->ks, tol, cap, ASD2G_SOLVER_MGPCG, 0.0, s->st);
+    launch_set_kstate(s->ks, tol, cap, ASD2G_SOLVER_UNET, 0.0, s->st);
+    launch_mg_setup(s->sys, s->lv, s->nlev, s->coarse_inv, s->st);
     launch_pc_setup(s->sys, g.nx, g.ny, s->pc_feats, s->pc_scal, s->partial, s->counter + 2, s->ks, s->st);
-    launch_fcg_pc_init(s->sys, g.nx, g.ny, s->x, s->r, s->pa, s->q, s->ks, s->partial, s->st);
-    rc = pc_apply(s);
+    if (!launch_fcg_init(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->pa, s->q, s->z, s->ks,
+                         s->mg_partial, s->mg_partial_n, s->st))
+        return fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
+    rc = pc_correct(s);
     if (rc) return rc;
     if (!s->chunk_exec[ASD2G_SOLVER_UNET]) {
         cudaGraph_t graph = nullptr;
@@ -921,8 +929,22 @@ int asd2g_pc_training_pair(asd2g_session *s, void *feats, void *target) {
         }
         s->allocs.push_back(s->pc_scal);
     }
-    launch_pc_pair(s->sys, s->g.nx, s->g.ny, s->x, s->ks, s->pc_scal, s->partial, s->counter + 2, (float *)feats,
-                   (float *)target, s->st);
+    int rc = mg_alloc(s);
+    if (rc) return rc;
+    const Grid &g = s->g;
+    const size_t N = s->N;
+    double *xs = s->t3, *e = s->t3 + N;  // the solution, kept; the V-cycle's error
+    cudaMemcpyAsync(xs, s->x, sizeof(double) * N, cudaMemcpyDeviceToDevice, s->st);
+    launch_set_kstate(s->ks, 0.0, 1, ASD2G_SOLVER_UNET, 0.0, s->st);
+    launch_mg_setup(s->sys, s->lv, s->nlev, s->coarse_inv, s->st);
+    if (!launch_fcg_init(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->pa, s->q, s->z, s->ks,
+                         s->mg_partial, s->mg_partial_n, s->st))
+        return fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
+    // r = b after the init: r1 = b - A V(b), its norm in the solver state
+    launch_pc_input(s->sys, g.nx, g.ny, s->r, s->z, s->rt, s->ks, s->pc_scal, (float *)feats, s->mg_partial, s->st);
+    launch_pc_pair(s->sys, g.nx, g.ny, xs, s->z, s->rt, e, s->ks, s->pc_scal, s->partial, s->counter + 2,
+                   (float *)feats, (float *)target, s->st);
+    cudaMemcpyAsync(s->x, xs, sizeof(double) * N, cudaMemcpyDeviceToDevice, s->st);
     return cuda_check("training pair");
 }
 

@@ -32,6 +32,7 @@ namespace asd2g {
 namespace {
 
 constexpr int MT_I = 16, MT_J = 32;  // tile (rows i, columns j), must be even
+constexpr int KMODE_LEARNED = 5;      // KState mode of ASD2G_SOLVER_UNET (V-cycle + learned correction)
 constexpr int MG_COARSE_MAX = 64;   // cells on the coarsest level
 constexpr int HI = MT_I + 4, HJ = MT_J + 4;
 
@@ -317,7 +318,8 @@ __global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float ome
     mg_post_tile<L0>(L, C, omega, r64, q64, z64, pinned, blockIdx.y * MT_I, blockIdx.x * MT_J, acc);
     if (L0) {
         double tot[2];
-        if (mg_grid_reduce<2>(acc, partial, &ks->counter, tot)) fcg_beta(ks, tot);
+        // in the learned mode the V-cycle's z is only part of the preconditioner: beta comes later
+        if (mg_grid_reduce<2>(acc, partial, &ks->counter, tot) && ks->mode != KMODE_LEARNED) fcg_beta(ks, tot);
     }
 }
 
@@ -888,9 +890,11 @@ __global__ void __launch_bounds__(256) k_bmg_post(const BInst *__restrict__ inst
 }
 
 // ------------------------------------------------- learned preconditioner --
-// Flexible CG with the U-Net as preconditioner (the FCG kernels above, the
-// V-cycle replaced by: features of r -> network -> z).  scal[0] = s, the
-// largest diagonal entry (the coefficient scale), set once per assembly.
+// Two-level preconditioner of ASD2G_SOLVER_UNET: the FP32 V-cycle gives z_mg
+// (the coarse, global part); the network sees what it leaves, r1 = r - A
+// z_mg, and returns u ~ A^-1 r1 up to scale; z = z_mg + omega u with omega
+// minimising the A-norm of the error left along u (FP64).  scal[0] = s = max diag (coefficient
+// scale of the features); |r1| in ks->snorm; omega in ks->omega.
 
 __global__ void __launch_bounds__(256) k_pc_diag_max(int64_t n, const double *__restrict__ diag, double *partial,
                                                      unsigned *counter, float *scal) {
@@ -919,18 +923,34 @@ __global__ void __launch_bounds__(256) k_pc_diag_max(int64_t n, const double *__
     *counter = 0u;
 }
 
-// feats [nx][ny][4]: channel 0 = r / rms(r) (rms from the solver scalars),
-// channels 1..3 = diag, ce, cn over s (written when consts != 0).
-__global__ void k_pc_features(int nx, int ny, Sys S, const double *__restrict__ r, const KState *ks,
+// r1 = r - A z (0 at the pinned row); |r1| -> ks->snorm
+__global__ void __launch_bounds__(256) k_pc_resid(int nx, int ny, Sys S, const double *__restrict__ r,
+                                                  const double *__restrict__ z, double *__restrict__ r1, KState *ks,
+                                                  double *partial) {
+    if (ks->done) return;
+    const int64_t n = (int64_t)nx * ny;
+    double v[1] = {0.0};
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const double rk = (S.pinned && k == 0) ? 0.0 : r[k] - sys_apply(S, nx, ny, z, k);
+        r1[k] = rk;
+        v[0] += rk * rk;
+    }
+    double tot[1];
+    if (mg_grid_reduce<1>(v, partial, &ks->counter, tot)) ks->snorm = sqrt(tot[0]);
+}
+
+// feats [nx][ny][4]: channel 0 = r1 / rms(r1), channels 1..3 = diag, ce, cn
+// over s (written when consts != 0).
+__global__ void k_pc_features(int nx, int ny, Sys S, const double *__restrict__ r1, const KState *ks,
                               const float *__restrict__ scal, float *__restrict__ feats, int consts) {
     if (ks->done && !consts) return;
     const int64_t n = (int64_t)nx * ny;
-    const double rms = ks->res * ks->bn / sqrt((double)n);
+    const double rms = ks->snorm / sqrt((double)n);
     const double inv = (rms > 0.0 && isfinite(rms)) ? 1.0 / rms : 0.0;
     const float is = 1.0f / scal[0];
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        feats[4 * k] = (float)(r[k] * inv);
-        if (consts) {
+        if (!consts) feats[4 * k] = (float)(r1[k] * inv);
+        else {
             feats[4 * k + 1] = (float)S.diag[k] * is;
             feats[4 * k + 2] = (float)S.ce[k] * is;
             feats[4 * k + 3] = (float)S.cn[k] * is;
@@ -938,16 +958,44 @@ __global__ void k_pc_features(int nx, int ny, Sys S, const double *__restrict__ 
     }
 }
 
-// z = out * rms / s (FP64; 0 at the pinned cell), then the FCG beta from z.r, z.q.
-__global__ void __launch_bounds__(256) k_pc_apply(int64_t n, const float *__restrict__ out,
-                                                  const float *__restrict__ scal, const double *__restrict__ r,
-                                                  const double *__restrict__ q, double *__restrict__ z, int pinned,
-                                                  KState *ks, double *partial) {
+// u: the network's FP32 output (0 at the pinned cell); omega =
+// (u . r1) / (u . A u) -> ks->omega, the step that minimises the A-norm of
+// the error left along u (A e1 = r1)
+__global__ void __launch_bounds__(256) k_pc_omega(int nx, int ny, Sys S, const float *__restrict__ u,
+                                                  const double *__restrict__ r1, KState *ks,
+                                                  double *partial) {
     if (ks->done) return;
-    const double rms = ks->res * ks->bn / sqrt((double)n), f = rms / (double)scal[0];
+    const int64_t n = (int64_t)nx * ny;
+    auto U = [&](int64_t m) { return (S.pinned && m == 0) ? 0.0 : (double)u[m]; };
     double acc[2] = {0.0, 0.0};
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        const double zk = (pinned && k == 0) ? 0.0 : (double)out[k] * f;
+        double y = 0.0;
+        if (!(S.pinned && k == 0)) {
+            const int ii = (int)(k / ny), jj = (int)(k % ny);
+            if (jj > 0) y += -S.cn[k - 1] * U(k - 1);
+            if (ii > 0) y += -S.ce[k - ny] * U(k - ny);
+            y += S.diag[k] * U(k);
+            if (ii < nx - 1) y += -S.ce[k] * U(k + ny);
+            if (jj < ny - 1) y += -S.cn[k] * U(k + 1);
+        }
+        const double uk = U(k);
+        acc[0] += uk * r1[k];
+        acc[1] += uk * y;
+    }
+    double tot[2];
+    if (mg_grid_reduce<2>(acc, partial, &ks->counter, tot))
+        ks->omega = (tot[1] > 0.0 && isfinite(tot[0] / tot[1])) ? tot[0] / tot[1] : 0.0;
+}
+
+// z += omega u; dots z.r, z.q -> the FCG beta
+__global__ void __launch_bounds__(256) k_pc_final(int64_t n, const float *__restrict__ u, double *__restrict__ z,
+                                                  const double *__restrict__ r, const double *__restrict__ q,
+                                                  int pinned, KState *ks, double *partial) {
+    if (ks->done) return;
+    const double om = ks->omega;
+    double acc[2] = {0.0, 0.0};
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const double zk = (pinned && k == 0) ? 0.0 : z[k] + om * (double)u[k];
         z[k] = zk;
         acc[0] += zk * r[k];
         acc[1] += zk * q[k];
@@ -956,32 +1004,35 @@ __global__ void __launch_bounds__(256) k_pc_apply(int64_t n, const float *__rest
     if (mg_grid_reduce<2>(acc, partial, &ks->counter, tot)) fcg_beta(ks, tot);
 }
 
-// Training pair from an assembled system and its solution x: feats = (b /
-// rms(b), diag / s, ce / s, cn / s), target = x / rms(x).  Flexible CG is
-// invariant to a scalar factor on the preconditioner's output, so the
-// network learns the direction of A^-1 b.  rms(b) from the KState (bn = |b|
-// of the last solve), |x|^2 into scal[2].
-__global__ void __launch_bounds__(256) k_pc_sumsq(int64_t n, const double *__restrict__ x, double *partial,
-                                                  unsigned *counter, float *scal) {
+// Training pair: feats = (r1 / rms(r1), diag / s, ce / s, cn / s) with r1 =
+// b - A V(b); target = e / rms(e) with e = x - V(b), the error the network
+// must supply (flexible CG and omega make the output scale irrelevant).
+__global__ void __launch_bounds__(256) k_pc_err(int64_t n, const double *__restrict__ x,
+                                                const double *__restrict__ z, double *__restrict__ e, double *partial,
+                                                unsigned *counter, float *scal) {
     double v[1] = {0.0};
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-        v[0] += x[k] * x[k];
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const double d = x[k] - z[k];
+        e[k] = d;
+        v[0] += d * d;
+    }
     double tot[1];
     if (mg_grid_reduce<1>(v, partial, counter, tot)) scal[2] = (float)tot[0];
 }
 
-__global__ void k_pc_pair(int nx, int ny, Sys S, const double *__restrict__ x, const KState *ks,
-                          const float *__restrict__ scal, float *__restrict__ feats, float *__restrict__ target) {
+__global__ void k_pc_pair(int nx, int ny, Sys S, const double *__restrict__ r1, const double *__restrict__ e,
+                          const KState *ks, const float *__restrict__ scal, float *__restrict__ feats,
+                          float *__restrict__ target) {
     const int64_t n = (int64_t)nx * ny;
-    const double rms = ks->bn / sqrt((double)n), inv = rms > 0.0 ? 1.0 / rms : 0.0;
-    const double xr = sqrt((double)scal[2] / (double)n), xinv = xr > 0.0 ? 1.0 / xr : 0.0;
+    const double rr = ks->snorm / sqrt((double)n), inv = rr > 0.0 ? 1.0 / rr : 0.0;
+    const double er = sqrt((double)scal[2] / (double)n), einv = er > 0.0 ? 1.0 / er : 0.0;
     const float is = 1.0f / scal[0];
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        feats[4 * k] = (float)(S.b[k] * inv);
+        feats[4 * k] = (float)(r1[k] * inv);
         feats[4 * k + 1] = (float)S.diag[k] * is;
         feats[4 * k + 2] = (float)S.ce[k] * is;
         feats[4 * k + 3] = (float)S.cn[k] * is;
-        target[k] = (float)(x[k] * xinv);
+        target[k] = (float)(e[k] * einv);
     }
 }
 
@@ -1171,47 +1222,32 @@ void launch_pc_setup(const Sys &S, int nx, int ny, float *feats, float *scal, do
     const int64_t n = (int64_t)nx * ny;
     const int nb = red_blocks(n);
     k_pc_diag_max<<<nb, 256, 0, st>>>(n, S.diag, partial, counter, scal);
-    k_pc_features<<<nb, 256, 0, st>>>(nx, ny, S, S.b, ks, scal, feats, 1);
+    k_pc_features<<<nb, 256, 0, st>>>(nx, ny, S, nullptr, ks, scal, feats, 1);
 }
 
-void launch_fcg_pc_init(const Sys &S, int nx, int ny, double *x, double *r, double *p, double *q, KState *ks,
-                        double *partial, cudaStream_t st) {
-    const int64_t n = (int64_t)nx * ny;
-    k_fcg_init<<<red_blocks(n), 256, 0, st>>>(n, S, x, r, p, ks, partial);
-    cudaMemsetAsync(q, 0, sizeof(double) * n, st);
+void launch_pc_input(const Sys &S, int nx, int ny, const double *r, const double *z, double *r1, KState *ks,
+                     const float *scal, float *feats, double *partial, cudaStream_t st) {
+    const int nb = red_blocks((int64_t)nx * ny);
+    k_pc_resid<<<nb, 256, 0, st>>>(nx, ny, S, r, z, r1, ks, partial);
+    k_pc_features<<<nb, 256, 0, st>>>(nx, ny, S, r1, ks, scal, feats, 0);
 }
 
-void launch_pc_features(const Sys &S, int nx, int ny, const double *r, const KState *ks, const float *scal,
-                        float *feats, cudaStream_t st) {
-    k_pc_features<<<red_blocks((int64_t)nx * ny), 256, 0, st>>>(nx, ny, S, r, ks, scal, feats, 0);
-}
-
-void launch_pc_apply(int nx, int ny, const float *out, const float *scal, const double *r, const double *q, double *z,
-                     int pinned, KState *ks, double *partial, cudaStream_t st) {
-    const int64_t n = (int64_t)nx * ny;
-    k_pc_apply<<<red_blocks(n), 256, 0, st>>>(n, out, scal, r, q, z, pinned, ks, partial);
-}
-
-void launch_fcg_pc_ab(const Sys &S, int nx, int ny, double *x, double *r, const double *p_old, double *p_new,
-                      double *q, const double *z, KState *ks, double *partial, cudaStream_t st) {
+void launch_pc_output(const Sys &S, int nx, int ny, const float *u, const double *r1, const double *r,
+                      const double *q, double *z, KState *ks, double *partial, cudaStream_t st) {
     const int64_t n = (int64_t)nx * ny;
     const int nb = red_blocks(n);
-    k_fcg_a<<<nb, 256, 0, st>>>(nx, ny, S, z, p_old, p_new, q, ks, partial);
-    k_fcg_b<<<nb, 256, 0, st>>>(n, x, r, p_new, q, ks, partial);
+    k_pc_omega<<<nb, 256, 0, st>>>(nx, ny, S, u, r1, ks, partial);
+    k_pc_final<<<nb, 256, 0, st>>>(n, u, z, r, q, S.pinned, ks, partial);
 }
 
-void launch_fcg_pc_replace(const Sys &S, int nx, int ny, const double *x, double *r, KState *ks, double *partial,
-                           cudaStream_t st) {
-    k_fcg_replace<<<red_blocks((int64_t)nx * ny), 256, 0, st>>>(nx, ny, S, x, r, ks, partial);
-}
-
-void launch_pc_pair(const Sys &S, int nx, int ny, const double *x, const KState *ks, float *scal, double *partial,
-                    unsigned *counter, float *feats, float *target, cudaStream_t st) {
+void launch_pc_pair(const Sys &S, int nx, int ny, const double *x, const double *z, const double *r1, double *e,
+                    const KState *ks, float *scal, double *partial, unsigned *counter, float *feats, float *target,
+                    cudaStream_t st) {
     const int64_t n = (int64_t)nx * ny;
     const int nb = red_blocks(n);
     k_pc_diag_max<<<nb, 256, 0, st>>>(n, S.diag, partial, counter, scal);
-    k_pc_sumsq<<<nb, 256, 0, st>>>(n, x, partial, counter, scal);
-    k_pc_pair<<<nb, 256, 0, st>>>(nx, ny, S, x, ks, scal, feats, target);
+    k_pc_err<<<nb, 256, 0, st>>>(n, x, z, e, partial, counter, scal);
+    k_pc_pair<<<nb, 256, 0, st>>>(nx, ny, S, r1, e, ks, scal, feats, target);
 }
 
 }  // namespace asd2g

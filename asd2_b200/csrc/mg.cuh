@@ -46,25 +46,22 @@ bool launch_fcg_check(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const
                       double *r, const double *q, double *z, KState *ks, double *partial, int64_t partial_len,
                       cudaStream_t st);
 
-// Flexible CG preconditioned by the learned network: set-up (coefficient
-// scale s and the constant feature channels), init (x = 0, r = b, p = q = 0),
-// the two FCG kernels of one iteration, the residual replacement, and the
-// preconditioner's input (features of r) and output (z and beta) stages.
-// feats: FP32 [nx][ny][4]; scal[0] = s.
+// Flexible CG with the two-level learned preconditioner (ASD2G_SOLVER_UNET),
+// on the launch_fcg_* iteration with the KState mode set to the solver id (the
+// V-cycle then leaves beta to launch_pc_output):
+// z_mg = V-cycle(r); r1 = r - A z_mg and the network's features; after the
+// network (u), omega = (u . r1) / (u . A u) (the A-norm optimal step) and z =
+// z_mg + omega u with the FCG beta.  feats: FP32 [nx][ny][4]; scal[0] = s = max diag.
 void launch_pc_setup(const Sys &S, int nx, int ny, float *feats, float *scal, double *partial, unsigned *counter,
                      const KState *ks, cudaStream_t st);
-void launch_fcg_pc_init(const Sys &S, int nx, int ny, double *x, double *r, double *p, double *q, KState *ks,
-                        double *partial, cudaStream_t st);
-void launch_pc_features(const Sys &S, int nx, int ny, const double *r, const KState *ks, const float *scal,
-                        float *feats, cudaStream_t st);
-void launch_pc_apply(int nx, int ny, const float *out, const float *scal, const double *r, const double *q, double *z,
-                     int pinned, KState *ks, double *partial, cudaStream_t st);
-void launch_fcg_pc_ab(const Sys &S, int nx, int ny, double *x, double *r, const double *p_old, double *p_new,
-                      double *q, const double *z, KState *ks, double *partial, cudaStream_t st);
-void launch_fcg_pc_replace(const Sys &S, int nx, int ny, const double *x, double *r, KState *ks, double *partial,
-                           cudaStream_t st);
-// Training pair (features of b, solution scaled to unit RMS) of the last solved system.
-void launch_pc_pair(const Sys &S, int nx, int ny, const double *x, const KState *ks, float *scal, double *partial,
-                    unsigned *counter, float *feats, float *target, cudaStream_t st);
+void launch_pc_input(const Sys &S, int nx, int ny, const double *r, const double *z, double *r1, KState *ks,
+                     const float *scal, float *feats, double *partial, cudaStream_t st);
+void launch_pc_output(const Sys &S, int nx, int ny, const float *u, const double *r1, const double *r,
+                      const double *q, double *z, KState *ks, double *partial, cudaStream_t st);
+// Training pair of a solved system x: e = x - z (z = V(b), r1 = b - A z
+// already computed), feats from r1, target e / rms(e).
+void launch_pc_pair(const Sys &S, int nx, int ny, const double *x, const double *z, const double *r1, double *e,
+                    const KState *ks, float *scal, double *partial, unsigned *counter, float *feats, float *target,
+                    cudaStream_t st);
 
 }  // namespace asd2g

@@ -7,13 +7,15 @@
 // X[p + off(t)][ci] * W[co][t][ci] for a tile of 128 consecutive output
 // pixels p of one image row (M = 128) and all output channels (N = Cout).
 // Activations are NHWC BF16 with Cin a multiple of 16.  For each chunk of 16
-// input channels the CTA stages in shared memory
+// input channels a pipeline stage in shared memory holds
 //   * the input patch (3 rows x 130 pixels) as two 8-channel half-planes of
 //     16-byte pixel rows -- the K-major canonical layout, so the A operand of
 //     tap (dy, dx) is the same buffer started dy * 130 + dx rows later;
-//   * the chunk's packed weights [tap][half][co][8] (the B operands);
-// then one thread issues the nine tcgen05.mma of the chunk and commits them
-// to an mbarrier.  The epilogue reads the accumulator from tensor memory
+//   * the chunk's packed weights [tap][half][co][8] (the B operands).
+// Stages are filled by cp.async (zero-fill outside the image) CONV_STAGES - 1
+// chunks ahead; one thread issues the nine tcgen05.mma of a chunk and commits
+// them to the stage's mbarrier, which frees the stage for the chunk
+// CONV_STAGES later.  The epilogue reads the accumulator from tensor memory
 // (warp w owns pixel rows 32w .. 32w+31), adds the bias, applies ReLU and
 // stores BF16 NHWC (and optionally channel 0 in FP32).
 #include <cuda_bf16.h>
@@ -30,8 +32,31 @@ constexpr int PATCH_W = CT_PIX + 2;     // patch row: one halo pixel each side
 constexpr int PATCH_PIX = 3 * PATCH_W;  // pixels per half-plane
 constexpr int PATCH_BYTES = 2 * PATCH_PIX * 16;
 constexpr int CONV_THREADS = 128;
+constexpr int CONV_STAGES = 3;
 
-__host__ __device__ constexpr int conv_smem_bytes(int cout) { return PATCH_BYTES + 288 * cout + 16; }
+__host__ __device__ constexpr int conv_stage_bytes(int cout) { return PATCH_BYTES + 288 * cout; }
+__host__ __device__ constexpr int conv_smem_bytes(int cout) {
+    return CONV_STAGES * conv_stage_bytes(cout) + 8 * CONV_STAGES + 16;
+}
+static_assert(conv_smem_bytes(192) <= 227 * 1024, "conv pipeline exceeds shared memory");
+
+// cp.async of chunk kc (patch + packed weights) into one stage.
+template <int COUT>
+__device__ __forceinline__ void conv_load_chunk(uint8_t *stage, const __nv_bfloat16 *__restrict__ inb, int H, int W,
+                                                int CIN, int y, int x0, int kc, const uint4 *__restrict__ wpack,
+                                                int tid) {
+    uint4 *patch = reinterpret_cast<uint4 *>(stage);
+    uint4 *wsm = reinterpret_cast<uint4 *>(stage + PATCH_BYTES);
+    for (int t = tid; t < 2 * PATCH_PIX; t += CONV_THREADS) {
+        const int h = t / PATCH_PIX, q = t % PATCH_PIX, r = q / PATCH_W, c = q % PATCH_W;
+        const int yy = y - 1 + r, xx = x0 - 1 + c;
+        const bool ok = yy >= 0 && yy < H && xx >= 0 && xx < W;
+        const __nv_bfloat16 *src = ok ? inb + ((size_t)yy * W + xx) * CIN + kc * 16 + h * 8 : inb;
+        cp_async16(patch + t, src, ok);
+    }
+    const uint4 *wk = wpack + (size_t)kc * 9 * 2 * COUT;
+    for (int t = tid; t < 9 * 2 * COUT; t += CONV_THREADS) cp_async16(wsm + t, wk + t, true);
+}
 
 template <int COUT>
 __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __nv_bfloat16 *__restrict__ in, int H, int W,
@@ -40,56 +65,67 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __nv_bfloat16
                                                              __nv_bfloat16 *__restrict__ out,
                                                              float *__restrict__ out32, int relu, int *err) {
     extern __shared__ __align__(128) uint8_t sm[];
-    uint4 *patch = reinterpret_cast<uint4 *>(sm);                // [2][PATCH_PIX]
-    uint4 *wsm = reinterpret_cast<uint4 *>(sm + PATCH_BYTES);    // [9][2][COUT]
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + PATCH_BYTES + 288 * COUT);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+    constexpr int SB = conv_stage_bytes(COUT);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + CONV_STAGES * SB);  // one per stage
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + CONV_STAGES);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int x0 = blockIdx.x * CT_PIX, y = blockIdx.y, img = blockIdx.z;
     const __nv_bfloat16 *inb = in + (size_t)img * H * W * CIN;
     constexpr uint32_t NCOL = COUT <= 32 ? 32 : COUT <= 64 ? 64 : COUT <= 128 ? 128 : 256;  // power of two
     constexpr uint32_t IDESC = umma_idesc_bf16(128, COUT);
+    const int nkc = CIN / 16;
+    // prologue: the first CONV_STAGES - 1 chunks in flight (one group each, empty past the end)
+    for (int k = 0; k < CONV_STAGES - 1; k++) {
+        if (k < nkc) conv_load_chunk<COUT>(sm + k * SB, inb, H, W, CIN, y, x0, k, wpack, tid);
+        cp_async_commit();
+    }
     if (warp == 0) {
         tmem_alloc(tslot, NCOL);
         tmem_relinquish();
     }
-    if (tid == 0) mbar_init(bar, 1);
+    if (tid == 0)
+        for (int k = 0; k < CONV_STAGES; k++) mbar_init(bar + k, 1);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tslot;
-    const int nkc = CIN / 16;
-    uint32_t phase = 0;
     bool ok = true;
-    for (int kc = 0; kc < nkc && ok; kc++) {
-        for (int t = tid; t < 2 * PATCH_PIX; t += CONV_THREADS) {
-            const int h = t / PATCH_PIX, q = t % PATCH_PIX, r = q / PATCH_W, c = q % PATCH_W;
-            const int yy = y - 1 + r, xx = x0 - 1 + c;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (yy >= 0 && yy < H && xx >= 0 && xx < W)
-                v = *reinterpret_cast<const uint4 *>(inb + ((size_t)yy * W + xx) * CIN + kc * 16 + h * 8);
-            patch[t] = v;
+    for (int kc = 0; kc < nkc; kc++) {
+        const int nk = kc + CONV_STAGES - 1;  // chunk to prefetch into the stage chunk kc - 1 used
+        if (nk < nkc) {  // block-uniform
+            bool freed = true;
+            if (kc >= 1) {
+                const int pk = kc - 1;
+                freed = mbar_wait(bar + pk % CONV_STAGES, (uint32_t)(pk / CONV_STAGES) & 1u, err, 1);
+            }
+            if (!__syncthreads_and(freed)) {  // every thread leaves the loop together
+                ok = false;
+                break;
+            }
+            conv_load_chunk<COUT>(sm + (nk % CONV_STAGES) * SB, inb, H, W, CIN, y, x0, nk, wpack, tid);
         }
-        const uint4 *wk = wpack + (size_t)kc * 9 * 2 * COUT;
-        for (int t = tid; t < 9 * 2 * COUT; t += CONV_THREADS) wsm[t] = wk[t];
+        cp_async_commit();
+        cp_async_wait<CONV_STAGES - 1>();  // chunk kc has landed (this thread's part)
         fence_async_smem();
-        __syncthreads();
+        __syncthreads();  // ... and every thread's part
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t pa = smem_u32(patch), pw = smem_u32(wsm);
+            const uint32_t base = smem_u32(sm + (kc % CONV_STAGES) * SB);
+            const uint32_t pa = base, pw = base + PATCH_BYTES;
             for (int tap = 0; tap < 9; tap++) {
                 const int dy = tap / 3, dx = tap % 3;
                 const uint64_t ad = umma_desc_k(pa + (uint32_t)(dy * PATCH_W + dx) * 16u, PATCH_PIX * 16u, 128u);
                 const uint64_t bd = umma_desc_k(pw + (uint32_t)tap * 2u * COUT * 16u, COUT * 16u, 128u);
                 umma_bf16(tmem, ad, bd, IDESC, (kc > 0 || tap > 0) ? 1u : 0u);
             }
-            umma_commit(bar);
+            umma_commit(bar + kc % CONV_STAGES);
         }
-        ok = mbar_wait(bar, phase, err, 1);
-        phase ^= 1u;
-        tc_fence_after();
-        __syncthreads();  // the next chunk overwrites shared memory only after every MMA has read it
     }
+    cp_async_wait<0>();  // no copy may still target shared memory when the CTA exits
+    // the last commit arrives once every MMA of the tile has completed
+    if (ok && nkc > 0) ok = mbar_wait(bar + (nkc - 1) % CONV_STAGES, (uint32_t)((nkc - 1) / CONV_STAGES) & 1u, err, 1);
+    ok = __syncthreads_and(ok);  // the TMEM loads below are warp-collective
+    tc_fence_after();
     if (ok) {
         const int x = x0 + warp * 32 + lane;
         const size_t pix = (size_t)img * H * W + (size_t)y * W + x;

@@ -169,6 +169,102 @@ __global__ void k_loss(const float *__restrict__ o, const float *__restrict__ t,
     }
 }
 
+// 5-point operator of the features at pixel k = h W + w: channels 1..3 =
+// diag, ce (coupling to h + 1), cn (coupling to w + 1), symmetric.
+__device__ __forceinline__ float stencil_apply(const float *__restrict__ f, const float *__restrict__ v, int H, int W,
+                                               int64_t k) {
+    const int h = (int)(k / W), w = (int)(k % W);
+    float y = f[4 * k + 1] * v[k];
+    if (h + 1 < H) y -= f[4 * k + 2] * v[k + W];
+    if (h > 0) y -= f[4 * (k - W) + 2] * v[k - W];
+    if (w + 1 < W) y -= f[4 * k + 3] * v[k + 1];
+    if (w > 0) y -= f[4 * (k - 1) + 3] * v[k - 1];
+    return y;
+}
+
+__device__ __forceinline__ void block_sum3(float (&v)[3], float (*sm)[32]) {
+    for (int o2 = 16; o2 > 0; o2 >>= 1)
+        for (int i = 0; i < 3; i++) v[i] += __shfl_down_sync(0xffffffffu, v[i], o2);
+    if ((threadIdx.x & 31) == 0)
+        for (int i = 0; i < 3; i++) sm[i][threadIdx.x >> 5] = v[i];
+    __syncthreads();
+    for (int i = 0; i < 3; i++) {
+        float t = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sm[i][w];
+        v[i] = t;
+    }
+}
+
+// Residual loss of each sample: with r = feats channel 0, A the operator of
+// channels 1..3 and a = A o, loss = 1 - (a.r)^2 / (|a|^2 |r|^2) -- the
+// squared relative residual |r - omega a|^2 / |r|^2 left by the best scalar
+// omega (the one the solver applies).  d loss / d a = -2 c / (q rr) (r - (c /
+// q) a) with c = a.r, q = a.a, rr = r.r; d loss / d o = A (d loss / d a).
+// One block per sample; scr holds a, then the gradient in a.
+__global__ void __launch_bounds__(1024) k_loss_stencil(const float *__restrict__ o, const float *__restrict__ feats,
+                                                       int H, int W, float *__restrict__ scr, bf16 *__restrict__ g,
+                                                       float *__restrict__ loss) {
+    const int b = blockIdx.x;
+    const int64_t npix = (int64_t)H * W;
+    const float *ob = o + b * npix, *fb = feats + 4 * b * npix;
+    float *sb = scr + b * npix;
+    __shared__ float sm[3][32];
+    float acc[3] = {0.0f, 0.0f, 0.0f};
+    for (int64_t k = threadIdx.x; k < npix; k += blockDim.x) {
+        const float a = stencil_apply(fb, ob, H, W, k), r = fb[4 * k];
+        sb[k] = a;
+        acc[0] += a * r;
+        acc[1] += a * a;
+        acc[2] += r * r;
+    }
+    block_sum3(acc, sm);
+    const float c = acc[0], q = acc[1] > 0.0f ? acc[1] : 1.0f, rr = acc[2] > 0.0f ? acc[2] : 1.0f;
+    if (threadIdx.x == 0) loss[b] = 1.0f - c * c / (q * rr);
+    const float f1 = -2.0f * c / (q * rr) / (float)gridDim.x, f2 = c / q;  // mean over the batch
+    __syncthreads();  // every a is stored before the gradient overwrites it
+    for (int64_t k = threadIdx.x; k < npix; k += blockDim.x) sb[k] = f1 * (fb[4 * k] - f2 * sb[k]);
+    __syncthreads();
+    for (int64_t k = threadIdx.x; k < npix; k += blockDim.x) {
+        bf16 *gp = g + (b * npix + k) * 16;
+        gp[0] = tobf(stencil_apply(fb, sb, H, W, k));
+        for (int ch = 1; ch < 16; ch++) gp[ch] = tobf(0.0f);
+    }
+}
+
+// Energy loss of each sample: with e = target, A the operator of channels
+// 1..3 and u = o, loss = 1 - (u' A e)^2 / ((u' A u)(e' A e)) -- the squared
+// relative A-norm error |e - omega u|_A^2 / |e|_A^2 left by the best scalar
+// omega (the one the solver applies).  d loss / d u = -2 p / (q E) (A e - (p
+// / q) A u) with p = u' A e, q = u' A u, E = e' A e.  One block per sample;
+// scr holds A u.
+__global__ void __launch_bounds__(1024) k_loss_energy(const float *__restrict__ o, const float *__restrict__ feats,
+                                                      const float *__restrict__ t, int H, int W,
+                                                      float *__restrict__ scr, bf16 *__restrict__ g,
+                                                      float *__restrict__ loss) {
+    const int b = blockIdx.x;
+    const int64_t npix = (int64_t)H * W;
+    const float *ob = o + b * npix, *fb = feats + 4 * b * npix, *tb = t + b * npix;
+    float *sb = scr + b * npix;
+    __shared__ float sm[3][32];
+    float acc[3] = {0.0f, 0.0f, 0.0f};
+    for (int64_t k = threadIdx.x; k < npix; k += blockDim.x) {
+        const float au = stencil_apply(fb, ob, H, W, k), ae = stencil_apply(fb, tb, H, W, k);
+        sb[k] = au;
+        acc[0] += ob[k] * ae;
+        acc[1] += ob[k] * au;
+        acc[2] += tb[k] * ae;
+    }
+    block_sum3(acc, sm);
+    const float pp = acc[0], q = acc[1] > 0.0f ? acc[1] : 1.0f, E = acc[2] > 0.0f ? acc[2] : 1.0f;
+    if (threadIdx.x == 0) loss[b] = 1.0f - pp * pp / (q * E);
+    const float f1 = -2.0f * pp / (q * E) / (float)gridDim.x, f2 = pp / q;  // mean over the batch
+    for (int64_t k = threadIdx.x; k < npix; k += blockDim.x) {
+        bf16 *gp = g + (b * npix + k) * 16;
+        gp[0] = tobf(f1 * (stencil_apply(fb, tb, H, W, k) - f2 * sb[k]));
+        for (int ch = 1; ch < 16; ch++) gp[ch] = tobf(0.0f);
+    }
+}
+
 // Weight gradient as a GEMM over pixels, dW[co][ci][t] += sum_p G[p][co] X[p + off(t)][ci]:
 // M = co, N = (t, ci) with n = t * CI + ci (real channels), K = pixels.  A
 // block owns a 32 x 32 output tile and a range of WG_PIX pixels (split K);
@@ -285,6 +381,7 @@ struct asd2g_unet {
     float *w = nullptr, *m = nullptr, *v = nullptr, *g = nullptr;
     float *wt_tmp = nullptr, *zero_bias = nullptr;
     int step = 0;
+    float lr = 0.0f;
     int *err = nullptr;
     std::vector<void *> allocs;
     bf16 *x0 = nullptr, *a[4] = {}, *e[4] = {}, *p[3] = {}, *c[3] = {}, *da[3] = {}, *d[3] = {};
@@ -292,6 +389,7 @@ struct asd2g_unet {
     bf16 *gA = nullptr, *gB = nullptr, *gC = nullptr, *gL = nullptr;
     float *dskip[3] = {};
     float *loss = nullptr, *loss_host = nullptr;
+    float *lscr = nullptr;  // residual loss: A out, then its gradient
 };
 
 namespace {
@@ -494,6 +592,7 @@ int asd2g_unet_create(int max_batch, int max_h, int max_w, void *stream, asd2g_u
     if (!rc) rc = ualloc(u, &u->gC, P * 16);
     if (!rc) rc = ualloc(u, &u->gL, P * 16);
     if (!rc) rc = ualloc(u, &u->loss, (size_t)max_batch);
+    if (!rc) rc = ualloc(u, &u->lscr, P);
     if (!rc && cudaMallocHost(&u->loss_host, sizeof(float) * max_batch) != cudaSuccess)
         rc = api_fail(ASD2G_E_NOMEM, "pinned allocation failed");
     if (rc) {
@@ -565,6 +664,27 @@ int asd2g_unet_forward(asd2g_unet *u, int B, int H, int W, const float *feats, f
     return cuda_ok("unet_forward");
 }
 
+static int train_finish(asd2g_unet *u, int B, int H, int W, float *loss_mean) {
+    cudaMemsetAsync(u->g, 0, sizeof(float) * u->nparam, u->st);
+    int rc = backward(u, B, H, W);
+    if (rc) return rc;
+    u->step++;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - std::pow(b1, (float)u->step), c2 = 1.0f - std::pow(b2, (float)u->step);
+    k_adam<<<blocks((int64_t)u->nparam), 256, 0, u->st>>>(u->w, u->m, u->v, u->g, (int64_t)u->nparam, u->lr, b1, b2,
+                                                         c1, c2, 1e-8f);
+    rc = repack(u);
+    if (rc) return rc;
+    if (loss_mean) {
+        cudaMemcpyAsync(u->loss_host, u->loss, sizeof(float) * B, cudaMemcpyDeviceToHost, u->st);
+        if (cudaStreamSynchronize(u->st) != cudaSuccess) return cuda_ok("train_step");
+        float s = 0.0f;
+        for (int b = 0; b < B; b++) s += u->loss_host[b];
+        *loss_mean = s / (float)B;
+    }
+    return cuda_ok("train_step");
+}
+
 // One Adam step on a batch: loss = mean over samples of |out - target|^2 / |target|^2.
 int asd2g_unet_train_step(asd2g_unet *u, int B, int H, int W, const float *feats, const float *target, float lr,
                           float *loss_mean) {
@@ -576,24 +696,39 @@ int asd2g_unet_train_step(asd2g_unet *u, int B, int H, int W, const float *feats
     rc = forward(u, B, H, W);
     if (rc) return rc;
     k_loss<<<B, 256, 0, u->st>>>(u->out, target, npix, u->gL, u->loss);
-    cudaMemsetAsync(u->g, 0, sizeof(float) * u->nparam, u->st);
-    rc = backward(u, B, H, W);
+    u->lr = lr;
+    return train_finish(u, B, H, W, loss_mean);
+}
+
+// One Adam step on the energy loss: mean over samples of the relative A-norm
+// error 1 - (out' A t)^2 / ((out' A out)(t' A t)).
+int asd2g_unet_train_step_energy(asd2g_unet *u, int B, int H, int W, const float *feats, const float *target,
+                                 float lr, float *loss_mean) {
+    int rc = check_shape(u, B, H, W);
     if (rc) return rc;
-    u->step++;
-    const float b1 = 0.9f, b2 = 0.999f;
-    const float c1 = 1.0f - std::pow(b1, (float)u->step), c2 = 1.0f - std::pow(b2, (float)u->step);
-    k_adam<<<blocks((int64_t)u->nparam), 256, 0, u->st>>>(u->w, u->m, u->v, u->g, (int64_t)u->nparam, lr, b1, b2, c1,
-                                                         c2, 1e-8f);
-    rc = repack(u);
+    if (!feats || !target) return api_fail(ASD2G_E_ARG, "null argument");
+    const int64_t npix = (int64_t)H * W;
+    k_feats_pack<<<blocks((int64_t)B * npix * 16), 256, 0, u->st>>>(feats, (int64_t)B * npix, u->x0);
+    rc = forward(u, B, H, W);
     if (rc) return rc;
-    if (loss_mean) {
-        cudaMemcpyAsync(u->loss_host, u->loss, sizeof(float) * B, cudaMemcpyDeviceToHost, u->st);
-        if (cudaStreamSynchronize(u->st) != cudaSuccess) return cuda_ok("train_step");
-        float s = 0.0f;
-        for (int b = 0; b < B; b++) s += u->loss_host[b];
-        *loss_mean = s / (float)B;
-    }
-    return cuda_ok("train_step");
+    k_loss_energy<<<B, 1024, 0, u->st>>>(u->out, feats, target, H, W, u->lscr, u->gL, u->loss);
+    u->lr = lr;
+    return train_finish(u, B, H, W, loss_mean);
+}
+
+// One Adam step on the residual loss: mean over samples of 1 - cos^2(A out, r).
+int asd2g_unet_train_step_residual(asd2g_unet *u, int B, int H, int W, const float *feats, float lr,
+                                   float *loss_mean) {
+    int rc = check_shape(u, B, H, W);
+    if (rc) return rc;
+    if (!feats) return api_fail(ASD2G_E_ARG, "null argument");
+    const int64_t npix = (int64_t)H * W;
+    k_feats_pack<<<blocks((int64_t)B * npix * 16), 256, 0, u->st>>>(feats, (int64_t)B * npix, u->x0);
+    rc = forward(u, B, H, W);
+    if (rc) return rc;
+    k_loss_stencil<<<B, 1024, 0, u->st>>>(u->out, feats, H, W, u->lscr, u->gL, u->loss);
+    u->lr = lr;
+    return train_finish(u, B, H, W, loss_mean);
 }
 
 // NULL returns the network to the stream it was created with.

@@ -6,8 +6,13 @@ grids -- two to four droplets per domain, density ratio log-uniform in
 [1, 1000] (eight log-spaced ratios, one session each), random smooth
 divergence fields as right-hand sides (plus the surface-tension jumps the
 assembly adds) -- each solved to a relative residual of 1e-10 by the
-MG-preconditioned FCG.  The pairs (features of b, unit-RMS solution) stay on
-the device; training is Adam on shuffled mini-batches with cosine decay.
+MG-preconditioned FCG.  A pair is what the network sees inside the two-level
+preconditioner of ASD2G_SOLVER_UNET: the features of r1 = b - A V(b), the
+residual one FP32 V-cycle leaves, and the unit-RMS error x - V(b) it must
+supply.  The pairs stay on the device; training is Adam on shuffled
+mini-batches with cosine decay, by default on the energy loss (the relative
+A-norm error that the best multiple of the output leaves, the quantity the
+solver's omega step minimises).
 
     python -m asd2_b200.train_unet --samples 20000 --epochs 3
 
@@ -68,9 +73,14 @@ def generate(samples: int, n: int = 256, seed: int = 0, log=print):
     return feats, targets
 
 
-def train(feats, targets, epochs: int = 3, batch: int = 16, lr: float = 1e-3, seed: int = 0, log=print):
+def train(feats, targets, epochs: int = 3, batch: int = 16, lr: float = 1e-3, seed: int = 0, log=print,
+          loss: str = "energy"):
     """Adam over shuffled mini-batches with cosine learning-rate decay;
-    returns the network and the per-epoch mean relative losses."""
+    returns the network and the per-epoch mean losses.  loss "energy": the
+    relative A-norm error the best multiple of u leaves against the error
+    target (what the solver's omega step minimises); "residual": 1 -
+    cos^2(A u, r1), the relative residual instead (targets unused); "mse":
+    relative squared error against the targets."""
     import torch
     from asd2_b200 import api
     S, n = feats.shape[0], feats.shape[1]
@@ -85,13 +95,18 @@ def train(feats, targets, epochs: int = 3, batch: int = 16, lr: float = 1e-3, se
         losses = []
         for b0 in range(0, S - batch + 1, batch):
             idx = perm[b0:b0 + batch]
-            fb, tb = feats[idx].contiguous(), targets[idx].contiguous()
+            fb = feats[idx].contiguous()
             cur = lr * 0.5 * (1.0 + np.cos(np.pi * step / max(steps_total, 1)))
-            losses.append(net.train_step(fb, tb, batch, n, n, cur))
+            if loss == "energy":
+                losses.append(net.train_step_energy(fb, targets[idx].contiguous(), batch, n, n, cur))
+            elif loss == "residual":
+                losses.append(net.train_step_residual(fb, batch, n, n, cur))
+            else:
+                losses.append(net.train_step(fb, targets[idx].contiguous(), batch, n, n, cur))
             step += 1
         history.append(float(np.mean(losses)))
         if log:
-            log(f"epoch {ep + 1}/{epochs}: mean relative loss {history[-1]:.4f} ({time.time() - t0:.1f} s)")
+            log(f"epoch {ep + 1}/{epochs}: mean {loss} loss {history[-1]:.4f} ({time.time() - t0:.1f} s)")
     if net.error_flag():
         raise RuntimeError("a tensor-core wait timed out during training")
     return net, history
@@ -113,13 +128,14 @@ def main():
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--loss", choices=("energy", "residual", "mse"), default="energy")
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     args = ap.parse_args()
     t0 = time.time()
     feats, targets = generate(args.samples, seed=args.seed)
     t_gen = time.time() - t0
-    net, hist = train(feats, targets, args.epochs, args.batch, args.lr, args.seed)
-    meta = dict(samples=args.samples, epochs=args.epochs, batch=args.batch, lr=args.lr, seed=args.seed,
+    net, hist = train(feats, targets, args.epochs, args.batch, args.lr, args.seed, loss=args.loss)
+    meta = dict(samples=args.samples, epochs=args.epochs, batch=args.batch, lr=args.lr, seed=args.seed, loss=args.loss,
                 grid=256, ratios=list(RATIOS), loss_history=hist, seconds_generate=t_gen,
                 seconds_total=time.time() - t0)
     save(net, args.out, meta)

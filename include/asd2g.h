@@ -80,8 +80,8 @@ enum asd2g_solver {
     ASD2G_SOLVER_BICGSTAB = 2,     /* right-Jacobi BiCGStab (rho_2 carried)       */
     ASD2G_SOLVER_BICGSTAB_REFERENCE = 3, /* poisson2d.cpp:403 as written (rho_2 = 1) */
     ASD2G_SOLVER_MGPCG = 4,        /* FP64 flexible CG preconditioned by an FP32 multigrid V-cycle */
-    ASD2G_SOLVER_UNET = 5          /* FP64 flexible CG preconditioned by the learned network
-                                      (asd2g_set_preconditioner_net), Jacobi-PCG fallback */
+    ASD2G_SOLVER_UNET = 5          /* FP64 flexible CG preconditioned by the V-cycle plus a learned
+                                      correction (asd2g_set_preconditioner_net), Jacobi-PCG fallback */
 };
 
 /* solver_flags bits */
@@ -308,6 +308,18 @@ int asd2g_unet_forward(asd2g_unet *u, int B, int H, int W, const float *feats, f
 /* One Adam step; *loss_mean = mean over the batch of |out - target|^2 / |target|^2 (may be NULL). */
 int asd2g_unet_train_step(asd2g_unet *u, int B, int H, int W, const float *feats, const float *target, float lr,
                           float *loss_mean);
+/* One Adam step on the residual loss, mean over samples of 1 - (a.r)^2 /
+ * (|a|^2 |r|^2) with r = feats channel 0, a = A out and A the symmetric
+ * 5-point operator of feats channels 1..3 (diag, coupling to the next image
+ * row, coupling to the next column): the squared relative residual that the
+ * best scalar multiple of out leaves.  No target is needed. */
+int asd2g_unet_train_step_residual(asd2g_unet *u, int B, int H, int W, const float *feats, float lr,
+                                   float *loss_mean);
+/* One Adam step on the energy loss, mean over samples of 1 - (out' A t)^2 /
+ * ((out' A out)(t' A t)) with t = target and A as above: the squared relative
+ * A-norm error that the best scalar multiple of out leaves. */
+int asd2g_unet_train_step_energy(asd2g_unet *u, int B, int H, int W, const float *feats, const float *target,
+                                 float lr, float *loss_mean);
 /* 1 if a tensor-core wait of any launch so far timed out. */
 int asd2g_unet_error_flag(asd2g_unet *u, int *flag);
 /* Run the network's launches on this stream from now on (NULL: the stream it
@@ -315,17 +327,21 @@ int asd2g_unet_error_flag(asd2g_unet *u, int *flag);
 int asd2g_unet_set_stream(asd2g_unet *u, void *stream);
 /* Attach (or detach with NULL) the network used by ASD2G_SOLVER_UNET: nx and
  * ny multiples of 8 and within the network's maximum image size; keep the
- * network alive while attached.  The solve is flexible CG in FP64 with z =
- * network(r) (BF16 / FP32 inside), convergence verified on the FP64 residual
- * as for ASD2G_SOLVER_MGPCG; if it does not converge within min(maxit, 500)
+ * network alive while attached.  The solve is flexible CG in FP64 with a
+ * two-level preconditioner: z_mg = one FP32 V-cycle of r (the multigrid of
+ * ASD2G_SOLVER_MGPCG), r1 = r - A z_mg, u = network(features of r1) (BF16 /
+ * FP32 inside), z = z_mg + omega u with omega = (u . r1) / (u . Au) in
+ * FP64.  Convergence is verified on the FP64 residual as for
+ * ASD2G_SOLVER_MGPCG; if it does not converge within min(maxit, 500)
  * iterations the system is solved again by Jacobi-PCG and
  * asd2g_last_fallback reports 1. */
 int asd2g_set_preconditioner_net(asd2g_session *s, asd2g_unet *net);
 int asd2g_last_fallback(asd2g_session *s, int *used);
 /* Training pair of the network from the session's last assembled and solved
- * system: feats (device FP32 [nx][ny][4]) = (b / rms(b), diag / s, ce / s,
- * cn / s), target (device FP32 [nx][ny]) = x / rms(x), s = max diag (flexible
- * CG is invariant to a scalar factor on the preconditioner's output). */
+ * system (solution x): z = V-cycle(b), r1 = b - A z, e = x - z; feats (device
+ * FP32 [nx][ny][4]) = (r1 / rms(r1), diag / s, ce / s, cn / s), target
+ * (device FP32 [nx][ny]) = e / rms(e), s = max diag (omega makes the
+ * output's scale irrelevant).  The session's solution is left in place. */
 int asd2g_pc_training_pair(asd2g_session *s, void *feats, void *target);
 
 /* ---- whole step (test_mac2d_large.cpp:496-552) ----
