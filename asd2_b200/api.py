@@ -71,7 +71,7 @@ EXPORTS = [
     "asd2g_unet_get_params", "asd2g_unet_get_grads", "asd2g_unet_forward", "asd2g_unet_train_step",
     "asd2g_unet_train_step_residual", "asd2g_unet_train_step_energy",
     "asd2g_unet_error_flag", "asd2g_unet_set_stream", "asd2g_set_preconditioner_net", "asd2g_last_fallback",
-    "asd2g_pc_training_pair",
+    "asd2g_pc_training_pair", "asd2g_pc_training_pair_at",
 ]
 
 _lib = None
@@ -141,6 +141,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_unet_error_flag": ([S, C.POINTER(I)], I), "asd2g_unet_set_stream": ([S, C.c_void_p], I),
         "asd2g_set_preconditioner_net": ([S, S], I), "asd2g_last_fallback": ([S, C.POINTER(I)], I),
         "asd2g_pc_training_pair": ([S, C.c_void_p, C.c_void_p], I),
+        "asd2g_pc_training_pair_at": ([S, I, C.c_void_p, C.c_void_p], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -386,10 +387,12 @@ class Session:
         self._check(self.L.asd2g_last_fallback(self.h, C.byref(f)))
         return f.value
 
-    def training_pair(self, feats, target):
-        """Features and unit-RMS solution of the last solved system into device tensors."""
-        self._check(self.L.asd2g_pc_training_pair(self.h, C.c_void_p(feats.data_ptr()),
-                                                  C.c_void_p(target.data_ptr())))
+    def training_pair(self, feats, target, iters=0):
+        """Learned-preconditioner training pair of the last solved system into
+        device tensors: features of the residual the V-cycle leaves at the
+        MG-FCG iterate after `iters` iterations, and the unit-RMS error it leaves."""
+        self._check(self.L.asd2g_pc_training_pair_at(self.h, int(iters), C.c_void_p(feats.data_ptr()),
+                                                     C.c_void_p(target.data_ptr())))
 
     def volume(self):
         """FP64 (sum H dx dy, sum HS dx dy) of the current level set."""

@@ -170,6 +170,7 @@ struct asd2g_session {
     // learned preconditioner (ASD2G_SOLVER_UNET): network, features, output, scale
     asd2g_unet *pc_net = nullptr;
     float *pc_feats = nullptr, *pc_out = nullptr, *pc_scal = nullptr;
+    FmDirs fm{};  // direction slots of the learned solver's truncated flexible CG
     int last_fallback = 0;
     // multigrid preconditioner (allocated on first use)
     MgLevel lv[MG_MAX_LEVELS] = {};
@@ -805,34 +806,46 @@ static int pc_correct(asd2g_session *s) {
     launch_pc_input(s->sys, g.nx, g.ny, s->r, s->z, s->rt, s->ks, s->pc_scal, s->pc_feats, s->mg_partial, s->st);
     const int rc = asd2g_unet_forward(s->pc_net, 1, g.nx, g.ny, s->pc_feats, s->pc_out);
     if (rc) return rc;
-    launch_pc_output(s->sys, g.nx, g.ny, s->pc_out, s->rt, s->r, s->q, s->z, s->ks, s->mg_partial, s->st);
+    launch_pc_output(s->sys, g.nx, g.ny, s->pc_out, s->rt, s->z, s->fm, s->ks, s->mg_partial, s->st);
     return cuda_check("learned preconditioner");
 }
 
 constexpr int PC_CHUNK = 8;          // iterations per captured chunk; the FP64 residual check closes it
 constexpr int PC_MAX_ITERS = 500;    // iterations of the learned phase before the Jacobi-PCG fallback
+static_assert(PC_CHUNK % FM_SLOTS == 0, "every replay of a chunk must write the direction slots in the same order");
 
 static int pc_chunk(asd2g_session *s) {
     const Grid &g = s->g;
     for (int k = 0; k < PC_CHUNK; k++) {
-        const double *po = k % 2 == 0 ? s->pa : s->pb;
-        double *pn = k % 2 == 0 ? s->pb : s->pa;
-        if (!launch_fcg_iter(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, po, pn, s->q, s->z, s->ks,
-                             s->mg_partial, s->mg_partial_n, s->st))
+        if (!launch_pcm_iter(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->z, s->fm, k % FM_SLOTS,
+                             s->ks, s->mg_partial, s->mg_partial_n, s->st))
             return fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
         const int rc = pc_correct(s);
         if (rc) return rc;
     }
-    if (!launch_fcg_check(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->q, s->z, s->ks,
+    if (!launch_pcm_check(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->z, s->fm, s->ks,
                           s->mg_partial, s->mg_partial_n, s->st))
         return fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
     return pc_correct(s);
+}
+
+static int fm_alloc(asd2g_session *s) {
+    if (s->fm.p[0]) return ASD2G_OK;
+    for (int j = 0; j < FM_SLOTS; j++) {
+        int rc = dalloc(s, &s->fm.p[j], s->N);
+        if (!rc) rc = dalloc(s, &s->fm.q[j], s->N);
+        if (rc) return rc;
+        cudaMemsetAsync(s->fm.p[j], 0, sizeof(double) * s->N, s->st);
+        cudaMemsetAsync(s->fm.q[j], 0, sizeof(double) * s->N, s->st);
+    }
+    return ASD2G_OK;
 }
 
 static int solve_learned(asd2g_session *s, double tol, int maxit, int *iters, double *resid) {
     const Grid &g = s->g;
     if (!s->pc_net) return fail(ASD2G_E_ARG, "no preconditioner network attached (asd2g_set_preconditioner_net)");
     int rc = mg_alloc(s);
+    if (!rc) rc = fm_alloc(s);
     if (rc) return rc;
     rc = asd2g_unet_set_stream(s->pc_net, s->st);
     if (rc) return rc;
@@ -919,8 +932,9 @@ int asd2g_last_fallback(asd2g_session *s, int *used) {
     return ASD2G_OK;
 }
 
-int asd2g_pc_training_pair(asd2g_session *s, void *feats, void *target) {
+int asd2g_pc_training_pair_at(asd2g_session *s, int iters, void *feats, void *target) {
     if (!s || !feats || !target) return fail(ASD2G_E_ARG, "null argument");
+    if (iters < 0 || iters > 1000) return fail(ASD2G_E_ARG, "iters must be in [0, 1000]");
     if (!s->assembled) return fail(ASD2G_E_ARG, "assemble and solve the system first");
     if (!s->pc_scal) {
         if (cudaMalloc(&s->pc_scal, sizeof(float) * 4) != cudaSuccess) {
@@ -933,19 +947,30 @@ int asd2g_pc_training_pair(asd2g_session *s, void *feats, void *target) {
     if (rc) return rc;
     const Grid &g = s->g;
     const size_t N = s->N;
-    double *xs = s->t3, *e = s->t3 + N;  // the solution, kept; the V-cycle's error
+    double *xs = s->t3, *e = s->t3 + N;  // the solution, kept; the error the pair's target is made of
     cudaMemcpyAsync(xs, s->x, sizeof(double) * N, cudaMemcpyDeviceToDevice, s->st);
-    launch_set_kstate(s->ks, 0.0, 1, ASD2G_SOLVER_UNET, 0.0, s->st);
+    // x0 = the iterate after `iters` MG-FCG iterations from 0 (tol 0: none stops early)
+    launch_set_kstate(s->ks, 0.0, 1 << 30, ASD2G_SOLVER_MGPCG, 0.0, s->st);
     launch_mg_setup(s->sys, s->lv, s->nlev, s->coarse_inv, s->st);
-    if (!launch_fcg_init(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->pa, s->q, s->z, s->ks,
-                         s->mg_partial, s->mg_partial_n, s->st))
-        return fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
-    // r = b after the init: r1 = b - A V(b), its norm in the solver state
+    bool ok = launch_fcg_init(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->pa, s->q, s->z,
+                              s->ks, s->mg_partial, s->mg_partial_n, s->st);
+    for (int k = 0; k < iters && ok; k++) {
+        const double *po = k % 2 == 0 ? s->pa : s->pb;
+        double *pn = k % 2 == 0 ? s->pb : s->pa;
+        ok = launch_fcg_iter(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, po, pn, s->q, s->z, s->ks,
+                             s->mg_partial, s->mg_partial_n, s->st);
+    }
+    if (!ok) return fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
+    // z = V(r) for r = b - A x0 (the recurrence residual); r1 = r - A z
     launch_pc_input(s->sys, g.nx, g.ny, s->r, s->z, s->rt, s->ks, s->pc_scal, (float *)feats, s->mg_partial, s->st);
-    launch_pc_pair(s->sys, g.nx, g.ny, xs, s->z, s->rt, e, s->ks, s->pc_scal, s->partial, s->counter + 2,
+    launch_pc_pair(s->sys, g.nx, g.ny, xs, s->x, s->z, s->rt, e, s->ks, s->pc_scal, s->partial, s->counter + 2,
                    (float *)feats, (float *)target, s->st);
     cudaMemcpyAsync(s->x, xs, sizeof(double) * N, cudaMemcpyDeviceToDevice, s->st);
     return cuda_check("training pair");
+}
+
+int asd2g_pc_training_pair(asd2g_session *s, void *feats, void *target) {
+    return asd2g_pc_training_pair_at(s, 0, feats, target);
 }
 
 int asd2g_solve_pressure(asd2g_session *s, int solver, double tol, int maxit, double dt, int *iters,

@@ -987,32 +987,90 @@ __global__ void __launch_bounds__(256) k_pc_omega(int nx, int ny, Sys S, const f
         ks->omega = (tot[1] > 0.0 && isfinite(tot[0] / tot[1])) ? tot[0] / tot[1] : 0.0;
 }
 
-// z += omega u; dots z.r, z.q -> the FCG beta
+// z += omega u; z . q_j for every slot -> the orthogonalisation
+// coefficients of the valid slots (none at the first iteration or after a
+// residual replacement)
 __global__ void __launch_bounds__(256) k_pc_final(int64_t n, const float *__restrict__ u, double *__restrict__ z,
-                                                  const double *__restrict__ r, const double *__restrict__ q,
-                                                  int pinned, KState *ks, double *partial) {
+                                                  FmDirs D, int pinned, KState *ks, double *partial) {
     if (ks->done) return;
     const double om = ks->omega;
-    double acc[2] = {0.0, 0.0};
+    double acc[FM_SLOTS] = {};
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         const double zk = (pinned && k == 0) ? 0.0 : z[k] + om * (double)u[k];
         z[k] = zk;
-        acc[0] += zk * r[k];
-        acc[1] += zk * q[k];
+#pragma unroll
+        for (int j = 0; j < FM_SLOTS; j++) acc[j] += zk * D.q[j][k];
+    }
+    double tot[FM_SLOTS];
+    if (mg_grid_reduce<FM_SLOTS>(acc, partial, &ks->counter, tot)) {
+        if (ks->it == 0 || ks->restart) {
+            ks->fm_mask = 0;
+            ks->restart = 0;
+        }
+        for (int j = 0; j < FM_SLOTS; j++)
+            ks->fm_beta[j] = ((ks->fm_mask >> j) & 1) ? -tot[j] / ks->fm_pq[j] : 0.0;
+    }
+}
+
+// p_w = z + sum over the other valid slots of beta_j p_j, q_w = A p_w;
+// alpha = (p_w . r) / (p_w . q_w)
+__global__ void __launch_bounds__(256) k_pcm_a(int nx, int ny, Sys S, const double *__restrict__ z, FmDirs D, int w,
+                                               const double *__restrict__ r, KState *ks, double *partial) {
+    if (ks->done) return;
+    double b[FM_SLOTS];
+#pragma unroll
+    for (int j = 0; j < FM_SLOTS; j++) b[j] = j == w ? 0.0 : ks->fm_beta[j];
+    const int64_t n = (int64_t)nx * ny;
+    double *__restrict__ pw = D.p[w];
+    double *__restrict__ qw = D.q[w];
+    double acc[2] = {0.0, 0.0};
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int ii = (int)(k / ny), jj = (int)(k % ny);
+        auto pv = [&](int64_t m) {
+            double v = z[m];
+#pragma unroll
+            for (int j = 0; j < FM_SLOTS; j++)
+                if (j != w) v += b[j] * D.p[j][m];
+            return v;
+        };
+        const double pc = pv(k);
+        double y = 0.0;
+        if (!(S.pinned && k == 0)) {
+            if (jj > 0) y += -S.cn[k - 1] * pv(k - 1);
+            if (ii > 0) y += -S.ce[k - ny] * pv(k - ny);
+            y += S.diag[k] * pc;
+            if (ii < nx - 1) y += -S.ce[k] * pv(k + ny);
+            if (jj < ny - 1) y += -S.cn[k] * pv(k + 1);
+        }
+        pw[k] = pc;
+        qw[k] = y;
+        acc[0] += pc * y;
+        acc[1] += pc * r[k];
     }
     double tot[2];
-    if (mg_grid_reduce<2>(acc, partial, &ks->counter, tot)) fcg_beta(ks, tot);
+    if (mg_grid_reduce<2>(acc, partial, &ks->counter, tot)) {
+        if (!(tot[0] > 0.0) || !isfinite(tot[0]) || !isfinite(tot[1])) {
+            ks->status = -6;
+            ks->done = 1;
+        } else {
+            ks->alpha = tot[1] / tot[0];
+            ks->fm_pq[w] = tot[0];
+            ks->fm_mask |= 1 << w;
+        }
+    }
 }
 
 // Training pair: feats = (r1 / rms(r1), diag / s, ce / s, cn / s) with r1 =
-// b - A V(b); target = e / rms(e) with e = x - V(b), the error the network
-// must supply (flexible CG and omega make the output scale irrelevant).
+// r - A V(r) for a residual r = b - A x0; target = e / rms(e) with e = x - x0
+// - V(r), the error the network must supply (omega makes the output scale
+// irrelevant).
 __global__ void __launch_bounds__(256) k_pc_err(int64_t n, const double *__restrict__ x,
-                                                const double *__restrict__ z, double *__restrict__ e, double *partial,
-                                                unsigned *counter, float *scal) {
+                                                const double *__restrict__ x0, const double *__restrict__ z,
+                                                double *__restrict__ e, double *partial, unsigned *counter,
+                                                float *scal) {
     double v[1] = {0.0};
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        const double d = x[k] - z[k];
+        const double d = x[k] - x0[k] - z[k];
         e[k] = d;
         v[0] += d * d;
     }
@@ -1068,7 +1126,7 @@ static dim3 tile_grid(const MgLevel &L) { return dim3((L.ny + MT_J - 1) / MT_J, 
 
 int64_t mg_partial_len(int nx, int ny) {
     const int64_t tiles = (int64_t)((ny + MT_J - 1) / MT_J) * ((nx + MT_I - 1) / MT_I);
-    const int64_t a = 2 * tiles, b = 3 * (int64_t)RED_BLOCKS_MAX;
+    const int64_t a = 2 * tiles, b = (int64_t)FM_SLOTS * RED_BLOCKS_MAX;  // the widest grid-stride reduction
     return a > b ? a : b;
 }
 
@@ -1232,21 +1290,43 @@ void launch_pc_input(const Sys &S, int nx, int ny, const double *r, const double
     k_pc_features<<<nb, 256, 0, st>>>(nx, ny, S, r1, ks, scal, feats, 0);
 }
 
-void launch_pc_output(const Sys &S, int nx, int ny, const float *u, const double *r1, const double *r,
-                      const double *q, double *z, KState *ks, double *partial, cudaStream_t st) {
+void launch_pc_output(const Sys &S, int nx, int ny, const float *u, const double *r1, double *z, const FmDirs &D,
+                      KState *ks, double *partial, cudaStream_t st) {
     const int64_t n = (int64_t)nx * ny;
     const int nb = red_blocks(n);
     k_pc_omega<<<nb, 256, 0, st>>>(nx, ny, S, u, r1, ks, partial);
-    k_pc_final<<<nb, 256, 0, st>>>(n, u, z, r, q, S.pinned, ks, partial);
+    k_pc_final<<<nb, 256, 0, st>>>(n, u, z, D, S.pinned, ks, partial);
 }
 
-void launch_pc_pair(const Sys &S, int nx, int ny, const double *x, const double *z, const double *r1, double *e,
+bool launch_pcm_iter(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, double *x,
+                     double *r, double *z, const FmDirs &D, int w, KState *ks, double *partial, int64_t partial_len,
+                     cudaStream_t st) {
+    if (partial_len < mg_partial_len(nx, ny) || w < 0 || w >= FM_SLOTS) return false;
+    const int64_t n = (int64_t)nx * ny;
+    const int nb = red_blocks(n);
+    k_pcm_a<<<nb, 256, 0, st>>>(nx, ny, S, z, D, w, r, ks, partial);
+    k_fcg_b<<<nb, 256, 0, st>>>(n, x, r, D.p[w], D.q[w], ks, partial);
+    enqueue_vcycle(lv, nlev, coarse_inv, r, D.q[w], z, S.pinned, ks, partial, st);
+    return true;
+}
+
+bool launch_pcm_check(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, const double *x,
+                      double *r, double *z, const FmDirs &D, KState *ks, double *partial, int64_t partial_len,
+                      cudaStream_t st) {
+    if (partial_len < mg_partial_len(nx, ny)) return false;
+    const int64_t n = (int64_t)nx * ny;
+    k_fcg_replace<<<red_blocks(n), 256, 0, st>>>(nx, ny, S, x, r, ks, partial);
+    enqueue_vcycle(lv, nlev, coarse_inv, r, D.q[0], z, S.pinned, ks, partial, st);
+    return true;
+}
+
+void launch_pc_pair(const Sys &S, int nx, int ny, const double *x, const double *x0, const double *z, const double *r1, double *e,
                     const KState *ks, float *scal, double *partial, unsigned *counter, float *feats, float *target,
                     cudaStream_t st) {
     const int64_t n = (int64_t)nx * ny;
     const int nb = red_blocks(n);
     k_pc_diag_max<<<nb, 256, 0, st>>>(n, S.diag, partial, counter, scal);
-    k_pc_err<<<nb, 256, 0, st>>>(n, x, z, e, partial, counter, scal);
+    k_pc_err<<<nb, 256, 0, st>>>(n, x, x0, z, e, partial, counter, scal);
     k_pc_pair<<<nb, 256, 0, st>>>(nx, ny, S, r1, e, ks, scal, feats, target);
 }
 

@@ -47,20 +47,40 @@ bool launch_fcg_check(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const
                       cudaStream_t st);
 
 // Flexible CG with the two-level learned preconditioner (ASD2G_SOLVER_UNET),
-// on the launch_fcg_* iteration with the KState mode set to the solver id (the
-// V-cycle then leaves beta to launch_pc_output):
-// z_mg = V-cycle(r); r1 = r - A z_mg and the network's features; after the
-// network (u), omega = (u . r1) / (u . A u) (the A-norm optimal step) and z =
-// z_mg + omega u with the FCG beta.  feats: FP32 [nx][ny][4]; scal[0] = s = max diag.
+// KState mode set to the solver id (the V-cycle then leaves the direction
+// update to launch_pc_output).  Preconditioner: z_mg = V-cycle(r); r1 = r - A
+// z_mg and the network's features; after the network (u), omega = (u . r1) /
+// (u . A u) (the A-norm optimal step) and z = z_mg + omega u.  The network
+// makes the preconditioner nonlinear, so each new direction is
+// A-orthogonalised against the FM_SLOTS - 1 directions before it (truncated
+// flexible CG), not only the last one: p = z - sum_j (z . q_j / p_j . q_j)
+// p_j, alpha = (p . r) / (p . A p).  Directions live in FM_SLOTS ring slots;
+// iteration k of a chunk writes slot k % FM_SLOTS (chunks are multiples of
+// FM_SLOTS long, so the slot order is the same in every replay).
+constexpr int FM_SLOTS = 4;
+struct FmDirs {
+    double *p[FM_SLOTS];
+    double *q[FM_SLOTS];
+};
 void launch_pc_setup(const Sys &S, int nx, int ny, float *feats, float *scal, double *partial, unsigned *counter,
                      const KState *ks, cudaStream_t st);
 void launch_pc_input(const Sys &S, int nx, int ny, const double *r, const double *z, double *r1, KState *ks,
                      const float *scal, float *feats, double *partial, cudaStream_t st);
-void launch_pc_output(const Sys &S, int nx, int ny, const float *u, const double *r1, const double *r,
-                      const double *q, double *z, KState *ks, double *partial, cudaStream_t st);
-// Training pair of a solved system x: e = x - z (z = V(b), r1 = b - A z
-// already computed), feats from r1, target e / rms(e).
-void launch_pc_pair(const Sys &S, int nx, int ny, const double *x, const double *z, const double *r1, double *e,
+void launch_pc_output(const Sys &S, int nx, int ny, const float *u, const double *r1, double *z, const FmDirs &D,
+                      KState *ks, double *partial, cudaStream_t st);
+// new direction in slot w (A-orthogonal to the other valid slots), x and r
+// updates, then the V-cycle of the new r into z
+bool launch_pcm_iter(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, double *x,
+                     double *r, double *z, const FmDirs &D, int w, KState *ks, double *partial, int64_t partial_len,
+                     cudaStream_t st);
+// FP64 residual replacement (as launch_fcg_check), then the V-cycle
+bool launch_pcm_check(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const double *coarse_inv, const double *x,
+                      double *r, double *z, const FmDirs &D, KState *ks, double *partial, int64_t partial_len,
+                      cudaStream_t st);
+// Training pair of a solved system x at the iterate x0: e = x - x0 - z (z =
+// V(r), r1 = r - A z already computed, r = b - A x0), feats from r1, target
+// e / rms(e).
+void launch_pc_pair(const Sys &S, int nx, int ny, const double *x, const double *x0, const double *z, const double *r1, double *e,
                     const KState *ks, float *scal, double *partial, unsigned *counter, float *feats, float *target,
                     cudaStream_t st);
 

@@ -24,6 +24,10 @@ struct KState {
     int verified;  // MG-FCG: the converged residual was confirmed by b - A x in FP64
     int restart;   // MG-FCG: the next V-cycle starts a new direction (beta = 0)
     double res_true_prev;  // MG-FCG: true residual at the previous replacement (-1: none yet)
+    // truncated flexible CG of the learned preconditioner: p_j . A p_j and the
+    // orthogonalisation coefficients of the stored directions, valid-slot mask
+    double fm_pq[4], fm_beta[4];
+    int fm_mask;
 };
 
 constexpr int RED_BLOCKS_MAX = 1184;  // 8 x 148 SMs

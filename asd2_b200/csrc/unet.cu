@@ -12,10 +12,11 @@
 //     16-byte pixel rows -- the K-major canonical layout, so the A operand of
 //     tap (dy, dx) is the same buffer started dy * 130 + dx rows later;
 //   * the chunk's packed weights [tap][half][co][8] (the B operands).
-// Stages are filled by cp.async (zero-fill outside the image) CONV_STAGES - 1
-// chunks ahead; one thread issues the nine tcgen05.mma of a chunk and commits
-// them to the stage's mbarrier, which frees the stage for the chunk
-// CONV_STAGES later.  The epilogue reads the accumulator from tensor memory
+// Stages are filled two chunks ahead: the patch by cp.async (zero-fill
+// outside the image), the chunk's weights by one bulk copy completing on the
+// stage's full barrier.  One thread waits for the weights, issues the nine
+// tcgen05.mma of a chunk and commits them to the stage's MMA barrier, which
+// frees the stage for the chunk that many stages later.  The epilogue reads the accumulator from tensor memory
 // (warp w owns pixel rows 32w .. 32w+31), adds the bias, applies ReLU and
 // stores BF16 NHWC (and optionally channel 0 in FP32).
 #include <cuda_bf16.h>
@@ -25,6 +26,9 @@
 #include "tc05.cuh"
 
 namespace asd2g {
+
+bool conv_cout_ok(int c) { return c == 16 || c == 32 || c == 48 || c == 64 || c == 96 || c == 128 || c == 192; }
+
 namespace {
 
 constexpr int CT_PIX = 128;             // output pixels per tile
@@ -32,99 +36,171 @@ constexpr int PATCH_W = CT_PIX + 2;     // patch row: one halo pixel each side
 constexpr int PATCH_PIX = 3 * PATCH_W;  // pixels per half-plane
 constexpr int PATCH_BYTES = 2 * PATCH_PIX * 16;
 constexpr int CONV_THREADS = 128;
-constexpr int CONV_STAGES = 3;
+constexpr int CONV_SMEM_MAX = 227 * 1024;
 
 __host__ __device__ constexpr int conv_stage_bytes(int cout) { return PATCH_BYTES + 288 * cout; }
+// Four stages where they fit (loads two chunks ahead, and the MMAs of a chunk
+// get one iteration to finish before their stage is refilled), else three
+// (loads two chunks ahead, the stage of the previous chunk is refilled).
+__host__ __device__ constexpr int conv_stages(int cout) {
+    return 4 * conv_stage_bytes(cout) + 16 * 4 + 16 <= CONV_SMEM_MAX ? 4 : 3;
+}
+// stages, then two mbarriers per stage, the TMEM address and the abort flag
 __host__ __device__ constexpr int conv_smem_bytes(int cout) {
-    return CONV_STAGES * conv_stage_bytes(cout) + 8 * CONV_STAGES + 16;
+    return conv_stages(cout) * conv_stage_bytes(cout) + 16 * conv_stages(cout) + 16;
 }
-static_assert(conv_smem_bytes(192) <= 227 * 1024, "conv pipeline exceeds shared memory");
+static_assert(conv_smem_bytes(192) <= CONV_SMEM_MAX, "conv pipeline exceeds shared memory");
 
-// cp.async of chunk kc (patch + packed weights) into one stage.
-template <int COUT>
-__device__ __forceinline__ void conv_load_chunk(uint8_t *stage, const __nv_bfloat16 *__restrict__ inb, int H, int W,
-                                                int CIN, int y, int x0, int kc, const uint4 *__restrict__ wpack,
-                                                int tid) {
-    uint4 *patch = reinterpret_cast<uint4 *>(stage);
-    uint4 *wsm = reinterpret_cast<uint4 *>(stage + PATCH_BYTES);
-    for (int t = tid; t < 2 * PATCH_PIX; t += CONV_THREADS) {
-        const int h = t / PATCH_PIX, q = t % PATCH_PIX, r = q / PATCH_W, c = q % PATCH_W;
-        const int yy = y - 1 + r, xx = x0 - 1 + c;
-        const bool ok = yy >= 0 && yy < H && xx >= 0 && xx < W;
-        const __nv_bfloat16 *src = ok ? inb + ((size_t)yy * W + xx) * CIN + kc * 16 + h * 8 : inb;
-        cp_async16(patch + t, src, ok);
+// Patch copies of one thread: slot i covers patch entry t = tid + 128 i of
+// the two half-planes (2 x 3 x 130 pixel rows of 16 bytes).  The pixel
+// offsets do not depend on the channel chunk, so they are formed once; a
+// chunk adds its channel offset.  With low != nullptr the input is the
+// channel concatenation of low (H/2 x W/2 x CL, nearest-upsampled: pixel
+// (y, x) reads (y/2, x/2)) and in (H x W x (CIN - CL)); CL is a multiple of
+// 16, so a chunk reads one of the two.
+constexpr int PATCH_SLOTS = (2 * PATCH_PIX + CONV_THREADS - 1) / CONV_THREADS;
+struct PatchPlan {
+    int off_in[PATCH_SLOTS];   // element offset in `in` (pixel * channels + half * 8), -1: outside
+    int off_low[PATCH_SLOTS];  // element offset in `low`
+};
+
+__device__ __forceinline__ void patch_plan(PatchPlan &P, int H, int W, int cs, int CL, int y, int x0, int tid) {
+#pragma unroll
+    for (int i = 0; i < PATCH_SLOTS; i++) {
+        const int t = tid + CONV_THREADS * i;
+        P.off_in[i] = -1;
+        P.off_low[i] = -1;
+        if (t < 2 * PATCH_PIX) {
+            const int h = t / PATCH_PIX, q = t % PATCH_PIX, r = q / PATCH_W, c = q % PATCH_W;
+            const int yy = y - 1 + r, xx = x0 - 1 + c;
+            if (yy >= 0 && yy < H && xx >= 0 && xx < W) {
+                P.off_in[i] = (yy * W + xx) * cs + h * 8;
+                P.off_low[i] = ((yy >> 1) * (W >> 1) + (xx >> 1)) * CL + h * 8;
+            }
+        }
     }
-    const uint4 *wk = wpack + (size_t)kc * 9 * 2 * COUT;
-    for (int t = tid; t < 9 * 2 * COUT; t += CONV_THREADS) cp_async16(wsm + t, wk + t, true);
+}
+
+// Chunk kc into one stage: the patch by cp.async (every thread), the
+// chunk's packed weights (contiguous) by one bulk copy of thread 0 that
+// completes on the stage's full barrier.
+template <int COUT>
+__device__ __forceinline__ void conv_load_chunk(uint8_t *stage, uint64_t *full, const PatchPlan &P,
+                                                const __nv_bfloat16 *__restrict__ inb,
+                                                const __nv_bfloat16 *__restrict__ lowb, int CL, int kc,
+                                                const uint4 *__restrict__ wpack, int tid) {
+    uint4 *patch = reinterpret_cast<uint4 *>(stage);
+    const bool from_low = lowb != nullptr && kc * 16 < CL;
+    const __nv_bfloat16 *base = from_low ? lowb + kc * 16 : inb + (lowb ? kc * 16 - CL : kc * 16);
+#pragma unroll
+    for (int i = 0; i < PATCH_SLOTS; i++) {
+        const int t = tid + CONV_THREADS * i;
+        if (t < 2 * PATCH_PIX) {
+            const int off = from_low ? P.off_low[i] : P.off_in[i];
+            cp_async16(patch + t, off >= 0 ? base + off : inb, off >= 0);
+        }
+    }
+    if (tid == 0) {
+        constexpr uint32_t WB = 288u * COUT;  // 9 taps x 16 channels x COUT x 2 bytes
+        mbar_arrive_expect_tx(full, WB);
+        bulk_g2s(stage + PATCH_BYTES, wpack + (size_t)kc * (WB / 16), WB, full);
+    }
 }
 
 template <int COUT>
-__global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __nv_bfloat16 *__restrict__ in, int H, int W,
-                                                             int CIN, const uint4 *__restrict__ wpack,
+__global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __nv_bfloat16 *__restrict__ in,
+                                                             const __nv_bfloat16 *__restrict__ low, int CL, int H,
+                                                             int W, int CIN, const uint4 *__restrict__ wpack,
                                                              const float *__restrict__ bias,
                                                              __nv_bfloat16 *__restrict__ out,
                                                              float *__restrict__ out32, int relu, int *err) {
     extern __shared__ __align__(128) uint8_t sm[];
     constexpr int SB = conv_stage_bytes(COUT);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + CONV_STAGES * SB);  // one per stage
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + CONV_STAGES);
+    constexpr int S = conv_stages(COUT);
+    constexpr int SLACK = S - 3;          // iterations a chunk's MMAs get before their stage is refilled
+    constexpr int AHEAD = S - 1 - SLACK;  // chunks in flight ahead of the one being multiplied
+    uint64_t *mma_bar = reinterpret_cast<uint64_t *>(sm + S * SB);  // per stage: its MMAs completed
+    uint64_t *full_bar = mma_bar + S;                               // per stage: its weights landed
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(full_bar + S);
+    int *abort_flag = reinterpret_cast<int *>(tslot + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int x0 = blockIdx.x * CT_PIX, y = blockIdx.y, img = blockIdx.z;
-    const __nv_bfloat16 *inb = in + (size_t)img * H * W * CIN;
+    const int cs = low ? CIN - CL : CIN;
+    const __nv_bfloat16 *inb = in + (size_t)img * H * W * cs;
+    const __nv_bfloat16 *lowb = low ? low + (size_t)img * (H >> 1) * (W >> 1) * CL : nullptr;
     constexpr uint32_t NCOL = COUT <= 32 ? 32 : COUT <= 64 ? 64 : COUT <= 128 ? 128 : 256;  // power of two
     constexpr uint32_t IDESC = umma_idesc_bf16(128, COUT);
     const int nkc = CIN / 16;
-    // prologue: the first CONV_STAGES - 1 chunks in flight (one group each, empty past the end)
-    for (int k = 0; k < CONV_STAGES - 1; k++) {
-        if (k < nkc) conv_load_chunk<COUT>(sm + k * SB, inb, H, W, CIN, y, x0, k, wpack, tid);
+    if (tid == 0) {
+        for (int k = 0; k < S; k++) {
+            mbar_init(mma_bar + k, 1);
+            mbar_init(full_bar + k, 1);
+        }
+        mbar_init_fence();
+        *abort_flag = 0;
+    }
+    PatchPlan P;
+    patch_plan(P, H, W, cs, CL, y, x0, tid);
+    __syncthreads();  // barriers initialised before the first copy arrives on one
+    // prologue: the first AHEAD chunks in flight (one cp.async group each, empty past the end)
+    for (int k = 0; k < AHEAD; k++) {
+        if (k < nkc) conv_load_chunk<COUT>(sm + k * SB, full_bar + k, P, inb, lowb, CL, k, wpack, tid);
         cp_async_commit();
     }
     if (warp == 0) {
         tmem_alloc(tslot, NCOL);
         tmem_relinquish();
     }
-    if (tid == 0)
-        for (int k = 0; k < CONV_STAGES; k++) mbar_init(bar + k, 1);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tslot;
     bool ok = true;
+    int issued = nkc < AHEAD ? nkc : AHEAD;  // chunks whose copies were started
+    int consumed = 0;                        // chunks whose weights thread 0 has waited for
     for (int kc = 0; kc < nkc; kc++) {
-        const int nk = kc + CONV_STAGES - 1;  // chunk to prefetch into the stage chunk kc - 1 used
-        if (nk < nkc) {  // block-uniform
+        const int nk = kc + AHEAD;  // chunk to prefetch, into the stage chunk nk - S used
+        if (nk < nkc) {             // block-uniform
             bool freed = true;
-            if (kc >= 1) {
-                const int pk = kc - 1;
-                freed = mbar_wait(bar + pk % CONV_STAGES, (uint32_t)(pk / CONV_STAGES) & 1u, err, 1);
-            }
-            if (!__syncthreads_and(freed)) {  // every thread leaves the loop together
+            const int pk = nk - S;
+            if (pk >= 0) freed = mbar_wait(mma_bar + pk % S, (uint32_t)(pk / S) & 1u, err, 1);
+            if (!__syncthreads_and(freed && !*abort_flag)) {  // every thread leaves the loop together
                 ok = false;
                 break;
             }
-            conv_load_chunk<COUT>(sm + (nk % CONV_STAGES) * SB, inb, H, W, CIN, y, x0, nk, wpack, tid);
+            conv_load_chunk<COUT>(sm + (nk % S) * SB, full_bar + nk % S, P, inb, lowb, CL, nk, wpack, tid);
+            issued = nk + 1;
         }
         cp_async_commit();
-        cp_async_wait<CONV_STAGES - 1>();  // chunk kc has landed (this thread's part)
+        cp_async_wait<AHEAD>();  // chunk kc's patch has landed (this thread's part)
         fence_async_smem();
         __syncthreads();  // ... and every thread's part
         if (tid == 0) {
+            const bool wok = mbar_wait(full_bar + kc % S, (uint32_t)(kc / S) & 1u, err, 2);
+            consumed = kc + 1;
             tc_fence_after();
-            const uint32_t base = smem_u32(sm + (kc % CONV_STAGES) * SB);
-            const uint32_t pa = base, pw = base + PATCH_BYTES;
-            for (int tap = 0; tap < 9; tap++) {
-                const int dy = tap / 3, dx = tap % 3;
-                const uint64_t ad = umma_desc_k(pa + (uint32_t)(dy * PATCH_W + dx) * 16u, PATCH_PIX * 16u, 128u);
-                const uint64_t bd = umma_desc_k(pw + (uint32_t)tap * 2u * COUT * 16u, COUT * 16u, 128u);
-                umma_bf16(tmem, ad, bd, IDESC, (kc > 0 || tap > 0) ? 1u : 0u);
+            if (wok) {
+                const uint32_t base = smem_u32(sm + (kc % S) * SB);
+                const uint32_t pa = base, pw = base + PATCH_BYTES;
+                for (int tap = 0; tap < 9; tap++) {
+                    const int dy = tap / 3, dx = tap % 3;
+                    const uint64_t ad = umma_desc_k(pa + (uint32_t)(dy * PATCH_W + dx) * 16u, PATCH_PIX * 16u, 128u);
+                    const uint64_t bd = umma_desc_k(pw + (uint32_t)tap * 2u * COUT * 16u, COUT * 16u, 128u);
+                    umma_bf16(tmem, ad, bd, IDESC, (kc > 0 || tap > 0) ? 1u : 0u);
+                }
+            } else {
+                *abort_flag = 1;
             }
-            umma_commit(bar + kc % CONV_STAGES);
+            umma_commit(mma_bar + kc % S);  // always, so that waits on this stage end
         }
     }
-    cp_async_wait<0>();  // no copy may still target shared memory when the CTA exits
+    cp_async_wait<0>();  // no cp.async may still target shared memory when the CTA exits
+    if (tid == 0)        // nor a bulk copy: wait (bounded) for the weights of chunks never multiplied
+        for (int c = consumed; c < issued; c++) mbar_wait(full_bar + c % S, (uint32_t)(c / S) & 1u, err, 2);
     // the last commit arrives once every MMA of the tile has completed
-    if (ok && nkc > 0) ok = mbar_wait(bar + (nkc - 1) % CONV_STAGES, (uint32_t)((nkc - 1) / CONV_STAGES) & 1u, err, 1);
-    ok = __syncthreads_and(ok);  // the TMEM loads below are warp-collective
+    if (ok && nkc > 0) ok = mbar_wait(mma_bar + (nkc - 1) % S, (uint32_t)((nkc - 1) / S) & 1u, err, 1);
+    __syncthreads();
+    ok = __syncthreads_and(ok && !*abort_flag);  // the TMEM loads below are warp-collective
     tc_fence_after();
     if (ok) {
         const int x = x0 + warp * 32 + lane;
@@ -192,29 +268,32 @@ template <int COUT> bool conv_prepare() {
 }
 
 template <int COUT>
-int conv_launch(const void *in, int n, int h, int w, int cin, const void *wpack, const float *bias, void *out,
-                float *out32, int relu, int *err, cudaStream_t st) {
+int conv_launch(const void *in, const void *low, int cl, int n, int h, int w, int cin, const void *wpack,
+                const float *bias, void *out, float *out32, int relu, int *err, cudaStream_t st) {
     if (!conv_prepare<COUT>()) return ASD2G_E_CUDA;
     const dim3 grid((w + CT_PIX - 1) / CT_PIX, h, n);
     k_conv3x3_tc<COUT><<<grid, CONV_THREADS, conv_smem_bytes(COUT), st>>>(
-        (const __nv_bfloat16 *)in, h, w, cin, (const uint4 *)wpack, bias, (__nv_bfloat16 *)out, out32, relu, err);
+        (const __nv_bfloat16 *)in, (const __nv_bfloat16 *)low, cl, h, w, cin, (const uint4 *)wpack, bias,
+        (__nv_bfloat16 *)out, out32, relu, err);
     return cudaGetLastError() == cudaSuccess ? ASD2G_OK : ASD2G_E_CUDA;
 }
 
 }  // namespace
 
-bool conv_cout_ok(int c) { return c == 16 || c == 32 || c == 48 || c == 64 || c == 96 || c == 128 || c == 192; }
 
 int conv3x3_tc(const void *in, int n, int h, int w, int cin, const void *wpack, const float *bias, int cout,
-               void *out, float *out32, int relu, int *err, cudaStream_t st) {
+               void *out, float *out32, int relu, int *err, cudaStream_t st, const void *low, int cl) {
+    if (low && (cl < 16 || cl % 16 || cl >= cin || h % 2 || w % 2)) return ASD2G_E_ARG;
+    if ((int64_t)h * w * cin >= (int64_t)1 << 31) return ASD2G_E_ARG;  // per-image offsets are 32-bit
+    if (((uintptr_t)wpack & 15u) != 0) return ASD2G_E_ARG;              // bulk copies start on 16 bytes
     switch (cout) {
-    case 16: return conv_launch<16>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
-    case 32: return conv_launch<32>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
-    case 48: return conv_launch<48>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
-    case 64: return conv_launch<64>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
-    case 96: return conv_launch<96>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
-    case 128: return conv_launch<128>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
-    case 192: return conv_launch<192>(in, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    case 16: return conv_launch<16>(in, low, cl, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    case 32: return conv_launch<32>(in, low, cl, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    case 48: return conv_launch<48>(in, low, cl, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    case 64: return conv_launch<64>(in, low, cl, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    case 96: return conv_launch<96>(in, low, cl, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    case 128: return conv_launch<128>(in, low, cl, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    case 192: return conv_launch<192>(in, low, cl, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
     default: return ASD2G_E_ARG;
     }
 }
@@ -241,7 +320,7 @@ int asd2g_conv3x3_bf16(const void *in, int n, int h, int w, int cin, const void 
                        void *out, float *out32, int relu, int *err, void *stream) {
     if (!in || !wpack || !bias || (!out && !out32) || n < 1 || h < 1 || w < 1 || cin < 16 || cin % 16)
         return ASD2G_E_ARG;
-    return conv3x3_tc(in, n, h, w, cin, wpack, bias, cout, out, out32, relu, err, (cudaStream_t)stream);
+    return conv3x3_tc(in, n, h, w, cin, wpack, bias, cout, out, out32, relu, err, (cudaStream_t)stream, nullptr, 0);
 }
 
 }  // extern "C"

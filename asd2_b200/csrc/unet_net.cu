@@ -27,8 +27,9 @@
 namespace asd2g {
 int api_fail(int code, const char *msg);
 bool conv_cout_ok(int c);
+// low != nullptr: the input is concat(nearest-upsampled low with cl channels, in)
 int conv3x3_tc(const void *in, int n, int h, int w, int cin, const void *wpack, const float *bias, int cout,
-               void *out, float *out32, int relu, int *err, cudaStream_t st);
+               void *out, float *out32, int relu, int *err, cudaStream_t st, const void *low = nullptr, int cl = 0);
 }  // namespace asd2g
 
 using namespace asd2g;
@@ -40,19 +41,37 @@ namespace {
 __device__ __forceinline__ float bf(bf16 v) { return __bfloat162float(v); }
 __device__ __forceinline__ bf16 tobf(float v) { return __float2bfloat16_rn(v); }
 
-// 2x2 average pooling, NHWC, C channels (H, W even).
+// 2x2 average pooling, NHWC, C channels (H, W even, C a multiple of 8):
+// one thread per 8 channels of an output pixel (16-byte loads and stores).
 __global__ void k_pool(const bf16 *__restrict__ in, int B, int H, int W, int C, bf16 *__restrict__ out) {
-    const int h = H / 2, w = W / 2;
-    const int64_t n = (int64_t)B * h * w * C;
+    const int h = H / 2, w = W / 2, c8 = C / 8;
+    const int64_t n = (int64_t)B * h * w * c8;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-        const int c = (int)(e % C);
-        int64_t q = e / C;
+        const int c = (int)(e % c8) * 8;
+        int64_t q = e / c8;
         const int x = (int)(q % w);
         q /= w;
         const int y = (int)(q % h);
         const int b = (int)(q / h);
         const bf16 *s = in + (((int64_t)b * H + 2 * y) * W + 2 * x) * C + c;
-        out[e] = tobf(0.25f * (bf(s[0]) + bf(s[C]) + bf(s[(int64_t)W * C]) + bf(s[(int64_t)W * C + C])));
+        const uint4 v[4] = {*reinterpret_cast<const uint4 *>(s), *reinterpret_cast<const uint4 *>(s + C),
+                            *reinterpret_cast<const uint4 *>(s + (int64_t)W * C),
+                            *reinterpret_cast<const uint4 *>(s + (int64_t)W * C + C)};
+        uint32_t o[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            float lo = 0.0f, hi = 0.0f;
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                const uint32_t wv = (&v[t].x)[i];
+                const __nv_bfloat162 b2 = *reinterpret_cast<const __nv_bfloat162 *>(&wv);
+                lo += __low2float(b2);
+                hi += __high2float(b2);
+            }
+            const __nv_bfloat162 r2 = __floats2bfloat162_rn(0.25f * lo, 0.25f * hi);
+            o[i] = *reinterpret_cast<const uint32_t *>(&r2);
+        }
+        *reinterpret_cast<uint4 *>(out + (((int64_t)b * h + y) * w + x) * C + c) = make_uint4(o[0], o[1], o[2], o[3]);
     }
 }
 
@@ -119,11 +138,15 @@ __global__ void k_pool_back_add(const float *__restrict__ dskip, const bf16 *__r
     }
 }
 
-// Features of B systems: feats FP32 [B][H][W][4] -> BF16 [B][H][W][16] (zero padded)
+// Features of B systems: feats FP32 [B][H][W][4] -> BF16 [B][H][W][16] (zero
+// padded), one thread per pixel (one 16-byte load, two 16-byte stores).
 __global__ void k_feats_pack(const float *__restrict__ f, int64_t npix, bf16 *__restrict__ out) {
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < npix * 16; e += (int64_t)gridDim.x * blockDim.x) {
-        const int c = (int)(e % 16);
-        out[e] = c < 4 ? tobf(f[(e / 16) * 4 + c]) : tobf(0.0f);
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < npix; p += (int64_t)gridDim.x * blockDim.x) {
+        const float4 v = *reinterpret_cast<const float4 *>(f + 4 * p);
+        const __nv_bfloat162 a = __floats2bfloat162_rn(v.x, v.y), b = __floats2bfloat162_rn(v.z, v.w);
+        uint4 *o = reinterpret_cast<uint4 *>(out + 16 * p);
+        o[0] = make_uint4(*reinterpret_cast<const uint32_t *>(&a), *reinterpret_cast<const uint32_t *>(&b), 0u, 0u);
+        o[1] = make_uint4(0u, 0u, 0u, 0u);
     }
 }
 
@@ -437,7 +460,10 @@ int conv(asd2g_unet *u, int li, const bf16 *in, int B, int H, int W, bf16 *out, 
     return rc ? api_fail(rc, "tensor-core convolution launch") : ASD2G_OK;
 }
 
-int forward(asd2g_unet *u, int B, int H, int W) {
+// keep_concat: materialise each decoder input (upsampled low + skip) in u->c
+// for the weight gradients; otherwise the decoder convolutions read the two
+// sources directly.
+int forward(asd2g_unet *u, int B, int H, int W, bool keep_concat) {
     int rc = ASD2G_OK;
     const bf16 *in = u->x0;
     for (int lv = 0; lv < 4 && !rc; lv++) {
@@ -445,8 +471,8 @@ int forward(asd2g_unet *u, int B, int H, int W) {
         rc = conv(u, 2 * lv, in, B, h, w, u->a[lv], nullptr);
         if (!rc) rc = conv(u, 2 * lv + 1, u->a[lv], B, h, w, u->e[lv], nullptr);
         if (!rc && lv < 3) {
-            k_pool<<<blocks((int64_t)B * (h / 2) * (w / 2) * CH[lv]), 256, 0, u->st>>>(u->e[lv], B, h, w, CH[lv],
-                                                                                     u->p[lv]);
+            k_pool<<<blocks((int64_t)B * (h / 2) * (w / 2) * (CH[lv] / 8)), 256, 0, u->st>>>(u->e[lv], B, h, w,
+                                                                                            CH[lv], u->p[lv]);
             in = u->p[lv];
         }
     }
@@ -454,9 +480,17 @@ int forward(asd2g_unet *u, int B, int H, int W) {
     int cl = 128;
     for (int lv = 2; lv >= 0 && !rc; lv--) {
         const int h = H >> lv, w = W >> lv, cs = CH[lv];
-        k_upcat<<<blocks((int64_t)B * h * w * (cl + cs)), 256, 0, u->st>>>(low, cl, u->e[lv], cs, B, h, w, u->c[lv]);
         const int li = 8 + 2 * (2 - lv);
-        rc = conv(u, li, u->c[lv], B, h, w, u->da[lv], nullptr);
+        if (keep_concat) {
+            k_upcat<<<blocks((int64_t)B * h * w * (cl + cs)), 256, 0, u->st>>>(low, cl, u->e[lv], cs, B, h, w,
+                                                                              u->c[lv]);
+            rc = conv(u, li, u->c[lv], B, h, w, u->da[lv], nullptr);
+        } else {
+            const UnetLayer &l = u->L[li];
+            const int rc2 = conv3x3_tc(u->e[lv], B, h, w, l.cin_p, l.wpack, u->w + l.boff, l.cout_p, u->da[lv],
+                                       nullptr, l.relu, u->err, u->st, low, cl);
+            rc = rc2 ? api_fail(rc2, "tensor-core convolution launch") : ASD2G_OK;
+        }
         if (!rc) rc = conv(u, li + 1, u->da[lv], B, h, w, u->d[lv], nullptr);
         low = u->d[lv];
         cl = cs;
@@ -657,8 +691,8 @@ int asd2g_unet_forward(asd2g_unet *u, int B, int H, int W, const float *feats, f
     if (rc) return rc;
     if (!feats || !out) return api_fail(ASD2G_E_ARG, "null argument");
     const int64_t npix = (int64_t)B * H * W;
-    k_feats_pack<<<blocks(npix * 16), 256, 0, u->st>>>(feats, npix, u->x0);
-    rc = forward(u, B, H, W);
+    k_feats_pack<<<blocks(npix), 256, 0, u->st>>>(feats, npix, u->x0);
+    rc = forward(u, B, H, W, false);
     if (rc) return rc;
     cudaMemcpyAsync(out, u->out, sizeof(float) * npix, cudaMemcpyDeviceToDevice, u->st);
     return cuda_ok("unet_forward");
@@ -692,8 +726,8 @@ int asd2g_unet_train_step(asd2g_unet *u, int B, int H, int W, const float *feats
     if (rc) return rc;
     if (!feats || !target) return api_fail(ASD2G_E_ARG, "null argument");
     const int64_t npix = (int64_t)H * W;
-    k_feats_pack<<<blocks((int64_t)B * npix * 16), 256, 0, u->st>>>(feats, (int64_t)B * npix, u->x0);
-    rc = forward(u, B, H, W);
+    k_feats_pack<<<blocks((int64_t)B * npix), 256, 0, u->st>>>(feats, (int64_t)B * npix, u->x0);
+    rc = forward(u, B, H, W, true);
     if (rc) return rc;
     k_loss<<<B, 256, 0, u->st>>>(u->out, target, npix, u->gL, u->loss);
     u->lr = lr;
@@ -708,8 +742,8 @@ int asd2g_unet_train_step_energy(asd2g_unet *u, int B, int H, int W, const float
     if (rc) return rc;
     if (!feats || !target) return api_fail(ASD2G_E_ARG, "null argument");
     const int64_t npix = (int64_t)H * W;
-    k_feats_pack<<<blocks((int64_t)B * npix * 16), 256, 0, u->st>>>(feats, (int64_t)B * npix, u->x0);
-    rc = forward(u, B, H, W);
+    k_feats_pack<<<blocks((int64_t)B * npix), 256, 0, u->st>>>(feats, (int64_t)B * npix, u->x0);
+    rc = forward(u, B, H, W, true);
     if (rc) return rc;
     k_loss_energy<<<B, 1024, 0, u->st>>>(u->out, feats, target, H, W, u->lscr, u->gL, u->loss);
     u->lr = lr;
@@ -723,8 +757,8 @@ int asd2g_unet_train_step_residual(asd2g_unet *u, int B, int H, int W, const flo
     if (rc) return rc;
     if (!feats) return api_fail(ASD2G_E_ARG, "null argument");
     const int64_t npix = (int64_t)H * W;
-    k_feats_pack<<<blocks((int64_t)B * npix * 16), 256, 0, u->st>>>(feats, (int64_t)B * npix, u->x0);
-    rc = forward(u, B, H, W);
+    k_feats_pack<<<blocks((int64_t)B * npix), 256, 0, u->st>>>(feats, (int64_t)B * npix, u->x0);
+    rc = forward(u, B, H, W, true);
     if (rc) return rc;
     k_loss_stencil<<<B, 1024, 0, u->st>>>(u->out, feats, H, W, u->lscr, u->gL, u->loss);
     u->lr = lr;

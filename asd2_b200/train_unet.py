@@ -7,9 +7,10 @@ grids -- two to four droplets per domain, density ratio log-uniform in
 divergence fields as right-hand sides (plus the surface-tension jumps the
 assembly adds) -- each solved to a relative residual of 1e-10 by the
 MG-preconditioned FCG.  A pair is what the network sees inside the two-level
-preconditioner of ASD2G_SOLVER_UNET: the features of r1 = b - A V(b), the
-residual one FP32 V-cycle leaves, and the unit-RMS error x - V(b) it must
-supply.  The pairs stay on the device; training is Adam on shuffled
+preconditioner of ASD2G_SOLVER_UNET: the features of r1 = r - A V(r), the
+residual one FP32 V-cycle leaves, and the unit-RMS error it must supply; r is
+the right-hand side for half of the pairs and the residual of a later MG-FCG
+iterate (1 to 12 iterations) for the other half.  The pairs stay on the device; training is Adam on shuffled
 mini-batches with cosine decay, by default on the energy loss (the relative
 A-norm error that the best multiple of the output leaves, the quantity the
 solver's omega step minimises).
@@ -35,6 +36,7 @@ if ROOT not in sys.path:
 
 DEFAULT_WEIGHTS = os.path.join(HERE, "unet_weights.npz")
 RATIOS = tuple(float(r) for r in np.geomspace(1.0, 1000.0, 8))
+MAX_PAIR_ITERS = 12
 
 
 def generate(samples: int, n: int = 256, seed: int = 0, log=print):
@@ -63,7 +65,8 @@ def generate(samples: int, n: int = 256, seed: int = 0, log=print):
         r = s.solve_pressure(api.MGPCG, tol=1e-10, maxit=2000, dt=1e-3)
         if r["status"] != 0:
             raise RuntimeError(f"training system {k} did not converge: {r}")
-        s.training_pair(feats[k], targets[k])
+        # the first residual, or one of a later Krylov iterate (what the network meets inside the solve)
+        s.training_pair(feats[k], targets[k], iters=int(rng.integers(0, MAX_PAIR_ITERS + 1)) if k % 2 else 0)
         if log and (k + 1) % 2000 == 0:
             s.sync()
             log(f"generated {k + 1}/{samples} systems in {time.time() - t0:.1f} s")

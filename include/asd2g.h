@@ -343,6 +343,10 @@ int asd2g_last_fallback(asd2g_session *s, int *used);
  * (device FP32 [nx][ny]) = e / rms(e), s = max diag (omega makes the
  * output's scale irrelevant).  The session's solution is left in place. */
 int asd2g_pc_training_pair(asd2g_session *s, void *feats, void *target);
+/* The same at a later Krylov iterate: x0 = the MG-FCG iterate after `iters`
+ * (0..1000) iterations from 0, r = b - A x0 (recurrence), z = V-cycle(r), r1 =
+ * r - A z, e = x - x0 - z.  iters = 0 is asd2g_pc_training_pair. */
+int asd2g_pc_training_pair_at(asd2g_session *s, int iters, void *feats, void *target);
 
 /* ---- whole step (test_mac2d_large.cpp:496-552) ----
  * lsB = LS; advect; reinit (reinit_mode); kappa; H, HS; intermediate velocity
