@@ -324,6 +324,92 @@ def batched_solves(sh, stream, flush, count=BATCH_COUNT):
             "l2": "flushed (256 MB write) before each timed batch / system"}
 
 
+def learned_pc_512(sh, stream, flush, weights=None, n=512, counts=tuple(range(1, 9))):
+    """The learned-preconditioner evaluation: eight 512^2 GFM systems with
+    1 to 8 droplets (radius [0.05, 0.15], density ratio log-uniform in
+    [1, 1000]), each taken after one full FP64 droplet step from rest (gravity
+    and surface tension drive the flow).  Timed per system (assembly + solve
+    to the FP64 relative residual 1e-8): the learned two-level preconditioner
+    (ASD2G_SOLVER_UNET, trained weights), the FP64 Jacobi-PCG (plain FP64 GPU
+    CG) and the MG-FCG.  The pressure error of the learned solve is measured
+    against an FP64 MG-FCG solve to 1e-12."""
+    import torch
+    from asd2_b200 import api
+    from asd2_b200 import workloads as W
+    from asd2_b200 import train_unet as T
+    path = weights or T.DEFAULT_WEIGHTS
+    if not os.path.exists(path):
+        return {"unavailable": f"no trained preconditioner weights at {os.path.relpath(path, ROOT)}"}
+    params, meta = T.load_params(path)
+    net = api.UNet(1, n, n, stream=sh)
+    net.set_params(params)
+    rng = np.random.Generator(np.random.PCG64(5))
+
+    def timed(fn):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return r, e0.elapsed_time(e1) / 1e3
+
+    rows, tot = [], {"unet": 0.0, "cg": 0.0, "mg": 0.0}
+    for count in counts:
+        ratio = float(10 ** rng.uniform(0.0, 3.0))
+        c = W.multi_droplet(n, seed=int(rng.integers(1 << 30)), count=count, rho_ratio=ratio)
+        with api.Session(api.Params.from_case(c), stream=sh) as ss:
+            ss.upload("ls", c.ls)
+            ss.upload("u", c.u)
+            ss.upload("v", c.v)
+            ss.apply_bc("ls", "P")
+            dt = ss.update_dt()
+            r = ss.droplet_step(dt, solver=api.MGPCG, tol=1e-10, maxit=100000)
+            if r["status"] != 0:
+                raise SystemExit(f"bench: learned-PC preparation step failed: {r}")
+            ss.assemble_gfm(dt, recompute_kappa=False)  # the step's own system (its kappa, H and divergence)
+            ref = ss.solve_pressure(api.MGPCG, tol=1e-12, maxit=100000, dt=dt)
+            p_ref = ss.download("ps")
+            ss.set_preconditioner_net(net)
+
+            def solve(sv):
+                ss.assemble_gfm(dt, recompute_kappa=False)
+                return ss.solve_pressure(sv, tol=TOL, maxit=100000, dt=dt)
+            out = {"droplets": count, "rho_ratio": ratio}
+            for key, sv in (("unet", api.UNET), ("cg", api.PCG), ("mg", api.MGPCG)):
+                solve(sv)
+                res, t = timed(lambda: solve(sv))
+                if res["status"] != 0:
+                    raise SystemExit(f"bench: {key} solve did not converge: {res}")
+                tot[key] += t
+                out[key] = {"ms": t * 1e3, "iters": res["iters"], "true_rel_residual": ss.true_residual()}
+                if key == "unet":
+                    out[key]["fallback"] = bool(ss.last_fallback())
+                    ps = ss.download("ps")
+                    inner = (slice(3, -3), slice(3, -3))
+                    out[key]["p_rel_err_max"] = float(np.abs(ps[inner] - p_ref[inner]).max()
+                                                      / np.abs(p_ref[inner]).max())
+            out["ref_resid"] = ref["resid"]
+            rows.append(out)
+    k = len(rows)
+    net.close()
+    return {"workload": f"{k} GFM systems of {n}x{n} with 1..{max(counts)} droplets (radius [0.05, 0.15], density "
+                        "ratio log-U[1, 1000]) after one full FP64 step from rest; assembly + solve to rel. residual "
+                        f"{TOL:g}",
+            "value": k / tot["unet"], "unit": "GFM Poisson solves/s",
+            "solver": "FP64 flexible CG (directions A-orthogonalised against the previous three), preconditioner "
+                      "= FP32 V-cycle + U-Net correction (BF16 tcgen05 convolutions) with the A-norm optimal step",
+            "fp64_cg": {"value": k / tot["cg"], "unit": "GFM Poisson solves/s"},
+            "mg_fcg": {"value": k / tot["mg"], "unit": "GFM Poisson solves/s"},
+            "speedup_vs_fp64_cg": tot["cg"] / tot["unet"],
+            "fallbacks": int(sum(r["unet"]["fallback"] for r in rows)),
+            "max_true_rel_residual": float(max(r["unet"]["true_rel_residual"] for r in rows)),
+            "max_p_rel_err": float(max(r["unet"]["p_rel_err_max"] for r in rows)),
+            "training": {kk: meta.get(kk) for kk in ("samples", "epochs", "loss", "grid", "seconds_total")},
+            "systems": rows, "l2": "flushed (256 MB write) before each timed solve"}
+
+
 def run_ours(args):
     import torch
     from asd2_b200 import api
@@ -469,6 +555,7 @@ def run_ours(args):
     ls_rates = level_set_rates(sh, stream, flush, peak) if not args.no_extra else None
     batched = batched_solves(sh, stream, flush) if not args.no_extra else None
     mixed = mixed_precision_errors(sh) if not args.no_extra else None
+    learned = learned_pc_512(sh, stream, flush, args.weights) if not args.no_extra else None
     nlev = len(_mg_levels(args.n, args.n))
     per_iter = 2 + 2 * (nlev - 1) + 1
     launches = int(sum(4 + (1 + nlev) + (1 + per_iter - 2) + 8 * per_iter * math.ceil(i / 8) + 3 for i in iters))
@@ -511,6 +598,7 @@ def run_ours(args):
         "batched_256": batched,
         "ls_large": ls_rates,
         "mixed_precision_1024": mixed,
+        "learned_pc_512": learned,
         "e2e": {"value": e2e_value, "unit": "GFM Poisson solves/s",
                 "h2d_bytes_per_step": 3 * G * 8, "d2h_bytes_per_step": G * 8},
         "gpu_launches": launches,
@@ -622,18 +710,19 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the 2048^2 level-set and 1024^2 mixed-precision reports")
-    ap.add_argument("--section", default=None, choices=["ls_large", "mixed_1024", "batched"],
+    ap.add_argument("--weights", default=None, help="learned-preconditioner weights (default: the committed ones)")
+    ap.add_argument("--section", default=None, choices=["ls_large", "mixed_1024", "batched", "learned_pc"],
                     help="run only this report (its JSON object on stdout), e.g. to profile it")
     args = ap.parse_args()
     if args.section:
-        run_section(args.section)
+        run_section(args.section, args)
     elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
 
 
-def run_section(name):
+def run_section(name, args):
     import torch
     torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
@@ -649,6 +738,9 @@ def run_section(name):
     elif name == "batched":
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
         out = batched_solves(stream.cuda_stream, stream, flush)
+    elif name == "learned_pc":
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        out = learned_pc_512(stream.cuda_stream, stream, flush, args.weights)
     else:
         out = mixed_precision_errors(stream.cuda_stream)
     print(json.dumps({"section": name, **out}), flush=True)
