@@ -33,7 +33,7 @@ NOT_CONVERGED = 1
 FLAG_NO_CLUSTER_PCG = 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "unsupported",
-          -5: "non-finite value", -6: "Krylov breakdown"}
+          -5: "non-finite value", -6: "Krylov breakdown", -7: "checkpoint I/O"}
 
 
 class Asd2gError(RuntimeError):
@@ -62,7 +62,8 @@ EXPORTS = [
     "asd2g_kappa", "asd2g_heaviside", "asd2g_convection", "asd2g_viscosity", "asd2g_momentum_rhs",
     "asd2g_intermediate_vel", "asd2g_divergence", "asd2g_update_vel", "asd2g_update_dt",
     "asd2g_assemble_gfm", "asd2g_get_system", "asd2g_solve_pressure", "asd2g_true_residual",
-    "asd2g_droplet_step", "asd2g_pcg_solve_static", "asd2g_weno5_line", "asd2g_weno_absgrad",
+    "asd2g_droplet_step", "asd2g_run_steps", "asd2g_checkpoint_save", "asd2g_checkpoint_load",
+    "asd2g_checkpoint_info", "asd2g_pcg_solve_static", "asd2g_weno5_line", "asd2g_weno_absgrad",
     "asd2g_apply_bc_side", "asd2g_update_ntk", "asd2g_csr_solve", "asd2g_volume", "asd2g_last_volume",
     "asd2g_batch_create", "asd2g_batch_destroy", "asd2g_batch_upload", "asd2g_batch_download",
     "asd2g_batch_field_ptr", "asd2g_batch_offset", "asd2g_batch_assemble", "asd2g_batch_solve", "asd2g_batch_sync",
@@ -111,6 +112,12 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_solve_pressure": ([S, I, D, I, D, C.POINTER(I), C.POINTER(D)], I),
         "asd2g_true_residual": ([S, C.POINTER(D)], I),
         "asd2g_droplet_step": ([S, C.POINTER(D), I, I, D, I, C.POINTER(I), C.POINTER(D)], I),
+        "asd2g_checkpoint_save": ([S, C.c_char_p, D, C.c_longlong, D], I),
+        "asd2g_checkpoint_load": ([S, C.c_char_p, C.POINTER(D), C.POINTER(C.c_longlong), C.POINTER(D)], I),
+        "asd2g_checkpoint_info": ([C.c_char_p, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_longlong),
+                                   C.POINTER(D)], I),
+        "asd2g_run_steps": ([S, I, C.POINTER(D), I, I, D, I, C.POINTER(I), C.POINTER(C.c_longlong), C.POINTER(D)],
+                            I),
         "asd2g_pcg_solve_static": ([I, I, I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, D, I,
                                     C.c_void_p, C.POINTER(I), C.POINTER(D)], I),
         "asd2g_weno5_line": ([S, dp, dp, dp, D, I], I), "asd2g_weno_absgrad": ([S, I, I, I], I),
@@ -378,6 +385,24 @@ class Session:
                                                    C.byref(it), C.byref(res)))
         return dict(status=rc, dt_next=d.value, iters=it.value, resid=res.value)
 
+    def run_steps(self, nsteps, dt, reinit_mode=REINIT_MINRK2, solver=MGPCG, tol=1e-10, maxit=10000):
+        """nsteps droplet steps on the device (one step graph per step, the
+        solver loop a device-side WHILE node, one synchronisation)."""
+        d, n, it, res = C.c_double(dt), C.c_int(), C.c_longlong(), C.c_double()
+        rc = self._check(self.L.asd2g_run_steps(self.h, int(nsteps), C.byref(d), reinit_mode, solver, tol, maxit,
+                                                C.byref(n), C.byref(it), C.byref(res)))
+        return dict(status=rc, dt_next=d.value, steps=n.value, iters=it.value, max_resid=res.value)
+
+    def checkpoint_save(self, path, t=0.0, step=0, dt=0.0):
+        """Write LS, U, V, PS, P (padded FP64) with t, step and dt to a checkpoint file."""
+        self._check(self.L.asd2g_checkpoint_save(self.h, os.fsencode(path), t, step, dt))
+
+    def checkpoint_load(self, path):
+        """Replace the fields from a checkpoint; returns dict(t, step, dt)."""
+        t, n, d = C.c_double(), C.c_longlong(), C.c_double()
+        self._check(self.L.asd2g_checkpoint_load(self.h, os.fsencode(path), C.byref(t), C.byref(n), C.byref(d)))
+        return dict(t=t.value, step=n.value, dt=d.value)
+
     def set_preconditioner_net(self, net):
         self._check(self.L.asd2g_set_preconditioner_net(self.h, net.h if net is not None else None))
         self._pc_net = net  # the session refers to it: keep it alive while attached
@@ -469,6 +494,17 @@ class Batch:
 UNET_LAYERS = [(4, 16, 1), (16, 16, 1), (16, 32, 1), (32, 32, 1), (32, 64, 1), (64, 64, 1), (64, 128, 1),
                (128, 128, 1), (192, 64, 1), (64, 64, 1), (96, 32, 1), (32, 32, 1), (48, 16, 1), (16, 16, 1),
                (16, 1, 0)]
+
+
+def checkpoint_info(path):
+    """Header of a checkpoint file after verifying its checksum (no GPU needed):
+    dict(nx, ny, t, step, dt); raises Asd2gError(-7) for an invalid file."""
+    L = load()
+    nx, ny, t, n, d = C.c_int(), C.c_int(), C.c_double(), C.c_longlong(), C.c_double()
+    rc = L.asd2g_checkpoint_info(os.fsencode(path), C.byref(nx), C.byref(ny), C.byref(t), C.byref(n), C.byref(d))
+    if rc < 0:
+        raise Asd2gError(rc, L.asd2g_last_error().decode())
+    return dict(nx=nx.value, ny=ny.value, t=t.value, step=n.value, dt=d.value)
 
 
 class UNet:

@@ -2,6 +2,8 @@
 // operations, enqueued on the session's stream.
 #include <cmath>
 #include <cstdarg>
+#include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -48,6 +50,65 @@ __global__ void k_set_scalar(double *p, double v) { *p = v; }
 __global__ void k_fill(double *a, int64_t n, double v) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
         a[k] = v;
+}
+
+// Statistics of a device-resident multi-step run (asd2g_run_steps).
+struct RunStats {
+    double max_res;      // largest final relative residual of the steps' solves
+    long long iters;     // solver iterations summed over the steps
+    int steps;           // steps executed
+    int fail_step;       // first step whose solve failed or whose next dt is not positive and finite (-1: none)
+    int fail_status;     // its solver status
+    int loops;           // passes of the current solve's WHILE body
+};
+
+__global__ void k_run_reset(RunStats *rs) {
+    rs->max_res = 0.0;
+    rs->iters = 0;
+    rs->steps = 0;
+    rs->fail_step = -1;
+    rs->fail_status = 0;
+    rs->loops = 0;
+}
+// IF condition of the step: no earlier step failed.
+__global__ void k_run_if(const RunStats *rs, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, rs->fail_step < 0 ? 1u : 0u);
+}
+// WHILE condition of the solve: not done; a hard cap on the passes ends the
+// loop (status -7) whatever the solver state.
+__global__ void k_run_while(KState *ks, RunStats *rs, int cap, cudaGraphConditionalHandle h) {
+    const int loops = ++rs->loops;
+    bool more = !ks->done;
+    if (more && loops >= cap) {
+        ks->status = -7;
+        ks->done = 1;
+        more = false;
+    }
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+// End of a step: accumulate, record a failure, hand the next dt to the next step.
+__global__ void k_run_step_end(const KState *ks, RunStats *rs, double tol, double *dsc) {
+    const bool conv = (ks->status == 0 && !(ks->res > tol)) || ks->status == 2;
+    const double dtn = dsc[1];
+    rs->iters += ks->it;
+    rs->max_res = fmax(rs->max_res, ks->res);
+    if ((!conv || !(dtn > 0.0) || !isfinite(dtn)) && rs->fail_step < 0) {
+        rs->fail_step = rs->steps;
+        rs->fail_status = conv ? -5 : ks->status;
+    }
+    rs->steps += 1;
+    rs->loops = 0;
+    dsc[0] = dtn;
+}
+void launch_run_reset(RunStats *rs, cudaStream_t st) { k_run_reset<<<1, 1, 0, st>>>(rs); }
+void launch_run_if(const RunStats *rs, cudaGraphConditionalHandle h, cudaStream_t st) {
+    k_run_if<<<1, 1, 0, st>>>(rs, h);
+}
+void launch_run_while(KState *ks, RunStats *rs, int cap, cudaGraphConditionalHandle h, cudaStream_t st) {
+    k_run_while<<<1, 1, 0, st>>>(ks, rs, cap, h);
+}
+void launch_run_step_end(const KState *ks, RunStats *rs, double tol, double *dsc, cudaStream_t st) {
+    k_run_step_end<<<1, 1, 0, st>>>(ks, rs, tol, dsc);
 }
 }  // namespace asd2g
 
@@ -181,6 +242,13 @@ struct asd2g_session {
     double last_volume[2] = {0.0, 0.0};  // volume check of the last droplet step (sharp, smoothed)
     int64_t mg_partial_n = 0;
     int chunk_len = 64;
+    // device-resident multi-step run (asd2g_run_steps): the step graph, the
+    // streams its conditional bodies are captured on, its statistics
+    cudaGraphExec_t run_exec = nullptr;
+    int run_reinit = -1, run_maxit = -1;
+    double run_tol = -1.0;
+    cudaStream_t aux_st[2] = {};
+    RunStats *run_stats = nullptr, *run_stats_host = nullptr;
     std::vector<void *> allocs;
 };
 
@@ -363,6 +431,10 @@ int asd2g_destroy(asd2g_session *s) {
     if (s->st) cudaStreamSynchronize(s->st);
     for (auto &e : s->chunk_exec)
         if (e) cudaGraphExecDestroy(e);
+    if (s->run_exec) cudaGraphExecDestroy(s->run_exec);
+    for (cudaStream_t a : s->aux_st)
+        if (a) cudaStreamDestroy(a);
+    if (s->run_stats_host) cudaFreeHost(s->run_stats_host);
     for (void *p : s->allocs) cudaFree(p);
     if (s->ks_host) cudaFreeHost(s->ks_host);
     if (s->dsc_host) cudaFreeHost(s->dsc_host);
@@ -1071,19 +1143,14 @@ int asd2g_csr_solve(asd2g_session *s, int solver, int rows, const int *ia, const
 }
 
 // ------------------------------------------------------------------ step --
-int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver, double tol, int maxit, int *iters,
-                       double *rel_resid) {
-    if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
-    int rc = p_supported(s);
-    if (rc) return rc;
+// The step up to the assembled pressure system (dt from the device scalar):
+// Solve_LevelSet_2D, the reinitialisation, kappa, H and HS, the FP64 volume
+// check, the intermediate velocity, its divergence and the GFM assembly.
+static int enqueue_step_pre(asd2g_session *s, int reinit_mode) {
     const Grid &g = s->g;
-    rc = set_dt(s, *dt);
-    if (rc) return rc;
     cudaMemcpyAsync(s->f[ASD2G_LSB], s->f[ASD2G_LS], sizeof(double) * s->G, cudaMemcpyDeviceToDevice, s->st);
-    // Solve_LevelSet_2D (dt from the device scalar) and the reinitialisation
     double *ls = s->f[ASD2G_LS];
-    const bool mixed = s->prm.precision == ASD2G_PRECISION_MIXED;
-    if (mixed) {
+    if (s->prm.precision == ASD2G_PRECISION_MIXED) {
         if (!ls32_supported(g, reinit_mode))
             return fail(ASD2G_E_UNSUPPORTED, "mixed precision implements reinit modes 0, 2 and 4, not %d", reinit_mode);
         launch_fill_p(g, ls, s->st);
@@ -1101,21 +1168,37 @@ int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver
     launch_heaviside(g, ls, s->f[ASD2G_H], s->f[ASD2G_HS], s->st);
     // FP64 volume check of the new level set (read by asd2g_last_volume)
     launch_volume(g, s->f[ASD2G_H], s->f[ASD2G_HS], s->partial, s->counter + 1, s->dsc + 5, s->st);
-    rc = intermediate(s, ASD2G_HS);
+    int rc = intermediate(s, ASD2G_HS);
     if (rc) return rc;
     launch_fill_uv(g, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->st);
     cudaMemsetAsync(s->f[ASD2G_DIV], 0, sizeof(double) * s->G, s->st);
     launch_divergence(g, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->f[ASD2G_DIV], s->st);
     // SolvePoisson recomputes kappa when kWe is finite and nonzero (mac2d.cpp:1307).
     const double we = s->prm.numbers_given ? s->prm.we : s->prm.rho_h / s->prm.sigma;
-    rc = assemble(s, (we != 0.0 && std::isfinite(we)) ? 1 : 0);
+    return assemble(s, (we != 0.0 && std::isfinite(we)) ? 1 : 0);
+}
+
+// After the solve: ps and p, the projection (UpdateVel) and the next dt (UpdateDt, into dsc[1]).
+static void enqueue_step_post(asd2g_session *s) {
+    const Grid &g = s->g;
+    launch_scatter_ps(g, s->x, s->f[ASD2G_PS], s->f[ASD2G_P], s->dsc, s->st);
+    launch_update_vel(g, s->M, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->f[ASD2G_PS], s->f[ASD2G_LS], s->f[ASD2G_H],
+                      s->f[ASD2G_KAPPA], s->f[ASD2G_U], s->f[ASD2G_V], s->dsc, s->st);
+    launch_update_dt(g, s->M, s->f[ASD2G_U], s->f[ASD2G_V], s->partial, s->counter, s->dsc + 1, s->st);
+}
+
+int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver, double tol, int maxit, int *iters,
+                       double *rel_resid) {
+    if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
+    int rc = p_supported(s);
+    if (rc) return rc;
+    rc = set_dt(s, *dt);
+    if (rc) return rc;
+    rc = enqueue_step_pre(s, reinit_mode);
     if (rc) return rc;
     const int st = solve(s, solver, tol, maxit, iters, rel_resid);
     if (st < 0) return st;
-    launch_scatter_ps(g, s->x, s->f[ASD2G_PS], s->f[ASD2G_P], s->dsc, s->st);
-    launch_update_vel(g, s->M, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->f[ASD2G_PS], ls, s->f[ASD2G_H],
-                      s->f[ASD2G_KAPPA], s->f[ASD2G_U], s->f[ASD2G_V], s->dsc, s->st);
-    launch_update_dt(g, s->M, s->f[ASD2G_U], s->f[ASD2G_V], s->partial, s->counter, s->dsc + 1, s->st);
+    enqueue_step_post(s);
     cudaMemcpyAsync(s->dsc_host, s->dsc, sizeof(double) * 7, cudaMemcpyDeviceToHost, s->st);
     rc = sync(s);
     if (rc) return rc;
@@ -1125,6 +1208,292 @@ int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver
     s->last_volume[0] = s->dsc_host[5];
     s->last_volume[1] = s->dsc_host[6];
     return st;
+}
+
+// ---- checkpoint / restart ----
+namespace {
+struct CkHeader {
+    char magic[8];
+    uint32_t version, header_bytes;
+    int32_t nx, ny, nbc, precision;
+    double t, dt;
+    int64_t step;
+    uint32_t nfields, field_bits;
+    uint64_t payload_bytes, checksum;
+    uint8_t reserved[48];
+};
+static_assert(sizeof(CkHeader) == 128, "checkpoint header is 128 bytes");
+constexpr char CK_MAGIC[8] = {'A', 'S', 'D', '2', 'G', 'C', 'K', '1'};
+constexpr int CK_FIELDS[5] = {ASD2G_LS, ASD2G_U, ASD2G_V, ASD2G_PS, ASD2G_P};
+
+// Weighted word sum  sum_i w_i (2 i + 1)  mod 2^64 over the payload's 64-bit words.
+uint64_t ck_checksum(const double *data, size_t nwords) {
+    uint64_t h = 0;
+    for (size_t i = 0; i < nwords; i++) {
+        uint64_t w;
+        std::memcpy(&w, data + i, 8);
+        h += w * (2u * (uint64_t)i + 1u);
+    }
+    return h;
+}
+
+// Reads and checks the header; with payload != nullptr also reads the payload.
+int ck_read(const char *path, CkHeader &h, std::vector<double> *payload) {
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(ASD2G_E_IO, "cannot open checkpoint %s", path);
+    int rc = ASD2G_OK;
+    if (std::fread(&h, sizeof h, 1, f) != 1) rc = fail(ASD2G_E_IO, "%s: short header", path);
+    else if (std::memcmp(h.magic, CK_MAGIC, 8) != 0 || h.version != 1 || h.header_bytes != sizeof(CkHeader))
+        rc = fail(ASD2G_E_IO, "%s: not an asd2g checkpoint (magic/version)", path);
+    else if (h.nx < 1 || h.ny < 1 || h.nbc != 3 || h.nfields != 5 ||
+             h.payload_bytes != (uint64_t)h.nfields * (uint64_t)(h.nx + 6) * (uint64_t)(h.ny + 6) * 8u)
+        rc = fail(ASD2G_E_IO, "%s: inconsistent sizes", path);
+    if (!rc) {
+        std::vector<double> buf(h.payload_bytes / 8);
+        if (std::fread(buf.data(), 1, h.payload_bytes, f) != h.payload_bytes)
+            rc = fail(ASD2G_E_IO, "%s: short payload", path);
+        else if (ck_checksum(buf.data(), buf.size()) != h.checksum)
+            rc = fail(ASD2G_E_IO, "%s: checksum mismatch", path);
+        else if (payload)
+            payload->swap(buf);
+    }
+    std::fclose(f);
+    return rc;
+}
+}  // namespace
+
+int asd2g_checkpoint_save(asd2g_session *s, const char *path, double t, long long step, double dt) {
+    if (!s || !path) return fail(ASD2G_E_ARG, "null argument");
+    const size_t G = s->G;
+    std::vector<double> buf(5 * G);
+    for (int k = 0; k < 5; k++)
+        cudaMemcpyAsync(buf.data() + k * G, s->f[CK_FIELDS[k]], sizeof(double) * G, cudaMemcpyDeviceToHost, s->st);
+    int rc = sync(s);
+    if (rc) return rc;
+    CkHeader h{};
+    std::memcpy(h.magic, CK_MAGIC, 8);
+    h.version = 1;
+    h.header_bytes = sizeof(CkHeader);
+    h.nx = s->g.nx;
+    h.ny = s->g.ny;
+    h.nbc = 3;
+    h.precision = s->prm.precision;
+    h.t = t;
+    h.dt = dt;
+    h.step = step;
+    h.nfields = 5;
+    for (int k : CK_FIELDS) h.field_bits |= 1u << k;
+    h.payload_bytes = sizeof(double) * buf.size();
+    h.checksum = ck_checksum(buf.data(), buf.size());
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(ASD2G_E_IO, "cannot create checkpoint %s", path);
+    const bool ok = std::fwrite(&h, sizeof h, 1, f) == 1 && std::fwrite(buf.data(), 1, h.payload_bytes, f) == h.payload_bytes;
+    const bool closed = std::fclose(f) == 0;
+    return ok && closed ? ASD2G_OK : fail(ASD2G_E_IO, "writing checkpoint %s failed", path);
+}
+
+int asd2g_checkpoint_load(asd2g_session *s, const char *path, double *t, long long *step, double *dt) {
+    if (!s || !path) return fail(ASD2G_E_ARG, "null argument");
+    CkHeader h{};
+    std::vector<double> buf;
+    int rc = ck_read(path, h, &buf);
+    if (rc) return rc;
+    if (h.nx != s->g.nx || h.ny != s->g.ny)
+        return fail(ASD2G_E_ARG, "checkpoint grid %d x %d does not match the session's %d x %d", h.nx, h.ny, s->g.nx,
+                    s->g.ny);
+    const size_t G = s->G;
+    for (int k = 0; k < 5; k++)
+        cudaMemcpyAsync(s->f[CK_FIELDS[k]], buf.data() + k * G, sizeof(double) * G, cudaMemcpyHostToDevice, s->st);
+    rc = sync(s);  // the host buffer must outlive the copies
+    if (rc) return rc;
+    s->assembled = false;
+    if (t) *t = h.t;
+    if (step) *step = h.step;
+    if (dt) *dt = h.dt;
+    return cuda_check("checkpoint load");
+}
+
+int asd2g_checkpoint_info(const char *path, int *nx, int *ny, double *t, long long *step, double *dt) {
+    if (!path) return fail(ASD2G_E_ARG, "null argument");
+    CkHeader h{};
+    const int rc = ck_read(path, h, nullptr);
+    if (rc) return rc;
+    if (nx) *nx = h.nx;
+    if (ny) *ny = h.ny;
+    if (t) *t = h.t;
+    if (step) *step = h.step;
+    if (dt) *dt = h.dt;
+    return ASD2G_OK;
+}
+
+// ---- device-resident multi-step run ----
+// One droplet step with the MG-FCG as a CUDA graph: the solver's iterations
+// are the body of a WHILE conditional node (8 iterations + the FP64 check per
+// pass; a kernel at the end of the body clears the condition once the solve
+// is done, or after ceil(maxit / 8) + 2 passes), and the whole step is the
+// body of an IF node that skips it once an earlier step failed.  The host
+// launches the step graph n times and synchronises once.
+static int capture_run_graph(asd2g_session *s, int reinit_mode, double tol, int maxit) {
+    for (cudaStream_t &a : s->aux_st)
+        if (!a && cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking) != cudaSuccess) return cuda_check("aux stream");
+    const cudaStream_t main_st = s->st;
+    const int cap = (maxit + 7) / 8 + 2;
+    cudaGraph_t graph = nullptr;
+    int rc = ASD2G_OK;
+    auto add_conditional = [&](cudaStream_t st, cudaGraphConditionalNodeType type, cudaGraphConditionalHandle *h,
+                               cudaGraph_t *body) -> bool {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t cg = nullptr;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &ndeps) != cudaSuccess ||
+            cs != cudaStreamCaptureStatusActive)
+            return false;
+        if (cudaGraphConditionalHandleCreate(h, cg, 1, cudaGraphCondAssignDefault) != cudaSuccess) return false;
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = *h;
+        np.conditional.type = type;
+        np.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        if (cudaGraphAddNode(&node, cg, deps, ndeps, &np) != cudaSuccess) return false;
+        *body = np.conditional.phGraph_out[0];
+        return cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies) == cudaSuccess;
+    };
+    if (cudaStreamBeginCapture(main_st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return cuda_check("capture");
+    cudaGraphConditionalHandle h_if = 0, h_while = 0;
+    cudaGraph_t if_body = nullptr, while_body = nullptr;
+    bool ok = true;
+    {
+        // the handle must exist before the kernel that sets it is captured: create it on the capture graph
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t cg = nullptr;
+        ok = cudaStreamGetCaptureInfo(main_st, &cs, nullptr, &cg, nullptr, nullptr) == cudaSuccess &&
+             cudaGraphConditionalHandleCreate(&h_if, cg, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+        if (ok) launch_run_if(s->run_stats, h_if, main_st);
+        if (ok) {
+            const cudaGraphNode_t *deps = nullptr;
+            size_t ndeps = 0;
+            ok = cudaStreamGetCaptureInfo(main_st, &cs, nullptr, &cg, &deps, &ndeps) == cudaSuccess;
+            cudaGraphNodeParams np{};
+            np.type = cudaGraphNodeTypeConditional;
+            np.conditional.handle = h_if;
+            np.conditional.type = cudaGraphCondTypeIf;
+            np.conditional.size = 1;
+            cudaGraphNode_t node = nullptr;
+            if (ok) ok = cudaGraphAddNode(&node, cg, deps, ndeps, &np) == cudaSuccess;
+            if (ok) if_body = np.conditional.phGraph_out[0];
+            if (ok) ok = cudaStreamUpdateCaptureDependencies(main_st, &node, 1, cudaStreamSetCaptureDependencies) ==
+                         cudaSuccess;
+        }
+    }
+    // IF body: the whole step, captured on the first auxiliary stream
+    if (ok) ok = cudaStreamBeginCaptureToGraph(s->aux_st[0], if_body, nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+        s->st = s->aux_st[0];
+        rc = enqueue_step_pre(s, reinit_mode);
+        if (!rc) {
+            launch_set_kstate(s->ks, tol, maxit, ASD2G_SOLVER_MGPCG, 0.0, s->st);
+            launch_mg_setup(s->sys, s->lv, s->nlev, s->coarse_inv, s->st);
+            if (!launch_fcg_init(s->sys, s->g.nx, s->g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->pa, s->q,
+                                 s->z, s->ks, s->mg_partial, s->mg_partial_n, s->st))
+                rc = fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
+        }
+        if (!rc) ok = add_conditional(s->st, cudaGraphCondTypeWhile, &h_while, &while_body);
+        // WHILE body: 8 iterations + the FP64 check, then the loop condition
+        if (!rc && ok)
+            ok = cudaStreamBeginCaptureToGraph(s->aux_st[1], while_body, nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (!rc && ok) {
+            s->st = s->aux_st[1];
+            if (!enqueue_iters(s, ASD2G_SOLVER_MGPCG, 8)) rc = fail(ASD2G_E_UNSUPPORTED, "multigrid buffer too small");
+            launch_run_while(s->ks, s->run_stats, cap, h_while, s->st);
+            cudaGraph_t wb = nullptr;
+            ok = cudaStreamEndCapture(s->aux_st[1], &wb) == cudaSuccess;
+            s->st = s->aux_st[0];
+        }
+        if (!rc && ok) {
+            enqueue_step_post(s);
+            launch_run_step_end(s->ks, s->run_stats, tol, s->dsc, s->st);
+        }
+        cudaGraph_t ib = nullptr;
+        const bool ended = cudaStreamEndCapture(s->aux_st[0], &ib) == cudaSuccess;
+        ok = ok && ended;
+        s->st = main_st;
+    }
+    const bool ended = cudaStreamEndCapture(main_st, &graph) == cudaSuccess;
+    s->st = main_st;
+    if (rc || !ok || !ended) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return rc ? rc : fail(ASD2G_E_CUDA, "capture of the device-resident step failed");
+    }
+    if (s->run_exec) cudaGraphExecDestroy(s->run_exec);
+    s->run_exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&s->run_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ASD2G_E_CUDA, "instantiating the device-resident step: %s", cudaGetErrorString(e));
+    }
+    s->run_reinit = reinit_mode;
+    s->run_tol = tol;
+    s->run_maxit = maxit;
+    return ASD2G_OK;
+}
+
+int asd2g_run_steps(asd2g_session *s, int nsteps, double *dt, int reinit_mode, int solver, double tol, int maxit,
+                    int *steps_done, long long *iters_total, double *max_resid) {
+    if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
+    if (nsteps < 0) return fail(ASD2G_E_ARG, "nsteps must be >= 0");
+    if (solver != ASD2G_SOLVER_MGPCG)
+        return fail(ASD2G_E_UNSUPPORTED, "the device-resident loop runs the MG-FCG pressure solver only");
+    if (maxit < 1 || !(tol >= 0.0)) return fail(ASD2G_E_ARG, "maxit must be >= 1 and tol >= 0");
+    if (reinit_mode < 0 || reinit_mode > 4) return fail(ASD2G_E_ARG, "reinit mode %d out of range", reinit_mode);
+    int rc = p_supported(s);
+    if (!rc) rc = mg_alloc(s);
+    if (rc) return rc;
+    if (stream_capturing(s)) return fail(ASD2G_E_UNSUPPORTED, "asd2g_run_steps inside a caller's stream capture");
+    if (!s->run_stats) {
+        if (cudaMalloc(&s->run_stats, sizeof(RunStats)) != cudaSuccess ||
+            cudaMallocHost(&s->run_stats_host, sizeof(RunStats)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ASD2G_E_NOMEM, "run statistics");
+        }
+        s->allocs.push_back(s->run_stats);
+    }
+    if (!s->run_exec || s->run_reinit != reinit_mode || s->run_tol != tol || s->run_maxit != maxit) {
+        // one eager step's worth of set-up first: attributes and first-use state outside the capture
+        launch_run_reset(s->run_stats, s->st);
+        rc = capture_run_graph(s, reinit_mode, tol, maxit);
+        if (rc) return rc;
+    }
+    rc = set_dt(s, *dt);
+    if (rc) return rc;
+    launch_run_reset(s->run_stats, s->st);
+    for (int k = 0; k < nsteps; k++)
+        if (cudaGraphLaunch(s->run_exec, s->st) != cudaSuccess) return cuda_check("step graph launch");
+    cudaMemcpyAsync(s->run_stats_host, s->run_stats, sizeof(RunStats), cudaMemcpyDeviceToHost, s->st);
+    cudaMemcpyAsync(s->dsc_host, s->dsc, sizeof(double) * 7, cudaMemcpyDeviceToHost, s->st);
+    rc = sync(s);
+    if (rc) return rc;
+    rc = cuda_check("run_steps");
+    if (rc) return rc;
+    const RunStats &R = *s->run_stats_host;
+    if (steps_done) *steps_done = R.fail_step >= 0 ? R.fail_step + 1 : R.steps;
+    if (iters_total) *iters_total = R.iters;
+    if (max_resid) *max_resid = R.max_res;
+    *dt = s->dsc_host[0];  // the next step's dt (copied from dsc[1] at each step's end)
+    s->last_volume[0] = s->dsc_host[5];
+    s->last_volume[1] = s->dsc_host[6];
+    s->assembled = true;
+    if (R.fail_step >= 0) {
+        if (R.fail_status == -5) return fail(ASD2G_E_NONFINITE, "non-finite value at step %d", R.fail_step);
+        if (R.fail_status == -6) return fail(ASD2G_E_BREAKDOWN, "Krylov breakdown at step %d", R.fail_step);
+        return ASD2G_NOT_CONVERGED;
+    }
+    return ASD2G_OK;
 }
 
 }  // extern "C"

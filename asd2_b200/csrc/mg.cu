@@ -1118,7 +1118,6 @@ void launch_mg_setup(const Sys &S, MgLevel *lv, int nlev, double *coarse_inv, cu
         k_mg_coarsen<<<red_blocks(n), 256, 0, st>>>(lv[l - 1], lv[l]);
     }
     const size_t smem = sizeof(double) * (MG_COARSE_MAX * 2 * MG_COARSE_MAX + MG_COARSE_MAX);
-    cudaFuncSetAttribute(k_mg_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_mg_coarse_invert<<<1, MG_INV_THREADS, smem, st>>>(lv[nlev - 1], coarse_inv);
 }
 
@@ -1147,6 +1146,11 @@ int mg_cta_first_level(const MgLevel *lv, int nlev) { return mg_cta_level(lv, nl
 // process-wide, so it must cover every session's hierarchy).
 constexpr size_t MG_CTA_SMEM_BOUND = 5 * sizeof(float) * 2 * (size_t)MG_CTA_CELLS;
 bool mg_cta_prepare(const MgLevel *lv, int nlev) {
+    // process-wide attributes, set when a hierarchy is allocated (before any stream capture uses them)
+    const size_t inv = sizeof(double) * (MG_COARSE_MAX * 2 * MG_COARSE_MAX + MG_COARSE_MAX);
+    if (cudaFuncSetAttribute(k_mg_coarse_invert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv) !=
+        cudaSuccess)
+        return false;
     MgHier H{};
     for (int l = 0; l < nlev; l++) H.l[l] = lv[l];
     if (mg_cta_smem(H, mg_cta_level(lv, nlev), nlev) > MG_CTA_SMEM_BOUND) return false;

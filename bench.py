@@ -222,6 +222,23 @@ def mixed_precision_errors(sh):
         res[prec] = dict(ls=ss.download("ls")[3:-3, 3:-3], p=ss.download("p")[3:-3, 3:-3], t=el, its=its,
                          vol0=vol0, vol=ss.last_volume())
         ss.close()
+    # the same mixed run device-resident: one graph per step, one synchronisation
+    ss = api.Session(api.Params.from_case(c, precision=api.PRECISION_MIXED), stream=sh)
+    ss.upload("ls", c.ls)
+    ss.upload("u", c.u)
+    ss.upload("v", c.v)
+    ss.apply_bc("ls", "P")
+    dt = ss.update_dt()
+    ss.run_steps(0, dt, reinit_mode=api.REINIT_MINRK2, tol=1e-10, maxit=500000)  # builds the step graph
+    ss.sync()
+    t0 = time.perf_counter()
+    r = ss.run_steps(CFG3_STEPS, dt, reinit_mode=api.REINIT_MINRK2, tol=1e-10, maxit=500000)
+    t_dev = time.perf_counter() - t0
+    if r["status"] != 0:
+        raise SystemExit(f"bench: device-resident run failed: {r}")
+    same = bool(np.array_equal(ss.download("ls")[3:-3, 3:-3], res[api.PRECISION_MIXED]["ls"]) and
+                np.array_equal(ss.download("p")[3:-3, 3:-3], res[api.PRECISION_MIXED]["p"]))
+    ss.close()
     a, b = res[api.PRECISION_MIXED], res[api.PRECISION_FP64]
     err = {}
     for k in ("ls", "p"):
@@ -233,7 +250,8 @@ def mixed_precision_errors(sh):
             "error_vs_fp64": err,
             "volume_rel_change": {"fp64": (b["vol"][1] - b["vol0"][1]) / b["vol0"][1],
                                   "mixed": (a["vol"][1] - a["vol0"][1]) / a["vol0"][1]},
-            "seconds": {"fp64": b["t"], "mixed": a["t"]},
+            "seconds": {"fp64": b["t"], "mixed": a["t"], "mixed_device_resident": t_dev},
+            "device_resident_identical": same,
             "pressure_iterations": {"fp64_jacobi_pcg": b["its"], "mixed_mg_fcg": a["its"]}}
 
 

@@ -35,6 +35,7 @@ extern "C" {
 #define ASD2G_E_UNSUPPORTED (-4)  /* configuration outside the implemented path */
 #define ASD2G_E_NONFINITE (-5)    /* NaN/Inf detected (the reference exit(1)s) */
 #define ASD2G_E_BREAKDOWN (-6)    /* Krylov breakdown (zero denominator) */
+#define ASD2G_E_IO (-7)           /* checkpoint file: open/read/write failed, or not a valid checkpoint */
 
 /* ---- boundary kinds: same values as enum class BC2D (include/common.h:4) ---- */
 enum asd2g_bc {
@@ -354,6 +355,41 @@ int asd2g_pc_training_pair_at(asd2g_session *s, int iters, void *feats, void *ta
  * new dt.  *dt is read as the step's dt and receives the next one. */
 int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver, double tol, int maxit,
                        int *iters, double *rel_resid);
+
+/* ---- device-resident multi-step run (no reference counterpart: the
+ * driver loop of test_mac2d_large.cpp:496-552 without host round trips) ----
+ * nsteps droplet steps as one CUDA graph per step, launched back to back
+ * with a single synchronisation at the end: the MG-FCG iterations run in a
+ * device-side WHILE loop (graph conditional node) and dt passes from one step
+ * to the next on the device.  solver must be ASD2G_SOLVER_MGPCG.  *dt is the
+ * first step's dt and receives the next one.  A step whose solve fails (or
+ * whose next dt is not positive and finite) ends the run: later steps are
+ * skipped on the device, *steps_done counts the steps executed including the
+ * failed one, and the status is that step's (ASD2G_NOT_CONVERGED,
+ * ASD2G_E_NONFINITE, ASD2G_E_BREAKDOWN).  iters_total / max_resid (may be
+ * NULL): iterations summed over the steps, largest final relative residual.
+ * The step's results are bit-identical to asd2g_droplet_step with the same
+ * arguments. */
+int asd2g_run_steps(asd2g_session *s, int nsteps, double *dt, int reinit_mode, int solver, double tol, int maxit,
+                    int *steps_done, long long *iters_total, double *max_resid);
+
+/* ---- checkpoint / restart (no reference counterpart: the reference writes
+ * Tecplot output only) ----
+ * A raw binary file: a 128-byte little-endian header
+ *   char magic[8] = "ASD2GCK1"; u32 version = 1; u32 header_bytes = 128;
+ *   i32 nx, ny, nbc (= 3), precision; f64 t, dt; i64 step;
+ *   u32 nfields, field_bits (bit f set for each field id stored);
+ *   u64 payload_bytes; u64 checksum; zero padding
+ * then the fields LS, U, V, PS, P in that order, each the padded
+ * (nx+6) x (ny+6) FP64 array of the session layout.  checksum = sum over the
+ * payload's little-endian 64-bit words w_i of w_i (2 i + 1), mod 2^64.  Enough to restart a
+ * run (with t, step and the next dt) and to hand fields between processes.
+ * save: writes the session's current fields.  load: checks magic, version,
+ * sizes (nx, ny must match the session) and checksum, then replaces the
+ * fields.  info: reads and verifies a file without a session (no GPU needed). */
+int asd2g_checkpoint_save(asd2g_session *s, const char *path, double t, long long step, double dt);
+int asd2g_checkpoint_load(asd2g_session *s, const char *path, double *t, long long *step, double *dt);
+int asd2g_checkpoint_info(const char *path, int *nx, int *ny, double *t, long long *step, double *dt);
 
 /* ---- allocation-free solve (no counterpart in the reference) ----
  * Jacobi-PCG (textbook recurrence, FP64) on a system the caller has already

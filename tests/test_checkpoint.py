@@ -1,0 +1,62 @@
+"""Checkpoint format (asd2g_checkpoint_*), host side: the numpy writer and
+the library's reader agree on the layout and the checksum, and the reader
+refuses damaged or foreign files.  No GPU needed (asd2g_checkpoint_info only
+reads the file)."""
+import numpy as np
+import pytest
+
+from asd2_b200 import api
+from asd2_b200 import checkpoint as CK
+
+
+def _fields(nx, ny, seed=0):
+    rng = np.random.default_rng(seed)
+    return {k: rng.standard_normal((nx + 6, ny + 6)) for k in CK.FIELDS}
+
+
+def test_numpy_round_trip(tmp_path):
+    f = _fields(20, 12)
+    p = tmp_path / "a.ck"
+    CK.write(p, f, t=0.25, step=7, dt=1e-3)
+    g, meta = CK.read(p)
+    assert meta["nx"] == 20 and meta["ny"] == 12 and meta["step"] == 7 and meta["t"] == 0.25
+    for k in CK.FIELDS:
+        assert np.array_equal(g[k], f[k])
+
+
+def test_library_reads_numpy_checkpoint(tmp_path):
+    p = tmp_path / "b.ck"
+    CK.write(p, _fields(16, 24, seed=3), t=1.5, step=42, dt=2e-4)
+    info = api.checkpoint_info(p)
+    assert info == dict(nx=16, ny=24, t=1.5, step=42, dt=2e-4)
+
+
+@pytest.mark.parametrize("damage", ["payload", "magic", "truncate"])
+def test_library_refuses_damaged_file(tmp_path, damage):
+    p = tmp_path / "c.ck"
+    CK.write(p, _fields(8, 8, seed=5))
+    raw = bytearray(p.read_bytes())
+    if damage == "payload":
+        raw[128 + 8 * 17 + 3] ^= 0x10
+    elif damage == "magic":
+        raw[0:8] = b"NOTACKPT"
+    else:
+        raw = raw[:-8]
+    p.write_bytes(bytes(raw))
+    with pytest.raises(api.Asd2gError) as e:
+        api.checkpoint_info(p)
+    assert e.value.code == -7
+    with pytest.raises(ValueError):
+        CK.read(p)
+
+
+def test_checksum_sees_swapped_words():
+    a = np.arange(1, 9, dtype="<f8").tobytes()
+    b = np.array([2, 1, 3, 4, 5, 6, 7, 8], dtype="<f8").tobytes()
+    assert CK.checksum(a) != CK.checksum(b)
+
+
+def test_missing_file(tmp_path):
+    with pytest.raises(api.Asd2gError) as e:
+        api.checkpoint_info(tmp_path / "nope.ck")
+    assert e.value.code == -7
