@@ -3,6 +3,9 @@
 // grid; every numerical method runs through the asd2g C ABI.
 #include "mac2d.h"
 
+#include <cstdio>
+#include <string>
+
 #include "asd2g.h"
 #include "session.h"
 
@@ -359,8 +362,65 @@ int MACSolver2D::SetPLTType(PLTTYPE type) {
     return 0;
 }
 
-int MACSolver2D::OutRes(const int, const double, const std::string, const std::string, const std::vector<double> &,
-                        const std::vector<double> &, const std::vector<double> &, const std::vector<double> &) {
+namespace {
+// One Tecplot ASCII zone (point packing, x fastest) of the cell-centred
+// interior: a zone line, then per cell "x,y,c0,c1,c2" with the values
+// formatted as an ostream's default double output (%g, 6 significant digits).
+bool write_zone(const std::string &path, bool header, const char *title, const char *vars, int iter, double t,
+                int nx, int ny, int nbc, double base_x, double base_y, double dx, double dy,
+                const std::vector<const std::vector<double> *> &cols) {
+    std::FILE *f = std::fopen(path.c_str(), header ? "w" : "a");
+    if (!f) return false;
+    if (header) std::fprintf(f, "TITLE = %s\nVARIABLES = %s \n", title, vars);
+    std::fprintf(f, "ZONE T=\"%d\", I=%d, J=%d, SOLUTIONTIME=%g, STRANDID=%d\n", iter, nx, ny, t, iter + 1);
+    const int64_t stride = ny + 2 * nbc;
+    std::string line;
+    char num[40];
+    for (int j = nbc; j < ny + nbc; j++)
+        for (int i = nbc; i < nx + nbc; i++) {
+            const int64_t k = j + stride * i;
+            line.clear();
+            std::snprintf(num, sizeof num, "%g", base_x + static_cast<double>(i + 0.5 - nbc) * dx);
+            line += num;
+            std::snprintf(num, sizeof num, ",%g", base_y + static_cast<double>(j + 0.5 - nbc) * dy);
+            line += num;
+            for (const std::vector<double> *c : cols) {
+                std::snprintf(num, sizeof num, ",%g", (*c)[k]);
+                line += num;
+            }
+            line += '\n';
+            std::fputs(line.c_str(), f);
+        }
+    return std::fclose(f) == 0;
+}
+}  // namespace
+
+// Tecplot ASCII output (mac2d.cpp:1990-2063): <vel>_ASCII.plt with X, Y, the
+// face velocities averaged to the cell centres, LS and PS; <div>_ASCII.plt
+// with X, Y, LS, the divergence of (u, v) and PS.  Both files are created
+// with their header when m_iter is 0 and get one zone per call.  The binary
+// .szplt output needs the closed TecIO library and is not written.
+int MACSolver2D::OutRes(const int iter, const double curTime, const std::string fname_vel_base,
+                        const std::string fname_div_base, const std::vector<double> &u, const std::vector<double> &v,
+                        const std::vector<double> &ps, const std::vector<double> &ls) {
+    if (m_PLTType != PLTTYPE::ASCII && m_PLTType != PLTTYPE::BOTH) return 0;
+    const int nbc = kNumBCGrid;
+    const int64_t stride = kNy + 2 * nbc;
+    std::vector<double> uc(kArrSize, 0.0), vc(kArrSize, 0.0);
+    for (int i = nbc; i < kNx + nbc; i++)
+        for (int j = nbc; j < kNy + nbc; j++) {
+            const int64_t k = j + stride * i;
+            uc[k] = (u[k] + u[k + stride]) * 0.5;
+            vc[k] = (v[k] + v[k + 1]) * 0.5;
+        }
+    const std::vector<double> div = GetDivergence(u, v);
+    const bool header = m_iter == 0;
+    const bool ok =
+        write_zone(fname_vel_base + "_ASCII.plt", header, "VEL", "\"X\", \"Y\", \"U\", \"V\", \"LS\", \"PS\"", iter,
+                   curTime, kNx, kNy, nbc, kBaseX, kBaseY, kDx, kDy, {&uc, &vc, &ls, &ps}) &&
+        write_zone(fname_div_base + "_ASCII.plt", header, "DIV", "\"X\", \"Y\", \"LS\", \"DIV\", \"PS\"", iter,
+                   curTime, kNx, kNy, nbc, kBaseX, kBaseY, kDx, kDy, {&ls, &div, &ps});
+    if (!ok) perror("MACSolver2D::OutRes");
     return 0;
 }
 

@@ -1,7 +1,7 @@
 // MACSolver2D with the interface of the reference's include/mac2d.h
 // (mac2d.h:31-168).  The momentum, GFM pressure and projection work runs on
-// the B200 through the asd2g C ABI.  Tecplot output (OutRes) is not part of
-// this build: it records the requested type and writes nothing.
+// the B200 through the asd2g C ABI.  OutRes writes the Tecplot ASCII files
+// (PLTTYPE::ASCII / BOTH); the binary .szplt output (closed TecIO) is not written.
 #ifndef __MAC2D_H_
 #define __MAC2D_H_
 

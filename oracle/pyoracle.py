@@ -363,6 +363,8 @@ class Reference:
             ("ref_mac_rhs", [V, _dp, _dp, _dp, _dp, _dp, _dp], None),
             ("ref_mac_intermediate", [V, _dp, _dp, _dp, _dp, _dp, _dp], None),
             ("ref_mac_div", [V, _dp, _dp, _dp], None),
+            ("ref_mac_outres", [V, C.c_int, C.c_int, C.c_double, C.c_char_p, C.c_char_p, _dp, _dp, _dp, _dp],
+             C.c_int),
             ("ref_mac_poisson", [V, _dp, _dp, _dp, _dp, _dp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                  C.POINTER(C.c_int)], C.c_int),
             ("ref_capture_copy", [_dp, _ip, _ip, _dp], C.c_int),
@@ -415,6 +417,11 @@ class Reference:
     def reinit(self, mode, ls):
         self.L.ref_reinit(self.h, mode, ls)
         return ls
+
+    def outres(self, m_iter, it, t, vel_base, div_base, u, v, ps, ls):
+        """MACSolver2D::OutRes (Tecplot ASCII) into <base>_ASCII.plt."""
+        return self.L.ref_mac_outres(self.h, m_iter, it, t, os.fsencode(vel_base), os.fsencode(div_base), u, v, ps,
+                                     ls)
 
     def _u(self, name, *arrs):
         out = self.z()

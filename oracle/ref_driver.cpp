@@ -251,6 +251,14 @@ void ref_mac_div(void *h, const double *u, const double *v, double *div) {
     RefCtx *c = static_cast<RefCtx *>(h);
     vout(c, c->mac->GetDivergence(vin(c, u), vin(c, v)), div);
 }
+// MACSolver2D::OutRes with PLTTYPE::ASCII; m_iter (0 writes the file headers) set first.
+int ref_mac_outres(void *h, int m_iter, int iter, double t, const char *vel_base, const char *div_base,
+                   const double *u, const double *v, const double *ps, const double *ls) {
+    RefCtx *c = static_cast<RefCtx *>(h);
+    c->mac->SetPLTType(PLTTYPE::ASCII);
+    c->mac->m_iter = m_iter;
+    return c->mac->OutRes(iter, t, vel_base, div_base, vin(c, u), vin(c, v), vin(c, ps), vin(c, ls));
+}
 // Runs MACSolver2D::SolvePoisson with maxiter iterations of the reference CG
 // and the capture hook armed.  Writes the solver's ps (and m_p) back, and
 // returns the captured system sizes in m/nnz/nb (-1 if nothing was captured).

@@ -21,14 +21,15 @@ from tests.helpers import assert_bitexact, assert_close, fluid_from_case, grid_f
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DRIVER = os.path.join(HERE, "dropin", "droplet_driver.cpp")
+OUTRES_DRIVER = os.path.join(HERE, "dropin", "outres_driver.cpp")
 
 
-def _compile(tmp_path):
+def _compile(tmp_path, src=DRIVER):
     if not os.path.exists(B.LIB):
         pytest.skip("libasd2g.so not built")
     B.build_dropin()
-    exe = os.path.join(str(tmp_path), "droplet_driver")
-    cmd = [B.gxx(), "-std=c++17", "-O2", "-Wall", "-I", os.path.join(B.ROOT, "include"), "-I", B.DROPIN, DRIVER,
+    exe = os.path.join(str(tmp_path), os.path.splitext(os.path.basename(src))[0])
+    cmd = [B.gxx(), "-std=c++17", "-O2", "-Wall", "-I", os.path.join(B.ROOT, "include"), "-I", B.DROPIN, src,
            "-o", exe, "-L", B.HERE, "-lasd2_dropin", "-lasd2g", f"-Wl,-rpath,{B.HERE}"]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
     return exe
@@ -139,3 +140,42 @@ def test_driver_droplet_steps_bicgstab(tmp_path):
     assert_close(v, vp, 0.0, 1e-12 * np.abs(vp).max(), "v from the driver's pressure")
     assert all(e <= 1e-6 for e in errs), errs
     assert all(np.isfinite(o[4]) and o[4] > 0 for o in out)
+
+
+@pytest.mark.gpu
+def test_outres_ascii_matches_reference_bytes(tmp_path):
+    """MACSolver2D::OutRes with PLTTYPE::ASCII writes the same two Tecplot
+    files, byte for byte, as the reference's own OutRes (mac2d.cpp:1990)
+    compiled unmodified: header on m_iter 0, one zone per call, cell-centred
+    velocities, the divergence, default ostream number formatting."""
+    from oracle.pyoracle import REF_SO, Reference
+    if not os.path.exists(REF_SO):
+        pytest.skip("reference library not built")
+    exe = _compile(tmp_path, OUTRES_DRIVER)
+    c = W.droplet(24, seed=3)
+    g, f = grid_from_case(c), fluid_from_case(c)
+    rng = np.random.default_rng(0)
+    zones = []
+    for z in range(2):
+        zones.append((0.125 * z + 1e-7, rng.standard_normal(c.ls.shape), rng.standard_normal(c.ls.shape),
+                      1e3 * rng.standard_normal(c.ls.shape), c.ls + 0.01 * z))
+    case = os.path.join(str(tmp_path), "outres.bin")
+    with open(case, "wb") as fh:
+        np.array([g.nx, g.ny, len(zones)], dtype=np.int32).tofile(fh)
+        np.array([0.25, -0.5, g.nx * g.dx, g.ny * g.dy]).tofile(fh)
+        for t, u, v, ps, ls in zones:
+            np.array([t]).tofile(fh)
+            for a in (u, v, ps, ls):
+                np.ascontiguousarray(a, dtype=np.float64).tofile(fh)
+    ours = [os.path.join(str(tmp_path), "ours_vel"), os.path.join(str(tmp_path), "ours_div")]
+    r = subprocess.run([exe, case] + ours, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    ref = Reference(g, f, base_x=0.25, base_y=-0.5)
+    theirs = [os.path.join(str(tmp_path), "ref_vel"), os.path.join(str(tmp_path), "ref_div")]
+    for z, (t, u, v, ps, ls) in enumerate(zones):
+        ref.outres(z, z, t, theirs[0], theirs[1], *(np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, ps, ls)))
+    ref.close()
+    for a, b in zip(ours, theirs):
+        mine, want = open(a + "_ASCII.plt", "rb").read(), open(b + "_ASCII.plt", "rb").read()
+        assert mine.count(b"ZONE") == 2
+        assert mine == want
