@@ -67,6 +67,7 @@ EXPORTS = [
     "asd2g_apply_bc_side", "asd2g_update_ntk", "asd2g_csr_solve", "asd2g_volume", "asd2g_last_volume",
     "asd2g_batch_create", "asd2g_batch_destroy", "asd2g_batch_upload", "asd2g_batch_download",
     "asd2g_batch_field_ptr", "asd2g_batch_offset", "asd2g_batch_assemble", "asd2g_batch_solve", "asd2g_batch_sync",
+    "asd2g_batch_step", "asd2g_batch_volume",
     "asd2g_conv_wpack_bytes", "asd2g_conv_pack_weights", "asd2g_conv3x3_bf16",
     "asd2g_unet_create", "asd2g_unet_destroy", "asd2g_unet_nparams", "asd2g_unet_init", "asd2g_unet_set_params",
     "asd2g_unet_get_params", "asd2g_unet_get_grads", "asd2g_unet_forward", "asd2g_unet_train_step",
@@ -132,6 +133,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_batch_offset": ([S, I, C.POINTER(C.c_size_t)], I),
         "asd2g_batch_assemble": ([S, dp], I),
         "asd2g_batch_solve": ([S, D, I, ip, dp], I),
+        "asd2g_batch_step": ([S, dp, I, D, I, ip, dp], I),
+        "asd2g_batch_volume": ([S, dp, dp], I),
         "asd2g_conv_wpack_bytes": ([I, I], C.c_size_t),
         "asd2g_conv_pack_weights": ([C.c_void_p, I, I, I, I, C.c_void_p, C.c_void_p], I),
         "asd2g_conv3x3_bf16": ([C.c_void_p, I, I, I, I, C.c_void_p, C.c_void_p, I, C.c_void_p, C.c_void_p, I,
@@ -486,6 +489,22 @@ class Batch:
         it, res = np.zeros(n, np.int32), np.zeros(n)
         rc = self._check(self.L.asd2g_batch_solve(self.h, tol, maxit, it, res))
         return dict(status=rc, iters=it, resid=res)
+
+    def step(self, dts, reinit_mode=REINIT_MINRK2, tol=1e-10, maxit=10000):
+        """One full droplet step of every instance (MG-FCG pressure solve);
+        returns dict(status, dt_next[count], iters[count], resid[count])."""
+        n = len(self.params)
+        d = np.array(dts, dtype=np.float64).copy()
+        it, res = np.zeros(n, np.int32), np.zeros(n)
+        rc = self._check(self.L.asd2g_batch_step(self.h, d, reinit_mode, tol, maxit, it, res))
+        return dict(status=rc, dt_next=d, iters=it, resid=res)
+
+    def volume(self):
+        """(sharp, smooth) FP64 volume of every instance after the last step."""
+        n = len(self.params)
+        a, b = np.zeros(n), np.zeros(n)
+        self._check(self.L.asd2g_batch_volume(self.h, a, b))
+        return a, b
 
     def sync(self):
         self._check(self.L.asd2g_batch_sync(self.h))

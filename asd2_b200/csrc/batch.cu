@@ -17,6 +17,8 @@
 namespace asd2g {
 int api_fail(int code, const char *msg);
 int api_grid_from_params(const asd2g_params *p, Grid &g, MomConst &M);
+LsConst make_lsconst(const Grid &g);              // levelset.cu
+int reinit_steps(double adt, double max_atime);  // levelset.cu
 }  // namespace asd2g
 
 using namespace asd2g;
@@ -30,10 +32,12 @@ struct asd2g_batch {
     BInst *dinst = nullptr;
     std::vector<size_t> goff;  // padded-field offset of each instance
     size_t gtot = 0;
-    double *pad = nullptr;     // 6 padded fields x gtot: LS, KAPPA, H, DIV, PS, P
+    double *pad = nullptr;     // BS_COUNT padded fields x gtot (BSlot order)
+    double *sc = nullptr;      // 8 scalars per instance (BInst::sc)
     BTile *cell_tiles = nullptr;
     int ncell_tiles = 0;
     BatchPlan plan{};
+    BStepPlan splan{};
     KState *ks = nullptr;
     KState *ks_host = nullptr;
     cudaGraphExec_t chunk_exec = nullptr;
@@ -43,16 +47,24 @@ struct asd2g_batch {
 namespace {
 
 constexpr int FCG_CHUNK_ITERS = 8;
-constexpr int PAD_FIELDS = 6;
+constexpr int PAD_FIELDS = BS_COUNT;
+constexpr int SC_PER_INST = 8;
 
 int pad_slot(int field) {
     switch (field) {
-    case ASD2G_LS: return 0;
-    case ASD2G_KAPPA: return 1;
-    case ASD2G_H: return 2;
-    case ASD2G_DIV: return 3;
-    case ASD2G_PS: return 4;
-    case ASD2G_P: return 5;
+    case ASD2G_LS: return BS_LS;
+    case ASD2G_KAPPA: return BS_KAPPA;
+    case ASD2G_H: return BS_H;
+    case ASD2G_DIV: return BS_DIV;
+    case ASD2G_PS: return BS_PS;
+    case ASD2G_P: return BS_P;
+    case ASD2G_U: return BS_U;
+    case ASD2G_V: return BS_V;
+    case ASD2G_HS: return BS_HS;
+    case ASD2G_UHAT: return BS_UHAT;
+    case ASD2G_VHAT: return BS_VHAT;
+    case ASD2G_LSB: return BS_LSB;
+    case ASD2G_LS0: return BS_LS0;
     default: return -1;
     }
 }
@@ -129,6 +141,7 @@ int build(asd2g_batch *b) {
     if (!rc) rc = balloc(b, &partial, ptot);
     if (!rc) rc = balloc(b, &inv, (size_t)count * MG_COARSE_CELLS * MG_COARSE_CELLS);
     if (!rc) rc = balloc(b, &b->ks, (size_t)count);
+    if (!rc) rc = balloc(b, &b->sc, (size_t)SC_PER_INST * count);
     std::vector<float *> mg_base(MG_MAX_LEVELS, nullptr);
     for (int l = 0; l < MG_MAX_LEVELS && !rc; l++)
         if (mg_cells[l]) rc = balloc(b, &mg_base[l], 6 * mg_cells[l]);
@@ -137,6 +150,8 @@ int build(asd2g_batch *b) {
         return api_fail(ASD2G_E_NOMEM, "pinned allocation failed");
     cudaMemsetAsync(b->pad, 0, sizeof(double) * PAD_FIELDS * b->gtot, b->st);
     cudaMemsetAsync(vec, 0, sizeof(double) * NVEC * ntot, b->st);
+    cudaMemsetAsync(b->sc, 0, sizeof(double) * SC_PER_INST * count, b->st);
+    cudaMemsetAsync(b->ks, 0, sizeof(KState) * count, b->st);  // tickets start at 0
     std::vector<size_t> mg_used(MG_MAX_LEVELS, 0);
     for (int i = 0; i < count; i++) {
         BInst &I = b->hinst[i];
@@ -147,6 +162,22 @@ int build(asd2g_batch *b) {
         I.div = b->pad + 3 * G + go;
         I.ps = b->pad + 4 * G + go;
         I.p = b->pad + 5 * G + go;
+        I.pad0 = b->pad + go;
+        I.gstride = G;
+        I.sc = b->sc + (size_t)SC_PER_INST * i;
+        I.K = make_lsconst(I.g);
+        I.ddx = make_divh(I.g.dx);
+        I.ddy = make_divh(I.g.dy);
+        I.d2x = make_divh(2.0 * I.g.dx);
+        I.d2y = make_divh(2.0 * I.g.dy);
+        const double hmin = I.g.dx < I.g.dy ? I.g.dx : I.g.dy;
+        I.kappa_lim = 1.0 / hmin;
+        I.hs_eps = hmin * 1.5;
+        {
+            const asd2g_params &pp = b->prm[i];
+            const double we = pp.numbers_given ? pp.we : pp.rho_h / pp.sigma;
+            I.kappa_fill = (we != 0.0 && std::isfinite(we)) ? 1 : 0;
+        }
         double *v = vec + noff[i];
         double **slots[NVEC] = {&I.S.diag, &I.S.cw, &I.S.ce, &I.S.cs, &I.S.cn, &I.S.minv, &I.S.b,
                                 &I.x, &I.r, &I.pa, &I.pb, &I.q, &I.z};
@@ -155,7 +186,6 @@ int build(asd2g_batch *b) {
         I.ks = b->ks + i;
         I.partial = partial + poff[i];
         I.coarse_inv = inv + (size_t)i * MG_COARSE_CELLS * MG_COARSE_CELLS;
-        I.dt = 1.0;
         const int *d = &dims[2 * MG_MAX_LEVELS * (size_t)i];
         for (int l = 0; l < I.nlev; l++) {
             MgLevel &L = I.lv[l];
@@ -177,7 +207,7 @@ int build(asd2g_batch *b) {
         if (mg_cells[l]) cudaMemsetAsync(mg_base[l], 0, sizeof(float) * 6 * mg_cells[l], b->st);
     // work lists
     std::vector<BTile> cells;
-    std::vector<BChunk> chunks;
+    std::vector<BChunk> chunks, padc, ghostc;
     std::vector<std::vector<BChunk>> lvl(MG_MAX_LEVELS);
     std::vector<std::vector<BTile>> mgt(MG_MAX_LEVELS);
     int max_s = 0, max_nlev = 0;
@@ -187,6 +217,9 @@ int build(asd2g_batch *b) {
         for (int by = 0; by < gy; by++)
             for (int bx = 0; bx < gx; bx++) cells.push_back({i, bx, by});
         for (int c = 0; c < I.chunks; c++) chunks.push_back({i, c});
+        const int64_t gi = (int64_t)I.g.sx * I.g.sy, ei = 2 * (int64_t)NB * (I.g.nx + I.g.ny);
+        for (int c = 0; c < (int)((gi + BSTEP_PAD_CHUNK - 1) / BSTEP_PAD_CHUNK); c++) padc.push_back({i, c});
+        for (int c = 0; c < (int)((ei + BSTEP_GHOST_CHUNK - 1) / BSTEP_GHOST_CHUNK); c++) ghostc.push_back({i, c});
         for (int l = 1; l < I.nlev; l++) {
             const int64_t m = (int64_t)I.lv[l].nx * I.lv[l].ny;
             for (int c = 0; c < (int)((m + FCG_CHUNK - 1) / FCG_CHUNK); c++) lvl[l].push_back({i, c});
@@ -219,6 +252,17 @@ int build(asd2g_batch *b) {
     }
     P.max_s = max_s;
     P.max_nlev = max_nlev;
+    BStepPlan &SP = b->splan;
+    SP.insts = b->dinst;
+    SP.count = count;
+    SP.tiles = b->cell_tiles;
+    SP.ntiles = b->ncell_tiles;
+    SP.chunks = P.chunks;
+    SP.nchunks = P.nchunks;
+    if (!rc) rc = upload_list(b, padc, &SP.pad_chunks);
+    SP.npad = (int)padc.size();
+    if (!rc) rc = upload_list(b, ghostc, &SP.ghost_chunks);
+    SP.nghost = (int)ghostc.size();
     if (rc) return rc;
     if (!batch_cta_prepare()) return api_fail(ASD2G_E_CUDA, "coarse-cycle shared memory attribute");
     return check("batch set-up");
@@ -302,19 +346,139 @@ int asd2g_batch_offset(asd2g_batch *b, int inst, size_t *offset_doubles) {
     return ASD2G_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// dt[i] -> sc[0] of every instance (one strided copy).
+int set_dts(asd2g_batch *b, const double *dt) {
+    for (int i = 0; i < b->count; i++)
+        if (!(dt[i] > 0.0) || !std::isfinite(dt[i])) return api_fail(ASD2G_E_ARG, "batch: dt must be positive and finite");
+    cudaMemcpy2DAsync(b->sc, sizeof(double) * SC_PER_INST, dt, sizeof(double), sizeof(double), b->count,
+                      cudaMemcpyHostToDevice, b->st);
+    // the host array must outlive the copy
+    if (cudaStreamSynchronize(b->st) != cudaSuccess) return check("batch dt upload");
+    return ASD2G_OK;
+}
+
+int solve_impl(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_resid);
+}  // namespace
+
+extern "C" {
+
 int asd2g_batch_assemble(asd2g_batch *b, const double *dt) {
     if (!b || !dt) return api_fail(ASD2G_E_ARG, "batch_assemble: null argument");
-    for (int i = 0; i < b->count; i++) {
-        if (!(dt[i] > 0.0) || !std::isfinite(dt[i])) return api_fail(ASD2G_E_ARG, "batch_assemble: dt must be positive");
-        b->hinst[i].dt = dt[i];
-    }
-    cudaMemcpyAsync(b->dinst, b->hinst.data(), sizeof(BInst) * b->count, cudaMemcpyHostToDevice, b->st);
+    int rc = set_dts(b, dt);
+    if (rc) return rc;
     launch_batch_assemble(b->dinst, b->cell_tiles, b->ncell_tiles, b->st);
     return check("batch_assemble");
 }
 
 int asd2g_batch_solve(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_resid) {
     if (!b || !(tol > 0.0) || maxit < 1) return api_fail(ASD2G_E_ARG, "batch_solve: bad arguments");
+    return solve_impl(b, tol, maxit, iters, rel_resid);
+}
+
+// The full droplet step of every instance (asd2g_droplet_step per instance,
+// MG-FCG pressure solve), one launch per phase for the whole batch.
+int asd2g_batch_step(asd2g_batch *b, double *dt, int reinit_mode, double tol, int maxit, int *iters,
+                     double *rel_resid) {
+    if (!b || !dt || !(tol > 0.0) || maxit < 1) return api_fail(ASD2G_E_ARG, "batch_step: bad arguments");
+    if (reinit_mode != ASD2G_REINIT_ORIGINAL && reinit_mode != ASD2G_REINIT_MINRK2)
+        return api_fail(ASD2G_E_UNSUPPORTED, "batch_step implements reinit modes 0 (original) and 2 (MinRK2)");
+    const int order = b->prm[0].time_order;
+    int steps = -1;
+    for (int i = 0; i < b->count; i++) {
+        const asd2g_params &pp = b->prm[i];
+        if (pp.precision != ASD2G_PRECISION_FP64)
+            return api_fail(ASD2G_E_UNSUPPORTED, "batch_step runs FP64 instances");
+        if (pp.time_order != order || order < 0 || order > 2)
+            return api_fail(ASD2G_E_UNSUPPORTED, "batch_step needs one time order (0, 1 or 2) for every instance");
+        const LsConst &K = b->hinst[i].K;
+        const double mt = pp.ls_max_atime > 0.0 ? pp.ls_max_atime : 1.5 * K.thick;
+        const int si = reinit_steps(K.adt, mt);
+        if (steps >= 0 && si != steps)
+            return api_fail(ASD2G_E_UNSUPPORTED, "batch_step needs one reinitialisation step count for every instance");
+        steps = si;
+    }
+    int rc = set_dts(b, dt);
+    if (rc) return rc;
+    const BStepPlan &P = b->splan;
+    cudaStream_t st = b->st;
+    const size_t slot_bytes = sizeof(double) * b->gtot;
+    auto slot = [&](int f) { return b->pad + (size_t)f * b->gtot; };
+    // Solve_LevelSet_2D: lsB = ls; centred velocities; TVD-RK3 of HJ-WENO5
+    cudaMemcpyAsync(slot(BS_LSB), slot(BS_LS), slot_bytes, cudaMemcpyDeviceToDevice, st);
+    launch_bstep_center_vel(P, st);
+    launch_bstep_fill_p(P, BS_LS, false, st);
+    launch_bstep_ls_stage(P, 1, BS_LS, BS_LS, BS_W1, st);
+    launch_bstep_ls_stage(P, 2, BS_W1, BS_LS, BS_W2, st);
+    launch_bstep_ls_stage(P, 3, BS_W2, BS_LS, BS_LS, st);
+    // reinitialisation (levelset2d.cpp:264-316, :433-486): lsInit, then the pseudo-steps
+    if (reinit_mode == ASD2G_REINIT_MINRK2) {
+        launch_bstep_fill_p(P, BS_LS, false, st);
+        cudaMemcpyAsync(slot(BS_LS0), slot(BS_LS), slot_bytes, cudaMemcpyDeviceToDevice, st);
+    } else {
+        cudaMemcpyAsync(slot(BS_LS0), slot(BS_LS), slot_bytes, cudaMemcpyDeviceToDevice, st);
+        launch_bstep_fill_p(P, BS_LS, false, st);
+    }
+    for (int k = 0; k < steps; k++) {
+        launch_bstep_reinit_pass(P, reinit_mode, false, st);
+        launch_bstep_reinit_pass(P, reinit_mode, true, st);
+    }
+    // curvature (with the ghost fill of SolvePoisson's recompute), Heaviside, volume check
+    launch_bstep_kappa(P, st);
+    launch_bstep_fill_p(P, BS_KAPPA, true, st);
+    launch_bstep_heaviside(P, st);
+    launch_bstep_volume(P, st);
+    // intermediate velocity (GetIntermediateVel, smoothed Heaviside), its divergence
+    if (order == 0) {
+        launch_bstep_mom_stage(P, 0, BS_U, BS_V, -1, -1, BS_UHAT, BS_VHAT, st);
+    } else if (order == 1) {
+        launch_bstep_mom_stage(P, 0, BS_U, BS_V, -1, -1, BS_UA, BS_VA, st);
+        launch_bstep_fill_uv(P, BS_UA, BS_VA, st);
+        launch_bstep_mom_stage(P, 3, BS_UA, BS_VA, BS_U, BS_V, BS_UHAT, BS_VHAT, st);
+    } else {
+        launch_bstep_mom_stage(P, 0, BS_U, BS_V, -1, -1, BS_UA, BS_VA, st);
+        launch_bstep_fill_uv(P, BS_UA, BS_VA, st);
+        launch_bstep_mom_stage(P, 1, BS_UA, BS_VA, BS_U, BS_V, BS_UB, BS_VB, st);
+        launch_bstep_fill_uv(P, BS_UB, BS_VB, st);
+        launch_bstep_mom_stage(P, 2, BS_UB, BS_VB, BS_U, BS_V, BS_UHAT, BS_VHAT, st);
+    }
+    launch_bstep_fill_uv(P, BS_UHAT, BS_VHAT, st);
+    cudaMemsetAsync(slot(BS_DIV), 0, slot_bytes, st);
+    launch_bstep_divergence(P, st);
+    // GFM assembly and the batched MG-FCG
+    launch_batch_assemble(b->dinst, b->cell_tiles, b->ncell_tiles, st);
+    rc = check("batch_step (before the solve)");
+    if (rc) return rc;
+    const int st_solve = solve_impl(b, tol, maxit, iters, rel_resid);
+    if (st_solve < 0) return st_solve;
+    // projection and the next dt
+    launch_bstep_update_vel(P, st);
+    launch_bstep_update_dt(P, st);
+    cudaMemcpy2DAsync(dt, sizeof(double), b->sc + 1, sizeof(double) * SC_PER_INST, sizeof(double), b->count,
+                      cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return check("batch_step");
+    rc = check("batch_step");
+    return rc ? rc : st_solve;
+}
+
+int asd2g_batch_volume(asd2g_batch *b, double *sharp, double *smooth) {
+    if (!b) return api_fail(ASD2G_E_ARG, "null batch");
+    if (sharp)
+        cudaMemcpy2DAsync(sharp, sizeof(double), b->sc + 2, sizeof(double) * SC_PER_INST, sizeof(double), b->count,
+                          cudaMemcpyDeviceToHost, b->st);
+    if (smooth)
+        cudaMemcpy2DAsync(smooth, sizeof(double), b->sc + 3, sizeof(double) * SC_PER_INST, sizeof(double), b->count,
+                          cudaMemcpyDeviceToHost, b->st);
+    if (cudaStreamSynchronize(b->st) != cudaSuccess) return check("batch_volume");
+    return check("batch_volume");
+}
+
+}  // extern "C"
+
+namespace {
+int solve_impl(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_resid) {
     const BatchPlan &P = b->plan;
     launch_batch_set_kstate(P, tol, maxit, b->st);
     launch_batch_mg_setup(P, b->st);
@@ -355,6 +519,9 @@ int asd2g_batch_solve(asd2g_batch *b, double tol, int maxit, int *iters, double 
     if (cudaStreamSynchronize(b->st) != cudaSuccess) return check("batch solve");
     return status;
 }
+}  // namespace
+
+extern "C" {
 
 int asd2g_batch_sync(asd2g_batch *b) {
     if (!b) return api_fail(ASD2G_E_ARG, "null batch");

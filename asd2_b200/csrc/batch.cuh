@@ -4,9 +4,19 @@
 // (batched assembly), mg.cu (batched multigrid-preconditioned flexible CG)
 // and batch.cu (host orchestration).
 #pragma once
+#include "lsmath.cuh"
 #include "mg.cuh"
 
 namespace asd2g {
+
+// Padded-field slots of a batch arena: field slot f of instance i is
+// pad + f * gtot + goff[i] (BInst::pad0 + f * gstride).  The first six
+// hold the pressure problem; the rest serve the full droplet step.
+enum BSlot {
+    BS_LS = 0, BS_KAPPA, BS_H, BS_DIV, BS_PS, BS_P,
+    BS_U, BS_V, BS_HS, BS_LSB, BS_LS0, BS_UHAT, BS_VHAT, BS_UA, BS_VA, BS_UB, BS_VB, BS_TU, BS_TV, BS_W1, BS_W2,
+    BS_COUNT
+};
 
 // One instance: its grid, physics and the pointers into the batch arenas.
 struct BInst {
@@ -15,7 +25,13 @@ struct BInst {
     DivH dxx, dyy;                                 // / dx^2, / dy^2
     const double *ls, *kappa, *H, *div;            // padded FP64 inputs
     double *ps, *p;                                // padded FP64 outputs (P = PS / dt)
-    double dt;                                     // this instance's step
+    double *pad0;                                  // slot 0 of this instance (pad + goff)
+    size_t gstride;                                // doubles between slots (gtot)
+    double *sc;                                    // [0] dt of the step, [1] next dt, [2..3] volume (sharp, smooth)
+    LsConst K;                                     // reinitialisation constants
+    DivH ddx, ddy, d2x, d2y;                       // / dx, / dy, / (2 dx), / (2 dy)
+    double kappa_lim, hs_eps;                      // 1 / min(dx, dy); 1.5 min(dx, dy)
+    int kappa_fill;                                // the step fills kappa's ghosts (SolvePoisson's recompute)
     Sys S;                                         // compact system (diag, cw, ce, cs, cn, minv, b)
     double *x, *r, *pa, *pb, *q, *z;               // flexible CG vectors (compact, FP64)
     KState *ks;                                    // this instance's solver scalars
@@ -64,6 +80,40 @@ bool launch_batch_fcg_init(const BatchPlan &P, cudaStream_t st);
 bool launch_batch_fcg_iter(const BatchPlan &P, int parity, cudaStream_t st);
 bool launch_batch_fcg_check(const BatchPlan &P, cudaStream_t st);
 void launch_batch_set_kstate(const BatchPlan &P, double tol, int maxit, cudaStream_t st);
+// Full droplet step of every instance (batch_step.cu): one launch per phase
+// over the cell-tile list (tiles of TJ x TI interior cells), the padded-cell
+// chunks (heaviside), the ghost-entry chunks (P-grid fill) or one CTA per
+// instance (U/V fill); per-instance reductions (volume, dt) over the FCG
+// chunks with the instance's partial slots and solver ticket.
+struct BStepPlan {
+    const BInst *insts;
+    int count;
+    const BTile *tiles;
+    int ntiles;
+    const BChunk *pad_chunks;    // 1024 padded cells each
+    int npad;
+    const BChunk *ghost_chunks;  // 256 P-grid ghost entries each
+    int nghost;
+    const BChunk *chunks;        // FCG chunks (1024 interior cells)
+    int nchunks;
+};
+__device__ __forceinline__ double *bslot(const BInst &I, int f) { return I.pad0 + (size_t)f * I.gstride; }
+void launch_bstep_center_vel(const BStepPlan &P, cudaStream_t st);
+void launch_bstep_fill_p(const BStepPlan &P, int slot, bool kappa_only_if_flagged, cudaStream_t st);
+void launch_bstep_fill_uv(const BStepPlan &P, int su, int sv, cudaStream_t st);
+void launch_bstep_ls_stage(const BStepPlan &P, int stage, int in, int n, int out, cudaStream_t st);
+void launch_bstep_reinit_pass(const BStepPlan &P, int mode, bool pass_b, cudaStream_t st);
+void launch_bstep_kappa(const BStepPlan &P, cudaStream_t st);
+void launch_bstep_heaviside(const BStepPlan &P, cudaStream_t st);
+void launch_bstep_volume(const BStepPlan &P, cudaStream_t st);
+void launch_bstep_mom_stage(const BStepPlan &P, int kind, int in_u, int in_v, int base_u, int base_v, int out_u,
+                            int out_v, cudaStream_t st);
+void launch_bstep_divergence(const BStepPlan &P, cudaStream_t st);
+void launch_bstep_update_vel(const BStepPlan &P, cudaStream_t st);
+void launch_bstep_update_dt(const BStepPlan &P, cudaStream_t st);
+constexpr int BSTEP_GHOST_CHUNK = 256;
+constexpr int BSTEP_PAD_CHUNK = 1024;
+
 // Partial-sum doubles one instance needs (2 per level-0 tile or per chunk).
 int64_t batch_partial_len(int nx, int ny);
 int batch_tiles0(int nx, int ny);

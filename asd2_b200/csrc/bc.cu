@@ -7,6 +7,7 @@
 // touches disjoint strips that only read interior cells for Neumann and
 // Dirichlet sides, so those run fully parallel; periodic and extrapolating
 // sides run side by side in order.
+#include "batch.cuh"
 #include "internal.cuh"
 
 namespace asd2g {
@@ -208,9 +209,9 @@ __device__ __forceinline__ void fill_p_lsfree(const Grid &g, double *a, int side
     }
 }
 
-// side_mask selects the sides handled by this launch.
-__global__ void k_fill_p(Grid g, double *a, int side_mask) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+// Ghost entry t of the P grid (W strip, E strip, S strip, N strip, each
+// NB layers); side_mask selects the sides handled.
+__device__ __forceinline__ void fill_p_entry(const Grid &g, double *a, int t, int side_mask) {
     const int nwe = NB * g.ny, nsn = NB * g.nx;
     int side, rem;
     if (t < nwe) { side = 0; rem = t; }
@@ -226,6 +227,40 @@ __global__ void k_fill_p(Grid g, double *a, int side_mask) {
     } else {
         fill_p_cell(g, a, side, layer, s);
     }
+}
+
+// side_mask selects the sides handled by this launch.
+__global__ void k_fill_p(Grid g, double *a, int side_mask) {
+    fill_p_entry(g, a, blockIdx.x * blockDim.x + threadIdx.x, side_mask);
+}
+
+// Batched fills (asd2g_batch_step): every instance's P grid in one launch
+// over the ghost-entry chunks (Neumann/Dirichlet sides: all four at once),
+// and the U/V fill with one CTA per instance.
+__global__ void k_bfill_p(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks, int slot,
+                          int only_flagged) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    if (only_flagged && !I.kappa_fill) return;
+    fill_p_entry(I.g, bslot(I, slot), w.c * BSTEP_GHOST_CHUNK + threadIdx.x, 0xF);
+}
+
+__global__ void __launch_bounds__(1024) k_bfill_uv(const BInst *__restrict__ insts, int su, int sv) {
+    const BInst &I = insts[blockIdx.x];
+    double *u = bslot(I, su), *v = bslot(I, sv);
+    for (int side = 0; side < 4; side++) {
+        fill_u_side(I.g, u, side, threadIdx.x, blockDim.x);
+        fill_v_side(I.g, v, side, threadIdx.x, blockDim.x);
+        __syncthreads();
+    }
+}
+
+void launch_bstep_fill_p(const BStepPlan &P, int slot, bool kappa_only_if_flagged, cudaStream_t st) {
+    k_bfill_p<<<P.nghost, BSTEP_GHOST_CHUNK, 0, st>>>(P.insts, P.ghost_chunks, slot, kappa_only_if_flagged ? 1 : 0);
+}
+
+void launch_bstep_fill_uv(const BStepPlan &P, int su, int sv, cudaStream_t st) {
+    k_bfill_uv<<<P.count, 1024, 0, st>>>(P.insts, su, sv);
 }
 
 // One side of one grid with an explicit fill kind (the per-side methods

@@ -2,6 +2,7 @@
 // the templated stencils of levelset_impl.cuh instantiated for double, the
 // reinitialisation driver and the building-block kernels of the ABI.
 #include "levelset_impl.cuh"
+#include "batch.cuh"
 
 namespace asd2g {
 
@@ -234,6 +235,63 @@ void launch_pointwise_ls(const Grid &g, int which, const double *a, double *out,
     const int64_t n = (int64_t)g.sx * g.sy;
     const double eps = g.dx < g.dy ? g.dx : g.dy;
     k_pointwise_ls<<<(int)((n + 255) / 256), 256, 0, st>>>(n, which, eps, a, out);
+}
+
+// ------------------------------------------------------------------------
+// Batched full step (asd2g_batch_step): the same tile functions over a work
+// list of (instance, tile), one launch per phase for the whole batch.  Every
+// batch grid mirrors its own P ghosts (Neumann/Dirichlet sides).
+__global__ void __launch_bounds__(TJ *TI) k_bcenter_vel(const BInst *__restrict__ insts,
+                                                          const BTile *__restrict__ tiles) {
+    const BTile t = tiles[blockIdx.x];
+    const BInst &I = insts[t.inst];
+    center_vel_tile<double>(I.g, bslot(I, BS_U), bslot(I, BS_V), bslot(I, BS_TU), bslot(I, BS_TV), t.bx, t.by);
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(TJ *TI) k_bls_stage(const BInst *__restrict__ insts, const BTile *__restrict__ tiles,
+                                                        int in, int n, int out) {
+    const BTile t = tiles[blockIdx.x];
+    const BInst &I = insts[t.inst];
+    ls_stage_tile<STAGE, double>(I.g, I.ddx, I.ddy, bslot(I, in), bslot(I, BS_TU), bslot(I, BS_TV), bslot(I, n),
+                                 bslot(I, out), I.sc, t.bx, t.by);
+}
+
+// LS1 = LS - adt S (|grad LS| - 1) into W1; LS = 0.5 (LS + LS2(W1)) (both with ghost mirrors)
+template <int MODE>
+__global__ void __launch_bounds__(TJ *TI) k_breinit_a(const BInst *__restrict__ insts, const BTile *__restrict__ tiles) {
+    const BTile t = tiles[blockIdx.x];
+    const BInst &I = insts[t.inst];
+    reinit_a_tile<MODE, double>(I.g, I.K, bslot(I, BS_LS), bslot(I, BS_LS0), bslot(I, BS_W1), 1, t.bx, t.by);
+}
+template <int MODE>
+__global__ void __launch_bounds__(TJ *TI) k_breinit_b(const BInst *__restrict__ insts, const BTile *__restrict__ tiles) {
+    const BTile t = tiles[blockIdx.x];
+    const BInst &I = insts[t.inst];
+    reinit_b_tile<MODE, double>(I.g, I.K, bslot(I, BS_W1), bslot(I, BS_LS0), bslot(I, BS_LS), bslot(I, BS_LS), 1,
+                                t.bx, t.by);
+}
+
+void launch_bstep_center_vel(const BStepPlan &P, cudaStream_t st) {
+    k_bcenter_vel<<<P.ntiles, dim3(TJ, TI), 0, st>>>(P.insts, P.tiles);
+}
+
+void launch_bstep_ls_stage(const BStepPlan &P, int stage, int in, int n, int out, cudaStream_t st) {
+    const dim3 blk(TJ, TI);
+    if (stage == 1) k_bls_stage<1><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, in, n, out);
+    else if (stage == 2) k_bls_stage<2><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, in, n, out);
+    else k_bls_stage<3><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, in, n, out);
+}
+
+void launch_bstep_reinit_pass(const BStepPlan &P, int mode, bool pass_b, cudaStream_t st) {
+    const dim3 blk(TJ, TI);
+    if (mode == RM_ORIG) {
+        if (pass_b) k_breinit_b<RM_ORIG><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles);
+        else k_breinit_a<RM_ORIG><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles);
+    } else {
+        if (pass_b) k_breinit_b<RM_MINRK2><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles);
+        else k_breinit_a<RM_MINRK2><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles);
+    }
 }
 
 }  // namespace asd2g

@@ -17,10 +17,15 @@ namespace asd2g {
 // ------------------------------------------------------------------------
 // Velocity centring (levelset2d.cpp:50-54).
 // The face velocities are FP64 in every precision; the centred values are T.
+// Every cell kernel below is a tile function of the TJ x TI tile (bx, by)
+// of interior cells (one thread per cell, threadIdx = position in the tile),
+// wrapped by a one-grid kernel (tile = blockIdx) and, in batch.cu, by a
+// batched kernel over a work list of (instance, tile).
 template <typename T>
-__global__ void k_center_vel(Grid g, const double *__restrict__ u, const double *__restrict__ v, T *__restrict__ tu,
-                             T *__restrict__ tv) {
-    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
+__device__ __forceinline__ void center_vel_tile(const Grid &g, const double *__restrict__ u,
+                                                const double *__restrict__ v, T *__restrict__ tu,
+                                                T *__restrict__ tv, int bx, int by) {
+    const int j = NB + bx * TJ + threadIdx.x, i = NB + by * TI + threadIdx.y;
     if (i >= g.nx + NB || j >= g.ny + NB) return;
     const T a = T((u[IX(g, i, j)] + u[IX(g, i + 1, j)]) * 0.5);
     const T b = T((v[IX(g, i, j)] + v[IX(g, i, j + 1)]) * 0.5);
@@ -30,6 +35,11 @@ __global__ void k_center_vel(Grid g, const double *__restrict__ u, const double 
         p_mirror_store(g, tu, i, j, a);
         p_mirror_store(g, tv, i, j, b);
     }
+}
+template <typename T>
+__global__ void k_center_vel(Grid g, const double *__restrict__ u, const double *__restrict__ v, T *__restrict__ tu,
+                             T *__restrict__ tv) {
+    center_vel_tile<T>(g, u, v, tu, tv, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------------------------------
@@ -47,12 +57,13 @@ __global__ void k_center_vel(Grid g, const double *__restrict__ u, const double 
 // phi_n only at its own cell before writing it.
 // dtp is the FP64 dt of the step (rounded to T for T = float).
 template <int STAGE, typename T>
-__global__ void __launch_bounds__(TJ *TI) k_ls_stage(Grid g, DivHT<T> ddx, DivHT<T> ddy, const T *__restrict__ phi_in,
-                                                       const T *__restrict__ tu, const T *__restrict__ tv,
-                                                       const T *phi_n, T *out, const double *__restrict__ dtp) {
+__device__ __forceinline__ void ls_stage_tile(const Grid &g, const DivHT<T> &ddx, const DivHT<T> &ddy,
+                                              const T *__restrict__ phi_in, const T *__restrict__ tu,
+                                              const T *__restrict__ tv, const T *phi_n, T *out,
+                                              const double *__restrict__ dtp, int bx, int by) {
     __shared__ T sFx[TI + 2 * NB][TJ];      // rows i0-3 .. i0+TI+2, cols j0 .. j0+TJ-1
     __shared__ T sFy[TI][TJ + 2 * NB + 1];  // rows i0 .. i0+TI-1, cols j0-3 .. j0+TJ+2
-    const int j0 = NB + blockIdx.x * TJ, i0 = NB + blockIdx.y * TI;
+    const int j0 = NB + bx * TJ, i0 = NB + by * TI;
     const int tid = threadIdx.y * TJ + threadIdx.x;
     for (int t = tid; t < (TI + 2 * NB) * TJ; t += TJ * TI) {
         const int r = t / TJ, c = t % TJ;
@@ -90,6 +101,12 @@ __global__ void __launch_bounds__(TJ *TI) k_ls_stage(Grid g, DivHT<T> ddx, DivHT
     out[c] = val;
     if (STAGE != 0 && g.p_mirror) p_mirror_store(g, out, i, j, val);
 }
+template <int STAGE, typename T>
+__global__ void __launch_bounds__(TJ *TI) k_ls_stage(Grid g, DivHT<T> ddx, DivHT<T> ddy, const T *__restrict__ phi_in,
+                                                       const T *__restrict__ tu, const T *__restrict__ tv,
+                                                       const T *phi_n, T *out, const double *__restrict__ dtp) {
+    ls_stage_tile<STAGE, T>(g, ddx, ddy, phi_in, tu, tv, phi_n, out, dtp, blockIdx.x, blockIdx.y);
+}
 
 // ------------------------------------------------------------------------
 // Reinitialisation passes.  Every pass reads its stencil input from buffers
@@ -105,9 +122,10 @@ template <typename T> __device__ __forceinline__ T reinit_sign(int mode, T l0, T
 
 // Pass A: out = src - adt * S * (|grad src| - 1)   (LS1 of every mode)
 template <int MODE, typename T>
-__global__ void k_reinit_a(Grid g, LsConstT<T> K, const T *__restrict__ src, const T *__restrict__ ls0,
-                           T *__restrict__ out, int mirror) {
-    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
+__device__ __forceinline__ void reinit_a_tile(const Grid &g, const LsConstT<T> &K, const T *__restrict__ src,
+                                              const T *__restrict__ ls0, T *__restrict__ out, int mirror, int bx,
+                                              int by) {
+    const int j = NB + bx * TJ + threadIdx.x, i = NB + by * TI + threadIdx.y;
     if (i >= g.nx + NB || j >= g.ny + NB) return;
     constexpr bool SUB = (MODE == RM_MINRK2 || MODE == RM_MINRK2_SUSS);
     const int64_t c = IX(g, i, j);
@@ -119,14 +137,20 @@ __global__ void k_reinit_a(Grid g, LsConstT<T> K, const T *__restrict__ src, con
     out[c] = val;
     if (mirror) p_mirror_store(g, out, i, j, val);
 }
+template <int MODE, typename T>
+__global__ void k_reinit_a(Grid g, LsConstT<T> K, const T *__restrict__ src, const T *__restrict__ ls0,
+                           T *__restrict__ out, int mirror) {
+    reinit_a_tile<MODE, T>(g, K, src, ls0, out, mirror, blockIdx.x, blockIdx.y);
+}
 
 // Pass B: LS2 = step_base - adt * S * (|grad ls1| - 1); out = 0.5 * (base + LS2)
 // step_base is ls1 itself except for the first-time mode, which steps from
 // phi again (levelset2d.cpp:413-416).
 template <int MODE, typename T>
-__global__ void k_reinit_b(Grid g, LsConstT<T> K, const T *__restrict__ ls1, const T *__restrict__ ls0, const T *base,
-                           T *out, int mirror) {
-    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
+__device__ __forceinline__ void reinit_b_tile(const Grid &g, const LsConstT<T> &K, const T *__restrict__ ls1,
+                                              const T *__restrict__ ls0, const T *base, T *out, int mirror, int bx,
+                                              int by) {
+    const int j = NB + bx * TJ + threadIdx.x, i = NB + by * TI + threadIdx.y;
     if (i >= g.nx + NB || j >= g.ny + NB) return;
     constexpr bool SUB = (MODE == RM_MINRK2 || MODE == RM_MINRK2_SUSS);
     const int64_t c = IX(g, i, j);
@@ -139,6 +163,11 @@ __global__ void k_reinit_b(Grid g, LsConstT<T> K, const T *__restrict__ ls1, con
     const T val = T(0.5) * (b + ls2);
     out[c] = val;
     if (mirror) p_mirror_store(g, out, i, j, val);
+}
+template <int MODE, typename T>
+__global__ void k_reinit_b(Grid g, LsConstT<T> K, const T *__restrict__ ls1, const T *__restrict__ ls0, const T *base,
+                           T *out, int mirror) {
+    reinit_b_tile<MODE, T>(g, K, ls1, ls0, base, out, mirror, blockIdx.x, blockIdx.y);
 }
 
 // Pass C (Sussman constraint, :787-893): out = base + constraint(tmp, ls0)

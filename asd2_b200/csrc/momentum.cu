@@ -1,6 +1,7 @@
 // MAC momentum kernels (mac2d.cpp): curvature, Heaviside functions, the
 // WENO5 convection + variable-viscosity + gravity right-hand side fused with
 // the Runge-Kutta stage update, divergence, projection and the CFL time step.
+#include "batch.cuh"
 #include "lsmath.cuh"
 #include "momentum.cuh"
 
@@ -9,9 +10,13 @@ namespace asd2g {
 // ---------------------------------------------------------------- kappa --
 // UpdateKappa, mac2d.cpp:221-252.  dLSdX is only defined on interior cells
 // (zero elsewhere), which matters for the cross term at j = 3 and ny+2.
-__global__ void k_kappa(Grid g, DivH d2x, DivH d2y, DivH dxx, DivH dyy, double lim, const double *__restrict__ ls,
-                        double *__restrict__ kappa) {
-    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
+// Cell kernels are tile functions of the TJ x TI interior tile (bx, by),
+// wrapped by one-grid kernels here and by batched kernels (work lists of
+// instance tiles) at the end of this file.
+__device__ __forceinline__ void kappa_tile(const Grid &g, const DivH &d2x, const DivH &d2y, const DivH &dxx,
+                                           const DivH &dyy, double lim, const double *__restrict__ ls,
+                                           double *__restrict__ kappa, int bx, int by) {
+    const int j = NB + bx * TJ + threadIdx.x, i = NB + by * TI + threadIdx.y;
     if (i >= g.nx + NB || j >= g.ny + NB) return;
     auto gx = [&](int jj) -> double {
         if (jj < NB || jj >= g.ny + NB) return 0.0;
@@ -28,21 +33,28 @@ __global__ void k_kappa(Grid g, DivH d2x, DivH d2y, DivH dxx, DivH dyy, double l
     k = isgn(k) * fabs(smin(fabs(k), lim));
     kappa[IX(g, i, j)] = k;
 }
+__global__ void k_kappa(Grid g, DivH d2x, DivH d2y, DivH dxx, DivH dyy, double lim, const double *__restrict__ ls,
+                        double *__restrict__ kappa) {
+    kappa_tile(g, d2x, d2y, dxx, dyy, lim, ls, kappa, blockIdx.x, blockIdx.y);
+}
 
 // ------------------------------------------------------------ Heaviside --
 // UpdateHeavisideFunc / UpdateSmoothHeavisideFunc over every cell
 // (mac2d.cpp:87-122).
+__device__ __forceinline__ void heaviside_cell(double eps, const double *__restrict__ ls, double *__restrict__ H,
+                                               double *__restrict__ HS, int64_t k) {
+    const double l = ls[k];
+    H[k] = l >= 0.0 ? 1.0 : 0.0;
+    double hs;
+    if (l > eps) hs = 1.0;
+    else if (l < -eps) hs = 0.0;
+    else hs = 0.5 * (1.0 + l / eps + 1.0 / kPi * sin(kPi * l / eps));
+    HS[k] = hs;
+}
 __global__ void k_heaviside(int64_t n, double eps, const double *__restrict__ ls, double *__restrict__ H,
                             double *__restrict__ HS) {
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        const double l = ls[k];
-        H[k] = l >= 0.0 ? 1.0 : 0.0;
-        double hs;
-        if (l > eps) hs = 1.0;
-        else if (l < -eps) hs = 0.0;
-        else hs = 0.5 * (1.0 + l / eps + 1.0 / kPi * sin(kPi * l / eps));
-        HS[k] = hs;
-    }
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        heaviside_cell(eps, ls, H, HS, k);
 }
 
 // ------------------------------------------------------- momentum terms --
@@ -191,12 +203,13 @@ __device__ double visc_v(const Grid &g, const MomConst &M, const double *u, cons
 // 2 out = 1/3 base + 2/3 (in + dt F); 3 out = 0.5 base + 0.5 (in + dt F);
 // 4 out = F(in); 5 out = convection; 6 out = viscosity.
 template <int KIND>
-__global__ void __launch_bounds__(TJ *TI) k_mom_stage(Grid g, MomConst M, const double *__restrict__ ls,
-                                                        const double *__restrict__ H, const double *__restrict__ uin,
-                                                        const double *__restrict__ vin, const double *__restrict__ ub,
-                                                        const double *__restrict__ vb, double *__restrict__ uout,
-                                                        double *__restrict__ vout, const double *__restrict__ dtp) {
-    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
+__device__ __forceinline__ void mom_stage_tile(const Grid &g, const MomConst &M, const double *__restrict__ ls,
+                                               const double *__restrict__ H, const double *__restrict__ uin,
+                                               const double *__restrict__ vin, const double *__restrict__ ub,
+                                               const double *__restrict__ vb, double *__restrict__ uout,
+                                               double *__restrict__ vout, const double *__restrict__ dtp, int bx,
+                                               int by) {
+    const int j = NB + bx * TJ + threadIdx.x, i = NB + by * TI + threadIdx.y;
     if (i >= g.nx + NB || j >= g.ny + NB) return;
     const double dt = (KIND <= 3) ? *dtp : 0.0;
     if (i >= NB + 1) {  // u interior faces i = 4 .. nx+2
@@ -231,14 +244,27 @@ __global__ void __launch_bounds__(TJ *TI) k_mom_stage(Grid g, MomConst M, const 
         vout[c] = o;
     }
 }
+template <int KIND>
+__global__ void __launch_bounds__(TJ *TI) k_mom_stage(Grid g, MomConst M, const double *__restrict__ ls,
+                                                        const double *__restrict__ H, const double *__restrict__ uin,
+                                                        const double *__restrict__ vin, const double *__restrict__ ub,
+                                                        const double *__restrict__ vb, double *__restrict__ uout,
+                                                        double *__restrict__ vout, const double *__restrict__ dtp) {
+    mom_stage_tile<KIND>(g, M, ls, H, uin, vin, ub, vb, uout, vout, dtp, blockIdx.x, blockIdx.y);
+}
 
 // ------------------------------------------------------------ divergence --
 // GetDivergence, mac2d.cpp:1729-1738
-__global__ void k_divergence(Grid g, DivH ddx, DivH ddy, const double *__restrict__ u, const double *__restrict__ v,
-                             double *__restrict__ div) {
-    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
+__device__ __forceinline__ void divergence_tile(const Grid &g, const DivH &ddx, const DivH &ddy,
+                                                const double *__restrict__ u, const double *__restrict__ v,
+                                                double *__restrict__ div, int bx, int by) {
+    const int j = NB + bx * TJ + threadIdx.x, i = NB + by * TI + threadIdx.y;
     if (i >= g.nx + NB || j >= g.ny + NB) return;
     div[IX(g, i, j)] = ddx(u[IX(g, i + 1, j)] - u[IX(g, i, j)]) + ddy(v[IX(g, i, j + 1)] - v[IX(g, i, j)]);
+}
+__global__ void k_divergence(Grid g, DivH ddx, DivH ddy, const double *__restrict__ u, const double *__restrict__ v,
+                             double *__restrict__ div) {
+    divergence_tile(g, ddx, ddy, u, v, div, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------------------ projection --
@@ -251,11 +277,13 @@ __device__ __forceinline__ void gfm_theta_first(double a, double b, double &thH,
 }
 
 // UpdateVel, mac2d.cpp:1740-1849
-__global__ void k_update_vel(Grid g, MomConst M, DivH ddx, DivH ddy, const double *__restrict__ us,
-                             const double *__restrict__ vs, const double *__restrict__ ps, const double *__restrict__ ls,
-                             const double *__restrict__ H, const double *__restrict__ kappa, double *__restrict__ u,
-                             double *__restrict__ v, const double *__restrict__ dtp) {
-    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
+__device__ __forceinline__ void update_vel_tile(const Grid &g, const MomConst &M, const DivH &ddx, const DivH &ddy,
+                                                const double *__restrict__ us, const double *__restrict__ vs,
+                                                const double *__restrict__ ps, const double *__restrict__ ls,
+                                                const double *__restrict__ H, const double *__restrict__ kappa,
+                                                double *__restrict__ u, double *__restrict__ v,
+                                                const double *__restrict__ dtp, int bx, int by) {
+    const int j = NB + bx * TJ + threadIdx.x, i = NB + by * TI + threadIdx.y;
     if (i >= g.nx + NB || j >= g.ny + NB) return;
     const double dt = *dtp;
     const int64_t c = IX(g, i, j);
@@ -282,11 +310,30 @@ __global__ void k_update_vel(Grid g, MomConst M, DivH ddx, DivH ddy, const doubl
         v[c] = val;
     }
 }
+__global__ void k_update_vel(Grid g, MomConst M, DivH ddx, DivH ddy, const double *__restrict__ us,
+                             const double *__restrict__ vs, const double *__restrict__ ps, const double *__restrict__ ls,
+                             const double *__restrict__ H, const double *__restrict__ kappa, double *__restrict__ u,
+                             double *__restrict__ v, const double *__restrict__ dtp) {
+    update_vel_tile(g, M, ddx, ddy, us, vs, ps, ls, H, kappa, u, v, dtp, blockIdx.x, blockIdx.y);
+}
 
 // --------------------------------------------------------------- UpdateDt --
 // mac2d.cpp:1851-1880.  max over interior of |u[i+1]*u[i]*0.5| and the v
 // analogue (max is order-free, so the GPU value is the reference's).  The
 // last block to finish computes dt.
+// The CFL time step from the largest |u u| / 2 (a) and |v v| / 2 (b).
+__device__ __forceinline__ double cfl_dt(const Grid &g, const MomConst &M, double a, double b) {
+    const double dx = g.dx, dy = g.dy;
+    const double C = a / dx + b / dy;
+    const double V = smax(M.mu_h, M.mu_l) * (2.0 / (dx * dx + dy * dy));
+    const double G = smax(sqrt(fabs(M.g) / dy), sqrt(fabs(M.g) / dx));
+    const double hmin = smin(dx, dy);
+    const double S = sqrt((M.sigma / hmin) / (smin(M.rho_h, M.rho_l) * (hmin * hmin)));
+    double dt = 1.79769313486231570815e+308;
+    dt = smin(dt, M.cfl / (0.5 * (C + V + sqrt((C + V) * (C + V) + 4.0 * G * G + 4.0 * S * S))));
+    return dt;
+}
+
 __global__ void k_update_dt(Grid g, MomConst M, const double *__restrict__ u, const double *__restrict__ v,
                             double *__restrict__ partial, unsigned *__restrict__ counter, double *__restrict__ dt_out) {
     double ua = 0.0, va = 0.0;
@@ -321,15 +368,7 @@ __global__ void k_update_dt(Grid g, MomConst M, const double *__restrict__ u, co
             a = smax(a, ((volatile double *)partial)[2 * k]);
             b = smax(b, ((volatile double *)partial)[2 * k + 1]);
         }
-        const double dx = g.dx, dy = g.dy;
-        const double C = a / dx + b / dy;
-        const double V = smax(M.mu_h, M.mu_l) * (2.0 / (dx * dx + dy * dy));
-        const double G = smax(sqrt(fabs(M.g) / dy), sqrt(fabs(M.g) / dx));
-        const double hmin = smin(dx, dy);
-        const double S = sqrt((M.sigma / hmin) / (smin(M.rho_h, M.rho_l) * (hmin * hmin)));
-        double dt = 1.79769313486231570815e+308;
-        dt = smin(dt, M.cfl / (0.5 * (C + V + sqrt((C + V) * (C + V) + 4.0 * G * G + 4.0 * S * S))));
-        *dt_out = dt;
+        *dt_out = cfl_dt(g, M, a, b);
         *counter = 0u;
     }
 }
@@ -436,6 +475,161 @@ void launch_update_vel(const Grid &g, const MomConst &M, const double *us, const
 void launch_update_dt(const Grid &g, const MomConst &M, const double *u, const double *v, double *partial,
                       unsigned *counter, double *dt_out, cudaStream_t st) {
     k_update_dt<<<DT_BLOCKS, 256, 0, st>>>(g, M, u, v, partial, counter, dt_out);
+}
+
+// ------------------------------------------------------------------------
+// Batched full step (asd2g_batch_step): the tile functions above over the
+// (instance, tile) work list, one launch per phase for the whole batch.
+__global__ void k_bkappa(const BInst *__restrict__ insts, const BTile *__restrict__ tiles) {
+    const BTile t = tiles[blockIdx.x];
+    const BInst &I = insts[t.inst];
+    kappa_tile(I.g, I.d2x, I.d2y, I.dxx, I.dyy, I.kappa_lim, bslot(I, BS_LS), bslot(I, BS_KAPPA), t.bx, t.by);
+}
+
+__global__ void k_bheaviside(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    const int64_t n = (int64_t)I.g.sx * I.g.sy, k0 = (int64_t)w.c * BSTEP_PAD_CHUNK;
+    for (int t = threadIdx.x; t < BSTEP_PAD_CHUNK; t += blockDim.x)
+        if (k0 + t < n) heaviside_cell(I.hs_eps, bslot(I, BS_LS), bslot(I, BS_H), bslot(I, BS_HS), k0 + t);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(TJ *TI) k_bmom_stage(const BInst *__restrict__ insts, const BTile *__restrict__ tiles,
+                                                         int in_u, int in_v, int base_u, int base_v, int out_u,
+                                                         int out_v) {
+    const BTile t = tiles[blockIdx.x];
+    const BInst &I = insts[t.inst];
+    mom_stage_tile<KIND>(I.g, I.M, bslot(I, BS_LS), bslot(I, BS_HS), bslot(I, in_u), bslot(I, in_v),
+                         base_u >= 0 ? bslot(I, base_u) : nullptr, base_v >= 0 ? bslot(I, base_v) : nullptr,
+                         bslot(I, out_u), bslot(I, out_v), I.sc, t.bx, t.by);
+}
+
+__global__ void k_bdivergence(const BInst *__restrict__ insts, const BTile *__restrict__ tiles) {
+    const BTile t = tiles[blockIdx.x];
+    const BInst &I = insts[t.inst];
+    divergence_tile(I.g, I.ddx, I.ddy, bslot(I, BS_UHAT), bslot(I, BS_VHAT), bslot(I, BS_DIV), t.bx, t.by);
+}
+
+__global__ void k_bupdate_vel(const BInst *__restrict__ insts, const BTile *__restrict__ tiles) {
+    const BTile t = tiles[blockIdx.x];
+    const BInst &I = insts[t.inst];
+    update_vel_tile(I.g, I.M, I.ddx, I.ddy, bslot(I, BS_UHAT), bslot(I, BS_VHAT), bslot(I, BS_PS), bslot(I, BS_LS),
+                    bslot(I, BS_H), bslot(I, BS_KAPPA), bslot(I, BS_U), bslot(I, BS_V), I.sc, t.bx, t.by);
+}
+
+// Per-instance two-value reduction over the instance's FCG chunks (block c of
+// I.chunks): MAX or SUM; the instance's last block gets the totals.
+template <bool MAX>
+__device__ __forceinline__ bool binst_reduce2(const BInst &I, int c, double a, double b, double &ta, double &tb) {
+    __shared__ double sa[32], sb[32];
+    __shared__ bool last;
+    for (int o = 16; o > 0; o >>= 1) {
+        const double oa = __shfl_down_sync(0xffffffffu, a, o), ob = __shfl_down_sync(0xffffffffu, b, o);
+        a = MAX ? smax(a, oa) : a + oa;
+        b = MAX ? smax(b, ob) : b + ob;
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        sa[wid] = a;
+        sb[wid] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double x = 0.0, y = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            x = MAX ? smax(x, sa[w]) : x + sa[w];
+            y = MAX ? smax(y, sb[w]) : y + sb[w];
+        }
+        I.partial[2 * c] = x;
+        I.partial[2 * c + 1] = y;
+        __threadfence();
+        last = atomicAdd(&I.ks->counter, 1u) == (unsigned)I.chunks - 1u;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return false;
+    __threadfence();
+    double x = 0.0, y = 0.0;
+    for (int k = 0; k < I.chunks; k++) {
+        const double pa = __ldcg(I.partial + 2 * k), pb = __ldcg(I.partial + 2 * k + 1);
+        x = MAX ? smax(x, pa) : x + pa;
+        y = MAX ? smax(y, pb) : y + pb;
+    }
+    ta = x;
+    tb = y;
+    I.ks->counter = 0u;
+    return true;
+}
+
+__global__ void __launch_bounds__(256) k_bupdate_dt(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    const Grid &g = I.g;
+    const double *u = bslot(I, BS_U), *v = bslot(I, BS_V);
+    double ua = 0.0, va = 0.0;
+    const int64_t k0 = (int64_t)w.c * FCG_CHUNK;
+    for (int t = threadIdx.x; t < FCG_CHUNK; t += blockDim.x) {
+        const int64_t k = k0 + t;
+        if (k >= I.n) break;
+        const int i = NB + (int)(k / g.ny), j = NB + (int)(k % g.ny);
+        ua = smax(ua, fabs((u[IX(g, i + 1, j)] * u[IX(g, i, j)]) * 0.5));
+        va = smax(va, fabs((v[IX(g, i, j + 1)] * v[IX(g, i, j)]) * 0.5));
+    }
+    double a, b;
+    if (binst_reduce2<true>(I, w.c, ua, va, a, b)) I.sc[1] = cfl_dt(g, I.M, a, b);
+}
+
+__global__ void __launch_bounds__(256) k_bvolume(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    const Grid &g = I.g;
+    const double *H = bslot(I, BS_H), *HS = bslot(I, BS_HS);
+    double sa = 0.0, sb = 0.0;
+    const int64_t k0 = (int64_t)w.c * FCG_CHUNK;
+    for (int t = threadIdx.x; t < FCG_CHUNK; t += blockDim.x) {
+        const int64_t k = k0 + t;
+        if (k >= I.n) break;
+        const int64_t c = IX(g, NB + (int)(k / g.ny), NB + (int)(k % g.ny));
+        sa += H[c];
+        sb += HS[c];
+    }
+    double a, b;
+    if (binst_reduce2<false>(I, w.c, sa, sb, a, b)) {
+        I.sc[2] = a * g.dx * g.dy;
+        I.sc[3] = b * g.dx * g.dy;
+    }
+}
+
+void launch_bstep_kappa(const BStepPlan &P, cudaStream_t st) {
+    k_bkappa<<<P.ntiles, dim3(TJ, TI), 0, st>>>(P.insts, P.tiles);
+}
+void launch_bstep_heaviside(const BStepPlan &P, cudaStream_t st) {
+    k_bheaviside<<<P.npad, 256, 0, st>>>(P.insts, P.pad_chunks);
+}
+void launch_bstep_volume(const BStepPlan &P, cudaStream_t st) {
+    k_bvolume<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks);
+}
+void launch_bstep_mom_stage(const BStepPlan &P, int kind, int in_u, int in_v, int base_u, int base_v, int out_u,
+                            int out_v, cudaStream_t st) {
+    const dim3 blk(TJ, TI);
+#define BMK(K) k_bmom_stage<K><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, in_u, in_v, base_u, base_v, out_u, out_v)
+    switch (kind) {
+    case 0: BMK(0); break;
+    case 1: BMK(1); break;
+    case 2: BMK(2); break;
+    default: BMK(3); break;
+    }
+#undef BMK
+}
+void launch_bstep_divergence(const BStepPlan &P, cudaStream_t st) {
+    k_bdivergence<<<P.ntiles, dim3(TJ, TI), 0, st>>>(P.insts, P.tiles);
+}
+void launch_bstep_update_vel(const BStepPlan &P, cudaStream_t st) {
+    k_bupdate_vel<<<P.ntiles, dim3(TJ, TI), 0, st>>>(P.insts, P.tiles);
+    launch_bstep_fill_uv(P, BS_U, BS_V, st);
+}
+void launch_bstep_update_dt(const BStepPlan &P, cudaStream_t st) {
+    k_bupdate_dt<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks);
 }
 
 }  // namespace asd2g

@@ -164,7 +164,7 @@ __global__ void k_bassemble(const BInst *__restrict__ insts, const BTile *__rest
     const BInst &I = insts[w.inst];
     const int j = NB + w.bx * TJ + threadIdx.x, i = NB + w.by * TI + threadIdx.y;
     if (i >= I.g.nx + NB || j >= I.g.ny + NB) return;
-    assemble_cell(I.g, I.M, I.dxx, I.dyy, I.ls, I.kappa, I.H, I.div, I.dt, I.S, i, j);
+    assemble_cell(I.g, I.M, I.dxx, I.dyy, I.ls, I.kappa, I.H, I.div, I.sc[0], I.S, i, j);
 }
 
 // Batched scatter: PS = x on the interior with its ghost mirrors (every
@@ -178,7 +178,7 @@ __global__ void k_bscatter(const BInst *__restrict__ insts, const BTile *__restr
     const double v = I.x[(int64_t)(j - NB) + (int64_t)g.ny * (i - NB)];
     I.ps[IX(g, i, j)] = v;
     p_mirror_store(g, I.ps, i, j, v);
-    I.p[IX(g, i, j)] = v / I.dt;  // mac2d.cpp:1722-1724
+    I.p[IX(g, i, j)] = v / I.sc[0];  // mac2d.cpp:1722-1724
 }
 
 // ------------------------------------------------------------------ SpMV --

@@ -428,6 +428,110 @@ def learned_pc_512(sh, stream, flush, weights=None, n=512, counts=tuple(range(1,
             "systems": rows, "l2": "flushed (256 MB write) before each timed solve"}
 
 
+def unet_forward(sh, stream, sizes=(256, 512), reps=20):
+    """Forward pass of the learned preconditioner's U-Net (random weights, one
+    image with the 4 feature channels) at each size: CUDA-event time per
+    pass after 3 warm-up passes, and the convolution FLOPs it performs."""
+    import torch
+    from asd2_b200 import api
+    lay, _ = api.UNet.layout()
+    out = {}
+    for n in sizes:
+        net = api.UNet(1, n, n, stream=sh)
+        net.init(1)
+        f = torch.randn(1, n, n, 4, device="cuda")
+        o = torch.empty(1, n, n, device="cuda")
+        for _ in range(3):
+            net.forward(f, o, 1, n, n)
+        with torch.cuda.stream(stream):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        for _ in range(reps):
+            net.forward(f, o, 1, n, n)
+        e1.record(stream)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / reps
+        # 2 * 9 * cin * cout per output pixel; layer i of the layout works at level (i // 2) for the
+        # encoder (i < 8), 2 - (i - 8) // 2 for the decoder, 0 for the output layer
+        flops = 0
+        for i, (wo, bo, cin, cout, relu) in enumerate(lay):
+            lv = i // 2 if i < 8 else (2 - (i - 8) // 2 if i < 14 else 0)
+            flops += 2 * 9 * cin * cout * (n >> lv) ** 2
+        out[str(n)] = {"us_per_forward": t * 1e6, "gflop": flops / 1e9, "tflops": flops / t / 1e12,
+                       "finite": bool(torch.isfinite(o).all())}
+        net.close()
+    return {"workload": "U-Net forward (15 tcgen05 convolutions, BF16), batch 1", "sizes": out}
+
+
+def batched_steps(sh, stream, count=BATCH_COUNT, steps=10):
+    """cfg 4 as a whole step: the 256-droplet batch (sides 64..512, radius
+    [0.08, 0.2], density ratio log-U[1, 1000], viscosity ratio log-U[1, 100])
+    advanced `steps` full droplet steps from rest by asd2g_batch_step (every
+    phase one launch for the whole batch, MG-FCG pressure to 1e-8), against the
+    same first step run instance by instance through sessions (MG-FCG)."""
+    import torch
+    from asd2_b200 import api
+    from asd2_b200 import workloads as W
+    cases = W.droplet_batch(count, seed=0)
+    params = [api.Params.from_case(c) for c in cases]
+    init, dts, t_seq, its_seq = [], [], 0.0, []
+    for c, p in zip(cases, params):
+        with api.Session(p, stream=sh) as ss:
+            ss.upload("ls", c.ls)
+            ss.upload("u", c.u)
+            ss.upload("v", c.v)
+            ss.apply_bc("ls", "P")
+            init.append({k: ss.download(k) for k in ("ls", "u", "v")})
+            dt = ss.update_dt()
+            dts.append(dt)
+            r = ss.droplet_step(dt, solver=api.MGPCG, tol=TOL, maxit=100000)  # first step: set-up, untimed
+            ss.sync()
+            with torch.cuda.stream(stream):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            r = ss.droplet_step(r["dt_next"], solver=api.MGPCG, tol=TOL, maxit=100000)
+            e1.record(stream)
+            e1.synchronize()
+            if r["status"] != 0:
+                raise SystemExit(f"bench: session step failed: {r}")
+            t_seq += e0.elapsed_time(e1) / 1e3
+            its_seq.append(r["iters"])
+    b = api.Batch(params, stream=sh)
+    for i, st in enumerate(init):
+        for k, a in st.items():
+            b.upload(i, k, a)
+    b.sync()
+    dt = np.array(dts)
+    times, its, worst = [], [], 0.0
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        r = b.step(dt, tol=TOL, maxit=100000)
+        e1.record(stream)
+        e1.synchronize()
+        if r["status"] != 0:
+            raise SystemExit(f"bench: batched step failed: {r['status']}")
+        times.append(e0.elapsed_time(e1) / 1e3)
+        its.append(float(np.mean(r["iters"])))
+        worst = max(worst, float(np.max(r["resid"])))
+        dt = r["dt_next"]
+    b.close()
+    cells = int(sum(c.nx * c.ny for c in cases))
+    t_b = float(sum(times))
+    return {"workload": f"{count} droplets, grid side uniform in {{64, 96, ..., 512}} ({cells / 1e6:.1f} M cells), "
+                        f"radius [0.08, 0.2], density ratio log-U[1, 1000], viscosity ratio log-U[1, 100]; {steps} "
+                        f"full steps from rest, pressure to rel. residual {TOL:g}",
+            "value": count * steps / t_b, "unit": "droplet steps/s",
+            "mcells_per_s": cells * steps / t_b / 1e6, "ms_per_batch_step": 1e3 * t_b / steps,
+            "ms_per_batch_step_each": [1e3 * t for t in times],
+            "iters_mean_per_step": its, "max_rel_residual": worst,
+            "sessions_one_by_one": {"value": count / t_seq, "unit": "droplet steps/s",
+                                    "iters_mean": float(np.mean(its_seq)),
+                                    "note": "second step of every instance, asd2g_droplet_step with the MG-FCG"},
+            "speedup_vs_sessions_second_step": t_seq / times[1]}
+
+
 def run_ours(args):
     import torch
     from asd2_b200 import api
@@ -574,6 +678,7 @@ def run_ours(args):
     batched = batched_solves(sh, stream, flush) if not args.no_extra else None
     mixed = mixed_precision_errors(sh) if not args.no_extra else None
     learned = learned_pc_512(sh, stream, flush, args.weights) if not args.no_extra else None
+    bsteps = batched_steps(sh, stream) if not args.no_extra else None
     nlev = len(_mg_levels(args.n, args.n))
     per_iter = 2 + 2 * (nlev - 1) + 1
     launches = int(sum(4 + (1 + nlev) + (1 + per_iter - 2) + 8 * per_iter * math.ceil(i / 8) + 3 for i in iters))
@@ -617,6 +722,7 @@ def run_ours(args):
         "ls_large": ls_rates,
         "mixed_precision_1024": mixed,
         "learned_pc_512": learned,
+        "batched_steps_256": bsteps,
         "e2e": {"value": e2e_value, "unit": "GFM Poisson solves/s",
                 "h2d_bytes_per_step": 3 * G * 8, "d2h_bytes_per_step": G * 8},
         "gpu_launches": launches,
@@ -729,7 +835,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the 2048^2 level-set and 1024^2 mixed-precision reports")
     ap.add_argument("--weights", default=None, help="learned-preconditioner weights (default: the committed ones)")
-    ap.add_argument("--section", default=None, choices=["ls_large", "mixed_1024", "batched", "learned_pc"],
+    ap.add_argument("--section", default=None,
+                    choices=["ls_large", "mixed_1024", "batched", "batched_steps", "learned_pc", "unet_forward"],
                     help="run only this report (its JSON object on stdout), e.g. to profile it")
     args = ap.parse_args()
     if args.section:
@@ -756,6 +863,10 @@ def run_section(name, args):
     elif name == "batched":
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
         out = batched_solves(stream.cuda_stream, stream, flush)
+    elif name == "batched_steps":
+        out = batched_steps(stream.cuda_stream, stream)
+    elif name == "unet_forward":
+        out = unet_forward(stream.cuda_stream, stream)
     elif name == "learned_pc":
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
         out = learned_pc_512(stream.cuda_stream, stream, flush, args.weights)

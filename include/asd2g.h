@@ -260,7 +260,8 @@ typedef struct asd2g_batch asd2g_batch;
 int asd2g_batch_create(const asd2g_params *params, int count, void *stream, asd2g_batch **out);
 int asd2g_batch_destroy(asd2g_batch *b);
 /* Padded (nx+6)*(ny+6) arrays of instance inst: LS, KAPPA, H, DIV (inputs of
- * the assembly), PS, P (outputs of the solve). */
+ * the assembly), PS, P (outputs of the solve), and for asd2g_batch_step U, V,
+ * HS, UHAT, VHAT, LSB, LS0. */
 int asd2g_batch_upload(asd2g_batch *b, int inst, int field, const double *host);
 int asd2g_batch_download(asd2g_batch *b, int inst, int field, double *host);
 /* Device arena of a field (all instances, instance i at offset(i) doubles). */
@@ -273,6 +274,19 @@ int asd2g_batch_assemble(asd2g_batch *b, const double *dt);
  * ASD2G_NOT_CONVERGED if any instance reached maxit. */
 int asd2g_batch_solve(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_resid);
 int asd2g_batch_sync(asd2g_batch *b);
+/* The full droplet step of every instance (what asd2g_droplet_step does for
+ * one session, with the MG-FCG pressure solve), one kernel launch per phase
+ * for the whole batch: level-set advection, reinitialisation (reinit_mode 0
+ * or 2), curvature, Heaviside, FP64 volume check, intermediate velocity,
+ * divergence, GFM assembly, batched MG-FCG to tol, projection, next dt.
+ * Instances: FP64, one time order and one reinitialisation step count.
+ * dt[count]: each instance's step dt, replaced by its next dt.  Fields LS, U,
+ * V (and the others) are uploaded/downloaded with asd2g_batch_upload/download
+ * (LS, U, V, PS, P, KAPPA, H, HS, DIV, UHAT, VHAT, LSB, LS0). */
+int asd2g_batch_step(asd2g_batch *b, double *dt, int reinit_mode, double tol, int maxit, int *iters,
+                     double *rel_resid);
+/* Volume check of the last batch step per instance: sum H dx dy, sum HS dx dy. */
+int asd2g_batch_volume(asd2g_batch *b, double *sharp, double *smooth);
 
 /* ---- learned preconditioner building blocks (no reference counterpart) ----
  * 3x3 "same" convolution on the tcgen05 tensor cores: BF16 NHWC activations
