@@ -23,6 +23,8 @@
 // separate sweeps (no grid-wide barrier between them).  The level-0 "post"
 // kernel also converts z to FP64 and forms the two FCG dot products.
 #include "lsmath.cuh"
+#include <cstdlib>
+
 #include "mg.cuh"
 #include "asd2g.h"
 #include "batch.cuh"
@@ -33,6 +35,16 @@ namespace {
 
 constexpr int MT_I = 16, MT_J = 32;  // tile (rows i, columns j), must be even
 constexpr int KMODE_LEARNED = 5;      // KState mode of ASD2G_SOLVER_UNET (V-cycle + learned correction)
+
+// Programmatic dependent launch: the single-system FCG / V-cycle kernels are
+// launched with programmatic stream serialisation, so the next kernel's CTAs
+// are scheduled while this one runs; each waits for its predecessor's
+// completion (and memory) before touching data, then lets its own successor
+// launch.  Both are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 constexpr int MG_COARSE_MAX = 64;   // cells on the coarsest level
 constexpr int HI = MT_I + 4, HJ = MT_J + 4;
 
@@ -235,6 +247,7 @@ __device__ __forceinline__ void mg_pre_tile(const MgLevel &L, const MgLevel &C, 
 template <bool L0>
 __global__ void __launch_bounds__(256) k_mg_pre(MgLevel L, MgLevel C, const double *__restrict__ r64,
                                                 const KState *ks) {
+    pdl_enter();
     if (ks->done) return;
     mg_pre_tile<L0>(L, C, r64, blockIdx.y * MT_I, blockIdx.x * MT_J);
 }
@@ -313,6 +326,7 @@ template <bool L0>
 __global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float omega, const double *__restrict__ r64,
                                                  const double *__restrict__ q64, double *__restrict__ z64, int pinned,
                                                  KState *ks, double *partial) {
+    pdl_enter();
     if (ks->done) return;
     double acc[2];
     mg_post_tile<L0>(L, C, omega, r64, q64, z64, pinned, blockIdx.y * MT_I, blockIdx.x * MT_J, acc);
@@ -513,6 +527,7 @@ __device__ __forceinline__ void mg_cta_body(const MgLevel *__restrict__ lv, int 
 __global__ void __launch_bounds__(MG_CTA_THREADS) k_mg_cta_cycle(MgHier H, int s, int nlev,
                                                                 const double *__restrict__ inv, float omega,
                                                                 const KState *ks) {
+    pdl_enter();
     if (ks->done) return;
     mg_cta_body(H.l, s, nlev, inv, omega);
 }
@@ -522,6 +537,7 @@ __global__ void __launch_bounds__(MG_CTA_THREADS) k_mg_cta_cycle(MgHier H, int s
 __global__ void __launch_bounds__(256) k_fcg_a(int nx, int ny, Sys S, const double *__restrict__ z,
                                                const double *__restrict__ p_old, double *__restrict__ p_new,
                                                double *__restrict__ q, KState *ks, double *partial) {
+    pdl_enter();
     if (ks->done) return;
     const double beta = ks->beta;
     const int64_t n = (int64_t)nx * ny;
@@ -557,6 +573,7 @@ __global__ void __launch_bounds__(256) k_fcg_a(int nx, int ny, Sys S, const doub
 __global__ void __launch_bounds__(256) k_fcg_b(int64_t n, double *__restrict__ x, double *__restrict__ r,
                                                const double *__restrict__ p, const double *__restrict__ q, KState *ks,
                                                double *partial) {
+    pdl_enter();
     if (ks->done) return;
     const double alpha = ks->alpha;
     double v[1] = {0.0};
@@ -589,6 +606,7 @@ __global__ void __launch_bounds__(256) k_fcg_b(int64_t n, double *__restrict__ x
 // otherwise it resumes from x with the fresh r and a new direction (beta = 0).
 __global__ void __launch_bounds__(256) k_fcg_replace(int nx, int ny, Sys S, const double *__restrict__ x,
                                                      double *__restrict__ r, KState *ks, double *partial) {
+    pdl_enter();
     if (!ks->done || ks->verified || ks->status != 0) return;
     const int64_t n = (int64_t)nx * ny;
     double v[1] = {0.0};
@@ -631,6 +649,7 @@ __global__ void __launch_bounds__(256) k_fcg_replace(int nx, int ny, Sys S, cons
 // r = b, x = 0, p = 0, ||b||; the first V-cycle follows.
 __global__ void k_fcg_init(int64_t n, Sys S, double *__restrict__ x, double *__restrict__ r, double *__restrict__ p,
                            KState *ks, double *partial) {
+    pdl_enter();
     double v[1] = {0.0};
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         const double bk = S.b[k];
@@ -1158,6 +1177,30 @@ bool mg_cta_prepare(const MgLevel *lv, int nlev) {
                                 (int)MG_CTA_SMEM_BOUND) == cudaSuccess;
 }
 
+// Launch with programmatic stream serialisation (see pdl_enter); ASD2G_PDL=0
+// in the environment launches plainly (for comparisons).
+static bool pdl_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("ASD2G_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+template <typename... P, typename... A>
+static void pdl_launch(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A... args) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k, static_cast<P>(args)...);
+}
+
 // One V-cycle: input r (FP64 level-0 rhs), output z (FP64), with the FCG
 // beta update folded into the level-0 post pass.  Levels 0 .. s-1 run as
 // tile kernels over the whole GPU, levels s .. nlev-1 in one CTA.
@@ -1166,19 +1209,20 @@ static void enqueue_vcycle(MgLevel *lv, int nlev, const double *coarse_inv, cons
     const dim3 blk(32, 8);
     const int s = mg_cta_level(lv, nlev);
     for (int l = 0; l < s; l++) {
-        if (l == 0) k_mg_pre<true><<<tile_grid(lv[0]), blk, 0, st>>>(lv[0], lv[1], r, ks);
-        else k_mg_pre<false><<<tile_grid(lv[l]), blk, 0, st>>>(lv[l], lv[l + 1], nullptr, ks);
+        if (l == 0) pdl_launch(k_mg_pre<true>, tile_grid(lv[0]), blk, 0, st, lv[0], lv[1], r, ks);
+        else pdl_launch(k_mg_pre<false>, tile_grid(lv[l]), blk, 0, st, lv[l], lv[l + 1], (const double *)nullptr, ks);
     }
     MgHier H{};
     for (int l = 0; l < nlev; l++) H.l[l] = lv[l];
     const float omega = 1.9f;
-    k_mg_cta_cycle<<<1, MG_CTA_THREADS, mg_cta_smem(H, s, nlev), st>>>(H, s, nlev, coarse_inv, omega, ks);
+    pdl_launch(k_mg_cta_cycle, dim3(1), dim3(MG_CTA_THREADS), mg_cta_smem(H, s, nlev), st, H, s, nlev, coarse_inv, omega,
+               ks);
     for (int l = s - 1; l >= 0; l--) {
         if (l == 0)
-            k_mg_post<true><<<tile_grid(lv[0]), blk, 0, st>>>(lv[0], lv[1], omega, r, q, z, pinned, ks, partial);
+            pdl_launch(k_mg_post<true>, tile_grid(lv[0]), blk, 0, st, lv[0], lv[1], omega, r, q, z, pinned, ks, partial);
         else
-            k_mg_post<false><<<tile_grid(lv[l]), blk, 0, st>>>(lv[l], lv[l + 1], omega, nullptr, nullptr, nullptr, 0,
-                                                              ks, partial);
+            pdl_launch(k_mg_post<false>, tile_grid(lv[l]), blk, 0, st, lv[l], lv[l + 1], omega, (const double *)nullptr,
+                       (const double *)nullptr, (double *)nullptr, 0, ks, partial);
     }
 }
 
@@ -1187,7 +1231,7 @@ bool launch_fcg_init(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const 
                      cudaStream_t st) {
     if (partial_len < mg_partial_len(nx, ny)) return false;
     const int64_t n = (int64_t)nx * ny;
-    k_fcg_init<<<red_blocks(n), 256, 0, st>>>(n, S, x, r, p, ks, partial);
+    pdl_launch(k_fcg_init, dim3(red_blocks(n)), dim3(256), 0, st, n, S, x, r, p, ks, partial);
     cudaMemsetAsync(q, 0, sizeof(double) * n, st);
     enqueue_vcycle(lv, nlev, coarse_inv, r, q, z, S.pinned, ks, partial, st);
     return true;
@@ -1199,8 +1243,8 @@ bool launch_fcg_iter(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const 
     if (partial_len < mg_partial_len(nx, ny)) return false;
     const int64_t n = (int64_t)nx * ny;
     const int nb = red_blocks(n);
-    k_fcg_a<<<nb, 256, 0, st>>>(nx, ny, S, z, p_old, p_new, q, ks, partial);
-    k_fcg_b<<<nb, 256, 0, st>>>(n, x, r, p_new, q, ks, partial);
+    pdl_launch(k_fcg_a, dim3(nb), dim3(256), 0, st, nx, ny, S, (const double *)z, p_old, p_new, q, ks, partial);
+    pdl_launch(k_fcg_b, dim3(nb), dim3(256), 0, st, n, x, r, (const double *)p_new, (const double *)q, ks, partial);
     enqueue_vcycle(lv, nlev, coarse_inv, r, q, z, S.pinned, ks, partial, st);
     return true;
 }
@@ -1210,7 +1254,7 @@ bool launch_fcg_check(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const
                       cudaStream_t st) {
     if (partial_len < mg_partial_len(nx, ny)) return false;
     const int64_t n = (int64_t)nx * ny;
-    k_fcg_replace<<<red_blocks(n), 256, 0, st>>>(nx, ny, S, x, r, ks, partial);
+    pdl_launch(k_fcg_replace, dim3(red_blocks(n)), dim3(256), 0, st, nx, ny, S, x, r, ks, partial);
     enqueue_vcycle(lv, nlev, coarse_inv, r, q, z, S.pinned, ks, partial, st);
     return true;
 }

@@ -537,15 +537,10 @@ def run_ours(args):
     from asd2_b200 import api
     from asd2_b200 import workloads as W
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from asd2_b200 import replicas as R
+    rank, world, local = R.rank_env()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist = R.init_group("nccl")
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
 
@@ -590,12 +585,8 @@ def run_ours(args):
     true_res = s.true_residual()
     if not true_res <= 10 * TOL:
         raise SystemExit(f"bench: true relative residual {true_res:.3e} above {10 * TOL:g}")
-    t_total = float(sum(times))
-    if dist:
-        t = torch.tensor([t_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_total = float(t.item())
-    value = world * args.steps / t_total
+    t_total = R.job_time(float(sum(times)), dist, "cuda")
+    value = R.job_rate(args.steps, world, t_total)
 
     # assembly alone (to split the iteration time out of the solve time)
     ta = []
@@ -639,12 +630,8 @@ def run_ours(args):
         e1.synchronize()
         if k >= args.warmup:
             e2e_t.append(e0.elapsed_time(e1) / 1e3)
-    e2e_total = float(sum(e2e_t))
-    if dist:
-        t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * args.steps / e2e_total
+    e2e_total = R.job_time(float(sum(e2e_t)), dist, "cuda")
+    e2e_value = R.job_rate(args.steps, world, e2e_total)
 
     # level-set Mcells/s on the 128^2 perturbed-circle workload
     lc = W.perturbed_circle(LS_GRID, seed=args.seed)
@@ -785,8 +772,8 @@ def cpu_baseline(snap, case, dt, args, procs=1, budget_s=None):
 
 def run_reference(args):
     """Reference arm: CPU implementation of the same solves on all host cores."""
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    from asd2_b200 import replicas as R
+    if not R.reference_rank_runs(R.rank_env()[0]):
         return
     # Inputs: the same GFM system, generated on the CPU by the restatement's
     # own droplet steps (no GPU is needed for this arm).
