@@ -174,15 +174,21 @@ __global__ void k_reinit_b(Grid g, LsConstT<T> K, const T *__restrict__ ls1, con
 // with hd = UpdateHeavisideFuncDeriv(tmp).  Sussman mode: base = phi
 // (levelset2d.cpp:368-372); MinRK2+Sussman: base = tmp.
 template <typename T>
-__global__ void k_reinit_c(Grid g, LsConstT<T> K, const T *__restrict__ tmp, const T *__restrict__ ls0, const T *base,
-                           T *out, int mirror) {
-    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
+__device__ __forceinline__ void reinit_c_tile(const Grid &g, const LsConstT<T> &K, const T *__restrict__ tmp,
+                                              const T *__restrict__ ls0, const T *base, T *out, int mirror, int bx,
+                                              int by) {
+    const int j = NB + bx * TJ + threadIdx.x, i = NB + by * TI + threadIdx.y;
     if (i >= g.nx + NB || j >= g.ny + NB) return;
     const int64_t c = IX(g, i, j);
     const T hd = heaviside_deriv(tmp[c], K.eps);
     const T val = base[c] + sussman_constraint(g, K, tmp, ls0, hd, i, j);
     out[c] = val;
     if (mirror) p_mirror_store(g, out, i, j, val);
+}
+template <typename T>
+__global__ void k_reinit_c(Grid g, LsConstT<T> K, const T *__restrict__ tmp, const T *__restrict__ ls0, const T *base,
+                           T *out, int mirror) {
+    reinit_c_tile<T>(g, K, tmp, ls0, base, out, mirror, blockIdx.x, blockIdx.y);
 }
 
 
