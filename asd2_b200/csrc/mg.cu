@@ -266,9 +266,16 @@ __device__ __forceinline__ void mg_post_tile(const MgLevel &L, const MgLevel &C,
                                              double (&acc)[2]) {
     __shared__ Tile T;
     __shared__ float ec[MT_I / 2 + 2][MT_J / 2 + 2];
-    load_tile<L0>(T, L, r64, i0, j0);
+    // the tile's global reads are issued before the first barrier: its
+    // coefficients and rhs, the pre-smoothed e, the coarse correction
     const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
+    load_tile<L0>(T, L, r64, i0, j0);
     const int I0 = i0 / 2 - 1, J0 = j0 / 2 - 1;
+    for (int t = tid; t < HI * HJ; t += nt) {
+        const int a = t / HJ, b = t % HJ;
+        const int i = i0 - 2 + a, j = j0 - 2 + b;
+        T.e[a][b] = (i >= 0 && i < L.nx && j >= 0 && j < L.ny) ? L.e[LK(L, i, j)] : 0.0f;
+    }
     for (int t = tid; t < (MT_I / 2 + 2) * (MT_J / 2 + 2); t += nt) {
         const int a = t / (MT_J / 2 + 2), b = t % (MT_J / 2 + 2);
         const int I = I0 + a, J = J0 + b;
@@ -278,9 +285,7 @@ __device__ __forceinline__ void mg_post_tile(const MgLevel &L, const MgLevel &C,
     for (int t = tid; t < HI * HJ; t += nt) {
         const int a = t / HJ, b = t % HJ;
         const int i = i0 - 2 + a, j = j0 - 2 + b;
-        float e = 0.0f;
-        if (i >= 0 && i < L.nx && j >= 0 && j < L.ny) e = L.e[LK(L, i, j)] + omega * ec[(i >> 1) - I0][(j >> 1) - J0];
-        T.e[a][b] = e;
+        if (i >= 0 && i < L.nx && j >= 0 && j < L.ny) T.e[a][b] += omega * ec[(i >> 1) - I0][(j >> 1) - J0];
     }
     __syncthreads();
     for (int t = tid; t < (HI - 2) * (HJ - 2); t += nt) {
@@ -724,17 +729,24 @@ __global__ void k_bset_kstate(const BInst *__restrict__ insts, int count, double
 __global__ void __launch_bounds__(256) k_bfcg_init(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks) {
     const BChunk w = chunks[blockIdx.x];
     const BInst &I = insts[w.inst];
-    const int64_t k0 = (int64_t)w.c * FCG_CHUNK;
+    const int64_t n = I.n, k0 = (int64_t)w.c * FCG_CHUNK;
+    const double *__restrict__ b = I.S.b;
+    double *__restrict__ x = I.x;
+    double *__restrict__ r = I.r;
+    double *__restrict__ pa = I.pa;
+    double *__restrict__ q = I.q;
     double v[1] = {0.0};
-    for (int t = threadIdx.x; t < FCG_CHUNK; t += blockDim.x) {
-        const int64_t k = k0 + t;
-        if (k >= I.n) break;
-        const double bk = I.S.b[k];
-        I.x[k] = 0.0;
-        I.r[k] = bk;
-        I.pa[k] = 0.0;
-        I.q[k] = 0.0;
-        v[0] += bk * bk;
+#pragma unroll
+    for (int u = 0; u < FCG_CHUNK / 256; u++) {
+        const int64_t k = k0 + threadIdx.x + 256 * u;
+        if (k < n) {
+            const double bk = b[k];
+            x[k] = 0.0;
+            r[k] = bk;
+            pa[k] = 0.0;
+            q[k] = 0.0;
+            v[0] += bk * bk;
+        }
     }
     double tot[1];
     KState *ks = I.ks;
@@ -766,6 +778,9 @@ __device__ __forceinline__ double sys_apply(const Sys &S, int nx, int ny, const 
     return y;
 }
 
+// The batched kernels copy what they use of the instance descriptor into
+// registers first: through a reference into global memory every store to a
+// field would force the compiler to reload the descriptor's pointers.
 __global__ void __launch_bounds__(256) k_bfcg_a(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks,
                                                 int parity) {
     const BChunk w = chunks[blockIdx.x];
@@ -773,28 +788,35 @@ __global__ void __launch_bounds__(256) k_bfcg_a(const BInst *__restrict__ insts,
     KState *ks = I.ks;
     if (ks->done) return;
     const double beta = ks->beta;
-    const double *p_old = parity ? I.pb : I.pa;
-    double *p_new = parity ? I.pa : I.pb;
-    const int nx = I.g.nx, ny = I.g.ny;
-    const int64_t k0 = (int64_t)w.c * FCG_CHUNK;
+    const double *__restrict__ p_old = parity ? I.pb : I.pa;
+    double *__restrict__ p_new = parity ? I.pa : I.pb;
+    const double *__restrict__ z = I.z;
+    const double *__restrict__ diag = I.S.diag;
+    const double *__restrict__ ce = I.S.ce;
+    const double *__restrict__ cn = I.S.cn;
+    double *__restrict__ q = I.q;
+    const int nx = I.g.nx, ny = I.g.ny, pinned = I.S.pinned;
+    const int64_t n = I.n, k0 = (int64_t)w.c * FCG_CHUNK;
     double v[1] = {0.0};
-    for (int t = threadIdx.x; t < FCG_CHUNK; t += blockDim.x) {
-        const int64_t k = k0 + t;
-        if (k >= I.n) break;
-        const int ii = (int)(k / ny), jj = (int)(k % ny);
-        auto pv = [&](int64_t m) { return I.z[m] + beta * p_old[m]; };
-        const double pc = pv(k);
-        double y = 0.0;
-        if (!(I.S.pinned && k == 0)) {
-            if (jj > 0) y += -I.S.cn[k - 1] * pv(k - 1);
-            if (ii > 0) y += -I.S.ce[k - ny] * pv(k - ny);
-            y += I.S.diag[k] * pc;
-            if (ii < nx - 1) y += -I.S.ce[k] * pv(k + ny);
-            if (jj < ny - 1) y += -I.S.cn[k] * pv(k + 1);
+#pragma unroll
+    for (int u = 0; u < FCG_CHUNK / 256; u++) {
+        const int64_t k = k0 + threadIdx.x + 256 * u;
+        if (k < n) {
+            const int ii = (int)(k / ny), jj = (int)(k % ny);
+            auto pv = [&](int64_t m) { return z[m] + beta * p_old[m]; };
+            const double pc = pv(k);
+            double y = 0.0;
+            if (!(pinned && k == 0)) {
+                if (jj > 0) y += -cn[k - 1] * pv(k - 1);
+                if (ii > 0) y += -ce[k - ny] * pv(k - ny);
+                y += diag[k] * pc;
+                if (ii < nx - 1) y += -ce[k] * pv(k + ny);
+                if (jj < ny - 1) y += -cn[k] * pv(k + 1);
+            }
+            p_new[k] = pc;
+            q[k] = y;
+            v[0] += pc * y;
         }
-        p_new[k] = pc;
-        I.q[k] = y;
-        v[0] += pc * y;
     }
     double tot[1];
     if (mg_reduce<1>(v, I.partial, &ks->counter, w.c, I.chunks, tot)) {
@@ -814,16 +836,21 @@ __global__ void __launch_bounds__(256) k_bfcg_b(const BInst *__restrict__ insts,
     KState *ks = I.ks;
     if (ks->done) return;
     const double alpha = ks->alpha;
-    const double *p = parity ? I.pa : I.pb;
-    const int64_t k0 = (int64_t)w.c * FCG_CHUNK;
+    const double *__restrict__ p = parity ? I.pa : I.pb;
+    const double *__restrict__ q = I.q;
+    double *__restrict__ x = I.x;
+    double *__restrict__ r = I.r;
+    const int64_t n = I.n, k0 = (int64_t)w.c * FCG_CHUNK;
     double v[1] = {0.0};
-    for (int t = threadIdx.x; t < FCG_CHUNK; t += blockDim.x) {
-        const int64_t k = k0 + t;
-        if (k >= I.n) break;
-        I.x[k] += alpha * p[k];
-        const double rk = I.r[k] - alpha * I.q[k];
-        I.r[k] = rk;
-        v[0] += rk * rk;
+#pragma unroll
+    for (int u = 0; u < FCG_CHUNK / 256; u++) {
+        const int64_t k = k0 + threadIdx.x + 256 * u;
+        if (k < n) {
+            x[k] += alpha * p[k];
+            const double rk = r[k] - alpha * q[k];
+            r[k] = rk;
+            v[0] += rk * rk;
+        }
     }
     double tot[1];
     if (mg_reduce<1>(v, I.partial, &ks->counter, w.c, I.chunks, tot)) {
@@ -846,14 +873,20 @@ __global__ void __launch_bounds__(256) k_bfcg_replace(const BInst *__restrict__ 
     const BInst &I = insts[w.inst];
     KState *ks = I.ks;
     if (!ks->done || ks->verified || ks->status != 0) return;
-    const int64_t k0 = (int64_t)w.c * FCG_CHUNK;
+    const Sys S = I.S;
+    const int nx = I.g.nx, ny = I.g.ny;
+    const double *__restrict__ x = I.x;
+    double *__restrict__ r = I.r;
+    const int64_t n = I.n, k0 = (int64_t)w.c * FCG_CHUNK;
     double v[1] = {0.0};
-    for (int t = threadIdx.x; t < FCG_CHUNK; t += blockDim.x) {
-        const int64_t k = k0 + t;
-        if (k >= I.n) break;
-        const double rk = (I.S.pinned && k == 0) ? 0.0 : I.S.b[k] - sys_apply(I.S, I.g.nx, I.g.ny, I.x, k);
-        I.r[k] = rk;
-        v[0] += rk * rk;
+#pragma unroll
+    for (int u = 0; u < FCG_CHUNK / 256; u++) {
+        const int64_t k = k0 + threadIdx.x + 256 * u;
+        if (k < n) {
+            const double rk = (S.pinned && k == 0) ? 0.0 : S.b[k] - sys_apply(S, nx, ny, x, k);
+            r[k] = rk;
+            v[0] += rk * rk;
+        }
     }
     double tot[1];
     if (mg_reduce<1>(v, I.partial, &ks->counter, w.c, I.chunks, tot)) {

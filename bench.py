@@ -328,6 +328,14 @@ def batched_solves(sh, stream, flush, count=BATCH_COUNT):
     b.close()
     t_b = float(np.median(times))
     cells = int(sum(c.nx * c.ny for c in cases))
+    peak = 6650.0
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = json.load(f).get("hbm_gbs", peak)
+    except Exception:
+        pass
+    # algorithmic bytes: assembly 64 B/unknown + MG-FCG 180 B/unknown/iteration (instances' own counts)
+    alg = float(sum((64 + MG_BYTES_PER_UNKNOWN_ITER * int(it)) * c.nx * c.ny for c, it in zip(cases, res["iters"])))
     return {"workload": f"{count} droplets, grid side uniform in {{64, 96, ..., 512}} ({cells / 1e6:.1f} M unknowns), "
                         "radius [0.08, 0.2], density ratio log-U[1, 1000], viscosity ratio log-U[1, 100]; "
                         "each system after one full step from rest",
@@ -339,6 +347,9 @@ def batched_solves(sh, stream, flush, count=BATCH_COUNT):
                                    "solver": "FP64 Jacobi-PCG per system, one system after another"},
             "single_mg_sequential": {"value": count / t_mg, "unit": "GFM Poisson solves/s"},
             "speedup_vs_fp64_cg": t_cg / t_b,
+            "roofline": {"bound": "hbm", "achieved": alg / t_b / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / t_b / 1e9 / peak,
+                         "bytes": "assembly 64 B + MG-FCG 180 B per unknown and iteration of each instance"},
             "l2": "flushed (256 MB write) before each timed batch / system"}
 
 
@@ -822,6 +833,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the 2048^2 level-set and 1024^2 mixed-precision reports")
     ap.add_argument("--weights", default=None, help="learned-preconditioner weights (default: the committed ones)")
+    ap.add_argument("--batch-count", type=int, default=BATCH_COUNT,
+                    help="droplets of the batched sections (default 256; smaller for profiling)")
     ap.add_argument("--section", default=None,
                     choices=["ls_large", "mixed_1024", "batched", "batched_steps", "learned_pc", "unet_forward"],
                     help="run only this report (its JSON object on stdout), e.g. to profile it")
@@ -849,9 +862,9 @@ def run_section(name, args):
         out = level_set_rates(stream.cuda_stream, stream, flush, peak)
     elif name == "batched":
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-        out = batched_solves(stream.cuda_stream, stream, flush)
+        out = batched_solves(stream.cuda_stream, stream, flush, count=args.batch_count)
     elif name == "batched_steps":
-        out = batched_steps(stream.cuda_stream, stream)
+        out = batched_steps(stream.cuda_stream, stream, count=args.batch_count)
     elif name == "unet_forward":
         out = unet_forward(stream.cuda_stream, stream)
     elif name == "learned_pc":
