@@ -67,7 +67,7 @@ EXPORTS = [
     "asd2g_apply_bc_side", "asd2g_update_ntk", "asd2g_csr_solve", "asd2g_volume", "asd2g_last_volume",
     "asd2g_batch_create", "asd2g_batch_destroy", "asd2g_batch_upload", "asd2g_batch_download",
     "asd2g_batch_field_ptr", "asd2g_batch_offset", "asd2g_batch_assemble", "asd2g_batch_solve", "asd2g_batch_sync",
-    "asd2g_batch_step", "asd2g_batch_volume",
+    "asd2g_batch_step", "asd2g_batch_volume", "asd2g_batch_tile_shape",
     "asd2g_conv_wpack_bytes", "asd2g_conv_pack_weights", "asd2g_conv3x3_bf16",
     "asd2g_unet_create", "asd2g_unet_destroy", "asd2g_unet_nparams", "asd2g_unet_init", "asd2g_unet_set_params",
     "asd2g_unet_get_params", "asd2g_unet_get_grads", "asd2g_unet_forward", "asd2g_unet_train_step",
@@ -135,6 +135,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_batch_solve": ([S, D, I, ip, dp], I),
         "asd2g_batch_step": ([S, dp, I, D, I, ip, dp], I),
         "asd2g_batch_volume": ([S, dp, dp], I),
+        "asd2g_batch_tile_shape": ([S, C.POINTER(I), C.POINTER(I), C.POINTER(C.c_float)], I),
         "asd2g_conv_wpack_bytes": ([I, I], C.c_size_t),
         "asd2g_conv_pack_weights": ([C.c_void_p, I, I, I, I, C.c_void_p, C.c_void_p], I),
         "asd2g_conv3x3_bf16": ([C.c_void_p, I, I, I, I, C.c_void_p, C.c_void_p, I, C.c_void_p, C.c_void_p, I,
@@ -505,6 +506,12 @@ class Batch:
         a, b = np.zeros(n), np.zeros(n)
         self._check(self.L.asd2g_batch_volume(self.h, a, b))
         return a, b
+
+    def tile_shape(self):
+        """(rows, cols) of the multigrid tiles in use and the tuning trial times (ms) per candidate."""
+        r, c, ms = C.c_int(), C.c_int(), (C.c_float * 3)()
+        self._check(self.L.asd2g_batch_tile_shape(self.h, C.byref(r), C.byref(c), ms))
+        return (r.value, c.value), list(ms)
 
     def sync(self):
         self._check(self.L.asd2g_batch_sync(self.h))

@@ -7,6 +7,7 @@
 // chunks of iterations are captured once in a CUDA graph and replayed until
 // every instance has converged.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -38,6 +39,10 @@ struct asd2g_batch {
     int ncell_tiles = 0;
     BatchPlan plan{};
     BStepPlan splan{};
+    const BTile *shape_lists[MG_NSHAPES][MG_MAX_LEVELS] = {};  // uploaded tile lists per shape
+    int shape_forced = -1;     // ASD2G_MG_TILE
+    bool shape_tuned = false;  // the first solve timed every shape
+    double shape_ms[MG_NSHAPES] = {};
     KState *ks = nullptr;
     KState *ks_host = nullptr;
     cudaGraphExec_t chunk_exec = nullptr;
@@ -101,6 +106,38 @@ void release(asd2g_batch *b) {
     if (b->ks_host) cudaFreeHost(b->ks_host);
     if (b->own_stream && b->st) cudaStreamDestroy(b->st);
     delete b;
+}
+
+// Tile lists of the multigrid tile levels for MG_SHAPES[shape], and every
+// instance's level-0 tile count (the ticket count of its level-0 dots).
+int set_mg_shape(asd2g_batch *b, int shape) {
+    const int ti = MG_SHAPES[shape][0], tj = MG_SHAPES[shape][1];
+    std::vector<std::vector<BTile>> mgt(MG_MAX_LEVELS);
+    for (int i = 0; i < b->count; i++) {
+        BInst &I = b->hinst[i];
+        for (int l = 0; l < I.s_cta; l++) {
+            const int tx = (I.lv[l].ny + tj - 1) / tj, ty = (I.lv[l].nx + ti - 1) / ti;
+            for (int by = 0; by < ty; by++)
+                for (int bx = 0; bx < tx; bx++) mgt[l].push_back({i, bx, by});
+        }
+        I.tiles0 = ((I.lv[0].ny + tj - 1) / tj) * ((I.lv[0].nx + ti - 1) / ti);
+    }
+    BatchPlan &P = b->plan;
+    int rc = ASD2G_OK;
+    for (int l = 0; l < MG_MAX_LEVELS && !rc; l++) {
+        if (b->shape_lists[shape][l] == nullptr && !mgt[l].empty())
+            rc = upload_list(b, mgt[l], &b->shape_lists[shape][l]);
+        P.mg_tiles[l] = b->shape_lists[shape][l];
+        P.nmg_tiles[l] = (int)mgt[l].size();
+    }
+    if (rc) return rc;
+    P.shape = shape;
+    cudaMemcpyAsync(b->dinst, b->hinst.data(), sizeof(BInst) * b->count, cudaMemcpyHostToDevice, b->st);
+    if (b->chunk_exec) {  // the captured chunk holds the previous shape's launches
+        cudaGraphExecDestroy(b->chunk_exec);
+        b->chunk_exec = nullptr;
+    }
+    return check("batch tile lists");
 }
 
 int build(asd2g_batch *b) {
@@ -209,7 +246,6 @@ int build(asd2g_batch *b) {
     std::vector<BTile> cells;
     std::vector<BChunk> chunks, padc, ghostc;
     std::vector<std::vector<BChunk>> lvl(MG_MAX_LEVELS);
-    std::vector<std::vector<BTile>> mgt(MG_MAX_LEVELS);
     int max_s = 0, max_nlev = 0;
     for (int i = 0; i < count; i++) {
         const BInst &I = b->hinst[i];
@@ -223,11 +259,6 @@ int build(asd2g_batch *b) {
         for (int l = 1; l < I.nlev; l++) {
             const int64_t m = (int64_t)I.lv[l].nx * I.lv[l].ny;
             for (int c = 0; c < (int)((m + FCG_CHUNK - 1) / FCG_CHUNK); c++) lvl[l].push_back({i, c});
-        }
-        for (int l = 0; l < I.s_cta; l++) {
-            const int tx = (I.lv[l].ny + 31) / 32, ty = (I.lv[l].nx + 15) / 16;
-            for (int by = 0; by < ty; by++)
-                for (int bx = 0; bx < tx; bx++) mgt[l].push_back({i, bx, by});
         }
         max_s = I.s_cta > max_s ? I.s_cta : max_s;
         max_nlev = I.nlev > max_nlev ? I.nlev : max_nlev;
@@ -246,12 +277,13 @@ int build(asd2g_batch *b) {
     P.nchunks = (int)chunks.size();
     for (int l = 0; l < MG_MAX_LEVELS && !rc; l++) {
         P.nlvl_chunks[l] = (int)lvl[l].size();
-        P.nmg_tiles[l] = (int)mgt[l].size();
         if (!lvl[l].empty()) rc = upload_list(b, lvl[l], &P.lvl_chunks[l]);
-        if (!rc && !mgt[l].empty()) rc = upload_list(b, mgt[l], &P.mg_tiles[l]);
     }
     P.max_s = max_s;
     P.max_nlev = max_nlev;
+    const char *forced = std::getenv("ASD2G_MG_TILE");  // a fixed shape index (no tuning)
+    b->shape_forced = forced && forced[0] >= '0' && forced[0] < '0' + MG_NSHAPES ? forced[0] - '0' : -1;
+    if (!rc) rc = set_mg_shape(b, b->shape_forced >= 0 ? b->shape_forced : 0);
     BStepPlan &SP = b->splan;
     SP.insts = b->dinst;
     SP.count = count;
@@ -482,6 +514,35 @@ int solve_impl(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_re
     const BatchPlan &P = b->plan;
     launch_batch_set_kstate(P, tol, maxit, b->st);
     launch_batch_mg_setup(P, b->st);
+    if (!b->shape_tuned && b->shape_forced < 0) {
+        // tile-shape tuning on this batch's own hierarchy (first solve only):
+        // four FCG iterations per shape, none allowed to stop early
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        int best = 0;
+        for (int sh = 0; sh < MG_NSHAPES; sh++) {
+            int rc = set_mg_shape(b, sh);
+            if (rc) return rc;
+            launch_batch_set_kstate(P, 0.0, 1 << 30, b->st);
+            launch_batch_fcg_init(P, b->st);
+            launch_batch_fcg_iter(P, 0, b->st);  // first launch of this shape's kernels
+            cudaEventRecord(e0, b->st);
+            for (int k = 0; k < 4; k++) launch_batch_fcg_iter(P, (k + 1) & 1, b->st);
+            cudaEventRecord(e1, b->st);
+            if (cudaEventSynchronize(e1) != cudaSuccess) return check("batch tile tuning");
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            b->shape_ms[sh] = ms;
+            if (ms < b->shape_ms[best]) best = sh;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        b->shape_tuned = true;
+        int rc = set_mg_shape(b, best);
+        if (rc) return rc;
+        launch_batch_set_kstate(P, tol, maxit, b->st);
+    }
     launch_batch_fcg_init(P, b->st);
     int rc = check("batch solve set-up");
     if (rc) return rc;
@@ -522,6 +583,15 @@ int solve_impl(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_re
 }  // namespace
 
 extern "C" {
+
+int asd2g_batch_tile_shape(asd2g_batch *b, int *rows, int *cols, float *trial_ms) {
+    if (!b) return api_fail(ASD2G_E_ARG, "null batch");
+    if (rows) *rows = MG_SHAPES[b->plan.shape][0];
+    if (cols) *cols = MG_SHAPES[b->plan.shape][1];
+    if (trial_ms)
+        for (int k = 0; k < MG_NSHAPES; k++) trial_ms[k] = (float)b->shape_ms[k];
+    return ASD2G_OK;
+}
 
 int asd2g_batch_sync(asd2g_batch *b) {
     if (!b) return api_fail(ASD2G_E_ARG, "null batch");

@@ -59,10 +59,17 @@ constexpr int FCG_CHUNK = 1024;  // 256 threads x 4
 void launch_batch_assemble(const BInst *insts, const BTile *tiles, int ntiles, cudaStream_t st);
 void launch_batch_scatter(const BInst *insts, const BTile *tiles, int ntiles, cudaStream_t st);
 
+// Multigrid tile shapes (rows i x columns j) the batched solve can use; the
+// first is the single-system tile and has the most tiles (it sizes the
+// partial-sum slots).
+constexpr int MG_SHAPES[3][2] = {{16, 32}, {32, 32}, {16, 64}};
+constexpr int MG_NSHAPES = 3;
+
 // mg.cu: set-up of every instance's hierarchy, then the solver phases.
 // lvl_chunks[l] lists the chunks of level-l cells of the instances that have
-// a level l (element-wise set-up kernels); mg_tiles[l] the 16 x 32 tiles of
-// level l of the instances whose level l is a tile level (l < s_cta).
+// a level l (element-wise set-up kernels); mg_tiles[l] the tiles (shape
+// MG_SHAPES[shape]) of level l of the instances whose level l is a tile level
+// (l < s_cta).
 struct BatchPlan {
     const BInst *insts;
     int count;
@@ -74,6 +81,7 @@ struct BatchPlan {
     int nmg_tiles[MG_MAX_LEVELS];
     int max_s;            // largest s_cta over the batch
     int max_nlev;
+    int shape;            // MG_SHAPES index of the tiles in mg_tiles
 };
 void launch_batch_mg_setup(const BatchPlan &P, cudaStream_t st);
 bool launch_batch_fcg_init(const BatchPlan &P, cudaStream_t st);

@@ -161,14 +161,18 @@ __global__ void k_mg_coarsen(MgLevel F, MgLevel C) {
 }
 
 // ---------------------------------------------------------- tile loads --
-struct Tile {
+// A tile of TI_ x TJ_ cells plus its 2-cell halo (the batched solve picks TI_
+// x TJ_ from MG_SHAPES by timing them on its own hierarchy).
+template <int TI_, int TJ_> struct TileT {
+    static constexpr int HI = TI_ + 4, HJ = TJ_ + 4;
     float e[HI][HJ], f[HI][HJ], d[HI][HJ], ce[HI][HJ], cn[HI][HJ];
 };
 
 // Load f, d, ce, cn on the tile + 2-cell halo (out of domain: f 0, d 1,
 // couplings 0).  Level 0 reads f from the FP64 residual.
-template <bool L0>
-__device__ __forceinline__ void load_tile(Tile &T, const MgLevel &L, const double *__restrict__ r64, int i0, int j0) {
+template <bool L0, class TT>
+__device__ __forceinline__ void load_tile(TT &T, const MgLevel &L, const double *__restrict__ r64, int i0, int j0) {
+    constexpr int HI = TT::HI, HJ = TT::HJ;
     const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
     for (int t = tid; t < HI * HJ; t += nt) {
         const int a = t / HJ, b = t % HJ;
@@ -189,7 +193,7 @@ __device__ __forceinline__ void load_tile(Tile &T, const MgLevel &L, const doubl
 }
 
 // Gauss-Seidel update of local cell (a, b) from its four neighbours.
-__device__ __forceinline__ float gs_cell(const Tile &T, int a, int b) {
+template <class TT> __device__ __forceinline__ float gs_cell(const TT &T, int a, int b) {
     const float s = T.f[a][b] + T.ce[a - 1][b] * T.e[a - 1][b] + T.ce[a][b] * T.e[a + 1][b] +
                     T.cn[a][b - 1] * T.e[a][b - 1] + T.cn[a][b] * T.e[a][b + 1];
     return s / T.d[a][b];
@@ -198,11 +202,13 @@ __device__ __forceinline__ float gs_cell(const Tile &T, int a, int b) {
 // ------------------------------------------------------------ pre pass --
 // From e = 0: red sweep on tile+2, black on tile+1, residual on the tile,
 // restriction (2x2 sums) into the next level's f.  Stores e (tile).
-template <bool L0>
+template <bool L0, int TI_ = MT_I, int TJ_ = MT_J>
 __device__ __forceinline__ void mg_pre_tile(const MgLevel &L, const MgLevel &C, const double *__restrict__ r64,
                                             int i0, int j0) {
-    __shared__ Tile T;
-    __shared__ float res[MT_I][MT_J];
+    using TT = TileT<TI_, TJ_>;
+    constexpr int HI = TT::HI, HJ = TT::HJ;
+    __shared__ TT T;
+    __shared__ float res[TI_][TJ_];
     load_tile<L0>(T, L, r64, i0, j0);
     __syncthreads();
     const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
@@ -221,9 +227,9 @@ __device__ __forceinline__ void mg_pre_tile(const MgLevel &L, const MgLevel &C, 
     }
     __syncthreads();
     // residual on the tile; store e
-    for (int t = tid; t < MT_I * MT_J; t += nt) {
-        const int a = 2 + t / MT_J, b = 2 + t % MT_J;
-        const int i = i0 + t / MT_J, j = j0 + t % MT_J;
+    for (int t = tid; t < TI_ * TJ_; t += nt) {
+        const int a = 2 + t / TJ_, b = 2 + t % TJ_;
+        const int i = i0 + t / TJ_, j = j0 + t % TJ_;
         float rr = 0.0f;
         if (i < L.nx && j < L.ny) {
             const float Ae = T.d[a][b] * T.e[a][b] - T.ce[a - 1][b] * T.e[a - 1][b] - T.ce[a][b] * T.e[a + 1][b] -
@@ -231,12 +237,12 @@ __device__ __forceinline__ void mg_pre_tile(const MgLevel &L, const MgLevel &C, 
             rr = T.f[a][b] - Ae;
             L.e[LK(L, i, j)] = T.e[a][b];
         }
-        res[t / MT_J][t % MT_J] = rr;
+        res[t / TJ_][t % TJ_] = rr;
     }
     __syncthreads();
     // restriction: coarse cells of this tile
-    for (int t = tid; t < (MT_I / 2) * (MT_J / 2); t += nt) {
-        const int ci = t / (MT_J / 2), cj = t % (MT_J / 2);
+    for (int t = tid; t < (TI_ / 2) * (TJ_ / 2); t += nt) {
+        const int ci = t / (TJ_ / 2), cj = t % (TJ_ / 2);
         const int I = i0 / 2 + ci, J = j0 / 2 + cj;
         if (I < C.nx && J < C.ny)
             C.f[LK(C, I, J)] = res[2 * ci][2 * cj] + res[2 * ci + 1][2 * cj] + res[2 * ci][2 * cj + 1] +
@@ -259,13 +265,15 @@ __global__ void __launch_bounds__(256) k_mg_pre(MgLevel L, MgLevel C, const doub
 // store would race with neighbours still reading their halo.  Level 0
 // instead writes z = (double) e (0 at the pinned cell) and reduces z.r and
 // z.q into the FCG beta.
-template <bool L0>
+template <bool L0, int TI_ = MT_I, int TJ_ = MT_J>
 __device__ __forceinline__ void mg_post_tile(const MgLevel &L, const MgLevel &C, float omega,
                                              const double *__restrict__ r64, const double *__restrict__ q64,
                                              double *__restrict__ z64, int pinned, int i0, int j0,
                                              double (&acc)[2]) {
-    __shared__ Tile T;
-    __shared__ float ec[MT_I / 2 + 2][MT_J / 2 + 2];
+    using TT = TileT<TI_, TJ_>;
+    constexpr int HI = TT::HI, HJ = TT::HJ;
+    __shared__ TT T;
+    __shared__ float ec[TI_ / 2 + 2][TJ_ / 2 + 2];
     // the tile's global reads are issued before the first barrier: its
     // coefficients and rhs, the pre-smoothed e, the coarse correction
     const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
@@ -276,8 +284,8 @@ __device__ __forceinline__ void mg_post_tile(const MgLevel &L, const MgLevel &C,
         const int i = i0 - 2 + a, j = j0 - 2 + b;
         T.e[a][b] = (i >= 0 && i < L.nx && j >= 0 && j < L.ny) ? L.e[LK(L, i, j)] : 0.0f;
     }
-    for (int t = tid; t < (MT_I / 2 + 2) * (MT_J / 2 + 2); t += nt) {
-        const int a = t / (MT_J / 2 + 2), b = t % (MT_J / 2 + 2);
+    for (int t = tid; t < (TI_ / 2 + 2) * (TJ_ / 2 + 2); t += nt) {
+        const int a = t / (TJ_ / 2 + 2), b = t % (TJ_ / 2 + 2);
         const int I = I0 + a, J = J0 + b;
         ec[a][b] = (I >= 0 && I < C.nx && J >= 0 && J < C.ny) ? C.ep[LK(C, I, J)] : 0.0f;
     }
@@ -295,9 +303,9 @@ __device__ __forceinline__ void mg_post_tile(const MgLevel &L, const MgLevel &C,
     }
     __syncthreads();
     acc[0] = acc[1] = 0.0;
-    for (int t = tid; t < MT_I * MT_J; t += nt) {
-        const int a = 2 + t / MT_J, b = 2 + t % MT_J;
-        const int i = i0 + t / MT_J, j = j0 + t % MT_J;
+    for (int t = tid; t < TI_ * TJ_; t += nt) {
+        const int a = 2 + t / TJ_, b = 2 + t % TJ_;
+        const int i = i0 + t / TJ_, j = j0 + t % TJ_;
         if (i < L.nx && j < L.ny) {
             float e = T.e[a][b];
             if (((i + j) & 1) == 0) e = gs_cell(T, a, b);
@@ -909,13 +917,13 @@ __global__ void __launch_bounds__(256) k_bfcg_replace(const BInst *__restrict__ 
     }
 }
 
-template <bool L0>
+template <bool L0, int TI_, int TJ_>
 __global__ void __launch_bounds__(256) k_bmg_pre(const BInst *__restrict__ insts, const BTile *__restrict__ tiles,
                                                  int l) {
     const BTile w = tiles[blockIdx.x];
     const BInst &I = insts[w.inst];
     if (I.ks->done) return;
-    mg_pre_tile<L0>(I.lv[l], I.lv[l + 1], L0 ? I.r : nullptr, w.by * MT_I, w.bx * MT_J);
+    mg_pre_tile<L0, TI_, TJ_>(I.lv[l], I.lv[l + 1], L0 ? I.r : nullptr, w.by * TI_, w.bx * TJ_);
 }
 
 __global__ void __launch_bounds__(MG_CTA_THREADS) k_bmg_cta(const BInst *__restrict__ insts, float omega) {
@@ -924,7 +932,7 @@ __global__ void __launch_bounds__(MG_CTA_THREADS) k_bmg_cta(const BInst *__restr
     mg_cta_body(I.lv, I.s_cta, I.nlev, I.coarse_inv, omega);
 }
 
-template <bool L0>
+template <bool L0, int TI_, int TJ_>
 __global__ void __launch_bounds__(256) k_bmg_post(const BInst *__restrict__ insts, const BTile *__restrict__ tiles,
                                                   int l, float omega) {
     const BTile w = tiles[blockIdx.x];
@@ -932,10 +940,10 @@ __global__ void __launch_bounds__(256) k_bmg_post(const BInst *__restrict__ inst
     KState *ks = I.ks;
     if (ks->done) return;
     double acc[2];
-    mg_post_tile<L0>(I.lv[l], I.lv[l + 1], omega, L0 ? I.r : nullptr, L0 ? I.q : nullptr, L0 ? I.z : nullptr,
-                     I.S.pinned, w.by * MT_I, w.bx * MT_J, acc);
+    mg_post_tile<L0, TI_, TJ_>(I.lv[l], I.lv[l + 1], omega, L0 ? I.r : nullptr, L0 ? I.q : nullptr,
+                               L0 ? I.z : nullptr, I.S.pinned, w.by * TI_, w.bx * TJ_, acc);
     if (L0) {
-        const int gx = (I.lv[0].ny + MT_J - 1) / MT_J;
+        const int gx = (I.lv[0].ny + TJ_ - 1) / TJ_;
         double tot[2];
         if (mg_reduce<2>(acc, I.partial, &ks->counter, w.bx + gx * w.by, I.tiles0, tot)) fcg_beta(ks, tot);
     }
@@ -1294,6 +1302,7 @@ bool launch_fcg_check(const Sys &S, int nx, int ny, MgLevel *lv, int nlev, const
 
 // ---------------------------------------------------------- batched host --
 int batch_tiles0(int nx, int ny) { return ((ny + MT_J - 1) / MT_J) * ((nx + MT_I - 1) / MT_I); }
+static_assert(MG_SHAPES[0][0] == MT_I && MG_SHAPES[0][1] == MT_J, "shape 0 is the single-system tile");
 
 int64_t batch_partial_len(int nx, int ny) {
     const int64_t chunks = ((int64_t)nx * ny + FCG_CHUNK - 1) / FCG_CHUNK;
@@ -1320,19 +1329,27 @@ void launch_batch_mg_setup(const BatchPlan &P, cudaStream_t st) {
     k_bmg_invert<<<P.count, MG_INV_THREADS, inv, st>>>(P.insts);
 }
 
-static void batch_vcycle(const BatchPlan &P, cudaStream_t st) {
+template <int TI_, int TJ_> static void batch_vcycle_t(const BatchPlan &P, cudaStream_t st) {
     const dim3 blk(32, 8);
     const float omega = 1.9f;
     for (int l = 0; l < P.max_s; l++) {
         if (P.nmg_tiles[l] == 0) continue;
-        if (l == 0) k_bmg_pre<true><<<P.nmg_tiles[0], blk, 0, st>>>(P.insts, P.mg_tiles[0], 0);
-        else k_bmg_pre<false><<<P.nmg_tiles[l], blk, 0, st>>>(P.insts, P.mg_tiles[l], l);
+        if (l == 0) k_bmg_pre<true, TI_, TJ_><<<P.nmg_tiles[0], blk, 0, st>>>(P.insts, P.mg_tiles[0], 0);
+        else k_bmg_pre<false, TI_, TJ_><<<P.nmg_tiles[l], blk, 0, st>>>(P.insts, P.mg_tiles[l], l);
     }
     k_bmg_cta<<<P.count, MG_CTA_THREADS, MG_CTA_SMEM_BOUND, st>>>(P.insts, omega);
     for (int l = P.max_s - 1; l >= 0; l--) {
         if (P.nmg_tiles[l] == 0) continue;
-        if (l == 0) k_bmg_post<true><<<P.nmg_tiles[0], blk, 0, st>>>(P.insts, P.mg_tiles[0], 0, omega);
-        else k_bmg_post<false><<<P.nmg_tiles[l], blk, 0, st>>>(P.insts, P.mg_tiles[l], l, omega);
+        if (l == 0) k_bmg_post<true, TI_, TJ_><<<P.nmg_tiles[0], blk, 0, st>>>(P.insts, P.mg_tiles[0], 0, omega);
+        else k_bmg_post<false, TI_, TJ_><<<P.nmg_tiles[l], blk, 0, st>>>(P.insts, P.mg_tiles[l], l, omega);
+    }
+}
+
+static void batch_vcycle(const BatchPlan &P, cudaStream_t st) {
+    switch (P.shape) {
+    case 1: batch_vcycle_t<MG_SHAPES[1][0], MG_SHAPES[1][1]>(P, st); break;
+    case 2: batch_vcycle_t<MG_SHAPES[2][0], MG_SHAPES[2][1]>(P, st); break;
+    default: batch_vcycle_t<MG_SHAPES[0][0], MG_SHAPES[0][1]>(P, st); break;
     }
 }
 

@@ -325,6 +325,7 @@ def batched_solves(sh, stream, flush, count=BATCH_COUNT):
         if res["status"] != 0:
             raise SystemExit(f"bench: batched solve did not converge: {res['status']}")
         times.append(t)
+    (trow, tcol), trial_ms = b.tile_shape()
     b.close()
     t_b = float(np.median(times))
     cells = int(sum(c.nx * c.ny for c in cases))
@@ -347,6 +348,8 @@ def batched_solves(sh, stream, flush, count=BATCH_COUNT):
                                    "solver": "FP64 Jacobi-PCG per system, one system after another"},
             "single_mg_sequential": {"value": count / t_mg, "unit": "GFM Poisson solves/s"},
             "speedup_vs_fp64_cg": t_cg / t_b,
+            "mg_tile": {"shape": [trow, tcol], "trial_ms": {"16x32": trial_ms[0], "32x32": trial_ms[1],
+                                                           "16x64": trial_ms[2]}},
             "roofline": {"bound": "hbm", "achieved": alg / t_b / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": alg / t_b / 1e9 / peak,
                          "bytes": "assembly 64 B + MG-FCG 180 B per unknown and iteration of each instance"},

@@ -285,6 +285,13 @@ int asd2g_batch_sync(asd2g_batch *b);
  * (LS, U, V, PS, P, KAPPA, H, HS, DIV, UHAT, VHAT, LSB, LS0). */
 int asd2g_batch_step(asd2g_batch *b, double *dt, int reinit_mode, double tol, int maxit, int *iters,
                      double *rel_resid);
+/* Multigrid tile shape the batch uses (rows x cols cells per tile).  The
+ * first asd2g_batch_solve / asd2g_batch_step times four FCG iterations with
+ * each candidate shape (16x32, 32x32, 16x64) on the batch's own hierarchy
+ * and keeps the fastest; trial_ms[3] (may be NULL) receives those times (0
+ * before tuning or when the environment variable ASD2G_MG_TILE=0|1|2 fixes
+ * the shape). */
+int asd2g_batch_tile_shape(asd2g_batch *b, int *rows, int *cols, float *trial_ms);
 /* Volume check of the last batch step per instance: sum H dx dy, sum HS dx dy. */
 int asd2g_batch_volume(asd2g_batch *b, double *sharp, double *smooth);
 

@@ -66,3 +66,36 @@ def test_batch_matches_sessions():
             np.testing.assert_allclose(interior(p), interior(ps) / dts[k], rtol=1e-15)
             s.upload("ps", ps)
             assert s.true_residual() <= 1e-9, k
+
+
+def test_tile_shapes_agree_and_tuning_picks_fastest(monkeypatch):
+    """Every multigrid tile shape solves the batch to the same pressure (the
+    smoothing of a cell does not depend on the tiling; only the order of the
+    dot-product sums does), and the tuned batch keeps the shape whose trial
+    was fastest."""
+    cases = [_inputs(k, nx, ny) for k, (nx, ny) in enumerate(SHAPES)]
+    dts = [1e-3 * (1 + k) for k in range(len(cases))]
+    ps = []
+    for shape in ("0", "1", "2", None):
+        if shape is None:
+            monkeypatch.delenv("ASD2G_MG_TILE", raising=False)
+        else:
+            monkeypatch.setenv("ASD2G_MG_TILE", shape)
+        with api.Batch([params_for(g, f) for g, f, _ in cases]) as b:
+            for i, (_, _, data) in enumerate(cases):
+                for f_, a in data.items():
+                    b.upload(i, f_, a)
+            b.assemble(dts)
+            r = b.solve(tol=1e-10, maxit=10000)
+            assert r["status"] == 0, r
+            (rows, cols), ms = b.tile_shape()
+            if shape is not None:
+                assert (rows, cols) == [(16, 32), (32, 32), (16, 64)][int(shape)]
+                assert ms == [0.0, 0.0, 0.0]
+            else:
+                assert all(m > 0 for m in ms)
+                assert (rows, cols) == [(16, 32), (32, 32), (16, 64)][int(np.argmin(ms))]
+            ps.append([interior(b.download(i, "ps")) for i in range(len(cases))])
+    for other in ps[1:]:
+        for a, ref in zip(other, ps[0]):
+            assert np.abs(a - ref).max() <= 1e-7 * max(np.abs(ref).max(), 1e-300)
