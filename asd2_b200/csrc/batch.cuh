@@ -59,12 +59,6 @@ constexpr int FCG_CHUNK = 1024;  // 256 threads x 4
 void launch_batch_assemble(const BInst *insts, const BTile *tiles, int ntiles, cudaStream_t st);
 void launch_batch_scatter(const BInst *insts, const BTile *tiles, int ntiles, cudaStream_t st);
 
-// Multigrid tile shapes (rows i x columns j) the batched solve can use; the
-// first is the single-system tile and has the most tiles (it sizes the
-// partial-sum slots).
-constexpr int MG_SHAPES[3][2] = {{16, 32}, {32, 32}, {16, 64}};
-constexpr int MG_NSHAPES = 3;
-
 // mg.cu: set-up of every instance's hierarchy, then the solver phases.
 // lvl_chunks[l] lists the chunks of level-l cells of the instances that have
 // a level l (element-wise set-up kernels); mg_tiles[l] the tiles (shape

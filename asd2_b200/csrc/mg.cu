@@ -250,12 +250,12 @@ __device__ __forceinline__ void mg_pre_tile(const MgLevel &L, const MgLevel &C, 
     }
 }
 
-template <bool L0>
+template <bool L0, int TI_ = MT_I, int TJ_ = MT_J>
 __global__ void __launch_bounds__(256) k_mg_pre(MgLevel L, MgLevel C, const double *__restrict__ r64,
                                                 const KState *ks) {
     pdl_enter();
     if (ks->done) return;
-    mg_pre_tile<L0>(L, C, r64, blockIdx.y * MT_I, blockIdx.x * MT_J);
+    mg_pre_tile<L0, TI_, TJ_>(L, C, r64, blockIdx.y * TI_, blockIdx.x * TJ_);
 }
 
 // ----------------------------------------------------------- post pass --
@@ -335,14 +335,14 @@ __device__ __forceinline__ void fcg_beta(KState *ks, const double (&tot)[2]) {
     }
 }
 
-template <bool L0>
+template <bool L0, int TI_ = MT_I, int TJ_ = MT_J>
 __global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float omega, const double *__restrict__ r64,
                                                  const double *__restrict__ q64, double *__restrict__ z64, int pinned,
                                                  KState *ks, double *partial) {
     pdl_enter();
     if (ks->done) return;
     double acc[2];
-    mg_post_tile<L0>(L, C, omega, r64, q64, z64, pinned, blockIdx.y * MT_I, blockIdx.x * MT_J, acc);
+    mg_post_tile<L0, TI_, TJ_>(L, C, omega, r64, q64, z64, pinned, blockIdx.y * TI_, blockIdx.x * TJ_, acc);
     if (L0) {
         double tot[2];
         // in the learned mode the V-cycle's z is only part of the preconditioner: beta comes later
@@ -1181,7 +1181,9 @@ void launch_mg_setup(const Sys &S, MgLevel *lv, int nlev, double *coarse_inv, cu
     k_mg_coarse_invert<<<1, MG_INV_THREADS, smem, st>>>(lv[nlev - 1], coarse_inv);
 }
 
-static dim3 tile_grid(const MgLevel &L) { return dim3((L.ny + MT_J - 1) / MT_J, (L.nx + MT_I - 1) / MT_I); }
+template <int TI_ = MT_I, int TJ_ = MT_J> static dim3 tile_grid(const MgLevel &L) {
+    return dim3((L.ny + TJ_ - 1) / TJ_, (L.nx + TI_ - 1) / TI_);
+}
 
 int64_t mg_partial_len(int nx, int ny) {
     const int64_t tiles = (int64_t)((ny + MT_J - 1) / MT_J) * ((nx + MT_I - 1) / MT_I);
@@ -1242,16 +1244,16 @@ static void pdl_launch(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cuda
     cudaLaunchKernelEx(&cfg, k, static_cast<P>(args)...);
 }
 
-// One V-cycle: input r (FP64 level-0 rhs), output z (FP64), with the FCG
-// beta update folded into the level-0 post pass.  Levels 0 .. s-1 run as
-// tile kernels over the whole GPU, levels s .. nlev-1 in one CTA.
-static void enqueue_vcycle(MgLevel *lv, int nlev, const double *coarse_inv, const double *r, const double *q,
-                           double *z, int pinned, KState *ks, double *partial, cudaStream_t st) {
+template <int TI_, int TJ_>
+static void enqueue_vcycle_t(MgLevel *lv, int nlev, const double *coarse_inv, const double *r, const double *q,
+                             double *z, int pinned, KState *ks, double *partial, cudaStream_t st) {
     const dim3 blk(32, 8);
     const int s = mg_cta_level(lv, nlev);
     for (int l = 0; l < s; l++) {
-        if (l == 0) pdl_launch(k_mg_pre<true>, tile_grid(lv[0]), blk, 0, st, lv[0], lv[1], r, ks);
-        else pdl_launch(k_mg_pre<false>, tile_grid(lv[l]), blk, 0, st, lv[l], lv[l + 1], (const double *)nullptr, ks);
+        if (l == 0) pdl_launch(k_mg_pre<true, TI_, TJ_>, tile_grid<TI_, TJ_>(lv[0]), blk, 0, st, lv[0], lv[1], r, ks);
+        else
+            pdl_launch(k_mg_pre<false, TI_, TJ_>, tile_grid<TI_, TJ_>(lv[l]), blk, 0, st, lv[l], lv[l + 1],
+                       (const double *)nullptr, ks);
     }
     MgHier H{};
     for (int l = 0; l < nlev; l++) H.l[l] = lv[l];
@@ -1260,10 +1262,28 @@ static void enqueue_vcycle(MgLevel *lv, int nlev, const double *coarse_inv, cons
                ks);
     for (int l = s - 1; l >= 0; l--) {
         if (l == 0)
-            pdl_launch(k_mg_post<true>, tile_grid(lv[0]), blk, 0, st, lv[0], lv[1], omega, r, q, z, pinned, ks, partial);
+            pdl_launch(k_mg_post<true, TI_, TJ_>, tile_grid<TI_, TJ_>(lv[0]), blk, 0, st, lv[0], lv[1], omega, r, q, z,
+                       pinned, ks, partial);
         else
-            pdl_launch(k_mg_post<false>, tile_grid(lv[l]), blk, 0, st, lv[l], lv[l + 1], omega, (const double *)nullptr,
-                       (const double *)nullptr, (double *)nullptr, 0, ks, partial);
+            pdl_launch(k_mg_post<false, TI_, TJ_>, tile_grid<TI_, TJ_>(lv[l]), blk, 0, st, lv[l], lv[l + 1], omega,
+                       (const double *)nullptr, (const double *)nullptr, (double *)nullptr, 0, ks, partial);
+    }
+}
+
+// One V-cycle: input r (FP64 level-0 rhs), output z (FP64), with the FCG
+// beta update folded into the level-0 post pass.  Levels 0 .. s-1 run as
+// tile kernels over the whole GPU (tiles of MG_SHAPES[lv[0].tile]), levels
+// s .. nlev-1 in one CTA.
+static void enqueue_vcycle(MgLevel *lv, int nlev, const double *coarse_inv, const double *r, const double *q,
+                           double *z, int pinned, KState *ks, double *partial, cudaStream_t st) {
+    switch (lv[0].tile) {
+    case 1:
+        enqueue_vcycle_t<MG_SHAPES[1][0], MG_SHAPES[1][1]>(lv, nlev, coarse_inv, r, q, z, pinned, ks, partial, st);
+        break;
+    case 2:
+        enqueue_vcycle_t<MG_SHAPES[2][0], MG_SHAPES[2][1]>(lv, nlev, coarse_inv, r, q, z, pinned, ks, partial, st);
+        break;
+    default: enqueue_vcycle_t<MT_I, MT_J>(lv, nlev, coarse_inv, r, q, z, pinned, ks, partial, st); break;
     }
 }
 

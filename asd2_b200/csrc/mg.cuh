@@ -7,8 +7,15 @@ namespace asd2g {
 // One level of the FP32 hierarchy, compact layout k = j + ny*i: operator
 // (diag, ce, cn), restricted residual f, pre-smoothed correction e and the
 // corrected, post-smoothed result ep (the coarsest level's exact solve).
+// Multigrid tile shapes (rows i x columns j) of the V-cycle's tile kernels,
+// chosen per session or batch by timing (the first has the most tiles and
+// sizes the partial-sum slots).
+constexpr int MG_SHAPES[3][2] = {{16, 32}, {32, 32}, {16, 64}};
+constexpr int MG_NSHAPES = 3;
+
 struct MgLevel {
     int nx, ny;
+    int tile;  // level 0 of a session's hierarchy: MG_SHAPES index of the V-cycle's tiles (host side)
     float *diag, *ce, *cn, *f, *e, *ep;
 };
 
