@@ -546,6 +546,62 @@ def batched_steps(sh, stream, count=BATCH_COUNT, steps=10):
             "speedup_vs_sessions_second_step": t_seq / times[1]}
 
 
+def full_steps_256(sh, stream, n=N_GRID, steps=20):
+    """cfg 2 as whole steps: the 256^2 droplet (density ratio 1000, viscosity
+    ratio 100) advanced `steps` full droplet steps from the state after the
+    warm-up steps, pressure to rel. residual 1e-10 (the configuration's
+    tolerance): FP64 with the FP64 Jacobi-PCG (the reference's method), FP64
+    with the MG-FCG, the same device-resident (asd2g_run_steps), and mixed
+    precision device-resident."""
+    import torch
+    from asd2_b200 import api
+    from asd2_b200 import workloads as W
+    c = W.droplet(n, seed=0)
+    out = {}
+    for name, prec, solver, device in (("fp64_jacobi_pcg", api.PRECISION_FP64, api.PCG, False),
+                                       ("fp64_mg_fcg", api.PRECISION_FP64, api.MGPCG, False),
+                                       ("fp64_mg_fcg_device_resident", api.PRECISION_FP64, api.MGPCG, True),
+                                       ("mixed_device_resident", api.PRECISION_MIXED, api.MGPCG, True)):
+        with api.Session(api.Params.from_case(c, precision=prec), stream=sh) as ss:
+            ss.upload("ls", c.ls)
+            ss.upload("u", c.u)
+            ss.upload("v", c.v)
+            ss.apply_bc("ls", "P")
+            dt = ss.update_dt()
+            for _ in range(3):  # warm-up steps (set-up, graph capture)
+                r = ss.droplet_step(dt, solver=solver, tol=1e-10, maxit=500000)
+                dt = r["dt_next"]
+            if device:
+                ss.run_steps(0, dt, tol=1e-10, maxit=500000)
+            ss.sync()
+            with torch.cuda.stream(stream):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            its = 0
+            if device:
+                r = ss.run_steps(steps, dt, tol=1e-10, maxit=500000)
+                its = r["iters"]
+                ok = r["status"] == 0
+            else:
+                ok = True
+                for _ in range(steps):
+                    r = ss.droplet_step(dt, solver=solver, tol=1e-10, maxit=500000)
+                    ok = ok and r["status"] == 0
+                    its += r["iters"]
+                    dt = r["dt_next"]
+            e1.record(stream)
+            e1.synchronize()
+            if not ok:
+                raise SystemExit(f"bench: full step {name} failed")
+            t = e0.elapsed_time(e1) / 1e3
+            out[name] = {"steps_per_s": steps / t, "ms_per_step": 1e3 * t / steps,
+                         "pressure_iters_per_step": its / steps, "mcells_per_s": n * n * steps / t / 1e6}
+    return {"workload": f"{n}x{n} droplet (rho ratio 1000, mu ratio 100), {steps} full steps after 3, "
+                        "pressure to rel. residual 1e-10", **out,
+            "speedup_mg_device_vs_jacobi": out["fp64_jacobi_pcg"]["ms_per_step"] /
+                                           out["fp64_mg_fcg_device_resident"]["ms_per_step"]}
+
+
 def run_ours(args):
     import torch
     from asd2_b200 import api
@@ -680,6 +736,7 @@ def run_ours(args):
     mixed = mixed_precision_errors(sh) if not args.no_extra else None
     learned = learned_pc_512(sh, stream, flush, args.weights) if not args.no_extra else None
     bsteps = batched_steps(sh, stream) if not args.no_extra else None
+    fsteps = full_steps_256(sh, stream) if not args.no_extra else None
     nlev = len(_mg_levels(args.n, args.n))
     per_iter = 2 + 2 * (nlev - 1) + 1
     launches = int(sum(4 + (1 + nlev) + (1 + per_iter - 2) + 8 * per_iter * math.ceil(i / 8) + 3 for i in iters))
@@ -724,6 +781,7 @@ def run_ours(args):
         "mixed_precision_1024": mixed,
         "learned_pc_512": learned,
         "batched_steps_256": bsteps,
+        "full_steps_256": fsteps,
         "e2e": {"value": e2e_value, "unit": "GFM Poisson solves/s",
                 "h2d_bytes_per_step": 3 * G * 8, "d2h_bytes_per_step": G * 8},
         "gpu_launches": launches,
@@ -839,7 +897,8 @@ def main():
     ap.add_argument("--batch-count", type=int, default=BATCH_COUNT,
                     help="droplets of the batched sections (default 256; smaller for profiling)")
     ap.add_argument("--section", default=None,
-                    choices=["ls_large", "mixed_1024", "batched", "batched_steps", "learned_pc", "unet_forward"],
+                    choices=["ls_large", "mixed_1024", "batched", "batched_steps", "learned_pc", "unet_forward",
+                             "full_steps"],
                     help="run only this report (its JSON object on stdout), e.g. to profile it")
     args = ap.parse_args()
     if args.section:
@@ -866,6 +925,8 @@ def run_section(name, args):
     elif name == "batched":
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
         out = batched_solves(stream.cuda_stream, stream, flush, count=args.batch_count)
+    elif name == "full_steps":
+        out = full_steps_256(stream.cuda_stream, stream)
     elif name == "batched_steps":
         out = batched_steps(stream.cuda_stream, stream, count=args.batch_count)
     elif name == "unet_forward":
