@@ -886,8 +886,13 @@ static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters
 // ---- flexible CG with the two-level learned preconditioner (ASD2G_SOLVER_UNET) ----
 // After each V-cycle (which leaves beta alone in this mode): r1 = r - A z_mg,
 // the network on r1's features, omega, z = z_mg + omega u and beta.
-static int pc_correct(asd2g_session *s) {
+// with_net false: the V-cycle alone (z = z_mg), the direction update as usual.
+static int pc_correct(asd2g_session *s, bool with_net = true) {
     const Grid &g = s->g;
+    if (!with_net) {
+        launch_pc_output(s->sys, g.nx, g.ny, nullptr, s->rt, s->z, s->fm, s->ks, s->mg_partial, s->st);
+        return cuda_check("learned preconditioner");
+    }
     launch_pc_input(s->sys, g.nx, g.ny, s->r, s->z, s->rt, s->ks, s->pc_scal, s->pc_feats, s->mg_partial, s->st);
     const int rc = asd2g_unet_forward(s->pc_net, 1, g.nx, g.ny, s->pc_feats, s->pc_out);
     if (rc) return rc;
@@ -899,13 +904,30 @@ constexpr int PC_CHUNK = 8;          // iterations per captured chunk; the FP64 
 constexpr int PC_MAX_ITERS = 500;    // iterations of the learned phase before the Jacobi-PCG fallback
 static_assert(PC_CHUNK % FM_SLOTS == 0, "every replay of a chunk must write the direction slots in the same order");
 
+// The network's correction on every PC_NET_EVERY-th iteration of a chunk
+// (ASD2G_PC_EVERY=1..8 in the environment), besides the first application
+// and the one after each residual replacement; the other iterations use the
+// V-cycle alone.  Measured on the 512^2 evaluation (solves/s, iterations):
+// every iteration 142 (13-15), every 2nd 199, every 3rd or 4th 260, every
+// 8th 306 (11-17): the correction is needed for a few modes the V-cycle
+// leaves, not at every step.
+constexpr int PC_NET_EVERY = 8;
+static bool pc_net_on(int k) {
+    static const int every = [] {
+        const char *e = std::getenv("ASD2G_PC_EVERY");
+        const int v = e ? std::atoi(e) : PC_NET_EVERY;
+        return v >= 1 && v <= 8 ? v : PC_NET_EVERY;
+    }();
+    return k % every == every - 1;
+}
+
 static int pc_chunk(asd2g_session *s) {
     const Grid &g = s->g;
     for (int k = 0; k < PC_CHUNK; k++) {
         if (!launch_pcm_iter(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->z, s->fm, k % FM_SLOTS,
                              s->ks, s->mg_partial, s->mg_partial_n, s->st))
             return fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
-        const int rc = pc_correct(s);
+        const int rc = pc_correct(s, pc_net_on(k));
         if (rc) return rc;
     }
     if (!launch_pcm_check(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->z, s->fm, s->ks,

@@ -1053,10 +1053,10 @@ __global__ void __launch_bounds__(256) k_pc_omega(int nx, int ny, Sys S, const f
 __global__ void __launch_bounds__(256) k_pc_final(int64_t n, const float *__restrict__ u, double *__restrict__ z,
                                                   FmDirs D, int pinned, KState *ks, double *partial) {
     if (ks->done) return;
-    const double om = ks->omega;
+    const double om = u ? ks->omega : 0.0;  // u == nullptr: the V-cycle alone this iteration
     double acc[FM_SLOTS] = {};
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        const double zk = (pinned && k == 0) ? 0.0 : z[k] + om * (double)u[k];
+        const double zk = (pinned && k == 0) ? 0.0 : z[k] + (u ? om * (double)u[k] : 0.0);
         z[k] = zk;
 #pragma unroll
         for (int j = 0; j < FM_SLOTS; j++) acc[j] += zk * D.q[j][k];
@@ -1412,7 +1412,7 @@ void launch_pc_output(const Sys &S, int nx, int ny, const float *u, const double
                       KState *ks, double *partial, cudaStream_t st) {
     const int64_t n = (int64_t)nx * ny;
     const int nb = red_blocks(n);
-    k_pc_omega<<<nb, 256, 0, st>>>(nx, ny, S, u, r1, ks, partial);
+    if (u) k_pc_omega<<<nb, 256, 0, st>>>(nx, ny, S, u, r1, ks, partial);
     k_pc_final<<<nb, 256, 0, st>>>(n, u, z, D, S.pinned, ks, partial);
 }
 

@@ -353,7 +353,9 @@ int asd2g_unet_set_stream(asd2g_unet *u, void *stream);
  * two-level preconditioner: z_mg = one FP32 V-cycle of r (the multigrid of
  * ASD2G_SOLVER_MGPCG), r1 = r - A z_mg, u = network(features of r1) (BF16 /
  * FP32 inside), z = z_mg + omega u with omega = (u . r1) / (u . Au) in
- * FP64.  Convergence is verified on the FP64 residual as for
+ * FP64; the network runs on the first application, after each residual
+ * replacement and on every 8th iteration, the V-cycle alone otherwise (each
+ * new direction is A-orthogonalised against the three before it).  Convergence is verified on the FP64 residual as for
  * ASD2G_SOLVER_MGPCG; if it does not converge within min(maxit, 500)
  * iterations the system is solved again by Jacobi-PCG and
  * asd2g_last_fallback reports 1. */
