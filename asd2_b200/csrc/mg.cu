@@ -1220,6 +1220,17 @@ bool mg_cta_prepare(const MgLevel *lv, int nlev) {
                                 (int)MG_CTA_SMEM_BOUND) == cudaSuccess;
 }
 
+// Over-correction of the coarse-grid correction (e += omega P e_c): 1.9
+// unless ASD2G_MG_OMEGA in the environment gives another value in (0, 2.5].
+static float mg_omega() {
+    static const float w = [] {
+        const char *e = std::getenv("ASD2G_MG_OMEGA");
+        const float v = e ? (float)std::atof(e) : 1.9f;
+        return v > 0.0f && v <= 2.5f ? v : 1.9f;
+    }();
+    return w;
+}
+
 // Launch with programmatic stream serialisation (see pdl_enter); ASD2G_PDL=0
 // in the environment launches plainly (for comparisons).
 static bool pdl_enabled() {
@@ -1257,7 +1268,7 @@ static void enqueue_vcycle_t(MgLevel *lv, int nlev, const double *coarse_inv, co
     }
     MgHier H{};
     for (int l = 0; l < nlev; l++) H.l[l] = lv[l];
-    const float omega = 1.9f;
+    const float omega = mg_omega();
     pdl_launch(k_mg_cta_cycle, dim3(1), dim3(MG_CTA_THREADS), mg_cta_smem(H, s, nlev), st, H, s, nlev, coarse_inv, omega,
                ks);
     for (int l = s - 1; l >= 0; l--) {
@@ -1351,7 +1362,7 @@ void launch_batch_mg_setup(const BatchPlan &P, cudaStream_t st) {
 
 template <int TI_, int TJ_> static void batch_vcycle_t(const BatchPlan &P, cudaStream_t st) {
     const dim3 blk(32, 8);
-    const float omega = 1.9f;
+    const float omega = mg_omega();
     for (int l = 0; l < P.max_s; l++) {
         if (P.nmg_tiles[l] == 0) continue;
         if (l == 0) k_bmg_pre<true, TI_, TJ_><<<P.nmg_tiles[0], blk, 0, st>>>(P.insts, P.mg_tiles[0], 0);
