@@ -588,6 +588,7 @@ int asd2g_smoothed_sign(asd2g_session *s, int ls, int out) {
 }
 
 int asd2g_ls_step(asd2g_session *s, double dt, int reinit_mode) {
+    NvtxRange nv("asd2g_ls_step");
     if (!s) return fail(ASD2G_E_ARG, "null session");
     if (s->prm.precision == ASD2G_PRECISION_MIXED) {
         if (!ls32_supported(s->g, reinit_mode))
@@ -755,6 +756,7 @@ static int p_supported(asd2g_session *s) {
 }
 
 static int assemble(asd2g_session *s, int recompute_kappa) {
+    NvtxRange nv("GFM assembly");
     int rc = p_supported(s);
     if (rc) return rc;
     const Grid &g = s->g;
@@ -815,6 +817,7 @@ static int capture_chunk(asd2g_session *s, int solver) {
 }
 
 static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters, double *resid) {
+    NvtxRange nv("pressure solve");
     const Grid &g = s->g;
     const int mode = solver;  // 0 PCG, 1 PCG (reference), 2 BiCGStab, 3 BiCGStab (reference), 4 MG-FCG
     const double reg = solver == 1 ? 1.0e-12 : 0.0;  // err_tol^2 in alpha (poisson2d.cpp:354)
@@ -949,6 +952,7 @@ static int fm_alloc(asd2g_session *s) {
 }
 
 static int solve_learned(asd2g_session *s, double tol, int maxit, int *iters, double *resid) {
+    NvtxRange nv("pressure solve (learned preconditioner)");
     const Grid &g = s->g;
     if (!s->pc_net) return fail(ASD2G_E_ARG, "no preconditioner network attached (asd2g_set_preconditioner_net)");
     int rc = mg_alloc(s);
@@ -1182,6 +1186,7 @@ int asd2g_csr_solve(asd2g_session *s, int solver, int rows, const int *ia, const
 // Solve_LevelSet_2D, the reinitialisation, kappa, H and HS, the FP64 volume
 // check, the intermediate velocity, its divergence and the GFM assembly.
 static int enqueue_step_pre(asd2g_session *s, int reinit_mode) {
+    NvtxRange nv("level set + momentum + assembly");
     const Grid &g = s->g;
     cudaMemcpyAsync(s->f[ASD2G_LSB], s->f[ASD2G_LS], sizeof(double) * s->G, cudaMemcpyDeviceToDevice, s->st);
     double *ls = s->f[ASD2G_LS];
@@ -1215,6 +1220,7 @@ static int enqueue_step_pre(asd2g_session *s, int reinit_mode) {
 
 // After the solve: ps and p, the projection (UpdateVel) and the next dt (UpdateDt, into dsc[1]).
 static void enqueue_step_post(asd2g_session *s) {
+    NvtxRange nv("projection + dt");
     const Grid &g = s->g;
     launch_scatter_ps(g, s->x, s->f[ASD2G_PS], s->f[ASD2G_P], s->dsc, s->st);
     launch_update_vel(g, s->M, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->f[ASD2G_PS], s->f[ASD2G_LS], s->f[ASD2G_H],
@@ -1224,6 +1230,7 @@ static void enqueue_step_post(asd2g_session *s) {
 
 int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver, double tol, int maxit, int *iters,
                        double *rel_resid) {
+    NvtxRange nv("asd2g_droplet_step");
     if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
     int rc = p_supported(s);
     if (rc) return rc;
@@ -1480,6 +1487,7 @@ static int capture_run_graph(asd2g_session *s, int reinit_mode, double tol, int 
 
 int asd2g_run_steps(asd2g_session *s, int nsteps, double *dt, int reinit_mode, int solver, double tol, int maxit,
                     int *steps_done, long long *iters_total, double *max_resid) {
+    NvtxRange nv("asd2g_run_steps");
     if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
     if (nsteps < 0) return fail(ASD2G_E_ARG, "nsteps must be >= 0");
     if (solver != ASD2G_SOLVER_MGPCG)

@@ -398,6 +398,7 @@ int solve_impl(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_re
 extern "C" {
 
 int asd2g_batch_assemble(asd2g_batch *b, const double *dt) {
+    NvtxRange nv("batched GFM assembly");
     if (!b || !dt) return api_fail(ASD2G_E_ARG, "batch_assemble: null argument");
     int rc = set_dts(b, dt);
     if (rc) return rc;
@@ -414,6 +415,7 @@ int asd2g_batch_solve(asd2g_batch *b, double tol, int maxit, int *iters, double 
 // MG-FCG pressure solve), one launch per phase for the whole batch.
 int asd2g_batch_step(asd2g_batch *b, double *dt, int reinit_mode, double tol, int maxit, int *iters,
                      double *rel_resid) {
+    NvtxRange nv("asd2g_batch_step");
     if (!b || !dt || !(tol > 0.0) || maxit < 1) return api_fail(ASD2G_E_ARG, "batch_step: bad arguments");
     if (reinit_mode != ASD2G_REINIT_ORIGINAL && reinit_mode != ASD2G_REINIT_MINRK2)
         return api_fail(ASD2G_E_UNSUPPORTED, "batch_step implements reinit modes 0 (original) and 2 (MinRK2)");
@@ -511,6 +513,7 @@ int asd2g_batch_volume(asd2g_batch *b, double *sharp, double *smooth) {
 
 namespace {
 int solve_impl(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_resid) {
+    NvtxRange nv("batched pressure solve");
     const BatchPlan &P = b->plan;
     launch_batch_set_kstate(P, tol, maxit, b->st);
     launch_batch_mg_setup(P, b->st);

@@ -2,10 +2,21 @@
 #pragma once
 #include <cstdio>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "common.cuh"
 
 namespace asd2g {
+
+// NVTX range for the host-side phases of the ABI calls (level set, momentum,
+// assembly, solve, projection, batch phases): visible in an NVTX-aware
+// profiler's timeline, free when none is attached.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // Division by a grid spacing.  When h is a power of two, x / h and
 // x * (1/h) are the same IEEE result, so the multiply is used; otherwise the

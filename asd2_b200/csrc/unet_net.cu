@@ -687,6 +687,7 @@ static int check_shape(asd2g_unet *u, int B, int H, int W) {
 
 // feats: device FP32 [B][H][W][4]; out: device FP32 [B][H][W].
 int asd2g_unet_forward(asd2g_unet *u, int B, int H, int W, const float *feats, float *out) {
+    NvtxRange nv("U-Net forward");
     int rc = check_shape(u, B, H, W);
     if (rc) return rc;
     if (!feats || !out) return api_fail(ASD2G_E_ARG, "null argument");
@@ -722,6 +723,7 @@ static int train_finish(asd2g_unet *u, int B, int H, int W, float *loss_mean) {
 // One Adam step on a batch: loss = mean over samples of |out - target|^2 / |target|^2.
 int asd2g_unet_train_step(asd2g_unet *u, int B, int H, int W, const float *feats, const float *target, float lr,
                           float *loss_mean) {
+    NvtxRange nv("U-Net train step (MSE)");
     int rc = check_shape(u, B, H, W);
     if (rc) return rc;
     if (!feats || !target) return api_fail(ASD2G_E_ARG, "null argument");
@@ -738,6 +740,7 @@ int asd2g_unet_train_step(asd2g_unet *u, int B, int H, int W, const float *feats
 // error 1 - (out' A t)^2 / ((out' A out)(t' A t)).
 int asd2g_unet_train_step_energy(asd2g_unet *u, int B, int H, int W, const float *feats, const float *target,
                                  float lr, float *loss_mean) {
+    NvtxRange nv("U-Net train step (energy)");
     int rc = check_shape(u, B, H, W);
     if (rc) return rc;
     if (!feats || !target) return api_fail(ASD2G_E_ARG, "null argument");
@@ -753,6 +756,7 @@ int asd2g_unet_train_step_energy(asd2g_unet *u, int B, int H, int W, const float
 // One Adam step on the residual loss: mean over samples of 1 - cos^2(A out, r).
 int asd2g_unet_train_step_residual(asd2g_unet *u, int B, int H, int W, const float *feats, float lr,
                                    float *loss_mean) {
+    NvtxRange nv("U-Net train step (residual)");
     int rc = check_shape(u, B, H, W);
     if (rc) return rc;
     if (!feats) return api_fail(ASD2G_E_ARG, "null argument");
