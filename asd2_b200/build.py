@@ -33,6 +33,8 @@ UNITS = {
     "pcg_cluster.cu": ["-fmad=false"],
     "mg.cu": [],
     "levelset32.cu": [],
+    "weno32.cu": [],
+    "reinit32.cu": [],
     "batch.cu": [],
     "unet.cu": [],
     "unet_net.cu": [],

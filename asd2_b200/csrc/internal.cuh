@@ -27,6 +27,15 @@ struct DivHT {
     int pow2;
     __device__ __forceinline__ T operator()(T x) const { return pow2 ? x * inv : x / h; }
 };
+// FP32 (the mixed-precision path, not bit-exact by design): always the
+// multiply by the rounded reciprocal, within 1.5 ulp of x / h and without
+// the per-call branch.
+template <>
+struct DivHT<float> {
+    float h, inv;
+    int pow2;
+    __device__ __forceinline__ float operator()(float x) const { return x * inv; }
+};
 using DivH = DivHT<double>;
 DivH make_divh(double h);
 DivHT<float> make_divh_f(double h);

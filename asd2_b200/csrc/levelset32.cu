@@ -9,6 +9,9 @@
 // as the FP64 path); only the arithmetic type changes.  It needs the
 // pressure-grid ghost fill to be producer-side (all P sides Neumann or
 // Dirichlet): every FP32 kernel then writes its own ghost mirrors.
+#include <cstdlib>
+#include <cstring>
+
 #include "levelset_impl.cuh"
 #include "ls32.cuh"
 
@@ -88,6 +91,20 @@ __global__ void __launch_bounds__(256) k_volume(Grid g, const double *__restrict
     *counter = 0u;
 }
 
+// The FP32 passes in their packed forms (weno32.cu, reinit32.cu: shared
+// smoothness triples and minmods, FP32x2 arithmetic, the Sussman constraint
+// on the interface band only) or in the per-cell tile forms (the FP64
+// kernels' templates instantiated for float).  Both compute the same scheme;
+// ASD2G_LS32_FORM = packed / cell selects.
+bool packed_forms() {
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("ASD2G_LS32_FORM");
+        v = (e && std::strcmp(e, "packed") == 0) ? 1 : 0;
+    }
+    return v == 1;
+}
+
 int64_t padded(const Grid &g) { return (int64_t)g.sx * g.sy; }
 int conv_blocks(int64_t n) { return (int)((n + 255) / 256 < 4 * 148 ? (n + 255) / 256 : 4 * 148); }
 
@@ -105,16 +122,28 @@ void launch_ls_step32(const Grid &g, int reinit_mode, double max_atime, const do
     const dim3 grd = cell_grid(g), blk(TJ, TI);
     k_to_f32<<<conv_blocks(n), 256, 0, st>>>(n, ls64, w.phi);
     k_center_vel<float><<<grd, blk, 0, st>>>(g, u, v, w.tu, w.tv);
-    const DivHT<float> ddx = make_divh_f(g.dx), ddy = make_divh_f(g.dy);
-    k_ls_stage<1, float><<<grd, blk, 0, st>>>(g, ddx, ddy, w.phi, w.tu, w.tv, w.phi, w.a, dtp);
-    k_ls_stage<2, float><<<grd, blk, 0, st>>>(g, ddx, ddy, w.a, w.tu, w.tv, w.phi, w.b, dtp);
-    k_ls_stage<3, float><<<grd, blk, 0, st>>>(g, ddx, ddy, w.b, w.tu, w.tv, w.phi, w.phi, dtp);
+    const bool packed = packed_forms();
+    if (!packed) {
+        const DivHT<float> ddx = make_divh_f(g.dx), ddy = make_divh_f(g.dy);
+        k_ls_stage<1, float><<<grd, blk, 0, st>>>(g, ddx, ddy, w.phi, w.tu, w.tv, w.phi, w.a, dtp);
+        k_ls_stage<2, float><<<grd, blk, 0, st>>>(g, ddx, ddy, w.a, w.tu, w.tv, w.phi, w.b, dtp);
+        k_ls_stage<3, float><<<grd, blk, 0, st>>>(g, ddx, ddy, w.b, w.tu, w.tv, w.phi, w.phi, dtp);
+    } else {
+        launch_ls_stage32(g, 1, w.phi, w.tu, w.tv, w.phi, w.a, dtp, st);
+        launch_ls_stage32(g, 2, w.a, w.tu, w.tv, w.phi, w.b, dtp, st);
+        launch_ls_stage32(g, 3, w.b, w.tu, w.tv, w.phi, w.phi, dtp, st);
+    }
     // reinitialisation: lsInit = phi, then the pseudo-steps (levelset2d.cpp:264-316, :433-486)
     const LsConstT<float> K = make_lsconst_t<float>(g);
     const double eps = g.dx < g.dy ? g.dx : g.dy;
     const double mt = max_atime > 0.0 ? max_atime : 1.5 * (1.5 * eps);  // kMaxATime, levelset2d.cpp:10
     const int steps = reinit_steps(eps * 0.5, mt);
     cudaMemcpyAsync(w.ls0, w.phi, sizeof(float) * (size_t)n, cudaMemcpyDeviceToDevice, st);
+    if (packed) {
+        launch_reinit32(g, K, reinit_mode, steps, w, st);
+        k_to_f64<<<conv_blocks(n), 256, 0, st>>>(n, w.phi, ls64);
+        return;
+    }
     for (int s = 0; s < steps; s++) {
         if (reinit_mode == 0) {
             k_reinit_a<0, float><<<grd, blk, 0, st>>>(g, K, w.phi, w.ls0, w.a, 1);
@@ -135,7 +164,8 @@ int ls32_launches(int reinit_mode, double max_atime, const Grid &g) {
     const double eps = g.dx < g.dy ? g.dx : g.dy;
     const double mt = max_atime > 0.0 ? max_atime : 1.5 * (1.5 * eps);
     const int steps = reinit_steps(eps * 0.5, mt);
-    return 5 + steps * (reinit_mode == 4 ? 3 : 2) + 1;  // memcpy not counted
+    if (packed_forms()) return 5 + reinit32_launches(reinit_mode, steps) + 1;  // memcpy not counted
+    return 5 + steps * (reinit_mode == 4 ? 3 : 2) + 1;
 }
 
 void launch_volume(const Grid &g, const double *H, const double *HS, double *partial, unsigned *counter, double *out2,

@@ -7,6 +7,10 @@ namespace asd2g {
 // FP32 work arrays of the mixed level-set step, each (nx+6) x (ny+6).
 struct Ls32Work {
     float *phi, *ls0, *a, *b, *tu, *tv;
+    // band cells of the Sussman constraint: linear indices, new values, count
+    int *band;
+    float *band_val;
+    unsigned *band_n;
 };
 constexpr int LS32_ARRAYS = 6;
 constexpr int VOLUME_BLOCKS = 592;  // partial sums: 2 per block
@@ -18,6 +22,18 @@ bool ls32_supported(const Grid &g, int reinit_mode);
 // reinitialisation pseudo-steps, -> ls64 (interior and ghosts).
 void launch_ls_step32(const Grid &g, int reinit_mode, double max_atime, const double *u, const double *v,
                       const double *dtp, double *ls64, const Ls32Work &w, cudaStream_t st);
+// One TVD-RK3 stage (1, 2 or 3) in FP32 (weno32.cu): out = stage(phi_n,
+// phi_in, dt * HJWENO5(phi_in; tu, tv)), interior and ghost mirrors.
+void launch_ls_stage32(const Grid &g, int stage, const float *phi_in, const float *tu, const float *tv,
+                       const float *phi_n, float *out, const double *dtp, cudaStream_t st);
+// steps reinitialisation pseudo-steps (modes 0, 2, 4) of w.phi against
+// lsInit = w.ls0 in FP32 (reinit32.cu); w.a and the band arrays are scratch.
+template <typename T> struct LsConstT;
+void launch_reinit32(const Grid &g, const LsConstT<float> &K, int reinit_mode, int steps, const Ls32Work &w,
+                     cudaStream_t st);
+int reinit32_launches(int reinit_mode, int steps);
+// Rows per warp of the FP32 strip kernels (64 columns x R rows per warp).
+int ls32_rows_per_warp(const Grid &g);
 // Kernel launches of one launch_ls_step32 call.
 int ls32_launches(int reinit_mode, double max_atime, const Grid &g);
 // out2[0] = sum over interior cells of H dx dy, out2[1] = of HS dx dy (FP64).

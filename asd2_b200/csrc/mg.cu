@@ -46,7 +46,6 @@ __device__ __forceinline__ void pdl_enter() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 constexpr int MG_COARSE_MAX = 64;   // cells on the coarsest level
-constexpr int HI = MT_I + 4, HJ = MT_J + 4;
 
 // block sum and grid reduction (same fixed-order scheme as pressure.cu)
 template <int NV>

@@ -72,6 +72,42 @@ def test_mixed_level_set_revolution():
     assert abs(v32[1] - v64[1]) <= 1e-4 * v64[1]
 
 
+@pytest.mark.parametrize("nx,ny,mode", [(150, 97, api.REINIT_MINRK2), (37, 211, api.REINIT_MINRK2_SUSSMAN),
+                                         (300, 64, api.REINIT_ORIGINAL), (150, 97, api.REINIT_MINRK2_SUSSMAN)])
+def test_mixed_level_set_ragged_grids(nx, ny, mode):
+    """The FP32 advection and reinitialisation kernels work on 64-column
+    strips and row pairs: grids whose sizes are not multiples of either (and
+    narrow ones) must track the FP64 step as closely as the square case
+    does, in every reinitialisation mode the FP32 path implements."""
+    h = 1.0 / max(nx, ny)
+    X = (np.arange(nx + 6) - 3 + 0.5)[:, None] * h
+    Y = (np.arange(ny + 6) - 3 + 0.5)[None, :] * h
+    xc, yc = 0.5 * nx * h, 0.45 * ny * h
+    r0 = 0.3 * min(nx, ny) * h
+    th = np.arctan2(Y - yc, X - xc)
+    ls = np.ascontiguousarray(r0 * (1.0 + 0.05 * np.cos(3 * th)) - np.sqrt((X - xc) ** 2 + (Y - yc) ** 2))
+    # rotation about the centre: u on west faces (a function of y only), v on south faces
+    u = np.ascontiguousarray(-2.0 * np.pi * (Y + 0.0 * X - yc))
+    v = np.ascontiguousarray(2.0 * np.pi * (X + 0.0 * Y - xc))
+    dt = 0.25 * h / (2.0 * np.pi * max(nx, ny) * h)
+    outs = {}
+    for prec in (api.PRECISION_FP64, api.PRECISION_MIXED):
+        p = api.Params(nx, ny, h, h, bc_u=("neumann",) * 4, bc_v=("neumann",) * 4, bc_p=("neumann",) * 4,
+                       precision=prec)
+        with api.Session(p) as s:
+            s.upload("ls", ls)
+            s.upload("u", u)
+            s.upload("v", v)
+            s.apply_bc("ls", "P")
+            for _ in range(30):
+                s.ls_step(dt, mode)
+            outs[prec] = (s.download("ls"), s.volume())
+    (l64, v64), (l32, v32) = outs[api.PRECISION_FP64], outs[api.PRECISION_MIXED]
+    assert np.isfinite(l32).all()
+    assert np.abs(interior(l32) - interior(l64)).max() <= 1e-4 * np.abs(interior(l64)).max()
+    assert abs(v32[1] - v64[1]) <= 1e-4 * v64[1]
+
+
 def test_mixed_droplet_steps():
     c = W.droplet(128, seed=7)
     ref = _run_steps(c, api.PRECISION_FP64, 10, api.PCG)
