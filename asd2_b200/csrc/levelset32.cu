@@ -94,16 +94,22 @@ __global__ void __launch_bounds__(256) k_volume(Grid g, const double *__restrict
 // The FP32 passes in their packed forms (weno32.cu, reinit32.cu: shared
 // smoothness triples and minmods, FP32x2 arithmetic, the Sussman constraint
 // on the interface band only) or in the per-cell tile forms (the FP64
-// kernels' templates instantiated for float).  Both compute the same scheme;
-// ASD2G_LS32_FORM = packed / cell selects.
-bool packed_forms() {
+// kernels' templates instantiated for float).  Both compute the same scheme.
+// ASD2G_LS32_FORM: packed (both passes packed), cell (neither), stage (the
+// advection stage packed), reinit (the reinitialisation packed).
+int form_bits() {
     static int v = -1;
     if (v < 0) {
         const char *e = getenv("ASD2G_LS32_FORM");
-        v = (e && std::strcmp(e, "packed") == 0) ? 1 : 0;
+        v = 0;
+        if (e && std::strcmp(e, "packed") == 0) v = 3;
+        if (e && std::strcmp(e, "stage") == 0) v = 1;
+        if (e && std::strcmp(e, "reinit") == 0) v = 2;
     }
-    return v == 1;
+    return v;
 }
+bool packed_stage() { return form_bits() & 1; }
+bool packed_reinit() { return form_bits() & 2; }
 
 int64_t padded(const Grid &g) { return (int64_t)g.sx * g.sy; }
 int conv_blocks(int64_t n) { return (int)((n + 255) / 256 < 4 * 148 ? (n + 255) / 256 : 4 * 148); }
@@ -122,8 +128,7 @@ void launch_ls_step32(const Grid &g, int reinit_mode, double max_atime, const do
     const dim3 grd = cell_grid(g), blk(TJ, TI);
     k_to_f32<<<conv_blocks(n), 256, 0, st>>>(n, ls64, w.phi);
     k_center_vel<float><<<grd, blk, 0, st>>>(g, u, v, w.tu, w.tv);
-    const bool packed = packed_forms();
-    if (!packed) {
+    if (!packed_stage()) {
         const DivHT<float> ddx = make_divh_f(g.dx), ddy = make_divh_f(g.dy);
         k_ls_stage<1, float><<<grd, blk, 0, st>>>(g, ddx, ddy, w.phi, w.tu, w.tv, w.phi, w.a, dtp);
         k_ls_stage<2, float><<<grd, blk, 0, st>>>(g, ddx, ddy, w.a, w.tu, w.tv, w.phi, w.b, dtp);
@@ -139,7 +144,7 @@ void launch_ls_step32(const Grid &g, int reinit_mode, double max_atime, const do
     const double mt = max_atime > 0.0 ? max_atime : 1.5 * (1.5 * eps);  // kMaxATime, levelset2d.cpp:10
     const int steps = reinit_steps(eps * 0.5, mt);
     cudaMemcpyAsync(w.ls0, w.phi, sizeof(float) * (size_t)n, cudaMemcpyDeviceToDevice, st);
-    if (packed) {
+    if (packed_reinit()) {
         launch_reinit32(g, K, reinit_mode, steps, w, st);
         k_to_f64<<<conv_blocks(n), 256, 0, st>>>(n, w.phi, ls64);
         return;
@@ -164,7 +169,7 @@ int ls32_launches(int reinit_mode, double max_atime, const Grid &g) {
     const double eps = g.dx < g.dy ? g.dx : g.dy;
     const double mt = max_atime > 0.0 ? max_atime : 1.5 * (1.5 * eps);
     const int steps = reinit_steps(eps * 0.5, mt);
-    if (packed_forms()) return 5 + reinit32_launches(reinit_mode, steps) + 1;  // memcpy not counted
+    if (packed_reinit()) return 5 + reinit32_launches(reinit_mode, steps) + 1;  // memcpy not counted
     return 5 + steps * (reinit_mode == 4 ? 3 : 2) + 1;
 }
 

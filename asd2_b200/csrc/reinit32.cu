@@ -14,7 +14,7 @@
 //    dd_{k+1}) serves dP at k and dM at k+1.  Along y (a row pair, packed)
 //    the pair's phi and phi0 rows pass through a per-warp shared-memory row.
 //    The Min-Gibou subcell fix runs only where phi0 changes sign between
-//    neighbours.  Sign: phi0 * rsqrt(phi0^2 + eps^2).
+//    neighbours, out of line.  Sign: phi0 * rsqrt(phi0^2 + eps^2).
 //  * Sussman constraint only where it is nonzero.  It is nonzero only where
 //    |tmp| <= eps (the Heaviside derivative of tmp vanishes elsewhere), a band
 //    of a few cells around the interface.  Pass B writes tmp over phi and
@@ -47,6 +47,17 @@ struct Pass32Const {
     float2 invx, invy, invx2, invy2, hhx, hhy;  // 1/h, 1/h^2, h/2 (both lanes)
     float eps2;
 };
+
+// The subcell branches run at a few cells per row near the interface; out of
+// line they keep the unrolled pass small enough for the instruction cache.
+__device__ __noinline__ float subcell_plus32(float h, DivHT<float> dh, DivHT<float> dh2, float c, float a, float b,
+                                             float cc, float d) {
+    return subcell_plus(h, dh, dh2, c, a, b, cc, d);
+}
+__device__ __noinline__ float subcell_minus32(float h, DivHT<float> dh, DivHT<float> dh2, float c, float a, float b,
+                                              float cc, float d) {
+    return subcell_minus(h, dh, dh2, c, a, b, cc, d);
+}
 
 template <int MODE>
 __device__ __forceinline__ float sign32(float l0, float eps2) {
@@ -98,7 +109,7 @@ __global__ void __launch_bounds__(32 * R32_WARPS, 4)
         z1 = pr(ls0, ib);
     }
 
-#pragma unroll
+#pragma unroll 1
     for (int k = 0; k < R / 2; k++) {
         const int i = ib + 2 * k;
         if (i >= ie) break;
@@ -158,16 +169,16 @@ __global__ void __launch_bounds__(32 * R32_WARPS, 4)
                     const float xm1 = c ? zu.y : zu.x, xp1 = c ? zd.y : zd.x;
                     const float ym1 = r ? zm[c].y : zm[c].x, yp1 = r ? zp[c].y : zp[c].x;
                     if (x0 * xp1 < 0.f)
-                        dpx = subcell_plus(K.dx, K.ddx, K.ddx2, cval, xm1, x0, xp1, ld(ls0, row + 2, col, cin));
+                        dpx = subcell_plus32(K.dx, K.ddx, K.ddx2, cval, xm1, x0, xp1, ld(ls0, row + 2, col, cin));
                     if (x0 * xm1 < 0.f)
-                        dmx = subcell_minus(K.dx, K.ddx, K.ddx2, cval, ld(ls0, row - 2, col, cin), xm1, x0, xp1);
+                        dmx = subcell_minus32(K.dx, K.ddx, K.ddx2, cval, ld(ls0, row - 2, col, cin), xm1, x0, xp1);
                     if (x0 * yp1 < 0.f) {
                         const float2 q = sz[lane + 32 * c + 4];
-                        dpy = subcell_plus(K.dy, K.ddy, K.ddy2, cval, ym1, x0, yp1, r ? q.y : q.x);
+                        dpy = subcell_plus32(K.dy, K.ddy, K.ddy2, cval, ym1, x0, yp1, r ? q.y : q.x);
                     }
                     if (x0 * ym1 < 0.f) {
                         const float2 q = sz[lane + 32 * c];
-                        dmy = subcell_minus(K.dy, K.ddy, K.ddy2, cval, r ? q.y : q.x, ym1, x0, yp1);
+                        dmy = subcell_minus32(K.dy, K.ddy, K.ddy2, cval, r ? q.y : q.x, ym1, x0, yp1);
                     }
                 }
                 const float a = godunov(x0, dpx, dmx, dpy, dmy);

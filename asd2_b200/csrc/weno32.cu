@@ -158,6 +158,8 @@ __global__ void __launch_bounds__(32 * W32_WARPS, 4)
     for (int k = 0; k < R / 2; k++) {
         const int i = ib + 2 * k;
         if (i >= ie) break;
+        // rows i+3, i+4 enter the x window (loads issued first, used last)
+        const float2 fa = fx(i + 3), fb = fx(i + 4);
         // own cells (rows i, i+1; columns cA, cB) and the y fluxes of the row pair
         float ph[2][2], ux[2][2], vy[2][2], pn[2][2];
 #pragma unroll
@@ -229,9 +231,8 @@ __global__ void __launch_bounds__(32 * W32_WARPS, 4)
             Y[c] = fma2(yp[c], fma2(a, nhy, hy), mul2(ym[c], fma2(a, hy, hy)));
         }
 
-        // x direction: rows i+3, i+4 enter the window
-        const float2 fa = fx(i + 3), d5 = sub2(fa, Fp);
-        const float2 fb = fx(i + 4), d6 = sub2(fb, fa);
+        // x direction
+        const float2 d5 = sub2(fa, Fp), d6 = sub2(fb, fa);
         Fp = fb;
         const Tri T1 = tri(d3, d4, d5, epsx), T2 = tri(d4, d5, d6, epsx);
         const float2 xm0 = weno2(d0, d1, d2, d3, d4, rAm2, rCm1, T0.b);
@@ -295,23 +296,19 @@ void launch_s(const Grid &g, const Weno32Const &K, const float *phi_in, const fl
 
 }  // namespace
 
-// Rows per warp of the FP32 strip kernels (weno32.cu, reinit32.cu): the
-// largest of 16, 8 that still gives two waves of 4-warp blocks on 148 SMs,
-// else 4.  ASD2G_LS32_ROWS = 4, 8 or 16 forces it.
-int ls32_rows_per_warp(const Grid &g) {
-    static int forced = -1;
-    if (forced < 0) {
+// Rows per warp of the FP32 strip kernels (weno32.cu, reinit32.cu): 4 (at
+// 2048^2 the advection took 0.19 / 0.22 / 0.30 ms with 4 / 8 / 16 rows: with
+// 16 warps per SM the serial row walk of a warp is latency-bound, and more,
+// shorter walks hide it better than the fewer window loads of long ones).
+// ASD2G_LS32_ROWS = 8 or 16 selects the longer walks.
+int ls32_rows_per_warp(const Grid &) {
+    static int rows = -1;
+    if (rows < 0) {
         const char *e = getenv("ASD2G_LS32_ROWS");
         const int v = e ? atoi(e) : 0;
-        forced = (v == 4 || v == 8 || v == 16) ? v : 0;
+        rows = (v == 8 || v == 16) ? v : 4;
     }
-    if (forced) return forced;
-    const int strips = (g.ny + W32_COLS - 1) / W32_COLS;
-    for (int r : {16, 8}) {
-        const int blocks = strips * ((g.nx + W32_WARPS * r - 1) / (W32_WARPS * r));
-        if (blocks >= 2 * 148 * 4) return r;
-    }
-    return 4;
+    return rows;
 }
 
 void launch_ls_stage32(const Grid &g, int stage, const float *phi_in, const float *tu, const float *tv,
