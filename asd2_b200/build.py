@@ -34,7 +34,6 @@ UNITS = {
     "mg.cu": [],
     "levelset32.cu": [],
     "weno32.cu": [],
-    "reinit32.cu": [],
     "batch.cu": [],
     "unet.cu": [],
     "unet_net.cu": [],

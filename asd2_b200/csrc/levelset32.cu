@@ -91,25 +91,21 @@ __global__ void __launch_bounds__(256) k_volume(Grid g, const double *__restrict
     *counter = 0u;
 }
 
-// The FP32 passes in their packed forms (weno32.cu, reinit32.cu: shared
-// smoothness triples and minmods, FP32x2 arithmetic, the Sussman constraint
-// on the interface band only) or in the per-cell tile forms (the FP64
-// kernels' templates instantiated for float).  Both compute the same scheme.
-// ASD2G_LS32_FORM: packed (both passes packed), cell (neither), stage (the
-// advection stage packed), reinit (the reinitialisation packed).
-int form_bits() {
+// The FP32 advection stage in its packed form (weno32.cu: shared smoothness
+// triples, FP32x2 arithmetic, a sliding row window) or in the per-cell tile
+// form (the FP64 kernel's template instantiated for float); both compute the
+// same scheme.  ASD2G_LS32_FORM=cell selects the per-cell form.  The
+// reinitialisation passes are the per-cell templates: a packed form of them
+// (shared minmods, FP32x2, the Sussman constraint on the interface band only)
+// measured slower at 2048^2 (0.112 vs 0.106 ms per pseudo-step).
+bool packed_stage() {
     static int v = -1;
     if (v < 0) {
         const char *e = getenv("ASD2G_LS32_FORM");
-        v = 0;
-        if (e && std::strcmp(e, "packed") == 0) v = 3;
-        if (e && std::strcmp(e, "stage") == 0) v = 1;
-        if (e && std::strcmp(e, "reinit") == 0) v = 2;
+        v = (e && std::strcmp(e, "cell") == 0) ? 0 : 1;
     }
-    return v;
+    return v == 1;
 }
-bool packed_stage() { return form_bits() & 1; }
-bool packed_reinit() { return form_bits() & 2; }
 
 int64_t padded(const Grid &g) { return (int64_t)g.sx * g.sy; }
 int conv_blocks(int64_t n) { return (int)((n + 255) / 256 < 4 * 148 ? (n + 255) / 256 : 4 * 148); }
@@ -144,11 +140,6 @@ void launch_ls_step32(const Grid &g, int reinit_mode, double max_atime, const do
     const double mt = max_atime > 0.0 ? max_atime : 1.5 * (1.5 * eps);  // kMaxATime, levelset2d.cpp:10
     const int steps = reinit_steps(eps * 0.5, mt);
     cudaMemcpyAsync(w.ls0, w.phi, sizeof(float) * (size_t)n, cudaMemcpyDeviceToDevice, st);
-    if (packed_reinit()) {
-        launch_reinit32(g, K, reinit_mode, steps, w, st);
-        k_to_f64<<<conv_blocks(n), 256, 0, st>>>(n, w.phi, ls64);
-        return;
-    }
     for (int s = 0; s < steps; s++) {
         if (reinit_mode == 0) {
             k_reinit_a<0, float><<<grd, blk, 0, st>>>(g, K, w.phi, w.ls0, w.a, 1);
@@ -169,8 +160,7 @@ int ls32_launches(int reinit_mode, double max_atime, const Grid &g) {
     const double eps = g.dx < g.dy ? g.dx : g.dy;
     const double mt = max_atime > 0.0 ? max_atime : 1.5 * (1.5 * eps);
     const int steps = reinit_steps(eps * 0.5, mt);
-    if (packed_reinit()) return 5 + reinit32_launches(reinit_mode, steps) + 1;  // memcpy not counted
-    return 5 + steps * (reinit_mode == 4 ? 3 : 2) + 1;
+    return 5 + steps * (reinit_mode == 4 ? 3 : 2) + 1;  // memcpy not counted
 }
 
 void launch_volume(const Grid &g, const double *H, const double *HS, double *partial, unsigned *counter, double *out2,

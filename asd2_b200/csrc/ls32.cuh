@@ -7,10 +7,6 @@ namespace asd2g {
 // FP32 work arrays of the mixed level-set step, each (nx+6) x (ny+6).
 struct Ls32Work {
     float *phi, *ls0, *a, *b, *tu, *tv;
-    // band cells of the Sussman constraint: linear indices, new values, count
-    int *band;
-    float *band_val;
-    unsigned *band_n;
 };
 constexpr int LS32_ARRAYS = 6;
 constexpr int VOLUME_BLOCKS = 592;  // partial sums: 2 per block
@@ -26,13 +22,7 @@ void launch_ls_step32(const Grid &g, int reinit_mode, double max_atime, const do
 // phi_in, dt * HJWENO5(phi_in; tu, tv)), interior and ghost mirrors.
 void launch_ls_stage32(const Grid &g, int stage, const float *phi_in, const float *tu, const float *tv,
                        const float *phi_n, float *out, const double *dtp, cudaStream_t st);
-// steps reinitialisation pseudo-steps (modes 0, 2, 4) of w.phi against
-// lsInit = w.ls0 in FP32 (reinit32.cu); w.a and the band arrays are scratch.
-template <typename T> struct LsConstT;
-void launch_reinit32(const Grid &g, const LsConstT<float> &K, int reinit_mode, int steps, const Ls32Work &w,
-                     cudaStream_t st);
-int reinit32_launches(int reinit_mode, int steps);
-// Rows per warp of the FP32 strip kernels (64 columns x R rows per warp).
+// Rows per warp of the FP32 stage kernel (64 columns x R rows per warp).
 int ls32_rows_per_warp(const Grid &g);
 // Kernel launches of one launch_ls_step32 call.
 int ls32_launches(int reinit_mode, double max_atime, const Grid &g);

@@ -296,7 +296,7 @@ void launch_s(const Grid &g, const Weno32Const &K, const float *phi_in, const fl
 
 }  // namespace
 
-// Rows per warp of the FP32 strip kernels (weno32.cu, reinit32.cu): 4 (at
+// Rows per warp of the FP32 stage kernel: 4 (at
 // 2048^2 the advection took 0.19 / 0.22 / 0.30 ms with 4 / 8 / 16 rows: with
 // 16 warps per SM the serial row walk of a warp is latency-bound, and more,
 // shorter walks hide it better than the fewer window loads of long ones).

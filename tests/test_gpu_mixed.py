@@ -75,16 +75,16 @@ def test_mixed_level_set_revolution():
 @pytest.mark.parametrize("nx,ny,mode", [(150, 97, api.REINIT_MINRK2), (37, 211, api.REINIT_MINRK2_SUSSMAN),
                                          (300, 64, api.REINIT_ORIGINAL), (150, 97, api.REINIT_MINRK2_SUSSMAN)])
 def test_mixed_level_set_ragged_grids(nx, ny, mode):
-    """The FP32 advection and reinitialisation kernels work on 64-column
-    strips and row pairs: grids whose sizes are not multiples of either (and
-    narrow ones) must track the FP64 step as closely as the square case
-    does, in every reinitialisation mode the FP32 path implements.
+    """The FP32 advection stage works on 64-column strips and row pairs:
+    grids whose sizes are not multiples of either (and narrow ones) must
+    track the FP64 step as closely as the square case does, in every
+    reinitialisation mode the FP32 path implements.
 
-    Measured after 30 steps (max |phi32 - phi64|): MinRK2 7e-5, all of it at
-    interface cells with |phi0| ~ 1e-5 where the subcell distance is tiny and
-    -c / nd amplifies FP32 rounding (the per-cell FP32 form: 2e-5 there);
-    Original and MinRK2 + Sussman ~1.4e-6; 99% of the cells within 2e-6 in
-    every mode.  Bars: about ten times those."""
+    Measured after 30 steps (max |phi32 - phi64|): MinRK2 2e-5 to 7e-5, all
+    of it at interface cells with |phi0| ~ 1e-5 where the subcell distance is
+    tiny and -c / nd amplifies FP32 rounding; Original and MinRK2 + Sussman
+    ~1.4e-6; 99% of the cells within 2e-6 in every mode.  Bars: about ten
+    times those."""
     h = 1.0 / max(nx, ny)
     X = (np.arange(nx + 6) - 3 + 0.5)[:, None] * h
     Y = (np.arange(ny + 6) - 3 + 0.5)[None, :] * h
