@@ -53,6 +53,11 @@ BYTES_PER_UNKNOWN_ITER = 112  # Jacobi-PCG: 14 FP64 streams per iteration (two f
 # (pre: r 8 + diag/ce/cn 12 + e 4 = 24 B; post: r 8 + coefficients 12 + e 4 +
 # q 8 + z 8 = 40 B) + coarse levels (~1/3 of level 0's 36 FP32 bytes, 12 B)
 MG_BYTES_PER_UNKNOWN_ITER = 180
+# DRAM bytes (read + write) of one MG-FCG iteration at 256^2, measured: ncu
+# --metrics dram__bytes_read.sum,dram__bytes_write.sum --cache-control none on
+# 5 iterations (35 launches) of the bench's own solve: 2.3 KB read and 4.56 MB
+# written in total
+MG_ITER_DRAM_BYTES_256 = 913408
 
 
 def metric_name():
@@ -795,7 +800,12 @@ def run_ours(args):
                                   "pseudo-steps with the Sussman constraint, FP64", "ms_per_step": t_ls * 1e3},
         "roofline": {"bound": "hbm", "kernel": "MG-FCG iteration (k_fcg_a, k_fcg_b, k_mg_pre/post, k_mg_coarse)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "bytes_per_unknown_iter": MG_BYTES_PER_UNKNOWN_ITER,
+                     "traffic": MG_ITER_DRAM_BYTES_256 if args.n == 256 else None,
+                     "traffic_note": "DRAM bytes read + written per FCG iteration (its 7 launches), one ncu "
+                                     "capture of 5 iterations with --cache-control none: "
+                                     "the level hierarchy stays in L2, "
+                                     "what reaches DRAM is L2 write-back",
+                     "bytes_per_unknown_iter": MG_BYTES_PER_UNKNOWN_ITER,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback",
                      "note": "working set is L2-resident at 256^2; iteration time from CUDA events "
                              "(solve minus assembly) / iterations"},
