@@ -98,21 +98,13 @@ __global__ void __launch_bounds__(256) k_volume(Grid g, const double *__restrict
 // the Sussman constraint evaluated on the interface band only (below); a
 // packed form of the passes themselves (shared minmods, FP32x2) measured
 // slower at 2048^2 (0.112 vs 0.106 ms per pseudo-step).
-// ASD2G_LS32_FORM=cell selects the per-cell stage, ASD2G_LS32_SUSSMAN=dense
-// the constraint pass over every cell.
+// ASD2G_LS32_FORM=cell selects the per-cell stage and the dense constraint
+// pass.
 bool packed_stage() {
     static int v = -1;
     if (v < 0) {
         const char *e = getenv("ASD2G_LS32_FORM");
         v = (e && std::strcmp(e, "cell") == 0) ? 0 : 1;
-    }
-    return v == 1;
-}
-bool band_constraint() {
-    static int v = -1;
-    if (v < 0) {
-        const char *e = getenv("ASD2G_LS32_SUSSMAN");
-        v = (e && std::strcmp(e, "dense") == 0) ? 0 : 1;
     }
     return v == 1;
 }
@@ -216,7 +208,7 @@ void launch_ls_step32(const Grid &g, int reinit_mode, double max_atime, const do
             k_reinit_b<2, float><<<grd, blk, 0, st>>>(g, K, w.a, w.ls0, w.phi, w.phi, 1);
         } else {
             k_reinit_a<4, float><<<grd, blk, 0, st>>>(g, K, w.phi, w.ls0, w.a, 1);
-            if (!band_constraint()) {  // dense constraint pass
+            if (!packed_stage()) {  // the per-cell forms throughout, dense constraint pass
                 k_reinit_b<4, float><<<grd, blk, 0, st>>>(g, K, w.a, w.ls0, w.phi, w.b, 1);
                 k_reinit_c<float><<<grd, blk, 0, st>>>(g, K, w.b, w.ls0, w.b, w.phi, 1);
             } else {
@@ -235,7 +227,7 @@ int ls32_launches(int reinit_mode, double max_atime, const Grid &g) {
     const double eps = g.dx < g.dy ? g.dx : g.dy;
     const double mt = max_atime > 0.0 ? max_atime : 1.5 * (1.5 * eps);
     const int steps = reinit_steps(eps * 0.5, mt);
-    if (reinit_mode == 4 && band_constraint()) return 5 + steps * 5 + 1;  // memcpy and memsets not counted
+    if (reinit_mode == 4 && packed_stage()) return 5 + steps * 5 + 1;  // memcpy and memsets not counted
     return 5 + steps * (reinit_mode == 4 ? 3 : 2) + 1;
 }
 

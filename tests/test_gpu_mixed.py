@@ -116,44 +116,6 @@ def test_mixed_level_set_ragged_grids(nx, ny, mode):
     assert abs(v32[1] - v64[1]) <= 1e-4 * v64[1]
 
 
-_BAND_SCRIPT = r"""
-import sys
-import numpy as np
-from asd2_b200 import api
-from asd2_b200 import workloads as W
-lc = W.perturbed_circle(160, seed=5)
-p = api.Params(lc.nx, lc.ny, lc.dx, lc.dy, bc_u=lc.bc_u, bc_v=lc.bc_v, bc_p=lc.bc_p, precision=api.PRECISION_MIXED)
-with api.Session(p) as s:
-    s.upload("ls", lc.ls)
-    s.upload("u", lc.u)
-    s.upload("v", lc.v)
-    for _ in range(12):
-        s.ls_step(lc.dt, api.REINIT_MINRK2_SUSSMAN)
-    np.save(sys.argv[1], s.download("ls"))
-"""
-
-
-def test_band_sussman_matches_dense_pass(tmp_path):
-    """The FP32 MinRK2 + Sussman reinitialisation evaluates the constraint
-    only on the interface band; the dense pass over every cell
-    (ASD2G_LS32_SUSSMAN=dense, read once per process) must give the same
-    level set bit for bit."""
-    import os
-    import subprocess
-    import sys
-    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    out = {}
-    for form in ("band", "dense"):
-        env = dict(os.environ, PYTHONPATH=root)
-        env.pop("ASD2G_LS32_SUSSMAN", None)
-        if form == "dense":
-            env["ASD2G_LS32_SUSSMAN"] = "dense"
-        f = tmp_path / f"{form}.npy"
-        subprocess.run([sys.executable, "-c", _BAND_SCRIPT, str(f)], env=env, cwd=root, check=True, timeout=300)
-        out[form] = np.load(f)
-    assert np.array_equal(out["band"], out["dense"])
-
-
 def test_mixed_droplet_steps():
     c = W.droplet(128, seed=7)
     ref = _run_steps(c, api.PRECISION_FP64, 10, api.PCG)
