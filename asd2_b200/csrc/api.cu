@@ -402,20 +402,6 @@ int asd2g_create(const asd2g_params *p, void *stream, asd2g_session **out) {
                 cudaMemsetAsync(*pp, 0, sizeof(float) * G, s->st);
             }
         }
-        void *bw[3] = {nullptr, nullptr, nullptr};
-        const size_t bsz[3] = {sizeof(int) * N, sizeof(float) * N, sizeof(unsigned)};
-        for (int k = 0; k < 3 && rc == ASD2G_OK; k++) {
-            if (cudaMalloc(&bw[k], bsz[k]) != cudaSuccess) {
-                cudaGetLastError();
-                rc = fail(ASD2G_E_NOMEM, "FP32 band allocation failed");
-            } else {
-                s->allocs.push_back(bw[k]);
-                cudaMemsetAsync(bw[k], 0, bsz[k], s->st);
-            }
-        }
-        s->w32.band = (int *)bw[0];
-        s->w32.band_val = (float *)bw[1];
-        s->w32.band_n = (unsigned *)bw[2];
     }
     if (rc == ASD2G_OK) rc = dalloc(s, &s->partial, 3 * RED_BLOCKS_MAX + 2 * DT_BLOCKS);
     if (rc == ASD2G_OK) rc = dalloc(s, &s->dsc, 8);

@@ -94,12 +94,10 @@ __global__ void __launch_bounds__(256) k_volume(Grid g, const double *__restrict
 // The FP32 advection stage in its packed form (weno32.cu: shared smoothness
 // triples, FP32x2 arithmetic, a sliding row window) or in the per-cell tile
 // form (the FP64 kernel's template instantiated for float); both compute the
-// same scheme.  The reinitialisation passes are the per-cell templates, with
-// the Sussman constraint evaluated on the interface band only (below); a
-// packed form of the passes themselves (shared minmods, FP32x2) measured
-// slower at 2048^2 (0.112 vs 0.106 ms per pseudo-step).
-// ASD2G_LS32_FORM=cell selects the per-cell stage and the dense constraint
-// pass.
+// same scheme.  ASD2G_LS32_FORM=cell selects the per-cell form.  The
+// reinitialisation passes are the per-cell templates: a packed form of them
+// (shared minmods, FP32x2, the Sussman constraint on the interface band only)
+// measured slower at 2048^2 (0.112 vs 0.106 ms per pseudo-step).
 bool packed_stage() {
     static int v = -1;
     if (v < 0) {
@@ -107,63 +105,6 @@ bool packed_stage() {
         v = (e && std::strcmp(e, "cell") == 0) ? 0 : 1;
     }
     return v == 1;
-}
-
-// Sussman constraint on the interface band only (MinRK2 + Sussman mode).
-// The constraint is nonzero only where the Heaviside derivative of tmp is,
-// i.e. |tmp| <= eps: a band of a few cells around the interface.  The second
-// MinRK2 pass writes tmp over phi; k_band_collect lists the band cells,
-// k_band_constraint evaluates phi = tmp + constraint there from tmp (read
-// only) and k_band_apply writes the values back.  Everywhere else the dense
-// pass wrote tmp + 0, so the result is the dense pass's bit for bit; corner
-// ghost cells of tmp read as 0 (the reference's tmpLS corners are never
-// written, and the dense pass reads a work array whose corners stay 0).
-__global__ void k_band_collect(Grid g, float eps, const float *__restrict__ tmp, int *__restrict__ band,
-                               unsigned *__restrict__ band_n) {
-    const int j = NB + blockIdx.x * TJ + threadIdx.x, i = NB + blockIdx.y * TI + threadIdx.y;
-    const bool in = i < g.nx + NB && j < g.ny + NB;
-    const bool hit = in && !(fabsf(tmp[IX(g, in ? i : NB, in ? j : NB)]) > eps);
-    const unsigned m = __ballot_sync(0xffffffffu, hit);  // a block row is one warp (TJ = 32)
-    if (!m) return;
-    const int lane = threadIdx.x;
-    unsigned b0 = 0;
-    if (lane == __ffs(m) - 1) b0 = atomicAdd(band_n, (unsigned)__popc(m));
-    b0 = __shfl_sync(0xffffffffu, b0, __ffs(m) - 1);
-    if (hit) band[b0 + __popc(m & ((1u << lane) - 1u))] = (int)IX(g, i, j);
-}
-
-__global__ void __launch_bounds__(256) k_band_constraint(Grid g, LsConstT<float> K, const float *__restrict__ tmp,
-                                                         const float *__restrict__ ls0, const int *__restrict__ band,
-                                                         const unsigned *__restrict__ band_n, float *__restrict__ vals) {
-    const unsigned n = *band_n;
-    for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        const int idx = band[e];
-        const int i = idx / g.sy, j = idx % g.sy;
-        float Lr[3][3], Ir[3][3];
-#pragma unroll
-        for (int a = 0; a < 3; a++)
-#pragma unroll
-            for (int b = 0; b < 3; b++) {
-                const int ii = i + a - 1, jj = j + b - 1;
-                const bool corner = (ii < NB || ii >= g.nx + NB) && (jj < NB || jj >= g.ny + NB);
-                Lr[a][b] = corner ? 0.f : tmp[IX(g, ii, jj)];
-                Ir[a][b] = ls0[IX(g, ii, jj)];
-            }
-        const float hd = heaviside_deriv(Lr[1][1], K.eps);
-        vals[e] = Lr[1][1] + (hd == 0.f ? 0.f : sussman_constraint_nb(K, Lr, Ir));
-    }
-}
-
-__global__ void __launch_bounds__(256) k_band_apply(Grid g, const int *__restrict__ band,
-                                                    const unsigned *__restrict__ band_n,
-                                                    const float *__restrict__ vals, float *__restrict__ phi) {
-    const unsigned n = *band_n;
-    for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        const int idx = band[e];
-        const float v = vals[e];
-        phi[idx] = v;
-        p_mirror_store(g, phi, idx / g.sy, idx % g.sy, v);
-    }
 }
 
 int64_t padded(const Grid &g) { return (int64_t)g.sx * g.sy; }
@@ -208,16 +149,8 @@ void launch_ls_step32(const Grid &g, int reinit_mode, double max_atime, const do
             k_reinit_b<2, float><<<grd, blk, 0, st>>>(g, K, w.a, w.ls0, w.phi, w.phi, 1);
         } else {
             k_reinit_a<4, float><<<grd, blk, 0, st>>>(g, K, w.phi, w.ls0, w.a, 1);
-            if (!packed_stage()) {  // the per-cell forms throughout, dense constraint pass
-                k_reinit_b<4, float><<<grd, blk, 0, st>>>(g, K, w.a, w.ls0, w.phi, w.b, 1);
-                k_reinit_c<float><<<grd, blk, 0, st>>>(g, K, w.b, w.ls0, w.b, w.phi, 1);
-            } else {
-                k_reinit_b<4, float><<<grd, blk, 0, st>>>(g, K, w.a, w.ls0, w.phi, w.phi, 1);
-                cudaMemsetAsync(w.band_n, 0, sizeof(unsigned), st);
-                k_band_collect<<<grd, blk, 0, st>>>(g, K.eps, w.phi, w.band, w.band_n);
-                k_band_constraint<<<2 * 148, 256, 0, st>>>(g, K, w.phi, w.ls0, w.band, w.band_n, w.band_val);
-                k_band_apply<<<2 * 148, 256, 0, st>>>(g, w.band, w.band_n, w.band_val, w.phi);
-            }
+            k_reinit_b<4, float><<<grd, blk, 0, st>>>(g, K, w.a, w.ls0, w.phi, w.b, 1);
+            k_reinit_c<float><<<grd, blk, 0, st>>>(g, K, w.b, w.ls0, w.b, w.phi, 1);
         }
     }
     k_to_f64<<<conv_blocks(n), 256, 0, st>>>(n, w.phi, ls64);
@@ -227,8 +160,7 @@ int ls32_launches(int reinit_mode, double max_atime, const Grid &g) {
     const double eps = g.dx < g.dy ? g.dx : g.dy;
     const double mt = max_atime > 0.0 ? max_atime : 1.5 * (1.5 * eps);
     const int steps = reinit_steps(eps * 0.5, mt);
-    if (reinit_mode == 4 && packed_stage()) return 5 + steps * 5 + 1;  // memcpy and memsets not counted
-    return 5 + steps * (reinit_mode == 4 ? 3 : 2) + 1;
+    return 5 + steps * (reinit_mode == 4 ? 3 : 2) + 1;  // memcpy not counted
 }
 
 void launch_volume(const Grid &g, const double *H, const double *HS, double *partial, unsigned *counter, double *out2,

@@ -7,10 +7,6 @@ namespace asd2g {
 // FP32 work arrays of the mixed level-set step, each (nx+6) x (ny+6).
 struct Ls32Work {
     float *phi, *ls0, *a, *b, *tu, *tv;
-    // interface band of the Sussman constraint: linear indices, new values, count
-    int *band;
-    float *band_val;
-    unsigned *band_n;
 };
 constexpr int LS32_ARRAYS = 6;
 constexpr int VOLUME_BLOCKS = 592;  // partial sums: 2 per block

@@ -186,14 +186,15 @@ __device__ __forceinline__ T absgrad(const Grid &g, const LsConstT<T> &K, const 
     return godunov(x0, dPX, dMX, dPY, dMY);
 }
 
-// GetSussmanReinitConstraint at one cell (levelset2d.cpp:787-893) from the
-// 3x3 neighbourhoods Lr[a+1][b+1] = ls(i+a, j+b) and Ir = ls0(i+a, j+b);
-// returns the value added to phi.
+// GetSussmanReinitConstraint at interior (i,j) (levelset2d.cpp:787-893);
+// returns the value added to phi (0 when hd == 0).
 template <typename T>
-__device__ __forceinline__ T sussman_constraint_nb(const LsConstT<T> &K, const T (&Lr)[3][3], const T (&Ir)[3][3]) {
+__device__ __forceinline__ T sussman_constraint(const Grid &g, const LsConstT<T> &K, const T *__restrict__ ls,
+                                                const T *__restrict__ ls0, T hd, int i, int j) {
+    if (hd == T(0.0)) return T(0.0);
     const DivHT<T> &ddx = K.ddx, &ddy = K.ddy;
-#define L_(a, b) Lr[(a) + 1][(b) + 1]
-#define I_(a, b) Ir[(a) + 1][(b) + 1]
+#define L_(a, b) ls[IX(g, i + (a), j + (b))]
+#define I_(a, b) ls0[IX(g, i + (a), j + (b))]
     T lf[3][3], lif[3][3], dA[3][3];
     lf[0][0] = T(0.25) * (L_(0, 0) + L_(-1, 0) + L_(-1, -1) + L_(0, -1));
     lf[0][1] = T(0.5) * (L_(0, -1) + L_(0, 0));
@@ -240,22 +241,6 @@ __device__ __forceinline__ T sussman_constraint_nb(const LsConstT<T> &K, const T
     s1 += T(15.0) * Hp11 * L11;
     s2 += T(15.0) * Hp11 * f11;
     return T(0.0) - K.adt * f11 * s1 / s2;
-}
-
-// ... at interior (i,j) of the padded arrays; 0 when hd == 0.
-template <typename T>
-__device__ __forceinline__ T sussman_constraint(const Grid &g, const LsConstT<T> &K, const T *__restrict__ ls,
-                                                const T *__restrict__ ls0, T hd, int i, int j) {
-    if (hd == T(0.0)) return T(0.0);
-    T Lr[3][3], Ir[3][3];
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-#pragma unroll
-        for (int b = 0; b < 3; b++) {
-            Lr[a][b] = ls[IX(g, i + a - 1, j + b - 1)];
-            Ir[a][b] = ls0[IX(g, i + a - 1, j + b - 1)];
-        }
-    return sussman_constraint_nb(K, Lr, Ir);
 }
 
 // UpdateHeavisideFuncDeriv at one value (levelset2d.cpp:27-41)
