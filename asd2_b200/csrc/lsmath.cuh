@@ -248,7 +248,11 @@ template <typename T> __device__ __forceinline__ T heaviside_deriv(T l, T eps) {
     return fabs(l) > eps ? T(0.0) : T(0.5) * (T(1.0) / eps + cos(T(kPi) * l / eps));
 }
 
-// GetSmoothedSignFunc at one value (:914-923)
-template <typename T> __device__ __forceinline__ T smoothed_sign(T l, T eps) { return l / sqrt(l * l + eps * eps); }
+// GetSmoothedSignFunc at one value (:914-923).  FP32 (the mixed path):
+// l * rsqrt(l^2 + eps^2), one MUFU op instead of a divide and a square root.
+template <typename T> __device__ __forceinline__ T smoothed_sign(T l, T eps) {
+    if constexpr (sizeof(T) == sizeof(float)) return l * rsqrtf(fmaf(l, l, eps * eps));
+    else return l / sqrt(l * l + eps * eps);
+}
 
 }  // namespace asd2g
