@@ -246,6 +246,9 @@ struct asd2g_session {
     // device-resident multi-step run (asd2g_run_steps): the step graph, the
     // streams its conditional bodies are captured on, its statistics
     cudaGraphExec_t run_exec = nullptr;
+    // asd2g_ls_step replayed as one graph per reinitialisation mode (dt is
+    // read from dsc[0] on the device, set before each replay)
+    cudaGraphExec_t ls_exec[5] = {};
     int run_reinit = -1, run_maxit = -1;
     double run_tol = -1.0;
     cudaStream_t aux_st[2] = {};
@@ -445,6 +448,8 @@ int asd2g_destroy(asd2g_session *s) {
     for (auto &e : s->chunk_exec)
         if (e) cudaGraphExecDestroy(e);
     if (s->run_exec) cudaGraphExecDestroy(s->run_exec);
+    for (auto &e : s->ls_exec)
+        if (e) cudaGraphExecDestroy(e);
     for (cudaStream_t a : s->aux_st)
         if (a) cudaStreamDestroy(a);
     if (s->run_stats_host) cudaFreeHost(s->run_stats_host);
@@ -522,10 +527,8 @@ int asd2g_apply_bc(asd2g_session *s, int field, char kind) {
 }
 
 // ------------------------------------------------------------ level set --
-int asd2g_ls_advect(asd2g_session *s, double dt) {
-    if (!s) return fail(ASD2G_E_ARG, "null session");
-    int rc = set_dt(s, dt);
-    if (rc) return rc;
+// TVD-RK3 advection of LS with dt = dsc[0] (FP64 kernels).
+static void enqueue_ls_advect(asd2g_session *s) {
     const Grid &g = s->g;
     double *ls = s->f[ASD2G_LS];
     launch_center_vel(g, s->f[ASD2G_U], s->f[ASD2G_V], s->tu, s->tv, s->st);
@@ -533,6 +536,13 @@ int asd2g_ls_advect(asd2g_session *s, double dt) {
     launch_ls_stage(1, g, ls, s->tu, s->tv, ls, s->w1, s->dsc, s->st);
     launch_ls_stage(2, g, s->w1, s->tu, s->tv, ls, s->w2, s->dsc, s->st);
     launch_ls_stage(3, g, s->w2, s->tu, s->tv, ls, ls, s->dsc, s->st);
+}
+
+int asd2g_ls_advect(asd2g_session *s, double dt) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    int rc = set_dt(s, dt);
+    if (rc) return rc;
+    enqueue_ls_advect(s);
     return cuda_check("ls_advect");
 }
 
@@ -587,22 +597,54 @@ int asd2g_smoothed_sign(asd2g_session *s, int ls, int out) {
     return cuda_check("smoothed_sign");
 }
 
-int asd2g_ls_step(asd2g_session *s, double dt, int reinit_mode) {
-    NvtxRange nv("asd2g_ls_step");
-    if (!s) return fail(ASD2G_E_ARG, "null session");
+// Advection + reinitialisation of LS with dt = dsc[0]: the FP32 path for
+// mixed sessions, else the FP64 kernels (asd2g_ls_advect + asd2g_reinit).
+static void enqueue_ls_step(asd2g_session *s, int reinit_mode) {
     if (s->prm.precision == ASD2G_PRECISION_MIXED) {
-        if (!ls32_supported(s->g, reinit_mode))
-            return fail(ASD2G_E_UNSUPPORTED, "mixed precision implements reinit modes 0, 2 and 4, not %d", reinit_mode);
-        int rc = set_dt(s, dt);
-        if (rc) return rc;
         launch_fill_p(s->g, s->f[ASD2G_LS], s->st);
         launch_ls_step32(s->g, reinit_mode, s->prm.ls_max_atime, s->f[ASD2G_U], s->f[ASD2G_V], s->dsc,
                          s->f[ASD2G_LS], s->w32, s->st);
-        return cuda_check("ls_step (mixed)");
+    } else {
+        enqueue_ls_advect(s);
+        launch_reinit(s->g, reinit_mode, s->prm.ls_max_atime, s->f[ASD2G_LS], s->f[ASD2G_LS0], s->w1, s->w2, s->w3,
+                      s->st);
     }
-    int rc = asd2g_ls_advect(s, dt);
+}
+
+// The step's launches (about 20 at the default reinitialisation) are
+// captured once per mode and replayed as one graph: at small grids the
+// kernels take a few microseconds each and launching them one by one from
+// the host is what bounds the step.  Inside a caller's own stream capture
+// they are enqueued directly.
+int asd2g_ls_step(asd2g_session *s, double dt, int reinit_mode) {
+    NvtxRange nv("asd2g_ls_step");
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    if (reinit_mode < 0 || reinit_mode > 4) return fail(ASD2G_E_ARG, "reinit mode %d out of range", reinit_mode);
+    if (s->prm.precision == ASD2G_PRECISION_MIXED && !ls32_supported(s->g, reinit_mode))
+        return fail(ASD2G_E_UNSUPPORTED, "mixed precision implements reinit modes 0, 2 and 4, not %d", reinit_mode);
+    int rc = set_dt(s, dt);
     if (rc) return rc;
-    return asd2g_reinit(s, reinit_mode);
+    if (stream_capturing(s)) {
+        enqueue_ls_step(s, reinit_mode);
+        return cuda_check("ls_step");
+    }
+    if (!s->ls_exec[reinit_mode]) {
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();  // a stream that cannot be captured: launch one by one
+            enqueue_ls_step(s, reinit_mode);
+            return cuda_check("ls_step");
+        }
+        enqueue_ls_step(s, reinit_mode);
+        if (cudaStreamEndCapture(s->st, &graph) != cudaSuccess) return cuda_check("ls_step capture end");
+        cudaGraphExec_t ex = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&ex, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return cuda_check("ls_step graph instantiate");
+        s->ls_exec[reinit_mode] = ex;
+    }
+    if (cudaGraphLaunch(s->ls_exec[reinit_mode], s->st) != cudaSuccess) return cuda_check("ls_step graph launch");
+    return cuda_check("ls_step");
 }
 
 int asd2g_last_volume(asd2g_session *s, double *sharp, double *smooth) {

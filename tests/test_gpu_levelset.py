@@ -142,3 +142,30 @@ def test_full_revolution_area():
     assert abs(a1 - a0) / a0 < 0.05
     band = np.abs(interior(ls0)) < 3 * c.dx
     assert np.abs(interior(ls1) - interior(ls0))[band].max() < 4 * c.dx
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 4])
+def test_ls_step_graph_matches_separate_launches(mode):
+    """asd2g_ls_step replays a captured graph of the advection and
+    reinitialisation launches (dt read from device memory, set before each
+    replay).  Several steps with changing dt must give exactly what
+    asd2g_ls_advect + asd2g_reinit give when launched one by one."""
+    from asd2_b200 import api
+    from asd2_b200 import workloads as W
+    lc = W.perturbed_circle(96, seed=11)
+    outs = []
+    for graph in (True, False):
+        p = api.Params(lc.nx, lc.ny, lc.dx, lc.dy, bc_u=lc.bc_u, bc_v=lc.bc_v, bc_p=lc.bc_p)
+        with api.Session(p) as s:
+            s.upload("ls", lc.ls)
+            s.upload("u", lc.u)
+            s.upload("v", lc.v)
+            for k in range(4):
+                dt = lc.dt * (1.0 - 0.1 * k)
+                if graph:
+                    s.ls_step(dt, mode)
+                else:
+                    s.ls_advect(dt)
+                    s.reinit(mode)
+            outs.append(s.download("ls"))
+    assert np.array_equal(outs[0], outs[1])
