@@ -249,6 +249,10 @@ struct asd2g_session {
     // asd2g_ls_step replayed as one graph per reinitialisation mode (dt is
     // read from dsc[0] on the device, set before each replay)
     cudaGraphExec_t ls_exec[5] = {};
+    // asd2g_droplet_step's phases before and after the solve, replayed as
+    // graphs from the second call on (per reinitialisation mode / one)
+    cudaGraphExec_t pre_exec[5] = {}, post_exec = nullptr;
+    int pre_calls[5] = {}, post_calls = 0;
     int run_reinit = -1, run_maxit = -1;
     double run_tol = -1.0;
     cudaStream_t aux_st[2] = {};
@@ -450,6 +454,9 @@ int asd2g_destroy(asd2g_session *s) {
     if (s->run_exec) cudaGraphExecDestroy(s->run_exec);
     for (auto &e : s->ls_exec)
         if (e) cudaGraphExecDestroy(e);
+    for (auto &e : s->pre_exec)
+        if (e) cudaGraphExecDestroy(e);
+    if (s->post_exec) cudaGraphExecDestroy(s->post_exec);
     for (cudaStream_t a : s->aux_st)
         if (a) cudaStreamDestroy(a);
     if (s->run_stats_host) cudaFreeHost(s->run_stats_host);
@@ -1270,19 +1277,62 @@ static void enqueue_step_post(asd2g_session *s) {
     launch_update_dt(g, s->M, s->f[ASD2G_U], s->f[ASD2G_V], s->partial, s->counter, s->dsc + 1, s->st);
 }
 
+// Runs enqueue() on the session stream: eagerly on the first call (first-use
+// set-up such as kernel attributes stays outside any capture) and inside a
+// caller's stream capture; afterwards as a graph captured once and replayed.
+// The launches are those of the eager call, so are the results.
+extern "C++" {
+namespace {
+template <class F>
+int replay_phase(asd2g_session *s, cudaGraphExec_t *ex, int *calls, const char *what, F enqueue) {
+    if (stream_capturing(s) || *calls == 0) {
+        ++*calls;
+        return enqueue();
+    }
+    if (!*ex) {
+        if (cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();  // a stream that cannot be captured: launch one by one
+            return enqueue();
+        }
+        const int rc = enqueue();
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s->st, &graph);
+        if (rc || e != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc ? rc : cuda_check(what);
+        }
+        const cudaError_t ie = cudaGraphInstantiate(ex, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) {
+            *ex = nullptr;
+            return cuda_check(what);
+        }
+    }
+    if (cudaGraphLaunch(*ex, s->st) != cudaSuccess) return cuda_check(what);
+    return ASD2G_OK;
+}
+}  // namespace
+}  // extern "C++"
+
 int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver, double tol, int maxit, int *iters,
                        double *rel_resid) {
     NvtxRange nv("asd2g_droplet_step");
     if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
+    if (reinit_mode < 0 || reinit_mode > 4) return fail(ASD2G_E_ARG, "reinit mode %d out of range", reinit_mode);
     int rc = p_supported(s);
     if (rc) return rc;
     rc = set_dt(s, *dt);
     if (rc) return rc;
-    rc = enqueue_step_pre(s, reinit_mode);
+    rc = replay_phase(s, &s->pre_exec[reinit_mode], &s->pre_calls[reinit_mode], "droplet_step (before the solve)",
+                      [&] { return enqueue_step_pre(s, reinit_mode); });
     if (rc) return rc;
     const int st = solve(s, solver, tol, maxit, iters, rel_resid);
     if (st < 0) return st;
-    enqueue_step_post(s);
+    rc = replay_phase(s, &s->post_exec, &s->post_calls, "droplet_step (after the solve)", [&] {
+        enqueue_step_post(s);
+        return cuda_check("droplet_step (after the solve)");
+    });
+    if (rc) return rc;
     cudaMemcpyAsync(s->dsc_host, s->dsc, sizeof(double) * 7, cudaMemcpyDeviceToHost, s->st);
     rc = sync(s);
     if (rc) return rc;
