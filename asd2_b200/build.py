@@ -12,6 +12,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -81,7 +82,7 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     headers.append(os.path.join(ROOT, "include", "asd2g.h"))
-    objs = []
+    objs, cmds = [], []
     for unit, extra in UNITS.items():
         src = os.path.join(CSRC, unit)
         obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
@@ -92,9 +93,17 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> str:
                "-I", os.path.join(ROOT, "include"), "-I", CSRC, *extra, "-c", src, "-o", obj]
         if ptxas_v:
             cmd.insert(1, "-Xptxas=-v")
+        cmds.append(cmd)
+    # the translation units are independent: compile them concurrently
+    jobs = max(1, min(len(cmds), os.cpu_count() or 1))
+
+    def run(cmd):
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+    if cmds:
+        with ThreadPoolExecutor(jobs) as ex:
+            list(ex.map(run, cmds))
     if _stale(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
         if verbose:

@@ -1376,20 +1376,34 @@ int ck_read(const char *path, CkHeader &h, std::vector<double> *payload) {
     FILE *f = std::fopen(path, "rb");
     if (!f) return fail(ASD2G_E_IO, "cannot open checkpoint %s", path);
     int rc = ASD2G_OK;
+    // the grid sides are bounded before any size arithmetic (in 64 bits), and
+    // the payload the header claims must be what the file holds before a
+    // buffer of that size is allocated
+    constexpr int32_t kMaxSide = 1 << 20;
+    long long file_bytes = -1;
+    if (std::fseek(f, 0, SEEK_END) == 0) file_bytes = std::ftell(f);
+    std::rewind(f);
     if (std::fread(&h, sizeof h, 1, f) != 1) rc = fail(ASD2G_E_IO, "%s: short header", path);
     else if (std::memcmp(h.magic, CK_MAGIC, 8) != 0 || h.version != 1 || h.header_bytes != sizeof(CkHeader))
         rc = fail(ASD2G_E_IO, "%s: not an asd2g checkpoint (magic/version)", path);
-    else if (h.nx < 1 || h.ny < 1 || h.nbc != 3 || h.nfields != 5 ||
-             h.payload_bytes != (uint64_t)h.nfields * (uint64_t)(h.nx + 6) * (uint64_t)(h.ny + 6) * 8u)
+    else if (h.nx < 1 || h.ny < 1 || h.nx > kMaxSide || h.ny > kMaxSide || h.nbc != 3 || h.nfields != 5 ||
+             h.payload_bytes != (uint64_t)h.nfields * (uint64_t)((int64_t)h.nx + 6) *
+                                    (uint64_t)((int64_t)h.ny + 6) * 8u)
         rc = fail(ASD2G_E_IO, "%s: inconsistent sizes", path);
+    else if (file_bytes < 0 || (uint64_t)file_bytes != sizeof(CkHeader) + h.payload_bytes)
+        rc = fail(ASD2G_E_IO, "%s: file length does not match the header", path);
     if (!rc) {
-        std::vector<double> buf(h.payload_bytes / 8);
-        if (std::fread(buf.data(), 1, h.payload_bytes, f) != h.payload_bytes)
-            rc = fail(ASD2G_E_IO, "%s: short payload", path);
-        else if (ck_checksum(buf.data(), buf.size()) != h.checksum)
-            rc = fail(ASD2G_E_IO, "%s: checksum mismatch", path);
-        else if (payload)
-            payload->swap(buf);
+        try {
+            std::vector<double> buf(h.payload_bytes / 8);
+            if (std::fread(buf.data(), 1, h.payload_bytes, f) != h.payload_bytes)
+                rc = fail(ASD2G_E_IO, "%s: short payload", path);
+            else if (ck_checksum(buf.data(), buf.size()) != h.checksum)
+                rc = fail(ASD2G_E_IO, "%s: checksum mismatch", path);
+            else if (payload)
+                payload->swap(buf);
+        } catch (const std::bad_alloc &) {
+            rc = fail(ASD2G_E_NOMEM, "%s: no host memory for the payload", path);
+        }
     }
     std::fclose(f);
     return rc;

@@ -520,9 +520,16 @@ int solve_impl(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_re
     if (!b->shape_tuned && b->shape_forced < 0) {
         // tile-shape tuning on this batch's own hierarchy (first solve only):
         // four FCG iterations per shape, none allowed to stop early
-        cudaEvent_t e0, e1;
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
+        struct Events {  // destroyed on every exit path
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            ~Events() {
+                if (e0) cudaEventDestroy(e0);
+                if (e1) cudaEventDestroy(e1);
+            }
+        } ev;
+        if (cudaEventCreate(&ev.e0) != cudaSuccess || cudaEventCreate(&ev.e1) != cudaSuccess)
+            return check("batch tile tuning events");
+        cudaEvent_t e0 = ev.e0, e1 = ev.e1;
         int best = 0;
         for (int sh = 0; sh < MG_NSHAPES; sh++) {
             int rc = set_mg_shape(b, sh);
@@ -539,8 +546,6 @@ int solve_impl(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_re
             b->shape_ms[sh] = ms;
             if (ms < b->shape_ms[best]) best = sh;
         }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
         b->shape_tuned = true;
         int rc = set_mg_shape(b, best);
         if (rc) return rc;

@@ -16,7 +16,10 @@
 //    on every GPU that loads the library until the process exits.
 //  * Set-up: the first call on a device resolves the array's device address
 //    (cudaGetSymbolAddress, with that device current) and caches it, so make
-//    that first call before any stream capture begins.
+//    that first call before any stream capture begins.  Later calls look
+//    the address up again unless their stream is capturing, so the cached
+//    address follows a cudaDeviceReset or another context made current on
+//    the device.
 //  * Sharing: every call on a device uses the same array and leaves its last
 //    contents behind.  Calls that overlap on the GPU (different streams or
 //    host threads at the same time) race on it and must be serialised by the
@@ -69,24 +72,36 @@ extern "C" int asd2g_pcg_solve_static(int nx, int ny, int pinned, const double *
                            "ASD2G_STATIC_MAX_UNKNOWNS = 262144 unknowns (512 x 512)");
     if (!diag || !ce || !cn || !b || !x) return static_fail(ASD2G_E_ARG, "asd2g_pcg_solve_static: null pointer");
     if (maxit < 0) return static_fail(ASD2G_E_ARG, "asd2g_pcg_solve_static: maxit must be >= 0");
+    // An error left pending by earlier work of the caller is reported as such,
+    // not blamed on this call's launches.
+    if (cudaGetLastError() != cudaSuccess)
+        return static_fail(ASD2G_E_CUDA, "asd2g_pcg_solve_static: a CUDA error was pending before the call");
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
         return static_fail(ASD2G_E_CUDA, "asd2g_pcg_solve_static: no current CUDA device");
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        return static_fail(ASD2G_E_CUDA, "asd2g_pcg_solve_static: invalid stream");
+    }
     double *base = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_scratch_mu);
-        if (!g_scratch_addr[dev]) {
+        // Looked up on every uncaptured call (cheap): a cudaDeviceReset or
+        // another context current on this device moves the array.
+        if (!g_scratch_addr[dev] || cap == cudaStreamCaptureStatusNone) {
             void *p = nullptr;
             const cudaError_t e = cudaGetSymbolAddress(&p, g_pcg_scratch);
             if (e != cudaSuccess || !p) {
                 cudaGetLastError();
+                g_scratch_addr[dev] = nullptr;
                 return static_fail(ASD2G_E_CUDA, "asd2g_pcg_solve_static: cudaGetSymbolAddress failed");
             }
             g_scratch_addr[dev] = static_cast<double *>(p);
         }
         base = g_scratch_addr[dev];
     }
-    const cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int64_t n = (int64_t)nx * ny;
     double *minv = base, *r = base + kMaxUnknowns, *pa = base + 2 * kMaxUnknowns, *pb = base + 3 * kMaxUnknowns,
            *q = base + 4 * kMaxUnknowns, *partial = base + 5 * kMaxUnknowns;
@@ -100,19 +115,28 @@ extern "C" int asd2g_pcg_solve_static(int nx, int ny, int pinned, const double *
     launch_set_kstate(ks, tol, maxit, 0, 0.0, st);
     launch_pcg_init(g, S, x, r, pa, ks, partial, st);
     if (cudaGetLastError() != cudaSuccess) return static_fail(ASD2G_E_CUDA, "asd2g_pcg_solve_static: launch failed");
-    const int chunk = 64;
+    // Iterations go in pairs (the direction vectors alternate); each one
+    // returns at entry once the solver scalars say done.  Chunks of up to 64
+    // iterations are launched between host checks, the last one cut so that
+    // no more than maxit (rounded up to even) iterations are launched.
+    const int64_t chunk = 64;
     KState hk{};
-    for (int launched = 0;; launched += chunk) {
-        for (int k = 0; k < chunk; k += 2) {
+    for (int64_t launched = 0;;) {
+        const int64_t left = (int64_t)maxit - launched;
+        const int64_t now = left < chunk ? left : chunk;
+        for (int64_t k = 0; k < now; k += 2) {
             launch_pcg_iter(g, S, x, r, pa, pb, q, ks, partial, st);
             launch_pcg_iter(g, S, x, r, pb, pa, q, ks, partial, st);
         }
+        launched += now + (now & 1);
+        if (cudaGetLastError() != cudaSuccess)
+            return static_fail(ASD2G_E_CUDA, "asd2g_pcg_solve_static: launch failed");
         if (cudaMemcpyAsync(&hk, ks, sizeof(KState), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess) {
             cudaGetLastError();
             return static_fail(ASD2G_E_CUDA, "asd2g_pcg_solve_static: CUDA error during the solve");
         }
-        if (hk.done || launched + chunk >= maxit + chunk) break;
+        if (hk.done || launched >= (int64_t)maxit) break;
     }
     if (iters) *iters = hk.it;
     if (rel_resid) *rel_resid = hk.res;

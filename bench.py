@@ -25,8 +25,9 @@ the time taken as the max over ranks.
 
 --impl reference: the CPU implementation of the same solve on the host's
 cores (the C restatement of the reference, one single-threaded process per
-core on the same system, since the reference's own all-Neumann solve is
-mis-indexed and cannot converge -- see DESIGN.md).
+core on the same system, since the reference's own all-Neumann solve pins
+cell 0 with mis-indexed CSR edits, src/mac2d.cpp:1585-1607, and cannot
+converge).
 """
 from __future__ import annotations
 

@@ -432,6 +432,11 @@ int asd2g_checkpoint_info(const char *path, int *nx, int *ny, double *t, long lo
  * stream) and the call returns when the solve has finished.
  * The first call on a device looks up the array's address (with that device
  * current) and caches it; make that first call before any stream capture.
+ * Later calls look the address up again unless their stream is capturing,
+ * so the cache follows a cudaDeviceReset or another context made current on
+ * the device.  An error pending before the call is reported as ASD2G_E_CUDA
+ * without launching anything.  At most maxit iterations (rounded up to
+ * even) are launched.
  * Every call shares the array, which keeps the last call's contents; each
  * call resets what it reads first, and calls that overlap on the GPU race. */
 #define ASD2G_STATIC_MAX_UNKNOWNS (512 * 512)

@@ -737,6 +737,28 @@ void ora_kappa(const ora_grid *g, const double *ls, double *kappa) {
     free(gx); free(gy); free(sz);
 }
 
+/* MACSolver2D::UpdateNTK, mac2d.cpp:124-219, as far as the reference goes.
+ * Q = |1 - |grad phi|| with the ENO gradient ENO_DerivAbsLS_2D(phi, phi)
+ * (:138-145).  Where Q <= 1e-4 the unit normal from central differences is
+ * stored (:204-209).  Where Q > 1e-4 the reference picks one-sided
+ * derivatives but its curve-fitting branch is empty, so nothing is stored
+ * (:150-201).  Cells not stored keep what nxo / nyo held on entry. */
+void ora_ntk(const ora_grid *g, const double *ls, double *nxo, double *nyo) {
+    const double eta = 0.0001, eps = 1.0e-100;
+    double *ab = zalloc(ASZ(g));
+    ora_eno_absgrad(g, ls, ls, ab);
+    for (int i = NB; i < g->nx + NB; i++)
+        for (int j = NB; j < g->ny + NB; j++) {
+            const long k = IX(g, i, j);
+            if (fabs(1.0 - ab[k]) > eta) continue;
+            const double gx = (ls[IX(g, i + 1, j)] - ls[IX(g, i - 1, j)]) / (2.0 * g->dx);
+            const double gy = (ls[IX(g, i, j + 1)] - ls[IX(g, i, j - 1)]) / (2.0 * g->dy);
+            nxo[k] = 1.0 / sqrt(gx * gx + gy * gy + eps) * gx;
+            nyo[k] = 1.0 / sqrt(gx * gx + gy * gy + eps) * gy;
+        }
+    free(ab);
+}
+
 /* UpdateHeavisideFunc, mac2d.cpp:87-101 (all cells) */
 void ora_heaviside(const ora_grid *g, const double *ls, double *H) {
     const long n = ASZ(g);

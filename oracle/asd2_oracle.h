@@ -66,6 +66,7 @@ void ora_reinit(const ora_grid *g, int mode, double max_atime, double *ls);
 
 /* ---- MAC momentum (mac2d.cpp) ---- */
 void ora_kappa(const ora_grid *g, const double *ls, double *kappa);
+void ora_ntk(const ora_grid *g, const double *ls, double *nxo, double *nyo);
 void ora_heaviside(const ora_grid *g, const double *ls, double *H);
 void ora_smooth_heaviside(const ora_grid *g, const double *ls, double *HS);
 void ora_conv_u(const ora_grid *g, const double *u, const double *v, double *cU);

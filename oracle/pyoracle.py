@@ -118,7 +118,7 @@ class Oracle:
             "ora_eno_absgrad": [G, _dp, _dp, _dp], "ora_subcell_eno_absgrad": [G, _dp, _dp, _dp],
             "ora_sussman_constraint": [G, _dp, _dp, _dp, _dp],
             "ora_reinit": [G, C.c_int, C.c_double, _dp],
-            "ora_kappa": [G, _dp, _dp], "ora_heaviside": [G, _dp, _dp], "ora_smooth_heaviside": [G, _dp, _dp],
+            "ora_kappa": [G, _dp, _dp], "ora_ntk": [G, _dp, _dp, _dp], "ora_heaviside": [G, _dp, _dp], "ora_smooth_heaviside": [G, _dp, _dp],
             "ora_conv_u": [G, _dp, _dp, _dp], "ora_conv_v": [G, _dp, _dp, _dp],
             "ora_visc_u": [G, F, _dp, _dp, _dp, _dp, _dp], "ora_visc_v": [G, F, _dp, _dp, _dp, _dp, _dp],
             "ora_rhs_u": [G, F, _dp, _dp, _dp, _dp, _dp], "ora_rhs_v": [G, F, _dp, _dp, _dp, _dp, _dp],
@@ -186,6 +186,11 @@ class Oracle:
     def subcell_eno_absgrad(self, g, ls, ls0): return self._unary("ora_subcell_eno_absgrad", g, ls, ls0)
     def sussman_constraint(self, g, ls, ls0, hd): return self._unary("ora_sussman_constraint", g, ls, ls0, hd)
     def heaviside(self, g, ls): return self._unary("ora_heaviside", g, ls)
+
+    def ntk(self, g, ls, nxo, nyo):
+        """UpdateNTK's unit normal into nxo / nyo (cells it skips keep their values)."""
+        self.L.ora_ntk(C.byref(g.c()), ls, nxo, nyo)
+        return nxo, nyo
     def smooth_heaviside(self, g, ls): return self._unary("ora_smooth_heaviside", g, ls)
     def conv_u(self, g, u, v): return self._unary("ora_conv_u", g, u, v)
     def conv_v(self, g, u, v): return self._unary("ora_conv_v", g, u, v)
@@ -357,7 +362,7 @@ class Reference:
             ("ref_mac_set_state", [V, _dp, _dp, _dp, C.c_double], None),
             ("ref_mac_get_state", [V, _dp, _dp, _dp, _dp, _dp], C.c_double),
             ("ref_mac_set_kappa", [V, _dp], None),
-            ("ref_mac_kappa", [V, _dp, _dp], None), ("ref_mac_heaviside", [V, _dp, _dp, _dp], None),
+            ("ref_mac_kappa", [V, _dp, _dp], None), ("ref_mac_ntk", [V, _dp, _dp, _dp], None), ("ref_mac_heaviside", [V, _dp, _dp, _dp], None),
             ("ref_mac_conv", [V, _dp, _dp, _dp, _dp], None),
             ("ref_mac_visc", [V, _dp, _dp, _dp, _dp, _dp, _dp], None),
             ("ref_mac_rhs", [V, _dp, _dp, _dp, _dp, _dp, _dp], None),
@@ -446,6 +451,10 @@ class Reference:
         self.L.ref_mac_set_kappa(self.h, k)
 
     def kappa(self, ls): return self._u("ref_mac_kappa", ls)
+
+    def ntk(self, ls, nxo, nyo):
+        self.L.ref_mac_ntk(self.h, ls, nxo, nyo)
+        return nxo, nyo
 
     def heaviside(self, ls):
         H, HS = self.z(), self.z()

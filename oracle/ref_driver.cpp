@@ -8,6 +8,7 @@
 #include <memory>
 #include <sstream>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "levelset2d.h"
@@ -216,6 +217,17 @@ void ref_mac_kappa(void *h, const double *ls, double *kappa) {
     RefCtx *c = static_cast<RefCtx *>(h);
     c->mac->UpdateKappa(vin(c, ls));
     vout(c, c->mac->m_kappa, kappa);
+}
+// UpdateNTK(LSolver, ls, (nx, ny), t1, t2, kappa): the normal components
+// start from nxo / nyo (the reference leaves cells it does not reach as they
+// were) and are copied back.
+void ref_mac_ntk(void *h, const double *ls, double *nxo, double *nyo) {
+    RefCtx *c = static_cast<RefCtx *>(h);
+    std::vector<double> nx = vin(c, nxo), ny = vin(c, nyo);
+    std::vector<double> t1x(c->n), t1y(c->n), t1z(c->n), t2x(c->n), t2y(c->n), t2z(c->n), kap(c->n);
+    c->mac->UpdateNTK(c->ls, vin(c, ls), std::tie(nx, ny), std::tie(t1x, t1y, t1z), std::tie(t2x, t2y, t2z), kap);
+    vout(c, nx, nxo);
+    vout(c, ny, nyo);
 }
 void ref_mac_heaviside(void *h, const double *ls, double *H, double *HS) {
     RefCtx *c = static_cast<RefCtx *>(h);

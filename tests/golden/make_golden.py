@@ -132,6 +132,17 @@ def mac_cases(name, nx, ny, dx, dy):
     out.update(ls=ls, u=u, v=v)
     k = R.kappa(ls)
     out["kappa"] = k
+    # UpdateNTK on the droplet's distance field and on a plane whose slope is
+    # 1 on the west half and 1.3 on the east half: the normal is stored where
+    # |1 - |grad phi|| <= 1e-4 only, so the outputs start from sentinels that
+    # mark the cells the reference leaves alone
+    Xc, Yc = centres(nx, ny, dx, dy)
+    plane = 0.6 * Xc + 0.8 * Yc - 0.4 * (nx * dx)
+    plane = np.where(Xc < 0.5 * nx * dx, plane, 1.3 * plane)
+    for tag2, phi in (("sdf", ls), ("plane", plane)):
+        n0, n1 = np.full(g.shape, 7.0), np.full(g.shape, -7.0)
+        R.ntk(phi, n0, n1)
+        out[f"ntk_{tag2}_phi"], out[f"ntk_{tag2}_nx"], out[f"ntk_{tag2}_ny"] = phi, n0, n1
     H, HS = R.heaviside(ls)
     out["H"], out["HS"] = H, HS
     cU, cV = R.conv(u, v)
@@ -229,6 +240,41 @@ def laplace_case():
     return {"L_ps": ps, "L_csr_a": a, "L_csr_b": b}
 
 
+BC_KINDS_UV = ["periodic", "neumann", "dirichlet", "axisym", "wall", "inlet", "outlet"]
+BC_KINDS_P = BC_KINDS_UV + ["pressure", "lsfree"]
+BC_TRIALS = 9
+
+
+def bc_kinds(trial):
+    """W/E/S/N kinds of the U/V grids and of the P grid in one trial: over the
+    trials every kind meets every side (velocity grids take no "pressure" or
+    "lsfree": the reference exits on a constant-pressure velocity side)."""
+    uv = tuple(BC_KINDS_UV[(trial + 2 * s) % len(BC_KINDS_UV)] for s in range(4))
+    vv = tuple(BC_KINDS_UV[(trial + 3 * s + 1) % len(BC_KINDS_UV)] for s in range(4))
+    pp = tuple(BC_KINDS_P[(trial + 2 * s) % len(BC_KINDS_P)] for s in range(4))
+    return uv, vv, pp
+
+
+def bc_cases():
+    """Ghost fills of the U, V and P grids (ApplyBC_{U,V,P}_2D,
+    src/bc2d.cpp:123-934) for every boundary kind on every side, with random
+    boundary constants, on a 13 x 9 grid of unequal spacings."""
+    rng = np.random.Generator(np.random.PCG64(21))
+    out = {}
+    for t in range(BC_TRIALS):
+        bu, bv, bp = bc_kinds(t)
+        cu, cv, cp = (rng.uniform(-1.0, 1.0, 4) for _ in range(3))
+        g = GridSpec(13, 9, 0.1, 0.125, bc_u=bu, bc_v=bv, bc_p=bp, cu=tuple(cu), cv=tuple(cv), cp=tuple(cp))
+        R = Reference(g)
+        out[f"{t}_consts"] = np.stack([cu, cv, cp])
+        for kind in ("U", "V", "P"):
+            a = rng.standard_normal(g.shape)
+            out[f"{t}_{kind}_in"] = a
+            out[f"{t}_{kind}_out"] = R.bc(kind, a.copy(), which=0)
+        R.close()
+    return {f"BC{k}": v for k, v in out.items()}
+
+
 def main():
     data = {}
     for name, (nx, ny, dx, dy) in GRIDS.items():
@@ -236,6 +282,7 @@ def main():
         data.update(mac_cases(name, nx, ny, dx, dy))
     data.update(dirichlet_cases())
     data.update(laplace_case())
+    data.update(bc_cases())
     path = os.path.join(OUT, "reference_golden.npz")
     np.savez_compressed(path, **data)
     print(f"wrote {path}: {len(data)} arrays, {os.path.getsize(path) / 1024:.0f} KB")

@@ -67,3 +67,14 @@ def assert_close(a, b, rtol, atol=0.0, what=""):
         idx = np.unravel_index(np.argmax(d - lim), d.shape)
         raise AssertionError(f"{what}: max |diff| {d.max():.3e} exceeds tolerance at {idx} "
                              f"({a[idx]!r} vs {b[idx]!r})")
+
+
+def bc_fixture(trial):
+    """The grid of one boundary-fill golden trial (tests/golden/make_golden.py
+    bc_cases) and a getter for its arrays."""
+    from tests.golden.make_golden import bc_kinds
+    G = golden()
+    bu, bv, bp = bc_kinds(trial)
+    cu, cv, cp = (tuple(float(x) for x in row) for row in G[f"BC{trial}_consts"])
+    g = GridSpec(13, 9, 0.1, 0.125, bc_u=bu, bc_v=bv, bc_p=bp, cu=cu, cv=cv, cp=cp)
+    return g, (lambda key: G[f"BC{trial}_{key}"])

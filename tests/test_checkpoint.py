@@ -60,3 +60,24 @@ def test_missing_file(tmp_path):
     with pytest.raises(api.Asd2gError) as e:
         api.checkpoint_info(tmp_path / "nope.ck")
     assert e.value.code == -7
+
+
+@pytest.mark.parametrize("claim", ["huge_side", "huge_consistent_payload"])
+def test_library_refuses_header_claiming_huge_grid(tmp_path, claim):
+    """A damaged or crafted header that claims an enormous grid is refused
+    with ASD2G_E_IO before any size arithmetic can overflow or a buffer of
+    the claimed size is allocated."""
+    import struct
+    p = tmp_path / "h.ck"
+    CK.write(p, _fields(8, 8, seed=6))
+    raw = bytearray(p.read_bytes())
+    if claim == "huge_side":
+        struct.pack_into("<i", raw, 16, 2 ** 31 - 4)
+    else:  # sides within int range and a payload size consistent with them, but absent from the file
+        nx = ny = 60000
+        struct.pack_into("<ii", raw, 16, nx, ny)
+        struct.pack_into("<Q", raw, 64, 5 * (nx + 6) * (ny + 6) * 8)
+    p.write_bytes(bytes(raw))
+    with pytest.raises(api.Asd2gError) as e:
+        api.checkpoint_info(p)
+    assert e.value.code == -7

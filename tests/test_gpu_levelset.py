@@ -13,8 +13,9 @@ import pytest
 from asd2_b200 import api
 from asd2_b200 import workloads as W
 from oracle.pyoracle import Oracle
-from tests.helpers import (GRIDS, assert_bitexact, assert_close, golden, grid_from_case, interior, ls_grid,
-                           params_for)
+from tests.golden.make_golden import BC_TRIALS
+from tests.helpers import (GRIDS, assert_bitexact, assert_close, bc_fixture, golden, grid_from_case, interior,
+                           ls_grid, params_for)
 
 pytestmark = pytest.mark.gpu
 O = Oracle()
@@ -99,6 +100,19 @@ def test_boundary_fills_all_kinds():
                 s.upload(f, a)
                 s.apply_bc(f, kind)
                 assert_bitexact(s.download(f), O.bc(g, kind, a.copy()), f"{kind} fill {bu, bv, bp}")
+
+
+@pytest.mark.parametrize("trial", range(BC_TRIALS))
+def test_boundary_fills_golden(trial):
+    """Every boundary kind on every side (periodic, inlet, outlet, axisym,
+    wall, neumann, dirichlet; pressure and lsfree on the P grid) against the
+    reference's own ApplyBC_{U,V,P}_2D output (src/bc2d.cpp:123-934)."""
+    g, k = bc_fixture(trial)
+    with session(g) as s:
+        for kind, f in (("U", "w0"), ("V", "w1"), ("P", "w2")):
+            s.upload(f, k(f"{kind}_in"))
+            s.apply_bc(f, kind)
+            assert_bitexact(s.download(f), k(f"{kind}_out"), f"{kind} fill {g.bc_u, g.bc_v, g.bc_p}")
 
 
 def test_level_set_steps_config1_shape():

@@ -23,6 +23,24 @@ O = Oracle()
 
 
 @pytest.mark.parametrize("name", list(GRIDS))
+def test_update_ntk_golden(name):
+    """UpdateNTK (src/mac2d.cpp:124-219) against the reference's own output:
+    unit normal where |1 - |grad phi|_ENO| <= 1e-4, sentinels kept elsewhere
+    (the reference's curve-fitting branch stores nothing)."""
+    G = golden()
+    g = mac_grid(name)
+    with api.Session(params_for(g)) as s:
+        for case in ("sdf", "plane"):
+            k = lambda t: G[f"{name}M_ntk_{case}_{t}"]
+            s.upload("ls", k("phi"))
+            s.upload("w0", np.full(g.shape, 7.0))
+            s.upload("w2", np.full(g.shape, -7.0))
+            s.update_ntk("ls", "w0", "w2")
+            assert_bitexact(s.download("w0"), k("nx"), f"UpdateNTK x, {case}")
+            assert_bitexact(s.download("w2"), k("ny"), f"UpdateNTK y, {case}")
+
+
+@pytest.mark.parametrize("name", list(GRIDS))
 def test_momentum_terms(name):
     G = golden()
     k = lambda s: G[f"{name}M_{s}"]

@@ -1,0 +1,273 @@
+"""GPU parity at the sizes the benchmark measures, against the oracle.
+
+The function-level tests pin every kernel to the reference on small grids.
+These tests run the measured workloads themselves, at their own sizes, and
+compare with the oracle (the C restatement: FP64, fixed summation order,
+itself pinned bit for bit to the reference) on the same seeded inputs.
+
+* The 256^2 GFM system behind the solves/s headline: the droplet after three
+  full steps.  The GPU solves it with the MG-FCG, the learned-preconditioner
+  FCG and the FP64 Jacobi-PCG to rel. residual 1e-8.  The oracle solves it
+  with its FP64 PCG to 1e-12.  Bar: pressure within 1e-6 of max |p|, true
+  FP64 residual <= 1e-8.
+* 20 full steps of the 256^2 droplet with the plain FP64 method.  Bars: level
+  set, velocity and pressure near the oracle's, interface-cell and
+  crossing-face masks equal at every step.
+* The full revolution of the 128^2 perturbed circle (1138 steps).  MinRK2 is
+  bit-identical.  MinRK2 with the Sussman constraint (cos() in the
+  constraint) stays within 1e-12 of max |phi|.  Masks and area loss are equal.
+* One instance of the mixed-precision run: the 256^2 droplet for 10 steps
+  with FP32 level set and V-cycle, against the FP64 oracle.  The error of
+  every field (phi, u, v, p, kappa, area) is checked against bars a few
+  times the measured ones.
+* One batched step of uneven droplets against the oracle, instance by
+  instance.
+* One 512^2 learned-preconditioner system (four droplets, density ratio
+  1000) against the oracle.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from asd2_b200 import api
+from asd2_b200 import workloads as W
+from oracle.pyoracle import Oracle
+from tests.helpers import assert_bitexact, fluid_from_case, grid_from_case, interior
+
+pytestmark = pytest.mark.gpu
+O = Oracle()
+
+
+def _rel(a, b):
+    """max |a - b| / max |b| over the interior cells."""
+    a, b = interior(np.asarray(a)), interior(np.asarray(b))
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _oracle_state(c):
+    g, f = grid_from_case(c), fluid_from_case(c)
+    st = dict(ls=c.ls.copy(), u=c.u.copy(), v=c.v.copy(), kappa=g.zeros(), ps=g.zeros(), p=g.zeros())
+    O.bc(g, "p", st["ls"])
+    st["dt"] = O.update_dt(g, f, st["u"], st["v"])
+    return g, f, st
+
+
+def _oracle_solve(g, f, dt, ls, kappa, H, div, tol=1e-12):
+    sysd = O.gfm_assemble(g, f, dt, ls, kappa.copy(), H, div, recompute_kappa=True)
+    x, it, _, tres = O.pcg(g, sysd, tol=tol, maxit=500000)
+    return sysd, O.scatter(g, x), it, tres
+
+
+def test_headline_system_256():
+    """The bench's 256^2 system (seed 0, three full steps from rest, the next
+    step's dt): GPU prep steps against the oracle's, then each GPU solver at
+    1e-8 against the oracle's FP64 PCG at 1e-12."""
+    import bench
+    c, s, snap, dt = bench.prepare_state(256, 0, None)
+    try:
+        g, f, st = _oracle_state(c)
+        for _ in range(bench.PREP_STEPS):
+            info = O.droplet_step(g, f, st, tol=1e-10, maxit=500000)
+        # the prep steps march with the oracle: same masks, level set and dt
+        assert np.array_equal(O.interface_mask(g, snap["ls"]), O.interface_mask(g, st["ls"]))
+        assert np.array_equal(O.ghost_face_mask(g, snap["ls"]), O.ghost_face_mask(g, st["ls"]))
+        assert np.array_equal(snap["H"], info["H"])
+        e_ls = _rel(snap["ls"], st["ls"])
+        assert e_ls <= 1e-10, e_ls
+        assert abs(dt - st["dt"]) <= 1e-9 * st["dt"], (dt, st["dt"])
+        # the system the bench times: assembled from the snapshot with dt
+        sysd, ps_ref, it_ref, tres_ref = _oracle_solve(g, f, dt, snap["ls"], snap["kappa"], snap["H"], snap["div"])
+        assert tres_ref < 1e-11
+        s.assemble_gfm(dt, recompute_kappa=True)
+        gsys = s.get_system()
+        for k in ("diag", "ce", "cn", "rhs"):
+            assert_bitexact(gsys[k] + 0.0, sysd[k] + 0.0, f"GFM {k} of the headline system")
+        scale = np.abs(interior(ps_ref)).max()
+        solvers = [("mg_fcg", api.MGPCG), ("jacobi_pcg", api.PCG)]
+        from asd2_b200 import train_unet as T
+        net = None
+        if os.path.exists(T.DEFAULT_WEIGHTS):
+            params, _ = T.load_params()
+            net = api.UNet(1, 256, 256)
+            net.set_params(params)
+            s.set_preconditioner_net(net)
+            solvers.append(("learned", api.UNET))
+        errs = {}
+        for name, sv in solvers:
+            s.assemble_gfm(dt, recompute_kappa=True)
+            r = s.solve_pressure(sv, tol=1e-8, maxit=500000, dt=dt)
+            assert r["status"] == 0, (name, r)
+            tres = s.true_residual()
+            assert tres <= 1e-8, (name, tres)
+            errs[name] = float(np.abs(interior(s.download("ps")) - interior(ps_ref)).max() / scale)
+            if sv == api.UNET:
+                assert not s.last_fallback()
+        print(f"headline 256^2: pressure error vs oracle (rel. to max) {errs}; oracle PCG {it_ref} iterations")
+        for name, e in errs.items():
+            assert e <= 1e-6, (name, e)
+        if net is not None:
+            s.set_preconditioner_net(None)
+            net.close()
+    finally:
+        s.close()
+
+
+def test_config2_20_steps_256():
+    """20 full steps of the 256^2 droplet (density ratio 1000, viscosity
+    ratio 100, no-slip walls) with the FP64 Jacobi-PCG to 1e-10, the oracle
+    marching beside it with its own dt."""
+    c = W.droplet(256, seed=0)
+    g, f, st = _oracle_state(c)
+    worst = dict(ls=0.0, u=0.0, v=0.0, ps=0.0)
+    with api.Session(api.Params.from_case(c)) as s:
+        s.upload("ls", st["ls"])
+        s.upload("u", st["u"])
+        s.upload("v", st["v"])
+        dt = st["dt"]
+        for k in range(20):
+            r = s.droplet_step(dt, solver=api.PCG, tol=1e-10, maxit=500000)
+            O.droplet_step(g, f, st, tol=1e-10, maxit=500000)
+            assert r["status"] == 0, (k, r)
+            gl = s.download("ls")
+            if k == 0:
+                assert_bitexact(gl, st["ls"], "level set after the first step")
+            assert np.array_equal(O.interface_mask(g, gl), O.interface_mask(g, st["ls"])), k
+            assert np.array_equal(O.ghost_face_mask(g, gl), O.ghost_face_mask(g, st["ls"])), k
+            for fld in worst:
+                worst[fld] = max(worst[fld], _rel(s.download(fld), st[fld]))
+            assert abs(r["dt_next"] - st["dt"]) <= 1e-8 * st["dt"], (k, r["dt_next"], st["dt"])
+            dt = st["dt"]
+    print(f"cfg 2, 20 steps at 256^2: worst error vs oracle (rel. to max) {worst}")
+    assert worst["ls"] <= 1e-10, worst
+    for fld in ("u", "v", "ps"):
+        assert worst[fld] <= 1e-6, worst
+
+
+def _area(g, ls):
+    """(cells with phi > 0, integral of the smoothed Heaviside) of the interior."""
+    return int((interior(ls) > 0).sum()), float(interior(O.smooth_heaviside(g, ls)).sum() * g.dx * g.dy)
+
+
+@pytest.mark.parametrize("mode", [api.REINIT_MINRK2, api.REINIT_MINRK2_SUSSMAN])
+def test_config1_full_revolution_128(mode):
+    """The 128^2 perturbed circle (seed 0) for one full revolution at CFL 0.5:
+    one MinRK2 reinitialisation of the initial field, then advection plus
+    five pseudo-steps per step."""
+    c = W.perturbed_circle(128, seed=0)
+    g = grid_from_case(c)
+    a = c.ls.copy()
+    O.reinit(g, api.REINIT_MINRK2, a)
+    a0 = a.copy()
+    p = api.Params(c.nx, c.ny, c.dx, c.dy, bc_u=c.bc_u, bc_v=c.bc_v, bc_p=c.bc_p)
+    with api.Session(p) as s:
+        s.upload("ls", c.ls)
+        s.upload("u", c.u)
+        s.upload("v", c.v)
+        s.reinit(api.REINIT_MINRK2)
+        assert_bitexact(s.download("ls"), a0, "initial reinitialisation")
+        for _ in range(c.steps):
+            s.ls_step(c.dt, mode)
+        got = s.download("ls")
+    for _ in range(c.steps):
+        O.ls_advect(g, a, c.u, c.v, c.dt)
+        O.reinit(g, mode, a)
+    assert c.steps == 1138
+    e = _rel(got, a)
+    print(f"cfg 1 full revolution, reinit mode {mode}: phi error {e:.3e}, area {_area(g, a0)} -> {_area(g, a)}")
+    if mode == api.REINIT_MINRK2:
+        assert_bitexact(got, a, "full revolution (MinRK2)")
+    else:
+        assert e <= 1e-12, e
+    assert np.array_equal(O.interface_mask(g, got), O.interface_mask(g, a))
+    (n0, s0), (ng, sg), (no, so) = _area(g, a0), _area(g, got), _area(g, a)
+    assert ng == no
+    assert abs((sg - s0) - (so - s0)) <= 1e-12 * s0
+
+
+def test_mixed_precision_vs_oracle_256():
+    """The mixed-precision droplet (FP32 level set and V-cycle, FP64 outer
+    solve) for 10 steps against the FP64 oracle on the same seed: every
+    field's error and the volume change, with bars a few times the measured
+    figures."""
+    c = W.droplet(256, seed=0)
+    g, f, st = _oracle_state(c)
+    vol0 = _area(g, st["ls"])[1]
+    with api.Session(api.Params.from_case(c, precision=api.PRECISION_MIXED)) as s:
+        s.upload("ls", st["ls"])
+        s.upload("u", st["u"])
+        s.upload("v", st["v"])
+        dt = st["dt"]
+        for k in range(10):
+            r = s.droplet_step(dt, reinit_mode=api.REINIT_MINRK2, solver=api.MGPCG, tol=1e-10, maxit=100000)
+            O.droplet_step(g, f, st, tol=1e-10, maxit=500000)
+            assert r["status"] == 0, (k, r)
+            dt = st["dt"]
+        got = {k: s.download(k) for k in ("ls", "u", "v", "p", "kappa")}
+    err = {k: _rel(got[k], st[k]) for k in got}
+    vol_gpu, vol_ora = _area(g, got["ls"])[1], _area(g, st["ls"])[1]
+    err["area"] = abs(vol_gpu - vol_ora) / vol0
+    print(f"mixed precision 256^2, 10 steps: error vs FP64 oracle (rel. to max) {err}")
+    bars = dict(ls=1e-4, u=1e-3, v=1e-3, p=1e-3, kappa=5e-2, area=1e-5)
+    for k, b in bars.items():
+        assert err[k] <= b, (k, err[k], b)
+
+
+def test_batched_step_vs_oracle():
+    """One asd2g_batch_step of three uneven droplets (sides 64, 96, 128,
+    density and viscosity ratios of the batched workload): each instance
+    against the oracle's droplet step.  Level set bit-identical, velocity
+    and pressure at the MG-FCG's 1e-10 tolerance."""
+    cases = [W.droplet(n, seed=31 + n, rho_ratio=rr, mu_ratio=mr, radius=(0.08, 0.2))
+             for n, rr, mr in ((64, 1000.0, 100.0), (96, 12.0, 3.0), (128, 250.0, 40.0))]
+    params = [api.Params.from_case(c) for c in cases]
+    states = [_oracle_state(c) for c in cases]
+    with api.Batch(params) as b:
+        for i, (g, f, st) in enumerate(states):
+            for k in ("ls", "u", "v"):
+                b.upload(i, k, st[k])
+        r = b.step(np.array([st["dt"] for _, _, st in states]), tol=1e-10, maxit=10000)
+        assert r["status"] == 0, r
+        for i, (g, f, st) in enumerate(states):
+            O.droplet_step(g, f, st, tol=1e-12, maxit=500000)
+            assert_bitexact(b.download(i, "ls"), st["ls"], f"instance {i} level set")
+            errs = {k: _rel(b.download(i, k), st[k]) for k in ("u", "v", "ps")}
+            print(f"batched instance {i} ({cases[i].nx}^2): error vs oracle {errs}")
+            for k, e in errs.items():
+                assert e <= 1e-6, (i, k, e)
+            assert abs(r["dt_next"][i] - st["dt"]) <= 1e-8 * st["dt"]
+
+
+def test_learned_system_512_vs_oracle():
+    """A 512^2 system of the learned-preconditioner evaluation (four
+    droplets, density ratio 1000, after one full step from rest): the
+    learned FCG at 1e-8 against the oracle's FP64 PCG at 1e-12."""
+    from asd2_b200 import train_unet as T
+    if not os.path.exists(T.DEFAULT_WEIGHTS):
+        pytest.skip("no trained weights in the package")
+    n = 512
+    c = W.multi_droplet(n, seed=17, count=4, rho_ratio=1000.0)
+    g, f = grid_from_case(c), fluid_from_case(c)
+    params, _ = T.load_params()
+    net = api.UNet(1, n, n)
+    net.set_params(params)
+    with api.Session(api.Params.from_case(c)) as s:
+        s.upload("ls", c.ls)
+        s.upload("u", c.u)
+        s.upload("v", c.v)
+        s.apply_bc("ls", "P")
+        dt = s.update_dt()
+        r = s.droplet_step(dt, solver=api.MGPCG, tol=1e-10, maxit=100000)
+        assert r["status"] == 0
+        snap = {k: s.download(k) for k in ("ls", "H", "div", "kappa")}
+        _, ps_ref, it_ref, tres_ref = _oracle_solve(g, f, dt, snap["ls"], snap["kappa"], snap["H"], snap["div"])
+        s.set_preconditioner_net(net)
+        s.assemble_gfm(dt, recompute_kappa=False)
+        r = s.solve_pressure(api.UNET, tol=1e-8, maxit=100000, dt=dt)
+        assert r["status"] == 0 and not s.last_fallback(), r
+        assert s.true_residual() <= 1e-8
+        e = float(np.abs(interior(s.download("ps")) - interior(ps_ref)).max() / np.abs(interior(ps_ref)).max())
+        s.set_preconditioner_net(None)
+    net.close()
+    print(f"learned 512^2: {r['iters']} iterations (oracle PCG {it_ref}), pressure error {e:.3e}")
+    assert e <= 1e-6, e

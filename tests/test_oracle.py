@@ -12,7 +12,8 @@ import numpy as np
 import pytest
 
 from oracle.pyoracle import FluidSpec, GridSpec, Oracle, Reference, have_reference
-from tests.helpers import GRIDS, assert_bitexact, golden, ls_grid, mac_grid
+from tests.golden.make_golden import BC_TRIALS
+from tests.helpers import GRIDS, assert_bitexact, bc_fixture, golden, ls_grid, mac_grid
 
 O = Oracle()
 
@@ -173,6 +174,30 @@ def test_laplace_known_answer():
     err = np.abs(O.scatter(g, x)[3:-3, 3:-3] - ex)
     # second-order interior error; the top corners carry the data's jump
     assert err[:, : ny // 2].max() < 1e-3 and err.max() < 0.05
+
+
+@pytest.mark.parametrize("name", list(GRIDS))
+def test_ntk_golden(name):
+    """UpdateNTK (src/mac2d.cpp:124-219): unit normal where the ENO gradient
+    has unit length to 1e-4, other cells left as they were."""
+    G = golden()
+    g = mac_grid(name)
+    for case in ("sdf", "plane"):
+        k = lambda s: G[f"{name}M_ntk_{case}_{s}"]
+        n0, n1 = O.ntk(g, k("phi"), np.full(g.shape, 7.0), np.full(g.shape, -7.0))
+        assert_bitexact(n0, k("nx"), f"UpdateNTK x, {case}")
+        assert_bitexact(n1, k("ny"), f"UpdateNTK y, {case}")
+
+
+@pytest.mark.parametrize("trial", range(BC_TRIALS))
+def test_boundary_fills_golden(trial):
+    """ApplyBC_{U,V,P}_2D for every kind on every side (periodic, neumann,
+    dirichlet, axisym, wall, inlet, outlet; pressure and lsfree on the P
+    grid), src/bc2d.cpp:123-934, against the reference's own fills."""
+    g, k = bc_fixture(trial)
+    for kind in ("U", "V", "P"):
+        got = O.bc(g, kind, k(f"{kind}_in").copy())
+        assert_bitexact(got, k(f"{kind}_out"), f"{kind} fill {g.bc_u, g.bc_v, g.bc_p}")
 
 
 @pytest.mark.skipif(not have_reference(), reason="reference build (oracle/_ref) not present")
