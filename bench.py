@@ -66,6 +66,15 @@ def metric_name():
         return json.load(f)["metric"]
 
 
+def headline_config(n, world):
+    """The workload of the headline line, the same for both arms."""
+    return {"workload": f"GFM pressure solve (assembly + solve) of a {n}x{n} two-phase droplet (rho ratio 1000, "
+                        f"mu ratio 100, sigma 0.0728, no-slip walls) after {PREP_STEPS} full steps, solved to "
+                        f"rel. residual {TOL:g}",
+            "grid": [n, n], "tol": TOL, "l2": "flushed (256 MB device write) between timed GPU steps",
+            "parallelism": "replicas" if world > 1 else "none"}
+
+
 # ---------------------------------------------------------------- clocks --
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
@@ -218,6 +227,95 @@ def level_set_rates(sh, stream, flush, peak):
     out["grid"] = [LS_MIXED_GRID, LS_MIXED_GRID]
     out["l2"] = "flushed (256 MB write) before each timed step"
     return out
+
+
+STENCIL_GRID = 2048          # momentum / assembly rooflines: every array (32 MB FP64) above L2
+MOM_BYTES_PER_CELL = 192     # 3 RK stages x (read u, v, phi, HS, u^n, v^n; write u, v) = 24 FP64 streams
+ASM_BYTES_PER_UNKNOWN = 64   # read phi, kappa, H, div; write diag, ce, cn, rhs = 8 FP64 streams
+
+
+def stencil_rooflines(sh, stream, flush, peak, n=STENCIL_GRID, reps=10):
+    """The momentum step (GetIntermediateVel: three RK3 stages of convection
+    + viscosity + gravity, k_mom_stage) and the GFM assembly (k_assemble) on
+    an n x n droplet with a smooth random velocity field: CUDA-event time per
+    call with L2 flushed before each, algorithmic GB/s against the HBM peak."""
+    import torch
+    from asd2_b200 import api
+    from asd2_b200 import workloads as W
+    c = W.droplet(n, seed=0)
+    rng = np.random.default_rng(0)
+    out = {}
+    with api.Session(api.Params.from_case(c), stream=sh) as ss:
+        ss.upload("ls", c.ls)
+        ss.upload("u", W.smooth_field(n, n, rng, amplitude=0.05))
+        ss.upload("v", W.smooth_field(n, n, rng, amplitude=0.05))
+        ss.apply_bc("ls", "P")
+        ss.apply_bc("u", "U")
+        ss.apply_bc("v", "V")
+        ss.heaviside()
+        ss.kappa()
+        ss.upload("div", W.smooth_field(n, n, rng))
+        dt = 1e-5
+
+        def timed(fn):
+            ts = []
+            for k in range(reps + 3):
+                with torch.cuda.stream(stream):
+                    flush.fill_(1.0)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                fn()
+                e1.record(stream)
+                e1.synchronize()
+                if k >= 3:
+                    ts.append(e0.elapsed_time(e1) / 1e3)
+            return float(np.median(ts))
+        t_mom = timed(lambda: ss.intermediate_vel(dt, "HS"))
+        t_asm = timed(lambda: ss.assemble_gfm(dt, recompute_kappa=False))
+    N = n * n
+    for name, t, b, what in (("momentum", t_mom, MOM_BYTES_PER_CELL, "3 x k_mom_stage + U/V ghost fills"),
+                             ("gfm_assembly", t_asm, ASM_BYTES_PER_UNKNOWN, "k_assemble")):
+        gbs = b * N / t / 1e9
+        out[name] = {"ms": t * 1e3, "kernels": what, "bytes_per_cell": b, "achieved_gbs": gbs,
+                     "frac_of_measured_hbm": gbs / peak, "mcells_per_s": N / t / 1e6}
+    return {"grid": [n, n], "l2": "flushed (256 MB write) before each timed call", **out}
+
+
+def ls_cpu_baseline(budget_s=8.0):
+    """The reference's own level-set step (Solve_LevelSet_2D + Reinit_MinRK2_2D
+    with the Sussman constraint, compiled unmodified in oracle/_ref) on the
+    128^2 perturbed circle, one core, for a bounded number of steps; the C
+    restatement when the reference build is absent."""
+    from asd2_b200 import workloads as W
+    from oracle.pyoracle import GridSpec, Oracle, Reference, have_reference
+    lc = W.perturbed_circle(LS_GRID, seed=0)
+    g = GridSpec(lc.nx, lc.ny, lc.dx, lc.dy, bc_u=lc.bc_u, bc_v=lc.bc_v, bc_p=lc.bc_p)
+    a = lc.ls.copy()
+    if have_reference():
+        R, kind = Reference(g), "reference"
+
+        def step():
+            R.ls_advect(a, lc.u, lc.v, lc.dt)
+            R.reinit(4, a)
+    else:
+        O, kind = Oracle(), "port"
+
+        def step():
+            O.ls_advect(g, a, lc.u, lc.v, lc.dt)
+            O.reinit(g, 4, a)
+    t0 = time.perf_counter()
+    n = 0
+    while n < 3 or time.perf_counter() - t0 < budget_s:
+        step()
+        n += 1
+        if n >= lc.steps:
+            break
+    t = time.perf_counter() - t0
+    return {"value": lc.nx * lc.ny * n / t / 1e6, "unit": "Mcells/s", "cores": 1, "kind": kind,
+            "sample": f"{n} level-set steps (WENO5/TVD-RK3 + 5 MinRK2 pseudo-steps with the Sussman constraint) "
+                      f"of the {lc.nx}x{lc.ny} perturbed circle in {t:.1f} s"
+                      + (", oracle/_ref (the reference's sources compiled unmodified, -O2)" if kind == "reference"
+                         else ", oracle/asd2_oracle.c -O2")}
 
 
 def mixed_precision_errors(sh):
@@ -385,7 +483,7 @@ def batched_solves(sh, stream, flush, count=BATCH_COUNT):
             "l2": "flushed (256 MB write) before each timed batch / system"}
 
 
-def learned_pc_512(sh, stream, flush, weights=None, n=512, counts=tuple(range(1, 9))):
+def learned_pc_512(sh, stream, flush, weights=None, n=512, counts=tuple(range(1, 9)), cpu_baseline=True):
     """The learned-preconditioner evaluation: eight 512^2 GFM systems with
     1 to 8 droplets (radius [0.05, 0.15], density ratio log-uniform in
     [1, 1000]), each taken after one full FP64 droplet step from rest (gravity
@@ -416,7 +514,7 @@ def learned_pc_512(sh, stream, flush, weights=None, n=512, counts=tuple(range(1,
         e1.synchronize()
         return r, e0.elapsed_time(e1) / 1e3
 
-    rows, tot = [], {"unet": 0.0, "cg": 0.0, "mg": 0.0}
+    rows, tot, snaps = [], {"unet": 0.0, "cg": 0.0, "mg": 0.0}, []
     for count in counts:
         ratio = float(10 ** rng.uniform(0.0, 3.0))
         c = W.multi_droplet(n, seed=int(rng.integers(1 << 30)), count=count, rho_ratio=ratio)
@@ -453,8 +551,12 @@ def learned_pc_512(sh, stream, flush, weights=None, n=512, counts=tuple(range(1,
                                                       / np.abs(p_ref[inner]).max())
             out["ref_resid"] = ref["resid"]
             rows.append(out)
+            snaps.append(dict(grid=dict(nx=c.nx, ny=c.ny, dx=c.dx, dy=c.dy, bc_u=c.bc_u, bc_v=c.bc_v, bc_p=c.bc_p),
+                              fluid=dict(c.fluid), dt=dt, budget_s=0.0, max_solves=1,
+                              **{kk: ss.download(kk) for kk in ("ls", "H", "div", "kappa")}))
     k = len(rows)
     net.close()
+    cpu = learned_cpu_baseline(snaps) if cpu_baseline else None
     return {"workload": f"{k} GFM systems of {n}x{n} with 1..{max(counts)} droplets (radius [0.05, 0.15], density "
                         "ratio log-U[1, 1000]) after one full FP64 step from rest; assembly + solve to rel. residual "
                         f"{TOL:g}",
@@ -467,6 +569,7 @@ def learned_pc_512(sh, stream, flush, weights=None, n=512, counts=tuple(range(1,
             "fallbacks": int(sum(r["unet"]["fallback"] for r in rows)),
             "max_true_rel_residual": float(max(r["unet"]["true_rel_residual"] for r in rows)),
             "max_p_rel_err": float(max(r["unet"]["p_rel_err_max"] for r in rows)),
+            "cpu_baseline": cpu,
             "training": {kk: meta.get(kk) for kk in ("samples", "epochs", "loss", "grid", "seconds_total")},
             "systems": rows, "l2": "flushed (256 MB write) before each timed solve"}
 
@@ -761,9 +864,11 @@ def run_ours(args):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     ls_rates = level_set_rates(sh, stream, flush, peak) if not args.no_extra else None
+    stencils = stencil_rooflines(sh, stream, flush, peak) if not args.no_extra else None
     batched = batched_solves(sh, stream, flush) if not args.no_extra else None
     mixed = mixed_precision_errors(sh) if not args.no_extra else None
-    learned = learned_pc_512(sh, stream, flush, args.weights) if not args.no_extra else None
+    learned = (learned_pc_512(sh, stream, flush, args.weights, cpu_baseline=rank == 0 and not args.no_cpu)
+               if not args.no_extra else None)
     bsteps = batched_steps(sh, stream) if not args.no_extra else None
     fsteps = full_steps_256(sh, stream) if not args.no_extra else None
     nlev = len(_mg_levels(args.n, args.n))
@@ -783,14 +888,9 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"GFM pressure solve of a {args.n}x{args.n} two-phase droplet (rho ratio 1000, "
-                               f"mu ratio 100, sigma 0.0728, no-slip walls) after {PREP_STEPS} full steps, solved to "
-                               f"rel. residual {TOL:g}",
-                   "grid": [args.n, args.n],
-                   "solver": "mixed precision: FP64 flexible CG + FP32 multigrid V(1,1) preconditioner "
-                             "(Galerkin 2x2 aggregation, fused red-black GS tiles)",
-                   "tol": TOL, "l2": "flushed (256 MB write) between timed steps",
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "config": headline_config(args.n, world),
+        "solver": "mixed precision: FP64 flexible CG + FP32 multigrid V(1,1) preconditioner "
+                  "(Galerkin 2x2 aggregation, fused red-black GS tiles)",
         "solver_iters_mean": it_mean,
         "fp64_cg": {"value": cg_value, "unit": "GFM Poisson solves/s", "iters_mean": float(np.mean(cg_iters)),
                     "solver": "FP64 Jacobi-PCG, one thread-block-cluster launch per solve"},
@@ -799,6 +899,7 @@ def run_ours(args):
         "ls_mcells_per_s": ls_mcells,
         "ls_config": {"workload": f"{LS_GRID}x{LS_GRID} perturbed circle, WENO5/TVD-RK3 + 5 MinRK2 subcell "
                                   "pseudo-steps with the Sussman constraint, FP64", "ms_per_step": t_ls * 1e3},
+        "ls_cpu_baseline": ls_cpu_baseline() if rank == 0 and not args.no_cpu else None,
         "roofline": {"bound": "hbm", "kernel": "MG-FCG iteration (k_fcg_a, k_fcg_b, k_mg_pre/post, k_mg_coarse)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": MG_ITER_DRAM_BYTES_256 if args.n == 256 else None,
@@ -812,6 +913,7 @@ def run_ours(args):
                              "(solve minus assembly) / iterations"},
         "batched_256": batched,
         "ls_large": ls_rates,
+        "stencils_2048": stencils,
         "mixed_precision_1024": mixed,
         "learned_pc_512": learned,
         "batched_steps_256": bsteps,
@@ -876,6 +978,23 @@ def cpu_baseline(snap, case, dt, args, procs=1, budget_s=None):
                       f"true rel. residual {tres:.1e}) in {tmax:.1f} s, oracle/asd2_oracle.c built -O2"}
 
 
+def learned_cpu_baseline(snaps):
+    """The C restatement's Jacobi-PCG (the reference's method) on the same
+    GFM systems, assembly + solve to rel. residual 1e-8, one single-threaded
+    process per system (up to the host's cores) running at the same time."""
+    import multiprocessing as mp
+    procs = max(1, min(len(snaps), os.cpu_count() or 1))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_cpu_worker, snaps)
+    span = max(r[1] for r in res)  # the processes solve at the same time; start-up is not counted
+    its = [r[2] for r in res]
+    return {"value": len(snaps) / span, "unit": "GFM Poisson solves/s", "cores": procs, "kind": "port",
+            "sample": f"the {len(snaps)} systems once each ({min(its)}-{max(its)} PCG iterations, max true rel. "
+                      f"residual {max(r[3] for r in res):.1e}), {procs} processes at once, longest {span:.1f} s; "
+                      "oracle/asd2_oracle.c -O2"}
+
+
 def run_reference(args):
     """Reference arm: CPU implementation of the same solves on all host cores."""
     from asd2_b200 import replicas as R
@@ -903,12 +1022,13 @@ def run_reference(args):
         if k >= args.warmup:
             vals.append(cb["value"])
     value = float(np.mean(vals))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     line = {"impl": "reference", "metric": metric_name(), "value": value, "unit": "GFM Poisson solves/s",
-            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"GFM pressure solve of a {args.n}x{args.n} two-phase droplet after "
-                                   f"{PREP_STEPS} full steps; Jacobi-PCG to true rel. residual {TOL:g}",
-                       "grid": [args.n, args.n]},
+            "config": headline_config(args.n, world),
+            "solver": "FP64 Jacobi-PCG (the reference's CG_2FUniformP_2D method), C restatement, one process "
+                      "per core",
             "cpu_baseline": {"value": value, "unit": "GFM Poisson solves/s", "cores": cores, "kind": "port",
                              "sample": cb["sample"] + f"; {cores} processes"},
             "e2e": {"value": value, "unit": "GFM Poisson solves/s", "h2d_bytes_per_step": 0,
@@ -932,7 +1052,7 @@ def main():
                     help="droplets of the batched sections (default 256; smaller for profiling)")
     ap.add_argument("--section", default=None,
                     choices=["ls_large", "mixed_1024", "batched", "batched_steps", "learned_pc", "unet_forward",
-                             "full_steps"],
+                             "full_steps", "stencils"],
                     help="run only this report (its JSON object on stdout), e.g. to profile it")
     args = ap.parse_args()
     if args.section:
@@ -959,6 +1079,16 @@ def run_section(name, args):
     elif name == "batched":
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
         out = batched_solves(stream.cuda_stream, stream, flush, count=args.batch_count)
+    elif name == "stencils":
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        peak = 6650.0
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                peak = json.load(f).get("hbm_gbs", peak)
+        except Exception:
+            pass
+        out = stencil_rooflines(stream.cuda_stream, stream, flush, peak, n=args.n if args.n != N_GRID
+                                else STENCIL_GRID)
     elif name == "full_steps":
         out = full_steps_256(stream.cuda_stream, stream)
     elif name == "batched_steps":
@@ -967,7 +1097,7 @@ def run_section(name, args):
         out = unet_forward(stream.cuda_stream, stream)
     elif name == "learned_pc":
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-        out = learned_pc_512(stream.cuda_stream, stream, flush, args.weights)
+        out = learned_pc_512(stream.cuda_stream, stream, flush, args.weights, cpu_baseline=not args.no_cpu)
     else:
         out = mixed_precision_errors(stream.cuda_stream)
     print(json.dumps({"section": name, **out}), flush=True)
