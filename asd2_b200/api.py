@@ -31,6 +31,7 @@ REINIT_ORIGINAL, REINIT_SUSSMAN, REINIT_MINRK2, REINIT_FIRSTTIME, REINIT_MINRK2_
 PCG, PCG_REFERENCE, BICGSTAB, BICGSTAB_REFERENCE, MGPCG, UNET = range(6)
 NOT_CONVERGED = 1
 FLAG_NO_CLUSTER_PCG = 1
+FLAG_NO_PERSIST_MG = 2
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "unsupported",
           -5: "non-finite value", -6: "Krylov breakdown", -7: "checkpoint I/O"}
@@ -73,6 +74,7 @@ EXPORTS = [
     "asd2g_unet_get_params", "asd2g_unet_get_grads", "asd2g_unet_forward", "asd2g_unet_train_step",
     "asd2g_unet_train_step_residual", "asd2g_unet_train_step_energy",
     "asd2g_unet_error_flag", "asd2g_unet_set_stream", "asd2g_set_preconditioner_net", "asd2g_last_fallback",
+    "asd2g_last_solve_one_launch",
     "asd2g_pc_training_pair", "asd2g_pc_training_pair_at",
 ]
 
@@ -151,6 +153,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
                                          I),
         "asd2g_unet_error_flag": ([S, C.POINTER(I)], I), "asd2g_unet_set_stream": ([S, C.c_void_p], I),
         "asd2g_set_preconditioner_net": ([S, S], I), "asd2g_last_fallback": ([S, C.POINTER(I)], I),
+        "asd2g_last_solve_one_launch": ([S, C.POINTER(I)], I),
         "asd2g_pc_training_pair": ([S, C.c_void_p, C.c_void_p], I),
         "asd2g_pc_training_pair_at": ([S, I, C.c_void_p, C.c_void_p], I),
     }
@@ -410,6 +413,12 @@ class Session:
     def set_preconditioner_net(self, net):
         self._check(self.L.asd2g_set_preconditioner_net(self.h, net.h if net is not None else None))
         self._pc_net = net  # the session refers to it: keep it alive while attached
+
+    def last_solve_one_launch(self) -> bool:
+        """True when the last pressure solve ran as one kernel launch."""
+        f = C.c_int()
+        self._check(self.L.asd2g_last_solve_one_launch(self.h, C.byref(f)))
+        return bool(f.value)
 
     def last_fallback(self) -> int:
         f = C.c_int()

@@ -33,6 +33,7 @@ UNITS = {
     "pcg_static.cu": ["-fmad=false"],
     "pcg_cluster.cu": ["-fmad=false"],
     "mg.cu": [],
+    "mg_persist.cu": [],
     "levelset32.cu": [],
     "weno32.cu": [],
     "batch.cu": [],

@@ -234,11 +234,13 @@ struct asd2g_session {
     float *pc_feats = nullptr, *pc_out = nullptr, *pc_scal = nullptr;
     FmDirs fm{};  // direction slots of the learned solver's truncated flexible CG
     int last_fallback = 0;
+    int last_one_launch = 0;  // the last pressure solve ran as one kernel launch
     // multigrid preconditioner (allocated on first use)
     MgLevel lv[MG_MAX_LEVELS] = {};
     int nlev = 0;
     double *coarse_inv = nullptr, *z = nullptr;
     double *mg_partial = nullptr;  // per-tile partial sums of the V-cycle's fused dots
+    unsigned *mgp_bar = nullptr;   // grid-barrier words of the one-launch MG-FCG solve
     Ls32Work w32{};                // FP32 level-set work arrays (precision = mixed)
     double last_volume[2] = {0.0, 0.0};  // volume check of the last droplet step (sharp, smoothed)
     int64_t mg_partial_n = 0;
@@ -305,6 +307,14 @@ int mg_alloc(asd2g_session *s) {
     if (rc == ASD2G_OK) rc = dalloc(s, &s->z, s->N);
     const int64_t np = mg_partial_len(s->g.nx, s->g.ny);
     if (rc == ASD2G_OK) rc = dalloc(s, &s->mg_partial, (size_t)np);
+    if (rc == ASD2G_OK) {
+        if (cudaMalloc(&s->mgp_bar, 4 * sizeof(unsigned)) != cudaSuccess) {
+            cudaGetLastError();
+            rc = fail(ASD2G_E_NOMEM, "grid-barrier words");
+        } else {
+            s->allocs.push_back(s->mgp_bar);
+        }
+    }
     if (rc) return rc;
     s->mg_partial_n = np;
     if (!mg_cta_prepare(s->lv, n)) return fail(ASD2G_E_UNSUPPORTED, "multigrid coarse cycle does not fit a CTA");
@@ -871,9 +881,11 @@ static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters
     const int mode = solver;  // 0 PCG, 1 PCG (reference), 2 BiCGStab, 3 BiCGStab (reference), 4 MG-FCG
     const double reg = solver == 1 ? 1.0e-12 : 0.0;  // err_tol^2 in alpha (poisson2d.cpp:354)
     launch_set_kstate(s->ks, tol, maxit, mode, reg, s->st);
+    s->last_one_launch = 0;
     if (solver == 0 && !(s->prm.solver_flags & ASD2G_FLAG_NO_CLUSTER_PCG) &&
         launch_pcg_cluster(g.nx, g.ny, s->sys, s->x, s->ks, tol, maxit, s->st)) {
         // one launch ran the whole solve
+        s->last_one_launch = 1;
         if (stream_capturing(s)) {
             if (iters) *iters = -1;
             if (resid) *resid = -1.0;
@@ -892,6 +904,30 @@ static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters
     if (solver == ASD2G_SOLVER_MGPCG) {
         int rc0 = mg_alloc(s);
         if (rc0) return rc0;
+        // systems up to about 256^2: the whole solve as one cooperative launch
+        if (mg_persist_enabled() && !(s->prm.solver_flags & ASD2G_FLAG_NO_PERSIST_MG) &&
+            launch_mg_persist(s->sys, g.nx, g.ny, s->lv, s->nlev, s->x, s->r, s->q, s->pa, s->pb, s->z, s->coarse_inv,
+                              s->mg_partial, s->mg_partial_n, s->mgp_bar, s->ks, tol, maxit, mg_omega_value(),
+                              s->st)) {
+            if (stream_capturing(s)) {
+                if (iters) *iters = -1;
+                if (resid) *resid = -1.0;
+                return cuda_check("one-launch MG-FCG");
+            }
+            cudaMemcpyAsync(s->ks_host, s->ks, sizeof(KState), cudaMemcpyDeviceToHost, s->st);
+            int rc2 = sync(s);
+            if (rc2) return rc2;
+            const KState &k = *s->ks_host;
+            if (k.status != -8) {  // -8: a grid-barrier wait gave up; solve again below
+                s->last_one_launch = 1;
+                if (iters) *iters = k.it;
+                if (resid) *resid = k.res;
+                if (k.status == -5) return fail(ASD2G_E_NONFINITE, "non-finite residual at iteration %d", k.it);
+                if (k.status == -6) return fail(ASD2G_E_BREAKDOWN, "Krylov breakdown at iteration %d", k.it);
+                return (!(k.res > tol) || k.status == 2) ? ASD2G_OK : ASD2G_NOT_CONVERGED;
+            }
+            launch_set_kstate(s->ks, tol, maxit, mode, reg, s->st);
+        }
         launch_mg_setup(s->sys, s->lv, s->nlev, s->coarse_inv, s->st);
         if (!launch_fcg_init(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->pa, s->q, s->z,
                              s->ks, s->mg_partial, s->mg_partial_n, s->st))
@@ -1003,6 +1039,7 @@ static int fm_alloc(asd2g_session *s) {
 static int solve_learned(asd2g_session *s, double tol, int maxit, int *iters, double *resid) {
     NvtxRange nv("pressure solve (learned preconditioner)");
     const Grid &g = s->g;
+    s->last_one_launch = 0;
     if (!s->pc_net) return fail(ASD2G_E_ARG, "no preconditioner network attached (asd2g_set_preconditioner_net)");
     int rc = mg_alloc(s);
     if (!rc) rc = fm_alloc(s);
@@ -1083,6 +1120,12 @@ int asd2g_set_preconditioner_net(asd2g_session *s, asd2g_unet *net) {
         cudaGraphExecDestroy(s->chunk_exec[ASD2G_SOLVER_UNET]);
         s->chunk_exec[ASD2G_SOLVER_UNET] = nullptr;
     }
+    return ASD2G_OK;
+}
+
+int asd2g_last_solve_one_launch(asd2g_session *s, int *one_launch) {
+    if (!s || !one_launch) return fail(ASD2G_E_ARG, "null argument");
+    *one_launch = s->last_one_launch;
     return ASD2G_OK;
 }
 

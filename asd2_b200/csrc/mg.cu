@@ -1230,6 +1230,8 @@ static float mg_omega() {
     return w;
 }
 
+float mg_omega_value() { return mg_omega(); }
+
 // Launch with programmatic stream serialisation (see pdl_enter); ASD2G_PDL=0
 // in the environment launches plainly (for comparisons).
 static bool pdl_enabled() {

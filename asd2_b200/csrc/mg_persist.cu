@@ -1,0 +1,917 @@
+// The whole multigrid-preconditioned flexible CG solve in ONE launch.
+//
+// Same method as the multi-kernel MG-FCG in mg.cu (FP64 flexible CG with
+// Polak-Ribiere beta and FP64 residual replacement; preconditioner one FP32
+// V(1,1)-cycle of Galerkin 2x2 aggregation with red-black Gauss-Seidel,
+// over-relaxed prolongation and an exact coarsest solve), run by a
+// cooperative grid of one CTA per 16 x 32 tile of the system with grid
+// barriers between the phases that exchange data.
+//
+// Why: at 256^2 every multi-kernel phase is latency-bound (7 dependent
+// launches of 7-11 us per iteration: launch gap, dependent L2 loads of the
+// tile, grid reduction, the one-SM coarse cycle).  Here each CTA keeps its
+// tile's state resident (level-0 FP32 operator on the tile + 2 halo, the
+// level-1 operator on its level-1 tile + 5, every level from 2 down in full)
+// and an iteration has four grid barriers:
+//
+//   A   p = z + beta p_old and q = A p on the tile + halo (FP64) -> p.q
+//   --- barrier 1: alpha
+//   B   r = r_old - alpha q on the tile + 2 (recomputed from the neighbours'
+//       q, which each CTA computed itself), x += alpha p, r.r; level-0
+//       pre-smoothing (red on the tile + 2, black on the tile + 1), residual,
+//       restriction into level 1
+//   --- barrier 2: convergence (FP64 residual replacement when met)
+//   D   level-1 pre-smoothing on the level-1 tile + 5 (red on +5, black on
+//       +4, so the pre-smoothed level-1 correction is right on +4 without a
+//       barrier), residual, restriction into level 2
+//   --- barrier 3: level-2 right-hand side complete
+//   E   every CTA gathers the level-2 right-hand side and runs levels 2..
+//       itself (redundantly: no barrier needed to share the result), then
+//       the level-1 post-smoothing on its tile + 1 and the level-0
+//       post-smoothing on its tile (the neighbours' pre-smoothed level-0
+//       correction read from global memory) -> z, z.r, z.q
+//   --- barrier 4: beta
+//
+// A value a CTA computes for a neighbour's cell (halo recomputation) uses the
+// same inputs and the same code as the owner's, so it is the owner's value.
+// Reductions: every CTA writes its block sum to a slot; after the barrier
+// every CTA adds the slots in the same fixed order, so all CTAs hold the same
+// scalars and take the same branches.  Data written by other CTAs during the
+// launch is read with L2-only loads (ld.global.cg); the system itself is
+// read-only for the launch.
+//
+// The grid barrier is a monotonic arrival counter (zeroed before the launch)
+// with a bounded wait: after SPIN_LIMIT polls a CTA sets the error word and
+// returns, every other CTA stops at its next barrier, the solve reports
+// status -8 and the host solves the system with the multi-kernel path.
+// The launch is cooperative (all CTAs co-resident) or is not made at all.
+#include <cstdint>
+#include <cstdlib>
+
+#include "asd2g.h"
+#include "mg.cuh"
+
+namespace asd2g {
+namespace {
+
+constexpr int PTI = 16, PTJ = 32;                      // level-0 tile (rows i x columns j)
+constexpr int NT = PTI * PTJ;                          // threads: one per tile cell
+constexpr int H3I = PTI + 6, H3J = PTJ + 6;            // tile + 3
+constexpr int H2I = PTI + 4, H2J = PTJ + 4;            // tile + 2
+constexpr int C1I = PTI / 2, C1J = PTJ / 2;            // level-1 cells under a tile
+constexpr int R1 = 5;                                  // level-1 halo kept by a CTA
+constexpr int R1I = C1I + 2 * R1, R1J = C1J + 2 * R1;  // 18 x 26
+constexpr int C2I = PTI / 4, C2J = PTJ / 4;            // level-2 cells under a tile
+constexpr int CMAX = 5440;                             // cells of levels 2.. (64^2 + 32^2 + 16^2 + 8^2)
+constexpr int NINV = MG_COARSE_CELLS;                  // coarsest level <= 64 cells
+constexpr unsigned SPIN_LIMIT = 1u << 22;              // polls before a barrier wait gives up
+constexpr int STATUS_BARRIER = -8;                     // KState.status when a barrier wait gave up
+
+struct Smem {
+    double p[H3I][H3J];        // direction on the tile + 3
+    double q[H2I][H2J];        // A p on the tile + 2
+    double r[H2I][H2J];        // residual on the tile + 2
+    double inv[NINV * NINV];   // coarsest inverse (row-major, stride NINV)
+    double red[4][NT / 32];    // per-warp partial sums
+    double tot[4];             // reduced sums (the same in every CTA)
+    float d0[H2I][H2J], ce0[H2I][H2J], cn0[H2I][H2J], f0[H2I][H2J], e0[H2I][H2J];  // level 0, tile + 2
+    float res0[PTI][PTJ];
+    float d1[R1I][R1J], ce1[R1I][R1J], cn1[R1I][R1J], f1[R1I][R1J], e1[R1I][R1J];  // level 1, tile + 5
+    float res1[C1I][C1J];
+    float co[5 * CMAX];        // levels 2..: d, ce, cn, f, e of each level
+    int flag;
+};
+
+struct PArgs {
+    int nx, ny, ntj, ncta, nlev;
+    int dims[2 * MG_MAX_LEVELS];
+    int off[MG_MAX_LEVELS];  // offset (floats) of level l >= 2 in Smem::co
+    Sys S;
+    double *x, *rbuf0, *rbuf1, *pbuf0, *pbuf1, *z;
+    float *e0g;                          // level-0 pre-smoothed correction
+    float *d1g, *ce1g, *cn1g, *f1g;      // level-1 operator and right-hand side
+    float *d2g, *ce2g, *cn2g, *f2g;      // level-2 operator and right-hand side
+    double *inv;                         // coarsest inverse (written by CTA 0)
+    double *partial;                     // 4 slots per CTA
+    unsigned *bar;                       // [0] arrivals, [1] error word
+    KState *ks;
+    double tol;
+    int maxit;
+    float omega;
+};
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid barrier; false when the wait gave up (or another CTA's did).
+__device__ bool gsync(const PArgs &A, Smem &sm, unsigned &epoch) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        epoch++;
+        __threadfence();
+        atomicAdd(A.bar, 1u);
+        const unsigned target = epoch * (unsigned)A.ncta;
+        int good = 1;
+        for (unsigned n = 0; ld_acquire(A.bar) < target; n++) {
+            if (n > SPIN_LIMIT || *(volatile unsigned *)(A.bar + 1)) {
+                atomicExch(A.bar + 1, 1u);
+                good = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+        sm.flag = good;
+    }
+    __syncthreads();
+    return sm.flag != 0;
+}
+
+// Block sums of NV values into this CTA's slots (read after the next barrier).
+template <int NV> __device__ void put_partial(const PArgs &A, Smem &sm, double (&v)[NV]) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; q++) {
+        double s = v[q];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) sm.red[q][wid] = s;
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; q++) {
+            double s = lane < NT / 32 ? sm.red[q][lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+            if (lane == 0) __stcg(A.partial + 4 * blockIdx.x + q, s);
+        }
+    }
+}
+
+// Sum of every CTA's slots, in the same order in every CTA -> sm.tot.
+template <int NV> __device__ void get_total(const PArgs &A, Smem &sm) {
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+#pragma unroll
+        for (int q = 0; q < NV; q++) {
+            double s = 0.0;
+            for (int c = lane; c < A.ncta; c += 32) s += __ldcg(A.partial + 4 * c + q);
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+            if (lane == 0) sm.tot[q] = s;
+        }
+    }
+    __syncthreads();
+}
+
+template <int W> __device__ __forceinline__ float gs(const float (*f)[W], const float (*d)[W], const float (*ce)[W],
+                                                     const float (*cn)[W], const float (*e)[W], int a, int b) {
+    const float s = f[a][b] + ce[a - 1][b] * e[a - 1][b] + ce[a][b] * e[a + 1][b] + cn[a][b - 1] * e[a][b - 1] +
+                    cn[a][b] * e[a][b + 1];
+    return s / d[a][b];
+}
+
+// Galerkin 2x2 aggregation of one coarse cell (as mg_coarsen_cell in mg.cu)
+// from a fine operator given by accessors.
+template <class FD, class FE, class FN>
+__device__ __forceinline__ void coarsen_cell(int fnx, int fny, int I, int J, FD fd, FE fe, FN fn, float &cd,
+                                             float &cce, float &ccn) {
+    const int i0 = 2 * I, j0 = 2 * J;
+    const bool hi = i0 + 1 < fnx, hj = j0 + 1 < fny;
+    float d = fd(i0, j0);
+    if (hi) d += fd(i0 + 1, j0);
+    if (hj) d += fd(i0, j0 + 1);
+    if (hi && hj) d += fd(i0 + 1, j0 + 1);
+    float inner = 0.0f;
+    if (hi) inner += fe(i0, j0);
+    if (hi && hj) inner += fe(i0, j0 + 1);
+    if (hj) inner += fn(i0, j0);
+    if (hi && hj) inner += fn(i0 + 1, j0);
+    cd = d - 2.0f * inner;
+    const int ie = hi ? i0 + 1 : i0, je = hj ? j0 + 1 : j0;
+    float ce = fe(ie, j0);
+    if (hj) ce += fe(ie, j0 + 1);
+    float cn = fn(i0, je);
+    if (hi) cn += fn(i0 + 1, je);
+    cce = ce;
+    ccn = cn;
+}
+
+// ---------------------------------------------------------------- level 0 --
+// Pre-smoothing of level 0 from the FP64 residual on the tile + 2 (sm.r):
+// red on +2 from zero, black on +1, residual on the tile; stores e0 (tile)
+// and the restricted residual of the tile's level-1 cells.
+__device__ void l0_pre(const PArgs &A, Smem &sm, int i0, int j0) {
+    const int tid = threadIdx.x, nx = A.nx, ny = A.ny;
+    for (int t = tid; t < H2I * H2J; t += NT) {
+        const int a = t / H2J, b = t % H2J, i = i0 - 2 + a, j = j0 - 2 + b;
+        const float f = (float)sm.r[a][b];
+        sm.f0[a][b] = f;
+        sm.e0[a][b] = (((i + j) & 1) == 0) ? f / sm.d0[a][b] : 0.0f;
+    }
+    __syncthreads();
+    for (int t = tid; t < (H2I - 2) * (H2J - 2); t += NT) {
+        const int a = 1 + t / (H2J - 2), b = 1 + t % (H2J - 2), i = i0 - 2 + a, j = j0 - 2 + b;
+        if (((i + j) & 1) == 1) sm.e0[a][b] = gs<H2J>(sm.f0, sm.d0, sm.ce0, sm.cn0, sm.e0, a, b);
+    }
+    __syncthreads();
+    {
+        const int ta = tid / PTJ, tb = tid % PTJ, a = 2 + ta, b = 2 + tb, i = i0 + ta, j = j0 + tb;
+        float rr = 0.0f;
+        if (i < nx && j < ny) {
+            const float Ae = sm.d0[a][b] * sm.e0[a][b] - sm.ce0[a - 1][b] * sm.e0[a - 1][b] -
+                             sm.ce0[a][b] * sm.e0[a + 1][b] - sm.cn0[a][b - 1] * sm.e0[a][b - 1] -
+                             sm.cn0[a][b] * sm.e0[a][b + 1];
+            rr = sm.f0[a][b] - Ae;
+            __stcg(A.e0g + (int64_t)j + (int64_t)ny * i, sm.e0[a][b]);
+        }
+        sm.res0[ta][tb] = rr;
+    }
+    __syncthreads();
+    if (tid < C1I * C1J) {
+        const int ci = tid / C1J, cj = tid % C1J, I = i0 / 2 + ci, J = j0 / 2 + cj;
+        const int n1x = A.dims[2], n1y = A.dims[3];
+        if (I < n1x && J < n1y)
+            __stcg(A.f1g + (int64_t)J + (int64_t)n1y * I, sm.res0[2 * ci][2 * cj] + sm.res0[2 * ci + 1][2 * cj] +
+                                                            sm.res0[2 * ci][2 * cj + 1] +
+                                                            sm.res0[2 * ci + 1][2 * cj + 1]);
+    }
+}
+
+// ---------------------------------------------------------------- level 1 --
+// Pre-smoothing of level 1 on the level-1 tile + 5 (red on +5, black on +4),
+// residual on the level-1 tile, restriction into the tile's level-2 cells.
+__device__ void l1_pre(const PArgs &A, Smem &sm, int I0, int J0) {
+    const int tid = threadIdx.x, n1x = A.dims[2], n1y = A.dims[3];
+    for (int t = tid; t < R1I * R1J; t += NT) {
+        const int a = t / R1J, b = t % R1J, I = I0 - R1 + a, J = J0 - R1 + b;
+        const bool in = I >= 0 && I < n1x && J >= 0 && J < n1y;
+        const float f = in ? __ldcg(A.f1g + (int64_t)J + (int64_t)n1y * I) : 0.0f;
+        sm.f1[a][b] = f;
+        sm.e1[a][b] = (((I + J) & 1) == 0) ? f / sm.d1[a][b] : 0.0f;
+    }
+    __syncthreads();
+    for (int t = tid; t < (R1I - 2) * (R1J - 2); t += NT) {
+        const int a = 1 + t / (R1J - 2), b = 1 + t % (R1J - 2), I = I0 - R1 + a, J = J0 - R1 + b;
+        if (((I + J) & 1) == 1) sm.e1[a][b] = gs<R1J>(sm.f1, sm.d1, sm.ce1, sm.cn1, sm.e1, a, b);
+    }
+    __syncthreads();
+    if (tid < C1I * C1J) {
+        const int ta = tid / C1J, tb = tid % C1J, a = R1 + ta, b = R1 + tb, I = I0 + ta, J = J0 + tb;
+        float rr = 0.0f;
+        if (I < n1x && J < n1y) {
+            const float Ae = sm.d1[a][b] * sm.e1[a][b] - sm.ce1[a - 1][b] * sm.e1[a - 1][b] -
+                             sm.ce1[a][b] * sm.e1[a + 1][b] - sm.cn1[a][b - 1] * sm.e1[a][b - 1] -
+                             sm.cn1[a][b] * sm.e1[a][b + 1];
+            rr = sm.f1[a][b] - Ae;
+        }
+        sm.res1[ta][tb] = rr;
+    }
+    __syncthreads();
+    if (tid < C2I * C2J) {
+        const int ci = tid / C2J, cj = tid % C2J, I = I0 / 2 + ci, J = J0 / 2 + cj;
+        const int n2x = A.dims[4], n2y = A.dims[5];
+        if (I < n2x && J < n2y)
+            __stcg(A.f2g + (int64_t)J + (int64_t)n2y * I, sm.res1[2 * ci][2 * cj] + sm.res1[2 * ci + 1][2 * cj] +
+                                                            sm.res1[2 * ci][2 * cj + 1] +
+                                                            sm.res1[2 * ci + 1][2 * cj + 1]);
+    }
+}
+
+// ------------------------------------------------------ levels 2 .. nlev-1 --
+// The coarse part of the V-cycle on the full levels held by this CTA (the
+// same sweeps as k_mg_cta_cycle in mg.cu): f of level 2 must be in place;
+// leaves the corrected, post-smoothed level-2 correction in its e.
+__device__ void coarse_cycle(const PArgs &A, Smem &sm) {
+    const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;  // 16 rows x 32 columns of threads
+    constexpr int RS = NT / 32;
+    const int nlev = A.nlev;
+    const float omega = A.omega;
+    for (int l = 2; l < nlev - 1; l++) {
+        const int nx = A.dims[2 * l], ny = A.dims[2 * l + 1], n = nx * ny;
+        const float *D = sm.co + A.off[l], *CE = D + n, *CN = CE + n, *F = CN + n;
+        float *E = sm.co + A.off[l] + 4 * n;
+        for (int i = ty; i < nx; i += RS)
+            for (int j = tx; j < ny; j += 32) {
+                const int k = j + ny * i;
+                if (((i + j) & 1) == 0) {
+                    E[k] = F[k] / D[k];
+                } else {
+                    float acc = F[k];
+                    if (i > 0) acc += CE[k - ny] * (F[k - ny] / D[k - ny]);
+                    if (i < nx - 1) acc += CE[k] * (F[k + ny] / D[k + ny]);
+                    if (j > 0) acc += CN[k - 1] * (F[k - 1] / D[k - 1]);
+                    if (j < ny - 1) acc += CN[k] * (F[k + 1] / D[k + 1]);
+                    E[k] = acc / D[k];
+                }
+            }
+        __syncthreads();
+        const int cnx = A.dims[2 * l + 2], cny = A.dims[2 * l + 3];
+        float *Fc = sm.co + A.off[l + 1] + 3 * cnx * cny;
+        for (int I = ty; I < cnx; I += RS)
+            for (int J = tx; J < cny; J += 32) {
+                float sum = 0.0f;
+#pragma unroll
+                for (int a = 0; a < 2; a++)
+#pragma unroll
+                    for (int b = 0; b < 2; b++) {
+                        const int i = 2 * I + a, j = 2 * J + b;
+                        if (i >= nx || j >= ny) continue;
+                        const int k = j + ny * i;
+                        float Ae = D[k] * E[k];
+                        if (i > 0) Ae -= CE[k - ny] * E[k - ny];
+                        if (i < nx - 1) Ae -= CE[k] * E[k + ny];
+                        if (j > 0) Ae -= CN[k - 1] * E[k - 1];
+                        if (j < ny - 1) Ae -= CN[k] * E[k + 1];
+                        sum += F[k] - Ae;
+                    }
+                Fc[J + cny * I] = sum;
+            }
+        __syncthreads();
+    }
+    {
+        // coarsest: e = inv f, 8 lanes per row
+        const int l = nlev - 1, n = A.dims[2 * l] * A.dims[2 * l + 1];
+        const float *F = sm.co + A.off[l] + 3 * n;
+        float *E = sm.co + A.off[l] + 4 * n;
+        const int row = tid >> 3, c = tid & 7;
+        double acc = 0.0;
+        if (row < n)
+#pragma unroll
+            for (int qq = 0; qq < NINV / 8; qq++)
+                if (c + 8 * qq < n) acc += sm.inv[row * NINV + c + 8 * qq] * (double)F[c + 8 * qq];
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, 8);
+        if (row < n && c == 0) E[row] = (float)acc;
+        __syncthreads();
+    }
+    for (int l = nlev - 2; l >= 2; l--) {
+        const int nx = A.dims[2 * l], ny = A.dims[2 * l + 1], n = nx * ny;
+        const int cny = A.dims[2 * l + 3], cn = A.dims[2 * l + 2] * cny;
+        const float *D = sm.co + A.off[l], *CE = D + n, *CN = CE + n, *F = CN + n;
+        float *E = sm.co + A.off[l] + 4 * n;
+        const float *Ec = sm.co + A.off[l + 1] + 4 * cn;
+        auto pe = [&](int k, int i, int j) { return E[k] + omega * Ec[(j >> 1) + cny * (i >> 1)]; };
+        for (int i = ty; i < nx; i += RS)
+            for (int j = 2 * tx + ((i + 1) & 1); j < ny; j += 64) {
+                const int k = j + ny * i;
+                float acc = F[k];
+                if (i > 0) acc += CE[k - ny] * pe(k - ny, i - 1, j);
+                if (i < nx - 1) acc += CE[k] * pe(k + ny, i + 1, j);
+                if (j > 0) acc += CN[k - 1] * pe(k - 1, i, j - 1);
+                if (j < ny - 1) acc += CN[k] * pe(k + 1, i, j + 1);
+                E[k] = acc / D[k];
+            }
+        __syncthreads();
+        for (int i = ty; i < nx; i += RS)
+            for (int j = 2 * tx + (i & 1); j < ny; j += 64) {
+                const int k = j + ny * i;
+                float acc = F[k];
+                if (i > 0) acc += CE[k - ny] * E[k - ny];
+                if (i < nx - 1) acc += CE[k] * E[k + ny];
+                if (j > 0) acc += CN[k - 1] * E[k - 1];
+                if (j < ny - 1) acc += CN[k] * E[k + 1];
+                E[k] = acc / D[k];
+            }
+        __syncthreads();
+    }
+}
+
+// Post-smoothing of level 1 on the level-1 tile + 1 (prolongation of the
+// level-2 correction with omega on +3, black on +2, red on +1), in sm.e1.
+__device__ void l1_post(const PArgs &A, Smem &sm, int I0, int J0) {
+    const int tid = threadIdx.x, n1x = A.dims[2], n1y = A.dims[3], n2y = A.dims[5];
+    const float *E2 = sm.co + A.off[2] + 4 * A.dims[4] * n2y;
+    for (int t = tid; t < (R1I - 4) * (R1J - 4); t += NT) {
+        const int a = 2 + t / (R1J - 4), b = 2 + t % (R1J - 4), I = I0 - R1 + a, J = J0 - R1 + b;
+        if (I >= 0 && I < n1x && J >= 0 && J < n1y) sm.e1[a][b] += A.omega * E2[(J >> 1) + n2y * (I >> 1)];
+    }
+    __syncthreads();
+    for (int t = tid; t < (R1I - 6) * (R1J - 6); t += NT) {
+        const int a = 3 + t / (R1J - 6), b = 3 + t % (R1J - 6), I = I0 - R1 + a, J = J0 - R1 + b;
+        if (((I + J) & 1) == 1 && I >= 0 && I < n1x && J >= 0 && J < n1y)
+            sm.e1[a][b] = gs<R1J>(sm.f1, sm.d1, sm.ce1, sm.cn1, sm.e1, a, b);
+    }
+    __syncthreads();
+    for (int t = tid; t < (R1I - 8) * (R1J - 8); t += NT) {
+        const int a = 4 + t / (R1J - 8), b = 4 + t % (R1J - 8), I = I0 - R1 + a, J = J0 - R1 + b;
+        if (((I + J) & 1) == 0 && I >= 0 && I < n1x && J >= 0 && J < n1y)
+            sm.e1[a][b] = gs<R1J>(sm.f1, sm.d1, sm.ce1, sm.cn1, sm.e1, a, b);
+    }
+    __syncthreads();
+}
+
+// Post-smoothing of level 0 on the tile: the neighbours' pre-smoothed e0 on
+// the tile + 2, prolongation of the level-1 correction (sm.e1 on the level-1
+// tile + 1) with omega, black on +1, red on the tile -> z (FP64; 0 at the
+// pinned cell) and the sums z.r, z.q of the tile.
+__device__ void l0_post(const PArgs &A, Smem &sm, int i0, int j0, double (&acc)[2]) {
+    const int tid = threadIdx.x, nx = A.nx, ny = A.ny, I0 = i0 / 2 - R1, J0 = j0 / 2 - R1;
+    for (int t = tid; t < H2I * H2J; t += NT) {
+        const int a = t / H2J, b = t % H2J, i = i0 - 2 + a, j = j0 - 2 + b;
+        float e = 0.0f;
+        if (i >= 0 && i < nx && j >= 0 && j < ny)
+            e = __ldcg(A.e0g + (int64_t)j + (int64_t)ny * i) + A.omega * sm.e1[(i >> 1) - I0][(j >> 1) - J0];
+        sm.e0[a][b] = e;
+    }
+    __syncthreads();
+    for (int t = tid; t < (H2I - 2) * (H2J - 2); t += NT) {
+        const int a = 1 + t / (H2J - 2), b = 1 + t % (H2J - 2), i = i0 - 2 + a, j = j0 - 2 + b;
+        if (((i + j) & 1) == 1 && i >= 0 && i < nx && j >= 0 && j < ny)
+            sm.e0[a][b] = gs<H2J>(sm.f0, sm.d0, sm.ce0, sm.cn0, sm.e0, a, b);
+    }
+    __syncthreads();
+    acc[0] = acc[1] = 0.0;
+    const int ta = tid / PTJ, tb = tid % PTJ, a = 2 + ta, b = 2 + tb, i = i0 + ta, j = j0 + tb;
+    if (i < nx && j < ny) {
+        float e = sm.e0[a][b];
+        if (((i + j) & 1) == 0) e = gs<H2J>(sm.f0, sm.d0, sm.ce0, sm.cn0, sm.e0, a, b);
+        const int64_t k = (int64_t)j + (int64_t)ny * i;
+        const double z = (A.S.pinned && k == 0) ? 0.0 : (double)e;
+        __stcg(A.z + k, z);
+        acc[0] = z * sm.r[a][b];
+        acc[1] = z * sm.q[a][b];
+    }
+}
+
+// ------------------------------------------------------------------ set-up --
+// Level-0 FP32 operator on the tile + 2 from the FP64 system; the tile's
+// level-1 and level-2 operator cells (Galerkin) written to global memory.
+__device__ void setup_local(const PArgs &A, Smem &sm, int i0, int j0) {
+    const int tid = threadIdx.x, nx = A.nx, ny = A.ny;
+    const Sys &S = A.S;
+    for (int t = tid; t < H2I * H2J; t += NT) {
+        const int a = t / H2J, b = t % H2J, i = i0 - 2 + a, j = j0 - 2 + b;
+        float d = 1.0f, ce = 0.0f, cn = 0.0f;
+        if (i >= 0 && i < nx && j >= 0 && j < ny) {
+            const int64_t k = (int64_t)j + (int64_t)ny * i;
+            const bool pin0 = S.pinned && k == 0;
+            d = (float)S.diag[k];
+            ce = (i < nx - 1 && !pin0) ? (float)S.ce[k] : 0.0f;
+            cn = (j < ny - 1 && !pin0) ? (float)S.cn[k] : 0.0f;
+        }
+        sm.d0[a][b] = d;
+        sm.ce0[a][b] = ce;
+        sm.cn0[a][b] = cn;
+    }
+    __syncthreads();
+    // level 1 of the tile (into the middle of the level-1 arrays), then level 2
+    const int n1x = A.dims[2], n1y = A.dims[3];
+    if (tid < C1I * C1J) {
+        const int ci = tid / C1J, cj = tid % C1J, I = i0 / 2 + ci, J = j0 / 2 + cj;
+        float cd = 1.0f, cce = 0.0f, ccn = 0.0f;
+        if (I < n1x && J < n1y) {
+            // fine cell (i, j) of the tile at sm index (i - i0 + 2, j - j0 + 2)
+            auto fd = [&](int i, int j) { return sm.d0[i - i0 + 2][j - j0 + 2]; };
+            auto fe = [&](int i, int j) { return sm.ce0[i - i0 + 2][j - j0 + 2]; };
+            auto fn = [&](int i, int j) { return sm.cn0[i - i0 + 2][j - j0 + 2]; };
+            coarsen_cell(nx, ny, I, J, fd, fe, fn, cd, cce, ccn);
+            const int64_t k = (int64_t)J + (int64_t)n1y * I;
+            __stcg(A.d1g + k, cd);
+            __stcg(A.ce1g + k, cce);
+            __stcg(A.cn1g + k, ccn);
+        }
+        sm.d1[R1 + ci][R1 + cj] = cd;
+        sm.ce1[R1 + ci][R1 + cj] = cce;
+        sm.cn1[R1 + ci][R1 + cj] = ccn;
+    }
+    __syncthreads();
+    const int n2x = A.dims[4], n2y = A.dims[5];
+    if (tid < C2I * C2J) {
+        const int ci = tid / C2J, cj = tid % C2J, I = i0 / 4 + ci, J = j0 / 4 + cj;
+        if (I < n2x && J < n2y) {
+            const int I0 = i0 / 2, J0 = j0 / 2;
+            auto fd = [&](int i, int j) { return sm.d1[i - I0 + R1][j - J0 + R1]; };
+            auto fe = [&](int i, int j) { return sm.ce1[i - I0 + R1][j - J0 + R1]; };
+            auto fn = [&](int i, int j) { return sm.cn1[i - I0 + R1][j - J0 + R1]; };
+            float cd, cce, ccn;
+            coarsen_cell(n1x, n1y, I, J, fd, fe, fn, cd, cce, ccn);
+            const int64_t k = (int64_t)J + (int64_t)n2y * I;
+            __stcg(A.d2g + k, cd);
+            __stcg(A.ce2g + k, cce);
+            __stcg(A.cn2g + k, ccn);
+        }
+    }
+}
+
+// After the level-1/2 operators are complete: this CTA's level-1 operator on
+// the level-1 tile + 5, the full level 2 and the coarser levels built here.
+__device__ void setup_coarse(const PArgs &A, Smem &sm, int i0, int j0) {
+    const int tid = threadIdx.x, n1x = A.dims[2], n1y = A.dims[3];
+    const int I0 = i0 / 2 - R1, J0 = j0 / 2 - R1;
+    for (int t = tid; t < R1I * R1J; t += NT) {
+        const int a = t / R1J, b = t % R1J, I = I0 + a, J = J0 + b;
+        float d = 1.0f, ce = 0.0f, cn = 0.0f;
+        if (I >= 0 && I < n1x && J >= 0 && J < n1y) {
+            const int64_t k = (int64_t)J + (int64_t)n1y * I;
+            d = __ldcg(A.d1g + k);
+            ce = __ldcg(A.ce1g + k);
+            cn = __ldcg(A.cn1g + k);
+        }
+        sm.d1[a][b] = d;
+        sm.ce1[a][b] = ce;
+        sm.cn1[a][b] = cn;
+    }
+    {
+        const int n2 = A.dims[4] * A.dims[5];
+        float *D = sm.co + A.off[2], *CE = D + n2, *CN = CE + n2;
+        for (int k = tid; k < n2; k += NT) {
+            D[k] = __ldcg(A.d2g + k);
+            CE[k] = __ldcg(A.ce2g + k);
+            CN[k] = __ldcg(A.cn2g + k);
+        }
+    }
+    __syncthreads();
+    for (int l = 3; l < A.nlev; l++) {
+        const int fnx = A.dims[2 * l - 2], fny = A.dims[2 * l - 1], fn = fnx * fny;
+        const int cnx = A.dims[2 * l], cny = A.dims[2 * l + 1], cn = cnx * cny;
+        const float *FD = sm.co + A.off[l - 1], *FE = FD + fn, *FN = FE + fn;
+        float *D = sm.co + A.off[l], *CE = D + cn, *CN = CE + cn;
+        (void)cnx;
+        for (int k = tid; k < cn; k += NT) {
+            const int I = k / cny, J = k % cny;
+            auto fd = [&](int i, int j) { return FD[j + fny * i]; };
+            auto fe = [&](int i, int j) { return FE[j + fny * i]; };
+            auto fnn = [&](int i, int j) { return FN[j + fny * i]; };
+            coarsen_cell(fnx, fny, I, J, fd, fe, fnn, D[k], CE[k], CN[k]);
+        }
+        __syncthreads();
+    }
+}
+
+// Dense inverse of the coarsest operator (SPD, <= 64 cells) by in-place
+// Gauss-Jordan without pivoting, FP64, in sm.inv; written to A.inv.  Each
+// step reads the old pivot row and column, then every entry is replaced.
+__device__ void coarsest_inverse(const PArgs &A, Smem &sm) {
+    const int tid = threadIdx.x, l = A.nlev - 1, nx = A.dims[2 * l], ny = A.dims[2 * l + 1], n = nx * ny;
+    const float *D = sm.co + A.off[l], *CE = D + n, *CN = CE + n;
+    double *M = sm.inv;
+    for (int t = tid; t < NINV * NINV; t += NT) M[t] = 0.0;
+    __syncthreads();
+    if (tid < n) {
+        const int i = tid / ny, j = tid % ny;
+        M[tid * NINV + tid] = D[tid];
+        if (i < nx - 1) M[tid * NINV + tid + ny] = M[(tid + ny) * NINV + tid] = -(double)CE[tid];
+        if (j < ny - 1) M[tid * NINV + tid + 1] = M[(tid + 1) * NINV + tid] = -(double)CN[tid];
+    }
+    __syncthreads();
+    // thread -> row tid >> 3, columns (tid & 7) + 8 m
+    const int row = tid >> 3, c0 = tid & 7;
+    for (int k = 0; k < n; k++) {
+        double nv[NINV / 8];
+        const double rp = 1.0 / M[k * NINV + k];
+        if (row < n) {
+            const double fik = M[row * NINV + k];
+#pragma unroll
+            for (int m = 0; m < NINV / 8; m++) {
+                const int c = c0 + 8 * m;
+                double v = 0.0;
+                if (c < n) {
+                    if (row == k) v = (c == k) ? rp : M[k * NINV + c] * rp;
+                    else if (c == k) v = -fik * rp;
+                    else v = M[row * NINV + c] - fik * (M[k * NINV + c] * rp);
+                }
+                nv[m] = v;
+            }
+        }
+        __syncthreads();
+        if (row < n)
+#pragma unroll
+            for (int m = 0; m < NINV / 8; m++)
+                if (c0 + 8 * m < n) M[row * NINV + c0 + 8 * m] = nv[m];
+        __syncthreads();
+    }
+    for (int t = tid; t < n * NINV; t += NT) __stcg(A.inv + t, M[t]);
+}
+
+__global__ void __launch_bounds__(NT, 1) k_mgfcg_persist(PArgs A) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    Smem &sm = *reinterpret_cast<Smem *>(smraw);
+    const int tid = threadIdx.x, nx = A.nx, ny = A.ny;
+    const int ti = blockIdx.x / A.ntj, tj = blockIdx.x % A.ntj, i0 = ti * PTI, j0 = tj * PTJ;
+    const int ta = tid / PTJ, tb = tid % PTJ, mi = i0 + ta, mj = j0 + tb;  // this thread's cell of the tile
+    const bool mine = mi < nx && mj < ny;
+    const int64_t mk = (int64_t)mj + (int64_t)ny * mi;
+    const Sys &S = A.S;
+    unsigned epoch = 0;
+    double *rcur = A.rbuf0, *rnext = A.rbuf1, *pold = A.pbuf0, *pnew = A.pbuf1;
+
+    // ---- set-up: x = 0, r = b, p = 0; operators of levels 0-2 ----
+    double xk = 0.0;
+    {
+        double v[1] = {0.0};
+        if (mine) {
+            const double bk = S.b[mk];
+            __stcg(rcur + mk, bk);
+            __stcg(pold + mk, 0.0);
+            v[0] = bk * bk;
+        }
+        setup_local(A, sm, i0, j0);
+        put_partial<1>(A, sm, v);
+    }
+    bool ok = gsync(A, sm, epoch);
+    double bn = 1.0, res = 0.0, rho = 0.0, alpha = 0.0, beta = 0.0, res_true_prev = -1.0;
+    int it = 0, status = 0, restart = 0;
+    bool done = true;
+    if (ok) {
+        get_total<1>(A, sm);
+        const double bb = sm.tot[0];
+        bn = sqrt(bb);
+        if (bn == 0.0) bn = 1.0;
+        res = sqrt(bb) / bn;
+        done = !(res > A.tol) || A.maxit <= 0;
+    }
+    if (ok && !done) {
+        setup_coarse(A, sm, i0, j0);
+        if (blockIdx.x == 0) coarsest_inverse(A, sm);
+        ok = gsync(A, sm, epoch);
+        if (ok) {
+            const int l = A.nlev - 1, n = A.dims[2 * l] * A.dims[2 * l + 1];
+            for (int t = tid; t < n * NINV; t += NT) sm.inv[t] = __ldcg(A.inv + t);
+            // the first V-cycle's right-hand side r = b on the tile + 2; q = 0
+            for (int t = tid; t < H2I * H2J; t += NT) {
+                const int a = t / H2J, b = t % H2J, i = i0 - 2 + a, j = j0 - 2 + b;
+                sm.r[a][b] = (i >= 0 && i < nx && j >= 0 && j < ny) ? __ldcg(rcur + (int64_t)j + (int64_t)ny * i)
+                                                                       : 0.0;
+                sm.q[a][b] = 0.0;
+            }
+            __syncthreads();
+            l0_pre(A, sm, i0, j0);
+            ok = gsync(A, sm, epoch);  // level-1 rhs and level-0 e of the first V-cycle complete
+        }
+    }
+    // ---- iterations: rest of the V-cycle (levels 1.., z, beta), then A, B ----
+    while (ok && !done) {
+        l1_pre(A, sm, i0 / 2, j0 / 2);
+        ok = gsync(A, sm, epoch);  // level-2 rhs complete
+        if (!ok) break;
+        {
+            const int n2 = A.dims[4] * A.dims[5];
+            float *F2 = sm.co + A.off[2] + 3 * n2;
+            for (int k = tid; k < n2; k += NT) F2[k] = __ldcg(A.f2g + k);
+            __syncthreads();
+        }
+        coarse_cycle(A, sm);
+        l1_post(A, sm, i0 / 2, j0 / 2);
+        {
+            double acc[2];
+            l0_post(A, sm, i0, j0, acc);
+            put_partial<2>(A, sm, acc);
+        }
+        ok = gsync(A, sm, epoch);  // z complete -> beta
+        if (!ok) break;
+        get_total<2>(A, sm);
+        {
+            const double zr = sm.tot[0], zq = sm.tot[1];
+            beta = (it == 0 || restart) ? 0.0 : -alpha * zq / rho;
+            restart = 0;
+            rho = zr;
+            if (!(zr > 0.0) && it == 0 && res > A.tol) {
+                status = -6;
+                break;
+            }
+        }
+        // A: p = z + beta p_old and q = A p on the tile + halo, p.q
+        for (int t = tid; t < H3I * H3J; t += NT) {
+            const int a = t / H3J, b = t % H3J, i = i0 - 3 + a, j = j0 - 3 + b;
+            double v = 0.0;
+            if (i >= 0 && i < nx && j >= 0 && j < ny) {
+                const int64_t k = (int64_t)j + (int64_t)ny * i;
+                v = __ldcg(A.z + k) + beta * __ldcg(pold + k);
+            }
+            sm.p[a][b] = v;
+        }
+        __syncthreads();
+        for (int t = tid; t < H2I * H2J; t += NT) {
+            const int a = t / H2J, b = t % H2J, i = i0 - 2 + a, j = j0 - 2 + b, ha = a + 1, hb = b + 1;
+            double y = 0.0;
+            if (i >= 0 && i < nx && j >= 0 && j < ny) {
+                const int64_t k = (int64_t)j + (int64_t)ny * i;
+                if (!(S.pinned && k == 0)) {
+                    if (j > 0) y += -__ldg(S.cn + k - 1) * sm.p[ha][hb - 1];
+                    if (i > 0) y += -__ldg(S.ce + k - ny) * sm.p[ha - 1][hb];
+                    y += __ldg(S.diag + k) * sm.p[ha][hb];
+                    if (i < nx - 1) y += -__ldg(S.ce + k) * sm.p[ha + 1][hb];
+                    if (j < ny - 1) y += -__ldg(S.cn + k) * sm.p[ha][hb + 1];
+                }
+            }
+            sm.q[a][b] = y;
+        }
+        __syncthreads();
+        {
+            double pq[1] = {0.0};
+            if (mine) {
+                __stcg(pnew + mk, sm.p[3 + ta][3 + tb]);
+                pq[0] = sm.p[3 + ta][3 + tb] * sm.q[2 + ta][2 + tb];
+            }
+            put_partial<1>(A, sm, pq);
+        }
+        ok = gsync(A, sm, epoch);  // p.q -> alpha
+        if (!ok) break;
+        get_total<1>(A, sm);
+        {
+            const double t = sm.tot[0];
+            if (!(t != 0.0) || !isfinite(t)) {
+                status = -6;
+                break;
+            }
+            alpha = rho / t;
+        }
+        // B: r and x updates, r.r, level-0 pre-smoothing of the new r
+        for (int t = tid; t < H2I * H2J; t += NT) {
+            const int a = t / H2J, b = t % H2J, i = i0 - 2 + a, j = j0 - 2 + b;
+            double v = 0.0;
+            if (i >= 0 && i < nx && j >= 0 && j < ny)
+                v = __ldcg(rcur + (int64_t)j + (int64_t)ny * i) - alpha * sm.q[a][b];
+            sm.r[a][b] = v;
+        }
+        __syncthreads();
+        {
+            double rr[1] = {0.0};
+            if (mine) {
+                xk += alpha * sm.p[3 + ta][3 + tb];
+                const double rk = sm.r[2 + ta][2 + tb];
+                __stcg(rnext + mk, rk);
+                rr[0] = rk * rk;
+            }
+            put_partial<1>(A, sm, rr);
+        }
+        l0_pre(A, sm, i0, j0);
+        {
+            double *tp = rcur;
+            rcur = rnext;
+            rnext = tp;
+            tp = pold;
+            pold = pnew;
+            pnew = tp;
+        }
+        ok = gsync(A, sm, epoch);  // r.r; level-1 rhs and level-0 e complete
+        if (!ok) break;
+        get_total<1>(A, sm);
+        it++;
+        res = sqrt(sm.tot[0]) / bn;
+        if (!isfinite(res)) {
+            status = -5;
+            break;
+        }
+        if (res > A.tol && it < A.maxit) continue;
+        // FP64 residual replacement: r = b - A x, judged in FP64
+        if (mine) __stcg(A.x + mk, xk);
+        ok = gsync(A, sm, epoch);
+        if (!ok) break;
+        {
+            double tr[1] = {0.0};
+            if (mine) {
+                double rk = 0.0;
+                if (!(S.pinned && mk == 0)) {
+                    double y = 0.0;
+                    if (mj > 0) y += -S.cn[mk - 1] * __ldcg(A.x + mk - 1);
+                    if (mi > 0) y += -S.ce[mk - ny] * __ldcg(A.x + mk - ny);
+                    y += S.diag[mk] * xk;
+                    if (mi < nx - 1) y += -S.ce[mk] * __ldcg(A.x + mk + ny);
+                    if (mj < ny - 1) y += -S.cn[mk] * __ldcg(A.x + mk + 1);
+                    rk = S.b[mk] - y;
+                }
+                __stcg(rcur + mk, rk);
+                tr[0] = rk * rk;
+            }
+            put_partial<1>(A, sm, tr);
+        }
+        ok = gsync(A, sm, epoch);
+        if (!ok) break;
+        get_total<1>(A, sm);
+        {
+            const double rt = sqrt(sm.tot[0]) / bn, prev = res_true_prev;
+            res = rt;
+            res_true_prev = rt;
+            if (!isfinite(rt)) {
+                status = -5;
+                break;
+            }
+            if (!(rt > A.tol) || it >= A.maxit) break;
+            if (prev >= 0.0 && rt > 0.5 * prev) {
+                status = 2;  // stagnated at rounding level
+                break;
+            }
+        }
+        // resume from x with the replaced r and a new direction
+        restart = 1;
+        for (int t = tid; t < H2I * H2J; t += NT) {
+            const int a = t / H2J, b = t % H2J, i = i0 - 2 + a, j = j0 - 2 + b;
+            sm.r[a][b] = (i >= 0 && i < nx && j >= 0 && j < ny) ? __ldcg(rcur + (int64_t)j + (int64_t)ny * i) : 0.0;
+        }
+        __syncthreads();
+        l0_pre(A, sm, i0, j0);
+        ok = gsync(A, sm, epoch);  // level-1 rhs and level-0 e complete
+    }
+    if (mine) __stcg(A.x + mk, xk);
+    if (blockIdx.x == 0 && tid == 0) {
+        KState *ks = A.ks;
+        ks->it = it;
+        ks->res = res;
+        ks->status = ok ? status : STATUS_BARRIER;
+        ks->done = 1;
+        ks->verified = 1;
+        ks->rho = rho;
+        ks->bn = bn;
+        ks->alpha = alpha;
+        ks->beta = beta;
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host --
+static bool persist_shape(const MgLevel *lv, int nlev, int nx, int ny, PArgs &A) {
+    if (nlev < 3 || nlev > MG_MAX_LEVELS) return false;
+    const int nti = (nx + PTI - 1) / PTI, ntj = (ny + PTJ - 1) / PTJ;
+    A.nx = nx;
+    A.ny = ny;
+    A.ntj = ntj;
+    A.ncta = nti * ntj;
+    A.nlev = nlev;
+    int off = 0;
+    for (int l = 0; l < nlev; l++) {
+        A.dims[2 * l] = lv[l].nx;
+        A.dims[2 * l + 1] = lv[l].ny;
+        A.off[l] = 0;
+        if (l >= 2) {
+            A.off[l] = off;
+            off += 5 * lv[l].nx * lv[l].ny;
+        }
+    }
+    const int last = lv[nlev - 1].nx * lv[nlev - 1].ny;
+    return off <= 5 * CMAX && last <= NINV && lv[1].nx == (nx + 1) / 2 && lv[1].ny == (ny + 1) / 2;
+}
+
+bool mg_persist_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("ASD2G_MG_PERSIST");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+bool launch_mg_persist(const Sys &S, int nx, int ny, const MgLevel *lv, int nlev, double *x, double *r0, double *r1,
+                       double *p0, double *p1, double *z, double *inv, double *partial, int64_t partial_len,
+                       unsigned *bar, KState *ks, double tol, int maxit, float omega, cudaStream_t st) {
+    PArgs A{};
+    if (!persist_shape(lv, nlev, nx, ny, A) || partial_len < 4 * (int64_t)A.ncta) return false;
+    static int smem_set = -1;  // the attribute is process-wide: set once
+    const size_t smem = sizeof(Smem);
+    if (smem_set < 0) {
+        smem_set = cudaFuncSetAttribute(k_mgfcg_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
+                           cudaSuccess
+                       ? 1
+                       : 0;
+        if (!smem_set) cudaGetLastError();
+    }
+    if (!smem_set) return false;
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mgfcg_persist, NT, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if ((int64_t)per_sm * sms < A.ncta) return false;
+    A.S = S;
+    A.x = x;
+    A.rbuf0 = r0;
+    A.rbuf1 = r1;
+    A.pbuf0 = p0;
+    A.pbuf1 = p1;
+    A.z = z;
+    A.e0g = lv[0].e;
+    A.d1g = lv[1].diag;
+    A.ce1g = lv[1].ce;
+    A.cn1g = lv[1].cn;
+    A.f1g = lv[1].f;
+    A.d2g = lv[2].diag;
+    A.ce2g = lv[2].ce;
+    A.cn2g = lv[2].cn;
+    A.f2g = lv[2].f;
+    A.inv = inv;
+    A.partial = partial;
+    A.bar = bar;
+    A.ks = ks;
+    A.tol = tol;
+    A.maxit = maxit;
+    A.omega = omega;
+    if (cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    void *args[] = {&A};
+    if (cudaLaunchCooperativeKernel((const void *)k_mgfcg_persist, dim3(A.ncta), dim3(NT), args, smem, st) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
+size_t mg_persist_smem() { return sizeof(Smem); }
+
+}  // namespace asd2g

@@ -87,6 +87,7 @@ enum asd2g_solver {
 
 /* solver_flags bits */
 #define ASD2G_FLAG_NO_CLUSTER_PCG 1 /* Jacobi-PCG always as per-iteration kernels (no cluster solver) */
+#define ASD2G_FLAG_NO_PERSIST_MG 2  /* MG-FCG always as per-phase kernels (no one-launch solve) */
 
 /* precision (no reference counterpart: the reference is FP64 throughout) */
 #define ASD2G_PRECISION_FP64 0  /* every field and kernel in FP64 (the drop-in) */
@@ -361,6 +362,11 @@ int asd2g_unet_set_stream(asd2g_unet *u, void *stream);
  * asd2g_last_fallback reports 1. */
 int asd2g_set_preconditioner_net(asd2g_session *s, asd2g_unet *net);
 int asd2g_last_fallback(asd2g_session *s, int *used);
+/* How the session's last pressure solve ran: *one_launch = 1 when the whole
+ * solve was one kernel launch (the thread-block-cluster Jacobi-PCG or the
+ * cooperative MG-FCG of systems up to about 256 x 256), 0 when it ran as
+ * per-phase kernels.  No reference counterpart (solver introspection). */
+int asd2g_last_solve_one_launch(asd2g_session *s, int *one_launch);
 /* Training pair of the network from the session's last assembled and solved
  * system (solution x): z = V-cycle(b), r1 = b - A z, e = x - z; feats (device
  * FP32 [nx][ny][4]) = (r1 / rms(r1), diag / s, ce / s, cn / s), target
