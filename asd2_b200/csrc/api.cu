@@ -318,6 +318,7 @@ int mg_alloc(asd2g_session *s) {
     if (rc) return rc;
     s->mg_partial_n = np;
     if (!mg_cta_prepare(s->lv, n)) return fail(ASD2G_E_UNSUPPORTED, "multigrid coarse cycle does not fit a CTA");
+    mg_persist_prepare();  // process-wide kernel attribute, set before any capture can need it
     s->lv[0].tile = mg_session_tile(s->g.nx, s->g.ny);
     s->nlev = n;
     return ASD2G_OK;
@@ -993,9 +994,9 @@ constexpr int PC_MAX_ITERS = 500;    // iterations of the learned phase before t
 static_assert(PC_CHUNK % FM_SLOTS == 0, "every replay of a chunk must write the direction slots in the same order");
 
 // The network's correction on every PC_NET_EVERY-th iteration of a chunk
-// (ASD2G_PC_EVERY=1..8 in the environment), besides the first application
-// and the one after each residual replacement; the other iterations use the
-// V-cycle alone.  Measured on the 512^2 evaluation (solves/s, iterations):
+// (ASD2G_PC_EVERY=1..8 in the environment), besides the first application;
+// the other iterations, and the restart after a residual replacement, use
+// the V-cycle alone.  Measured on the 512^2 evaluation (solves/s, iterations):
 // every iteration 142 (13-15), every 2nd 199, every 3rd or 4th 260, every
 // 8th 306 (11-17): the correction is needed for a few modes the V-cycle
 // leaves, not at every step.
@@ -1021,7 +1022,10 @@ static int pc_chunk(asd2g_session *s) {
     if (!launch_pcm_check(s->sys, g.nx, g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->z, s->fm, s->ks,
                           s->mg_partial, s->mg_partial_n, s->st))
         return fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
-    return pc_correct(s);
+    // after a residual replacement that restarts the solve: the V-cycle of
+    // the new residual alone (mid-solve the check changes nothing and these
+    // kernels return at entry)
+    return pc_correct(s, false);
 }
 
 static int fm_alloc(asd2g_session *s) {
@@ -1524,7 +1528,9 @@ int asd2g_checkpoint_info(const char *path, int *nx, int *ny, double *t, long lo
 // is done, or after ceil(maxit / 8) + 2 passes), and the whole step is the
 // body of an IF node that skips it once an earlier step failed.  The host
 // launches the step graph n times and synchronises once.
-static int capture_run_graph(asd2g_session *s, int reinit_mode, double tol, int maxit) {
+// persist: the step's solve as the one-launch MG-FCG (systems that fit it)
+// instead of the WHILE loop over chunks of per-phase kernels.
+static int capture_run_graph(asd2g_session *s, int reinit_mode, double tol, int maxit, bool persist) {
     for (cudaStream_t &a : s->aux_st)
         if (!a && cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking) != cudaSuccess) return cuda_check("aux stream");
     const cudaStream_t main_st = s->st;
@@ -1584,19 +1590,25 @@ static int capture_run_graph(asd2g_session *s, int reinit_mode, double tol, int 
     if (ok) {
         s->st = s->aux_st[0];
         rc = enqueue_step_pre(s, reinit_mode);
-        if (!rc) {
+        if (!rc && persist) {
+            launch_set_kstate(s->ks, tol, maxit, ASD2G_SOLVER_MGPCG, 0.0, s->st);
+            if (!launch_mg_persist(s->sys, s->g.nx, s->g.ny, s->lv, s->nlev, s->x, s->r, s->q, s->pa, s->pb, s->z,
+                                   s->coarse_inv, s->mg_partial, s->mg_partial_n, s->mgp_bar, s->ks, tol, maxit,
+                                   mg_omega_value(), s->st))
+                rc = fail(ASD2G_E_UNSUPPORTED, "one-launch MG-FCG not available");
+        } else if (!rc) {
             launch_set_kstate(s->ks, tol, maxit, ASD2G_SOLVER_MGPCG, 0.0, s->st);
             launch_mg_setup(s->sys, s->lv, s->nlev, s->coarse_inv, s->st);
             if (!launch_fcg_init(s->sys, s->g.nx, s->g.ny, s->lv, s->nlev, s->coarse_inv, s->x, s->r, s->pa, s->q,
                                  s->z, s->ks, s->mg_partial, s->mg_partial_n, s->st))
                 rc = fail(ASD2G_E_UNSUPPORTED, "multigrid partial-sum buffer too small");
         }
-        if (!rc) ok = add_conditional(s->st, cudaGraphCondTypeWhile, &h_while, &while_body);
+        if (!rc && !persist) ok = add_conditional(s->st, cudaGraphCondTypeWhile, &h_while, &while_body);
         // WHILE body: 8 iterations + the FP64 check, then the loop condition
-        if (!rc && ok)
+        if (!rc && ok && !persist)
             ok = cudaStreamBeginCaptureToGraph(s->aux_st[1], while_body, nullptr, nullptr, 0,
                                                cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-        if (!rc && ok) {
+        if (!rc && ok && !persist) {
             s->st = s->aux_st[1];
             if (!enqueue_iters(s, ASD2G_SOLVER_MGPCG, 8)) rc = fail(ASD2G_E_UNSUPPORTED, "multigrid buffer too small");
             launch_run_while(s->ks, s->run_stats, cap, h_while, s->st);
@@ -1658,7 +1670,10 @@ int asd2g_run_steps(asd2g_session *s, int nsteps, double *dt, int reinit_mode, i
     if (!s->run_exec || s->run_reinit != reinit_mode || s->run_tol != tol || s->run_maxit != maxit) {
         // one eager step's worth of set-up first: attributes and first-use state outside the capture
         launch_run_reset(s->run_stats, s->st);
-        rc = capture_run_graph(s, reinit_mode, tol, maxit);
+        const bool persist = mg_persist_enabled() && !(s->prm.solver_flags & ASD2G_FLAG_NO_PERSIST_MG) &&
+                             mg_persist_fits(s->lv, s->nlev, s->g.nx, s->g.ny, s->mg_partial_n);
+        rc = capture_run_graph(s, reinit_mode, tol, maxit, persist);
+        if (rc && persist) rc = capture_run_graph(s, reinit_mode, tol, maxit, false);
         if (rc) return rc;
     }
     rc = set_dt(s, *dt);

@@ -253,7 +253,7 @@ template <bool L0, int TI_ = MT_I, int TJ_ = MT_J>
 __global__ void __launch_bounds__(256) k_mg_pre(MgLevel L, MgLevel C, const double *__restrict__ r64,
                                                 const KState *ks) {
     pdl_enter();
-    if (ks->done) return;
+    if (ks->done || ks->skip_vc) return;
     mg_pre_tile<L0, TI_, TJ_>(L, C, r64, blockIdx.y * TI_, blockIdx.x * TJ_);
 }
 
@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(256) k_mg_post(MgLevel L, MgLevel C, float ome
                                                  const double *__restrict__ q64, double *__restrict__ z64, int pinned,
                                                  KState *ks, double *partial) {
     pdl_enter();
-    if (ks->done) return;
+    if (ks->done || ks->skip_vc) return;
     double acc[2];
     mg_post_tile<L0, TI_, TJ_>(L, C, omega, r64, q64, z64, pinned, blockIdx.y * TI_, blockIdx.x * TJ_, acc);
     if (L0) {
@@ -540,7 +540,7 @@ __global__ void __launch_bounds__(MG_CTA_THREADS) k_mg_cta_cycle(MgHier H, int s
                                                                 const double *__restrict__ inv, float omega,
                                                                 const KState *ks) {
     pdl_enter();
-    if (ks->done) return;
+    if (ks->done || ks->skip_vc) return;
     mg_cta_body(H.l, s, nlev, inv, omega);
 }
 
@@ -551,6 +551,7 @@ __global__ void __launch_bounds__(256) k_fcg_a(int nx, int ny, Sys S, const doub
                                                double *__restrict__ q, KState *ks, double *partial) {
     pdl_enter();
     if (ks->done) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) ks->skip_vc = 0;
     const double beta = ks->beta;
     const int64_t n = (int64_t)nx * ny;
     double v[1] = {0.0};
@@ -619,7 +620,11 @@ __global__ void __launch_bounds__(256) k_fcg_b(int64_t n, double *__restrict__ x
 __global__ void __launch_bounds__(256) k_fcg_replace(int nx, int ny, Sys S, const double *__restrict__ x,
                                                      double *__restrict__ r, KState *ks, double *partial) {
     pdl_enter();
-    if (!ks->done || ks->verified || ks->status != 0) return;
+    if (!ks->done) {  // mid-solve: nothing to replace, and the V-cycle after the check must not run
+        if (blockIdx.x == 0 && threadIdx.x == 0) ks->skip_vc = 1;
+        return;
+    }
+    if (ks->verified || ks->status != 0) return;
     const int64_t n = (int64_t)nx * ny;
     double v[1] = {0.0};
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
@@ -682,6 +687,7 @@ __global__ void k_fcg_init(int64_t n, Sys S, double *__restrict__ x, double *__r
         ks->verified = 0;
         ks->restart = 0;
         ks->res_true_prev = -1.0;
+        ks->skip_vc = 0;
         ks->done = (!(ks->res > ks->tol) || ks->maxit <= 0) ? 1 : 0;
     }
 }
@@ -731,6 +737,7 @@ __global__ void k_bset_kstate(const BInst *__restrict__ insts, int count, double
     ks->verified = 0;
     ks->restart = 0;
     ks->res_true_prev = -1.0;
+    ks->skip_vc = 0;
 }
 
 __global__ void __launch_bounds__(256) k_bfcg_init(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks) {
@@ -794,6 +801,7 @@ __global__ void __launch_bounds__(256) k_bfcg_a(const BInst *__restrict__ insts,
     const BInst &I = insts[w.inst];
     KState *ks = I.ks;
     if (ks->done) return;
+    if (w.c == 0 && threadIdx.x == 0) ks->skip_vc = 0;
     const double beta = ks->beta;
     const double *__restrict__ p_old = parity ? I.pb : I.pa;
     double *__restrict__ p_new = parity ? I.pa : I.pb;
@@ -879,7 +887,11 @@ __global__ void __launch_bounds__(256) k_bfcg_replace(const BInst *__restrict__ 
     const BChunk w = chunks[blockIdx.x];
     const BInst &I = insts[w.inst];
     KState *ks = I.ks;
-    if (!ks->done || ks->verified || ks->status != 0) return;
+    if (!ks->done) {  // mid-solve: the V-cycle after the check must not run
+        if (w.c == 0 && threadIdx.x == 0) ks->skip_vc = 1;
+        return;
+    }
+    if (ks->verified || ks->status != 0) return;
     const Sys S = I.S;
     const int nx = I.g.nx, ny = I.g.ny;
     const double *__restrict__ x = I.x;
@@ -921,13 +933,13 @@ __global__ void __launch_bounds__(256) k_bmg_pre(const BInst *__restrict__ insts
                                                  int l) {
     const BTile w = tiles[blockIdx.x];
     const BInst &I = insts[w.inst];
-    if (I.ks->done) return;
+    if (I.ks->done || I.ks->skip_vc) return;
     mg_pre_tile<L0, TI_, TJ_>(I.lv[l], I.lv[l + 1], L0 ? I.r : nullptr, w.by * TI_, w.bx * TJ_);
 }
 
 __global__ void __launch_bounds__(MG_CTA_THREADS) k_bmg_cta(const BInst *__restrict__ insts, float omega) {
     const BInst &I = insts[blockIdx.x];
-    if (I.ks->done) return;
+    if (I.ks->done || I.ks->skip_vc) return;
     mg_cta_body(I.lv, I.s_cta, I.nlev, I.coarse_inv, omega);
 }
 
@@ -937,7 +949,7 @@ __global__ void __launch_bounds__(256) k_bmg_post(const BInst *__restrict__ inst
     const BTile w = tiles[blockIdx.x];
     const BInst &I = insts[w.inst];
     KState *ks = I.ks;
-    if (ks->done) return;
+    if (ks->done || ks->skip_vc) return;
     double acc[2];
     mg_post_tile<L0, TI_, TJ_>(I.lv[l], I.lv[l + 1], omega, L0 ? I.r : nullptr, L0 ? I.q : nullptr,
                                L0 ? I.z : nullptr, I.S.pinned, w.by * TI_, w.bx * TJ_, acc);
@@ -1051,7 +1063,7 @@ __global__ void __launch_bounds__(256) k_pc_omega(int nx, int ny, Sys S, const f
 // residual replacement)
 __global__ void __launch_bounds__(256) k_pc_final(int64_t n, const float *__restrict__ u, double *__restrict__ z,
                                                   FmDirs D, int pinned, KState *ks, double *partial) {
-    if (ks->done) return;
+    if (ks->done || ks->skip_vc) return;
     const double om = u ? ks->omega : 0.0;  // u == nullptr: the V-cycle alone this iteration
     double acc[FM_SLOTS] = {};
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
@@ -1076,6 +1088,7 @@ __global__ void __launch_bounds__(256) k_pc_final(int64_t n, const float *__rest
 __global__ void __launch_bounds__(256) k_pcm_a(int nx, int ny, Sys S, const double *__restrict__ z, FmDirs D, int w,
                                                const double *__restrict__ r, KState *ks, double *partial) {
     if (ks->done) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) ks->skip_vc = 0;
     double b[FM_SLOTS];
 #pragma unroll
     for (int j = 0; j < FM_SLOTS; j++) b[j] = j == w ? 0.0 : ks->fm_beta[j];

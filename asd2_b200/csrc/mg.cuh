@@ -101,6 +101,11 @@ void launch_pc_pair(const Sys &S, int nx, int ny, const double *x, const double 
 // up, the solve did not finish) and done.  Returns false (nothing launched)
 // when the system does not fit or the device cannot co-schedule the grid.
 bool mg_persist_enabled();
+// Sets the kernel's shared-memory attribute (once per process; call outside
+// any stream capture); false if the device refuses it.
+bool mg_persist_prepare();
+// Whether launch_mg_persist would launch for this hierarchy (no launch).
+bool mg_persist_fits(const MgLevel *lv, int nlev, int nx, int ny, int64_t partial_len);
 bool launch_mg_persist(const Sys &S, int nx, int ny, const MgLevel *lv, int nlev, double *x, double *r0, double *r1,
                        double *p0, double *p1, double *z, double *inv, double *partial, int64_t partial_len,
                        unsigned *bar, KState *ks, double tol, int maxit, float omega, cudaStream_t st);

@@ -853,29 +853,42 @@ bool mg_persist_enabled() {
     return on;
 }
 
-bool launch_mg_persist(const Sys &S, int nx, int ny, const MgLevel *lv, int nlev, double *x, double *r0, double *r1,
-                       double *p0, double *p1, double *z, double *inv, double *partial, int64_t partial_len,
-                       unsigned *bar, KState *ks, double tol, int maxit, float omega, cudaStream_t st) {
-    PArgs A{};
-    if (!persist_shape(lv, nlev, nx, ny, A) || partial_len < 4 * (int64_t)A.ncta) return false;
-    static int smem_set = -1;  // the attribute is process-wide: set once
-    const size_t smem = sizeof(Smem);
+bool mg_persist_prepare() {
+    static int smem_set = -1;  // the attribute is process-wide: set once, outside any capture
     if (smem_set < 0) {
-        smem_set = cudaFuncSetAttribute(k_mgfcg_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
-                           cudaSuccess
+        smem_set = cudaFuncSetAttribute(k_mgfcg_persist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sizeof(Smem)) == cudaSuccess
                        ? 1
                        : 0;
         if (!smem_set) cudaGetLastError();
     }
-    if (!smem_set) return false;
+    return smem_set == 1;
+}
+
+static bool persist_fits(const MgLevel *lv, int nlev, int nx, int ny, int64_t partial_len, PArgs &A) {
+    if (!persist_shape(lv, nlev, nx, ny, A) || partial_len < 4 * (int64_t)A.ncta || !mg_persist_prepare())
+        return false;
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mgfcg_persist, NT, smem) != cudaSuccess) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mgfcg_persist, NT, sizeof(Smem)) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    if ((int64_t)per_sm * sms < A.ncta) return false;
+    return (int64_t)per_sm * sms >= A.ncta;
+}
+
+bool mg_persist_fits(const MgLevel *lv, int nlev, int nx, int ny, int64_t partial_len) {
+    PArgs A{};
+    return persist_fits(lv, nlev, nx, ny, partial_len, A);
+}
+
+bool launch_mg_persist(const Sys &S, int nx, int ny, const MgLevel *lv, int nlev, double *x, double *r0, double *r1,
+                       double *p0, double *p1, double *z, double *inv, double *partial, int64_t partial_len,
+                       unsigned *bar, KState *ks, double tol, int maxit, float omega, cudaStream_t st) {
+    PArgs A{};
+    if (!persist_fits(lv, nlev, nx, ny, partial_len, A)) return false;
+    const size_t smem = sizeof(Smem);
     A.S = S;
     A.x = x;
     A.rbuf0 = r0;

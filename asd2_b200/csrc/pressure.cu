@@ -567,6 +567,7 @@ __global__ void k_set_kstate(KState *ks, double tol, int maxit, int mode, double
     ks->verified = 0;
     ks->restart = 0;
     ks->res_true_prev = -1.0;
+    ks->skip_vc = 0;
 }
 
 // ------------------------------------------------------------------ host --

@@ -28,6 +28,11 @@ struct KState {
     // orthogonalisation coefficients of the stored directions, valid-slot mask
     double fm_pq[4], fm_beta[4];
     int fm_mask;
+    // MG-FCG: set by the residual check of a chunk when it changed nothing
+    // (mid-solve), so the V-cycle enqueued after the check returns at entry
+    // instead of redoing the last V-cycle and the direction update; cleared
+    // by the next iteration's first kernel
+    int skip_vc;
 };
 
 constexpr int RED_BLOCKS_MAX = 1184;  // 8 x 148 SMs
