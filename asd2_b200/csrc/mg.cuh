@@ -93,7 +93,7 @@ void launch_pc_pair(const Sys &S, int nx, int ny, const double *x, const double 
 
 // mg_persist.cu: the whole MG-FCG solve (same method as launch_fcg_init /
 // iter / check) as ONE cooperative launch of one CTA per 16 x 32 tile, for
-// systems whose tiles fit the GPU at once and whose levels from 2 down fit
+// systems whose tiles fit the GPU at once and whose levels from 3 down fit
 // one CTA's shared memory (up to about 256 x 256).  x receives the solution;
 // r0/r1 and p0/p1 are two n-vectors each, z one; inv holds the coarsest
 // inverse; partial at least 4 doubles per tile; bar two words (zeroed by the

@@ -9,10 +9,13 @@
 //
 // Why: at 256^2 every multi-kernel phase is latency-bound (7 dependent
 // launches of 7-11 us per iteration: launch gap, dependent L2 loads of the
-// tile, grid reduction, the one-SM coarse cycle).  Here each CTA keeps its
+// tile, grid reduction, the one-SM coarse cycle).  The smoothers multiply by
+// stored reciprocal diagonals (the per-phase kernels divide), so the two
+// paths agree to FP32 rounding of the V-cycle, not bit for bit.  Here each CTA keeps its
 // tile's state resident (level-0 FP32 operator on the tile + 2 halo, the
-// level-1 operator on its level-1 tile + 5, every level from 2 down in full)
-// and an iteration has four grid barriers:
+// level-1 operator on its level-1 cells + 5, the level-2 operator on its
+// level-2 cells + 6, every level from 3 down in full) and an iteration has
+// five grid barriers:
 //
 //   A   p = z + beta p_old and q = A p on the tile + halo (FP64) -> p.q
 //   --- barrier 1: alpha
@@ -21,16 +24,20 @@
 //       pre-smoothing (red on the tile + 2, black on the tile + 1), residual,
 //       restriction into level 1
 //   --- barrier 2: convergence (FP64 residual replacement when met)
-//   D   level-1 pre-smoothing on the level-1 tile + 5 (red on +5, black on
-//       +4, so the pre-smoothed level-1 correction is right on +4 without a
-//       barrier), residual, restriction into level 2
+//   D   level-1 pre-smoothing on the CTA's level-1 cells + 5 (red on +5,
+//       black on +4, so the pre-smoothed level-1 correction is right on +4
+//       without a barrier), residual, restriction into level 2
 //   --- barrier 3: level-2 right-hand side complete
-//   E   every CTA gathers the level-2 right-hand side and runs levels 2..
+//   D2  the same for level 2 on its level-2 cells + 6, restriction into
+//       level 3
+//   --- barrier 4: level-3 right-hand side complete
+//   E   every CTA gathers the level-3 right-hand side and runs levels 3..
 //       itself (redundantly: no barrier needed to share the result), then
-//       the level-1 post-smoothing on its tile + 1 and the level-0
-//       post-smoothing on its tile (the neighbours' pre-smoothed level-0
-//       correction read from global memory) -> z, z.r, z.q
-//   --- barrier 4: beta
+//       the level-2 post-smoothing on its cells + 2, the level-1 one on its
+//       cells + 1 and the level-0 one on its tile (the neighbours'
+//       pre-smoothed level-0 correction read from global memory) -> z, z.r,
+//       z.q
+//   --- barrier 5: beta
 //
 // A value a CTA computes for a neighbour's cell (halo recomputation) uses the
 // same inputs and the same code as the owner's, so it is the owner's value.
@@ -58,14 +65,24 @@ constexpr int PTI = 16, PTJ = 32;                      // level-0 tile (rows i x
 constexpr int NT = PTI * PTJ;                          // threads: one per tile cell
 constexpr int H3I = PTI + 6, H3J = PTJ + 6;            // tile + 3
 constexpr int H2I = PTI + 4, H2J = PTJ + 4;            // tile + 2
-constexpr int C1I = PTI / 2, C1J = PTJ / 2;            // level-1 cells under a tile
-constexpr int R1 = 5;                                  // level-1 halo kept by a CTA
-constexpr int R1I = C1I + 2 * R1, R1J = C1J + 2 * R1;  // 18 x 26
-constexpr int C2I = PTI / 4, C2J = PTJ / 4;            // level-2 cells under a tile
-constexpr int CMAX = 5440;                             // cells of levels 2.. (64^2 + 32^2 + 16^2 + 8^2)
+constexpr int CMAX = 1800;                             // cells of levels 3.. (32^2 + 16^2 + 8^2 and odd sizes)
 constexpr int NINV = MG_COARSE_CELLS;                  // coarsest level <= 64 cells
 constexpr unsigned SPIN_LIMIT = 1u << 22;              // polls before a barrier wait gives up
 constexpr int STATUS_BARRIER = -8;                     // KState.status when a barrier wait gave up
+
+// A level distributed over the CTAs: the CTA's CI x CJ cells of it (the
+// cells under its level-0 tile) plus a halo of H cells, recomputed rather
+// than exchanged.  Pre-smoothing (red on +H, black on +(H-1)) makes the
+// pre-smoothed correction right on +(H-1); the post-smoothing of a target
+// region +T (prolongation on +(T+2), black on +(T+1), red on +T) needs it on
+// +(T+2), so T + 2 <= H - 1.
+template <int CI_, int CJ_, int H_> struct DLev {
+    static constexpr int CI = CI_, CJ = CJ_, H = H_, RI = CI_ + 2 * H_, RJ = CJ_ + 2 * H_;
+    float d[RI][RJ], di[RI][RJ], ce[RI][RJ], cn[RI][RJ], f[RI][RJ], e[RI][RJ];
+    float res[CI_][CJ_];
+};
+using Lev1 = DLev<PTI / 2, PTJ / 2, 5>;  // post target +1 (what level-0 post-smoothing reads)
+using Lev2 = DLev<PTI / 4, PTJ / 4, 6>;  // post target +2 (what level-1 post-smoothing reads)
 
 struct Smem {
     double p[H3I][H3J];        // direction on the tile + 3
@@ -74,23 +91,22 @@ struct Smem {
     double inv[NINV * NINV];   // coarsest inverse (row-major, stride NINV)
     double red[4][NT / 32];    // per-warp partial sums
     double tot[4];             // reduced sums (the same in every CTA)
-    float d0[H2I][H2J], ce0[H2I][H2J], cn0[H2I][H2J], f0[H2I][H2J], e0[H2I][H2J];  // level 0, tile + 2
+    float d0[H2I][H2J], di0[H2I][H2J], ce0[H2I][H2J], cn0[H2I][H2J], f0[H2I][H2J], e0[H2I][H2J];  // level 0
     float res0[PTI][PTJ];
-    float d1[R1I][R1J], ce1[R1I][R1J], cn1[R1I][R1J], f1[R1I][R1J], e1[R1I][R1J];  // level 1, tile + 5
-    float res1[C1I][C1J];
-    float co[5 * CMAX];        // levels 2..: d, ce, cn, f, e of each level
+    Lev1 l1;
+    Lev2 l2;
+    float co[6 * CMAX];        // levels 3..: d, ce, cn, f, e, 1/d of each level
     int flag;
 };
 
 struct PArgs {
     int nx, ny, ntj, ncta, nlev;
     int dims[2 * MG_MAX_LEVELS];
-    int off[MG_MAX_LEVELS];  // offset (floats) of level l >= 2 in Smem::co
+    int off[MG_MAX_LEVELS];  // offset (floats) of level l >= 3 in Smem::co
     Sys S;
     double *x, *rbuf0, *rbuf1, *pbuf0, *pbuf1, *z;
     float *e0g;                          // level-0 pre-smoothed correction
-    float *d1g, *ce1g, *cn1g, *f1g;      // level-1 operator and right-hand side
-    float *d2g, *ce2g, *cn2g, *f2g;      // level-2 operator and right-hand side
+    float *lg[4][4];                     // levels 1..3: [l][0..3] = diag, ce, cn, f (global)
     double *inv;                         // coarsest inverse (written by CTA 0)
     double *partial;                     // 4 slots per CTA
     unsigned *bar;                       // [0] arrivals, [1] error word
@@ -165,11 +181,13 @@ template <int NV> __device__ void get_total(const PArgs &A, Smem &sm) {
     __syncthreads();
 }
 
-template <int W> __device__ __forceinline__ float gs(const float (*f)[W], const float (*d)[W], const float (*ce)[W],
+// Gauss-Seidel update of local cell (a, b) from its four neighbours (times
+// the stored reciprocal of the diagonal).
+template <int W> __device__ __forceinline__ float gs(const float (*f)[W], const float (*di)[W], const float (*ce)[W],
                                                      const float (*cn)[W], const float (*e)[W], int a, int b) {
     const float s = f[a][b] + ce[a - 1][b] * e[a - 1][b] + ce[a][b] * e[a + 1][b] + cn[a][b - 1] * e[a][b - 1] +
                     cn[a][b] * e[a][b + 1];
-    return s / d[a][b];
+    return s * di[a][b];
 }
 
 // Galerkin 2x2 aggregation of one coarse cell (as mg_coarsen_cell in mg.cu)
@@ -208,12 +226,12 @@ __device__ void l0_pre(const PArgs &A, Smem &sm, int i0, int j0) {
         const int a = t / H2J, b = t % H2J, i = i0 - 2 + a, j = j0 - 2 + b;
         const float f = (float)sm.r[a][b];
         sm.f0[a][b] = f;
-        sm.e0[a][b] = (((i + j) & 1) == 0) ? f / sm.d0[a][b] : 0.0f;
+        sm.e0[a][b] = (((i + j) & 1) == 0) ? f * sm.di0[a][b] : 0.0f;
     }
     __syncthreads();
     for (int t = tid; t < (H2I - 2) * (H2J - 2); t += NT) {
         const int a = 1 + t / (H2J - 2), b = 1 + t % (H2J - 2), i = i0 - 2 + a, j = j0 - 2 + b;
-        if (((i + j) & 1) == 1) sm.e0[a][b] = gs<H2J>(sm.f0, sm.d0, sm.ce0, sm.cn0, sm.e0, a, b);
+        if (((i + j) & 1) == 1) sm.e0[a][b] = gs<H2J>(sm.f0, sm.di0, sm.ce0, sm.cn0, sm.e0, a, b);
     }
     __syncthreads();
     {
@@ -229,82 +247,115 @@ __device__ void l0_pre(const PArgs &A, Smem &sm, int i0, int j0) {
         sm.res0[ta][tb] = rr;
     }
     __syncthreads();
-    if (tid < C1I * C1J) {
-        const int ci = tid / C1J, cj = tid % C1J, I = i0 / 2 + ci, J = j0 / 2 + cj;
+    if (tid < (PTI / 2) * (PTJ / 2)) {
+        const int ci = tid / (PTJ / 2), cj = tid % (PTJ / 2), I = i0 / 2 + ci, J = j0 / 2 + cj;
         const int n1x = A.dims[2], n1y = A.dims[3];
         if (I < n1x && J < n1y)
-            __stcg(A.f1g + (int64_t)J + (int64_t)n1y * I, sm.res0[2 * ci][2 * cj] + sm.res0[2 * ci + 1][2 * cj] +
-                                                            sm.res0[2 * ci][2 * cj + 1] +
-                                                            sm.res0[2 * ci + 1][2 * cj + 1]);
+            __stcg(A.lg[1][3] + (int64_t)J + (int64_t)n1y * I, sm.res0[2 * ci][2 * cj] + sm.res0[2 * ci + 1][2 * cj] +
+                                                                sm.res0[2 * ci][2 * cj + 1] +
+                                                                sm.res0[2 * ci + 1][2 * cj + 1]);
     }
 }
 
-// ---------------------------------------------------------------- level 1 --
-// Pre-smoothing of level 1 on the level-1 tile + 5 (red on +5, black on +4),
-// residual on the level-1 tile, restriction into the tile's level-2 cells.
-__device__ void l1_pre(const PArgs &A, Smem &sm, int I0, int J0) {
-    const int tid = threadIdx.x, n1x = A.dims[2], n1y = A.dims[3];
-    for (int t = tid; t < R1I * R1J; t += NT) {
-        const int a = t / R1J, b = t % R1J, I = I0 - R1 + a, J = J0 - R1 + b;
-        const bool in = I >= 0 && I < n1x && J >= 0 && J < n1y;
-        const float f = in ? __ldcg(A.f1g + (int64_t)J + (int64_t)n1y * I) : 0.0f;
-        sm.f1[a][b] = f;
-        sm.e1[a][b] = (((I + J) & 1) == 0) ? f / sm.d1[a][b] : 0.0f;
+// ------------------------------------------------- distributed levels 1, 2 --
+// Pre-smoothing of level l on the CTA's cells + H (tile origin I0, J0 in
+// level-l cells): right-hand side from global memory, red on +H from zero,
+// black on +(H-1), residual on the tile, restriction into the tile's level
+// l+1 cells (global).
+template <class L> __device__ void dist_pre(const PArgs &A, L &v, int l, int I0, int J0) {
+    const int tid = threadIdx.x, nx = A.dims[2 * l], ny = A.dims[2 * l + 1];
+    const float *fg = A.lg[l][3];
+    for (int t = tid; t < L::RI * L::RJ; t += NT) {
+        const int a = t / L::RJ, b = t % L::RJ, I = I0 - L::H + a, J = J0 - L::H + b;
+        const bool in = I >= 0 && I < nx && J >= 0 && J < ny;
+        const float f = in ? __ldcg(fg + (int64_t)J + (int64_t)ny * I) : 0.0f;
+        v.f[a][b] = f;
+        v.e[a][b] = (((I + J) & 1) == 0) ? f * v.di[a][b] : 0.0f;
     }
     __syncthreads();
-    for (int t = tid; t < (R1I - 2) * (R1J - 2); t += NT) {
-        const int a = 1 + t / (R1J - 2), b = 1 + t % (R1J - 2), I = I0 - R1 + a, J = J0 - R1 + b;
-        if (((I + J) & 1) == 1) sm.e1[a][b] = gs<R1J>(sm.f1, sm.d1, sm.ce1, sm.cn1, sm.e1, a, b);
+    for (int t = tid; t < (L::RI - 2) * (L::RJ - 2); t += NT) {
+        const int a = 1 + t / (L::RJ - 2), b = 1 + t % (L::RJ - 2), I = I0 - L::H + a, J = J0 - L::H + b;
+        if (((I + J) & 1) == 1) v.e[a][b] = gs<L::RJ>(v.f, v.di, v.ce, v.cn, v.e, a, b);
     }
     __syncthreads();
-    if (tid < C1I * C1J) {
-        const int ta = tid / C1J, tb = tid % C1J, a = R1 + ta, b = R1 + tb, I = I0 + ta, J = J0 + tb;
+    if (tid < L::CI * L::CJ) {
+        const int ta = tid / L::CJ, tb = tid % L::CJ, a = L::H + ta, b = L::H + tb, I = I0 + ta, J = J0 + tb;
         float rr = 0.0f;
-        if (I < n1x && J < n1y) {
-            const float Ae = sm.d1[a][b] * sm.e1[a][b] - sm.ce1[a - 1][b] * sm.e1[a - 1][b] -
-                             sm.ce1[a][b] * sm.e1[a + 1][b] - sm.cn1[a][b - 1] * sm.e1[a][b - 1] -
-                             sm.cn1[a][b] * sm.e1[a][b + 1];
-            rr = sm.f1[a][b] - Ae;
+        if (I < nx && J < ny) {
+            const float Ae = v.d[a][b] * v.e[a][b] - v.ce[a - 1][b] * v.e[a - 1][b] - v.ce[a][b] * v.e[a + 1][b] -
+                             v.cn[a][b - 1] * v.e[a][b - 1] - v.cn[a][b] * v.e[a][b + 1];
+            rr = v.f[a][b] - Ae;
         }
-        sm.res1[ta][tb] = rr;
+        v.res[ta][tb] = rr;
     }
     __syncthreads();
-    if (tid < C2I * C2J) {
-        const int ci = tid / C2J, cj = tid % C2J, I = I0 / 2 + ci, J = J0 / 2 + cj;
-        const int n2x = A.dims[4], n2y = A.dims[5];
-        if (I < n2x && J < n2y)
-            __stcg(A.f2g + (int64_t)J + (int64_t)n2y * I, sm.res1[2 * ci][2 * cj] + sm.res1[2 * ci + 1][2 * cj] +
-                                                            sm.res1[2 * ci][2 * cj + 1] +
-                                                            sm.res1[2 * ci + 1][2 * cj + 1]);
+    if (tid < (L::CI / 2) * (L::CJ / 2)) {
+        const int ci = tid / (L::CJ / 2), cj = tid % (L::CJ / 2), I = I0 / 2 + ci, J = J0 / 2 + cj;
+        const int cnx = A.dims[2 * l + 2], cny = A.dims[2 * l + 3];
+        if (I < cnx && J < cny)
+            __stcg(A.lg[l + 1][3] + (int64_t)J + (int64_t)cny * I,
+                   v.res[2 * ci][2 * cj] + v.res[2 * ci + 1][2 * cj] + v.res[2 * ci][2 * cj + 1] +
+                       v.res[2 * ci + 1][2 * cj + 1]);
     }
 }
 
-// ------------------------------------------------------ levels 2 .. nlev-1 --
+// Post-smoothing of level l on the CTA's cells + T: prolongation of the
+// coarse correction ec(I >> 1, J >> 1) with omega on +(T+2), black on +(T+1),
+// red on +T, in v.e.
+template <int T, class L, class EC> __device__ void dist_post(const PArgs &A, L &v, int l, int I0, int J0, EC ec) {
+    static_assert(T + 2 <= L::H - 1, "the pre-smoothed correction must be right where it is prolonged");
+    const int tid = threadIdx.x, nx = A.dims[2 * l], ny = A.dims[2 * l + 1];
+    constexpr int P = L::H - T - 2;  // first local index of the +(T+2) region
+    for (int t = tid; t < (L::RI - 2 * P) * (L::RJ - 2 * P); t += NT) {
+        const int a = P + t / (L::RJ - 2 * P), b = P + t % (L::RJ - 2 * P), I = I0 - L::H + a, J = J0 - L::H + b;
+        if (I >= 0 && I < nx && J >= 0 && J < ny) v.e[a][b] += A.omega * ec(I >> 1, J >> 1);
+    }
+    __syncthreads();
+    for (int t = tid; t < (L::RI - 2 * P - 2) * (L::RJ - 2 * P - 2); t += NT) {
+        const int a = P + 1 + t / (L::RJ - 2 * P - 2), b = P + 1 + t % (L::RJ - 2 * P - 2);
+        const int I = I0 - L::H + a, J = J0 - L::H + b;
+        if (((I + J) & 1) == 1 && I >= 0 && I < nx && J >= 0 && J < ny)
+            v.e[a][b] = gs<L::RJ>(v.f, v.di, v.ce, v.cn, v.e, a, b);
+    }
+    __syncthreads();
+    for (int t = tid; t < (L::RI - 2 * P - 4) * (L::RJ - 2 * P - 4); t += NT) {
+        const int a = P + 2 + t / (L::RJ - 2 * P - 4), b = P + 2 + t % (L::RJ - 2 * P - 4);
+        const int I = I0 - L::H + a, J = J0 - L::H + b;
+        if (((I + J) & 1) == 0 && I >= 0 && I < nx && J >= 0 && J < ny)
+            v.e[a][b] = gs<L::RJ>(v.f, v.di, v.ce, v.cn, v.e, a, b);
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------ levels 3 .. nlev-1 --
 // The coarse part of the V-cycle on the full levels held by this CTA (the
-// same sweeps as k_mg_cta_cycle in mg.cu): f of level 2 must be in place;
-// leaves the corrected, post-smoothed level-2 correction in its e.
+// same sweeps as k_mg_cta_cycle in mg.cu, red and black in separate passes):
+// f of level 3 must be in place; leaves the corrected, post-smoothed level-3
+// correction in its e.
 __device__ void coarse_cycle(const PArgs &A, Smem &sm) {
     const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;  // 16 rows x 32 columns of threads
     constexpr int RS = NT / 32;
     const int nlev = A.nlev;
     const float omega = A.omega;
-    for (int l = 2; l < nlev - 1; l++) {
+    for (int l = 3; l < nlev - 1; l++) {
         const int nx = A.dims[2 * l], ny = A.dims[2 * l + 1], n = nx * ny;
-        const float *D = sm.co + A.off[l], *CE = D + n, *CN = CE + n, *F = CN + n;
+        const float *D = sm.co + A.off[l], *CE = D + n, *CN = CE + n, *F = CN + n, *DI = F + 2 * n;
         float *E = sm.co + A.off[l] + 4 * n;
         for (int i = ty; i < nx; i += RS)
             for (int j = tx; j < ny; j += 32) {
                 const int k = j + ny * i;
-                if (((i + j) & 1) == 0) {
-                    E[k] = F[k] / D[k];
-                } else {
-                    float acc = F[k];
-                    if (i > 0) acc += CE[k - ny] * (F[k - ny] / D[k - ny]);
-                    if (i < nx - 1) acc += CE[k] * (F[k + ny] / D[k + ny]);
-                    if (j > 0) acc += CN[k - 1] * (F[k - 1] / D[k - 1]);
-                    if (j < ny - 1) acc += CN[k] * (F[k + 1] / D[k + 1]);
-                    E[k] = acc / D[k];
-                }
+                E[k] = (((i + j) & 1) == 0) ? F[k] * DI[k] : 0.0f;
+            }
+        __syncthreads();
+        for (int i = ty; i < nx; i += RS)
+            for (int j = 2 * tx + ((i + 1) & 1); j < ny; j += 64) {
+                const int k = j + ny * i;
+                float acc = F[k];
+                if (i > 0) acc += CE[k - ny] * E[k - ny];
+                if (i < nx - 1) acc += CE[k] * E[k + ny];
+                if (j > 0) acc += CN[k - 1] * E[k - 1];
+                if (j < ny - 1) acc += CN[k] * E[k + 1];
+                E[k] = acc * DI[k];
             }
         __syncthreads();
         const int cnx = A.dims[2 * l + 2], cny = A.dims[2 * l + 3];
@@ -346,87 +397,60 @@ __device__ void coarse_cycle(const PArgs &A, Smem &sm) {
         if (row < n && c == 0) E[row] = (float)acc;
         __syncthreads();
     }
-    for (int l = nlev - 2; l >= 2; l--) {
+    for (int l = nlev - 2; l >= 3; l--) {
         const int nx = A.dims[2 * l], ny = A.dims[2 * l + 1], n = nx * ny;
         const int cny = A.dims[2 * l + 3], cn = A.dims[2 * l + 2] * cny;
-        const float *D = sm.co + A.off[l], *CE = D + n, *CN = CE + n, *F = CN + n;
+        const float *D = sm.co + A.off[l], *CE = D + n, *CN = CE + n, *F = CN + n, *DI = F + 2 * n;
         float *E = sm.co + A.off[l] + 4 * n;
         const float *Ec = sm.co + A.off[l + 1] + 4 * cn;
-        auto pe = [&](int k, int i, int j) { return E[k] + omega * Ec[(j >> 1) + cny * (i >> 1)]; };
+        (void)D;
         for (int i = ty; i < nx; i += RS)
-            for (int j = 2 * tx + ((i + 1) & 1); j < ny; j += 64) {
+            for (int j = tx; j < ny; j += 32) {
                 const int k = j + ny * i;
-                float acc = F[k];
-                if (i > 0) acc += CE[k - ny] * pe(k - ny, i - 1, j);
-                if (i < nx - 1) acc += CE[k] * pe(k + ny, i + 1, j);
-                if (j > 0) acc += CN[k - 1] * pe(k - 1, i, j - 1);
-                if (j < ny - 1) acc += CN[k] * pe(k + 1, i, j + 1);
-                E[k] = acc / D[k];
+                E[k] += omega * Ec[(j >> 1) + cny * (i >> 1)];
             }
         __syncthreads();
-        for (int i = ty; i < nx; i += RS)
-            for (int j = 2 * tx + (i & 1); j < ny; j += 64) {
-                const int k = j + ny * i;
-                float acc = F[k];
-                if (i > 0) acc += CE[k - ny] * E[k - ny];
-                if (i < nx - 1) acc += CE[k] * E[k + ny];
-                if (j > 0) acc += CN[k - 1] * E[k - 1];
-                if (j < ny - 1) acc += CN[k] * E[k + 1];
-                E[k] = acc / D[k];
-            }
-        __syncthreads();
+        for (int pass = 1; pass >= 0; pass--) {  // black (i + j odd), then red
+            for (int i = ty; i < nx; i += RS)
+                for (int j = 2 * tx + ((i + pass) & 1); j < ny; j += 64) {
+                    const int k = j + ny * i;
+                    float acc = F[k];
+                    if (i > 0) acc += CE[k - ny] * E[k - ny];
+                    if (i < nx - 1) acc += CE[k] * E[k + ny];
+                    if (j > 0) acc += CN[k - 1] * E[k - 1];
+                    if (j < ny - 1) acc += CN[k] * E[k + 1];
+                    E[k] = acc * DI[k];
+                }
+            __syncthreads();
+        }
     }
-}
-
-// Post-smoothing of level 1 on the level-1 tile + 1 (prolongation of the
-// level-2 correction with omega on +3, black on +2, red on +1), in sm.e1.
-__device__ void l1_post(const PArgs &A, Smem &sm, int I0, int J0) {
-    const int tid = threadIdx.x, n1x = A.dims[2], n1y = A.dims[3], n2y = A.dims[5];
-    const float *E2 = sm.co + A.off[2] + 4 * A.dims[4] * n2y;
-    for (int t = tid; t < (R1I - 4) * (R1J - 4); t += NT) {
-        const int a = 2 + t / (R1J - 4), b = 2 + t % (R1J - 4), I = I0 - R1 + a, J = J0 - R1 + b;
-        if (I >= 0 && I < n1x && J >= 0 && J < n1y) sm.e1[a][b] += A.omega * E2[(J >> 1) + n2y * (I >> 1)];
-    }
-    __syncthreads();
-    for (int t = tid; t < (R1I - 6) * (R1J - 6); t += NT) {
-        const int a = 3 + t / (R1J - 6), b = 3 + t % (R1J - 6), I = I0 - R1 + a, J = J0 - R1 + b;
-        if (((I + J) & 1) == 1 && I >= 0 && I < n1x && J >= 0 && J < n1y)
-            sm.e1[a][b] = gs<R1J>(sm.f1, sm.d1, sm.ce1, sm.cn1, sm.e1, a, b);
-    }
-    __syncthreads();
-    for (int t = tid; t < (R1I - 8) * (R1J - 8); t += NT) {
-        const int a = 4 + t / (R1J - 8), b = 4 + t % (R1J - 8), I = I0 - R1 + a, J = J0 - R1 + b;
-        if (((I + J) & 1) == 0 && I >= 0 && I < n1x && J >= 0 && J < n1y)
-            sm.e1[a][b] = gs<R1J>(sm.f1, sm.d1, sm.ce1, sm.cn1, sm.e1, a, b);
-    }
-    __syncthreads();
 }
 
 // Post-smoothing of level 0 on the tile: the neighbours' pre-smoothed e0 on
-// the tile + 2, prolongation of the level-1 correction (sm.e1 on the level-1
-// tile + 1) with omega, black on +1, red on the tile -> z (FP64; 0 at the
-// pinned cell) and the sums z.r, z.q of the tile.
+// the tile + 2, prolongation of the level-1 correction (sm.l1.e on the
+// level-1 tile + 1) with omega, black on +1, red on the tile -> z (FP64; 0 at
+// the pinned cell) and the sums z.r, z.q of the tile.
 __device__ void l0_post(const PArgs &A, Smem &sm, int i0, int j0, double (&acc)[2]) {
-    const int tid = threadIdx.x, nx = A.nx, ny = A.ny, I0 = i0 / 2 - R1, J0 = j0 / 2 - R1;
+    const int tid = threadIdx.x, nx = A.nx, ny = A.ny, I0 = i0 / 2 - Lev1::H, J0 = j0 / 2 - Lev1::H;
     for (int t = tid; t < H2I * H2J; t += NT) {
         const int a = t / H2J, b = t % H2J, i = i0 - 2 + a, j = j0 - 2 + b;
         float e = 0.0f;
         if (i >= 0 && i < nx && j >= 0 && j < ny)
-            e = __ldcg(A.e0g + (int64_t)j + (int64_t)ny * i) + A.omega * sm.e1[(i >> 1) - I0][(j >> 1) - J0];
+            e = __ldcg(A.e0g + (int64_t)j + (int64_t)ny * i) + A.omega * sm.l1.e[(i >> 1) - I0][(j >> 1) - J0];
         sm.e0[a][b] = e;
     }
     __syncthreads();
     for (int t = tid; t < (H2I - 2) * (H2J - 2); t += NT) {
         const int a = 1 + t / (H2J - 2), b = 1 + t % (H2J - 2), i = i0 - 2 + a, j = j0 - 2 + b;
         if (((i + j) & 1) == 1 && i >= 0 && i < nx && j >= 0 && j < ny)
-            sm.e0[a][b] = gs<H2J>(sm.f0, sm.d0, sm.ce0, sm.cn0, sm.e0, a, b);
+            sm.e0[a][b] = gs<H2J>(sm.f0, sm.di0, sm.ce0, sm.cn0, sm.e0, a, b);
     }
     __syncthreads();
     acc[0] = acc[1] = 0.0;
     const int ta = tid / PTJ, tb = tid % PTJ, a = 2 + ta, b = 2 + tb, i = i0 + ta, j = j0 + tb;
     if (i < nx && j < ny) {
         float e = sm.e0[a][b];
-        if (((i + j) & 1) == 0) e = gs<H2J>(sm.f0, sm.d0, sm.ce0, sm.cn0, sm.e0, a, b);
+        if (((i + j) & 1) == 0) e = gs<H2J>(sm.f0, sm.di0, sm.ce0, sm.cn0, sm.e0, a, b);
         const int64_t k = (int64_t)j + (int64_t)ny * i;
         const double z = (A.S.pinned && k == 0) ? 0.0 : (double)e;
         __stcg(A.z + k, z);
@@ -452,89 +476,96 @@ __device__ void setup_local(const PArgs &A, Smem &sm, int i0, int j0) {
             cn = (j < ny - 1 && !pin0) ? (float)S.cn[k] : 0.0f;
         }
         sm.d0[a][b] = d;
+        sm.di0[a][b] = 1.0f / d;
         sm.ce0[a][b] = ce;
         sm.cn0[a][b] = cn;
     }
     __syncthreads();
-    // level 1 of the tile (into the middle of the level-1 arrays), then level 2
+    // the tile's level-1 cells (into the middle of sm.l1), then its level-2 cells
     const int n1x = A.dims[2], n1y = A.dims[3];
-    if (tid < C1I * C1J) {
-        const int ci = tid / C1J, cj = tid % C1J, I = i0 / 2 + ci, J = j0 / 2 + cj;
+    constexpr int H1 = Lev1::H;
+    if (tid < Lev1::CI * Lev1::CJ) {
+        const int ci = tid / Lev1::CJ, cj = tid % Lev1::CJ, I = i0 / 2 + ci, J = j0 / 2 + cj;
         float cd = 1.0f, cce = 0.0f, ccn = 0.0f;
         if (I < n1x && J < n1y) {
-            // fine cell (i, j) of the tile at sm index (i - i0 + 2, j - j0 + 2)
             auto fd = [&](int i, int j) { return sm.d0[i - i0 + 2][j - j0 + 2]; };
             auto fe = [&](int i, int j) { return sm.ce0[i - i0 + 2][j - j0 + 2]; };
             auto fn = [&](int i, int j) { return sm.cn0[i - i0 + 2][j - j0 + 2]; };
             coarsen_cell(nx, ny, I, J, fd, fe, fn, cd, cce, ccn);
             const int64_t k = (int64_t)J + (int64_t)n1y * I;
-            __stcg(A.d1g + k, cd);
-            __stcg(A.ce1g + k, cce);
-            __stcg(A.cn1g + k, ccn);
+            __stcg(A.lg[1][0] + k, cd);
+            __stcg(A.lg[1][1] + k, cce);
+            __stcg(A.lg[1][2] + k, ccn);
         }
-        sm.d1[R1 + ci][R1 + cj] = cd;
-        sm.ce1[R1 + ci][R1 + cj] = cce;
-        sm.cn1[R1 + ci][R1 + cj] = ccn;
+        sm.l1.d[H1 + ci][H1 + cj] = cd;
+        sm.l1.ce[H1 + ci][H1 + cj] = cce;
+        sm.l1.cn[H1 + ci][H1 + cj] = ccn;
     }
     __syncthreads();
     const int n2x = A.dims[4], n2y = A.dims[5];
-    if (tid < C2I * C2J) {
-        const int ci = tid / C2J, cj = tid % C2J, I = i0 / 4 + ci, J = j0 / 4 + cj;
+    if (tid < Lev2::CI * Lev2::CJ) {
+        const int ci = tid / Lev2::CJ, cj = tid % Lev2::CJ, I = i0 / 4 + ci, J = j0 / 4 + cj;
         if (I < n2x && J < n2y) {
             const int I0 = i0 / 2, J0 = j0 / 2;
-            auto fd = [&](int i, int j) { return sm.d1[i - I0 + R1][j - J0 + R1]; };
-            auto fe = [&](int i, int j) { return sm.ce1[i - I0 + R1][j - J0 + R1]; };
-            auto fn = [&](int i, int j) { return sm.cn1[i - I0 + R1][j - J0 + R1]; };
+            auto fd = [&](int i, int j) { return sm.l1.d[i - I0 + H1][j - J0 + H1]; };
+            auto fe = [&](int i, int j) { return sm.l1.ce[i - I0 + H1][j - J0 + H1]; };
+            auto fn = [&](int i, int j) { return sm.l1.cn[i - I0 + H1][j - J0 + H1]; };
             float cd, cce, ccn;
             coarsen_cell(n1x, n1y, I, J, fd, fe, fn, cd, cce, ccn);
             const int64_t k = (int64_t)J + (int64_t)n2y * I;
-            __stcg(A.d2g + k, cd);
-            __stcg(A.ce2g + k, cce);
-            __stcg(A.cn2g + k, ccn);
+            __stcg(A.lg[2][0] + k, cd);
+            __stcg(A.lg[2][1] + k, cce);
+            __stcg(A.lg[2][2] + k, ccn);
         }
     }
 }
 
-// After the level-1/2 operators are complete: this CTA's level-1 operator on
-// the level-1 tile + 5, the full level 2 and the coarser levels built here.
-__device__ void setup_coarse(const PArgs &A, Smem &sm, int i0, int j0) {
-    const int tid = threadIdx.x, n1x = A.dims[2], n1y = A.dims[3];
-    const int I0 = i0 / 2 - R1, J0 = j0 / 2 - R1;
-    for (int t = tid; t < R1I * R1J; t += NT) {
-        const int a = t / R1J, b = t % R1J, I = I0 + a, J = J0 + b;
+// A distributed level's operator on the CTA's cells + H from global memory.
+template <class L> __device__ void load_dist_op(const PArgs &A, L &v, int l, int I0, int J0) {
+    const int nx = A.dims[2 * l], ny = A.dims[2 * l + 1];
+    for (int t = threadIdx.x; t < L::RI * L::RJ; t += NT) {
+        const int a = t / L::RJ, b = t % L::RJ, I = I0 - L::H + a, J = J0 - L::H + b;
         float d = 1.0f, ce = 0.0f, cn = 0.0f;
-        if (I >= 0 && I < n1x && J >= 0 && J < n1y) {
-            const int64_t k = (int64_t)J + (int64_t)n1y * I;
-            d = __ldcg(A.d1g + k);
-            ce = __ldcg(A.ce1g + k);
-            cn = __ldcg(A.cn1g + k);
+        if (I >= 0 && I < nx && J >= 0 && J < ny) {
+            const int64_t k = (int64_t)J + (int64_t)ny * I;
+            d = __ldcg(A.lg[l][0] + k);
+            ce = __ldcg(A.lg[l][1] + k);
+            cn = __ldcg(A.lg[l][2] + k);
         }
-        sm.d1[a][b] = d;
-        sm.ce1[a][b] = ce;
-        sm.cn1[a][b] = cn;
+        v.d[a][b] = d;
+        v.di[a][b] = 1.0f / d;
+        v.ce[a][b] = ce;
+        v.cn[a][b] = cn;
     }
-    {
-        const int n2 = A.dims[4] * A.dims[5];
-        float *D = sm.co + A.off[2], *CE = D + n2, *CN = CE + n2;
-        for (int k = tid; k < n2; k += NT) {
-            D[k] = __ldcg(A.d2g + k);
-            CE[k] = __ldcg(A.ce2g + k);
-            CN[k] = __ldcg(A.cn2g + k);
-        }
-    }
-    __syncthreads();
+}
+
+// After the level-1/2 operators are complete: the CTA's parts of levels 1
+// and 2, level 3 aggregated from the global level 2, and the coarser levels
+// built here (all with reciprocal diagonals).
+__device__ void setup_coarse(const PArgs &A, Smem &sm, int i0, int j0) {
+    const int tid = threadIdx.x;
+    load_dist_op(A, sm.l1, 1, i0 / 2, j0 / 2);
+    load_dist_op(A, sm.l2, 2, i0 / 4, j0 / 4);
     for (int l = 3; l < A.nlev; l++) {
         const int fnx = A.dims[2 * l - 2], fny = A.dims[2 * l - 1], fn = fnx * fny;
-        const int cnx = A.dims[2 * l], cny = A.dims[2 * l + 1], cn = cnx * cny;
-        const float *FD = sm.co + A.off[l - 1], *FE = FD + fn, *FN = FE + fn;
-        float *D = sm.co + A.off[l], *CE = D + cn, *CN = CE + cn;
-        (void)cnx;
+        const int cny = A.dims[2 * l + 1], cn = A.dims[2 * l] * cny;
+        float *D = sm.co + A.off[l], *CE = D + cn, *CN = CE + cn, *DI = CN + 3 * cn;
         for (int k = tid; k < cn; k += NT) {
             const int I = k / cny, J = k % cny;
-            auto fd = [&](int i, int j) { return FD[j + fny * i]; };
-            auto fe = [&](int i, int j) { return FE[j + fny * i]; };
-            auto fnn = [&](int i, int j) { return FN[j + fny * i]; };
-            coarsen_cell(fnx, fny, I, J, fd, fe, fnn, D[k], CE[k], CN[k]);
+            if (l == 3) {
+                const float *FD = A.lg[2][0], *FE = A.lg[2][1], *FN = A.lg[2][2];
+                auto fd = [&](int i, int j) { return __ldcg(FD + j + fny * i); };
+                auto fe = [&](int i, int j) { return __ldcg(FE + j + fny * i); };
+                auto fnn = [&](int i, int j) { return __ldcg(FN + j + fny * i); };
+                coarsen_cell(fnx, fny, I, J, fd, fe, fnn, D[k], CE[k], CN[k]);
+            } else {
+                const float *FD = sm.co + A.off[l - 1], *FE = FD + fn, *FN = FE + fn;
+                auto fd = [&](int i, int j) { return FD[j + fny * i]; };
+                auto fe = [&](int i, int j) { return FE[j + fny * i]; };
+                auto fnn = [&](int i, int j) { return FN[j + fny * i]; };
+                coarsen_cell(fnx, fny, I, J, fd, fe, fnn, D[k], CE[k], CN[k]);
+            }
+            DI[k] = 1.0f / D[k];
         }
         __syncthreads();
     }
@@ -643,17 +674,26 @@ __global__ void __launch_bounds__(NT, 1) k_mgfcg_persist(PArgs A) {
     }
     // ---- iterations: rest of the V-cycle (levels 1.., z, beta), then A, B ----
     while (ok && !done) {
-        l1_pre(A, sm, i0 / 2, j0 / 2);
+        dist_pre(A, sm.l1, 1, i0 / 2, j0 / 2);
         ok = gsync(A, sm, epoch);  // level-2 rhs complete
         if (!ok) break;
+        dist_pre(A, sm.l2, 2, i0 / 4, j0 / 4);
+        ok = gsync(A, sm, epoch);  // level-3 rhs complete
+        if (!ok) break;
         {
-            const int n2 = A.dims[4] * A.dims[5];
-            float *F2 = sm.co + A.off[2] + 3 * n2;
-            for (int k = tid; k < n2; k += NT) F2[k] = __ldcg(A.f2g + k);
+            const int n3 = A.dims[6] * A.dims[7];
+            float *F3 = sm.co + A.off[3] + 3 * n3;
+            for (int k = tid; k < n3; k += NT) F3[k] = __ldcg(A.lg[3][3] + k);
             __syncthreads();
         }
         coarse_cycle(A, sm);
-        l1_post(A, sm, i0 / 2, j0 / 2);
+        {
+            const int n3x = A.dims[6], n3y = A.dims[7];
+            const float *E3 = sm.co + A.off[3] + 4 * n3x * n3y;
+            dist_post<2>(A, sm.l2, 2, i0 / 4, j0 / 4, [&](int I, int J) { return E3[J + n3y * I]; });
+            const int I2 = i0 / 4 - Lev2::H, J2 = j0 / 4 - Lev2::H;
+            dist_post<1>(A, sm.l1, 1, i0 / 2, j0 / 2, [&](int I, int J) { return sm.l2.e[I - I2][J - J2]; });
+        }
         {
             double acc[2];
             l0_post(A, sm, i0, j0, acc);
@@ -824,7 +864,7 @@ __global__ void __launch_bounds__(NT, 1) k_mgfcg_persist(PArgs A) {
 
 // ------------------------------------------------------------------ host --
 static bool persist_shape(const MgLevel *lv, int nlev, int nx, int ny, PArgs &A) {
-    if (nlev < 3 || nlev > MG_MAX_LEVELS) return false;
+    if (nlev < 4 || nlev > MG_MAX_LEVELS) return false;
     const int nti = (nx + PTI - 1) / PTI, ntj = (ny + PTJ - 1) / PTJ;
     A.nx = nx;
     A.ny = ny;
@@ -836,13 +876,14 @@ static bool persist_shape(const MgLevel *lv, int nlev, int nx, int ny, PArgs &A)
         A.dims[2 * l] = lv[l].nx;
         A.dims[2 * l + 1] = lv[l].ny;
         A.off[l] = 0;
-        if (l >= 2) {
+        if (l >= 3) {
             A.off[l] = off;
-            off += 5 * lv[l].nx * lv[l].ny;
+            off += 6 * lv[l].nx * lv[l].ny;
         }
+        if (l >= 1 && (lv[l].nx != (lv[l - 1].nx + 1) / 2 || lv[l].ny != (lv[l - 1].ny + 1) / 2)) return false;
     }
     const int last = lv[nlev - 1].nx * lv[nlev - 1].ny;
-    return off <= 5 * CMAX && last <= NINV && lv[1].nx == (nx + 1) / 2 && lv[1].ny == (ny + 1) / 2;
+    return off <= 6 * CMAX && last <= NINV;
 }
 
 bool mg_persist_enabled() {
@@ -897,14 +938,12 @@ bool launch_mg_persist(const Sys &S, int nx, int ny, const MgLevel *lv, int nlev
     A.pbuf1 = p1;
     A.z = z;
     A.e0g = lv[0].e;
-    A.d1g = lv[1].diag;
-    A.ce1g = lv[1].ce;
-    A.cn1g = lv[1].cn;
-    A.f1g = lv[1].f;
-    A.d2g = lv[2].diag;
-    A.ce2g = lv[2].ce;
-    A.cn2g = lv[2].cn;
-    A.f2g = lv[2].f;
+    for (int l = 1; l <= 3; l++) {
+        A.lg[l][0] = lv[l].diag;
+        A.lg[l][1] = lv[l].ce;
+        A.lg[l][2] = lv[l].cn;
+        A.lg[l][3] = lv[l].f;
+    }
     A.inv = inv;
     A.partial = partial;
     A.bar = bar;

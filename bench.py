@@ -59,6 +59,10 @@ MG_BYTES_PER_UNKNOWN_ITER = 180
 # 5 iterations (35 launches) of the bench's own solve: 2.3 KB read and 4.56 MB
 # written in total
 MG_ITER_DRAM_BYTES_256 = 913408
+# the same for the one-launch solve (k_mgfcg_persist): DRAM bytes of one
+# launch divided by its iterations, from the ncu capture summarised in
+# profiles/mgfcg_persist_256.md (None until captured)
+MG_PERSIST_DRAM_BYTES_PER_ITER_256 = None
 
 
 def metric_name():
@@ -784,6 +788,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
+    one_launch = s.last_solve_one_launch()
     true_res = s.true_residual()
     if not true_res <= 10 * TOL:
         raise SystemExit(f"bench: true relative residual {true_res:.3e} above {10 * TOL:g}")
@@ -871,9 +876,13 @@ def run_ours(args):
                if not args.no_extra else None)
     bsteps = batched_steps(sh, stream) if not args.no_extra else None
     fsteps = full_steps_256(sh, stream) if not args.no_extra else None
-    nlev = len(_mg_levels(args.n, args.n))
-    per_iter = 2 + 2 * (nlev - 1) + 1
-    launches = int(sum(4 + (1 + nlev) + (1 + per_iter - 2) + 8 * per_iter * math.ceil(i / 8) + 3 for i in iters))
+    if one_launch:
+        # per solve: dt, curvature, P ghost fill, k_assemble; dt, solver scalars, k_mgfcg_persist, ps and p
+        launches = 9 * args.steps
+    else:
+        nlev = len(_mg_levels(args.n, args.n))
+        per_iter = 2 + 2 * (nlev - 1) + 1
+        launches = int(sum(4 + (1 + nlev) + (1 + per_iter - 2) + 8 * per_iter * math.ceil(i / 8) + 3 for i in iters))
 
     line = {
         "metric": metric_name(),
@@ -890,7 +899,8 @@ def run_ours(args):
         "data": "synthetic",
         "config": headline_config(args.n, world),
         "solver": "mixed precision: FP64 flexible CG + FP32 multigrid V(1,1) preconditioner "
-                  "(Galerkin 2x2 aggregation, fused red-black GS tiles)",
+                  "(Galerkin 2x2 aggregation, red-black GS), " +
+                  ("the whole solve as one cooperative kernel launch" if one_launch else "per-phase kernels"),
         "solver_iters_mean": it_mean,
         "fp64_cg": {"value": cg_value, "unit": "GFM Poisson solves/s", "iters_mean": float(np.mean(cg_iters)),
                     "solver": "FP64 Jacobi-PCG, one thread-block-cluster launch per solve"},
@@ -900,13 +910,14 @@ def run_ours(args):
         "ls_config": {"workload": f"{LS_GRID}x{LS_GRID} perturbed circle, WENO5/TVD-RK3 + 5 MinRK2 subcell "
                                   "pseudo-steps with the Sussman constraint, FP64", "ms_per_step": t_ls * 1e3},
         "ls_cpu_baseline": ls_cpu_baseline() if rank == 0 and not args.no_cpu else None,
-        "roofline": {"bound": "hbm", "kernel": "MG-FCG iteration (k_fcg_a, k_fcg_b, k_mg_pre/post, k_mg_coarse)",
+        "roofline": {"bound": "hbm",
+                     "kernel": ("k_mgfcg_persist (the whole MG-FCG solve, one cooperative launch)" if one_launch
+                                else "MG-FCG iteration (k_fcg_a, k_fcg_b, k_mg_pre/post, k_mg_cta_cycle)"),
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": MG_ITER_DRAM_BYTES_256 if args.n == 256 else None,
-                     "traffic_note": "DRAM bytes read + written per FCG iteration (its 7 launches), one ncu "
-                                     "capture of 5 iterations with --cache-control none: "
-                                     "the level hierarchy stays in L2, "
-                                     "what reaches DRAM is L2 write-back",
+                     "traffic": (MG_PERSIST_DRAM_BYTES_PER_ITER_256 if one_launch else MG_ITER_DRAM_BYTES_256)
+                     if args.n == 256 else None,
+                     "traffic_note": "DRAM bytes read + written per FCG iteration from one ncu capture of the "
+                                     "solve (--cache-control none); the hierarchy stays in L2",
                      "bytes_per_unknown_iter": MG_BYTES_PER_UNKNOWN_ITER,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback",
                      "note": "working set is L2-resident at 256^2; iteration time from CUDA events "

@@ -60,7 +60,7 @@ def test_batch_matches_sessions():
             if k == 3:
                 assert r["iters"][k] == 0 and np.abs(interior(ps)).max() == 0.0
                 continue
-            assert abs(int(r["iters"][k]) - rs["iters"]) <= 8, (k, r["iters"][k], rs["iters"])
+            assert abs(int(r["iters"][k]) - rs["iters"]) <= 2, (k, r["iters"][k], rs["iters"])
             scale = np.abs(interior(ps_ref)).max()
             assert np.abs(interior(ps) - interior(ps_ref)).max() <= 1e-7 * scale, k
             np.testing.assert_allclose(interior(p), interior(ps) / dts[k], rtol=1e-15)

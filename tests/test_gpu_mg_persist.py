@@ -59,7 +59,8 @@ def _solve(g, f, ls, div, flags, tol=1e-10, maxit=1000, zero_rhs=False):
 
 
 @pytest.mark.parametrize("nx,ny,bc", [(256, 256, "neumann"), (96, 80, "neumann"), (200, 250, "dirichlet"),
-                                      (33, 47, "neumann"), (130, 66, "dirichlet"), (32, 16, "neumann")])
+                                      (33, 47, "neumann"), (130, 66, "dirichlet"), (48, 40, "neumann"),
+                                      (256, 288, "dirichlet")])
 def test_one_launch_matches_multi_kernel_and_oracle(nx, ny, bc):
     g, f, ls, div = _case(nx, ny, bc)
     a = _solve(g, f, ls, div, 0)
