@@ -907,7 +907,7 @@ static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters
         if (rc0) return rc0;
         // systems up to about 256^2: the whole solve as one cooperative launch
         if (mg_persist_enabled() && !(s->prm.solver_flags & ASD2G_FLAG_NO_PERSIST_MG) &&
-            launch_mg_persist(s->sys, g.nx, g.ny, s->lv, s->nlev, s->x, s->r, s->q, s->pa, s->pb, s->z, s->coarse_inv,
+            launch_mg_persist(s->sys, g.nx, g.ny, s->lv, s->nlev, s->x, s->r, s->q, s->pa, s->pb, s->z,
                               s->mg_partial, s->mg_partial_n, s->mgp_bar, s->ks, tol, maxit, mg_omega_value(),
                               s->st)) {
             if (stream_capturing(s)) {
@@ -1593,7 +1593,7 @@ static int capture_run_graph(asd2g_session *s, int reinit_mode, double tol, int 
         if (!rc && persist) {
             launch_set_kstate(s->ks, tol, maxit, ASD2G_SOLVER_MGPCG, 0.0, s->st);
             if (!launch_mg_persist(s->sys, s->g.nx, s->g.ny, s->lv, s->nlev, s->x, s->r, s->q, s->pa, s->pb, s->z,
-                                   s->coarse_inv, s->mg_partial, s->mg_partial_n, s->mgp_bar, s->ks, tol, maxit,
+                                   s->mg_partial, s->mg_partial_n, s->mgp_bar, s->ks, tol, maxit,
                                    mg_omega_value(), s->st))
                 rc = fail(ASD2G_E_UNSUPPORTED, "one-launch MG-FCG not available");
         } else if (!rc) {

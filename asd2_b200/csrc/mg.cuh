@@ -95,9 +95,9 @@ void launch_pc_pair(const Sys &S, int nx, int ny, const double *x, const double 
 // iter / check) as ONE cooperative launch of one CTA per 16 x 32 tile, for
 // systems whose tiles fit the GPU at once and whose levels from 3 down fit
 // one CTA's shared memory (up to about 256 x 256).  x receives the solution;
-// r0/r1 and p0/p1 are two n-vectors each, z one; inv holds the coarsest
-// inverse; partial at least 4 doubles per tile; bar two words (zeroed by the
-// launch).  KState receives it, res, status (-8: a grid-barrier wait gave
+// r0/r1 and p0/p1 are two n-vectors each, z one; partial at least 4
+// doubles per tile; bar two words (zeroed by the launch).  The levels'
+// diag/ce/cn/f arrays of levels 1-3 and level 0's e serve as work space.  KState receives it, res, status (-8: a grid-barrier wait gave
 // up, the solve did not finish) and done.  Returns false (nothing launched)
 // when the system does not fit or the device cannot co-schedule the grid.
 bool mg_persist_enabled();
@@ -107,7 +107,7 @@ bool mg_persist_prepare();
 // Whether launch_mg_persist would launch for this hierarchy (no launch).
 bool mg_persist_fits(const MgLevel *lv, int nlev, int nx, int ny, int64_t partial_len);
 bool launch_mg_persist(const Sys &S, int nx, int ny, const MgLevel *lv, int nlev, double *x, double *r0, double *r1,
-                       double *p0, double *p1, double *z, double *inv, double *partial, int64_t partial_len,
+                       double *p0, double *p1, double *z, double *partial, int64_t partial_len,
                        unsigned *bar, KState *ks, double tol, int maxit, float omega, cudaStream_t st);
 size_t mg_persist_smem();
 // The V-cycle's over-relaxation of the coarse-grid correction (mg.cu).

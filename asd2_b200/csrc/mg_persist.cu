@@ -89,6 +89,7 @@ struct Smem {
     double q[H2I][H2J];        // A p on the tile + 2
     double r[H2I][H2J];        // residual on the tile + 2
     double inv[NINV * NINV];   // coarsest inverse (row-major, stride NINV)
+    double piv_row[2][NINV], piv_col[2][NINV];  // Gauss-Jordan pivot row / column (double-buffered)
     double red[4][NT / 32];    // per-warp partial sums
     double tot[4];             // reduced sums (the same in every CTA)
     float d0[H2I][H2J], di0[H2I][H2J], ce0[H2I][H2J], cn0[H2I][H2J], f0[H2I][H2J], e0[H2I][H2J];  // level 0
@@ -107,7 +108,6 @@ struct PArgs {
     double *x, *rbuf0, *rbuf1, *pbuf0, *pbuf1, *z;
     float *e0g;                          // level-0 pre-smoothed correction
     float *lg[4][4];                     // levels 1..3: [l][0..3] = diag, ce, cn, f (global)
-    double *inv;                         // coarsest inverse (written by CTA 0)
     double *partial;                     // 4 slots per CTA
     unsigned *bar;                       // [0] arrivals, [1] error word
     KState *ks;
@@ -571,49 +571,65 @@ __device__ void setup_coarse(const PArgs &A, Smem &sm, int i0, int j0) {
     }
 }
 
-// Dense inverse of the coarsest operator (SPD, <= 64 cells) by in-place
-// Gauss-Jordan without pivoting, FP64, in sm.inv; written to A.inv.  Each
-// step reads the old pivot row and column, then every entry is replaced.
+// 1/x in FP64: the hardware approximation refined by two Newton steps
+// (each squares the relative error: 2^-20 -> 2^-40 -> below FP64 rounding).
+__device__ __forceinline__ double recip64(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    r = fma(r, fma(-x, r, 1.0), r);
+    return fma(r, fma(-x, r, 1.0), r);
+}
+
+// Dense inverse of the coarsest operator (SPD, <= 64 cells) in sm.inv,
+// computed by every CTA: Gauss-Jordan without pivoting in FP64 with the
+// matrix held in registers (thread -> row tid >> 3, columns (tid & 7) + 8 m).
+// Each pivot step publishes only the pivot row and column through small
+// double-buffered shared arrays (one barrier per step): streaming the whole
+// 64 x 64 matrix through shared memory at every step made it bound by
+// shared-memory bandwidth (about 1 us per step).
 __device__ void coarsest_inverse(const PArgs &A, Smem &sm) {
     const int tid = threadIdx.x, l = A.nlev - 1, nx = A.dims[2 * l], ny = A.dims[2 * l + 1], n = nx * ny;
     const float *D = sm.co + A.off[l], *CE = D + n, *CN = CE + n;
-    double *M = sm.inv;
-    for (int t = tid; t < NINV * NINV; t += NT) M[t] = 0.0;
-    __syncthreads();
-    if (tid < n) {
-        const int i = tid / ny, j = tid % ny;
-        M[tid * NINV + tid] = D[tid];
-        if (i < nx - 1) M[tid * NINV + tid + ny] = M[(tid + ny) * NINV + tid] = -(double)CE[tid];
-        if (j < ny - 1) M[tid * NINV + tid + 1] = M[(tid + 1) * NINV + tid] = -(double)CN[tid];
-    }
-    __syncthreads();
-    // thread -> row tid >> 3, columns (tid & 7) + 8 m
     const int row = tid >> 3, c0 = tid & 7;
-    for (int k = 0; k < n; k++) {
-        double nv[NINV / 8];
-        const double rp = 1.0 / M[k * NINV + k];
-        if (row < n) {
-            const double fik = M[row * NINV + k];
+    double a[NINV / 8];
 #pragma unroll
-            for (int m = 0; m < NINV / 8; m++) {
-                const int c = c0 + 8 * m;
-                double v = 0.0;
-                if (c < n) {
-                    if (row == k) v = (c == k) ? rp : M[k * NINV + c] * rp;
-                    else if (c == k) v = -fik * rp;
-                    else v = M[row * NINV + c] - fik * (M[k * NINV + c] * rp);
-                }
-                nv[m] = v;
-            }
+    for (int m = 0; m < NINV / 8; m++) {
+        const int c = c0 + 8 * m;
+        double v = 0.0;
+        if (row < n && c < n) {
+            const int lo = row < c ? row : c, hi = row < c ? c : row;
+            if (c == row) v = D[row];
+            else if (hi - lo == ny) v = -(double)CE[lo];
+            else if (hi - lo == 1 && (hi % ny) != 0) v = -(double)CN[lo];
         }
-        __syncthreads();
-        if (row < n)
+        a[m] = v;
+    }
+    for (int k = 0; k < n; k++) {
+        double *prow = sm.piv_row[k & 1], *pcol = sm.piv_col[k & 1];
+        if (row == k)
+#pragma unroll
+            for (int m = 0; m < NINV / 8; m++) prow[c0 + 8 * m] = a[m];
+        if (c0 == (k & 7)) {
 #pragma unroll
             for (int m = 0; m < NINV / 8; m++)
-                if (c0 + 8 * m < n) M[row * NINV + c0 + 8 * m] = nv[m];
+                if (m == (k >> 3)) pcol[row] = a[m];
+        }
         __syncthreads();
+        const double rp = recip64(prow[k]), fik = pcol[row];
+#pragma unroll
+        for (int m = 0; m < NINV / 8; m++) {
+            const int c = c0 + 8 * m;
+            const double bk = prow[c];
+            if (row == k) a[m] = (c == k) ? rp : bk * rp;
+            else if (c == k) a[m] = -fik * rp;
+            else a[m] = a[m] - fik * (bk * rp);
+        }
     }
-    for (int t = tid; t < n * NINV; t += NT) __stcg(A.inv + t, M[t]);
+    if (row < n)
+#pragma unroll
+        for (int m = 0; m < NINV / 8; m++)
+            if (c0 + 8 * m < n) sm.inv[row * NINV + c0 + 8 * m] = a[m];
+    __syncthreads();
 }
 
 __global__ void __launch_bounds__(NT, 1) k_mgfcg_persist(PArgs A) {
@@ -655,11 +671,8 @@ __global__ void __launch_bounds__(NT, 1) k_mgfcg_persist(PArgs A) {
     }
     if (ok && !done) {
         setup_coarse(A, sm, i0, j0);
-        if (blockIdx.x == 0) coarsest_inverse(A, sm);
-        ok = gsync(A, sm, epoch);
-        if (ok) {
-            const int l = A.nlev - 1, n = A.dims[2 * l] * A.dims[2 * l + 1];
-            for (int t = tid; t < n * NINV; t += NT) sm.inv[t] = __ldcg(A.inv + t);
+        coarsest_inverse(A, sm);
+        {
             // the first V-cycle's right-hand side r = b on the tile + 2; q = 0
             for (int t = tid; t < H2I * H2J; t += NT) {
                 const int a = t / H2J, b = t % H2J, i = i0 - 2 + a, j = j0 - 2 + b;
@@ -925,7 +938,7 @@ bool mg_persist_fits(const MgLevel *lv, int nlev, int nx, int ny, int64_t partia
 }
 
 bool launch_mg_persist(const Sys &S, int nx, int ny, const MgLevel *lv, int nlev, double *x, double *r0, double *r1,
-                       double *p0, double *p1, double *z, double *inv, double *partial, int64_t partial_len,
+                       double *p0, double *p1, double *z, double *partial, int64_t partial_len,
                        unsigned *bar, KState *ks, double tol, int maxit, float omega, cudaStream_t st) {
     PArgs A{};
     if (!persist_fits(lv, nlev, nx, ny, partial_len, A)) return false;
@@ -944,7 +957,6 @@ bool launch_mg_persist(const Sys &S, int nx, int ny, const MgLevel *lv, int nlev
         A.lg[l][2] = lv[l].cn;
         A.lg[l][3] = lv[l].f;
     }
-    A.inv = inv;
     A.partial = partial;
     A.bar = bar;
     A.ks = ks;
