@@ -59,10 +59,10 @@ MG_BYTES_PER_UNKNOWN_ITER = 180
 # 5 iterations (35 launches) of the bench's own solve: 2.3 KB read and 4.56 MB
 # written in total
 MG_ITER_DRAM_BYTES_256 = 913408
-# the same for the one-launch solve (k_mgfcg_persist): DRAM bytes of one
-# launch divided by its iterations, from the ncu capture summarised in
-# profiles/mgfcg_persist_256.md (None until captured)
-MG_PERSIST_DRAM_BYTES_PER_ITER_256 = None
+# the same for the one-launch solve (k_mgfcg_persist): DRAM bytes read +
+# written by one launch (2.19008 MB + 13.3 KB, 15 iterations) divided by its
+# iterations, from the ncu capture summarised in profiles/mgfcg_persist_256.md
+MG_PERSIST_DRAM_BYTES_PER_ITER_256 = 146893
 
 
 def metric_name():
