@@ -57,7 +57,7 @@ class _Params(C.Structure):
 
 EXPORTS = [
     "asd2g_version", "asd2g_last_error", "asd2g_create", "asd2g_destroy", "asd2g_sync", "asd2g_field_ptr",
-    "asd2g_upload", "asd2g_download", "asd2g_copy_field", "asd2g_fill_field", "asd2g_apply_bc",
+    "asd2g_upload", "asd2g_upload_async", "asd2g_download", "asd2g_copy_field", "asd2g_fill_field", "asd2g_apply_bc",
     "asd2g_ls_advect", "asd2g_ls_weno_rhs", "asd2g_reinit", "asd2g_subcell_eno", "asd2g_eno",
     "asd2g_sussman_constraint", "asd2g_heaviside_deriv", "asd2g_smoothed_sign", "asd2g_ls_step",
     "asd2g_kappa", "asd2g_heaviside", "asd2g_convection", "asd2g_viscosity", "asd2g_momentum_rhs",
@@ -100,6 +100,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_destroy": ([S], I), "asd2g_sync": ([S], I),
         "asd2g_field_ptr": ([S, I, C.POINTER(C.c_void_p)], I),
         "asd2g_upload": ([S, I, dp], I), "asd2g_download": ([S, I, dp], I),
+        "asd2g_upload_async": ([S, I, dp], I),
         "asd2g_copy_field": ([S, I, I], I), "asd2g_fill_field": ([S, I, D], I),
         "asd2g_apply_bc": ([S, I, C.c_char], I),
         "asd2g_ls_advect": ([S, D], I), "asd2g_ls_weno_rhs": ([S, I, I, I, I], I), "asd2g_reinit": ([S, I], I),
@@ -264,6 +265,15 @@ class Session:
         a = np.ascontiguousarray(arr, dtype=np.float64)
         assert a.shape == self.shape, (a.shape, self.shape)
         self._check(self.L.asd2g_upload(self.h, self._f(f), a))
+
+    def upload_async(self, f, arr):
+        """Queue the upload without waiting: arr must be a C-contiguous
+        float64 array of the field's shape (ideally pinned) that stays
+        unchanged until the session next synchronises."""
+        if not (isinstance(arr, np.ndarray) and arr.dtype == np.float64 and arr.flags.c_contiguous
+                and arr.shape == self.shape):
+            raise ValueError("upload_async needs a C-contiguous float64 array of the field's shape")
+        self._check(self.L.asd2g_upload_async(self.h, self._f(f), arr))
 
     def download(self, f):
         out = np.empty(self.shape)

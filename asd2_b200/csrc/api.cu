@@ -308,7 +308,7 @@ int mg_alloc(asd2g_session *s) {
     const int64_t np = mg_partial_len(s->g.nx, s->g.ny);
     if (rc == ASD2G_OK) rc = dalloc(s, &s->mg_partial, (size_t)np);
     if (rc == ASD2G_OK) {
-        if (cudaMalloc(&s->mgp_bar, 4 * sizeof(unsigned)) != cudaSuccess) {
+        if (cudaMalloc(&s->mgp_bar, 512 * sizeof(unsigned)) != cudaSuccess) {
             cudaGetLastError();
             rc = fail(ASD2G_E_NOMEM, "grid-barrier words");
         } else {
@@ -495,6 +495,13 @@ int asd2g_upload(asd2g_session *s, int field, const double *host) {
     if (cudaMemcpyAsync(s->f[field], host, sizeof(double) * s->G, cudaMemcpyHostToDevice, s->st) != cudaSuccess)
         return cuda_check("upload");
     return sync(s);
+}
+
+int asd2g_upload_async(asd2g_session *s, int field, const double *host) {
+    if (!s || !host || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field or null argument");
+    if (cudaMemcpyAsync(s->f[field], host, sizeof(double) * s->G, cudaMemcpyHostToDevice, s->st) != cudaSuccess)
+        return cuda_check("upload");
+    return ASD2G_OK;
 }
 
 int asd2g_download(asd2g_session *s, int field, double *host) {

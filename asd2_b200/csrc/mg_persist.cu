@@ -67,7 +67,8 @@ constexpr int H3I = PTI + 6, H3J = PTJ + 6;            // tile + 3
 constexpr int H2I = PTI + 4, H2J = PTJ + 4;            // tile + 2
 constexpr int CMAX = 1800;                             // cells of levels 3.. (32^2 + 16^2 + 8^2 and odd sizes)
 constexpr int NINV = MG_COARSE_CELLS;                  // coarsest level <= 64 cells
-constexpr unsigned SPIN_LIMIT = 1u << 22;              // polls before a barrier wait gives up
+static_assert(NINV == 64, "the coarsest inverse works on 8 x 8 blocks of a 64 x 64 matrix");
+constexpr unsigned SPIN_LIMIT = 1u << 22;              // polls (L2 round trips, ~0.3 us) before a wait gives up
 constexpr int STATUS_BARRIER = -8;                     // KState.status when a barrier wait gave up
 
 // A level distributed over the CTAs: the CTA's CI x CJ cells of it (the
@@ -89,7 +90,7 @@ struct Smem {
     double q[H2I][H2J];        // A p on the tile + 2
     double r[H2I][H2J];        // residual on the tile + 2
     double inv[NINV * NINV];   // coarsest inverse (row-major, stride NINV)
-    double piv_row[2][NINV], piv_col[2][NINV];  // Gauss-Jordan pivot row / column (double-buffered)
+    double gj_row[8][NINV], gj_col[NINV][8], gj_q[8][NINV], gj_p[8][8];  // block Gauss-Jordan panels
     double red[4][NT / 32];    // per-warp partial sums
     double tot[4];             // reduced sums (the same in every CTA)
     float d0[H2I][H2J], di0[H2I][H2J], ce0[H2I][H2J], cn0[H2I][H2J], f0[H2I][H2J], e0[H2I][H2J];  // level 0
@@ -122,13 +123,15 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
     return v;
 }
 
-// Grid barrier; false when the wait gave up (or another CTA's did).
+// Grid barrier; false when the wait gave up (or another CTA's did).  Thread
+// 0 arrives with a release reduction (ordering the CTA's writes, made
+// visible to it by the CTA barrier, before its arrival) and polls with
+// acquire loads; the CTA barrier after it orders the others' reads.
 __device__ bool gsync(const PArgs &A, Smem &sm, unsigned &epoch) {
     __syncthreads();
     if (threadIdx.x == 0) {
         epoch++;
-        __threadfence();
-        atomicAdd(A.bar, 1u);
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(A.bar) : "memory");
         const unsigned target = epoch * (unsigned)A.ncta;
         int good = 1;
         for (unsigned n = 0; ld_acquire(A.bar) < target; n++) {
@@ -137,9 +140,7 @@ __device__ bool gsync(const PArgs &A, Smem &sm, unsigned &epoch) {
                 good = 0;
                 break;
             }
-            __nanosleep(32);
         }
-        __threadfence();
         sm.flag = good;
     }
     __syncthreads();
@@ -581,22 +582,28 @@ __device__ __forceinline__ double recip64(double x) {
 }
 
 // Dense inverse of the coarsest operator (SPD, <= 64 cells) in sm.inv,
-// computed by every CTA: Gauss-Jordan without pivoting in FP64 with the
-// matrix held in registers (thread -> row tid >> 3, columns (tid & 7) + 8 m).
-// Each pivot step publishes only the pivot row and column through small
-// double-buffered shared arrays (one barrier per step): streaming the whole
-// 64 x 64 matrix through shared memory at every step made it bound by
-// shared-memory bandwidth (about 1 us per step).
+// computed by every CTA: block Gauss-Jordan without pivoting in FP64 over
+// 8 x 8 blocks of the matrix padded to 64 x 64 with the identity (the
+// inverse of diag(A, I) is diag(A^-1, I)), so 8 sequential block steps
+// instead of 64 scalar ones (each scalar step cost ~1600 cycles of
+// dependent latency).  The matrix lives in registers: thread -> row
+// tid >> 3, columns (tid & 7) + 8 m (one column in each block column m).
+// Block step K with pivot block B = M_KK, P = B^-1:
+//   M_KJ <- P M_KJ,  M_IJ <- M_IJ - M_IK P M_KJ,  M_IK <- -M_IK P,  M_KK <- P.
+// P comes from an 8 x 8 Gauss-Jordan inside warp 0 (two entries per lane,
+// shuffles), Q = P M_K* from all threads, then each thread's rank-8 update.
 __device__ void coarsest_inverse(const PArgs &A, Smem &sm) {
     const int tid = threadIdx.x, l = A.nlev - 1, nx = A.dims[2 * l], ny = A.dims[2 * l + 1], n = nx * ny;
     const float *D = sm.co + A.off[l], *CE = D + n, *CN = CE + n;
     const int row = tid >> 3, c0 = tid & 7;
-    double a[NINV / 8];
+    double a[8];
 #pragma unroll
-    for (int m = 0; m < NINV / 8; m++) {
+    for (int m = 0; m < 8; m++) {
         const int c = c0 + 8 * m;
         double v = 0.0;
-        if (row < n && c < n) {
+        if (row >= n || c >= n) {
+            v = row == c ? 1.0 : 0.0;
+        } else {
             const int lo = row < c ? row : c, hi = row < c ? c : row;
             if (c == row) v = D[row];
             else if (hi - lo == ny) v = -(double)CE[lo];
@@ -604,30 +611,71 @@ __device__ void coarsest_inverse(const PArgs &A, Smem &sm) {
         }
         a[m] = v;
     }
-    for (int k = 0; k < n; k++) {
-        double *prow = sm.piv_row[k & 1], *pcol = sm.piv_col[k & 1];
-        if (row == k)
+    for (int K = 0; K < 8; K++) {
+        // publish the pivot block row and this row's entries of block column K
+        if ((row >> 3) == K)
 #pragma unroll
-            for (int m = 0; m < NINV / 8; m++) prow[c0 + 8 * m] = a[m];
-        if (c0 == (k & 7)) {
+            for (int m = 0; m < 8; m++) sm.gj_row[row & 7][8 * m + c0] = a[m];
 #pragma unroll
-            for (int m = 0; m < NINV / 8; m++)
-                if (m == (k >> 3)) pcol[row] = a[m];
+        for (int m = 0; m < 8; m++)
+            if (m == K) sm.gj_col[row][c0] = a[m];
+        __syncthreads();
+        if (tid < 32) {  // P = inverse of the pivot block, lane -> row r, columns cc, cc + 1
+            const int lane = tid, r = lane >> 2, cc = 2 * (lane & 3);
+            double p0 = sm.gj_row[r][8 * K + cc], p1 = sm.gj_row[r][8 * K + cc + 1];
+            for (int t = 0; t < 8; t++) {
+                const int src_piv = (t << 2) + (t >> 1), src_col = (r << 2) + (t >> 1), src_row = (t << 2) + (lane & 3);
+                const double vt = (t & 1) ? p1 : p0;
+                const double piv = __shfl_sync(0xffffffffu, vt, src_piv);
+                const double f = __shfl_sync(0xffffffffu, vt, src_col);
+                const double q0 = __shfl_sync(0xffffffffu, p0, src_row), q1 = __shfl_sync(0xffffffffu, p1, src_row);
+                const double rp = recip64(piv);
+                if (r == t) {
+                    p0 = (cc == t) ? rp : q0 * rp;
+                    p1 = (cc + 1 == t) ? rp : q1 * rp;
+                } else {
+                    p0 = (cc == t) ? -f * rp : p0 - f * (q0 * rp);
+                    p1 = (cc + 1 == t) ? -f * rp : p1 - f * (q1 * rp);
+                }
+            }
+            sm.gj_p[r][cc] = p0;
+            sm.gj_p[r][cc + 1] = p1;
         }
         __syncthreads();
-        const double rp = recip64(prow[k]), fik = pcol[row];
+        {  // Q = P M_K* (the new pivot block row), thread -> (t, column)
+            const int t = tid >> 6, col = tid & 63;
+            double q = 0.0;
 #pragma unroll
-        for (int m = 0; m < NINV / 8; m++) {
-            const int c = c0 + 8 * m;
-            const double bk = prow[c];
-            if (row == k) a[m] = (c == k) ? rp : bk * rp;
-            else if (c == k) a[m] = -fik * rp;
-            else a[m] = a[m] - fik * (bk * rp);
+            for (int u = 0; u < 8; u++) q += sm.gj_p[t][u] * sm.gj_row[u][col];
+            sm.gj_q[t][col] = q;
         }
+        __syncthreads();
+        if ((row >> 3) == K) {
+#pragma unroll
+            for (int m = 0; m < 8; m++) a[m] = (m == K) ? sm.gj_p[row & 7][c0] : sm.gj_q[row & 7][8 * m + c0];
+        } else {
+            double f[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) f[t] = sm.gj_col[row][t];
+#pragma unroll
+            for (int m = 0; m < 8; m++) {
+                double acc = 0.0;
+                if (m == K) {
+#pragma unroll
+                    for (int t = 0; t < 8; t++) acc -= f[t] * sm.gj_p[t][c0];
+                    a[m] = acc;
+                } else {
+#pragma unroll
+                    for (int t = 0; t < 8; t++) acc += f[t] * sm.gj_q[t][8 * m + c0];
+                    a[m] -= acc;
+                }
+            }
+        }
+        __syncthreads();
     }
     if (row < n)
 #pragma unroll
-        for (int m = 0; m < NINV / 8; m++)
+        for (int m = 0; m < 8; m++)
             if (c0 + 8 * m < n) sm.inv[row * NINV + c0 + 8 * m] = a[m];
     __syncthreads();
 }

@@ -350,7 +350,7 @@ def mixed_precision_errors(sh):
             its += r["iters"]
         ss.sync()
         el = time.perf_counter() - t0
-        res[prec] = dict(ls=ss.download("ls")[3:-3, 3:-3], p=ss.download("p")[3:-3, 3:-3], t=el, its=its,
+        res[prec] = dict(**{k: ss.download(k)[3:-3, 3:-3] for k in ("ls", "u", "v", "p", "kappa")}, t=el, its=its,
                          vol0=vol0, vol=ss.last_volume())
         ss.close()
     # the same mixed run device-resident: one graph per step, one synchronisation
@@ -372,10 +372,12 @@ def mixed_precision_errors(sh):
     ss.close()
     a, b = res[api.PRECISION_MIXED], res[api.PRECISION_FP64]
     err = {}
-    for k in ("ls", "p"):
+    for k in ("ls", "u", "v", "p", "kappa"):
         d = a[k] - b[k]
         err[k] = {"rel_max": float(np.abs(d).max() / np.abs(b[k]).max()),
                   "rel_l2": float(np.sqrt((d ** 2).mean() / (b[k] ** 2).mean()))}
+    # area: the smoothed-Heaviside volume of each run, relative to the FP64 run's
+    err["area"] = {"rel": float(abs(a["vol"][1] - b["vol"][1]) / b["vol"][1])}
     return {"workload": f"{CFG3_GRID}x{CFG3_GRID} droplet (rho ratio 1000, mu ratio 100), {CFG3_STEPS} full steps, "
                         "pressure to rel. residual 1e-10",
             "error_vs_fp64": err,
@@ -829,7 +831,7 @@ def run_ours(args):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
         for f in ("ls", "H", "div"):
-            s.upload(f, host[f])
+            s.upload_async(f, host[f])  # pinned buffers, unchanged until the solve synchronises
         s.assemble_gfm(dt, recompute_kappa=True)
         r = s.solve_pressure(solver, tol=TOL, maxit=500000, dt=dt)
         s.L.asd2g_download(s.h, api.PS, out.numpy())

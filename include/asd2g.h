@@ -141,6 +141,12 @@ int asd2g_field_ptr(asd2g_session *s, int field, double **dptr);
 /* Host <-> device copies of a whole padded field (synchronous). */
 int asd2g_upload(asd2g_session *s, int field, const double *host);
 int asd2g_download(asd2g_session *s, int field, double *host);
+/* The same upload queued on the session's stream without waiting for it (no
+ * reference counterpart: the reference keeps its fields on the host).  The
+ * host buffer must stay valid and unchanged until the session next
+ * synchronises (asd2g_sync, a pressure solve, a download); from pinned host
+ * memory the copy overlaps the host's next calls. */
+int asd2g_upload_async(asd2g_session *s, int field, const double *host);
 int asd2g_copy_field(asd2g_session *s, int dst, int src);
 int asd2g_fill_field(asd2g_session *s, int field, double value);
 

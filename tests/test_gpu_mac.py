@@ -282,3 +282,20 @@ def test_droplet_steps(n, steps):
             assert_close(interior(s.download("ps")), interior(ps_ref), 0.0, 1e-8 * np.abs(ps_ref).max(), "ps")
             assert abs(r["dt_next"] - st["dt"]) <= 1e-9 * st["dt"]
             dt = st["dt"]  # march both with the oracle's dt
+
+
+def test_upload_async_then_solve():
+    """asd2g_upload_async queues the copy; the next synchronising call (here
+    the pressure solve) sees it: same pressure as with synchronous uploads."""
+    g, f, ls, H, div = _pressure_case()
+    out = []
+    for use_async in (False, True):
+        with api.Session(params_for(g, f)) as s:
+            for fld, a in (("ls", ls), ("H", H), ("div", div)):
+                a = np.ascontiguousarray(a, dtype=np.float64)
+                s.upload_async(fld, a) if use_async else s.upload(fld, a)
+            s.assemble_gfm(1e-3, recompute_kappa=True)
+            r = s.solve_pressure(api.MGPCG, tol=1e-10, maxit=1000, dt=1e-3)
+            assert r["status"] == 0
+            out.append(s.download("ps"))
+    assert np.array_equal(out[0], out[1])
