@@ -32,6 +32,7 @@ UNITS = {
     "api.cu": [],
     "pcg_static.cu": ["-fmad=false"],
     "pcg_cluster.cu": ["-fmad=false"],
+    "pcg_persist.cu": ["-fmad=false"],
     "mg.cu": [],
     "mg_persist.cu": [],
     "levelset32.cu": [],

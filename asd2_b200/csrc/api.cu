@@ -240,7 +240,7 @@ struct asd2g_session {
     int nlev = 0;
     double *coarse_inv = nullptr, *z = nullptr;
     double *mg_partial = nullptr;  // per-tile partial sums of the V-cycle's fused dots
-    unsigned *mgp_bar = nullptr;   // grid-barrier words of the one-launch MG-FCG solve
+    unsigned *mgp_bar = nullptr;   // grid-barrier words of the one-launch solvers
     Ls32Work w32{};                // FP32 level-set work arrays (precision = mixed)
     double last_volume[2] = {0.0, 0.0};  // volume check of the last droplet step (sharp, smoothed)
     int64_t mg_partial_n = 0;
@@ -307,14 +307,6 @@ int mg_alloc(asd2g_session *s) {
     if (rc == ASD2G_OK) rc = dalloc(s, &s->z, s->N);
     const int64_t np = mg_partial_len(s->g.nx, s->g.ny);
     if (rc == ASD2G_OK) rc = dalloc(s, &s->mg_partial, (size_t)np);
-    if (rc == ASD2G_OK) {
-        if (cudaMalloc(&s->mgp_bar, 512 * sizeof(unsigned)) != cudaSuccess) {
-            cudaGetLastError();
-            rc = fail(ASD2G_E_NOMEM, "grid-barrier words");
-        } else {
-            s->allocs.push_back(s->mgp_bar);
-        }
-    }
     if (rc) return rc;
     s->mg_partial_n = np;
     if (!mg_cta_prepare(s->lv, n)) return fail(ASD2G_E_UNSUPPORTED, "multigrid coarse cycle does not fit a CTA");
@@ -430,6 +422,10 @@ int asd2g_create(const asd2g_params *p, void *stream, asd2g_session **out) {
     if (rc == ASD2G_OK) {
         if (cudaMalloc(&s->counter, sizeof(unsigned) * 4) != cudaSuccess) rc = fail(ASD2G_E_NOMEM, "counter allocation failed");
         else s->allocs.push_back(s->counter);
+    }
+    if (rc == ASD2G_OK) {  // grid-barrier words of the one-launch solvers
+        if (cudaMalloc(&s->mgp_bar, 512 * sizeof(unsigned)) != cudaSuccess) rc = fail(ASD2G_E_NOMEM, "barrier words");
+        else s->allocs.push_back(s->mgp_bar);
     }
     if (rc == ASD2G_OK && cudaMallocHost(&s->ks_host, sizeof(KState)) != cudaSuccess) rc = fail(ASD2G_E_NOMEM, "pinned alloc");
     if (rc == ASD2G_OK && cudaMallocHost(&s->dsc_host, sizeof(double) * 8) != cudaSuccess) rc = fail(ASD2G_E_NOMEM, "pinned alloc");
@@ -890,6 +886,29 @@ static int solve(asd2g_session *s, int solver, double tol, int maxit, int *iters
     const double reg = solver == 1 ? 1.0e-12 : 0.0;  // err_tol^2 in alpha (poisson2d.cpp:354)
     launch_set_kstate(s->ks, tol, maxit, mode, reg, s->st);
     s->last_one_launch = 0;
+    if (solver == 0 && !(s->prm.solver_flags & ASD2G_FLAG_NO_CLUSTER_PCG) &&
+        launch_pcg_persist(g.nx, g.ny, s->sys, s->x, s->r, s->pa, s->pb, s->partial,
+                           3 * RED_BLOCKS_MAX + 2 * DT_BLOCKS, s->mgp_bar, s->ks, tol, maxit, s->st)) {
+        // one cooperative launch ran the whole solve (all SMs)
+        if (stream_capturing(s)) {
+            if (iters) *iters = -1;
+            if (resid) *resid = -1.0;
+            return cuda_check("one-launch pcg");
+        }
+        cudaMemcpyAsync(s->ks_host, s->ks, sizeof(KState), cudaMemcpyDeviceToHost, s->st);
+        int rc2 = sync(s);
+        if (rc2) return rc2;
+        const KState &k = *s->ks_host;
+        if (k.status != -8) {  // -8: a grid-barrier wait gave up; solve again below
+            s->last_one_launch = 1;
+            if (iters) *iters = k.it;
+            if (resid) *resid = k.res;
+            if (k.status == -5) return fail(ASD2G_E_NONFINITE, "non-finite residual at iteration %d", k.it);
+            if (k.status == -6) return fail(ASD2G_E_BREAKDOWN, "Krylov breakdown at iteration %d", k.it);
+            return !(k.res > tol) ? ASD2G_OK : ASD2G_NOT_CONVERGED;
+        }
+        launch_set_kstate(s->ks, tol, maxit, mode, reg, s->st);
+    }
     if (solver == 0 && !(s->prm.solver_flags & ASD2G_FLAG_NO_CLUSTER_PCG) &&
         launch_pcg_cluster(g.nx, g.ny, s->sys, s->x, s->ks, tol, maxit, s->st)) {
         // one launch ran the whole solve

@@ -48,7 +48,7 @@
 // read-only for the launch.
 //
 // The grid barrier is a monotonic arrival counter (zeroed before the launch)
-// with a bounded wait: after SPIN_LIMIT polls a CTA sets the error word and
+// with a bounded wait: after GRID_SPIN_LIMIT polls a CTA sets the error word and
 // returns, every other CTA stops at its next barrier, the solve reports
 // status -8 and the host solves the system with the multi-kernel path.
 // The launch is cooperative (all CTAs co-resident) or is not made at all.
@@ -56,6 +56,7 @@
 #include <cstdlib>
 
 #include "asd2g.h"
+#include "gridsync.cuh"
 #include "mg.cuh"
 
 namespace asd2g {
@@ -68,7 +69,6 @@ constexpr int H2I = PTI + 4, H2J = PTJ + 4;            // tile + 2
 constexpr int CMAX = 1800;                             // cells of levels 3.. (32^2 + 16^2 + 8^2 and odd sizes)
 constexpr int NINV = MG_COARSE_CELLS;                  // coarsest level <= 64 cells
 static_assert(NINV == 64, "the coarsest inverse works on 8 x 8 blocks of a 64 x 64 matrix");
-constexpr unsigned SPIN_LIMIT = 1u << 22;              // polls (L2 round trips, ~0.3 us) before a wait gives up
 constexpr int STATUS_BARRIER = -8;                     // KState.status when a barrier wait gave up
 
 // A level distributed over the CTAs: the CTA's CI x CJ cells of it (the
@@ -117,69 +117,14 @@ struct PArgs {
     float omega;
 };
 
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
+__device__ __forceinline__ bool gsync(const PArgs &A, Smem &sm, unsigned &epoch) {
+    return grid_sync(A.bar, A.ncta, epoch, sm.flag);
 }
-
-// Grid barrier; false when the wait gave up (or another CTA's did).  Thread
-// 0 arrives with a release reduction (ordering the CTA's writes, made
-// visible to it by the CTA barrier, before its arrival) and polls with
-// acquire loads; the CTA barrier after it orders the others' reads.
-__device__ bool gsync(const PArgs &A, Smem &sm, unsigned &epoch) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        epoch++;
-        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(A.bar) : "memory");
-        const unsigned target = epoch * (unsigned)A.ncta;
-        int good = 1;
-        for (unsigned n = 0; ld_acquire(A.bar) < target; n++) {
-            if (n > SPIN_LIMIT || *(volatile unsigned *)(A.bar + 1)) {
-                atomicExch(A.bar + 1, 1u);
-                good = 0;
-                break;
-            }
-        }
-        sm.flag = good;
-    }
-    __syncthreads();
-    return sm.flag != 0;
+template <int NV> __device__ __forceinline__ void put_partial(const PArgs &A, Smem &sm, double (&v)[NV]) {
+    grid_put_partial<NV, NT>(A.partial, &sm.red[0][0], v);
 }
-
-// Block sums of NV values into this CTA's slots (read after the next barrier).
-template <int NV> __device__ void put_partial(const PArgs &A, Smem &sm, double (&v)[NV]) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int q = 0; q < NV; q++) {
-        double s = v[q];
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (lane == 0) sm.red[q][wid] = s;
-    }
-    __syncthreads();
-    if (wid == 0) {
-#pragma unroll
-        for (int q = 0; q < NV; q++) {
-            double s = lane < NT / 32 ? sm.red[q][lane] : 0.0;
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-            if (lane == 0) __stcg(A.partial + 4 * blockIdx.x + q, s);
-        }
-    }
-}
-
-// Sum of every CTA's slots, in the same order in every CTA -> sm.tot.
-template <int NV> __device__ void get_total(const PArgs &A, Smem &sm) {
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-#pragma unroll
-        for (int q = 0; q < NV; q++) {
-            double s = 0.0;
-            for (int c = lane; c < A.ncta; c += 32) s += __ldcg(A.partial + 4 * c + q);
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-            if (lane == 0) sm.tot[q] = s;
-        }
-    }
-    __syncthreads();
+template <int NV> __device__ __forceinline__ void get_total(const PArgs &A, Smem &sm) {
+    grid_get_total<NV>(A.partial, A.ncta, sm.tot);
 }
 
 // Gauss-Seidel update of local cell (a, b) from its four neighbours (times

@@ -65,6 +65,13 @@ void launch_csr_pcg_iter(const int *ia, const int *ja, const double *a, int rows
 void launch_csr_bicg_iter(const int *ia, const int *ja, const double *a, int rows, const Sys &S, double *x, double *r,
                           const double *rt, double *p, double *v, double *s, double *t, KState *ks, double *partial,
                           cudaStream_t st);
+// pcg_persist.cu: whole textbook PCG solve (mode 0) as one cooperative launch
+// of one 512-thread CTA per 16 x 32 tile; false (nothing launched) when the
+// tiles do not fit the GPU at once.  r, p0, p1: n-vectors of work space;
+// partial: 4 doubles per tile; bar: two words, zeroed by the launch.  KState
+// receives it, res, status (-8: a grid-barrier wait gave up) and done.
+bool launch_pcg_persist(int nx, int ny, const Sys &S, double *x, double *r, double *p0, double *p1, double *partial,
+                        int64_t partial_len, unsigned *bar, KState *ks, double tol, int maxit, cudaStream_t st);
 // pcg_cluster.cu: whole textbook PCG solve in one thread-block cluster;
 // false when the system does not fit one cluster or cannot be scheduled.
 int pcg_cluster_size(int nx, int ny);

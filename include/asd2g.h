@@ -86,7 +86,7 @@ enum asd2g_solver {
 };
 
 /* solver_flags bits */
-#define ASD2G_FLAG_NO_CLUSTER_PCG 1 /* Jacobi-PCG always as per-iteration kernels (no cluster solver) */
+#define ASD2G_FLAG_NO_CLUSTER_PCG 1 /* Jacobi-PCG always as per-iteration kernels (no one-launch or cluster solver) */
 #define ASD2G_FLAG_NO_PERSIST_MG 2  /* MG-FCG always as per-phase kernels (no one-launch solve) */
 
 /* precision (no reference counterpart: the reference is FP64 throughout) */

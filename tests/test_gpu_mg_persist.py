@@ -1,6 +1,6 @@
 """GPU: the MG-FCG solve as one cooperative launch (mg_persist.cu).
 
-Systems up to about 256 x 256 are solved by one kernel launch: one CTA per
+Systems up to about 256 x 288 are solved by one kernel launch: one CTA per
 16 x 32 tile, grid barriers between the phases, levels from 2 down solved
 by every CTA itself.  The method is the multi-kernel MG-FCG's (same
 V-cycle, same flexible CG, same FP64 residual replacement); only the
@@ -89,3 +89,30 @@ def test_large_grid_falls_back():
     g, f, ls, div = _case(512, 512, "neumann")
     r = _solve(g, f, ls, div, 0, tol=1e-8)
     assert r["status"] == 0 and not r["one_launch"]
+
+
+@pytest.mark.parametrize("nx,ny,bc", [(256, 256, "neumann"), (130, 66, "dirichlet"), (33, 47, "neumann")])
+def test_one_launch_jacobi_pcg(nx, ny, bc):
+    """The FP64 Jacobi-PCG as one cooperative launch (pcg_persist.cu) against
+    the per-iteration kernels (FLAG_NO_CLUSTER_PCG) and the oracle: the same
+    recurrence, so iteration counts agree to summation-order rounding."""
+    g, f, ls, div = _case(nx, ny, bc)
+
+    def run(flags):
+        with api.Session(params_for(g, f, solver_flags=flags)) as s:
+            s.upload("ls", ls)
+            s.heaviside()
+            s.upload("div", div)
+            s.assemble_gfm(1e-3, recompute_kappa=True)
+            r = s.solve_pressure(api.PCG, tol=1e-10, maxit=200000, dt=1e-3)
+            return r, s.last_solve_one_launch(), interior(s.download("ps")), s.get_system()
+    a, a1, ps_a, sysd = run(0)
+    b, b1, ps_b, _ = run(api.FLAG_NO_CLUSTER_PCG)
+    assert a1 and not b1
+    assert a["status"] == 0 and b["status"] == 0
+    assert abs(a["iters"] - b["iters"]) <= max(3, b["iters"] // 50), (a["iters"], b["iters"])
+    x, it_ref, _, _ = O.pcg(g, sysd, tol=1e-12, maxit=500000)
+    ref = interior(O.scatter(g, x))
+    scale = np.abs(ref).max()
+    assert_close(ps_a, ref, 0.0, 1e-6 * scale, "one-launch Jacobi-PCG vs oracle")
+    assert_close(ps_a, ps_b, 0.0, 1e-6 * scale, "one launch vs per-iteration kernels")
