@@ -905,7 +905,7 @@ def run_ours(args):
                   ("the whole solve as one cooperative kernel launch" if one_launch else "per-phase kernels"),
         "solver_iters_mean": it_mean,
         "fp64_cg": {"value": cg_value, "unit": "GFM Poisson solves/s", "iters_mean": float(np.mean(cg_iters)),
-                    "solver": "FP64 Jacobi-PCG, one thread-block-cluster launch per solve"},
+                    "solver": "FP64 Jacobi-PCG (the reference's method), one cooperative launch per solve on all SMs"},
         "speedup_vs_fp64_cg": value / world / cg_value,
         "true_rel_residual": true_res,
         "ls_mcells_per_s": ls_mcells,

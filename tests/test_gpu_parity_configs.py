@@ -10,8 +10,10 @@ itself pinned bit for bit to the reference) on the same seeded inputs.
   FCG and the FP64 Jacobi-PCG to rel. residual 1e-8.  The oracle solves it
   with its FP64 PCG to 1e-12.  Bar: pressure within 1e-6 of max |p|, true
   FP64 residual <= 1e-8.
-* 20 full steps of the 256^2 droplet with the plain FP64 method.  Bars: level
-  set, velocity and pressure near the oracle's, interface-cell and
+* 20 full steps of the 256^2 droplet with the plain FP64 method (Jacobi-PCG
+  to 1e-10 on both sides).  Bars: level set within 1e-9 and velocity and
+  pressure within 5e-6 of their maxima (the solves' own error at 1e-10),
+  the first step's level set bit-identical, interface-cell and
   crossing-face masks equal at every step.
 * The full revolution of the 128^2 perturbed circle (1129 steps at CFL 0.5).  MinRK2 is
   bit-identical.  MinRK2 with the Sussman constraint (cos() in the
@@ -140,9 +142,14 @@ def test_config2_20_steps_256():
             assert abs(r["dt_next"] - st["dt"]) <= 1e-8 * st["dt"], (k, r["dt_next"], st["dt"])
             dt = st["dt"]
     print(f"cfg 2, 20 steps at 256^2: worst error vs oracle (rel. to max) {worst}")
-    assert worst["ls"] <= 1e-10, worst
+    # both sides stop their PCG at the configuration's rel. residual 1e-10,
+    # so each pressure carries its own solve error (a few 1e-7 of max |p| at
+    # density ratio 1000); summed in different orders, the two differ by up
+    # to 2e-6 after 20 steps (measured), and the level set advected with
+    # them by 4e-10
+    assert worst["ls"] <= 1e-9, worst
     for fld in ("u", "v", "ps"):
-        assert worst[fld] <= 1e-6, worst
+        assert worst[fld] <= 5e-6, worst
 
 
 def _area(g, ls):
