@@ -37,6 +37,7 @@ UNITS = {
     "mg_persist.cu": [],
     "levelset32.cu": [],
     "weno32.cu": [],
+    "reinit32.cu": [],
     "batch.cu": [],
     "unet.cu": [],
     "unet_net.cu": [],

@@ -412,6 +412,20 @@ int asd2g_create(const asd2g_params *p, void *stream, asd2g_session **out) {
                 cudaMemsetAsync(*pp, 0, sizeof(float) * G, s->st);
             }
         }
+        // the Sussman band list: a 128-byte header holding the count, then nx * ny offsets
+        const size_t nb = 32 + (size_t)p->nx * p->ny;
+        void *bl = nullptr;
+        if (rc == ASD2G_OK) {
+            if (cudaMalloc(&bl, sizeof(int) * nb) != cudaSuccess) {
+                cudaGetLastError();
+                rc = fail(ASD2G_E_NOMEM, "FP32 band list allocation failed");
+            } else {
+                s->allocs.push_back(bl);
+                cudaMemsetAsync(bl, 0, sizeof(int) * nb, s->st);
+                s->w32.band_n = static_cast<unsigned *>(bl);
+                s->w32.band = static_cast<int *>(bl) + 32;
+            }
+        }
     }
     if (rc == ASD2G_OK) rc = dalloc(s, &s->partial, 3 * RED_BLOCKS_MAX + 2 * DT_BLOCKS);
     if (rc == ASD2G_OK) rc = dalloc(s, &s->dsc, 8);

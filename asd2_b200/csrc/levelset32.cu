@@ -95,16 +95,19 @@ __global__ void __launch_bounds__(256) k_volume(Grid g, const double *__restrict
 // triples, FP32x2 arithmetic, a sliding row window) or in the per-cell tile
 // form (the FP64 kernel's template instantiated for float); both compute the
 // same scheme.  ASD2G_LS32_FORM=cell selects the per-cell form.  The
-// reinitialisation passes are the per-cell templates: a packed form of them
-// (shared minmods, FP32x2, the Sussman constraint on the interface band only)
-// measured slower at 2048^2 (0.112 vs 0.106 ms per pseudo-step).
+// reinitialisation pseudo-steps likewise run in their packed form
+// (reinit32.cu) or as the per-cell templates (ASD2G_RI32_FORM=cell).
+bool env_is_cell(const char *name) {
+    const char *e = getenv(name);
+    return e && std::strcmp(e, "cell") == 0;
+}
 bool packed_stage() {
-    static int v = -1;
-    if (v < 0) {
-        const char *e = getenv("ASD2G_LS32_FORM");
-        v = (e && std::strcmp(e, "cell") == 0) ? 0 : 1;
-    }
-    return v == 1;
+    static const bool v = !env_is_cell("ASD2G_LS32_FORM");
+    return v;
+}
+bool packed_reinit() {
+    static const bool v = !env_is_cell("ASD2G_RI32_FORM");
+    return v;
 }
 
 int64_t padded(const Grid &g) { return (int64_t)g.sx * g.sy; }
@@ -115,7 +118,9 @@ int conv_blocks(int64_t n) { return (int)((n + 255) / 256 < 4 * 148 ? (n + 255) 
 int reinit_steps(double adt, double max_atime);  // levelset.cu
 
 bool ls32_supported(const Grid &g, int reinit_mode) {
-    return g.p_mirror && (reinit_mode == 0 || reinit_mode == 2 || reinit_mode == 4);
+    // the band list of the Sussman pass holds 32-bit cell offsets
+    return g.p_mirror && (reinit_mode == 0 || reinit_mode == 2 || reinit_mode == 4) &&
+           (int64_t)g.sx * g.sy < ((int64_t)1 << 31);
 }
 
 void launch_ls_step32(const Grid &g, int reinit_mode, double max_atime, const double *u, const double *v,
@@ -141,7 +146,9 @@ void launch_ls_step32(const Grid &g, int reinit_mode, double max_atime, const do
     const int steps = reinit_steps(eps * 0.5, mt);
     cudaMemcpyAsync(w.ls0, w.phi, sizeof(float) * (size_t)n, cudaMemcpyDeviceToDevice, st);
     for (int s = 0; s < steps; s++) {
-        if (reinit_mode == 0) {
+        if (packed_reinit()) {
+            launch_reinit32_step(g, reinit_mode, w, st);
+        } else if (reinit_mode == 0) {
             k_reinit_a<0, float><<<grd, blk, 0, st>>>(g, K, w.phi, w.ls0, w.a, 1);
             k_reinit_b<0, float><<<grd, blk, 0, st>>>(g, K, w.a, w.ls0, w.phi, w.phi, 1);
         } else if (reinit_mode == 2) {

@@ -7,6 +7,8 @@ namespace asd2g {
 // FP32 work arrays of the mixed level-set step, each (nx+6) x (ny+6).
 struct Ls32Work {
     float *phi, *ls0, *a, *b, *tu, *tv;
+    int *band;         // offsets of the Sussman band cells (capacity nx * ny)
+    unsigned *band_n;  // their count
 };
 constexpr int LS32_ARRAYS = 6;
 constexpr int VOLUME_BLOCKS = 592;  // partial sums: 2 per block
@@ -24,6 +26,9 @@ void launch_ls_stage32(const Grid &g, int stage, const float *phi_in, const floa
                        const float *phi_n, float *out, const double *dtp, cudaStream_t st);
 // Rows per warp of the FP32 stage kernel (64 columns x R rows per warp).
 int ls32_rows_per_warp(const Grid &g);
+// One reinitialisation pseudo-step (mode 0, 2 or 4) in FP32, packed form
+// (reinit32.cu): phi <- pseudo-step(phi; phi0 = ls0), a and b as scratch.
+void launch_reinit32_step(const Grid &g, int reinit_mode, const Ls32Work &w, cudaStream_t st);
 // Kernel launches of one launch_ls_step32 call.
 int ls32_launches(int reinit_mode, double max_atime, const Grid &g);
 // out2[0] = sum over interior cells of H dx dy, out2[1] = of HS dx dy (FP64).

