@@ -69,6 +69,7 @@ EXPORTS = [
     "asd2g_batch_create", "asd2g_batch_destroy", "asd2g_batch_upload", "asd2g_batch_download",
     "asd2g_batch_field_ptr", "asd2g_batch_offset", "asd2g_batch_assemble", "asd2g_batch_solve", "asd2g_batch_sync",
     "asd2g_batch_step", "asd2g_batch_volume", "asd2g_batch_tile_shape",
+    "asd2g_batch_set_preconditioner_net", "asd2g_batch_solve_with", "asd2g_batch_last_fallback",
     "asd2g_conv_wpack_bytes", "asd2g_conv_pack_weights", "asd2g_conv3x3_bf16",
     "asd2g_unet_create", "asd2g_unet_destroy", "asd2g_unet_nparams", "asd2g_unet_init", "asd2g_unet_set_params",
     "asd2g_unet_get_params", "asd2g_unet_get_grads", "asd2g_unet_forward", "asd2g_unet_train_step",
@@ -139,6 +140,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_batch_step": ([S, dp, I, D, I, ip, dp], I),
         "asd2g_batch_volume": ([S, dp, dp], I),
         "asd2g_batch_tile_shape": ([S, C.POINTER(I), C.POINTER(I), C.POINTER(C.c_float)], I),
+        "asd2g_batch_set_preconditioner_net": ([S, S], I),
+        "asd2g_batch_solve_with": ([S, I, C.c_double, I, ip, dp], I),
+        "asd2g_batch_last_fallback": ([S, C.POINTER(I)], I),
         "asd2g_conv_wpack_bytes": ([I, I], C.c_size_t),
         "asd2g_conv_pack_weights": ([C.c_void_p, I, I, I, I, C.c_void_p, C.c_void_p], I),
         "asd2g_conv3x3_bf16": ([C.c_void_p, I, I, I, I, C.c_void_p, C.c_void_p, I, C.c_void_p, C.c_void_p, I,
@@ -504,11 +508,23 @@ class Batch:
     def assemble(self, dts):
         self._check(self.L.asd2g_batch_assemble(self.h, np.ascontiguousarray(dts, dtype=np.float64)))
 
-    def solve(self, tol=1e-8, maxit=10000):
+    def solve(self, tol=1e-8, maxit=10000, solver=None):
+        """Solve every assembled system; solver MGPCG (default) or UNET (the
+        learned preconditioner, after set_preconditioner_net).  Returns
+        dict(status, iters[count], resid[count]) and, for UNET, fallback."""
         n = len(self.params)
         it, res = np.zeros(n, np.int32), np.zeros(n)
-        rc = self._check(self.L.asd2g_batch_solve(self.h, tol, maxit, it, res))
-        return dict(status=rc, iters=it, resid=res)
+        if solver is None or solver == MGPCG:
+            rc = self._check(self.L.asd2g_batch_solve(self.h, tol, maxit, it, res))
+            return dict(status=rc, iters=it, resid=res)
+        rc = self._check(self.L.asd2g_batch_solve_with(self.h, solver, tol, maxit, it, res))
+        fb = C.c_int()
+        self._check(self.L.asd2g_batch_last_fallback(self.h, C.byref(fb)))
+        return dict(status=rc, iters=it, resid=res, fallback=bool(fb.value))
+
+    def set_preconditioner_net(self, net):
+        """Copy the network's weights into the batch for solver=UNET (None detaches)."""
+        self._check(self.L.asd2g_batch_set_preconditioner_net(self.h, net.h if net is not None else None))
 
     def step(self, dts, reinit_mode=REINIT_MINRK2, tol=1e-10, maxit=10000):
         """One full droplet step of every instance (MG-FCG pressure solve);

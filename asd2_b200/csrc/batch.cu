@@ -47,6 +47,18 @@ struct asd2g_batch {
     KState *ks_host = nullptr;
     cudaGraphExec_t chunk_exec = nullptr;
     std::vector<void *> allocs;
+    // learned preconditioner: the batch's own copy of the attached network,
+    // and the instances grouped by grid size (one network pass per group,
+    // whose feature planes are contiguous)
+    struct PcGroup {
+        int nx, ny, count;
+        float *feats, *out;
+    };
+    asd2g_unet *net = nullptr;
+    std::vector<PcGroup> groups;
+    bool pc_ready = false;
+    cudaGraphExec_t pc_exec = nullptr;
+    int last_fallback = 0;
 };
 
 namespace {
@@ -102,6 +114,8 @@ int check(const char *what) {
 
 void release(asd2g_batch *b) {
     if (b->chunk_exec) cudaGraphExecDestroy(b->chunk_exec);
+    if (b->pc_exec) cudaGraphExecDestroy(b->pc_exec);
+    if (b->net) asd2g_unet_destroy(b->net);
     for (void *p : b->allocs) cudaFree(p);
     if (b->ks_host) cudaFreeHost(b->ks_host);
     if (b->own_stream && b->st) cudaStreamDestroy(b->st);
@@ -512,47 +526,55 @@ int asd2g_batch_volume(asd2g_batch *b, double *sharp, double *smooth) {
 }  // extern "C"
 
 namespace {
+// Tile-shape tuning on this batch's own hierarchy (first solve only, after
+// the multigrid set-up): four FCG iterations per shape, none allowed to stop
+// early.  Leaves the fastest shape selected; the caller sets the solver
+// scalars again.
+int tune_shape(asd2g_batch *b) {
+    if (b->shape_tuned || b->shape_forced >= 0) return ASD2G_OK;
+    const BatchPlan &P = b->plan;
+    struct Events {  // destroyed on every exit path
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        ~Events() {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        }
+    } ev;
+    if (cudaEventCreate(&ev.e0) != cudaSuccess || cudaEventCreate(&ev.e1) != cudaSuccess)
+        return check("batch tile tuning events");
+    cudaEvent_t e0 = ev.e0, e1 = ev.e1;
+    int best = 0;
+    for (int sh = 0; sh < MG_NSHAPES; sh++) {
+        int rc = set_mg_shape(b, sh);
+        if (rc) return rc;
+        launch_batch_set_kstate(P, 0.0, 1 << 30, b->st);
+        launch_batch_fcg_init(P, b->st);
+        launch_batch_fcg_iter(P, 0, b->st);  // first launch of this shape's kernels
+        cudaEventRecord(e0, b->st);
+        for (int k = 0; k < 4; k++) launch_batch_fcg_iter(P, (k + 1) & 1, b->st);
+        cudaEventRecord(e1, b->st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) return check("batch tile tuning");
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        b->shape_ms[sh] = ms;
+        if (ms < b->shape_ms[best]) best = sh;
+    }
+    b->shape_tuned = true;
+    int rc = set_mg_shape(b, best);
+    if (rc) return rc;
+    return ASD2G_OK;
+}
+
 int solve_impl(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_resid) {
     NvtxRange nv("batched pressure solve");
     const BatchPlan &P = b->plan;
     launch_batch_set_kstate(P, tol, maxit, b->st);
     launch_batch_mg_setup(P, b->st);
-    if (!b->shape_tuned && b->shape_forced < 0) {
-        // tile-shape tuning on this batch's own hierarchy (first solve only):
-        // four FCG iterations per shape, none allowed to stop early
-        struct Events {  // destroyed on every exit path
-            cudaEvent_t e0 = nullptr, e1 = nullptr;
-            ~Events() {
-                if (e0) cudaEventDestroy(e0);
-                if (e1) cudaEventDestroy(e1);
-            }
-        } ev;
-        if (cudaEventCreate(&ev.e0) != cudaSuccess || cudaEventCreate(&ev.e1) != cudaSuccess)
-            return check("batch tile tuning events");
-        cudaEvent_t e0 = ev.e0, e1 = ev.e1;
-        int best = 0;
-        for (int sh = 0; sh < MG_NSHAPES; sh++) {
-            int rc = set_mg_shape(b, sh);
-            if (rc) return rc;
-            launch_batch_set_kstate(P, 0.0, 1 << 30, b->st);
-            launch_batch_fcg_init(P, b->st);
-            launch_batch_fcg_iter(P, 0, b->st);  // first launch of this shape's kernels
-            cudaEventRecord(e0, b->st);
-            for (int k = 0; k < 4; k++) launch_batch_fcg_iter(P, (k + 1) & 1, b->st);
-            cudaEventRecord(e1, b->st);
-            if (cudaEventSynchronize(e1) != cudaSuccess) return check("batch tile tuning");
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            b->shape_ms[sh] = ms;
-            if (ms < b->shape_ms[best]) best = sh;
-        }
-        b->shape_tuned = true;
-        int rc = set_mg_shape(b, best);
-        if (rc) return rc;
-        launch_batch_set_kstate(P, tol, maxit, b->st);
-    }
+    int rc = tune_shape(b);
+    if (rc) return rc;
+    launch_batch_set_kstate(P, tol, maxit, b->st);
     launch_batch_fcg_init(P, b->st);
-    int rc = check("batch solve set-up");
+    rc = check("batch solve set-up");
     if (rc) return rc;
     if (!b->chunk_exec) {
         cudaGraph_t graph = nullptr;
@@ -588,6 +610,172 @@ int solve_impl(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_re
     if (cudaStreamSynchronize(b->st) != cudaSuccess) return check("batch solve");
     return status;
 }
+
+// ------------------------------------------ learned preconditioner (UNET) --
+constexpr int BPC_MAX_ITERS = 500;  // learned iterations before the MG-FCG fallback
+
+// The network's correction on every every-th iteration of a chunk of
+// FCG_CHUNK_ITERS (ASD2G_PC_EVERY = 1..8, default 8, as for single systems),
+// besides the first application; the other iterations use the V-cycle alone.
+bool pc_net_on(int k) {
+    static const int every = [] {
+        const char *e = std::getenv("ASD2G_PC_EVERY");
+        const int v = e ? std::atoi(e) : 8;
+        return v >= 1 && v <= 8 ? v : 8;
+    }();
+    return k % every == every - 1;
+}
+
+// Per-instance buffers of the learned preconditioner; instances with one grid
+// size form a group whose feature and output planes are contiguous, so that
+// one network pass serves the group.
+int pc_alloc(asd2g_batch *b) {
+    if (b->pc_ready) return ASD2G_OK;
+    const int count = b->count;
+    std::vector<int> gid(count);
+    b->groups.clear();
+    for (int i = 0; i < count; i++) {
+        const Grid &g = b->hinst[i].g;
+        int k = 0;
+        while (k < (int)b->groups.size() && !(b->groups[k].nx == g.nx && b->groups[k].ny == g.ny)) k++;
+        if (k == (int)b->groups.size()) b->groups.push_back({g.nx, g.ny, 0, nullptr, nullptr});
+        gid[i] = k;
+        b->groups[k].count++;
+    }
+    size_t ntot = 0;
+    for (int i = 0; i < count; i++) ntot += (size_t)b->hinst[i].n;
+    double *dv = nullptr;
+    float *fv = nullptr;
+    constexpr int NDV = 2 * FM_SLOTS + 1;  // direction slots p, q; r1
+    int rc = balloc(b, &dv, NDV * ntot);
+    if (!rc) rc = balloc(b, &fv, 5 * ntot + (size_t)count);  // features (4), output (1); scales
+    if (rc) return rc;
+    cudaMemsetAsync(dv, 0, sizeof(double) * NDV * ntot, b->st);
+    cudaMemsetAsync(fv, 0, sizeof(float) * (5 * ntot + (size_t)count), b->st);
+    // group planes in group order, instances in batch order inside a group
+    std::vector<size_t> gbase(b->groups.size());
+    size_t off = 0;
+    for (size_t k = 0; k < b->groups.size(); k++) {
+        gbase[k] = off;
+        off += (size_t)b->groups[k].count * b->groups[k].nx * b->groups[k].ny;
+        b->groups[k].feats = fv + 4 * gbase[k];
+        b->groups[k].out = fv + 4 * ntot + gbase[k];
+    }
+    std::vector<size_t> gused(b->groups.size(), 0);
+    size_t voff = 0;
+    for (int i = 0; i < count; i++) {
+        BInst &I = b->hinst[i];
+        const int k = gid[i];
+        const size_t at = gbase[k] + gused[k];
+        gused[k] += (size_t)I.n;
+        I.pc_feats = fv + 4 * at;
+        I.pc_out = fv + 4 * ntot + at;
+        I.pc_scal = fv + 5 * ntot + i;
+        for (int j = 0; j < FM_SLOTS; j++) {
+            I.fm.p[j] = dv + (size_t)j * ntot + voff;
+            I.fm.q[j] = dv + (size_t)(FM_SLOTS + j) * ntot + voff;
+        }
+        I.pc_r1 = dv + (size_t)2 * FM_SLOTS * ntot + voff;
+        voff += (size_t)I.n;
+    }
+    cudaMemcpyAsync(b->dinst, b->hinst.data(), sizeof(BInst) * count, cudaMemcpyHostToDevice, b->st);
+    b->pc_ready = true;
+    return check("learned preconditioner buffers");
+}
+
+// z = V-cycle(r) [+ omega u with u = network(r - A z)] for every instance
+int pc_correct(asd2g_batch *b, bool with_net) {
+    const BatchPlan &P = b->plan;
+    if (with_net) {
+        launch_batch_pc_input(P, b->st);
+        for (const auto &G : b->groups) {
+            const int rc = asd2g_unet_forward(b->net, G.count, G.nx, G.ny, G.feats, G.out);
+            if (rc) return rc;
+        }
+    }
+    launch_batch_pc_output(P, with_net, b->st);
+    return check("batched learned preconditioner");
+}
+
+// FCG_CHUNK_ITERS truncated-FCG iterations (direction slot k % FM_SLOTS), the
+// FP64 residual check, and the V-cycle alone after a restart
+int pc_chunk(asd2g_batch *b) {
+    const BatchPlan &P = b->plan;
+    for (int k = 0; k < FCG_CHUNK_ITERS; k++) {
+        launch_batch_pcm_iter(P, k % FM_SLOTS, b->st);
+        const int rc = pc_correct(b, pc_net_on(k));
+        if (rc) return rc;
+    }
+    launch_batch_fcg_check(P, b->st);
+    return pc_correct(b, false);
+}
+static_assert(FCG_CHUNK_ITERS % FM_SLOTS == 0, "every replay of a chunk must write the direction slots in the same order");
+
+int solve_learned_impl(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_resid) {
+    NvtxRange nv("batched pressure solve (learned preconditioner)");
+    if (!b->net) return api_fail(ASD2G_E_ARG, "no preconditioner network attached (asd2g_batch_set_preconditioner_net)");
+    const BatchPlan &P = b->plan;
+    const int cap = maxit < BPC_MAX_ITERS ? maxit : BPC_MAX_ITERS;
+    b->last_fallback = 0;
+    launch_batch_set_kstate(P, tol, cap, b->st, ASD2G_SOLVER_UNET);
+    launch_batch_mg_setup(P, b->st);
+    int rc = tune_shape(b);
+    if (rc) return rc;
+    launch_batch_set_kstate(P, tol, cap, b->st, ASD2G_SOLVER_UNET);
+    launch_batch_pc_setup(P, b->st);
+    launch_batch_fcg_init(P, b->st);  // r = b, x = 0, z = V-cycle(r)
+    rc = pc_correct(b, true);
+    if (rc) return rc;
+    if (!b->pc_exec) {
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return check("capture");
+        const int rc2 = pc_chunk(b);
+        if (cudaStreamEndCapture(b->st, &graph) != cudaSuccess) return check("capture end");
+        if (rc2) {
+            cudaGraphDestroy(graph);
+            return rc2;
+        }
+        const cudaError_t e = cudaGraphInstantiate(&b->pc_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return check("graph instantiate");
+    }
+    bool all_done = false;
+    for (int launched = 0; !all_done && launched < cap + 2 * FCG_CHUNK_ITERS; launched += FCG_CHUNK_ITERS) {
+        if (cudaGraphLaunch(b->pc_exec, b->st) != cudaSuccess) return check("graph launch");
+        cudaMemcpyAsync(b->ks_host, b->ks, sizeof(KState) * b->count, cudaMemcpyDeviceToHost, b->st);
+        if (cudaStreamSynchronize(b->st) != cudaSuccess) return check("batch solve");
+        all_done = true;
+        for (int i = 0; i < b->count; i++)
+            if (!b->ks_host[i].done) all_done = false;
+    }
+    int net_flag = 0;
+    asd2g_unet_error_flag(b->net, &net_flag);
+    bool ok = all_done && !net_flag;
+    for (int i = 0; i < b->count && ok; i++) {
+        const KState &k = b->ks_host[i];
+        ok = (k.status == 0 || k.status == 2) && (!(k.res > tol) || k.status == 2);
+    }
+    if (!ok) {
+        // the batched MG-FCG from zero, judged by the same FP64 residual
+        std::vector<int> it1(b->count);
+        for (int i = 0; i < b->count; i++) it1[i] = b->ks_host[i].it;
+        b->last_fallback = 1;
+        const int st2 = solve_impl(b, tol, maxit, iters, rel_resid);
+        if (iters)
+            for (int i = 0; i < b->count; i++) iters[i] += it1[i];
+        return st2;
+    }
+    launch_batch_scatter(b->dinst, b->cell_tiles, b->ncell_tiles, b->st);
+    rc = check("batch scatter");
+    if (rc) return rc;
+    for (int i = 0; i < b->count; i++) {
+        if (iters) iters[i] = b->ks_host[i].it;
+        if (rel_resid) rel_resid[i] = b->ks_host[i].res;
+    }
+    if (cudaStreamSynchronize(b->st) != cudaSuccess) return check("batch solve");
+    return ASD2G_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -598,6 +786,50 @@ int asd2g_batch_tile_shape(asd2g_batch *b, int *rows, int *cols, float *trial_ms
     if (cols) *cols = MG_SHAPES[b->plan.shape][1];
     if (trial_ms)
         for (int k = 0; k < MG_NSHAPES; k++) trial_ms[k] = (float)b->shape_ms[k];
+    return ASD2G_OK;
+}
+
+int asd2g_batch_set_preconditioner_net(asd2g_batch *b, asd2g_unet *net) {
+    if (!b) return api_fail(ASD2G_E_ARG, "null batch");
+    if (b->pc_exec) {  // the captured chunk holds the previous network's launches
+        cudaGraphExecDestroy(b->pc_exec);
+        b->pc_exec = nullptr;
+    }
+    if (!net) return ASD2G_OK;
+    for (int i = 0; i < b->count; i++)
+        if (b->hinst[i].g.nx % 8 || b->hinst[i].g.ny % 8)
+            return api_fail(ASD2G_E_UNSUPPORTED, "the learned preconditioner needs nx and ny multiples of 8");
+    int rc = pc_alloc(b);
+    if (rc) return rc;
+    if (!b->net) {
+        // the batch's own network, its activation buffers sized for the largest size group
+        size_t maxpix = 0;
+        for (const auto &G : b->groups) {
+            const size_t px = (size_t)G.count * G.nx * G.ny;
+            maxpix = px > maxpix ? px : maxpix;
+        }
+        const size_t w = (maxpix / 8 + 7) / 8 * 8;
+        if (w > (size_t)1 << 30) return api_fail(ASD2G_E_UNSUPPORTED, "batch too large for one network pass");
+        rc = asd2g_unet_create(1, 8, (int)w, b->st, &b->net);
+        if (rc) return rc;
+    }
+    std::vector<float> h(asd2g_unet_nparams(net));
+    if (h.size() != asd2g_unet_nparams(b->net)) return api_fail(ASD2G_E_ARG, "network size mismatch");
+    rc = asd2g_unet_get_params(net, h.data());
+    if (!rc) rc = asd2g_unet_set_params(b->net, h.data());
+    return rc;
+}
+
+int asd2g_batch_solve_with(asd2g_batch *b, int solver, double tol, int maxit, int *iters, double *rel_resid) {
+    if (!b || !(tol > 0.0) || maxit < 1) return api_fail(ASD2G_E_ARG, "batch_solve: bad arguments");
+    if (solver == ASD2G_SOLVER_MGPCG) return solve_impl(b, tol, maxit, iters, rel_resid);
+    if (solver == ASD2G_SOLVER_UNET) return solve_learned_impl(b, tol, maxit, iters, rel_resid);
+    return api_fail(ASD2G_E_ARG, "batch solver must be ASD2G_SOLVER_MGPCG or ASD2G_SOLVER_UNET");
+}
+
+int asd2g_batch_last_fallback(asd2g_batch *b, int *used) {
+    if (!b || !used) return api_fail(ASD2G_E_ARG, "null argument");
+    *used = b->last_fallback;
     return ASD2G_OK;
 }
 

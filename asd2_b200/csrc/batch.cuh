@@ -4,6 +4,7 @@
 // (batched assembly), mg.cu (batched multigrid-preconditioned flexible CG)
 // and batch.cu (host orchestration).
 #pragma once
+#include "asd2g.h"
 #include "lsmath.cuh"
 #include "mg.cuh"
 
@@ -42,6 +43,12 @@ struct BInst {
     int nlev, s_cta;                               // levels; first level of the one-CTA coarse cycle
     MgLevel lv[MG_MAX_LEVELS];
     double *coarse_inv;                            // MG_COARSE_CELLS^2
+    // learned preconditioner (allocated when a network is attached)
+    FmDirs fm;                                     // truncated flexible CG direction slots
+    double *pc_r1;                                 // r - A z_mg
+    float *pc_feats;                               // network input [nx][ny][4] (inside its size group)
+    float *pc_out;                                 // network output [nx][ny]
+    float *pc_scal;                            // [0] coefficient scale (max |diag|)
 };
 
 // Work-list entries.  A cell tile is 32 x 8 padded cells of one instance
@@ -81,7 +88,16 @@ void launch_batch_mg_setup(const BatchPlan &P, cudaStream_t st);
 bool launch_batch_fcg_init(const BatchPlan &P, cudaStream_t st);
 bool launch_batch_fcg_iter(const BatchPlan &P, int parity, cudaStream_t st);
 bool launch_batch_fcg_check(const BatchPlan &P, cudaStream_t st);
-void launch_batch_set_kstate(const BatchPlan &P, double tol, int maxit, cudaStream_t st);
+void launch_batch_set_kstate(const BatchPlan &P, double tol, int maxit, cudaStream_t st,
+                             int mode = ASD2G_SOLVER_MGPCG);
+// Batched learned preconditioner (ASD2G_SOLVER_UNET): set-up of the constant
+// feature channels; r1 = r - A z and feature channel 0; omega and z += omega
+// u (with_u) with the direction coefficients; one truncated-FCG iteration
+// writing direction slot wslot, then the V-cycle of the new residual.
+void launch_batch_pc_setup(const BatchPlan &P, cudaStream_t st);
+void launch_batch_pc_input(const BatchPlan &P, cudaStream_t st);
+void launch_batch_pc_output(const BatchPlan &P, bool with_u, cudaStream_t st);
+void launch_batch_pcm_iter(const BatchPlan &P, int wslot, cudaStream_t st);
 // Full droplet step of every instance (batch_step.cu): one launch per phase
 // over the cell-tile list (tiles of TJ x TI interior cells), the padded-cell
 // chunks (heaviside), the ghost-entry chunks (P-grid fill) or one CTA per

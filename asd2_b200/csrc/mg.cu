@@ -722,13 +722,14 @@ __global__ void __launch_bounds__(MG_INV_THREADS) k_bmg_invert(const BInst *__re
     mg_invert_body(I.lv[I.nlev - 1], I.coarse_inv);
 }
 
-__global__ void k_bset_kstate(const BInst *__restrict__ insts, int count, double tol, int maxit) {
+__global__ void k_bset_kstate(const BInst *__restrict__ insts, int count, double tol, int maxit, int mode) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= count) return;
     KState *ks = insts[b].ks;
     ks->tol = tol;
     ks->maxit = maxit;
-    ks->mode = ASD2G_SOLVER_MGPCG;
+    ks->mode = mode;
+    ks->fm_mask = 0;
     ks->reg = 0.0;
     ks->done = 0;
     ks->status = 0;
@@ -928,6 +929,265 @@ __global__ void __launch_bounds__(256) k_bfcg_replace(const BInst *__restrict__ 
     }
 }
 
+// ------------------------------------- batched learned preconditioner --
+// The two-level preconditioner of ASD2G_SOLVER_UNET (the single-system
+// kernels k_pc_* / k_pcm_a below) for every instance of a batch: one launch
+// per phase over the FCG chunks, per-instance sums with the instance's
+// partial slots and ticket.  The network itself runs between these phases
+// on the instances' feature planes, grouped by grid size.
+
+// scal[0] = max |diag| of each instance (1 if zero): one CTA per instance
+__global__ void __launch_bounds__(1024) k_bpc_diag_max(const BInst *__restrict__ insts) {
+    const BInst &I = insts[blockIdx.x];
+    const double *__restrict__ diag = I.S.diag;
+    double v = 0.0;
+    for (int64_t k = threadIdx.x; k < I.n; k += blockDim.x) v = fmax(v, fabs(diag[k]));
+    __shared__ double sm[32];
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mx = 0.0;
+        for (int wi = 0; wi < (int)(blockDim.x >> 5); wi++) mx = fmax(mx, sm[wi]);
+        I.pc_scal[0] = (float)(mx > 0.0 ? mx : 1.0);
+    }
+}
+
+// feature channels 1..3: diag, ce, cn over the instance's scale
+__global__ void __launch_bounds__(256) k_bpc_consts(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    const Sys S = I.S;
+    float *__restrict__ f = I.pc_feats;
+    const float is = 1.0f / I.pc_scal[0];
+    const int64_t n = I.n, k0 = (int64_t)w.c * FCG_CHUNK;
+#pragma unroll
+    for (int u = 0; u < FCG_CHUNK / 256; u++) {
+        const int64_t k = k0 + threadIdx.x + 256 * u;
+        if (k < n) {
+            f[4 * k + 1] = (float)S.diag[k] * is;
+            f[4 * k + 2] = (float)S.ce[k] * is;
+            f[4 * k + 3] = (float)S.cn[k] * is;
+        }
+    }
+}
+
+// r1 = r - A z (0 at the pinned row); |r1| -> ks->snorm
+__global__ void __launch_bounds__(256) k_bpc_resid(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    KState *ks = I.ks;
+    if (ks->done) return;
+    const Sys S = I.S;
+    const int nx = I.g.nx, ny = I.g.ny;
+    const double *__restrict__ r = I.r;
+    const double *__restrict__ z = I.z;
+    double *__restrict__ r1 = I.pc_r1;
+    const int64_t n = I.n, k0 = (int64_t)w.c * FCG_CHUNK;
+    double v[1] = {0.0};
+#pragma unroll
+    for (int u = 0; u < FCG_CHUNK / 256; u++) {
+        const int64_t k = k0 + threadIdx.x + 256 * u;
+        if (k < n) {
+            const double rk = (S.pinned && k == 0) ? 0.0 : r[k] - sys_apply(S, nx, ny, z, k);
+            r1[k] = rk;
+            v[0] += rk * rk;
+        }
+    }
+    double tot[1];
+    if (mg_reduce<1>(v, I.partial, &ks->counter, w.c, I.chunks, tot)) ks->snorm = sqrt(tot[0]);
+}
+
+// feature channel 0: r1 / rms(r1)
+__global__ void __launch_bounds__(256) k_bpc_feat0(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    const KState *ks = I.ks;
+    if (ks->done) return;
+    const int64_t n = I.n, k0 = (int64_t)w.c * FCG_CHUNK;
+    const double rms = ks->snorm / sqrt((double)n);
+    const double inv = (rms > 0.0 && isfinite(rms)) ? 1.0 / rms : 0.0;
+    const double *__restrict__ r1 = I.pc_r1;
+    float *__restrict__ f = I.pc_feats;
+#pragma unroll
+    for (int u = 0; u < FCG_CHUNK / 256; u++) {
+        const int64_t k = k0 + threadIdx.x + 256 * u;
+        if (k < n) f[4 * k] = (float)(r1[k] * inv);
+    }
+}
+
+// omega = (u . r1) / (u . A u) -> ks->omega (u: the network output, 0 at the pinned cell)
+__global__ void __launch_bounds__(256) k_bpc_omega(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    KState *ks = I.ks;
+    if (ks->done) return;
+    const Sys S = I.S;
+    const int nx = I.g.nx, ny = I.g.ny;
+    const float *__restrict__ uo = I.pc_out;
+    const double *__restrict__ r1 = I.pc_r1;
+    auto U = [&](int64_t m) { return (S.pinned && m == 0) ? 0.0 : (double)uo[m]; };
+    const int64_t n = I.n, k0 = (int64_t)w.c * FCG_CHUNK;
+    double acc[2] = {0.0, 0.0};
+#pragma unroll
+    for (int u = 0; u < FCG_CHUNK / 256; u++) {
+        const int64_t k = k0 + threadIdx.x + 256 * u;
+        if (k < n) {
+            double y = 0.0;
+            if (!(S.pinned && k == 0)) {
+                const int ii = (int)(k / ny), jj = (int)(k % ny);
+                if (jj > 0) y += -S.cn[k - 1] * U(k - 1);
+                if (ii > 0) y += -S.ce[k - ny] * U(k - ny);
+                y += S.diag[k] * U(k);
+                if (ii < nx - 1) y += -S.ce[k] * U(k + ny);
+                if (jj < ny - 1) y += -S.cn[k] * U(k + 1);
+            }
+            const double uk = U(k);
+            acc[0] += uk * r1[k];
+            acc[1] += uk * y;
+        }
+    }
+    double tot[2];
+    if (mg_reduce<2>(acc, I.partial, &ks->counter, w.c, I.chunks, tot))
+        ks->omega = (tot[1] > 0.0 && isfinite(tot[0] / tot[1])) ? tot[0] / tot[1] : 0.0;
+}
+
+// z += omega u (with_u) and the orthogonalisation coefficients of the valid
+// direction slots from z . q_j (none at the first iteration or after a
+// residual replacement)
+__global__ void __launch_bounds__(256) k_bpc_final(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks,
+                                                   int with_u) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    KState *ks = I.ks;
+    if (ks->done || ks->skip_vc) return;
+    const double om = with_u ? ks->omega : 0.0;
+    const float *__restrict__ uo = I.pc_out;
+    double *__restrict__ z = I.z;
+    const FmDirs D = I.fm;
+    const int pinned = I.S.pinned;
+    const int64_t n = I.n, k0 = (int64_t)w.c * FCG_CHUNK;
+    double acc[FM_SLOTS] = {};
+#pragma unroll
+    for (int u = 0; u < FCG_CHUNK / 256; u++) {
+        const int64_t k = k0 + threadIdx.x + 256 * u;
+        if (k < n) {
+            const double zk = (pinned && k == 0) ? 0.0 : z[k] + (with_u ? om * (double)uo[k] : 0.0);
+            z[k] = zk;
+#pragma unroll
+            for (int j = 0; j < FM_SLOTS; j++) acc[j] += zk * D.q[j][k];
+        }
+    }
+    double tot[FM_SLOTS];
+    if (mg_reduce<FM_SLOTS>(acc, I.partial, &ks->counter, w.c, I.chunks, tot)) {
+        if (ks->it == 0 || ks->restart) {
+            ks->fm_mask = 0;
+            ks->restart = 0;
+        }
+        for (int j = 0; j < FM_SLOTS; j++)
+            ks->fm_beta[j] = ((ks->fm_mask >> j) & 1) ? -tot[j] / ks->fm_pq[j] : 0.0;
+    }
+}
+
+// p_w = z + sum over the other valid slots of beta_j p_j, q_w = A p_w;
+// alpha = (p_w . r) / (p_w . q_w)
+__global__ void __launch_bounds__(256) k_bpcm_a(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks,
+                                                int wslot) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    KState *ks = I.ks;
+    if (ks->done) return;
+    if (w.c == 0 && threadIdx.x == 0) ks->skip_vc = 0;
+    double b[FM_SLOTS];
+#pragma unroll
+    for (int j = 0; j < FM_SLOTS; j++) b[j] = j == wslot ? 0.0 : ks->fm_beta[j];
+    const Sys S = I.S;
+    const int nx = I.g.nx, ny = I.g.ny;
+    const FmDirs D = I.fm;
+    const double *__restrict__ z = I.z;
+    const double *__restrict__ r = I.r;
+    double *__restrict__ pw = D.p[wslot];
+    double *__restrict__ qw = D.q[wslot];
+    const int64_t n = I.n, k0 = (int64_t)w.c * FCG_CHUNK;
+    auto pv = [&](int64_t m) {
+        double v = z[m];
+#pragma unroll
+        for (int j = 0; j < FM_SLOTS; j++)
+            if (j != wslot) v += b[j] * D.p[j][m];
+        return v;
+    };
+    double acc[2] = {0.0, 0.0};
+#pragma unroll
+    for (int u = 0; u < FCG_CHUNK / 256; u++) {
+        const int64_t k = k0 + threadIdx.x + 256 * u;
+        if (k < n) {
+            const int ii = (int)(k / ny), jj = (int)(k % ny);
+            const double pc = pv(k);
+            double y = 0.0;
+            if (!(S.pinned && k == 0)) {
+                if (jj > 0) y += -S.cn[k - 1] * pv(k - 1);
+                if (ii > 0) y += -S.ce[k - ny] * pv(k - ny);
+                y += S.diag[k] * pc;
+                if (ii < nx - 1) y += -S.ce[k] * pv(k + ny);
+                if (jj < ny - 1) y += -S.cn[k] * pv(k + 1);
+            }
+            pw[k] = pc;
+            qw[k] = y;
+            acc[0] += pc * y;
+            acc[1] += pc * r[k];
+        }
+    }
+    double tot[2];
+    if (mg_reduce<2>(acc, I.partial, &ks->counter, w.c, I.chunks, tot)) {
+        if (!(tot[0] > 0.0) || !isfinite(tot[0]) || !isfinite(tot[1])) {
+            ks->status = -6;
+            ks->done = 1;
+        } else {
+            ks->alpha = tot[1] / tot[0];
+            ks->fm_pq[wslot] = tot[0];
+            ks->fm_mask |= 1 << wslot;
+        }
+    }
+}
+
+// x += alpha p_w, r -= alpha q_w; |r| and the stopping test (k_bfcg_b on the slot's vectors)
+__global__ void __launch_bounds__(256) k_bpcm_b(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks,
+                                                int wslot) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    KState *ks = I.ks;
+    if (ks->done) return;
+    const double alpha = ks->alpha;
+    const double *__restrict__ p = I.fm.p[wslot];
+    const double *__restrict__ q = I.fm.q[wslot];
+    double *__restrict__ x = I.x;
+    double *__restrict__ r = I.r;
+    const int64_t n = I.n, k0 = (int64_t)w.c * FCG_CHUNK;
+    double v[1] = {0.0};
+#pragma unroll
+    for (int u = 0; u < FCG_CHUNK / 256; u++) {
+        const int64_t k = k0 + threadIdx.x + 256 * u;
+        if (k < n) {
+            x[k] += alpha * p[k];
+            const double rk = r[k] - alpha * q[k];
+            r[k] = rk;
+            v[0] += rk * rk;
+        }
+    }
+    double tot[1];
+    if (mg_reduce<1>(v, I.partial, &ks->counter, w.c, I.chunks, tot)) {
+        const int it = ks->it + 1;
+        ks->it = it;
+        ks->res = sqrt(tot[0]) / ks->bn;
+        if (!isfinite(ks->res)) {
+            ks->status = -5;
+            ks->done = 1;
+        } else if (!(ks->res > ks->tol) || it >= ks->maxit) {
+            ks->done = 1;
+        }
+    }
+}
+
 template <bool L0, int TI_, int TJ_>
 __global__ void __launch_bounds__(256) k_bmg_pre(const BInst *__restrict__ insts, const BTile *__restrict__ tiles,
                                                  int l) {
@@ -956,7 +1216,9 @@ __global__ void __launch_bounds__(256) k_bmg_post(const BInst *__restrict__ inst
     if (L0) {
         const int gx = (I.lv[0].ny + TJ_ - 1) / TJ_;
         double tot[2];
-        if (mg_reduce<2>(acc, I.partial, &ks->counter, w.bx + gx * w.by, I.tiles0, tot)) fcg_beta(ks, tot);
+        if (mg_reduce<2>(acc, I.partial, &ks->counter, w.bx + gx * w.by, I.tiles0, tot) &&
+            ks->mode != KMODE_LEARNED)
+            fcg_beta(ks, tot);
     }
 }
 
@@ -1351,7 +1613,7 @@ static_assert(MG_SHAPES[0][0] == MT_I && MG_SHAPES[0][1] == MT_J, "shape 0 is th
 
 int64_t batch_partial_len(int nx, int ny) {
     const int64_t chunks = ((int64_t)nx * ny + FCG_CHUNK - 1) / FCG_CHUNK;
-    const int64_t a = 2 * (int64_t)batch_tiles0(nx, ny), b = 2 * chunks;
+    const int64_t a = 2 * (int64_t)batch_tiles0(nx, ny), b = (int64_t)FM_SLOTS * chunks;  // learned: 4 sums
     return a > b ? a : b;
 }
 
@@ -1362,8 +1624,8 @@ bool batch_cta_prepare() {
            cudaFuncSetAttribute(k_bmg_invert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv) == cudaSuccess;
 }
 
-void launch_batch_set_kstate(const BatchPlan &P, double tol, int maxit, cudaStream_t st) {
-    k_bset_kstate<<<(P.count + 127) / 128, 128, 0, st>>>(P.insts, P.count, tol, maxit);
+void launch_batch_set_kstate(const BatchPlan &P, double tol, int maxit, cudaStream_t st, int mode) {
+    k_bset_kstate<<<(P.count + 127) / 128, 128, 0, st>>>(P.insts, P.count, tol, maxit, mode);
 }
 
 void launch_batch_mg_setup(const BatchPlan &P, cudaStream_t st) {
@@ -1415,6 +1677,27 @@ bool launch_batch_fcg_check(const BatchPlan &P, cudaStream_t st) {
     k_bfcg_replace<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks);
     batch_vcycle(P, st);
     return true;
+}
+
+void launch_batch_pc_setup(const BatchPlan &P, cudaStream_t st) {
+    k_bpc_diag_max<<<P.count, 1024, 0, st>>>(P.insts);
+    k_bpc_consts<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks);
+}
+
+void launch_batch_pc_input(const BatchPlan &P, cudaStream_t st) {
+    k_bpc_resid<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks);
+    k_bpc_feat0<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks);
+}
+
+void launch_batch_pc_output(const BatchPlan &P, bool with_u, cudaStream_t st) {
+    if (with_u) k_bpc_omega<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks);
+    k_bpc_final<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks, with_u ? 1 : 0);
+}
+
+void launch_batch_pcm_iter(const BatchPlan &P, int wslot, cudaStream_t st) {
+    k_bpcm_a<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks, wslot);
+    k_bpcm_b<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks, wslot);
+    batch_vcycle(P, st);
 }
 
 // ------------------------------------------------- learned preconditioner --

@@ -679,8 +679,14 @@ int asd2g_unet_get_params(asd2g_unet *u, float *host) {
     return cudaStreamSynchronize(u->st) == cudaSuccess ? ASD2G_OK : cuda_ok("get_params");
 }
 
-static int check_shape(asd2g_unet *u, int B, int H, int W) {
-    if (!u || B < 1 || B > u->max_b || H < 8 || W < 8 || H % 8 || W % 8 || (size_t)H * W > (size_t)u->max_h * u->max_w)
+// A forward pass fits when its B * H * W pixels fit the activation buffers
+// (max_batch * max_h * max_w pixels, every level a quarter of the one
+// above); a training step also needs B <= max_batch (per-image losses) and
+// H * W <= max_h * max_w.
+static int check_shape(asd2g_unet *u, int B, int H, int W, bool training = true) {
+    const size_t cap = u ? (size_t)u->max_b * u->max_h * u->max_w : 0;
+    if (!u || B < 1 || H < 8 || W < 8 || H % 8 || W % 8 || (size_t)B * H * W > cap ||
+        (training && (B > u->max_b || (size_t)H * W > (size_t)u->max_h * u->max_w)))
         return api_fail(ASD2G_E_ARG, "U-Net batch or image size outside the created maximum (multiples of 8)");
     return ASD2G_OK;
 }
@@ -688,7 +694,7 @@ static int check_shape(asd2g_unet *u, int B, int H, int W) {
 // feats: device FP32 [B][H][W][4]; out: device FP32 [B][H][W].
 int asd2g_unet_forward(asd2g_unet *u, int B, int H, int W, const float *feats, float *out) {
     NvtxRange nv("U-Net forward");
-    int rc = check_shape(u, B, H, W);
+    int rc = check_shape(u, B, H, W, false);
     if (rc) return rc;
     if (!feats || !out) return api_fail(ASD2G_E_ARG, "null argument");
     const int64_t npix = (int64_t)B * H * W;

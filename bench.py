@@ -459,6 +459,7 @@ def batched_solves(sh, stream, flush, count=BATCH_COUNT):
             raise SystemExit(f"bench: batched solve did not converge: {res['status']}")
         times.append(t)
     (trow, tcol), trial_ms = b.tile_shape()
+    learned = batched_learned(b, dts, timed)
     b.close()
     t_b = float(np.median(times))
     cells = int(sum(c.nx * c.ny for c in cases))
@@ -486,7 +487,42 @@ def batched_solves(sh, stream, flush, count=BATCH_COUNT):
             "roofline": {"bound": "hbm", "achieved": alg / t_b / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": alg / t_b / 1e9 / peak,
                          "bytes": "assembly 64 B + MG-FCG 180 B per unknown and iteration of each instance"},
+            "learned_pc": learned,
             "l2": "flushed (256 MB write) before each timed batch / system"}
+
+
+def batched_learned(b, dts, timed):
+    """The same batch solved with the learned two-level preconditioner
+    (asd2g_batch_solve_with(..., ASD2G_SOLVER_UNET), trained weights; one
+    network pass per grid-size group): assembly + solve to rel. residual 1e-8,
+    median of five after two untimed."""
+    from asd2_b200 import api
+    from asd2_b200 import train_unet as T
+    if not os.path.exists(T.DEFAULT_WEIGHTS):
+        return {"unavailable": "no trained preconditioner weights in the package"}
+    params, _ = T.load_params()
+    net = api.UNet(1, 64, 64)
+    net.set_params(params)
+    b.set_preconditioner_net(net)
+    net.close()
+
+    def once():
+        b.assemble(dts)
+        return b.solve(tol=TOL, maxit=10000, solver=api.UNET)
+    for _ in range(2):
+        once()
+    times, res = [], None
+    for _ in range(5):
+        res, t = timed(once)
+        if res["status"] != 0:
+            raise SystemExit(f"bench: batched learned solve did not converge: {res['status']}")
+        times.append(t)
+    t = float(np.median(times))
+    return {"value": len(dts) / t, "unit": "GFM Poisson solves/s", "ms_per_batch": t * 1e3,
+            "iters": {"max": int(np.max(res["iters"])), "mean": float(np.mean(res["iters"]))},
+            "max_true_rel_residual": float(np.max(res["resid"])), "fallback": bool(res["fallback"]),
+            "solver": "FP64 truncated flexible CG, preconditioner = FP32 V-cycle + U-Net correction (BF16 "
+                      "tcgen05 convolutions, one pass per grid-size group) with the A-norm optimal step"}
 
 
 def learned_pc_512(sh, stream, flush, weights=None, n=512, counts=tuple(range(1, 9)), cpu_baseline=True):

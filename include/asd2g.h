@@ -320,7 +320,9 @@ int asd2g_conv3x3_bf16(const void *in, int n, int h, int w, int cin, const void 
  * average pooling, nearest upsampling + skip concatenation); forward and
  * input-gradient convolutions on the tcgen05 tensor cores (BF16, FP32
  * accumulation), weight gradients in FP32, Adam on FP32 master weights.
- * Images: H x W, both multiples of 8, up to the sizes given at creation.
+ * Images: H x W, both multiples of 8.  A forward pass takes B images with
+ * B * H * W <= max_batch * max_h * max_w; a training step B <= max_batch
+ * images of H * W <= max_h * max_w.
  * feats: device FP32 [B][H][W][4] (vector / RMS, diag / s, ce / s, cn / s);
  * out and target: device FP32 [B][H][W]. */
 typedef struct asd2g_unet asd2g_unet;
@@ -360,14 +362,28 @@ int asd2g_unet_set_stream(asd2g_unet *u, void *stream);
  * two-level preconditioner: z_mg = one FP32 V-cycle of r (the multigrid of
  * ASD2G_SOLVER_MGPCG), r1 = r - A z_mg, u = network(features of r1) (BF16 /
  * FP32 inside), z = z_mg + omega u with omega = (u . r1) / (u . Au) in
- * FP64; the network runs on the first application, after each residual
- * replacement and on every 8th iteration, the V-cycle alone otherwise (each
- * new direction is A-orthogonalised against the three before it).  Convergence is verified on the FP64 residual as for
+ * FP64; the network runs on the first application and on every 8th
+ * iteration, the V-cycle alone otherwise and after a residual replacement
+ * (each new direction is A-orthogonalised against the three before it).
+ * Convergence is verified on the FP64 residual as for
  * ASD2G_SOLVER_MGPCG; if it does not converge within min(maxit, 500)
  * iterations the system is solved again by Jacobi-PCG and
  * asd2g_last_fallback reports 1. */
 int asd2g_set_preconditioner_net(asd2g_session *s, asd2g_unet *net);
 int asd2g_last_fallback(asd2g_session *s, int *used);
+/* The same learned preconditioner for a batch (no reference counterpart):
+ * the batch copies the network's weights (later changes to net are not seen
+ * until it is attached again) and groups its instances by grid size, one
+ * network pass per group; every instance needs nx and ny multiples of 8.
+ * asd2g_batch_solve_with(b, ASD2G_SOLVER_UNET, ...) then runs the truncated
+ * flexible CG above for every instance, each phase one launch for the whole
+ * batch, each instance stopping on its own; if any instance has not
+ * converged within min(maxit, 500) iterations, the whole batch is solved
+ * again by the batched MG-FCG and asd2g_batch_last_fallback reports 1.
+ * solver ASD2G_SOLVER_MGPCG is asd2g_batch_solve. */
+int asd2g_batch_set_preconditioner_net(asd2g_batch *b, asd2g_unet *net);
+int asd2g_batch_solve_with(asd2g_batch *b, int solver, double tol, int maxit, int *iters, double *rel_resid);
+int asd2g_batch_last_fallback(asd2g_batch *b, int *used);
 /* How the session's last pressure solve ran: *one_launch = 1 when the whole
  * solve was one kernel launch (the thread-block-cluster Jacobi-PCG or the
  * cooperative MG-FCG of systems up to about 256 x 256), 0 when it ran as
