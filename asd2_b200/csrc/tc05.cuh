@@ -113,6 +113,29 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
     return false;
 }
 
+// Bounded wait through mbarrier.try_wait, which may suspend the thread in
+// hardware until the phase completes or the suspend-time hint (2 us) ends the
+// attempt (no software back-off): false, and *err set to code, after
+// MBAR_TRY_LIMIT unsuccessful attempts (at most about half a second).  For
+// short waits on copies and MMAs.
+constexpr uint32_t MBAR_TRY_LIMIT = 1u << 18;
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, 2000;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_hw(uint64_t *bar, uint32_t parity, int *err, int code) {
+    for (uint32_t it = 0; it < MBAR_TRY_LIMIT; it++)
+        if (mbar_try(bar, parity)) return true;
+    if (err) atomicExch(err, code);
+    return false;
+}
+
 // 32 TMEM lanes x 16 columns of 32 bits: thread t of the warp gets lane
 // (base lane + t), columns col .. col + 15.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {

@@ -19,6 +19,9 @@
 // frees the stage for the chunk that many stages later.  The epilogue reads the accumulator from tensor memory
 // (warp w owns pixel rows 32w .. 32w+31), adds the bias, applies ReLU and
 // stores BF16 NHWC (and optionally channel 0 in FP32).
+#include <cstdlib>
+#include <cstring>
+
 #include <cuda_bf16.h>
 
 #include "asd2g.h"
@@ -107,7 +110,10 @@ __device__ __forceinline__ void conv_load_chunk(uint8_t *stage, uint64_t *full, 
     }
 }
 
-template <int COUT>
+// S pipeline stages (conv_stages(COUT), or 1 / 2 for layers of one / two
+// input-channel chunks: every chunk then has its own stage, all are loaded
+// at once, and the smaller footprint lets more CTAs share an SM).
+template <int COUT, int S>
 __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __nv_bfloat16 *__restrict__ in,
                                                              const __nv_bfloat16 *__restrict__ low, int CL, int H,
                                                              int W, int CIN, const uint4 *__restrict__ wpack,
@@ -116,9 +122,8 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __nv_bfloat16
                                                              float *__restrict__ out32, int relu, int *err) {
     extern __shared__ __align__(128) uint8_t sm[];
     constexpr int SB = conv_stage_bytes(COUT);
-    constexpr int S = conv_stages(COUT);
-    constexpr int SLACK = S - 3;          // iterations a chunk's MMAs get before their stage is refilled
-    constexpr int AHEAD = S - 1 - SLACK;  // chunks in flight ahead of the one being multiplied
+    constexpr int SLACK = S >= 3 ? S - 3 : 0;            // iterations a chunk's MMAs get before their stage is refilled
+    constexpr int AHEAD = S >= 3 ? S - 1 - SLACK : S;  // chunks in flight ahead of the one being multiplied
     uint64_t *mma_bar = reinterpret_cast<uint64_t *>(sm + S * SB);  // per stage: its MMAs completed
     uint64_t *full_bar = mma_bar + S;                               // per stage: its weights landed
     uint32_t *tslot = reinterpret_cast<uint32_t *>(full_bar + S);
@@ -131,6 +136,10 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __nv_bfloat16
     constexpr uint32_t NCOL = COUT <= 32 ? 32 : COUT <= 64 ? 64 : COUT <= 128 ? 128 : 256;  // power of two
     constexpr uint32_t IDESC = umma_idesc_bf16(128, COUT);
     const int nkc = CIN / 16;
+    if (S < 3 && nkc > S) {  // the launcher never does this: no stage may be refilled with S < 3
+        if (tid == 0) atomicExch(err, 4);
+        return;
+    }
     if (tid == 0) {
         for (int k = 0; k < S; k++) {
             mbar_init(mma_bar + k, 1);
@@ -163,7 +172,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __nv_bfloat16
         if (nk < nkc) {             // block-uniform
             bool freed = true;
             const int pk = nk - S;
-            if (pk >= 0) freed = mbar_wait(mma_bar + pk % S, (uint32_t)(pk / S) & 1u, err, 1);
+            if (pk >= 0) freed = mbar_wait_hw(mma_bar + pk % S, (uint32_t)(pk / S) & 1u, err, 1);
             if (!__syncthreads_and(freed && !*abort_flag)) {  // every thread leaves the loop together
                 ok = false;
                 break;
@@ -176,7 +185,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __nv_bfloat16
         fence_async_smem();
         __syncthreads();  // ... and every thread's part
         if (tid == 0) {
-            const bool wok = mbar_wait(full_bar + kc % S, (uint32_t)(kc / S) & 1u, err, 2);
+            const bool wok = mbar_wait_hw(full_bar + kc % S, (uint32_t)(kc / S) & 1u, err, 2);
             consumed = kc + 1;
             tc_fence_after();
             if (wok) {
@@ -198,7 +207,7 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __nv_bfloat16
     if (tid == 0)        // nor a bulk copy: wait (bounded) for the weights of chunks never multiplied
         for (int c = consumed; c < issued; c++) mbar_wait(full_bar + c % S, (uint32_t)(c / S) & 1u, err, 2);
     // the last commit arrives once every MMA of the tile has completed
-    if (ok && nkc > 0) ok = mbar_wait(mma_bar + (nkc - 1) % S, (uint32_t)((nkc - 1) / S) & 1u, err, 1);
+    if (ok && nkc > 0) ok = mbar_wait_hw(mma_bar + (nkc - 1) % S, (uint32_t)((nkc - 1) / S) & 1u, err, 1);
     __syncthreads();
     ok = __syncthreads_and(ok && !*abort_flag);  // the TMEM loads below are warp-collective
     tc_fence_after();
@@ -237,6 +246,209 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3x3_tc(const __nv_bfloat16
     if (warp == 0) tmem_dealloc(tmem, NCOL);
 }
 
+// The patch of one tile and chunk into a patch stage (cp.async, every thread).
+__device__ __forceinline__ void conv_load_patch(uint8_t *stage, const PatchPlan &P,
+                                                const __nv_bfloat16 *__restrict__ inb,
+                                                const __nv_bfloat16 *__restrict__ lowb, int CL, int kc, int tid) {
+    uint4 *patch = reinterpret_cast<uint4 *>(stage);
+    const bool from_low = lowb != nullptr && kc * 16 < CL;
+    const __nv_bfloat16 *base = from_low ? lowb + kc * 16 : inb + (lowb ? kc * 16 - CL : kc * 16);
+#pragma unroll
+    for (int i = 0; i < PATCH_SLOTS; i++) {
+        const int t = tid + CONV_THREADS * i;
+        if (t < 2 * PATCH_PIX) {
+            const int off = from_low ? P.off_low[i] : P.off_in[i];
+            cp_async16(patch + t, off >= 0 ? base + off : inb, off >= 0);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- workers --
+// Layers of one or two 16-channel input chunks (the full-resolution and
+// half-resolution convolutions, most of the network's time) as persistent
+// CTAs of NW independent workers.  A worker is four warps (TMEM lanes
+// 0..127 for the epilogue) that loops over its own row tiles: the layer's
+// weights are copied into the worker's shared memory once, the patch of the
+// next tile is copied while the current one is multiplied and written out
+// (two patch buffers), one thread issues the tile's MMAs into the worker's
+// accumulator and commits them to the worker's barrier.  The per-tile CTAs
+// above are held by the rate at which CTAs can be launched (a few hundred
+// nanoseconds of work each, ~2 of 12 possible resident per SM); here a CTA
+// lives for the whole layer and NW tile chains run side by side per SM.
+template <int COUT, int NKC> struct ConvW {
+    static constexpr int NCOL = COUT <= 32 ? 32 : COUT <= 64 ? 64 : COUT <= 128 ? 128 : 256;
+    static constexpr int WB = 288 * COUT;                       // one weight chunk
+    static constexpr int PER = NKC * WB + 2 * NKC * PATCH_BYTES;  // weights + two patch buffers
+    static constexpr int FIT = (220 * 1024) / PER;
+    static constexpr int NW0 = FIT > 8 ? 8 : FIT;
+    static constexpr int NW = NW0 * NCOL > 512 ? 512 / NCOL : NW0;  // workers per CTA
+    static constexpr int COLS = NW * NCOL <= 32 ? 32 : NW * NCOL <= 64 ? 64 : NW * NCOL <= 128 ? 128
+                                : NW * NCOL <= 256 ? 256 : 512;   // TMEM allocation (power of two)
+    static constexpr int BAR_OFF = NW * PER;
+    static constexpr int SMEM = BAR_OFF + NW * 16 + 16;           // per worker: weights and MMA barriers
+};
+
+__device__ __forceinline__ void bar_sync(int id, int count) {
+    asm volatile("barrier.cta.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+// named-barrier AND over the count threads of barrier id
+__device__ __forceinline__ bool bar_and(int id, int count, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbarrier.cta.red.and.pred p, %2, %3, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id), "r"(count)
+        : "memory");
+    return r != 0;
+}
+
+template <int COUT, int NKC>
+__global__ void __launch_bounds__(CONV_THREADS *ConvW<COUT, NKC>::NW, 1)
+    k_conv3x3_tcw(const __nv_bfloat16 *__restrict__ in, const __nv_bfloat16 *__restrict__ low, int CL, int H,
+                  int W, int CIN, const uint4 *__restrict__ wpack, const float *__restrict__ bias,
+                  __nv_bfloat16 *__restrict__ out, float *__restrict__ out32, int relu, int *err, int tiles_x,
+                  int ntiles) {
+    using C = ConvW<COUT, NKC>;
+    constexpr int NW = C::NW, WB = C::WB;
+    constexpr uint32_t NCOL = C::NCOL;
+    constexpr uint32_t IDESC = umma_idesc_bf16(128, COUT);
+    extern __shared__ __align__(128) uint8_t sm[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int wk = warp >> 2, wt = tid & (CONV_THREADS - 1);  // worker, thread within the worker
+    uint8_t *wreg = sm + wk * C::PER;                          // the worker's weights, then its two patch buffers
+    uint8_t *pbuf = wreg + NKC * WB;
+    uint64_t *wfull = reinterpret_cast<uint64_t *>(sm + C::BAR_OFF) + 2 * wk;  // weights landed
+    uint64_t *mbar = wfull + 1;                                                 // the tile's MMAs completed
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + C::BAR_OFF + NW * 16);
+    const int bid = 1 + wk;  // the worker's named barrier
+    const int cs = low ? CIN - CL : CIN;
+    if (CIN != 16 * NKC) {  // the launcher never does this
+        if (tid == 0) atomicExch(err, 4);
+        return;
+    }
+    if (wt == 0) {
+        mbar_init(wfull, 1);
+        mbar_init(mbar, 1);
+        mbar_init_fence();
+    }
+    if (warp == 0) {
+        tmem_alloc(tslot, (uint32_t)C::COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tacc = *tslot + (uint32_t)wk * NCOL;
+    const int workers = (int)gridDim.x * NW, gw = (int)blockIdx.x * NW + wk;
+    const int my = gw < ntiles ? (ntiles - 1 - gw) / workers + 1 : 0;  // this worker's tiles
+    auto coords = [&](int i, int &img, int &y, int &x0) {  // the worker's i-th tile
+        const int t = gw + i * workers;
+        const int r = t / tiles_x;
+        x0 = (t - r * tiles_x) * CT_PIX;
+        y = r % H;
+        img = r / H;
+    };
+    PatchPlan P;
+    auto load_tile = [&](int i) {  // every chunk's patch of tile i into buffer i & 1
+        int img, y, x0;
+        coords(i, img, y, x0);
+        patch_plan(P, H, W, cs, CL, y, x0, wt);
+        const __nv_bfloat16 *inb = in + (size_t)img * H * W * cs;
+        const __nv_bfloat16 *lowb = low ? low + (size_t)img * (H >> 1) * (W >> 1) * CL : nullptr;
+#pragma unroll
+        for (int kc = 0; kc < NKC; kc++)
+            conv_load_patch(pbuf + ((i & 1) * NKC + kc) * PATCH_BYTES, P, inb, lowb, CL, kc, wt);
+    };
+    bool ok = true, wwait = false;
+    if (my > 0) {
+        if (wt == 0) {  // the layer's weights, once
+            mbar_arrive_expect_tx(wfull, (uint32_t)(NKC * WB));
+            bulk_g2s(wreg, wpack, (uint32_t)(NKC * WB), wfull);
+        }
+        load_tile(0);
+    }
+    cp_async_commit();
+    for (int i = 0; i < my; i++) {
+        // the next tile's patches go into the other buffer (its MMAs, of tile
+        // i - 1, completed before that tile's epilogue)
+        if (i + 1 < my) load_tile(i + 1);
+        cp_async_commit();
+        cp_async_wait<1>();  // tile i's patches have landed (this thread's part)
+        fence_async_smem();
+        bar_sync(bid, CONV_THREADS);  // ... and the whole worker's
+        tc_fence_after();
+        bool good = true;
+        if (wt == 0) {
+            if (!wwait) {
+                good = mbar_wait_hw(wfull, 0u, err, 2);
+                wwait = true;
+            }
+            if (good) {
+                const uint32_t pw0 = smem_u32(wreg);
+#pragma unroll 1
+                for (int kc = 0; kc < NKC; kc++) {
+                    const uint32_t pa = smem_u32(pbuf + ((i & 1) * NKC + kc) * PATCH_BYTES);
+                    const uint32_t pw = pw0 + (uint32_t)(kc * WB);
+                    for (int tap = 0; tap < 9; tap++) {
+                        const int dy = tap / 3, dx = tap % 3;
+                        const uint64_t ad =
+                            umma_desc_k(pa + (uint32_t)(dy * PATCH_W + dx) * 16u, PATCH_PIX * 16u, 128u);
+                        const uint64_t bd = umma_desc_k(pw + (uint32_t)tap * 2u * COUT * 16u, COUT * 16u, 128u);
+                        umma_bf16(tacc, ad, bd, IDESC, (kc > 0 || tap > 0) ? 1u : 0u);
+                    }
+                }
+            }
+            umma_commit(mbar);  // always, so that the wait below ends
+            good = mbar_wait_hw(mbar, (uint32_t)(i & 1), err, 1) && good;
+        }
+        if (!bar_and(bid, CONV_THREADS, good)) {  // the TMEM loads below are warp-collective
+            ok = false;
+            break;
+        }
+        tc_fence_after();
+        int img, y, x0;
+        coords(i, img, y, x0);
+        const int x = x0 + (warp & 3) * 32 + lane;
+        const size_t pix = (size_t)img * H * W + (size_t)y * W + x;
+        const uint32_t tb = tacc + ((uint32_t)((warp & 3) * 32) << 16);
+#pragma unroll
+        for (int c0 = 0; c0 < COUT; c0 += 16) {
+            uint32_t r[16];
+            tmem_ld16(tb + (uint32_t)c0, r);
+            tmem_wait_ld();
+            if (x < W) {
+                float v[16];
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    v[k] = __uint_as_float(r[k]) + bias[c0 + k];
+                    if (relu) v[k] = fmaxf(v[k], 0.0f);
+                }
+                if (out) {
+                    uint32_t wv[8];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+                        wv[k] = *reinterpret_cast<const uint32_t *>(&b2);
+                    }
+                    uint4 *o = reinterpret_cast<uint4 *>(out + pix * COUT + c0);
+                    o[0] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+                    o[1] = make_uint4(wv[4], wv[5], wv[6], wv[7]);
+                }
+                if (out32 && c0 == 0) out32[pix] = v[0];
+            }
+        }
+        tc_fence_before();
+        bar_sync(bid, CONV_THREADS);  // every TMEM read of this tile precedes the next tile's MMAs
+    }
+    (void)ok;
+    cp_async_wait<0>();  // no cp.async may still target shared memory when the CTA exits
+    if (wt == 0 && my > 0 && !wwait) mbar_wait(wfull, 0u, err, 2);  // nor the weights' bulk copy
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(*tslot, (uint32_t)C::COLS);
+}
+
 // w[co][ci][3][3] (FP32, cout x cin real channels) -> wpack[kc][tap][half][co][8]
 // (BF16, padded to cout_pad x cin_pad with zeros).
 __global__ void k_pack_conv(const float *__restrict__ w, int cout, int cin, int cout_pad, int cin_pad,
@@ -259,23 +471,100 @@ __global__ void k_pack_conv(const float *__restrict__ w, int cout, int cin, int 
     }
 }
 
-template <int COUT> bool conv_prepare() {
+__host__ __device__ constexpr int conv_smem_s(int cout, int S) { return S * conv_stage_bytes(cout) + 16 * S + 16; }
+
+template <int COUT, int S> bool conv_prepare() {
     static bool done = false;
     if (!done)
-        done = cudaFuncSetAttribute(k_conv3x3_tc<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    conv_smem_bytes(COUT)) == cudaSuccess;
+        done = cudaFuncSetAttribute(k_conv3x3_tc<COUT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    conv_smem_s(COUT, S)) == cudaSuccess;
     return done;
+}
+
+template <int COUT, int S>
+int conv_launch_s(const void *in, const void *low, int cl, int n, int h, int w, int cin, const void *wpack,
+                  const float *bias, void *out, float *out32, int relu, int *err, cudaStream_t st) {
+    if (!conv_prepare<COUT, S>()) return ASD2G_E_CUDA;
+    const dim3 grid((w + CT_PIX - 1) / CT_PIX, h, n);
+    k_conv3x3_tc<COUT, S><<<grid, CONV_THREADS, conv_smem_s(COUT, S), st>>>(
+        (const __nv_bfloat16 *)in, (const __nv_bfloat16 *)low, cl, h, w, cin, (const uint4 *)wpack, bias,
+        (__nv_bfloat16 *)out, out32, relu, err);
+    return cudaGetLastError() == cudaSuccess ? ASD2G_OK : ASD2G_E_CUDA;
+}
+
+// One or two input-channel chunks: as many stages as chunks (ASD2G_CONV_STAGES
+// = full keeps the full pipeline for them, for measurements).
+bool conv_small_stages() {
+    static const bool v = [] {
+        const char *e = std::getenv("ASD2G_CONV_STAGES");
+        return !(e && std::strcmp(e, "full") == 0);
+    }();
+    return v;
+}
+
+int sm_count() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 148;
+    }
+    return n;
+}
+
+// ASD2G_CONV_FORM=tile: the per-tile CTAs for every layer (no workers).
+bool conv_workers() {
+    static const bool v = [] {
+        const char *e = std::getenv("ASD2G_CONV_FORM");
+        return !(e && std::strcmp(e, "tile") == 0);
+    }();
+    return v;
+}
+
+// The worker form for NKC chunks, if it fits at least two workers per CTA;
+// returns 1 when it does not apply.
+template <int COUT, int NKC>
+int conv_launch_w(const void *in, const void *low, int cl, int n, int h, int w, int cin, const void *wpack,
+                  const float *bias, void *out, float *out32, int relu, int *err, cudaStream_t st) {
+    using C = ConvW<COUT, NKC>;
+    if constexpr (C::NW >= 2) {
+        static bool attr = false;
+        if (!attr)
+            attr = cudaFuncSetAttribute(k_conv3x3_tcw<COUT, NKC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        C::SMEM) == cudaSuccess;
+        if (!attr) return ASD2G_E_CUDA;
+        const int tiles_x = (w + CT_PIX - 1) / CT_PIX;
+        const int64_t nt = (int64_t)tiles_x * h * n;
+        if (nt >= ((int64_t)1 << 31)) return ASD2G_E_ARG;
+        const int64_t need = (nt + C::NW - 1) / C::NW, cap = sm_count();
+        const int grid = (int)(need < cap ? need : cap);
+        k_conv3x3_tcw<COUT, NKC><<<grid, CONV_THREADS * C::NW, C::SMEM, st>>>(
+            (const __nv_bfloat16 *)in, (const __nv_bfloat16 *)low, cl, h, w, cin, (const uint4 *)wpack, bias,
+            (__nv_bfloat16 *)out, out32, relu, err, tiles_x, (int)nt);
+        return cudaGetLastError() == cudaSuccess ? ASD2G_OK : ASD2G_E_CUDA;
+    } else {
+        return 1;
+    }
 }
 
 template <int COUT>
 int conv_launch(const void *in, const void *low, int cl, int n, int h, int w, int cin, const void *wpack,
                 const float *bias, void *out, float *out32, int relu, int *err, cudaStream_t st) {
-    if (!conv_prepare<COUT>()) return ASD2G_E_CUDA;
-    const dim3 grid((w + CT_PIX - 1) / CT_PIX, h, n);
-    k_conv3x3_tc<COUT><<<grid, CONV_THREADS, conv_smem_bytes(COUT), st>>>(
-        (const __nv_bfloat16 *)in, (const __nv_bfloat16 *)low, cl, h, w, cin, (const uint4 *)wpack, bias,
-        (__nv_bfloat16 *)out, out32, relu, err);
-    return cudaGetLastError() == cudaSuccess ? ASD2G_OK : ASD2G_E_CUDA;
+    const int nkc = cin / 16;
+    // one or two chunks: the worker form (three chunks fit two workers per CTA
+    // at 16 output channels, measured slower than the per-tile CTAs)
+    if (conv_workers() && nkc <= 2) {
+        const int rc = nkc == 1
+                           ? conv_launch_w<COUT, 1>(in, low, cl, n, h, w, cin, wpack, bias, out, out32, relu, err, st)
+                           : conv_launch_w<COUT, 2>(in, low, cl, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+        if (rc != 1) return rc;
+    }
+    if (conv_small_stages() && nkc == 1)
+        return conv_launch_s<COUT, 1>(in, low, cl, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    if (conv_small_stages() && nkc == 2)
+        return conv_launch_s<COUT, 2>(in, low, cl, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
+    return conv_launch_s<COUT, conv_stages(COUT)>(in, low, cl, n, h, w, cin, wpack, bias, out, out32, relu, err,
+                                                   st);
 }
 
 }  // namespace
