@@ -228,6 +228,9 @@ int build(asd2g_batch *b) {
             const asd2g_params &pp = b->prm[i];
             const double we = pp.numbers_given ? pp.we : pp.rho_h / pp.sigma;
             I.kappa_fill = (we != 0.0 && std::isfinite(we)) ? 1 : 0;
+            const double mt = pp.ls_max_atime > 0.0 ? pp.ls_max_atime : 1.5 * I.K.thick;
+            I.nreinit = reinit_steps(I.K.adt, mt);
+            I.order = pp.time_order;
         }
         double *v = vec + noff[i];
         double **slots[NVEC] = {&I.S.diag, &I.S.cw, &I.S.ce, &I.S.cs, &I.S.cn, &I.S.minv, &I.S.b,
@@ -433,20 +436,17 @@ int asd2g_batch_step(asd2g_batch *b, double *dt, int reinit_mode, double tol, in
     if (!b || !dt || !(tol > 0.0) || maxit < 1) return api_fail(ASD2G_E_ARG, "batch_step: bad arguments");
     if (reinit_mode != ASD2G_REINIT_ORIGINAL && reinit_mode != ASD2G_REINIT_MINRK2)
         return api_fail(ASD2G_E_UNSUPPORTED, "batch_step implements reinit modes 0 (original) and 2 (MinRK2)");
-    const int order = b->prm[0].time_order;
-    int steps = -1;
+    // instances keep their own time order and reinitialisation step count:
+    // the phases run up to the largest, instances without a phase skip it
+    int steps = 0, omax = 0;
     for (int i = 0; i < b->count; i++) {
         const asd2g_params &pp = b->prm[i];
         if (pp.precision != ASD2G_PRECISION_FP64)
             return api_fail(ASD2G_E_UNSUPPORTED, "batch_step runs FP64 instances");
-        if (pp.time_order != order || order < 0 || order > 2)
-            return api_fail(ASD2G_E_UNSUPPORTED, "batch_step needs one time order (0, 1 or 2) for every instance");
-        const LsConst &K = b->hinst[i].K;
-        const double mt = pp.ls_max_atime > 0.0 ? pp.ls_max_atime : 1.5 * K.thick;
-        const int si = reinit_steps(K.adt, mt);
-        if (steps >= 0 && si != steps)
-            return api_fail(ASD2G_E_UNSUPPORTED, "batch_step needs one reinitialisation step count for every instance");
-        steps = si;
+        if (pp.time_order < 0 || pp.time_order > 2)
+            return api_fail(ASD2G_E_UNSUPPORTED, "batch_step implements time orders 0, 1 and 2");
+        steps = b->hinst[i].nreinit > steps ? b->hinst[i].nreinit : steps;
+        omax = pp.time_order > omax ? pp.time_order : omax;
     }
     int rc = set_dts(b, dt);
     if (rc) return rc;
@@ -470,8 +470,8 @@ int asd2g_batch_step(asd2g_batch *b, double *dt, int reinit_mode, double tol, in
         launch_bstep_fill_p(P, BS_LS, false, st);
     }
     for (int k = 0; k < steps; k++) {
-        launch_bstep_reinit_pass(P, reinit_mode, false, st);
-        launch_bstep_reinit_pass(P, reinit_mode, true, st);
+        launch_bstep_reinit_pass(P, reinit_mode, false, k, st);
+        launch_bstep_reinit_pass(P, reinit_mode, true, k, st);
     }
     // curvature (with the ghost fill of SolvePoisson's recompute), Heaviside, volume check
     launch_bstep_kappa(P, st);
@@ -479,18 +479,14 @@ int asd2g_batch_step(asd2g_batch *b, double *dt, int reinit_mode, double tol, in
     launch_bstep_heaviside(P, st);
     launch_bstep_volume(P, st);
     // intermediate velocity (GetIntermediateVel, smoothed Heaviside), its divergence
-    if (order == 0) {
-        launch_bstep_mom_stage(P, 0, BS_U, BS_V, -1, -1, BS_UHAT, BS_VHAT, st);
-    } else if (order == 1) {
-        launch_bstep_mom_stage(P, 0, BS_U, BS_V, -1, -1, BS_UA, BS_VA, st);
-        launch_bstep_fill_uv(P, BS_UA, BS_VA, st);
-        launch_bstep_mom_stage(P, 3, BS_UA, BS_VA, BS_U, BS_V, BS_UHAT, BS_VHAT, st);
-    } else {
-        launch_bstep_mom_stage(P, 0, BS_U, BS_V, -1, -1, BS_UA, BS_VA, st);
-        launch_bstep_fill_uv(P, BS_UA, BS_VA, st);
-        launch_bstep_mom_stage(P, 1, BS_UA, BS_VA, BS_U, BS_V, BS_UB, BS_VB, st);
-        launch_bstep_fill_uv(P, BS_UB, BS_VB, st);
-        launch_bstep_mom_stage(P, 2, BS_UB, BS_VB, BS_U, BS_V, BS_UHAT, BS_VHAT, st);
+    launch_bstep_mom_slot(P, 0, st);
+    if (omax >= 1) {
+        launch_bstep_fill_uv(P, BS_UA, BS_VA, st, 1);
+        launch_bstep_mom_slot(P, 1, st);
+    }
+    if (omax >= 2) {
+        launch_bstep_fill_uv(P, BS_UB, BS_VB, st, 2);
+        launch_bstep_mom_slot(P, 2, st);
     }
     launch_bstep_fill_uv(P, BS_UHAT, BS_VHAT, st);
     cudaMemsetAsync(slot(BS_DIV), 0, slot_bytes, st);

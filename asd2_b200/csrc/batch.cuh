@@ -33,6 +33,8 @@ struct BInst {
     DivH ddx, ddy, d2x, d2y;                       // / dx, / dy, / (2 dx), / (2 dy)
     double kappa_lim, hs_eps;                      // 1 / min(dx, dy); 1.5 min(dx, dy)
     int kappa_fill;                                // the step fills kappa's ghosts (SolvePoisson's recompute)
+    int nreinit;                                   // reinitialisation pseudo-steps of its step
+    int order;                                     // time order of its intermediate velocity (0, 1, 2)
     Sys S;                                         // compact system (diag, cw, ce, cs, cn, minv, b)
     double *x, *r, *pa, *pb, *q, *z;               // flexible CG vectors (compact, FP64)
     KState *ks;                                    // this instance's solver scalars
@@ -118,14 +120,20 @@ struct BStepPlan {
 __device__ __forceinline__ double *bslot(const BInst &I, int f) { return I.pad0 + (size_t)f * I.gstride; }
 void launch_bstep_center_vel(const BStepPlan &P, cudaStream_t st);
 void launch_bstep_fill_p(const BStepPlan &P, int slot, bool kappa_only_if_flagged, cudaStream_t st);
-void launch_bstep_fill_uv(const BStepPlan &P, int su, int sv, cudaStream_t st);
+// U/V ghost fill of slots su, sv of the instances whose time order is at least min_order
+void launch_bstep_fill_uv(const BStepPlan &P, int su, int sv, cudaStream_t st, int min_order = 0);
 void launch_bstep_ls_stage(const BStepPlan &P, int stage, int in, int n, int out, cudaStream_t st);
-void launch_bstep_reinit_pass(const BStepPlan &P, int mode, bool pass_b, cudaStream_t st);
+// pass a or b of pseudo-step k (instances with fewer pseudo-steps skip it)
+void launch_bstep_reinit_pass(const BStepPlan &P, int mode, bool pass_b, int k, cudaStream_t st);
 void launch_bstep_kappa(const BStepPlan &P, cudaStream_t st);
 void launch_bstep_heaviside(const BStepPlan &P, cudaStream_t st);
 void launch_bstep_volume(const BStepPlan &P, cudaStream_t st);
-void launch_bstep_mom_stage(const BStepPlan &P, int kind, int in_u, int in_v, int base_u, int base_v, int out_u,
-                            int out_v, cudaStream_t st);
+// RK stage `slot` (0, 1, 2) of every instance's intermediate velocity in its
+// own time order: order 0: slot 0 = U -> UHAT; order 1: slot 0 = U -> UA,
+// slot 1 = UA (base U) -> UHAT; order 2: slot 0 = U -> UA, slot 1 = UA -> UB,
+// slot 2 = UB -> UHAT (GetIntermediateVel, mac2d.cpp); instances without the
+// slot skip it
+void launch_bstep_mom_slot(const BStepPlan &P, int slot, cudaStream_t st);
 void launch_bstep_divergence(const BStepPlan &P, cudaStream_t st);
 void launch_bstep_update_vel(const BStepPlan &P, cudaStream_t st);
 void launch_bstep_update_dt(const BStepPlan &P, cudaStream_t st);

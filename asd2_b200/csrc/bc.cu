@@ -174,8 +174,9 @@ __global__ void k_bfill_p(const BInst *__restrict__ insts, const BChunk *__restr
     fill_p_entry(I.g, bslot(I, slot), w.c * BSTEP_GHOST_CHUNK + threadIdx.x, 0xF);
 }
 
-__global__ void __launch_bounds__(1024) k_bfill_uv(const BInst *__restrict__ insts, int su, int sv) {
+__global__ void __launch_bounds__(1024) k_bfill_uv(const BInst *__restrict__ insts, int su, int sv, int min_order) {
     const BInst &I = insts[blockIdx.x];
+    if (I.order < min_order) return;
     double *u = bslot(I, su), *v = bslot(I, sv);
     for (int side = 0; side < 4; side++) {
         fill_u_side(I.g, u, side, threadIdx.x, blockDim.x);
@@ -188,8 +189,8 @@ void launch_bstep_fill_p(const BStepPlan &P, int slot, bool kappa_only_if_flagge
     k_bfill_p<<<P.nghost, BSTEP_GHOST_CHUNK, 0, st>>>(P.insts, P.ghost_chunks, slot, kappa_only_if_flagged ? 1 : 0);
 }
 
-void launch_bstep_fill_uv(const BStepPlan &P, int su, int sv, cudaStream_t st) {
-    k_bfill_uv<<<P.count, 1024, 0, st>>>(P.insts, su, sv);
+void launch_bstep_fill_uv(const BStepPlan &P, int su, int sv, cudaStream_t st, int min_order) {
+    k_bfill_uv<<<P.count, 1024, 0, st>>>(P.insts, su, sv, min_order);
 }
 
 // One side of one grid with an explicit fill kind (the per-side methods

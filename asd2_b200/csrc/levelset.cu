@@ -259,15 +259,19 @@ __global__ void __launch_bounds__(TJ *TI) k_bls_stage(const BInst *__restrict__ 
 
 // LS1 = LS - adt S (|grad LS| - 1) into W1; LS = 0.5 (LS + LS2(W1)) (both with ghost mirrors)
 template <int MODE>
-__global__ void __launch_bounds__(TJ *TI) k_breinit_a(const BInst *__restrict__ insts, const BTile *__restrict__ tiles) {
+__global__ void __launch_bounds__(TJ *TI) k_breinit_a(const BInst *__restrict__ insts, const BTile *__restrict__ tiles,
+                                                      int k) {
     const BTile t = tiles[blockIdx.x];
     const BInst &I = insts[t.inst];
+    if (k >= I.nreinit) return;
     reinit_a_tile<MODE, double>(I.g, I.K, bslot(I, BS_LS), bslot(I, BS_LS0), bslot(I, BS_W1), 1, t.bx, t.by);
 }
 template <int MODE>
-__global__ void __launch_bounds__(TJ *TI) k_breinit_b(const BInst *__restrict__ insts, const BTile *__restrict__ tiles) {
+__global__ void __launch_bounds__(TJ *TI) k_breinit_b(const BInst *__restrict__ insts, const BTile *__restrict__ tiles,
+                                                      int k) {
     const BTile t = tiles[blockIdx.x];
     const BInst &I = insts[t.inst];
+    if (k >= I.nreinit) return;
     reinit_b_tile<MODE, double>(I.g, I.K, bslot(I, BS_W1), bslot(I, BS_LS0), bslot(I, BS_LS), bslot(I, BS_LS), 1,
                                 t.bx, t.by);
 }
@@ -283,14 +287,14 @@ void launch_bstep_ls_stage(const BStepPlan &P, int stage, int in, int n, int out
     else k_bls_stage<3><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, in, n, out);
 }
 
-void launch_bstep_reinit_pass(const BStepPlan &P, int mode, bool pass_b, cudaStream_t st) {
+void launch_bstep_reinit_pass(const BStepPlan &P, int mode, bool pass_b, int k, cudaStream_t st) {
     const dim3 blk(TJ, TI);
     if (mode == RM_ORIG) {
-        if (pass_b) k_breinit_b<RM_ORIG><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles);
-        else k_breinit_a<RM_ORIG><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles);
+        if (pass_b) k_breinit_b<RM_ORIG><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, k);
+        else k_breinit_a<RM_ORIG><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, k);
     } else {
-        if (pass_b) k_breinit_b<RM_MINRK2><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles);
-        else k_breinit_a<RM_MINRK2><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles);
+        if (pass_b) k_breinit_b<RM_MINRK2><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, k);
+        else k_breinit_a<RM_MINRK2><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, k);
     }
 }
 

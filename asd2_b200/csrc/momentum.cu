@@ -1,6 +1,8 @@
 // MAC momentum kernels (mac2d.cpp): curvature, Heaviside functions, the
 // WENO5 convection + variable-viscosity + gravity right-hand side fused with
 // the Runge-Kutta stage update, divergence, projection and the CFL time step.
+#include <type_traits>
+
 #include "batch.cuh"
 #include "lsmath.cuh"
 #include "momentum.cuh"
@@ -494,15 +496,30 @@ __global__ void k_bheaviside(const BInst *__restrict__ insts, const BChunk *__re
         if (k0 + t < n) heaviside_cell(I.hs_eps, bslot(I, BS_LS), bslot(I, BS_H), bslot(I, BS_HS), k0 + t);
 }
 
-template <int KIND>
-__global__ void __launch_bounds__(TJ *TI) k_bmom_stage(const BInst *__restrict__ insts, const BTile *__restrict__ tiles,
-                                                         int in_u, int in_v, int base_u, int base_v, int out_u,
-                                                         int out_v) {
+template <int SLOT>
+__global__ void __launch_bounds__(TJ *TI) k_bmom_slot(const BInst *__restrict__ insts, const BTile *__restrict__ tiles) {
     const BTile t = tiles[blockIdx.x];
     const BInst &I = insts[t.inst];
-    mom_stage_tile<KIND>(I.g, I.M, bslot(I, BS_LS), bslot(I, BS_HS), bslot(I, in_u), bslot(I, in_v),
-                         base_u >= 0 ? bslot(I, base_u) : nullptr, base_v >= 0 ? bslot(I, base_v) : nullptr,
-                         bslot(I, out_u), bslot(I, out_v), I.sc, t.bx, t.by);
+    const int o = I.order;
+    auto stage = [&](auto kind, int in_u, int in_v, int base_u, int base_v, int out_u, int out_v) {
+        mom_stage_tile<decltype(kind)::value>(I.g, I.M, bslot(I, BS_LS), bslot(I, BS_HS), bslot(I, in_u),
+                                              bslot(I, in_v), base_u >= 0 ? bslot(I, base_u) : nullptr,
+                                              base_v >= 0 ? bslot(I, base_v) : nullptr, bslot(I, out_u),
+                                              bslot(I, out_v), I.sc, t.bx, t.by);
+    };
+    using K0 = std::integral_constant<int, 0>;
+    using K1 = std::integral_constant<int, 1>;
+    using K2 = std::integral_constant<int, 2>;
+    using K3 = std::integral_constant<int, 3>;
+    if (SLOT == 0) {
+        if (o == 0) stage(K0{}, BS_U, BS_V, -1, -1, BS_UHAT, BS_VHAT);
+        else stage(K0{}, BS_U, BS_V, -1, -1, BS_UA, BS_VA);
+    } else if (SLOT == 1) {
+        if (o == 1) stage(K3{}, BS_UA, BS_VA, BS_U, BS_V, BS_UHAT, BS_VHAT);
+        else if (o == 2) stage(K1{}, BS_UA, BS_VA, BS_U, BS_V, BS_UB, BS_VB);
+    } else {
+        if (o == 2) stage(K2{}, BS_UB, BS_VB, BS_U, BS_V, BS_UHAT, BS_VHAT);
+    }
 }
 
 __global__ void k_bdivergence(const BInst *__restrict__ insts, const BTile *__restrict__ tiles) {
@@ -609,17 +626,11 @@ void launch_bstep_heaviside(const BStepPlan &P, cudaStream_t st) {
 void launch_bstep_volume(const BStepPlan &P, cudaStream_t st) {
     k_bvolume<<<P.nchunks, 256, 0, st>>>(P.insts, P.chunks);
 }
-void launch_bstep_mom_stage(const BStepPlan &P, int kind, int in_u, int in_v, int base_u, int base_v, int out_u,
-                            int out_v, cudaStream_t st) {
+void launch_bstep_mom_slot(const BStepPlan &P, int slot, cudaStream_t st) {
     const dim3 blk(TJ, TI);
-#define BMK(K) k_bmom_stage<K><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, in_u, in_v, base_u, base_v, out_u, out_v)
-    switch (kind) {
-    case 0: BMK(0); break;
-    case 1: BMK(1); break;
-    case 2: BMK(2); break;
-    default: BMK(3); break;
-    }
-#undef BMK
+    if (slot == 0) k_bmom_slot<0><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles);
+    else if (slot == 1) k_bmom_slot<1><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles);
+    else k_bmom_slot<2><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles);
 }
 void launch_bstep_divergence(const BStepPlan &P, cudaStream_t st) {
     k_bdivergence<<<P.ntiles, dim3(TJ, TI), 0, st>>>(P.insts, P.tiles);

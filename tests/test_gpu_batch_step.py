@@ -83,6 +83,43 @@ def test_batch_step_matches_sessions(reinit):
     b.close()
 
 
+def test_batch_step_mixed_orders_and_reinit_counts():
+    """Instances with time orders 0, 1, 2, 2 and reinitialisation pseudo-time
+    limits of 2.25 (the default), 1 and 4 cells (5, about 2 and about 8
+    pseudo-steps) in one batch: each still gives its session's step (level
+    set bit-identical, velocity and pressure to 1e-7)."""
+    import dataclasses
+    spec = [(0, 0.0), (1, 1.0), (2, 4.0), (2, 0.0)]  # (time order, ls_max_atime in cells; 0: default)
+    cases, params, init, dts, sessions = [], [], [], [], []
+    for k, (order, mt) in enumerate(spec):
+        c, g, f = _case(k, *SIDES[k])
+        f = dataclasses.replace(f, time_order=order)
+        p = params_for(g, f, ls_max_atime=mt * min(g.dx, g.dy))
+        s = api.Session(params_for(g, f, ls_max_atime=mt * min(g.dx, g.dy), solver_flags=api.FLAG_NO_PERSIST_MG))
+        s.upload("ls", c.ls)
+        s.upload("u", c.u)
+        s.upload("v", c.v)
+        s.apply_bc("ls", "P")
+        init.append({k2: s.download(k2) for k2 in ("ls", "u", "v")})
+        dts.append(s.update_dt())
+        sessions.append(s)
+        params.append(p)
+    with api.Batch(params) as b:
+        for i, st in enumerate(init):
+            for k2, a in st.items():
+                b.upload(i, k2, a)
+        out = b.step(dts, reinit_mode=api.REINIT_MINRK2, tol=1e-10, maxit=10000)
+        assert out["status"] == 0, out
+        for i, s in enumerate(sessions):
+            r = s.droplet_step(dts[i], reinit_mode=api.REINIT_MINRK2, solver=api.MGPCG, tol=1e-10, maxit=10000)
+            assert r["status"] == 0
+            assert np.array_equal(b.download(i, "ls"), s.download("ls")), i
+            for k2 in ("u", "v", "ps"):
+                assert _rel(interior(b.download(i, k2)), interior(s.download(k2))) <= 1e-7, (i, k2)
+            assert abs(out["dt_next"][i] - r["dt_next"]) <= 1e-7 * r["dt_next"], i
+            s.close()
+
+
 def test_batch_step_refusals():
     c, g, f = _case(0, 48, 48)
     with api.Batch([params_for(g, f)]) as b:
