@@ -19,6 +19,8 @@ namespace asd2g {
 int api_fail(int code, const char *msg);
 int api_grid_from_params(const asd2g_params *p, Grid &g, MomConst &M);
 LsConst make_lsconst(const Grid &g);              // levelset.cu
+template <typename T> LsConstT<T> make_lsconst_t(const Grid &g);
+template <> LsConstT<float> make_lsconst_t<float>(const Grid &g);  // levelset32.cu
 int reinit_steps(double adt, double max_atime);  // levelset.cu
 }  // namespace asd2g
 
@@ -260,7 +262,36 @@ int build(asd2g_batch *b) {
     for (int l = 0; l < MG_MAX_LEVELS; l++)
         if (mg_cells[l]) cudaMemsetAsync(mg_base[l], 0, sizeof(float) * 6 * mg_cells[l], b->st);
     // work lists
-    std::vector<BTile> cells;
+    // mixed instances: the FP32 level-set work arrays, each instance's start
+    // rounded to 64 floats (paired FP32 accesses need 8-byte alignment)
+    {
+        size_t f32tot = 0;
+        std::vector<size_t> f32off(count, 0);
+        for (int i = 0; i < count; i++) {
+            if (b->prm[i].precision != ASD2G_PRECISION_MIXED) continue;
+            f32off[i] = f32tot;
+            f32tot += ((size_t)b->hinst[i].g.sx * b->hinst[i].g.sy + 63) / 64 * 64;
+        }
+        float *f32 = nullptr;
+        if (f32tot) {
+            rc = balloc(b, &f32, (size_t)LS32_ARRAYS * f32tot);
+            if (rc) return rc;
+            cudaMemsetAsync(f32, 0, sizeof(float) * LS32_ARRAYS * f32tot, b->st);
+        }
+        for (int i = 0; i < count; i++) {
+            BInst &I = b->hinst[i];
+            I.mixed = b->prm[i].precision == ASD2G_PRECISION_MIXED ? 1 : 0;
+            if (!I.mixed) continue;
+            float *base = f32 + f32off[i];
+            float **arr[LS32_ARRAYS] = {&I.w32.phi, &I.w32.ls0, &I.w32.a, &I.w32.b, &I.w32.tu, &I.w32.tv};
+            for (int a = 0; a < LS32_ARRAYS; a++) *arr[a] = base + (size_t)a * f32tot;
+            I.w32.band = nullptr;
+            I.w32.band_n = nullptr;
+            I.wk32 = make_weno32_const(I.g);
+            I.K32 = make_lsconst_t<float>(I.g);
+        }
+    }
+    std::vector<BTile> cells, s32, r32;
     std::vector<BChunk> chunks, padc, ghostc;
     std::vector<std::vector<BChunk>> lvl(MG_MAX_LEVELS);
     int max_s = 0, max_nlev = 0;
@@ -270,6 +301,12 @@ int build(asd2g_batch *b) {
         for (int by = 0; by < gy; by++)
             for (int bx = 0; bx < gx; bx++) cells.push_back({i, bx, by});
         for (int c = 0; c < I.chunks; c++) chunks.push_back({i, c});
+        if (I.mixed) {  // FP32 strips: advection 64 columns x 16 rows, reinitialisation 60 x 8
+            for (int by = 0; by < (I.g.nx + 15) / 16; by++)
+                for (int bx = 0; bx < (I.g.ny + 63) / 64; bx++) s32.push_back({i, bx, by});
+            for (int by = 0; by < (I.g.nx + 7) / 8; by++)
+                for (int bx = 0; bx < (I.g.ny + 1 + 59) / 60; bx++) r32.push_back({i, bx, by});
+        }
         const int64_t gi = (int64_t)I.g.sx * I.g.sy, ei = 2 * (int64_t)NB * (I.g.nx + I.g.ny);
         for (int c = 0; c < (int)((gi + BSTEP_PAD_CHUNK - 1) / BSTEP_PAD_CHUNK); c++) padc.push_back({i, c});
         for (int c = 0; c < (int)((ei + BSTEP_GHOST_CHUNK - 1) / BSTEP_GHOST_CHUNK); c++) ghostc.push_back({i, c});
@@ -312,6 +349,11 @@ int build(asd2g_batch *b) {
     SP.npad = (int)padc.size();
     if (!rc) rc = upload_list(b, ghostc, &SP.ghost_chunks);
     SP.nghost = (int)ghostc.size();
+    SP.ns32 = (int)s32.size();
+    SP.nr32 = (int)r32.size();
+    SP.any_mixed = SP.ns32 > 0 ? 1 : 0;
+    if (!rc && SP.ns32) rc = upload_list(b, s32, &SP.s32_tiles);
+    if (!rc && SP.nr32) rc = upload_list(b, r32, &SP.r32_tiles);
     if (rc) return rc;
     if (!batch_cta_prepare()) return api_fail(ASD2G_E_CUDA, "coarse-cycle shared memory attribute");
     return check("batch set-up");
@@ -441,8 +483,8 @@ int asd2g_batch_step(asd2g_batch *b, double *dt, int reinit_mode, double tol, in
     int steps = 0, omax = 0;
     for (int i = 0; i < b->count; i++) {
         const asd2g_params &pp = b->prm[i];
-        if (pp.precision != ASD2G_PRECISION_FP64)
-            return api_fail(ASD2G_E_UNSUPPORTED, "batch_step runs FP64 instances");
+        if (pp.precision != ASD2G_PRECISION_FP64 && pp.precision != ASD2G_PRECISION_MIXED)
+            return api_fail(ASD2G_E_UNSUPPORTED, "batch_step runs FP64 and mixed-precision instances");
         if (pp.time_order < 0 || pp.time_order > 2)
             return api_fail(ASD2G_E_UNSUPPORTED, "batch_step implements time orders 0, 1 and 2");
         steps = b->hinst[i].nreinit > steps ? b->hinst[i].nreinit : steps;
@@ -472,6 +514,29 @@ int asd2g_batch_step(asd2g_batch *b, double *dt, int reinit_mode, double tol, in
     for (int k = 0; k < steps; k++) {
         launch_bstep_reinit_pass(P, reinit_mode, false, k, st);
         launch_bstep_reinit_pass(P, reinit_mode, true, k, st);
+    }
+    // mixed instances: the same level-set step in FP32 (a session's
+    // launch_ls_step32: LS with its ghosts -> FP32, centred velocities, three
+    // packed WENO5/TVD-RK3 stages, lsInit, the packed reinitialisation
+    // pseudo-steps, FP32 -> LS with its ghosts); the FP64 kernels above
+    // skipped these instances and only refilled their P ghosts
+    if (P.any_mixed) {
+        launch_bstep_ls32_convert(P, false, st);
+        launch_bstep_center_vel32(P, st);
+        launch_bstep_ls_stage32(P, 1, 0, 0, 2, st);  // phi -> a
+        launch_bstep_ls_stage32(P, 2, 2, 0, 3, st);  // a -> b
+        launch_bstep_ls_stage32(P, 3, 3, 0, 0, st);  // b -> phi
+        // lsInit: the phi array of the FP32 arena -> its ls0 array, every mixed
+        // instance at once (the first mixed instance starts both arrays)
+        int first = 0;
+        while (!b->hinst[first].mixed) first++;
+        const Ls32Work &w0 = b->hinst[first].w32;
+        cudaMemcpyAsync(w0.ls0, w0.phi, sizeof(float) * (size_t)(w0.ls0 - w0.phi), cudaMemcpyDeviceToDevice, st);
+        for (int k = 0; k < steps; k++) {
+            launch_bstep_reinit32(P, reinit_mode, false, k, st);
+            launch_bstep_reinit32(P, reinit_mode, true, k, st);
+        }
+        launch_bstep_ls32_convert(P, true, st);
     }
     // curvature (with the ghost fill of SolvePoisson's recompute), Heaviside, volume check
     launch_bstep_kappa(P, st);

@@ -5,6 +5,7 @@
 // and batch.cu (host orchestration).
 #pragma once
 #include "asd2g.h"
+#include "ls32.cuh"
 #include "lsmath.cuh"
 #include "mg.cuh"
 
@@ -35,6 +36,11 @@ struct BInst {
     int kappa_fill;                                // the step fills kappa's ghosts (SolvePoisson's recompute)
     int nreinit;                                   // reinitialisation pseudo-steps of its step
     int order;                                     // time order of its intermediate velocity (0, 1, 2)
+    // mixed precision: the level-set advection and reinitialisation in FP32
+    int mixed;
+    Ls32Work w32;                                  // FP32 work arrays (the batch's FP32 arena)
+    Weno32Const wk32;                              // FP32 advection constants
+    LsConstT<float> K32;                           // FP32 reinitialisation constants
     Sys S;                                         // compact system (diag, cw, ce, cs, cn, minv, b)
     double *x, *r, *pa, *pb, *q, *z;               // flexible CG vectors (compact, FP64)
     KState *ks;                                    // this instance's solver scalars
@@ -116,6 +122,11 @@ struct BStepPlan {
     int nghost;
     const BChunk *chunks;        // FCG chunks (1024 interior cells)
     int nchunks;
+    const BTile *s32_tiles;      // mixed instances: FP32 advection strips (64 columns x 16 rows)
+    int ns32;
+    const BTile *r32_tiles;      // mixed instances: FP32 reinitialisation strips (60 columns x 8 rows)
+    int nr32;
+    int any_mixed;
 };
 __device__ __forceinline__ double *bslot(const BInst &I, int f) { return I.pad0 + (size_t)f * I.gstride; }
 void launch_bstep_center_vel(const BStepPlan &P, cudaStream_t st);
@@ -125,6 +136,14 @@ void launch_bstep_fill_uv(const BStepPlan &P, int su, int sv, cudaStream_t st, i
 void launch_bstep_ls_stage(const BStepPlan &P, int stage, int in, int n, int out, cudaStream_t st);
 // pass a or b of pseudo-step k (instances with fewer pseudo-steps skip it)
 void launch_bstep_reinit_pass(const BStepPlan &P, int mode, bool pass_b, int k, cudaStream_t st);
+// Mixed instances' FP32 level-set step (levelset32.cu, weno32.cu,
+// reinit32.cu): FP64 LS <-> FP32 phi (interior and ghosts), the FP32
+// centred velocities, one TVD-RK3 stage (arrays 0 phi, 2 a, 3 b), pass a or
+// b of FP32 reinitialisation pseudo-step k.
+void launch_bstep_ls32_convert(const BStepPlan &P, bool to64, cudaStream_t st);
+void launch_bstep_center_vel32(const BStepPlan &P, cudaStream_t st);
+void launch_bstep_ls_stage32(const BStepPlan &P, int stage, int in, int n, int out, cudaStream_t st);
+void launch_bstep_reinit32(const BStepPlan &P, int mode, bool pass_b, int k, cudaStream_t st);
 void launch_bstep_kappa(const BStepPlan &P, cudaStream_t st);
 void launch_bstep_heaviside(const BStepPlan &P, cudaStream_t st);
 void launch_bstep_volume(const BStepPlan &P, cudaStream_t st);

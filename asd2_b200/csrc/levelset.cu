@@ -245,6 +245,7 @@ __global__ void __launch_bounds__(TJ *TI) k_bcenter_vel(const BInst *__restrict_
                                                           const BTile *__restrict__ tiles) {
     const BTile t = tiles[blockIdx.x];
     const BInst &I = insts[t.inst];
+    if (I.mixed) return;  // the FP32 path
     center_vel_tile<double>(I.g, bslot(I, BS_U), bslot(I, BS_V), bslot(I, BS_TU), bslot(I, BS_TV), t.bx, t.by);
 }
 
@@ -253,6 +254,7 @@ __global__ void __launch_bounds__(TJ *TI) k_bls_stage(const BInst *__restrict__ 
                                                         int in, int n, int out) {
     const BTile t = tiles[blockIdx.x];
     const BInst &I = insts[t.inst];
+    if (I.mixed) return;
     ls_stage_tile<STAGE, double>(I.g, I.ddx, I.ddy, bslot(I, in), bslot(I, BS_TU), bslot(I, BS_TV), bslot(I, n),
                                  bslot(I, out), I.sc, t.bx, t.by);
 }
@@ -263,7 +265,7 @@ __global__ void __launch_bounds__(TJ *TI) k_breinit_a(const BInst *__restrict__ 
                                                       int k) {
     const BTile t = tiles[blockIdx.x];
     const BInst &I = insts[t.inst];
-    if (k >= I.nreinit) return;
+    if (k >= I.nreinit || I.mixed) return;
     reinit_a_tile<MODE, double>(I.g, I.K, bslot(I, BS_LS), bslot(I, BS_LS0), bslot(I, BS_W1), 1, t.bx, t.by);
 }
 template <int MODE>
@@ -271,7 +273,7 @@ __global__ void __launch_bounds__(TJ *TI) k_breinit_b(const BInst *__restrict__ 
                                                       int k) {
     const BTile t = tiles[blockIdx.x];
     const BInst &I = insts[t.inst];
-    if (k >= I.nreinit) return;
+    if (k >= I.nreinit || I.mixed) return;
     reinit_b_tile<MODE, double>(I.g, I.K, bslot(I, BS_W1), bslot(I, BS_LS0), bslot(I, BS_LS), bslot(I, BS_LS), 1,
                                 t.bx, t.by);
 }

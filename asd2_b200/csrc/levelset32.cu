@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstring>
 
+#include "batch.cuh"
 #include "levelset_impl.cuh"
 #include "ls32.cuh"
 
@@ -113,7 +114,36 @@ bool packed_reinit() {
 int64_t padded(const Grid &g) { return (int64_t)g.sx * g.sy; }
 int conv_blocks(int64_t n) { return (int)((n + 255) / 256 < 4 * 148 ? (n + 255) / 256 : 4 * 148); }
 
+// Batched (mixed instances): FP64 LS <-> FP32 phi over each instance's
+// padded cells, and the FP32 centred velocities over its cell tiles.
+__global__ void k_bls32_convert(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks, int to64) {
+    const BChunk w = chunks[blockIdx.x];
+    const BInst &I = insts[w.inst];
+    if (!I.mixed) return;
+    const int64_t n = (int64_t)I.g.sx * I.g.sy, k = (int64_t)w.c * BSTEP_PAD_CHUNK + threadIdx.x;
+    if (k >= n) return;
+    double *ls = bslot(I, BS_LS);
+    if (to64) ls[k] = (double)I.w32.phi[k];
+    else I.w32.phi[k] = (float)ls[k];
+}
+
+__global__ void __launch_bounds__(TJ *TI) k_bcenter_vel32(const BInst *__restrict__ insts,
+                                                            const BTile *__restrict__ tiles) {
+    const BTile t = tiles[blockIdx.x];
+    const BInst &I = insts[t.inst];
+    if (!I.mixed) return;
+    center_vel_tile<float>(I.g, bslot(I, BS_U), bslot(I, BS_V), I.w32.tu, I.w32.tv, t.bx, t.by);
+}
+
 }  // namespace
+
+void launch_bstep_ls32_convert(const BStepPlan &P, bool to64, cudaStream_t st) {
+    if (P.any_mixed) k_bls32_convert<<<P.npad, BSTEP_PAD_CHUNK, 0, st>>>(P.insts, P.pad_chunks, to64 ? 1 : 0);
+}
+
+void launch_bstep_center_vel32(const BStepPlan &P, cudaStream_t st) {
+    if (P.any_mixed) k_bcenter_vel32<<<P.ntiles, dim3(TJ, TI), 0, st>>>(P.insts, P.tiles);
+}
 
 int reinit_steps(double adt, double max_atime);  // levelset.cu
 

@@ -4,6 +4,13 @@
 
 namespace asd2g {
 
+// Constants of the FP32 advection stage.
+struct Weno32Const {
+    float hx, hy;      // 0.5 / dx, 0.5 / dy
+    float epsx, epsy;  // 1e-6 dx^2, 1e-6 dy^2
+};
+Weno32Const make_weno32_const(const Grid &g);
+
 // FP32 work arrays of the mixed level-set step, each (nx+6) x (ny+6).
 struct Ls32Work {
     float *phi, *ls0, *a, *b, *tu, *tv;

@@ -46,6 +46,7 @@
 #include <cstdint>
 #include <cstdlib>
 
+#include "batch.cuh"
 #include "levelset_impl.cuh"
 #include "ls32.cuh"
 
@@ -117,18 +118,20 @@ __device__ __noinline__ float4 subcell_fix(const float *__restrict__ src, const 
 // modes use the subcell derivatives next to the interface.  out2, when not
 // null, receives the same values (the Sussman mode's phi).  base may alias
 // out2: it is read only at the lane's own cells, before they are written.
+// The strip bx x row block by; the single-grid kernel takes them from its
+// block index, the batched one from its work list.
 template <int PASS, int MODE, bool VEC, int R>
-__global__ void __launch_bounds__(32 * RI_WARPS, R == 1 ? 8 : (R == 2 ? 7 : (R == 4 ? 6 : 4)))
-    k_reinit32(Grid g, LsConstT<float> K, const float *__restrict__ src, const float *__restrict__ ls0,
-               const float *base, float *out, float *out2, int *band, unsigned *band_n) {
+__device__ __forceinline__ void reinit32_strip(const Grid &g, const LsConstT<float> &K, const float *__restrict__ src,
+                                               const float *__restrict__ ls0, const float *base, float *out,
+                                               float *out2, int *band, unsigned *band_n, int bx, int by) {
     constexpr bool SUB = (MODE == RM_MINRK2 || MODE == RM_MINRK2_SUSS);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     // the first pass of a pseudo-step empties the band list the second fills
-    if (PASS == 0 && band_n && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *band_n = 0u;
-    const int ib = NB + (blockIdx.y * RI_WARPS + w) * R;
+    if (PASS == 0 && band_n && bx == 0 && by == 0 && threadIdx.x == 0) *band_n = 0u;
+    const int ib = NB + (by * RI_WARPS + w) * R;
     if (ib >= g.nx + NB) return;  // whole warp
     const int ie = min(ib + R, g.nx + NB);
-    const int J0 = blockIdx.x * RI_OUT;
+    const int J0 = bx * RI_OUT;
     const int c0 = J0 + 2 * lane;
     const int sx = g.sx, sy = g.sy;
     const bool own = lane >= 1 && lane <= 30;
@@ -302,6 +305,32 @@ __global__ void __launch_bounds__(128)
     }
 }
 
+template <int PASS, int MODE, bool VEC, int R>
+__global__ void __launch_bounds__(32 * RI_WARPS, R == 1 ? 8 : (R == 2 ? 7 : (R == 4 ? 6 : 4)))
+    k_reinit32(Grid g, LsConstT<float> K, const float *__restrict__ src, const float *__restrict__ ls0,
+               const float *base, float *out, float *out2, int *band, unsigned *band_n) {
+    reinit32_strip<PASS, MODE, VEC, R>(g, K, src, ls0, base, out, out2, band, band_n, blockIdx.x, blockIdx.y);
+}
+
+// Batched (modes Original and MinRK2, 2 rows per warp): work-list entry =
+// (instance, strip, row block) of the mixed instances; pseudo-step k of
+// every instance that has it.  Pass a: phi -> a; pass b: (phi, a) -> phi.
+template <int PASS, int MODE>
+__global__ void __launch_bounds__(32 * RI_WARPS, 7)
+    k_breinit32(const BInst *__restrict__ insts, const BTile *__restrict__ tiles, int k) {
+    const BTile t = tiles[blockIdx.x];
+    const BInst &I = insts[t.inst];
+    if (k >= I.nreinit) return;
+    const Grid g = I.g;
+    const LsConstT<float> K = I.K32;
+    const Ls32Work w = I.w32;
+    const float *src = PASS == 0 ? w.phi : w.a;
+    float *out = PASS == 0 ? w.a : w.phi;
+    const float *base = PASS == 0 ? nullptr : w.phi;
+    if (g.sy % 2 == 0) reinit32_strip<PASS, MODE, true, 2>(g, K, src, w.ls0, base, out, nullptr, nullptr, nullptr, t.bx, t.by);
+    else reinit32_strip<PASS, MODE, false, 2>(g, K, src, w.ls0, base, out, nullptr, nullptr, nullptr, t.bx, t.by);
+}
+
 template <int PASS, int MODE, bool VEC>
 void launch_v(const Grid &g, const LsConstT<float> &K, int rows, const float *src, const float *ls0,
               const float *base, float *out, float *out2, int *band, unsigned *band_n, cudaStream_t st) {
@@ -329,6 +358,18 @@ void launch_p(const Grid &g, const LsConstT<float> &K, int rows, bool vec, const
 bool aligned8(const void *p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 7u) == 0; }
 
 }  // namespace
+
+void launch_bstep_reinit32(const BStepPlan &P, int mode, bool pass_b, int k, cudaStream_t st) {
+    if (P.nr32 == 0) return;
+    const int nt = 32 * RI_WARPS;
+    if (mode == RM_ORIG) {
+        if (pass_b) k_breinit32<1, RM_ORIG><<<P.nr32, nt, 0, st>>>(P.insts, P.r32_tiles, k);
+        else k_breinit32<0, RM_ORIG><<<P.nr32, nt, 0, st>>>(P.insts, P.r32_tiles, k);
+    } else {
+        if (pass_b) k_breinit32<1, RM_MINRK2><<<P.nr32, nt, 0, st>>>(P.insts, P.r32_tiles, k);
+        else k_breinit32<0, RM_MINRK2><<<P.nr32, nt, 0, st>>>(P.insts, P.r32_tiles, k);
+    }
+}
 
 // Rows per warp of the FP32 reinitialisation passes: 2 (one pseudo-step at
 // 2048^2 took 50.7 / 48.6 / 55.8 / 74.7 us with 1 / 2 / 4 / 8 rows: the

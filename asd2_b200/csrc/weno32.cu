@@ -35,6 +35,7 @@
 // producer-side P fills).
 #include <cstdlib>
 
+#include "batch.cuh"
 #include "internal.cuh"
 #include "ls32.cuh"
 
@@ -94,23 +95,21 @@ __device__ __forceinline__ float2 weno2(float2 v0, float2 v1, float2 v2, float2 
     return mul2(num, rcp2(den));
 }
 
-struct Weno32Const {
-    float hx, hy;      // 0.5 / dx, 0.5 / dy
-    float epsx, epsy;  // 1e-6 dx^2, 1e-6 dy^2
-};
-
+// One strip (64 columns, bx) x row block (by) of the stage; the single-grid
+// kernel takes them from its block index, the batched one from its work list.
 template <int STAGE, int R>
-__global__ void __launch_bounds__(32 * W32_WARPS, 4)
-    k_ls_stage32(Grid g, Weno32Const K, const float *__restrict__ phi_in, const float *__restrict__ tu,
-                 const float *__restrict__ tv, const float *phi_n, float *out, const double *__restrict__ dtp) {
+__device__ __forceinline__ void ls_stage32_strip(const Grid &g, const Weno32Const &K, const float *__restrict__ phi_in,
+                                                 const float *__restrict__ tu, const float *__restrict__ tv,
+                                                 const float *phi_n, float *out, const double *__restrict__ dtp,
+                                                 int bx, int by) {
     __shared__ float2 sF[W32_WARPS][W32_COLS + 6];     // F_y of rows (i, i+1) at column j0-3+k
     __shared__ float2 sT[W32_WARPS][3][W32_COLS + 4];  // reciprocals a, b, c of rows (i, i+1) at column j0-2+k
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sx = g.sx, sy = g.sy;
-    const int ib = NB + (blockIdx.y * W32_WARPS + w) * R;
+    const int ib = NB + (by * W32_WARPS + w) * R;
     if (ib >= g.nx + NB) return;  // whole warp
     const int ie = min(ib + R, g.nx + NB);
-    const int j0 = NB + blockIdx.x * W32_COLS;
+    const int j0 = NB + bx * W32_COLS;
     const int cA = j0 + lane, cB = cA + 32;
     const bool inA = cA < sy, inB = cB < sy;
     float2 *sf = sF[w];
@@ -118,7 +117,7 @@ __global__ void __launch_bounds__(32 * W32_WARPS, 4)
     const float2 epsx = p2(K.epsx), epsy = p2(K.epsy);
     const float dt = (float)*dtp;
     // warps whose cells include ones within three of a boundary write ghost mirrors
-    const bool edge = blockIdx.x == 0 || j0 + W32_COLS > g.ny || ib < 2 * NB || ie > g.nx;
+    const bool edge = bx == 0 || j0 + W32_COLS > g.ny || ib < 2 * NB || ie > g.nx;
 
     auto ld = [&](const float *a, int i, int c, bool in) -> float {
         return (in && i < sx) ? __ldg(a + (int64_t)i * sy + c) : 0.f;
@@ -278,6 +277,26 @@ __global__ void __launch_bounds__(32 * W32_WARPS, 4)
 }
 
 template <int STAGE, int R>
+__global__ void __launch_bounds__(32 * W32_WARPS, 4)
+    k_ls_stage32(Grid g, Weno32Const K, const float *__restrict__ phi_in, const float *__restrict__ tu,
+                 const float *__restrict__ tv, const float *phi_n, float *out, const double *__restrict__ dtp) {
+    ls_stage32_strip<STAGE, R>(g, K, phi_in, tu, tv, phi_n, out, dtp, blockIdx.x, blockIdx.y);
+}
+
+// Batched: work-list entry = (instance, strip, row block) of the mixed
+// instances; arrays by index into the instance's FP32 work (0 phi, 2 a, 3 b).
+template <int STAGE, int R>
+__global__ void __launch_bounds__(32 * W32_WARPS, 4)
+    k_bls_stage32(const BInst *__restrict__ insts, const BTile *__restrict__ tiles, int in, int n, int out) {
+    const BTile t = tiles[blockIdx.x];
+    const BInst &I = insts[t.inst];
+    const Grid g = I.g;
+    const Weno32Const K = I.wk32;
+    float *const a[4] = {I.w32.phi, I.w32.ls0, I.w32.a, I.w32.b};
+    ls_stage32_strip<STAGE, R>(g, K, a[in], I.w32.tu, I.w32.tv, a[n], a[out], I.sc, t.bx, t.by);
+}
+
+template <int STAGE, int R>
 void launch_r(const Grid &g, const Weno32Const &K, const float *phi_in, const float *tu, const float *tv,
               const float *phi_n, float *out, const double *dtp, cudaStream_t st) {
     const dim3 grd((g.ny + W32_COLS - 1) / W32_COLS, (g.nx + W32_WARPS * R - 1) / (W32_WARPS * R));
@@ -311,13 +330,28 @@ int ls32_rows_per_warp(const Grid &) {
     return rows;
 }
 
-void launch_ls_stage32(const Grid &g, int stage, const float *phi_in, const float *tu, const float *tv,
-                       const float *phi_n, float *out, const double *dtp, cudaStream_t st) {
+Weno32Const make_weno32_const(const Grid &g) {
     Weno32Const K;
     K.hx = (float)(0.5 / g.dx);
     K.hy = (float)(0.5 / g.dy);
     K.epsx = (float)(1e-6 * g.dx * g.dx);
     K.epsy = (float)(1e-6 * g.dy * g.dy);
+    return K;
+}
+
+void launch_bstep_ls_stage32(const BStepPlan &P, int stage, int in, int n, int out, cudaStream_t st) {
+    if (P.ns32 == 0) return;
+    constexpr int R = 4;  // the tile lists are built for 4 rows per warp
+#define BS32(S) k_bls_stage32<S, R><<<P.ns32, 32 * W32_WARPS, 0, st>>>(P.insts, P.s32_tiles, in, n, out)
+    if (stage == 1) BS32(1);
+    else if (stage == 2) BS32(2);
+    else BS32(3);
+#undef BS32
+}
+
+void launch_ls_stage32(const Grid &g, int stage, const float *phi_in, const float *tu, const float *tv,
+                       const float *phi_n, float *out, const double *dtp, cudaStream_t st) {
+    const Weno32Const K = make_weno32_const(g);
     if (stage == 1) launch_s<1>(g, K, phi_in, tu, tv, phi_n, out, dtp, st);
     else if (stage == 2) launch_s<2>(g, K, phi_in, tu, tv, phi_n, out, dtp, st);
     else launch_s<3>(g, K, phi_in, tu, tv, phi_n, out, dtp, st);

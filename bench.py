@@ -705,9 +705,34 @@ def batched_steps(sh, stream, count=BATCH_COUNT, steps=10):
         worst = max(worst, float(np.max(r["resid"])))
         dt = r["dt_next"]
     b.close()
+    # the same batch with every instance in mixed precision (FP32 level-set
+    # advection and reinitialisation); steps 2.. timed
+    bm = api.Batch([api.Params.from_case(c, precision=api.PRECISION_MIXED) for c in cases], stream=sh)
+    for i, st in enumerate(init):
+        for k, a in st.items():
+            bm.upload(i, k, a)
+    dtm = np.array(dts)
+    tm = []
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        r = bm.step(dtm, tol=TOL, maxit=100000)
+        e1.record(stream)
+        e1.synchronize()
+        if r["status"] != 0:
+            raise SystemExit(f"bench: batched mixed step failed: {r['status']}")
+        if k > 0:
+            tm.append(e0.elapsed_time(e1) / 1e3)
+        dtm = r["dt_next"]
+    bm.close()
+    mixed = {"value": count * len(tm) / float(sum(tm)), "unit": "droplet steps/s",
+             "ms_per_batch_step": 1e3 * float(np.mean(tm)), "steps_timed": len(tm),
+             "precision": "mixed (FP32 level-set advection and reinitialisation, packed kernels over the batch)"}
     cells = int(sum(c.nx * c.ny for c in cases))
     t_b = float(sum(times))
-    return {"workload": f"{count} droplets, grid side uniform in {{64, 96, ..., 512}} ({cells / 1e6:.1f} M cells), "
+    return {"mixed_precision": mixed,
+            "workload": f"{count} droplets, grid side uniform in {{64, 96, ..., 512}} ({cells / 1e6:.1f} M cells), "
                         f"radius [0.08, 0.2], density ratio log-U[1, 1000], viscosity ratio log-U[1, 100]; {steps} "
                         f"full steps from rest, pressure to rel. residual {TOL:g}",
             "value": count * steps / t_b, "unit": "droplet steps/s",

@@ -286,7 +286,9 @@ int asd2g_batch_sync(asd2g_batch *b);
  * for the whole batch: level-set advection, reinitialisation (reinit_mode 0
  * or 2), curvature, Heaviside, FP64 volume check, intermediate velocity,
  * divergence, GFM assembly, batched MG-FCG to tol, projection, next dt.
- * Instances: FP64; each keeps its own time order (0, 1, 2) and its own
+ * Instances: FP64 or mixed precision (the level-set advection and
+ * reinitialisation in FP32, as asd2g_droplet_step of a mixed session does);
+ * each keeps its own time order (0, 1, 2) and its own
  * reinitialisation step count (ls_max_atime), the phases running up to the
  * largest and the instances without a phase skipping it.
  * dt[count]: each instance's step dt, replaced by its next dt.  Fields LS, U,

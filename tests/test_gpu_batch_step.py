@@ -120,6 +120,57 @@ def test_batch_step_mixed_orders_and_reinit_counts():
             s.close()
 
 
+def test_batch_step_mixed_precision_instances():
+    """Mixed-precision instances (FP32 level-set advection and
+    reinitialisation) beside FP64 ones in one batch: each gives its
+    session's step in the same precision, the level set bit-identical (the
+    batched FP32 kernels run the sessions' strip functions), pressure to
+    1e-7, velocity to 5e-6; after a second step the level set agrees to 1e-9 (FP64)
+    and 1e-6 (mixed: FP32 rounding of the slightly different velocities)."""
+    precs = [api.PRECISION_MIXED, api.PRECISION_FP64, api.PRECISION_MIXED, api.PRECISION_MIXED, api.PRECISION_FP64,
+             api.PRECISION_MIXED]
+    cases, params, init, dts, sessions = [], [], [], [], []
+    for k, (nx, ny) in enumerate(SIDES):
+        c, g, f = _case(k, nx, ny)
+        params.append(params_for(g, f, precision=precs[k]))
+        s = api.Session(params_for(g, f, precision=precs[k], solver_flags=api.FLAG_NO_PERSIST_MG))
+        s.upload("ls", c.ls)
+        s.upload("u", c.u)
+        s.upload("v", c.v)
+        s.apply_bc("ls", "P")
+        init.append({k2: s.download(k2) for k2 in ("ls", "u", "v")})
+        dts.append(s.update_dt())
+        sessions.append(s)
+    with api.Batch(params) as b:
+        for i, st in enumerate(init):
+            for k2, a in st.items():
+                b.upload(i, k2, a)
+        out = b.step(dts, reinit_mode=api.REINIT_MINRK2, tol=1e-10, maxit=10000)
+        assert out["status"] == 0, out
+        nxt = []
+        for i, s in enumerate(sessions):
+            r = s.droplet_step(dts[i], reinit_mode=api.REINIT_MINRK2, solver=api.MGPCG, tol=1e-10, maxit=10000)
+            assert r["status"] == 0
+            assert np.array_equal(b.download(i, "ls"), s.download("ls")), i
+            # pressure to 1e-7; the velocities of a droplet one step from rest
+            # are the small remainder of pressure gradient against surface
+            # tension, so the solves' 1e-10 reaches them amplified (measured
+            # up to 5.6e-7)
+            for k2, bar in (("ps", 1e-7), ("u", 5e-6), ("v", 5e-6)):
+                assert _rel(interior(b.download(i, k2)), interior(s.download(k2))) <= bar, (i, k2)
+            nxt.append(r["dt_next"])
+        out2 = b.step(out["dt_next"], reinit_mode=api.REINIT_MINRK2, tol=1e-10, maxit=10000)
+        assert out2["status"] == 0
+        for i, s in enumerate(sessions):
+            r = s.droplet_step(nxt[i], reinit_mode=api.REINIT_MINRK2, solver=api.MGPCG, tol=1e-10, maxit=10000)
+            assert r["status"] == 0
+            # the velocities entering step 2 differ by the solves' 1e-10; in
+            # FP32 that moves phi by a few ulps (6e-8 relative)
+            bar = 1e-6 if precs[i] == api.PRECISION_MIXED else 1e-9
+            assert _rel(interior(b.download(i, "ls")), interior(s.download("ls"))) <= bar, i
+            s.close()
+
+
 def test_batch_step_refusals():
     c, g, f = _case(0, 48, 48)
     with api.Batch([params_for(g, f)]) as b:
