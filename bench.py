@@ -616,26 +616,27 @@ def learned_pc_512(sh, stream, flush, weights=None, n=512, counts=tuple(range(1,
             "systems": rows, "l2": "flushed (256 MB write) before each timed solve"}
 
 
-def unet_forward(sh, stream, sizes=(256, 512), reps=20):
-    """Forward pass of the learned preconditioner's U-Net (random weights, one
-    image with the 4 feature channels) at each size: CUDA-event time per
-    pass after 3 warm-up passes, and the convolution FLOPs it performs."""
+def unet_forward(sh, stream, shapes=((1, 256), (1, 512), (22, 192)), reps=20):
+    """Forward pass of the learned preconditioner's U-Net (random weights, B
+    images of n x n with the 4 feature channels; 22 x 192² is one size group
+    of the 256-droplet batch): CUDA-event time per pass after 3 warm-up
+    passes, and the convolution FLOPs it performs."""
     import torch
     from asd2_b200 import api
     lay, _ = api.UNet.layout()
     out = {}
-    for n in sizes:
-        net = api.UNet(1, n, n, stream=sh)
+    for B, n in shapes:
+        net = api.UNet(B, n, n, stream=sh)
         net.init(1)
-        f = torch.randn(1, n, n, 4, device="cuda")
-        o = torch.empty(1, n, n, device="cuda")
+        f = torch.randn(B, n, n, 4, device="cuda")
+        o = torch.empty(B, n, n, device="cuda")
         for _ in range(3):
-            net.forward(f, o, 1, n, n)
+            net.forward(f, o, B, n, n)
         with torch.cuda.stream(stream):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
         for _ in range(reps):
-            net.forward(f, o, 1, n, n)
+            net.forward(f, o, B, n, n)
         e1.record(stream)
         e1.synchronize()
         t = e0.elapsed_time(e1) / 1e3 / reps
@@ -644,8 +645,8 @@ def unet_forward(sh, stream, sizes=(256, 512), reps=20):
         flops = 0
         for i, (wo, bo, cin, cout, relu) in enumerate(lay):
             lv = i // 2 if i < 8 else (2 - (i - 8) // 2 if i < 14 else 0)
-            flops += 2 * 9 * cin * cout * (n >> lv) ** 2
-        out[str(n)] = {"us_per_forward": t * 1e6, "gflop": flops / 1e9, "tflops": flops / t / 1e12,
+            flops += 2 * 9 * cin * cout * B * (n >> lv) ** 2
+        out[str(n) if B == 1 else f"{B}x{n}"] = {"us_per_forward": t * 1e6, "gflop": flops / 1e9, "tflops": flops / t / 1e12,
                        "finite": bool(torch.isfinite(o).all())}
         net.close()
     return {"workload": "U-Net forward (15 tcgen05 convolutions, BF16), batch 1", "sizes": out}
