@@ -1,7 +1,8 @@
 // Tensor-core building blocks of the learned preconditioner (U-Net): a 3x3
 // "same" convolution as an implicit GEMM on tcgen05 (BF16 activations and
 // weights, FP32 accumulation in tensor memory), and the weight packing it
-// reads.  No reference counterpart (the reference has no learned solver).
+// reads, and the weight gradient of a 3x3 convolution (k_wgrad_tc).  No
+// reference counterpart (the reference has no learned solver).
 //
 // Implicit GEMM: D[p][co] = sum over taps t and input channels ci of
 // X[p + off(t)][ci] * W[co][t][ci] for a tile of 128 consecutive output
@@ -449,6 +450,175 @@ __global__ void __launch_bounds__(CONV_THREADS *ConvW<COUT, NKC>::NW, 1)
     if (warp == 0) tmem_dealloc(*tslot, (uint32_t)C::COLS);
 }
 
+// ------------------------------------------------------------ weight grad --
+// Weight gradient of a 3x3 convolution on the tensor cores:
+//   dW[co][ci][t] = sum_p G[p][co] X[p + off(t)][ci],   db[co] = sum_p G[p][co]
+// as D[r][co] = sum_p A[r][p] B[co][p] with rows r = t CI + ci (and one row of
+// ones for the bias after the last), columns co (Cout padded, N = COS), K =
+// output pixels.  A CTA owns one 128-row tile of r and a contiguous range of
+// pixels (split-K); per chunk of 64 pixels its threads gather and transpose
+// the X and G values into the K-major canonical layout (thread r of the tile
+// builds row r; columns from consecutive channels, so each pixel's loads are
+// coalesced across the warp), one thread issues four tcgen05.mma (K = 16
+// each) into the TMEM accumulator, and two stages alternate.  The partial
+// sums of every CTA go to a buffer that one more kernel adds in a fixed
+// order (deterministic, no atomics).
+constexpr int WG_KC = 64;                       // pixels per stage
+constexpr int WG_ROWS = 128;                    // rows of r per CTA (M)
+constexpr int WG_A_BYTES = WG_ROWS * WG_KC * 2; // 16 KB
+__host__ __device__ constexpr int wg_b_bytes(int cos) { return cos * WG_KC * 2; }
+__host__ __device__ constexpr int wg_smem(int cos) { return 2 * (WG_A_BYTES + wg_b_bytes(cos)) + 2 * 8 + 16; }
+
+// 8 consecutive BF16 values -> one 16-byte core-matrix row
+__device__ __forceinline__ uint4 pack8(const __nv_bfloat16 (&v)[8]) {
+    uint4 u;
+    u.x = (uint32_t)__bfloat16_as_ushort(v[0]) | ((uint32_t)__bfloat16_as_ushort(v[1]) << 16);
+    u.y = (uint32_t)__bfloat16_as_ushort(v[2]) | ((uint32_t)__bfloat16_as_ushort(v[3]) << 16);
+    u.z = (uint32_t)__bfloat16_as_ushort(v[4]) | ((uint32_t)__bfloat16_as_ushort(v[5]) << 16);
+    u.w = (uint32_t)__bfloat16_as_ushort(v[6]) | ((uint32_t)__bfloat16_as_ushort(v[7]) << 16);
+    return u;
+}
+
+template <int COS>
+__global__ void __launch_bounds__(WG_ROWS) k_wgrad_tc(const __nv_bfloat16 *__restrict__ X,
+                                                      const __nv_bfloat16 *__restrict__ G, int H, int W, int CIS,
+                                                      int CI, int64_t P, int64_t KP, float *__restrict__ part,
+                                                      int *err) {
+    extern __shared__ __align__(128) uint8_t sm[];
+    constexpr int BB = wg_b_bytes(COS);
+    constexpr int SB = WG_A_BYTES + BB;  // one stage: A then B
+    constexpr uint32_t NCOL = COS <= 32 ? 32 : COS <= 64 ? 64 : COS <= 128 ? 128 : 256;
+    constexpr uint32_t IDESC = umma_idesc_bf16(128, COS);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + 2 * SB);  // per stage: its MMAs completed
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int R = 9 * CI;                    // rows of dW; row R is the bias (ones)
+    const int r = blockIdx.y * WG_ROWS + tid;  // this thread's A row
+    const int t = r < R ? r / CI : 0, ci = r < R ? r - t * CI : 0;
+    const int dy = t / 3 - 1, dx = t % 3 - 1;
+    const int64_t p_begin = (int64_t)blockIdx.x * KP;
+    const int64_t p_end = p_begin + KP < P ? p_begin + KP : P;
+    const int nch = (int)((p_end - p_begin + WG_KC - 1) / WG_KC);
+    if (tid == 0) {
+        mbar_init(mbar, 1);
+        mbar_init(mbar + 1, 1);
+        mbar_init_fence();
+    }
+    if (warp == 0) {
+        tmem_alloc(tslot, NCOL);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f), one = __float2bfloat16_rn(1.0f);
+    bool ok = true;
+    int issued = 0;  // chunks whose MMAs were committed
+    for (int c = 0; c < nch; c++) {
+        const int st = c & 1;
+        uint8_t *A = sm + st * SB, *Bm = A + WG_A_BYTES;
+        if (c >= 2) {  // the stage's previous MMAs (chunk c - 2) are done
+            const bool w = tid != 0 || mbar_wait_hw(mbar + st, (uint32_t)((c - 2) >> 1) & 1u, err, 5);
+            if (!__syncthreads_and(w)) {
+                ok = false;
+                break;
+            }
+        }
+        // gather and transpose: 8 groups of 8 pixels, group g -> core-matrix plane g
+        const int64_t p0 = p_begin + (int64_t)c * WG_KC;
+        int64_t q = p0 / W;
+        int x = (int)(p0 - q * W);
+        int y = (int)(q % H);
+        int64_t b = q / H;
+#pragma unroll 1
+        for (int g = 0; g < WG_KC / 8; g++) {
+            __nv_bfloat16 va[8], vb0[8], vb1[8];
+#pragma unroll
+            for (int e = 0; e < 8; e++) {
+                const int64_t p = p0 + g * 8 + e;
+                const bool in = p < p_end;
+                __nv_bfloat16 a = zero;
+                if (in && r < R) {
+                    const int yy = y + dy, xx = x + dx;
+                    if (yy >= 0 && yy < H && xx >= 0 && xx < W) a = X[((b * H + yy) * W + xx) * CIS + ci];
+                } else if (in && r == R) {
+                    a = one;
+                }
+                va[e] = a;
+                vb0[e] = (in && tid < COS) ? G[p * COS + tid] : zero;
+                if (COS > WG_ROWS) vb1[e] = (in && tid + WG_ROWS < COS) ? G[p * COS + tid + WG_ROWS] : zero;
+                if (++x == W) {  // next pixel
+                    x = 0;
+                    if (++y == H) {
+                        y = 0;
+                        b++;
+                    }
+                }
+            }
+            *reinterpret_cast<uint4 *>(A + g * (WG_ROWS * 16) + tid * 16) = pack8(va);
+            if (tid < COS) *reinterpret_cast<uint4 *>(Bm + g * (COS * 16) + tid * 16) = pack8(vb0);
+            if (COS > WG_ROWS && tid + WG_ROWS < COS)
+                *reinterpret_cast<uint4 *>(Bm + g * (COS * 16) + (tid + WG_ROWS) * 16) = pack8(vb1);
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(A), b0 = smem_u32(Bm);
+#pragma unroll
+            for (int s = 0; s < WG_KC / 16; s++) {
+                const uint64_t ad = umma_desc_k(a0 + (uint32_t)(2 * s) * (WG_ROWS * 16), WG_ROWS * 16, 128u);
+                const uint64_t bd = umma_desc_k(b0 + (uint32_t)(2 * s) * (COS * 16), COS * 16, 128u);
+                umma_bf16(tmem, ad, bd, IDESC, (c > 0 || s > 0) ? 1u : 0u);
+            }
+            umma_commit(mbar + st);
+        }
+        issued = c + 1;
+    }
+    // the last commit arrives once every MMA of the CTA completed (also
+    // before TMEM is released on an early exit)
+    const bool w = tid != 0 || issued == 0 ||
+                   mbar_wait_hw(mbar + ((issued - 1) & 1), (uint32_t)((issued - 1) >> 1) & 1u, err, 5);
+    ok = __syncthreads_and(ok && w && issued == nch && nch > 0);
+    tc_fence_after();
+    if (ok) {
+        const int row = warp * 32 + lane;
+        float *dst = part + ((size_t)blockIdx.x * gridDim.y + blockIdx.y) * (size_t)WG_ROWS * COS + (size_t)row * COS;
+#pragma unroll
+        for (int c0 = 0; c0 < COS; c0 += 16) {
+            uint32_t v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int i = 0; i < 16; i++) dst[c0 + i] = __uint_as_float(v[i]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, NCOL);
+}
+
+// dW[co][ci][t] += sum over the split-K partials (fixed order), db[co] += the bias row's
+__global__ void k_wgrad_reduce(const float *__restrict__ part, int Z, int MT, int COS, int CI, int CO,
+                               float *__restrict__ dW, float *__restrict__ db) {
+    const int R = 9 * CI;
+    const int64_t n = (int64_t)(R + 1) * CO;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e / CO), co = (int)(e - (int64_t)r * CO);
+        const size_t stride = (size_t)MT * WG_ROWS * COS;
+        const size_t off = (size_t)(r / WG_ROWS) * WG_ROWS * COS + (size_t)(r % WG_ROWS) * COS + co;
+        float s = 0.0f;
+        for (int z = 0; z < Z; z++) s += part[(size_t)z * stride + off];
+        if (r < R) {
+            const int t = r / CI, ci = r - t * CI;
+            dW[((size_t)co * CI + ci) * 9 + t] += s;
+        } else {
+            db[co] += s;
+        }
+    }
+}
+
 // w[co][ci][3][3] (FP32, cout x cin real channels) -> wpack[kc][tap][half][co][8]
 // (BF16, padded to cout_pad x cin_pad with zeros).
 __global__ void k_pack_conv(const float *__restrict__ w, int cout, int cin, int cout_pad, int cin_pad,
@@ -585,6 +755,42 @@ int conv3x3_tc(const void *in, int n, int h, int w, int cin, const void *wpack, 
     case 192: return conv_launch<192>(in, low, cl, n, h, w, cin, wpack, bias, out, out32, relu, err, st);
     default: return ASD2G_E_ARG;
     }
+}
+
+// Weight and bias gradients of one 3x3 convolution (k_wgrad_tc + the fixed-
+// order reduction), added into dW [CO][CI][9] and db [CO]; part is a work
+// buffer of part_len floats.  Returns 1 when COS has no tensor-core form.
+int wgrad_tc(const void *X, const void *G, int B, int H, int W, int CIS, int CI, int COS, int CO, float *dW,
+             float *db, float *part, size_t part_len, int *err, cudaStream_t st) {
+    const int64_t P = (int64_t)B * H * W;
+    const int MT = (9 * CI + 1 + WG_ROWS - 1) / WG_ROWS;
+    int64_t Z = (2 * sm_count() + MT - 1) / MT;  // about two CTAs per SM
+    int64_t KP = (P + Z - 1) / Z;
+    KP = (KP + WG_KC - 1) / WG_KC * WG_KC;
+    while ((size_t)((P + KP - 1) / KP) * MT * WG_ROWS * COS > part_len) KP *= 2;
+    Z = (P + KP - 1) / KP;
+    const dim3 grid((unsigned)Z, (unsigned)MT);
+#define WGL(C)                                                                                                      \
+    {                                                                                                                \
+        static bool attr = false;                                                                                    \
+        if (!attr)                                                                                                   \
+            attr = cudaFuncSetAttribute(k_wgrad_tc<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, wg_smem(C)) == \
+                   cudaSuccess;                                                                                      \
+        if (!attr) return ASD2G_E_CUDA;                                                                              \
+        k_wgrad_tc<C><<<grid, WG_ROWS, wg_smem(C), st>>>((const __nv_bfloat16 *)X, (const __nv_bfloat16 *)G, H, W,   \
+                                                        CIS, CI, P, KP, part, err);                                  \
+    }
+    switch (COS) {
+    case 16: WGL(16); break;
+    case 32: WGL(32); break;
+    case 64: WGL(64); break;
+    case 128: WGL(128); break;
+    default: return 1;
+    }
+#undef WGL
+    const int64_t n = (int64_t)(9 * CI + 1) * CO;
+    k_wgrad_reduce<<<(int)((n + 255) / 256), 256, 0, st>>>(part, (int)Z, MT, COS, CI, CO, dW, db);
+    return cudaGetLastError() == cudaSuccess ? ASD2G_OK : ASD2G_E_CUDA;
 }
 
 }  // namespace asd2g

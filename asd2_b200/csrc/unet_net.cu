@@ -14,6 +14,7 @@
 // vector is that times RMS / s (the network sees a unit-scale problem, and
 // the map is homogeneous of degree one in the input vector).
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <random>
@@ -28,6 +29,8 @@ namespace asd2g {
 int api_fail(int code, const char *msg);
 bool conv_cout_ok(int c);
 // low != nullptr: the input is concat(nearest-upsampled low with cl channels, in)
+int wgrad_tc(const void *X, const void *G, int B, int H, int W, int CIS, int CI, int COS, int CO, float *dW,
+             float *db, float *part, size_t part_len, int *err, cudaStream_t st);
 int conv3x3_tc(const void *in, int n, int h, int w, int cin, const void *wpack, const float *bias, int cout,
                void *out, float *out32, int relu, int *err, cudaStream_t st, const void *low = nullptr, int cl = 0);
 }  // namespace asd2g
@@ -413,6 +416,7 @@ struct asd2g_unet {
     float *dskip[3] = {};
     float *loss = nullptr, *loss_host = nullptr;
     float *lscr = nullptr;  // residual loss: A out, then its gradient
+    float *wpart = nullptr; // split-K partial sums of the tensor-core weight gradients
 };
 
 namespace {
@@ -433,6 +437,18 @@ template <typename T> int ualloc(asd2g_unet *u, T **p, size_t n) {
 }
 
 int pad16(int c) { return (c + 15) / 16 * 16; }
+
+// split-K work buffer of the tensor-core weight gradient: about 2 x 148 CTAs
+// of 128 rows x up to 128 columns (larger products take longer K ranges)
+constexpr size_t UNET_WPART = (size_t)340 * 128 * 128;
+
+bool wgrad_tensor_cores() {
+    static const bool v = [] {
+        const char *e = std::getenv("ASD2G_WGRAD");
+        return !(e && std::strcmp(e, "cuda") == 0);
+    }();
+    return v;
+}
 
 int cuda_ok(const char *what) {
     const cudaError_t e = cudaGetLastError();
@@ -510,9 +526,20 @@ int layer_back(asd2g_unet *u, int li, const bf16 *X, const bf16 *Y, const bf16 *
         k_relu_mask<<<blocks(n), 256, 0, u->st>>>(dY, Y, n, u->gC);
         G = u->gC;
     }
-    const int64_t P = (int64_t)B * H * W;
-    const dim3 grid((l.cout + WG_TM - 1) / WG_TM, (9 * l.cin + WG_TN - 1) / WG_TN, (int)((P + WG_PIX - 1) / WG_PIX));
-    k_wgrad<<<grid, 256, 0, u->st>>>(X, G, B, H, W, l.cin_p, l.cin, l.cout_p, l.cout, u->g + l.woff, u->g + l.boff);
+    // weight and bias gradients on the tensor cores (FP32 CUDA-core form for
+    // other padded widths, or with ASD2G_WGRAD=cuda)
+    int wrc = 1;
+    if (wgrad_tensor_cores())
+        wrc = wgrad_tc(X, G, B, H, W, l.cin_p, l.cin, l.cout_p, l.cout, u->g + l.woff, u->g + l.boff, u->wpart,
+                       UNET_WPART, u->err, u->st);
+    if (wrc < 0) return api_fail(wrc, "tensor-core weight gradient launch");
+    if (wrc == 1) {
+        const int64_t P = (int64_t)B * H * W;
+        const dim3 grid((l.cout + WG_TM - 1) / WG_TM, (9 * l.cin + WG_TN - 1) / WG_TN,
+                        (int)((P + WG_PIX - 1) / WG_PIX));
+        k_wgrad<<<grid, 256, 0, u->st>>>(X, G, B, H, W, l.cin_p, l.cin, l.cout_p, l.cout, u->g + l.woff,
+                                         u->g + l.boff);
+    }
     if (dx) {
         const int rc = conv3x3_tc(G, B, H, W, l.cout_p, l.wpack_t, u->zero_bias, pad16(l.cin), dx, nullptr, 0, u->err,
                                   u->st);
@@ -627,6 +654,7 @@ int asd2g_unet_create(int max_batch, int max_h, int max_w, void *stream, asd2g_u
     if (!rc) rc = ualloc(u, &u->gL, P * 16);
     if (!rc) rc = ualloc(u, &u->loss, (size_t)max_batch);
     if (!rc) rc = ualloc(u, &u->lscr, P);
+    if (!rc) rc = ualloc(u, &u->wpart, UNET_WPART);
     if (!rc && cudaMallocHost(&u->loss_host, sizeof(float) * max_batch) != cudaSuccess)
         rc = api_fail(ASD2G_E_NOMEM, "pinned allocation failed");
     if (rc) {

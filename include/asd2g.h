@@ -322,8 +322,8 @@ int asd2g_conv3x3_bf16(const void *in, int n, int h, int w, int cin, const void 
 /* ---- the learned preconditioner (no reference counterpart) ----
  * A 4-level U-Net (16/32/64/128 channels, 15 3x3 convolutions, ReLU, 2x2
  * average pooling, nearest upsampling + skip concatenation); forward and
- * input-gradient convolutions on the tcgen05 tensor cores (BF16, FP32
- * accumulation), weight gradients in FP32, Adam on FP32 master weights.
+ * input-gradient convolutions and the weight gradients on the tcgen05
+ * tensor cores (BF16, FP32 accumulation), Adam on FP32 master weights.
  * Images: H x W, both multiples of 8.  A forward pass takes B images with
  * B * H * W <= max_batch * max_h * max_w; a training step B <= max_batch
  * images of H * W <= max_h * max_w.
