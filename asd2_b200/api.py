@@ -30,6 +30,7 @@ REINIT_ORIGINAL, REINIT_SUSSMAN, REINIT_MINRK2, REINIT_FIRSTTIME, REINIT_MINRK2_
 # solvers
 PCG, PCG_REFERENCE, BICGSTAB, BICGSTAB_REFERENCE, MGPCG, UNET = range(6)
 NOT_CONVERGED = 1
+CURVATURE_REFERENCE, CURVATURE_DIVERGENCE = 0, 1
 FLAG_NO_CLUSTER_PCG = 1
 FLAG_NO_PERSIST_MG = 2
 PRECISION_FP64, PRECISION_MIXED = 0, 1
@@ -51,7 +52,7 @@ class _Params(C.Structure):
                 ("rho_h", C.c_double), ("rho_l", C.c_double), ("mu_h", C.c_double), ("mu_l", C.c_double),
                 ("sigma", C.c_double), ("gravity", C.c_double), ("g_axis", C.c_int32), ("fix_gravity", C.c_int32),
                 ("time_order", C.c_int32), ("solver_flags", C.c_int32), ("cfl", C.c_double),
-                ("ls_max_atime", C.c_double), ("numbers_given", C.c_int32), ("reserved1", C.c_int32),
+                ("ls_max_atime", C.c_double), ("numbers_given", C.c_int32), ("curvature", C.c_int32),
                 ("re", C.c_double), ("we", C.c_double), ("fr", C.c_double)]
 
 
@@ -201,6 +202,7 @@ class Params:
     base_y: float = 0.0
     precision: int = 0
     solver_flags: int = 0
+    curvature: int = 0  # CURVATURE_REFERENCE or CURVATURE_DIVERGENCE
 
     def c(self) -> _Params:
         p = _Params()
@@ -213,6 +215,7 @@ class Params:
         p.sigma, p.gravity, p.g_axis, p.fix_gravity = self.sigma, self.g, self.g_axis, self.fix_gravity
         p.time_order, p.cfl, p.ls_max_atime = self.time_order, self.cfl, self.ls_max_atime
         p.solver_flags = self.solver_flags
+        p.curvature = self.curvature
         return p
 
     @classmethod

@@ -197,6 +197,9 @@ int grid_from_params(const asd2g_params *p, Grid &g, MomConst &M) {
     }
     g.p_mirror = mirror ? 1 : 0;
     g.pinned = pinned ? 1 : 0;
+    if (p->curvature != ASD2G_CURVATURE_REFERENCE && p->curvature != ASD2G_CURVATURE_DIVERGENCE)
+        return fail(ASD2G_E_ARG, "curvature must be ASD2G_CURVATURE_REFERENCE or ASD2G_CURVATURE_DIVERGENCE");
+    g.kappa_mode = p->curvature;
     if (p->precision == ASD2G_PRECISION_MIXED && !g.p_mirror)
         return fail(ASD2G_E_UNSUPPORTED, "mixed precision needs Neumann or Dirichlet pressure on all four sides");
     MomParams mp{p->rho_h, p->rho_l, p->mu_h, p->mu_l, p->sigma, p->gravity, p->cfl, p->g_axis, p->fix_gravity,

@@ -22,6 +22,7 @@ struct Grid {
     double cu[4], cv[4], cp[4];   // Dirichlet constants
     int32_t p_mirror;             // all four P sides are K_NEU/K_DIR: producers write ghost mirrors
     int32_t pinned;               // all four P sides Neumann/axisym/wall (mac2d.cpp:1496-1500)
+    int32_t kappa_mode;           // ASD2G_CURVATURE_*
 };
 
 __host__ __device__ __forceinline__ int64_t IX(const Grid &g, int i, int j) { return (int64_t)j + (int64_t)g.sy * i; }

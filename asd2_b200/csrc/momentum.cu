@@ -35,9 +35,37 @@ __device__ __forceinline__ void kappa_tile(const Grid &g, const DivH &d2x, const
     k = isgn(k) * fabs(smin(fabs(k), lim));
     kappa[IX(g, i, j)] = k;
 }
+
+// ASD2G_CURVATURE_DIVERGENCE: kappa = div(n), n = grad phi / |grad phi| on
+// the cell faces.  x face (i+1/2, j): phi_x = (phi(i+1,j) - phi(i,j)) / dx,
+// phi_y = (phi(i,j+1) + phi(i+1,j+1) - phi(i,j-1) - phi(i+1,j-1)) / (4 dy);
+// y faces alike; kappa = (nx(i+1/2) - nx(i-1/2)) / dx + (ny(j+1/2) -
+// ny(j-1/2)) / dy, limited as UpdateKappa limits it.  Reads phi on the
+// 3 x 3 block around each face pair (ghost cells included).
+__device__ __forceinline__ void kappa_div_tile(const Grid &g, double lim, const double *__restrict__ ls,
+                                               double *__restrict__ kappa, int bx, int by) {
+    const int j = NB + bx * TJ + threadIdx.x, i = NB + by * TI + threadIdx.y;
+    if (i >= g.nx + NB || j >= g.ny + NB) return;
+    const double dx = g.dx, dy = g.dy;
+    auto L = [&](int a, int b) { return ls[IX(g, i + a, j + b)]; };
+    auto nx = [&](int a) {  // x face between cells i + a and i + a + 1
+        const double px = (L(a + 1, 0) - L(a, 0)) / dx;
+        const double py = (L(a, 1) + L(a + 1, 1) - L(a, -1) - L(a + 1, -1)) / (4.0 * dy);
+        return px / sqrt(px * px + py * py + 1.0e-100);
+    };
+    auto ny = [&](int b) {  // y face between cells j + b and j + b + 1
+        const double py = (L(0, b + 1) - L(0, b)) / dy;
+        const double px = (L(1, b) + L(1, b + 1) - L(-1, b) - L(-1, b + 1)) / (4.0 * dx);
+        return py / sqrt(px * px + py * py + 1.0e-100);
+    };
+    double k = (nx(0) - nx(-1)) / dx + (ny(0) - ny(-1)) / dy;
+    k = isgn(k) * fabs(smin(fabs(k), lim));
+    kappa[IX(g, i, j)] = k;
+}
 __global__ void k_kappa(Grid g, DivH d2x, DivH d2y, DivH dxx, DivH dyy, double lim, const double *__restrict__ ls,
                         double *__restrict__ kappa) {
-    kappa_tile(g, d2x, d2y, dxx, dyy, lim, ls, kappa, blockIdx.x, blockIdx.y);
+    if (g.kappa_mode == 1) kappa_div_tile(g, lim, ls, kappa, blockIdx.x, blockIdx.y);
+    else kappa_tile(g, d2x, d2y, dxx, dyy, lim, ls, kappa, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------------------ Heaviside --
@@ -485,7 +513,8 @@ void launch_update_dt(const Grid &g, const MomConst &M, const double *u, const d
 __global__ void k_bkappa(const BInst *__restrict__ insts, const BTile *__restrict__ tiles) {
     const BTile t = tiles[blockIdx.x];
     const BInst &I = insts[t.inst];
-    kappa_tile(I.g, I.d2x, I.d2y, I.dxx, I.dyy, I.kappa_lim, bslot(I, BS_LS), bslot(I, BS_KAPPA), t.bx, t.by);
+    if (I.g.kappa_mode == 1) kappa_div_tile(I.g, I.kappa_lim, bslot(I, BS_LS), bslot(I, BS_KAPPA), t.bx, t.by);
+    else kappa_tile(I.g, I.d2x, I.d2y, I.dxx, I.dyy, I.kappa_lim, bslot(I, BS_LS), bslot(I, BS_KAPPA), t.bx, t.by);
 }
 
 __global__ void k_bheaviside(const BInst *__restrict__ insts, const BChunk *__restrict__ chunks) {

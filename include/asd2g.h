@@ -97,6 +97,18 @@ enum asd2g_solver {
                                    Needs Neumann/Dirichlet pressure on all sides and reinit mode
                                    0, 2 or 4. */
 
+/* Curvature of the level set (asd2g_params.curvature).
+ * ASD2G_CURVATURE_REFERENCE: UpdateKappa (mac2d.cpp:221-252), the expanded
+ *   (phi_x^2 phi_yy - 2 phi_x phi_y phi_xy + phi_y^2 phi_xx) / |grad phi|^3
+ *   with central differences (the cross term from differenced phi_x).
+ * ASD2G_CURVATURE_DIVERGENCE: kappa = div(grad phi / |grad phi|) in
+ *   conservative form: normals on the four cell faces (the normal component
+ *   from the two cells beside the face, the tangential one from the four
+ *   cells around it), differenced across the cell; the same limiter
+ *   |kappa| <= 1 / min(dx, dy).  The reference lists better curvature
+ *   discretisations as future work (README.md:73). */
+enum { ASD2G_CURVATURE_REFERENCE = 0, ASD2G_CURVATURE_DIVERGENCE = 1 };
+
 typedef struct asd2g_params {
     int32_t nx, ny;          /* interior cells (>= 4 each) */
     int32_t nbc;             /* ghost layers: must be 3 (WENO5) */
@@ -115,7 +127,8 @@ typedef struct asd2g_params {
     double ls_max_atime;     /* reinit pseudo-time; <= 0: 1.5*kThickness (levelset2d.cpp:10) */
     int32_t numbers_given;   /* 1: use re/we/fr below; 0: kRe = rho_h/mu_h, kWe = rho_h/sigma,
                                 kFr = 1/gravity (the second MACSolver2D constructor with L = U = 1) */
-    int32_t reserved1;
+    int32_t curvature;       /* ASD2G_CURVATURE_*: 0 UpdateKappa's formula (mac2d.cpp:221), 1 the
+                                divergence of face normals (no reference counterpart) */
     double re, we, fr;       /* kRe, kWe, kFr of MACSolver2D (mac2d.h:37): viscosity is skipped when
                                 kRe <= 0, the curvature is recomputed in the solve when kWe is finite and
                                 nonzero, gravity needs kFr finite (mac2d.cpp:598, :1307, :1047) */
