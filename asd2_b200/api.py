@@ -58,7 +58,8 @@ class _Params(C.Structure):
 
 EXPORTS = [
     "asd2g_version", "asd2g_last_error", "asd2g_create", "asd2g_destroy", "asd2g_sync", "asd2g_field_ptr",
-    "asd2g_upload", "asd2g_upload_async", "asd2g_download", "asd2g_copy_field", "asd2g_fill_field", "asd2g_apply_bc",
+    "asd2g_upload", "asd2g_upload_async", "asd2g_upload_staged", "asd2g_download_staged", "asd2g_join_copies",
+    "asd2g_sync_copies", "asd2g_download", "asd2g_copy_field", "asd2g_fill_field", "asd2g_apply_bc",
     "asd2g_ls_advect", "asd2g_ls_weno_rhs", "asd2g_reinit", "asd2g_subcell_eno", "asd2g_eno",
     "asd2g_sussman_constraint", "asd2g_heaviside_deriv", "asd2g_smoothed_sign", "asd2g_ls_step",
     "asd2g_kappa", "asd2g_heaviside", "asd2g_convection", "asd2g_viscosity", "asd2g_momentum_rhs",
@@ -103,6 +104,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_field_ptr": ([S, I, C.POINTER(C.c_void_p)], I),
         "asd2g_upload": ([S, I, dp], I), "asd2g_download": ([S, I, dp], I),
         "asd2g_upload_async": ([S, I, dp], I),
+        "asd2g_upload_staged": ([S, I, dp], I), "asd2g_download_staged": ([S, I, dp], I),
+        "asd2g_join_copies": ([S, I], I), "asd2g_sync_copies": ([S], I),
         "asd2g_copy_field": ([S, I, I], I), "asd2g_fill_field": ([S, I, D], I),
         "asd2g_apply_bc": ([S, I, C.c_char], I),
         "asd2g_ls_advect": ([S, D], I), "asd2g_ls_weno_rhs": ([S, I, I, I, I], I), "asd2g_reinit": ([S, I], I),
@@ -282,6 +285,30 @@ class Session:
             raise ValueError("upload_async needs a C-contiguous float64 array of the field's shape")
         self._check(self.L.asd2g_upload_async(self.h, self._f(f), arr))
 
+
+    def _check_host(self, arr, what):
+        if not (isinstance(arr, np.ndarray) and arr.dtype == np.float64 and arr.flags.c_contiguous
+                and arr.shape == self.shape):
+            raise ValueError(f"{what} needs a C-contiguous float64 array of the field's shape")
+
+    def upload_staged(self, f, arr):
+        """Upload on the session's copy stream after the compute work queued
+        so far (asd2g_upload_staged); join_copies(1) before its first reader."""
+        self._check_host(arr, "upload_staged")
+        self._check(self.L.asd2g_upload_staged(self.h, self._f(f), arr))
+
+    def download_staged(self, f, out):
+        """Download into out (pinned, float64, the field's shape) on the copy
+        stream after the compute work queued so far (asd2g_download_staged)."""
+        self._check_host(out, "download_staged")
+        self._check(self.L.asd2g_download_staged(self.h, self._f(f), out))
+
+    def join_copies(self, which=3):
+        """Later compute work waits for the staged uploads (1), downloads (2) or both (3)."""
+        self._check(self.L.asd2g_join_copies(self.h, which))
+
+    def sync_copies(self):
+        self._check(self.L.asd2g_sync_copies(self.h))
     def download(self, f):
         out = np.empty(self.shape)
         self._check(self.L.asd2g_download(self.h, self._f(f), out))

@@ -261,6 +261,9 @@ struct asd2g_session {
     int run_reinit = -1, run_maxit = -1;
     double run_tol = -1.0;
     cudaStream_t aux_st[2] = {};
+    // staged copies: the session's copy stream and its events
+    cudaStream_t copy_st = nullptr;
+    cudaEvent_t ev_cmp = nullptr, ev_up = nullptr, ev_down = nullptr;
     RunStats *run_stats = nullptr, *run_stats_host = nullptr;
     std::vector<void *> allocs;
 };
@@ -483,6 +486,12 @@ int asd2g_destroy(asd2g_session *s) {
     if (s->post_exec) cudaGraphExecDestroy(s->post_exec);
     for (cudaStream_t a : s->aux_st)
         if (a) cudaStreamDestroy(a);
+    if (s->copy_st) {
+        cudaStreamSynchronize(s->copy_st);
+        cudaStreamDestroy(s->copy_st);
+    }
+    for (cudaEvent_t e : {s->ev_cmp, s->ev_up, s->ev_down})
+        if (e) cudaEventDestroy(e);
     if (s->run_stats_host) cudaFreeHost(s->run_stats_host);
     for (void *p : s->allocs) cudaFree(p);
     if (s->ks_host) cudaFreeHost(s->ks_host);
@@ -514,6 +523,48 @@ int asd2g_upload_async(asd2g_session *s, int field, const double *host) {
     if (!s || !host || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field or null argument");
     if (cudaMemcpyAsync(s->f[field], host, sizeof(double) * s->G, cudaMemcpyHostToDevice, s->st) != cudaSuccess)
         return cuda_check("upload");
+    return ASD2G_OK;
+}
+
+// Staged copies: the session's copy stream waits for the compute work
+// enqueued so far, copies, and records the upload or download event that
+// asd2g_join_copies makes the compute stream wait for.
+static int staged(asd2g_session *s, int field, void *host, bool up) {
+    if (!s || !host || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field or null argument");
+    if (!s->copy_st) {
+        if (cudaStreamCreateWithFlags(&s->copy_st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s->ev_cmp, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s->ev_up, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s->ev_down, cudaEventDisableTiming) != cudaSuccess)
+            return cuda_check("copy stream");
+    }
+    cudaEventRecord(s->ev_cmp, s->st);
+    cudaStreamWaitEvent(s->copy_st, s->ev_cmp, 0);
+    const size_t bytes = sizeof(double) * s->G;
+    const cudaError_t e = up ? cudaMemcpyAsync(s->f[field], host, bytes, cudaMemcpyHostToDevice, s->copy_st)
+                             : cudaMemcpyAsync(host, s->f[field], bytes, cudaMemcpyDeviceToHost, s->copy_st);
+    if (e != cudaSuccess) return cuda_check(up ? "staged upload" : "staged download");
+    cudaEventRecord(up ? s->ev_up : s->ev_down, s->copy_st);
+    return cuda_check("staged copy");
+}
+
+int asd2g_upload_staged(asd2g_session *s, int field, const double *host) {
+    return staged(s, field, const_cast<double *>(host), true);
+}
+
+int asd2g_download_staged(asd2g_session *s, int field, double *host) { return staged(s, field, host, false); }
+
+int asd2g_join_copies(asd2g_session *s, int which) {
+    if (!s || which < 1 || which > 3) return fail(ASD2G_E_ARG, "which: 1 uploads, 2 downloads, 3 both");
+    if (!s->copy_st) return ASD2G_OK;
+    if (which & 1) cudaStreamWaitEvent(s->st, s->ev_up, 0);
+    if (which & 2) cudaStreamWaitEvent(s->st, s->ev_down, 0);
+    return cuda_check("join copies");
+}
+
+int asd2g_sync_copies(asd2g_session *s) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    if (s->copy_st && cudaStreamSynchronize(s->copy_st) != cudaSuccess) return cuda_check("copy stream");
     return ASD2G_OK;
 }
 

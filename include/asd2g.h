@@ -160,6 +160,21 @@ int asd2g_download(asd2g_session *s, int field, double *host);
  * synchronises (asd2g_sync, a pressure solve, a download); from pinned host
  * memory the copy overlaps the host's next calls. */
 int asd2g_upload_async(asd2g_session *s, int field, const double *host);
+/* Staged copies on the session's own copy stream, for callers that overlap
+ * the transfers of one step with the computation of another (no reference
+ * counterpart).  Each staged copy first waits for the compute work enqueued
+ * on the session so far (so it never overwrites a field an earlier call
+ * still reads, nor reads one an earlier call still writes) and then runs
+ * beside later compute calls.  asd2g_join_copies(s, which) makes the compute
+ * work enqueued after it wait for the staged uploads (which = 1), downloads
+ * (2) or both (3) issued so far; call it before the first call that reads an
+ * uploaded field or writes a downloaded one.  asd2g_sync_copies waits on the
+ * host for every staged copy.  Host buffers: pinned for a truly
+ * asynchronous copy, untouched until the copy is known complete. */
+int asd2g_upload_staged(asd2g_session *s, int field, const double *host);
+int asd2g_download_staged(asd2g_session *s, int field, double *host);
+int asd2g_join_copies(asd2g_session *s, int which);
+int asd2g_sync_copies(asd2g_session *s);
 int asd2g_copy_field(asd2g_session *s, int dst, int src);
 int asd2g_fill_field(asd2g_session *s, int field, double value);
 
