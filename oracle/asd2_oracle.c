@@ -1402,6 +1402,468 @@ double ora_update_dt(const ora_grid *g, const ora_fluid *f, const double *u, con
     return dt;
 }
 
+/* ======================================================================= */
+/* Axisymmetric MAC solver: MACSolver2DAxisym, mac2dAxisym.cpp             */
+/* x is r (i, nx = kNr, dx = kDr), y is z (j, ny = kNz, dy = kDz).          */
+/* ======================================================================= */
+static inline double axi_mu(const ora_fluid *f, const double *H, long c) { return f->mu_l + (f->mu_h - f->mu_l) * H[c]; }
+static inline double axi_q(const double *a, long c0, long c1, long c2, long c3) {
+    /* 0.25 * (a0 + a1 + a2 + a3), summed left to right as the reference writes it */
+    return 0.25 * (a[c0] + a[c1] + a[c2] + a[c3]);
+}
+/* Heavy fraction of a face between level-set values a and b, the rule of the
+ * implicit viscous step (mac2dAxisym.cpp:1027-1043): both >= 0 heavy, both
+ * <= 0 light, else the fraction on the heavy side. */
+static inline double axi_heavy(double a, double b) {
+    if (a >= 0.0 && b >= 0.0) return 1.0;
+    if (a <= 0.0 && b <= 0.0) return 0.0;
+    if (a >= 0.0 && b < 0.0) return fabs(a) / (fabs(a) + fabs(b));
+    return fabs(b) / (fabs(a) + fabs(b));
+}
+/* Effective density of the explicit viscous terms (mac2dAxisym.cpp:682-736):
+ * the pure cases take the fluid density itself. */
+static inline double axi_rho_face(const ora_fluid *f, double a, double b) {
+    if (a >= 0.0 && b >= 0.0) return f->rho_h;
+    if (a <= 0.0 && b <= 0.0) return f->rho_l;
+    const double t = (a >= 0.0) ? fabs(a) / (fabs(a) + fabs(b)) : fabs(b) / (fabs(a) + fabs(b));
+    return f->rho_h * t + f->rho_l * (1.0 - t);
+}
+
+/* UpdateKappa, mac2dAxisym.cpp:222-262.  The r-derivative is one-sided in the
+ * first column (the axis); dphi/dz of a neighbour column outside the
+ * interior is 0 (never computed there); r = kBaseR + (i + 1/2) dr. */
+void ora_axi_kappa(const ora_grid *g, double base_r, const double *ls, double *kappa) {
+    const int nx = g->nx, ny = g->ny;
+    const long n = ASZ(g);
+    const double dr = g->dx, dz = g->dy, eps = 1.0e-100;
+    double *gr = zalloc(n), *gz = zalloc(n), *sz = zalloc(n);
+    for (int i = NB; i < nx + NB; i++)
+        for (int j = NB; j < ny + NB; j++) {
+            const long k = IX(g, i, j);
+            gr[k] = (ls[IX(g, i + 1, j)] - ls[IX(g, i - 1, j)]) / (2.0 * dr);
+            gz[k] = (ls[IX(g, i, j + 1)] - ls[IX(g, i, j - 1)]) / (2.0 * dz);
+            if (i == NB) gr[k] = (ls[IX(g, i + 1, j)] - ls[k]) / dr;
+            sz[k] = sqrt(gr[k] * gr[k] + gz[k] * gz[k] + eps);
+        }
+    const double lim = 1.0 / smin(dr, dz);
+    for (int i = NB; i < nx + NB; i++)
+        for (int j = NB; j < ny + NB; j++) {
+            const long k = IX(g, i, j);
+            const double r = base_r + (i + 0.5 - NB) * dr;
+            const double dR = gr[k], dZ = gz[k], s = sz[k];
+            double kap = ((ls[IX(g, i - 1, j)] - 2.0 * ls[k] + ls[IX(g, i + 1, j)]) / (dr * dr) * dZ * dZ -
+                          2.0 * (gz[IX(g, i + 1, j)] - gz[IX(g, i - 1, j)]) / (2.0 * dr) * dR * dZ +
+                          (ls[IX(g, i, j - 1)] - 2.0 * ls[k] + ls[IX(g, i, j + 1)]) / (dz * dz) * dR * dR +
+                          dR * (s * s) / r) /
+                         pow(s, 3.0);
+            kappa[k] = isgn(kap) * fabs(smin(fabs(kap), lim));
+        }
+    free(gr); free(gz); free(sz);
+}
+
+/* AddExternalViscosityFU, mac2dAxisym.cpp:590-753: the z-part of the viscous
+ * stress on u faces, over the density of the face's z-neighbourhood. */
+void ora_axi_visc_u(const ora_grid *g, const ora_fluid *f, const double *u, const double *v, const double *ls,
+                    const double *H, double *dU) {
+    (void)u;
+    const int nx = g->nx, ny = g->ny;
+    const double dr = g->dx, dz = g->dy;
+    memset(dU, 0, sizeof(double) * ASZ(g));
+    if (!(re_positive(f) > 0.0)) return;
+    for (int i = NB + 1; i < nx + NB; i++)
+        for (int j = NB; j < ny + NB; j++) {
+            const long M = IX(g, i, j), W = IX(g, i - 1, j), Nn = IX(g, i, j + 1), WN = IX(g, i - 1, j + 1),
+                       S = IX(g, i, j - 1), WS = IX(g, i - 1, j - 1);
+            const double lsN = axi_q(ls, M, W, WN, Nn), lsS = axi_q(ls, M, W, WS, S);
+            const double muN = 0.25 * (axi_mu(f, H, M) + axi_mu(f, H, W) + axi_mu(f, H, WN) + axi_mu(f, H, Nn));
+            const double muS = 0.25 * (axi_mu(f, H, M) + axi_mu(f, H, W) + axi_mu(f, H, WS) + axi_mu(f, H, S));
+            const double rhoSN = axi_rho_face(f, lsS, lsN);
+            const double visZ = (muN * (v[Nn] - v[WN]) / dr - muS * (v[M] - v[W]) / dr) / dz;
+            dU[M] = visZ / rhoSN;
+        }
+}
+
+/* AddExternalViscosityFV, mac2dAxisym.cpp:755-910: the r-part on v faces plus
+ * the hoop term built from the new uhat, r = (i + 1/2) dr (no kBaseR). */
+void ora_axi_visc_v(const ora_grid *g, const ora_fluid *f, const double *u, const double *uhat, const double *v,
+                    const double *ls, const double *H, double *dV) {
+    (void)v;
+    const int nx = g->nx, ny = g->ny;
+    const double dr = g->dx, dz = g->dy;
+    memset(dV, 0, sizeof(double) * ASZ(g));
+    if (!(re_positive(f) > 0.0)) return;
+    for (int i = NB; i < nx + NB; i++)
+        for (int j = NB + 1; j < ny + NB; j++) {
+            const long M = IX(g, i, j), W = IX(g, i - 1, j), E = IX(g, i + 1, j), S = IX(g, i, j - 1),
+                       WS = IX(g, i - 1, j - 1), ES = IX(g, i + 1, j - 1);
+            const double r = (i + 0.5 - NB) * dr;
+            const double lsVW = axi_q(ls, M, W, WS, S), lsVE = axi_q(ls, M, E, ES, S);
+            const double muVW = 0.25 * (axi_mu(f, H, M) + axi_mu(f, H, W) + axi_mu(f, H, WS) + axi_mu(f, H, S));
+            const double muVE = 0.25 * (axi_mu(f, H, M) + axi_mu(f, H, E) + axi_mu(f, H, ES) + axi_mu(f, H, S));
+            const double rhoWE = axi_rho_face(f, lsVW, lsVE);
+            const double rhoSN = axi_rho_face(f, ls[S], ls[M]);
+            const double visR = (muVE * (u[E] - u[ES]) / dz - muVW * (u[M] - u[S]) / dz) / dr;
+            const double visZ = 0.5 * (axi_mu(f, H, M) + axi_mu(f, H, S)) / r *
+                                (0.5 * (uhat[M] + uhat[E]) - 0.5 * (uhat[S] + uhat[ES])) / dz;
+            dV[M] = visR / rhoWE + visZ / rhoSN;
+        }
+}
+
+/* GetRHSU, mac2dAxisym.cpp:264-292: u + dt (-conv + gravity + viscous) on the
+ * interior u faces, zero elsewhere, then the U ghost fill. */
+void ora_axi_rhs_u(const ora_grid *g, const ora_fluid *f, double dt, const double *ls, const double *u,
+                   const double *v, const double *H, double *rhs) {
+    const long n = ASZ(g);
+    double *cU = zalloc(n), *vU = zalloc(n);
+    ora_conv_u(g, u, v, cU);
+    ora_axi_visc_u(g, f, u, v, ls, H, vU);
+    const double gU = gravity_on(f, 0) ? -f->g : 0.0; /* AddGravityFU, :912-929 (axis R) */
+    memset(rhs, 0, sizeof(double) * n);
+    for (int i = NB + 1; i < g->nx + NB; i++)
+        for (int j = NB; j < g->ny + NB; j++) {
+            const long k = IX(g, i, j);
+            rhs[k] = u[k] + dt * (-cU[k] + gU + vU[k]);
+        }
+    ora_bc_u(g, rhs);
+    free(cU); free(vU);
+}
+
+/* GetRHSV, mac2dAxisym.cpp:294-322.  Its gravity is AddGravityFU() (:306),
+ * nonzero only where the U pattern is (i >= 4, axis R), unless fix_gravity
+ * selects AddGravityFV (axis Z). */
+void ora_axi_rhs_v(const ora_grid *g, const ora_fluid *f, double dt, const double *ls, const double *u,
+                   const double *uhat, const double *v, const double *H, double *rhs) {
+    const long n = ASZ(g);
+    double *cV = zalloc(n), *vV = zalloc(n);
+    ora_conv_v(g, u, v, cV);
+    ora_axi_visc_v(g, f, u, uhat, v, ls, H, vV);
+    memset(rhs, 0, sizeof(double) * n);
+    for (int i = NB; i < g->nx + NB; i++)
+        for (int j = NB + 1; j < g->ny + NB; j++) {
+            const long k = IX(g, i, j);
+            double gV;
+            if (f->fix_gravity) gV = gravity_on(f, 1) ? -f->g : 0.0;
+            else gV = (gravity_on(f, 0) && i >= NB + 1) ? -f->g : 0.0;
+            rhs[k] = v[k] + dt * (-cV[k] + gV + vV[k]);
+        }
+    ora_bc_v(g, rhs);
+    free(cV); free(vV);
+}
+
+/* The Thomas algorithm for lo[k] x[k-1] + di[k] x[k] + up[k] x[k+1] = x[k],
+ * k = 0..n-1 (n >= 2), in the elimination order of SolveTDMA
+ * (mac2dAxisym.cpp:2255-2306): up and x are overwritten, x holds the result. */
+static void axi_thomas(int n, const double *lo, const double *di, double *up, double *x) {
+    up[0] = up[0] / di[0];
+    x[0] = x[0] / di[0];
+    for (int k = 1; k < n; k++) {
+        const double piv = di[k] - lo[k] * up[k - 1];
+        if (k < n - 1) up[k] = up[k] / piv;
+        x[k] = (x[k] - lo[k] * x[k - 1]) / piv;
+    }
+    for (int k = n - 2; k >= 0; k--) x[k] = x[k] - up[k] * x[k + 1];
+}
+
+/* GetUHat, mac2dAxisym.cpp:950-1229: the u faces i = 4 .. nx+2 solved
+ * implicitly for the viscous r- and z-terms, one Thomas sweep per z row
+ * (r-direction, the (1/r) d/dr (r mu du/dr) stencil) and then one per r
+ * column (z-direction), and finally divided by 1 + dt/rho (mu_W + mu_M)/r^2.
+ * Raw U kinds and constants pick the end rows (:1047-1086, :1138-1177). */
+void ora_axi_uhat(const ora_grid *g, const ora_fluid *f, double dt, const double *ls, const double *rhs,
+                  const double *H, double *uhat) {
+    const int nr = g->nx, nz = g->ny, m = nr - 1;
+    const double dr = g->dx, dz = g->dy, rH = f->rho_h, rL = f->rho_l;
+    const int bW = g->bc_u[0], bE = g->bc_u[1], bS = g->bc_u[2], bN = g->bc_u[3];
+    const int L = (m > nz ? m : nz);
+    double *lo = zalloc(L), *di = zalloc(L), *up = zalloc(L), *x = zalloc(L);
+    double *s2 = zalloc((long)m * nz), *s1 = zalloc((long)m * nz);
+    memset(uhat, 0, sizeof(double) * ASZ(g));
+    for (int jj = 0; jj < nz; jj++) { /* r lines */
+        const int J = jj + NB;
+        for (int k = 0; k < m; k++) {
+            const int I = k + NB + 1;
+            const double rUM = (k + 1.0) * dr, rPW = (k + 0.5) * dr, rPM = (k + 1.5) * dr;
+            const double muW = axi_mu(f, H, IX(g, I - 1, J)), muM = axi_mu(f, H, IX(g, I, J));
+            const double thH = axi_heavy(ls[IX(g, I - 1, J)], ls[IX(g, I, J)]);
+            const double rho = rH * thH + rL * (1.0 - thH);
+            x[k] = rhs[IX(g, I, J)];
+            lo[k] = -dt / (rho * rUM) * (2.0 * rPW * muW) / (dr * dr);
+            di[k] = 1.0 + dt / (rho * rUM) * 2.0 * (rPW * muW + rPM * muM) / (dr * dr);
+            up[k] = -dt / (rho * rUM) * (2.0 * rPM * muM) / (dr * dr);
+            if (k == 0) {
+                if (bW == ORA_NEUMANN || bW == ORA_OUTLET) { di[k] += lo[k]; lo[k] = 0.0; }
+                else if (bW == ORA_DIRICHLET || bW == ORA_AXISYM || bW == ORA_INLET || bW == ORA_WALL) { x[k] -= lo[k] * g->cu[0]; lo[k] = 0.0; }
+                else if (bW == ORA_PERIODIC) { x[k] -= lo[k] * rhs[IX(g, m - 1 + NB + 1, J)]; lo[k] = 0.0; }
+            }
+            if (k == m - 1) {
+                if (bE == ORA_NEUMANN || bE == ORA_OUTLET) { di[k] += up[k]; up[k] = 0.0; }
+                else if (bE == ORA_DIRICHLET || bE == ORA_AXISYM || bE == ORA_INLET || bE == ORA_WALL) { x[k] -= up[k] * g->cu[1]; up[k] = 0.0; }
+                else if (bE == ORA_PERIODIC) { x[k] -= up[k] * rhs[IX(g, NB + 1, J)]; up[k] = 0.0; }
+            }
+        }
+        axi_thomas(m, lo, di, up, x);
+        for (int k = 0; k < m; k++) s2[jj + (long)nz * k] = x[k];
+    }
+    for (int k = 0; k < m; k++) { /* z lines */
+        const int I = k + NB + 1;
+        for (int jj = 0; jj < nz; jj++) {
+            const int J = jj + NB;
+            const long M = IX(g, I, J), W = IX(g, I - 1, J), S = IX(g, I, J - 1), WS = IX(g, I - 1, J - 1),
+                       Nn = IX(g, I, J + 1), WN = IX(g, I - 1, J + 1);
+            const double lsS = axi_q(ls, M, W, WS, S), lsN = axi_q(ls, M, W, WN, Nn);
+            const double muS = 0.25 * (axi_mu(f, H, M) + axi_mu(f, H, W) + axi_mu(f, H, WS) + axi_mu(f, H, S));
+            const double muN = 0.25 * (axi_mu(f, H, M) + axi_mu(f, H, W) + axi_mu(f, H, WN) + axi_mu(f, H, Nn));
+            const double thH = axi_heavy(lsS, lsN);
+            const double rho = rH * thH + rL * (1.0 - thH);
+            x[jj] = s2[jj + (long)nz * k];
+            lo[jj] = -dt / rho * muS / (dz * dz);
+            di[jj] = 1.0 + dt / rho * (muS + muN) / (dz * dz);
+            up[jj] = -dt / rho * muN / (dz * dz);
+            if (jj == 0) {
+                if (bS == ORA_NEUMANN || bS == ORA_AXISYM || bS == ORA_OUTLET) { di[jj] += lo[jj]; lo[jj] = 0.0; }
+                else if (bS == ORA_DIRICHLET || bS == ORA_INLET || bS == ORA_WALL) { x[jj] -= lo[jj] * 2.0 * g->cu[2]; lo[jj] = 0.0; }
+                else if (bS == ORA_PERIODIC) { x[jj] -= lo[jj] * s2[(nz - 1) + (long)nz * k]; lo[jj] = 0.0; }
+            }
+            if (jj == nz - 1) {
+                if (bN == ORA_NEUMANN || bN == ORA_AXISYM || bN == ORA_OUTLET) { di[jj] += up[jj]; up[jj] = 0.0; }
+                else if (bN == ORA_DIRICHLET || bN == ORA_INLET || bN == ORA_WALL) { x[jj] -= up[jj] * 2.0 * g->cu[3]; up[jj] = 0.0; }
+                else if (bN == ORA_PERIODIC) { x[jj] -= up[jj] * s2[0 + (long)nz * k]; up[jj] = 0.0; }
+            }
+        }
+        axi_thomas(nz, lo, di, up, x);
+        for (int jj = 0; jj < nz; jj++) s1[jj + (long)nz * k] = x[jj];
+    }
+    for (int k = 0; k < m; k++) {
+        const int I = k + NB + 1;
+        const double rUM = (I - NB) * dr;
+        for (int jj = 0; jj < nz; jj++) {
+            const int J = jj + NB;
+            const long M = IX(g, I, J), W = IX(g, I - 1, J);
+            const double thH = axi_heavy(ls[W], ls[M]);
+            const double rho = rH * thH + rL * (1.0 - thH);
+            uhat[M] = s1[jj + (long)nz * k] / (1.0 + dt / rho * (axi_mu(f, H, W) + axi_mu(f, H, M)) / (rUM * rUM));
+        }
+    }
+    free(lo); free(di); free(up); free(x); free(s1); free(s2);
+}
+
+/* GetVHat, mac2dAxisym.cpp:1231-1478: the v faces j = 4 .. ny+2, r lines over
+ * all nx cells (the (1/r) d/dr (r mu dv/dr) stencil) then z lines. */
+void ora_axi_vhat(const ora_grid *g, const ora_fluid *f, double dt, const double *ls, const double *rhs,
+                  const double *H, double *vhat) {
+    const int nr = g->nx, nz = g->ny, m = nz - 1;
+    const double dr = g->dx, dz = g->dy, rH = f->rho_h, rL = f->rho_l;
+    const int bW = g->bc_v[0], bE = g->bc_v[1], bS = g->bc_v[2], bN = g->bc_v[3];
+    const int L = (nr > m ? nr : m);
+    double *lo = zalloc(L), *di = zalloc(L), *up = zalloc(L), *x = zalloc(L);
+    double *s1 = zalloc((long)nr * m);
+    memset(vhat, 0, sizeof(double) * ASZ(g));
+    for (int jj = 0; jj < m; jj++) { /* r lines */
+        const int J = jj + NB + 1;
+        for (int k = 0; k < nr; k++) {
+            const int I = k + NB;
+            const long M = IX(g, I, J), W = IX(g, I - 1, J), E = IX(g, I + 1, J), S = IX(g, I, J - 1),
+                       WS = IX(g, I - 1, J - 1), ES = IX(g, I + 1, J - 1);
+            const double rVM = (k + 0.5) * dr, rVW = k * dr, rVE = (k + 1.0) * dr;
+            const double lsVW = axi_q(ls, M, W, S, WS), lsVE = axi_q(ls, M, E, S, ES);
+            const double muVW = 0.25 * (axi_mu(f, H, M) + axi_mu(f, H, W) + axi_mu(f, H, S) + axi_mu(f, H, WS));
+            const double muVE = 0.25 * (axi_mu(f, H, M) + axi_mu(f, H, E) + axi_mu(f, H, S) + axi_mu(f, H, ES));
+            const double thH = axi_heavy(lsVW, lsVE);
+            const double rho = rH * thH + rL * (1.0 - thH);
+            x[k] = rhs[M];
+            lo[k] = -dt / (rho * rVM) * rVW * muVW / (dr * dr);
+            di[k] = 1.0 + dt / (rho * rVM) * (rVW * muVW + rVE * muVE) / (dr * dr);
+            up[k] = -dt / (rho * rVM) * rVE * muVE / (dr * dr);
+            if (k == 0) {
+                if (bW == ORA_NEUMANN || bW == ORA_AXISYM || bW == ORA_OUTLET) { di[k] += lo[k]; lo[k] = 0.0; }
+                else if (bW == ORA_DIRICHLET || bW == ORA_INLET || bW == ORA_WALL) { x[k] -= lo[k] * 2.0 * g->cv[0]; lo[k] = 0.0; }
+                else if (bW == ORA_PERIODIC) { x[k] -= lo[k] * rhs[IX(g, nr - 1 + NB, J)]; lo[k] = 0.0; }
+            }
+            if (k == nr - 1) {
+                if (bE == ORA_NEUMANN || bE == ORA_AXISYM || bE == ORA_OUTLET) { di[k] += up[k]; up[k] = 0.0; }
+                else if (bE == ORA_DIRICHLET || bE == ORA_INLET || bE == ORA_WALL) { x[k] -= up[k] * 2.0 * g->cv[1]; up[k] = 0.0; }
+                else if (bE == ORA_PERIODIC) { x[k] -= up[k] * rhs[IX(g, NB, J)]; up[k] = 0.0; }
+            }
+        }
+        axi_thomas(nr, lo, di, up, x);
+        for (int k = 0; k < nr; k++) s1[jj + (long)m * k] = x[k];
+    }
+    for (int k = 0; k < nr; k++) { /* z lines */
+        const int I = k + NB;
+        for (int jj = 0; jj < m; jj++) {
+            const int J = jj + NB + 1;
+            const long M = IX(g, I, J), S = IX(g, I, J - 1);
+            const double muS = axi_mu(f, H, S), muM = axi_mu(f, H, M);
+            const double thH = axi_heavy(ls[S], ls[M]);
+            const double rho = rH * thH + rL * (1.0 - thH);
+            x[jj] = s1[jj + (long)m * k];
+            lo[jj] = -dt / rho * (2.0 * muS) / (dz * dz);
+            di[jj] = 1.0 + dt / rho * 2.0 * (muS + muM) / (dz * dz);
+            up[jj] = -dt / rho * (2.0 * muM) / (dz * dz);
+            if (jj == 0) {
+                if (bS == ORA_NEUMANN || bS == ORA_OUTLET) { di[jj] += lo[jj]; lo[jj] = 0.0; }
+                else if (bS == ORA_DIRICHLET || bS == ORA_AXISYM || bS == ORA_INLET || bS == ORA_WALL) { x[jj] -= lo[jj] * g->cv[2]; lo[jj] = 0.0; }
+                else if (bS == ORA_PERIODIC) { x[jj] -= lo[jj] * s1[(m - 1) + (long)m * k]; lo[jj] = 0.0; }
+            }
+            if (jj == m - 1) {
+                if (bN == ORA_NEUMANN || bN == ORA_OUTLET) { di[jj] += up[jj]; up[jj] = 0.0; }
+                else if (bN == ORA_DIRICHLET || bN == ORA_AXISYM || bN == ORA_INLET || bN == ORA_WALL) { x[jj] -= up[jj] * g->cv[3]; up[jj] = 0.0; }
+                else if (bN == ORA_PERIODIC) { x[jj] -= up[jj] * s1[0 + (long)m * k]; up[jj] = 0.0; }
+            }
+        }
+        axi_thomas(m, lo, di, up, x);
+        for (int jj = 0; jj < m; jj++) vhat[IX(g, I, jj + NB + 1)] = x[jj];
+    }
+    free(lo); free(di); free(up); free(x); free(s1);
+}
+
+/* GetDivergence4Poisson, mac2dAxisym.cpp:1980-1994: r times the divergence,
+ * (r_e u_e - r_w u_w) / dr + r_c (v_n - v_s) / dz. */
+void ora_axi_div4p(const ora_grid *g, double base_r, const double *u, const double *v, double *div) {
+    const double dr = g->dx, dz = g->dy;
+    memset(div, 0, sizeof(double) * ASZ(g));
+    for (int i = NB; i < g->nx + NB; i++)
+        for (int j = NB; j < g->ny + NB; j++) {
+            const double rc = base_r + (i + 0.5 - NB) * dr, re = base_r + (i + 1.0 - NB) * dr,
+                         rw = base_r + (i - NB) * dr;
+            div[IX(g, i, j)] = (re * u[IX(g, i + 1, j)] - rw * u[IX(g, i, j)]) / dr +
+                               rc * (v[IX(g, i, j + 1)] - v[IX(g, i, j)]) / dz;
+        }
+}
+
+/* GetDivergence, mac2dAxisym.cpp:1996-2008: u/r + du/dr + dv/dz at centres. */
+void ora_axi_divergence(const ora_grid *g, double base_r, const double *u, const double *v, double *div) {
+    const double dr = g->dx, dz = g->dy;
+    memset(div, 0, sizeof(double) * ASZ(g));
+    for (int i = NB; i < g->nx + NB; i++)
+        for (int j = NB; j < g->ny + NB; j++) {
+            const double rc = base_r + (i + 0.5 - NB) * dr;
+            const double uw = u[IX(g, i, j)], ue = u[IX(g, i + 1, j)];
+            div[IX(g, i, j)] = 0.5 * (uw + ue) / rc + (ue - uw) / dr + (v[IX(g, i, j + 1)] - v[IX(g, i, j)]) / dz;
+        }
+}
+
+static int axi_p_neumann(int b) { return b == ORA_NEUMANN || b == ORA_AXISYM || b == ORA_WALL; }
+static int axi_p_dirichlet(int b) {
+    return b == ORA_DIRICHLET || b == ORA_INLET || b == ORA_OUTLET || b == ORA_PRESSURE;
+}
+
+/* SolvePoisson's assembly, mac2dAxisym.cpp:1488-1916: the r-weighted GFM
+ * operator.  West/east faces carry r at the face, or (across the interface)
+ * r interpolated between the two centres with the kappa weight theta (the
+ * west one clamped at 0); south/north faces carry the centre's r.  Neumann
+ * group: Neumann, axisym, wall; Dirichlet group: Dirichlet, inlet, outlet,
+ * pressure (with the 2 * constant of :1797-1801).  ps is zeroed before the
+ * assembly (:1558-1562), which makes the -ps terms -0. */
+int ora_axi_assemble(const ora_grid *g, const ora_fluid *f, double base_r, double dt, const double *ls,
+                     double *kappa, const double *H, const double *div, int recompute_kappa, double *diag,
+                     double *cw, double *ce, double *cs, double *cn, double *rhs) {
+    const int nx = g->nx, ny = g->ny;
+    const double dr = g->dx, dz = g->dy, rH = f->rho_h, rL = f->rho_l, sig = f->sigma;
+    if (recompute_kappa) {
+        ora_axi_kappa(g, base_r, ls, kappa);
+        ora_bc_p(g, kappa);
+    }
+    int pin = 1;
+    for (int s = 0; s < 4; s++) pin &= axi_p_neumann(g->bc_p[s]);
+    for (int j = NB; j < ny + NB; j++)
+        for (int i = NB; i < nx + NB; i++) {
+            const long c = IX(g, i, j), w = IX(g, i - 1, j), e = IX(g, i + 1, j), s = IX(g, i, j - 1),
+                       nn = IX(g, i, j + 1);
+            const int k = (i - NB) + nx * (j - NB);
+            const double lsW = ls[w], lsE = ls[e], lsM = ls[c], lsS = ls[s], lsN = ls[nn];
+            const double rPW = base_r + (i - 0.5 - NB) * dr, rPM = base_r + (i + 0.5 - NB) * dr,
+                         rPE = base_r + (i + 1.5 - NB) * dr, rWf = base_r + (i - NB) * dr,
+                         rEf = base_r + (i + 1.0 - NB) * dr;
+            double thH, th, rEff, rho, kEff;
+            /* west face (:1579-1611) */
+            if (lsW >= 0.0 && lsM >= 0.0) { thH = 1.0; th = 0.0; rEff = rWf; }
+            else if (lsW < 0.0 && lsM < 0.0) { thH = 0.0; th = 0.0; rEff = rWf; }
+            else {
+                gfm_theta_first(lsW, lsM, &thH, &th);
+                rEff = smax(rPM * th + rPW * (1.0 - th), 0.0);
+            }
+            rho = rH * thH + rL * (1.0 - thH);
+            kEff = kappa[c] * th + kappa[w] * (1.0 - th);
+            double pW = rEff / rho;
+            double FW = -dt * (-sig * kEff) * (H[c] - H[w]);
+            FW *= pW / (dr * dr);
+            /* east face (:1614-1644), not clamped */
+            if (lsM >= 0.0 && lsE >= 0.0) { thH = 1.0; th = 0.0; rEff = rEf; }
+            else if (lsM < 0.0 && lsE < 0.0) { thH = 0.0; th = 0.0; rEff = rEf; }
+            else {
+                gfm_theta_second(lsM, lsE, &thH, &th);
+                rEff = rPM * th + rPE * (1.0 - th);
+            }
+            rho = rH * thH + rL * (1.0 - thH);
+            kEff = kappa[c] * th + kappa[e] * (1.0 - th);
+            double pE = rEff / rho;
+            double FE = dt * (-sig * kEff) * (H[e] - H[c]);
+            FE *= pE / (dr * dr);
+            /* south and north faces (:1646-1700): the centre's r */
+            gfm_theta_first(lsS, lsM, &thH, &th);
+            rho = rH * thH + rL * (1.0 - thH);
+            kEff = kappa[c] * th + kappa[s] * (1.0 - th);
+            double pS = rPM / rho;
+            double FS = -dt * (-sig * kEff) * (H[c] - H[s]);
+            FS *= pS / (dz * dz);
+            gfm_theta_second(lsM, lsN, &thH, &th);
+            rho = rH * thH + rL * (1.0 - thH);
+            kEff = kappa[c] * th + kappa[nn] * (1.0 - th);
+            double pN = rPM / rho;
+            double FN = dt * (-sig * kEff) * (H[nn] - H[c]);
+            FN *= pN / (dz * dz);
+            double r = 0.0;
+            r -= FW + FE + FS + FN;
+            r -= div[c];
+            pS *= -1.0; pW *= -1.0; pE *= -1.0; pN *= -1.0;
+            double aS = pS / (dz * dz), aW = pW / (dr * dr), aE = pE / (dr * dr), aN = pN / (dz * dz);
+            double aC = -(pW + pE) / (dr * dr) - (pS + pN) / (dz * dz);
+            if (i == NB && axi_p_neumann(g->bc_p[0])) { aW = 0.0; aC += pW / (dr * dr); }
+            else if (i == NB && axi_p_dirichlet(g->bc_p[0])) { aW = 0.0; r -= pW / (dr * dr) * (-0.0 + 2.0 * g->cp[0]); }
+            if (i == NB + nx - 1 && axi_p_neumann(g->bc_p[1])) { aE = 0.0; aC += pE / (dr * dr); }
+            else if (i == NB + nx - 1 && axi_p_dirichlet(g->bc_p[1])) { aE = 0.0; r -= pE / (dr * dr) * (-0.0 + 2.0 * g->cp[1]); }
+            if (j == NB && axi_p_neumann(g->bc_p[2])) { aS = 0.0; aC += pS / (dz * dz); }
+            else if (j == NB && axi_p_dirichlet(g->bc_p[2])) { aS = 0.0; r -= pS / (dz * dz) * (-0.0 + 2.0 * g->cp[2]); }
+            if (j == NB + ny - 1 && axi_p_neumann(g->bc_p[3])) { aN = 0.0; aC += pN / (dz * dz); }
+            else if (j == NB + ny - 1 && axi_p_dirichlet(g->bc_p[3])) { aN = 0.0; r -= pN / (dz * dz) * (-0.0 + 2.0 * g->cp[3]); }
+            diag[k] = aC;
+            cw[k] = -aW;
+            ce[k] = -aE;
+            cs[k] = -aS;
+            cn[k] = -aN;
+            rhs[k] = r;
+        }
+    if (pin) { /* the corrected pin of ora_gfm_assemble (cell 0 held at 0) */
+        rhs[0] = 0.0;
+        if (nx > 1) cw[1] = 0.0;
+        if (ny > 1) cs[nx] = 0.0;
+    }
+    return pin;
+}
+
+/* UpdateDt, mac2dAxisym.cpp:2104-2133: the CFL bound of the convective,
+ * gravity and surface-tension speeds (the viscous one is computed there but
+ * not used); the surface-tension speed uses max |kappa|. */
+double ora_axi_update_dt(const ora_grid *g, const ora_fluid *f, const double *u, const double *v,
+                         const double *kappa) {
+    const double dr = g->dx, dz = g->dy;
+    double uA = 0.0, vA = 0.0, kA = 0.0;
+    for (int i = NB; i < g->nx + NB; i++)
+        for (int j = NB; j < g->ny + NB; j++) {
+            uA = smax(uA, fabs((u[IX(g, i + 1, j)] * u[IX(g, i, j)]) * 0.5));
+            vA = smax(vA, fabs((v[IX(g, i, j + 1)] * v[IX(g, i, j)]) * 0.5));
+            kA = smax(kA, fabs(kappa[IX(g, i, j)]));
+        }
+    const double C = uA / dr + vA / dz;
+    const double G = smax(sqrt(fabs(f->g) / dz), sqrt(fabs(f->g) / dr));
+    const double h = smin(dr, dz);
+    const double S = sqrt((f->sigma * kA) / (smin(f->rho_h, f->rho_l) * (h * h)));
+    double dt = 1.79769313486231570815e+308;
+    dt = smin(dt, f->cfl / (0.5 * (C + sqrt(C * C + 4.0 * (G * G) + 4.0 * (S * S)))));
+    return dt;
+}
+
 void ora_gather(const ora_grid *g, const double *padded, double *nat) {
     for (int j = 0; j < g->ny; j++)
         for (int i = 0; i < g->nx; i++) nat[i + g->nx * j] = padded[IX(g, i + NB, j + NB)];

@@ -129,6 +129,36 @@ int ora_bicgstab(int nx, int ny, const double *diag, const double *cw, const dou
                  const double *cn, int pinned, const double *b, double *x, double tol, int maxit, int mode,
                  double *resid, double *true_resid);
 
+/* ---- axisymmetric MAC solver (MACSolver2DAxisym, mac2dAxisym.cpp) ----
+ * The grid's x is r (index i, kNr = nx, kDr = dx) and y is z (j).  base_r is
+ * kBaseR; the reference uses it in the curvature, the divergence and the
+ * assembly but not in the viscous terms (which take r = (i + 1/2) dr). */
+void ora_axi_kappa(const ora_grid *g, double base_r, const double *ls, double *kappa);
+void ora_axi_visc_u(const ora_grid *g, const ora_fluid *f, const double *u, const double *v, const double *ls,
+                    const double *H, double *dU);
+void ora_axi_visc_v(const ora_grid *g, const ora_fluid *f, const double *u, const double *uhat, const double *v,
+                    const double *ls, const double *H, double *dV);
+/* GetRHSU / GetRHSV with time step dt, including their U / V ghost fill. */
+void ora_axi_rhs_u(const ora_grid *g, const ora_fluid *f, double dt, const double *ls, const double *u,
+                   const double *v, const double *H, double *rhs);
+void ora_axi_rhs_v(const ora_grid *g, const ora_fluid *f, double dt, const double *ls, const double *u,
+                   const double *uhat, const double *v, const double *H, double *rhs);
+/* GetUHat / GetVHat: the implicit viscous step (no ghost fill). */
+void ora_axi_uhat(const ora_grid *g, const ora_fluid *f, double dt, const double *ls, const double *rhs,
+                  const double *H, double *uhat);
+void ora_axi_vhat(const ora_grid *g, const ora_fluid *f, double dt, const double *ls, const double *rhs,
+                  const double *H, double *vhat);
+/* GetDivergence4Poisson (r-weighted) and GetDivergence. */
+void ora_axi_div4p(const ora_grid *g, double base_r, const double *u, const double *v, double *div);
+void ora_axi_divergence(const ora_grid *g, double base_r, const double *u, const double *v, double *div);
+/* SolvePoisson's assembly (mac2dAxisym.cpp:1488-1916) in the matrix-free
+ * form of ora_gfm_assemble. */
+int ora_axi_assemble(const ora_grid *g, const ora_fluid *f, double base_r, double dt, const double *ls,
+                     double *kappa, const double *H, const double *div, int recompute_kappa, double *diag,
+                     double *cw, double *ce, double *cs, double *cn, double *rhs);
+double ora_axi_update_dt(const ora_grid *g, const ora_fluid *f, const double *u, const double *v,
+                         const double *kappa);
+
 /* Scatter/gather between natural-order vectors and padded cell arrays. */
 void ora_gather(const ora_grid *g, const double *padded, double *nat);
 void ora_scatter(const ora_grid *g, const double *nat, double *padded);

@@ -134,6 +134,17 @@ class Oracle:
                              C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)],
             "ora_gather": [G, _dp, _dp], "ora_scatter": [G, _dp, _dp],
             "ora_interface_mask": [G, _dp, _u8], "ora_ghost_face_mask": [G, _dp, _u8],
+            "ora_axi_kappa": [G, C.c_double, _dp, _dp],
+            "ora_axi_visc_u": [G, F, _dp, _dp, _dp, _dp, _dp],
+            "ora_axi_visc_v": [G, F, _dp, _dp, _dp, _dp, _dp, _dp],
+            "ora_axi_rhs_u": [G, F, C.c_double, _dp, _dp, _dp, _dp, _dp],
+            "ora_axi_rhs_v": [G, F, C.c_double, _dp, _dp, _dp, _dp, _dp, _dp],
+            "ora_axi_uhat": [G, F, C.c_double, _dp, _dp, _dp, _dp],
+            "ora_axi_vhat": [G, F, C.c_double, _dp, _dp, _dp, _dp],
+            "ora_axi_div4p": [G, C.c_double, _dp, _dp, _dp],
+            "ora_axi_divergence": [G, C.c_double, _dp, _dp, _dp],
+            "ora_axi_assemble": [G, F, C.c_double, C.c_double, _dp, _dp, _dp, _dp, C.c_int, _dp, _dp, _dp, _dp,
+                                 _dp, _dp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -147,6 +158,9 @@ class Oracle:
         L.ora_gfm_to_csr.restype = C.c_int
         L.ora_pcg.restype = C.c_int
         L.ora_bicgstab.restype = C.c_int
+        L.ora_axi_assemble.restype = C.c_int
+        L.ora_axi_update_dt.argtypes = [G, F, _dp, _dp, _dp]
+        L.ora_axi_update_dt.restype = C.c_double
 
     # ---- boundary ----
     def bc(self, g: GridSpec, kind: str, a: np.ndarray) -> np.ndarray:
@@ -331,6 +345,97 @@ class Oracle:
         return dict(iters=it, resid=res, true_resid=tres, sys=sysd, div=div, H=H, HS=HS, uhat=uh, vhat=vh)
 
 
+    # ---- axisymmetric MAC solver (mac2dAxisym.cpp); x is r, y is z ----
+    def axi_kappa(self, g, base_r, ls, kappa=None):
+        k = g.zeros() if kappa is None else kappa
+        self.L.ora_axi_kappa(C.byref(g.c()), base_r, ls, k)
+        return k
+
+    def axi_visc(self, g, f, u, uhat, v, ls, H):
+        a, b = g.zeros(), g.zeros()
+        self.L.ora_axi_visc_u(C.byref(g.c()), C.byref(f.c()), u, v, ls, H, a)
+        self.L.ora_axi_visc_v(C.byref(g.c()), C.byref(f.c()), u, uhat, v, ls, H, b)
+        return a, b
+
+    def axi_rhs_u(self, g, f, dt, ls, u, v, H):
+        out = g.zeros()
+        self.L.ora_axi_rhs_u(C.byref(g.c()), C.byref(f.c()), dt, ls, u, v, H, out)
+        return out
+
+    def axi_rhs_v(self, g, f, dt, ls, u, uhat, v, H):
+        out = g.zeros()
+        self.L.ora_axi_rhs_v(C.byref(g.c()), C.byref(f.c()), dt, ls, u, uhat, v, H, out)
+        return out
+
+    def axi_uhat(self, g, f, dt, ls, rhs, H):
+        out = g.zeros()
+        self.L.ora_axi_uhat(C.byref(g.c()), C.byref(f.c()), dt, ls, rhs, H, out)
+        return out
+
+    def axi_vhat(self, g, f, dt, ls, rhs, H):
+        out = g.zeros()
+        self.L.ora_axi_vhat(C.byref(g.c()), C.byref(f.c()), dt, ls, rhs, H, out)
+        return out
+
+    def axi_div4p(self, g, base_r, u, v):
+        out = g.zeros()
+        self.L.ora_axi_div4p(C.byref(g.c()), base_r, u, v, out)
+        return out
+
+    def axi_divergence(self, g, base_r, u, v):
+        out = g.zeros()
+        self.L.ora_axi_divergence(C.byref(g.c()), base_r, u, v, out)
+        return out
+
+    def axi_assemble(self, g, f, base_r, dt, ls, kappa, H, div, recompute_kappa=True):
+        n = g.nx * g.ny
+        d, cw, ce, cs, cn, rhs = (np.zeros(n) for _ in range(6))
+        pinned = self.L.ora_axi_assemble(C.byref(g.c()), C.byref(f.c()), base_r, dt, ls, kappa, H, div,
+                                         1 if recompute_kappa else 0, d, cw, ce, cs, cn, rhs)
+        return dict(diag=d, cw=cw, ce=ce, cs=cs, cn=cn, rhs=rhs, pinned=pinned)
+
+    def axi_update_dt(self, g, f, u, v, kappa) -> float:
+        return self.L.ora_axi_update_dt(C.byref(g.c()), C.byref(f.c()), u, v, kappa)
+
+    def axi_step(self, g, f, st, base_r=0.0, ls_grid=None, tol=1e-10, maxit=200000, reinit_mode=2):
+        """One step of the reference's axisymmetric driver
+        (tests/LargeTests/test_mac2d_large.cpp:1264-1303): level set advected
+        and reinitialised on ``ls_grid`` (the level-set solver's boundary
+        kinds; default g), curvature, Heaviside, the implicit viscous uhat and
+        vhat, the r-weighted divergence, the assembly solved by the
+        fixed-order FP64 PCG to ``tol``, the projection and the next dt.
+        ``st`` holds ls, u, v, kappa (padded) and dt; updated in place."""
+        lg = g if ls_grid is None else ls_grid
+        ls, u, v = st["ls"], st["u"], st["v"]
+        dt = st["dt"]
+        lsB = ls.copy()
+        self.ls_advect(lg, ls, u, v, dt)
+        self.bc(lg, "p", ls)
+        self.reinit(lg, reinit_mode, ls)
+        self.bc(lg, "p", ls)
+        self.axi_kappa(g, base_r, ls, st["kappa"])
+        H = self.heaviside(g, ls)
+        HS = self.smooth_heaviside(g, ls)
+        rhs_u = self.axi_rhs_u(g, f, dt, ls, u, v, HS)
+        uh = self.axi_uhat(g, f, dt, ls, rhs_u, HS)
+        self.bc(g, "u", uh)
+        rhs_v = self.axi_rhs_v(g, f, dt, ls, u, uh, v, HS)
+        vh = self.axi_vhat(g, f, dt, ls, rhs_v, HS)
+        self.bc(g, "v", vh)
+        div = self.axi_div4p(g, base_r, uh, vh)
+        sysd = self.axi_assemble(g, f, base_r, dt, ls, st["kappa"], H, div, recompute_kappa=f.sigma != 0.0)
+        x, it, res, tres = self.pcg(g, sysd, tol=tol, maxit=maxit, mode=0)
+        ps = g.zeros()
+        self.scatter(g, x, ps)
+        self.bc(g, "p", ps)
+        st["ps"] = ps
+        self.update_vel(g, f, dt, u, v, uh, vh, ps, ls, H, st["kappa"])
+        st["dt_used"] = dt
+        st["dt"] = self.axi_update_dt(g, f, u, v, st["kappa"])
+        return dict(iters=it, resid=res, true_resid=tres, sys=sysd, div=div, H=H, HS=HS, uhat=uh, vhat=vh,
+                    rhs_u=rhs_u, rhs_v=rhs_v)
+
+
 class Reference:
     """The reference's own classes, compiled unmodified (oracle/_ref)."""
 
@@ -513,6 +618,123 @@ class Reference:
 
     def update_dt(self, u, v) -> float:
         return self.L.ref_mac_update_dt(self.h, u, v)
+
+
+class AxiReference:
+    """The reference's MACSolver2DAxisym, compiled unmodified (oracle/_ref).
+    Grid x is r, y is z; gravity axis 0 = R, 1 = Z."""
+
+    def __init__(self, g: GridSpec, f: FluidSpec | None = None, base_r=0.0, base_z=0.0, path: str = REF_SO):
+        L = self.L = _load(path)
+        f = f or FluidSpec()
+        self.g = g
+        V = C.c_void_p
+        L.ref_axi_create.restype = V
+        L.ref_axi_create.argtypes = [C.c_int, C.c_int] + [C.c_double] * 9 + [C.c_int, C.c_double, C.c_double]
+        self.h = V(L.ref_axi_create(g.nx, g.ny, base_r, base_z, g.dx * g.nx, g.dy * g.ny, f.rho_h, f.rho_l, f.mu_h,
+                                    f.mu_l, f.g, f.g_axis, f.sigma, f.cfl))
+        for name, args, res in [
+            ("ref_axi_set_bc", [V, C.c_char, C.c_char_p, _dp], None),
+            ("ref_axi_apply_bc", [V, C.c_char, _dp], None),
+            ("ref_axi_set_state", [V, _dp, _dp, _dp, C.c_double], None),
+            ("ref_axi_get_state", [V, _dp, _dp, _dp, _dp, _dp], None),
+            ("ref_axi_kappa", [V, _dp, _dp], None),
+            ("ref_axi_visc", [V, _dp, _dp, _dp, _dp, _dp, _dp, _dp], None),
+            ("ref_axi_rhs_u", [V, _dp, _dp, _dp, _dp, _dp], None),
+            ("ref_axi_rhs_v", [V, _dp, _dp, _dp, _dp, _dp, _dp], None),
+            ("ref_axi_uhat", [V, _dp, _dp, _dp, _dp, _dp], None),
+            ("ref_axi_vhat", [V, _dp, _dp, _dp, _dp, _dp], None),
+            ("ref_axi_div", [V, _dp, _dp, _dp, _dp], None),
+            ("ref_axi_poisson", [V, _dp, _dp, _dp, _dp, _dp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                 C.POINTER(C.c_int)], C.c_int),
+            ("ref_capture_copy", [_dp, _ip, _ip, _dp], C.c_int),
+            ("ref_axi_update_vel", [V, _dp, _dp, _dp, _dp, _dp, _dp], None),
+            ("ref_axi_update_dt", [V, _dp, _dp], C.c_double),
+            ("ref_axi_destroy", [V], None),
+        ]:
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        for kind, names, consts in (("U", g.bc_u, g.cu), ("V", g.bc_v, g.cv), ("P", g.bc_p, g.cp)):
+            L.ref_axi_set_bc(self.h, kind.encode(), " ".join(names).encode(), np.array(consts, dtype=np.float64))
+
+    def close(self):
+        if self.h:
+            self.L.ref_axi_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def z(self):
+        return self.g.zeros()
+
+    def bc(self, kind, a):
+        self.L.ref_axi_apply_bc(self.h, kind.upper().encode(), a)
+        return a
+
+    def set_state(self, u, v, kappa, dt):
+        self.L.ref_axi_set_state(self.h, u, v, kappa, dt)
+
+    def get_state(self):
+        u, v, ps, p, k = (self.z() for _ in range(5))
+        self.L.ref_axi_get_state(self.h, u, v, ps, p, k)
+        return dict(u=u, v=v, ps=ps, p=p, kappa=k)
+
+    def kappa(self, ls):
+        out = self.z()
+        self.L.ref_axi_kappa(self.h, ls, out)
+        return out
+
+    def visc(self, u, uhat, v, ls, H):
+        a, b = self.z(), self.z()
+        self.L.ref_axi_visc(self.h, u, uhat, v, ls, H, a, b)
+        return a, b
+
+    def rhs_u(self, ls, u, v, H):
+        out = self.z()
+        self.L.ref_axi_rhs_u(self.h, ls, u, v, H, out)
+        return out
+
+    def rhs_v(self, ls, u, uhat, v, H):
+        out = self.z()
+        self.L.ref_axi_rhs_v(self.h, ls, u, uhat, v, H, out)
+        return out
+
+    def uhat(self, ls, u, rhs, H):
+        out = self.z()
+        self.L.ref_axi_uhat(self.h, ls, u, rhs, H, out)
+        return out
+
+    def vhat(self, ls, v, rhs, H):
+        out = self.z()
+        self.L.ref_axi_vhat(self.h, ls, v, rhs, H, out)
+        return out
+
+    def divergences(self, u, v):
+        a, b = self.z(), self.z()
+        self.L.ref_axi_div(self.h, u, v, a, b)
+        return a, b
+
+    def poisson_capture(self, div, ls, lsB, H, maxiter=0):
+        ps = self.z()
+        m, nnz, nb = C.c_int(), C.c_int(), C.c_int()
+        rc = self.L.ref_axi_poisson(self.h, ps, div, ls, lsB, H, maxiter, C.byref(m), C.byref(nnz), C.byref(nb))
+        if rc != 0:
+            raise RuntimeError("no system captured")
+        a, ia, ja, b = np.zeros(nnz.value), np.zeros(m.value + 1, np.int32), np.zeros(nnz.value, np.int32), \
+            np.zeros(nb.value)
+        self.L.ref_capture_copy(a, ia, ja, b)
+        return ps, (a, ia, ja, b)
+
+    def update_vel(self, uhat, vhat, ps, ls, lsB, H):
+        self.L.ref_axi_update_vel(self.h, uhat, vhat, ps, ls, lsB, H)
+
+    def update_dt(self, u, v) -> float:
+        return self.L.ref_axi_update_dt(self.h, u, v)
 
 
 def have_reference() -> bool:
