@@ -78,6 +78,8 @@ EXPORTS = [
     "asd2g_unet_train_step_residual", "asd2g_unet_train_step_energy",
     "asd2g_unet_error_flag", "asd2g_unet_set_stream", "asd2g_set_preconditioner_net", "asd2g_last_fallback",
     "asd2g_last_solve_one_launch",
+    "asd2g_axi_kappa", "asd2g_axi_rhs_u", "asd2g_axi_rhs_v", "asd2g_axi_hat", "asd2g_axi_divergence",
+    "asd2g_axi_assemble", "asd2g_axi_update_dt", "asd2g_axi_step",
     "asd2g_pc_training_pair", "asd2g_pc_training_pair_at",
 ]
 
@@ -131,6 +133,11 @@ def load(path: str = LIB_PATH) -> C.CDLL:
                                     C.c_void_p, C.POINTER(I), C.POINTER(D)], I),
         "asd2g_weno5_line": ([S, dp, dp, dp, D, I], I), "asd2g_weno_absgrad": ([S, I, I, I], I),
         "asd2g_apply_bc_side": ([S, I, C.c_char, I, I], I), "asd2g_update_ntk": ([S, I, I, I], I),
+        "asd2g_axi_kappa": ([S], I), "asd2g_axi_rhs_u": ([S, D, I, I, I, I, I], I),
+        "asd2g_axi_rhs_v": ([S, D, I, I, I, I, I, I], I), "asd2g_axi_hat": ([S, I, D, I, I, I, I], I),
+        "asd2g_axi_divergence": ([S, I, I, I, I], I), "asd2g_axi_assemble": ([S, D, I], I),
+        "asd2g_axi_update_dt": ([S, C.POINTER(D)], I),
+        "asd2g_axi_step": ([S, C.POINTER(D), I, C.c_void_p, C.c_void_p, I, D, I, C.POINTER(I), C.POINTER(D)], I),
         "asd2g_csr_solve": ([S, I, I, ip, ip, dp, dp, dp, dp, D, I, C.POINTER(I), C.POINTER(D)], I),
         "asd2g_volume": ([S, C.POINTER(D), C.POINTER(D)], I),
         "asd2g_last_volume": ([S, C.POINTER(D), C.POINTER(D)], I),
@@ -434,6 +441,49 @@ class Session:
         d, it, res = C.c_double(dt), C.c_int(), C.c_double()
         rc = self._check(self.L.asd2g_droplet_step(self.h, C.byref(d), reinit_mode, solver, tol, maxit,
                                                    C.byref(it), C.byref(res)))
+        return dict(status=rc, dt_next=d.value, iters=it.value, resid=res.value)
+
+    # ---- axisymmetric MAC solver (x is r, y is z; base_x is kBaseR) ----
+    def axi_kappa(self):
+        self._check(self.L.asd2g_axi_kappa(self.h))
+
+    def axi_rhs_u(self, dt, ls="ls", u="u", v="v", h="HS", out="w0"):
+        self._check(self.L.asd2g_axi_rhs_u(self.h, dt, *(self._f(x) for x in (ls, u, v, h, out))))
+
+    def axi_rhs_v(self, dt, ls="ls", u="u", uhat="uhat", v="v", h="HS", out="w0"):
+        self._check(self.L.asd2g_axi_rhs_v(self.h, dt, *(self._f(x) for x in (ls, u, uhat, v, h, out))))
+
+    def axi_hat(self, comp, dt, ls="ls", rhs="w0", h="HS", out=None):
+        """GetUHat (comp 0) / GetVHat (comp 1) into out (default uhat / vhat)."""
+        out = ("uhat" if comp == 0 else "vhat") if out is None else out
+        self._check(self.L.asd2g_axi_hat(self.h, comp, dt, *(self._f(x) for x in (ls, rhs, h, out))))
+
+    def axi_divergence(self, u="uhat", v="vhat", div="div", for_poisson=True):
+        self._check(self.L.asd2g_axi_divergence(self.h, self._f(u), self._f(v), self._f(div),
+                                                1 if for_poisson else 0))
+
+    def axi_assemble(self, dt, recompute_kappa=True):
+        self._check(self.L.asd2g_axi_assemble(self.h, dt, 1 if recompute_kappa else 0))
+
+    def axi_update_dt(self) -> float:
+        d = C.c_double()
+        self._check(self.L.asd2g_axi_update_dt(self.h, C.byref(d)))
+        return d.value
+
+    def axi_step(self, dt, reinit_mode=REINIT_MINRK2, ls_bc=None, ls_bcc=None, solver=PCG, tol=1e-10,
+                 maxit=200000):
+        """One step of the reference's axisymmetric driver; ls_bc: the level-set
+        solver's four P-grid kinds (names or asd2g_bc values; None: the
+        session's pressure kinds) with constants ls_bcc."""
+        kinds = consts = None
+        if ls_bc is not None:
+            kinds = (C.c_int32 * 4)(*[BC[k] if isinstance(k, str) else int(k) for k in ls_bc])
+            consts = (C.c_double * 4)(*(ls_bcc if ls_bcc is not None else (0.0,) * 4))
+        d, it, res = C.c_double(dt), C.c_int(), C.c_double()
+        rc = self._check(self.L.asd2g_axi_step(self.h, C.byref(d), reinit_mode,
+                                               C.cast(kinds, C.c_void_p) if kinds is not None else None,
+                                               C.cast(consts, C.c_void_p) if consts is not None else None,
+                                               solver, tol, maxit, C.byref(it), C.byref(res)))
         return dict(status=rc, dt_next=d.value, iters=it.value, resid=res.value)
 
     def run_steps(self, nsteps, dt, reinit_mode=REINIT_MINRK2, solver=MGPCG, tol=1e-10, maxit=10000):

@@ -28,6 +28,7 @@ UNITS = {
     "bc.cu": ["-fmad=false"],
     "levelset.cu": ["-fmad=false"],
     "momentum.cu": ["-fmad=false"],
+    "axisym.cu": ["-fmad=false"],
     "pressure.cu": ["-fmad=false"],
     "api.cu": [],
     "pcg_static.cu": ["-fmad=false"],

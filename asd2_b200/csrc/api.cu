@@ -183,12 +183,15 @@ int grid_from_params(const asd2g_params *p, Grid &g, MomConst &M) {
     g.sy = p->ny + 2 * NB;
     g.dx = p->dx;
     g.dy = p->dy;
+    g.base_x = p->base_x;
     bool mirror = true, pinned = true;
     for (int k = 0; k < 4; k++) {
         g.ku[k] = kind_u(k, p->bc_u[k]);
         g.kv[k] = kind_v(k, p->bc_v[k]);
         g.kp[k] = kind_p(p->bc_p[k]);
         g.bp[k] = p->bc_p[k];
+        g.bu[k] = p->bc_u[k];
+        g.bv[k] = p->bc_v[k];
         g.cu[k] = p->bcc_u[k];
         g.cv[k] = p->bcc_v[k];
         g.cp[k] = p->bcc_p[k];
@@ -1482,6 +1485,184 @@ int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver
     *dt = s->dsc_host[1];
     s->last_volume[0] = s->dsc_host[5];
     s->last_volume[1] = s->dsc_host[6];
+    return st;
+}
+
+
+// ---- axisymmetric MAC solver (MACSolver2DAxisym, mac2dAxisym.cpp) ----
+// x is r, y is z; base_x of the parameters is kBaseR.  Convection, Heaviside,
+// UpdateVel and the Krylov solvers are the 2D ones (same arithmetic).
+namespace {
+int axi_p_supported(asd2g_session *s) {
+    for (int k = 0; k < 4; k++) {
+        const int b = s->prm.bc_p[k];
+        if (b == ASD2G_BC_PERIODIC || b == ASD2G_BC_LSFREE || b == ASD2G_BC_CUSTOM)
+            return fail(ASD2G_E_UNSUPPORTED,
+                        "pressure boundary kind %d on side %d: the axisymmetric assembly supports Neumann, axisym, "
+                        "wall, Dirichlet, inlet, outlet and pressure sides",
+                        b, k);
+    }
+    return ASD2G_OK;
+}
+
+// GetRHSU / GetRHSV: the 2D convection term into ua, then the axisymmetric
+// right side over the whole padded array, then the U / V ghost fill.
+int axi_rhs(asd2g_session *s, int comp, int ls, int u, int v, int uhat, int h, int out) {
+    const Grid &g = s->g;
+    launch_mom_stage(5, g, s->M, s->f[ls], s->f[h], s->f[u], s->f[v], nullptr, nullptr, comp == 0 ? s->ua : s->va,
+                     comp == 0 ? s->va : s->ua, s->dsc, s->st);
+    if (comp == 0) {
+        launch_axi_rhs_u(g, s->M, s->f[ls], s->f[u], s->f[v], s->f[h], s->ua, s->dsc, s->f[out], s->st);
+        launch_fill_uv(g, s->f[out], nullptr, s->st);
+    } else {
+        launch_axi_rhs_v(g, s->M, s->f[ls], s->f[u], s->f[uhat], s->f[v], s->f[h], s->ua, s->dsc, s->f[out], s->st);
+        launch_fill_uv(g, nullptr, s->f[out], s->st);
+    }
+    return cuda_check(comp == 0 ? "axi_rhs_u" : "axi_rhs_v");
+}
+
+void axi_assemble_enqueue(asd2g_session *s, int recompute_kappa) {
+    const Grid &g = s->g;
+    if (recompute_kappa) {
+        launch_axi_kappa(g, s->f[ASD2G_LS], s->f[ASD2G_KAPPA], s->st);
+        launch_fill_p(g, s->f[ASD2G_KAPPA], s->st);
+    }
+    launch_axi_assemble(g, s->M, s->f[ASD2G_LS], s->f[ASD2G_KAPPA], s->f[ASD2G_H], s->f[ASD2G_DIV], s->dsc, s->sys,
+                        s->st);
+    s->assembled = true;
+}
+
+int axi_we_finite(const asd2g_session *s) {
+    const double we = s->prm.numbers_given ? s->prm.we : s->prm.rho_h / s->prm.sigma;
+    return (we != 0.0 && std::isfinite(we)) ? 1 : 0;
+}
+}  // namespace
+
+int asd2g_axi_kappa(asd2g_session *s) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    launch_axi_kappa(s->g, s->f[ASD2G_LS], s->f[ASD2G_KAPPA], s->st);
+    return cuda_check("axi_kappa");
+}
+
+int asd2g_axi_rhs_u(asd2g_session *s, double dt, int ls, int u, int v, int h, int out) {
+    if (!s || !valid_field(ls) || !valid_field(u) || !valid_field(v) || !valid_field(h) || !valid_field(out) ||
+        out == ls || out == u || out == v || out == h)
+        return fail(ASD2G_E_ARG, "bad field");
+    int rc = set_dt(s, dt);
+    return rc ? rc : axi_rhs(s, 0, ls, u, v, -1, h, out);
+}
+
+int asd2g_axi_rhs_v(asd2g_session *s, double dt, int ls, int u, int uhat, int v, int h, int out) {
+    if (!s || !valid_field(ls) || !valid_field(u) || !valid_field(uhat) || !valid_field(v) || !valid_field(h) ||
+        !valid_field(out) || out == ls || out == u || out == uhat || out == v || out == h)
+        return fail(ASD2G_E_ARG, "bad field");
+    int rc = set_dt(s, dt);
+    return rc ? rc : axi_rhs(s, 1, ls, u, v, uhat, h, out);
+}
+
+int asd2g_axi_hat(asd2g_session *s, int comp, double dt, int ls, int rhs, int h, int out) {
+    if (!s || (comp != 0 && comp != 1) || !valid_field(ls) || !valid_field(rhs) || !valid_field(h) ||
+        !valid_field(out) || out == ls || out == rhs || out == h)
+        return fail(ASD2G_E_ARG, "bad field or component");
+    int rc = set_dt(s, dt);
+    if (rc) return rc;
+    launch_axi_hat(s->g, s->M, comp, s->f[ls], s->f[rhs], s->f[h], s->dsc, s->f[out], s->ub, s->vb, s->va, s->st);
+    return cuda_check("axi_hat");
+}
+
+int asd2g_axi_divergence(asd2g_session *s, int u, int v, int div, int for_poisson) {
+    if (!s || !valid_field(u) || !valid_field(v) || !valid_field(div) || div == u || div == v)
+        return fail(ASD2G_E_ARG, "bad field");
+    launch_axi_div(s->g, for_poisson ? 1 : 0, s->f[u], s->f[v], s->f[div], s->st);
+    return cuda_check("axi_divergence");
+}
+
+int asd2g_axi_assemble(asd2g_session *s, double dt, int recompute_kappa) {
+    if (!s) return fail(ASD2G_E_ARG, "null session");
+    int rc = axi_p_supported(s);
+    if (rc) return rc;
+    rc = set_dt(s, dt);
+    if (rc) return rc;
+    axi_assemble_enqueue(s, recompute_kappa);
+    return cuda_check("axi_assemble");
+}
+
+int asd2g_axi_update_dt(asd2g_session *s, double *dt) {
+    if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
+    launch_axi_update_dt(s->g, s->M, s->f[ASD2G_U], s->f[ASD2G_V], s->f[ASD2G_KAPPA], s->partial, s->counter,
+                         s->dsc + 1, s->st);
+    cudaMemcpyAsync(s->dsc_host, s->dsc, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
+    int rc = sync(s);
+    if (rc) return rc;
+    *dt = s->dsc_host[1];
+    return ASD2G_OK;
+}
+
+int asd2g_axi_step(asd2g_session *s, double *dt, int reinit_mode, const int32_t *ls_bc, const double *ls_bcc,
+                   int solver, double tol, int maxit, int *iters, double *rel_resid) {
+    NvtxRange nv("asd2g_axi_step");
+    if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
+    if (reinit_mode < 0 || reinit_mode > 4) return fail(ASD2G_E_ARG, "reinit mode %d out of range", reinit_mode);
+    if (s->prm.precision != ASD2G_PRECISION_FP64)
+        return fail(ASD2G_E_UNSUPPORTED, "the axisymmetric step runs in FP64 only");
+    if (solver < 0 || solver > ASD2G_SOLVER_MGPCG) return fail(ASD2G_E_ARG, "solver %d out of range", solver);
+    int rc = axi_p_supported(s);
+    if (rc) return rc;
+    // the level-set solver's own P-grid boundary (LevelSetSolver2D has its own BoundaryCondition2D)
+    Grid gl = s->g;
+    if (ls_bc) {
+        bool mirror = true;
+        for (int k = 0; k < 4; k++) {
+            if (ls_bc[k] < 0 || ls_bc[k] > 9) return fail(ASD2G_E_ARG, "level-set boundary kind out of range");
+            gl.kp[k] = kind_p(ls_bc[k]);
+            gl.bp[k] = ls_bc[k];
+            gl.cp[k] = ls_bcc ? ls_bcc[k] : 0.0;
+            mirror &= (gl.kp[k] == K_NEU || gl.kp[k] == K_DIR);
+        }
+        gl.p_mirror = mirror ? 1 : 0;
+    }
+    rc = set_dt(s, *dt);
+    if (rc) return rc;
+    const Grid &g = s->g;
+    double *ls = s->f[ASD2G_LS], *u = s->f[ASD2G_U], *v = s->f[ASD2G_V];
+    double *uh = s->f[ASD2G_UHAT], *vh = s->f[ASD2G_VHAT], *HS = s->f[ASD2G_HS];
+    // level set (test_mac2d_large.cpp:1269-1274)
+    cudaMemcpyAsync(s->f[ASD2G_LSB], ls, sizeof(double) * s->G, cudaMemcpyDeviceToDevice, s->st);
+    launch_center_vel(gl, u, v, s->tu, s->tv, s->st);
+    launch_fill_p(gl, ls, s->st);
+    launch_ls_stage(1, gl, ls, s->tu, s->tv, ls, s->w1, s->dsc, s->st);
+    launch_ls_stage(2, gl, s->w1, s->tu, s->tv, ls, s->w2, s->dsc, s->st);
+    launch_ls_stage(3, gl, s->w2, s->tu, s->tv, ls, ls, s->dsc, s->st);
+    launch_fill_p(gl, ls, s->st);
+    launch_reinit(gl, reinit_mode, s->prm.ls_max_atime, ls, s->f[ASD2G_LS0], s->w1, s->w2, s->w3, s->st);
+    launch_fill_p(gl, ls, s->st);
+    // momentum (:1276-1292)
+    launch_axi_kappa(g, ls, s->f[ASD2G_KAPPA], s->st);
+    launch_heaviside(g, ls, s->f[ASD2G_H], HS, s->st);
+    rc = axi_rhs(s, 0, ASD2G_LS, ASD2G_U, ASD2G_V, -1, ASD2G_HS, ASD2G_W0);
+    if (rc) return rc;
+    launch_axi_hat(g, s->M, 0, ls, s->f[ASD2G_W0], HS, s->dsc, uh, s->ub, s->vb, s->va, s->st);
+    launch_fill_uv(g, uh, nullptr, s->st);
+    rc = axi_rhs(s, 1, ASD2G_LS, ASD2G_U, ASD2G_V, ASD2G_UHAT, ASD2G_HS, ASD2G_W0);
+    if (rc) return rc;
+    launch_axi_hat(g, s->M, 1, ls, s->f[ASD2G_W0], HS, s->dsc, vh, s->ub, s->vb, s->va, s->st);
+    launch_fill_uv(g, nullptr, vh, s->st);
+    launch_axi_div(g, 1, uh, vh, s->f[ASD2G_DIV], s->st);
+    axi_assemble_enqueue(s, axi_we_finite(s));
+    rc = cuda_check("axi_step (before the solve)");
+    if (rc) return rc;
+    // pressure, projection, dt (:1294-1306)
+    const int st = solve(s, solver, tol, maxit, iters, rel_resid);
+    if (st < 0) return st;
+    launch_scatter_ps(g, s->x, s->f[ASD2G_PS], s->f[ASD2G_P], s->dsc, s->st);
+    launch_update_vel(g, s->M, uh, vh, s->f[ASD2G_PS], ls, s->f[ASD2G_H], s->f[ASD2G_KAPPA], u, v, s->dsc, s->st);
+    launch_axi_update_dt(g, s->M, u, v, s->f[ASD2G_KAPPA], s->partial, s->counter, s->dsc + 1, s->st);
+    cudaMemcpyAsync(s->dsc_host, s->dsc, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
+    rc = sync(s);
+    if (rc) return rc;
+    rc = cuda_check("axi_step");
+    if (rc) return rc;
+    *dt = s->dsc_host[1];
     return st;
 }
 

@@ -23,6 +23,8 @@ struct Grid {
     int32_t p_mirror;             // all four P sides are K_NEU/K_DIR: producers write ghost mirrors
     int32_t pinned;               // all four P sides Neumann/axisym/wall (mac2d.cpp:1496-1500)
     int32_t kappa_mode;           // ASD2G_CURVATURE_*
+    int32_t bu[4], bv[4];         // raw BC2D values of U and V (the axisymmetric implicit step's end rows)
+    double base_x;                // lower-left corner x (kBaseR of the axisymmetric solver)
 };
 
 __host__ __device__ __forceinline__ int64_t IX(const Grid &g, int i, int j) { return (int64_t)j + (int64_t)g.sy * i; }

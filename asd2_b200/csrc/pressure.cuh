@@ -77,5 +77,8 @@ bool launch_pcg_persist(int nx, int ny, const Sys &S, double *x, double *r, doub
 int pcg_cluster_size(int nx, int ny);
 bool launch_pcg_cluster(int nx, int ny, const Sys &S, double *x, KState *ks, double tol, int maxit,
                         cudaStream_t st);
+// axisym.cu: SolvePoisson's r-weighted assembly of the axisymmetric solver.
+void launch_axi_assemble(const Grid &g, const MomConst &M, const double *ls, const double *kappa, const double *H,
+                         const double *div, const double *dtp, const Sys &S, cudaStream_t st);
 
 }  // namespace asd2g

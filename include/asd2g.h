@@ -252,6 +252,50 @@ int asd2g_update_dt(asd2g_session *s, double *dt);
  * (ENO gradient), written into fields nxf and nyf; other cells untouched. */
 int asd2g_update_ntk(asd2g_session *s, int ls, int nxf, int nyf);
 
+/* ---- axisymmetric MAC solver (MACSolver2DAxisym, mac2dAxisym.cpp) ----
+ * The session's grid is read as (r, z): x is r (nx = kNr, dx = kDr, base_x =
+ * kBaseR), y is z.  Gravity axis 0 is R, 1 is Z (GAXISENUM2DAXISYM).  The
+ * convection term, Heaviside, UpdateVel and the pressure solvers are the 2D
+ * entry points (the reference's axisymmetric versions are the same
+ * arithmetic; asd2g_heaviside, asd2g_update_vel, asd2g_solve_pressure). */
+/* UpdateKappa(LS) -> KAPPA interior, mac2dAxisym.cpp:222 (the hoop term
+ * uses r = base_x + (i + 1/2) dr). */
+int asd2g_axi_kappa(asd2g_session *s);
+/* GetRHSU(ls, u, v, h) with time step dt -> out (whole padded array, U ghost
+ * fill applied), :264.  Viscosity is skipped when kRe <= 0. */
+int asd2g_axi_rhs_u(asd2g_session *s, double dt, int ls, int u, int v, int h, int out);
+/* GetRHSV(ls, u, uhat, v, h) -> out (V ghost fill applied), :294. */
+int asd2g_axi_rhs_v(asd2g_session *s, double dt, int ls, int u, int uhat, int v, int h, int out);
+/* GetUHat (comp 0, :950) / GetVHat (comp 1, :1231)(ls, rhs, h) with time step
+ * dt -> out: the implicit viscous step, one tridiagonal solve per r line and
+ * per z line; only the interior faces of out are written (the rest 0, no
+ * ghost fill). */
+int asd2g_axi_hat(asd2g_session *s, int comp, double dt, int ls, int rhs, int h, int out);
+/* GetDivergence4Poisson (for_poisson = 1, :1980) or GetDivergence (0,
+ * :1996) of (u, v) -> div (0 outside the interior). */
+int asd2g_axi_divergence(asd2g_session *s, int u, int v, int div, int for_poisson);
+/* SolvePoisson's assembly (:1488-1916) from LS, KAPPA, H, DIV with time step
+ * dt into the session's system (then asd2g_solve_pressure solves it).
+ * recompute_kappa: the axisymmetric curvature and its P ghosts first (what
+ * SolvePoisson does when kWe is finite and nonzero).  Pressure sides:
+ * Neumann, axisym, wall (zero flux), Dirichlet, inlet, outlet, pressure (the
+ * constant); periodic is ASD2G_E_UNSUPPORTED.  The Krylov solvers store each
+ * face coefficient once (from its east / north cell); the reference's west
+ * and south entries of a face crossed by the interface differ from those by
+ * rounding (the two cells interpolate the face radius in different orders). */
+int asd2g_axi_assemble(asd2g_session *s, double dt, int recompute_kappa);
+/* UpdateDt(U, V) with max |KAPPA| in the surface-tension bound, :2104. */
+int asd2g_axi_update_dt(asd2g_session *s, double *dt);
+/* One step of the axisymmetric driver (tests/LargeTests/test_mac2d_large.cpp
+ * :1264-1306): lsB = LS; advect and reinitialise LS (reinit_mode) with the
+ * level-set solver's own P-grid kinds ls_bc[4] and constants ls_bcc[4] (NULL:
+ * the session's pressure kinds); curvature; H, HS; rhs_u, uhat (U fill);
+ * rhs_v, vhat (V fill); the r-weighted divergence; assembly; pressure solve
+ * (solver ASD2G_SOLVER_PCG .. ASD2G_SOLVER_MGPCG); projection; next dt.  FP64
+ * sessions only.  *dt is the step's dt and receives the next one. */
+int asd2g_axi_step(asd2g_session *s, double *dt, int reinit_mode, const int32_t *ls_bc, const double *ls_bcc,
+                   int solver, double tol, int maxit, int *iters, double *rel_resid);
+
 /* ---- GFM pressure (mac2d.cpp:1249-1727, poisson2d.cpp) ---- */
 /* Assemble the matrix-free GFM system from LS, KAPPA, H, DIV with time step
  * dt.  recompute_kappa: recompute KAPPA from LS and fill its P ghosts first
