@@ -104,6 +104,30 @@ def droplet(n: int = 256, seed: int = 0, rho_ratio: float = 1000.0, mu_ratio: fl
                 meta=dict(seed=seed, radius=r, centre=(cx, cy)))
 
 
+def axisym_bubble(nr: int = 64, nz: int = 128) -> Case:
+    """An air bubble at rest in water on the axisymmetric (r, z) grid, the
+    configuration of the reference's stationary-bubble driver
+    (test_mac2d_large.cpp:1346-1420, 0.02 x 0.04 m, R = 5 mm at z = 0.02 m):
+    density 1000 / 1.226, viscosity 1.137e-3 / 1.78e-5, sigma 0.0728, no
+    gravity; U/V axisym-wall-Neumann-Neumann, pressure axisym-wall-Neumann-
+    outlet, the level set's own sides axisym-lsfree-lsfree-lsfree
+    (meta["bc_ls"]).  x is r, y is z; phi > 0 is the water (heavy)."""
+    lr, lz, R, zc = 0.02, 0.04, 0.005, 0.02
+    dr, dz = lr / nr, lz / nz
+    r = (np.arange(nr + 6)[:, None] - 3 + 0.5) * dr
+    z = (np.arange(nz + 6)[None, :] - 3 + 0.5) * dz
+    ls = np.ascontiguousarray(np.sqrt(r ** 2 + (z - zc) ** 2) - R)
+    u = np.zeros_like(ls)
+    v = np.zeros_like(ls)
+    fluid = dict(rho_h=1000.0, rho_l=1.226, mu_h=1.137e-3, mu_l=1.78e-5, sigma=0.0728, g=0.0, g_axis=1,
+                 fix_gravity=0, time_order=0, cfl=0.5)
+    bu = ("axisym", "wall", "neumann", "neumann")
+    # the driver's first dt (cfl min(dr, dz) / U with U = 1; its UpdateDt of a fluid at rest is unbounded)
+    return Case(nr, nz, dr, dz, ls, u, v, dt=0.5 * min(dr, dz), bc_u=bu, bc_v=bu,
+                bc_p=("axisym", "wall", "neumann", "outlet"), fluid=fluid,
+                meta=dict(bc_ls=("axisym", "lsfree", "lsfree", "lsfree"), radius=R, centre=(0.0, zc)))
+
+
 def droplet_batch(count: int = 256, seed: int = 0, sides=tuple(range(64, 513, 32))) -> list:
     """Uneven batch: per-droplet grid side from ``sides``, radius in
     [0.08, 0.2], density ratio log-uniform in [1, 1000] and viscosity ratio

@@ -802,6 +802,82 @@ def full_steps_256(sh, stream, n=N_GRID, steps=20):
                                            out["fp64_mg_fcg_device_resident"]["ms_per_step"]}
 
 
+AXI_GRIDS = ((64, 128), (256, 512), (1024, 2048))
+
+
+def axisym_steps(sh, stream, grids=AXI_GRIDS, steps=10, cpu=True):
+    """The axisymmetric MAC step (asd2g_axi_step) on the stationary bubble of
+    the reference's axisymmetric driver, at its 64 x 128 grid and two finer
+    grids of the same domain: level set (WENO5 + MinRK2), curvature, the
+    implicit viscous uhat / vhat (a Thomas solve per grid line), the r-weighted
+    GFM assembly and the pressure solve to rel. residual 1e-10 with the FP64
+    Jacobi-PCG (the reference's method) or the MG-FCG; `steps` steps after 2
+    warm-up steps, CUDA events on the session's stream (each step ends with its
+    host read of dt).  CPU baseline: the oracle's restatement of the same step
+    (bit-exact to the reference function by function) at 64 x 128, one core."""
+    import torch
+    from asd2_b200 import api
+    from asd2_b200 import workloads as W
+    out = {}
+    for nr, nz in grids:
+        c = W.axisym_bubble(nr, nz)
+        res = {}
+        for name, solver in (("fp64_jacobi_pcg", api.PCG), ("fp64_mg_fcg", api.MGPCG)):
+            with api.Session(api.Params.from_case(c), stream=sh) as ss:
+                ss.upload("ls", c.ls)
+                ss.upload("u", c.u)
+                ss.upload("v", c.v)
+                dt = c.dt
+                for _ in range(2):
+                    r = ss.axi_step(dt, ls_bc=c.meta["bc_ls"], solver=solver, tol=1e-10, maxit=500000)
+                    dt = r["dt_next"]
+                ss.sync()
+                with torch.cuda.stream(stream):
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                its, ok = 0, True
+                for _ in range(steps):
+                    r = ss.axi_step(dt, ls_bc=c.meta["bc_ls"], solver=solver, tol=1e-10, maxit=500000)
+                    ok = ok and r["status"] == 0
+                    its += r["iters"]
+                    dt = r["dt_next"]
+                e1.record(stream)
+                e1.synchronize()
+                if not ok:
+                    raise SystemExit(f"bench: axisymmetric step {nr}x{nz} {name} failed")
+                t = e0.elapsed_time(e1) / 1e3
+                res[name] = {"steps_per_s": steps / t, "ms_per_step": 1e3 * t / steps,
+                             "pressure_iters_per_step": its / steps, "mcells_per_s": nr * nz * steps / t / 1e6}
+        out[f"{nr}x{nz}"] = res
+    rep = {"workload": f"axisymmetric stationary bubble (rho 1000 / 1.226, sigma 0.0728), {steps} steps after 2, "
+                       "pressure to rel. residual 1e-10", **out}
+    if cpu:
+        rep["cpu_baseline"] = axisym_cpu_baseline()
+        g0 = f"{grids[0][0]}x{grids[0][1]}"
+        rep["speedup_vs_cpu_" + g0] = out[g0]["fp64_mg_fcg"]["steps_per_s"] / rep["cpu_baseline"]["value"]
+    return rep
+
+
+def axisym_cpu_baseline(nr=64, nz=128, steps=5):
+    """CPU baseline of axisym_steps: the oracle's axisymmetric step, one core."""
+    from asd2_b200 import workloads as W
+    from oracle.pyoracle import FluidSpec, GridSpec, Oracle
+    O = Oracle()
+    c = W.axisym_bubble(nr, nz)
+    g = GridSpec(nr, nz, c.dx, c.dy, bc_u=c.bc_u, bc_v=c.bc_v, bc_p=c.bc_p)
+    lg = GridSpec(nr, nz, c.dx, c.dy, bc_u=c.bc_u, bc_v=c.bc_v, bc_p=c.meta["bc_ls"])
+    f = FluidSpec(**c.fluid)
+    st = dict(ls=c.ls.copy(), u=c.u.copy(), v=c.v.copy(), kappa=np.zeros_like(c.ls), dt=c.dt)
+    O.axi_step(g, f, st, ls_grid=lg, tol=1e-10)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        O.axi_step(g, f, st, ls_grid=lg, tol=1e-10)
+    t = time.perf_counter() - t0
+    return {"value": steps / t, "unit": "axisymmetric steps/s", "cores": 1, "kind": "port",
+            "sample": f"{steps} steps of the {nr}x{nz} bubble after 1, pressure by the oracle's FP64 Jacobi-PCG "
+                      "to 1e-10"}
+
+
 def run_ours(args):
     import torch
     from asd2_b200 import api
@@ -979,6 +1055,7 @@ def run_ours(args):
                if not args.no_extra else None)
     bsteps = batched_steps(sh, stream) if not args.no_extra else None
     fsteps = full_steps_256(sh, stream) if not args.no_extra else None
+    axi = axisym_steps(sh, stream, cpu=rank == 0 and not args.no_cpu) if not args.no_extra else None
     if one_launch:
         # per solve: dt, curvature, P ghost fill, k_assemble; dt, solver scalars, k_mgfcg_persist, ps and p
         launches = 9 * args.steps
@@ -1032,6 +1109,7 @@ def run_ours(args):
         "learned_pc_512": learned,
         "batched_steps_256": bsteps,
         "full_steps_256": fsteps,
+        "axisym_steps": axi,
         "e2e_overlapped": e2e_overlapped,
         "e2e": {"value": e2e_value, "unit": "GFM Poisson solves/s",
                 "h2d_bytes_per_step": 3 * G * 8, "d2h_bytes_per_step": G * 8},
@@ -1167,7 +1245,7 @@ def main():
                     help="droplets of the batched sections (default 256; smaller for profiling)")
     ap.add_argument("--section", default=None,
                     choices=["ls_large", "mixed_1024", "batched", "batched_steps", "learned_pc", "unet_forward",
-                             "full_steps", "stencils"],
+                             "full_steps", "stencils", "axisym"],
                     help="run only this report (its JSON object on stdout), e.g. to profile it")
     args = ap.parse_args()
     if args.section:
@@ -1206,6 +1284,8 @@ def run_section(name, args):
                                 else STENCIL_GRID)
     elif name == "full_steps":
         out = full_steps_256(stream.cuda_stream, stream)
+    elif name == "axisym":
+        out = axisym_steps(stream.cuda_stream, stream, cpu=not args.no_cpu)
     elif name == "batched_steps":
         out = batched_steps(stream.cuda_stream, stream, count=args.batch_count)
     elif name == "unet_forward":
