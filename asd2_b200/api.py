@@ -78,7 +78,8 @@ EXPORTS = [
     "asd2g_unet_train_step_residual", "asd2g_unet_train_step_energy",
     "asd2g_unet_error_flag", "asd2g_unet_set_stream", "asd2g_set_preconditioner_net", "asd2g_last_fallback",
     "asd2g_last_solve_one_launch",
-    "asd2g_axi_kappa", "asd2g_axi_rhs_u", "asd2g_axi_rhs_v", "asd2g_axi_hat", "asd2g_axi_divergence",
+    "asd2g_axi_kappa", "asd2g_axi_rhs_u", "asd2g_axi_rhs_v", "asd2g_axi_viscosity", "asd2g_axi_hat",
+    "asd2g_axi_divergence",
     "asd2g_axi_assemble", "asd2g_axi_update_dt", "asd2g_axi_step",
     "asd2g_pc_training_pair", "asd2g_pc_training_pair_at",
 ]
@@ -135,6 +136,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "asd2g_apply_bc_side": ([S, I, C.c_char, I, I], I), "asd2g_update_ntk": ([S, I, I, I], I),
         "asd2g_axi_kappa": ([S], I), "asd2g_axi_rhs_u": ([S, D, I, I, I, I, I], I),
         "asd2g_axi_rhs_v": ([S, D, I, I, I, I, I, I], I), "asd2g_axi_hat": ([S, I, D, I, I, I, I], I),
+        "asd2g_axi_viscosity": ([S, I, I, I, I, I, I, I], I),
         "asd2g_axi_divergence": ([S, I, I, I, I], I), "asd2g_axi_assemble": ([S, D, I], I),
         "asd2g_axi_update_dt": ([S, C.POINTER(D)], I),
         "asd2g_axi_step": ([S, C.POINTER(D), I, C.c_void_p, C.c_void_p, I, D, I, C.POINTER(I), C.POINTER(D)], I),
@@ -452,6 +454,9 @@ class Session:
 
     def axi_rhs_v(self, dt, ls="ls", u="u", uhat="uhat", v="v", h="HS", out="w0"):
         self._check(self.L.asd2g_axi_rhs_v(self.h, dt, *(self._f(x) for x in (ls, u, uhat, v, h, out))))
+
+    def axi_viscosity(self, ls="ls", u="u", uhat="uhat", v="v", h="HS", du="w0", dv="w1"):
+        self._check(self.L.asd2g_axi_viscosity(self.h, *(self._f(x) for x in (ls, u, uhat, v, h, du, dv))))
 
     def axi_hat(self, comp, dt, ls="ls", rhs="w0", h="HS", out=None):
         """GetUHat (comp 0) / GetVHat (comp 1) into out (default uhat / vhat)."""

@@ -1560,13 +1560,27 @@ int asd2g_axi_rhs_v(asd2g_session *s, double dt, int ls, int u, int uhat, int v,
     return rc ? rc : axi_rhs(s, 1, ls, u, v, uhat, h, out);
 }
 
+int asd2g_axi_viscosity(asd2g_session *s, int ls, int u, int uhat, int v, int h, int du, int dv) {
+    if (!s || !valid_field(ls) || !valid_field(u) || !valid_field(uhat) || !valid_field(v) || !valid_field(h) ||
+        !valid_field(du) || !valid_field(dv) || du == dv)
+        return fail(ASD2G_E_ARG, "bad field");
+    for (int in : {ls, u, uhat, v, h})
+        if (in == du || in == dv) return fail(ASD2G_E_ARG, "outputs must differ from the inputs");
+    const Grid &g = s->g;
+    launch_axi_rhs_u(g, s->M, s->f[ls], s->f[u], s->f[v], s->f[h], s->f[du], s->dsc, s->f[du], s->st, 1);
+    launch_axi_rhs_v(g, s->M, s->f[ls], s->f[u], s->f[uhat], s->f[v], s->f[h], s->f[dv], s->dsc, s->f[dv], s->st,
+                     1);
+    return cuda_check("axi_viscosity");
+}
+
 int asd2g_axi_hat(asd2g_session *s, int comp, double dt, int ls, int rhs, int h, int out) {
     if (!s || (comp != 0 && comp != 1) || !valid_field(ls) || !valid_field(rhs) || !valid_field(h) ||
         !valid_field(out) || out == ls || out == rhs || out == h)
         return fail(ASD2G_E_ARG, "bad field or component");
     int rc = set_dt(s, dt);
     if (rc) return rc;
-    launch_axi_hat(s->g, s->M, comp, s->f[ls], s->f[rhs], s->f[h], s->dsc, s->f[out], s->ub, s->vb, s->va, s->st);
+    double *const w[6] = {s->ua, s->va, s->ub, s->vb, s->w1, s->w2};
+    launch_axi_hat(s->g, s->M, comp, s->f[ls], s->f[rhs], s->f[h], s->dsc, s->f[out], w, s->st);
     return cuda_check("axi_hat");
 }
 
@@ -1641,13 +1655,15 @@ int asd2g_axi_step(asd2g_session *s, double *dt, int reinit_mode, const int32_t 
     launch_heaviside(g, ls, s->f[ASD2G_H], HS, s->st);
     rc = axi_rhs(s, 0, ASD2G_LS, ASD2G_U, ASD2G_V, -1, ASD2G_HS, ASD2G_W0);
     if (rc) return rc;
-    launch_axi_hat(g, s->M, 0, ls, s->f[ASD2G_W0], HS, s->dsc, uh, s->ub, s->vb, s->va, s->st);
+    double *const w[6] = {s->ua, s->va, s->ub, s->vb, s->w1, s->w2};
+    launch_axi_hat(g, s->M, 0, ls, s->f[ASD2G_W0], HS, s->dsc, uh, w, s->st);
     launch_fill_uv(g, uh, nullptr, s->st);
     rc = axi_rhs(s, 1, ASD2G_LS, ASD2G_U, ASD2G_V, ASD2G_UHAT, ASD2G_HS, ASD2G_W0);
     if (rc) return rc;
-    launch_axi_hat(g, s->M, 1, ls, s->f[ASD2G_W0], HS, s->dsc, vh, s->ub, s->vb, s->va, s->st);
+    launch_axi_hat(g, s->M, 1, ls, s->f[ASD2G_W0], HS, s->dsc, vh, w, s->st);
     launch_fill_uv(g, nullptr, vh, s->st);
     launch_axi_div(g, 1, uh, vh, s->f[ASD2G_DIV], s->st);
+    launch_fill_p(gl, ls, s->st);  // the driver fills the level set again before the solve (:1294)
     axi_assemble_enqueue(s, axi_we_finite(s));
     rc = cuda_check("axi_step (before the solve)");
     if (rc) return rc;
@@ -1655,7 +1671,12 @@ int asd2g_axi_step(asd2g_session *s, double *dt, int reinit_mode, const int32_t 
     const int st = solve(s, solver, tol, maxit, iters, rel_resid);
     if (st < 0) return st;
     launch_scatter_ps(g, s->x, s->f[ASD2G_PS], s->f[ASD2G_P], s->dsc, s->st);
+    // The driver repeats the fills that SolvePoisson and UpdateVel end with
+    // (:1299, :1304-1305); with a Neumann side next to a Dirichlet one a
+    // second fill changes the corner ghosts, so it is repeated here too.
+    launch_fill_p(g, s->f[ASD2G_PS], s->st);
     launch_update_vel(g, s->M, uh, vh, s->f[ASD2G_PS], ls, s->f[ASD2G_H], s->f[ASD2G_KAPPA], u, v, s->dsc, s->st);
+    launch_fill_uv(g, u, v, s->st);
     launch_axi_update_dt(g, s->M, u, v, s->f[ASD2G_KAPPA], s->partial, s->counter, s->dsc + 1, s->st);
     cudaMemcpyAsync(s->dsc_host, s->dsc, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
     rc = sync(s);

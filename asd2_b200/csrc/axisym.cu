@@ -94,10 +94,12 @@ __global__ void k_axi_kappa(Grid g, double base_r, double lim, const double *__r
 // ----------------------------------------------------------- right sides --
 // GetRHSU (mac2dAxisym.cpp:264-292) over the whole padded array: interior u
 // faces get u + dt (-cU + gU + vU) with the viscous term of
-// AddExternalViscosityFU (:590-753) computed here, every other entry 0.
+// AddExternalViscosityFU (:590-753) computed here, every other entry 0
+// (visc_only: the viscous term alone, AddExternalViscosityFU itself).
 __global__ void k_axi_rhs_u(Grid g, MomConst M, const double *__restrict__ ls, const double *__restrict__ u,
                             const double *__restrict__ v, const double *__restrict__ H,
-                            const double *__restrict__ cU, const double *__restrict__ dtp, double *__restrict__ out) {
+                            const double *__restrict__ cU, const double *__restrict__ dtp, int visc_only,
+                            double *__restrict__ out) {
     const int j = blockIdx.x * TJ + threadIdx.x, i = blockIdx.y * TI + threadIdx.y;
     if (i >= g.sx || j >= g.sy) return;
     const int64_t c = IX(g, i, j);
@@ -114,7 +116,7 @@ __global__ void k_axi_rhs_u(Grid g, MomConst M, const double *__restrict__ ls, c
         const double visZ = (muN * (v[Nn] - v[WN]) / g.dx - muS * (v[c] - v[W]) / g.dx) / g.dy;
         vU = visZ / rho_face(M, lsS, lsN);
     }
-    out[c] = u[c] + *dtp * (-cU[c] + M.gu + vU);
+    out[c] = visc_only ? vU : u[c] + *dtp * (-cU[c] + M.gu + vU);
 }
 
 // GetRHSV (mac2dAxisym.cpp:294-322) with AddExternalViscosityFV (:755-910):
@@ -124,7 +126,7 @@ __global__ void k_axi_rhs_u(Grid g, MomConst M, const double *__restrict__ ls, c
 __global__ void k_axi_rhs_v(Grid g, MomConst M, const double *__restrict__ ls, const double *__restrict__ u,
                             const double *__restrict__ uhat, const double *__restrict__ v,
                             const double *__restrict__ H, const double *__restrict__ cV,
-                            const double *__restrict__ dtp, double *__restrict__ out) {
+                            const double *__restrict__ dtp, int visc_only, double *__restrict__ out) {
     const int j = blockIdx.x * TJ + threadIdx.x, i = blockIdx.y * TI + threadIdx.y;
     if (i >= g.sx || j >= g.sy) return;
     const int64_t c = IX(g, i, j);
@@ -145,37 +147,26 @@ __global__ void k_axi_rhs_v(Grid g, MomConst M, const double *__restrict__ ls, c
         vV = visR / rho_face(M, lsVW, lsVE) + visZ / rho_face(M, ls[S], ls[c]);
     }
     const double gV = (M.gv_from_u && i < NB + 1) ? 0.0 : M.gv;
-    out[c] = v[c] + *dtp * (-cV[c] + gV + vV);
+    out[c] = visc_only ? vV : v[c] + *dtp * (-cV[c] + gV + vV);
 }
 
 // ------------------------------------------------------ implicit viscous --
 // GetUHat / GetVHat (mac2dAxisym.cpp:950-1229, :1231-1478): per grid line a
-// tridiagonal system lo x[k-1] + di x[k] + up x[k+1] = d, solved by one
-// thread in the elimination order of SolveTDMA (:2255-2306): forward sweep
-// storing the scaled upper diagonal and right side, back substitution.  The
-// r lines of one launch read and write a row j each (a warp covers 32
-// consecutive j: coalesced); the z lines walk j within a column.  The end
-// rows take the configured U / V kinds and constants (raw BC2D values).
+// tridiagonal system lo x[k-1] + di x[k] + up x[k+1] = d, solved in the
+// elimination order of SolveTDMA (:2255-2306): scale the first row, pivot
+// di - lo up', back-substitute.  Bit-exact parity needs that serial
+// recurrence per line, so the work is split: fully parallel kernels compute
+// every row's coefficients and end-row edits (raw U / V kinds, Grid bu / bv)
+// into line-ordered arrays, then one thread per line runs only the
+// recurrence, streaming its four arrays with the next row prefetched.  The
+// r lines use the padded layout (line = j, consecutive threads read
+// consecutive j); the z lines a transposed copy (element (i, j) at i + sx j)
+// so that their reads are coalesced too.
 struct Tri {
     double lo, di, up, d;
 };
 
-// One step of the forward sweep at position k of a line of n unknowns.
-__device__ __forceinline__ void thomas_fwd(int k, int n, Tri t, double &up_prev, double &x_prev, double *up_out,
-                                           double *x_out) {
-    if (k == 0) {
-        up_prev = t.up / t.di;
-        x_prev = t.d / t.di;
-    } else {
-        const double piv = t.di - t.lo * up_prev;
-        up_prev = (k < n - 1) ? t.up / piv : t.up;
-        x_prev = (t.d - t.lo * x_prev) / piv;
-    }
-    *up_out = up_prev;
-    *x_out = x_prev;
-}
-
-// End-row edits of a line: which = 0 the first row (lo dropped), 1 the last
+// End-row edits of a line: first = the first row (lo dropped), else the last
 // (up dropped).  neu: the kind folds the dropped entry into the diagonal;
 // dir: it moves scale * constant to the right side; per: the other end's
 // right side value.
@@ -199,141 +190,235 @@ __device__ __forceinline__ bool k_neu3(int b) { return b == 1 || b == 3 /*AXISYM
 __device__ __forceinline__ bool k_dir3(int b) { return b == 2 /*DIRICHLET*/ || b == 5 /*INLET*/ || b == 4 /*WALL*/; }
 __device__ __forceinline__ bool k_dir4(int b) { return k_dir3(b) || b == 3; }
 
-// u, r lines: faces i = 4 .. nx+2 of row j; result (the r-solved field) in xr.
-__global__ void k_axi_u_rlines(Grid g, MomConst M, const double *__restrict__ ls, const double *__restrict__ rhs,
-                               const double *__restrict__ H, const double *__restrict__ dtp, double *__restrict__ upw,
-                               double *__restrict__ xr) {
-    const int jj = blockIdx.x * blockDim.x + threadIdx.x;
-    if (jj >= g.ny) return;
-    const int J = jj + NB, m = g.nx - 1;
-    const double dr = g.dx, dt = *dtp;
-    double up_prev = 0.0, x_prev = 0.0;
-    for (int k = 0; k < m; k++) {
-        const int I = k + NB + 1;
-        const int64_t c = IX(g, I, J), w = IX(g, I - 1, J);
-        const double rUM = (k + 1.0) * dr, rPW = (k + 0.5) * dr, rPM = (k + 1.5) * dr;
-        const double muW = mu_of(M, H, w), muM = mu_of(M, H, c);
-        const double rho = rho_mix(M, heavy_frac(ls[w], ls[c]));
-        Tri t;
-        t.d = rhs[c];
-        t.lo = -dt / (rho * rUM) * (2.0 * rPW * muW) / (dr * dr);
-        t.di = 1.0 + dt / (rho * rUM) * 2.0 * (rPW * muW + rPM * muM) / (dr * dr);
-        t.up = -dt / (rho * rUM) * (2.0 * rPM * muM) / (dr * dr);
-        if (k == 0)
-            end_row(t, true, k_neu2(g.bu[0]), k_dir4(g.bu[0]), g.bu[0] == 0, 1.0, g.cu[0], rhs[IX(g, m + NB, J)]);
-        if (k == m - 1)
-            end_row(t, false, k_neu2(g.bu[1]), k_dir4(g.bu[1]), g.bu[1] == 0, 1.0, g.cu[1], rhs[IX(g, NB + 1, J)]);
-        thomas_fwd(k, m, t, up_prev, x_prev, upw + c, xr + c);
-    }
-    for (int k = m - 2; k >= 0; k--) {
-        const int64_t c = IX(g, k + NB + 1, J);
-        x_prev = xr[c] - upw[c] * x_prev;
-        xr[c] = x_prev;
-    }
+// transposed (z-line) position of cell (i, j)
+__device__ __forceinline__ int64_t TX(const Grid &g, int i, int j) { return (int64_t)i + (int64_t)g.sx * j; }
+
+__device__ __forceinline__ void store_tri(const Tri &t, int64_t a, double *lo, double *di, double *up, double *d) {
+    lo[a] = t.lo;
+    di[a] = t.di;
+    up[a] = t.up;
+    d[a] = t.d;
 }
 
-// u, z lines of column i (faces i = 4 .. nx+2), then the 1/r^2 term:
-// uhat = x / (1 + dt / rho (mu_W + mu_M) / r^2).
-__global__ void k_axi_u_zlines(Grid g, MomConst M, const double *__restrict__ ls, const double *__restrict__ H,
-                               const double *__restrict__ dtp, const double *__restrict__ xr, double *__restrict__ upw,
-                               double *__restrict__ xz, double *__restrict__ uhat) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= g.nx - 1) return;
-    const int I = k + NB + 1, n = g.ny;
+// u, r lines: faces i = 4 .. nx+2 of every row j (k = i - 4, m = nx - 1 rows).
+__global__ void k_axi_coef_u_r(Grid g, MomConst M, const double *__restrict__ ls, const double *__restrict__ rhs,
+                               const double *__restrict__ H, const double *__restrict__ dtp, double *lo, double *di,
+                               double *up, double *d) {
+    const int J = NB + blockIdx.x * TJ + threadIdx.x, I = NB + 1 + blockIdx.y * TI + threadIdx.y;
+    if (J >= g.ny + NB || I >= g.nx + NB) return;
+    const int k = I - NB - 1, m = g.nx - 1;
+    const double dr = g.dx, dt = *dtp;
+    const int64_t c = IX(g, I, J), w = IX(g, I - 1, J);
+    const double rUM = (k + 1.0) * dr, rPW = (k + 0.5) * dr, rPM = (k + 1.5) * dr;
+    const double muW = mu_of(M, H, w), muM = mu_of(M, H, c);
+    const double rho = rho_mix(M, heavy_frac(ls[w], ls[c]));
+    Tri t;
+    t.d = rhs[c];
+    t.lo = -dt / (rho * rUM) * (2.0 * rPW * muW) / (dr * dr);
+    t.di = 1.0 + dt / (rho * rUM) * 2.0 * (rPW * muW + rPM * muM) / (dr * dr);
+    t.up = -dt / (rho * rUM) * (2.0 * rPM * muM) / (dr * dr);
+    if (k == 0)
+        end_row(t, true, k_neu2(g.bu[0]), k_dir4(g.bu[0]), g.bu[0] == 0, 1.0, g.cu[0], rhs[IX(g, m + NB, J)]);
+    if (k == m - 1)
+        end_row(t, false, k_neu2(g.bu[1]), k_dir4(g.bu[1]), g.bu[1] == 0, 1.0, g.cu[1], rhs[IX(g, NB + 1, J)]);
+    store_tri(t, c, lo, di, up, d);
+}
+
+// u, z lines of every column i (rows j = 3 .. ny+2) from the r-solved field
+// xr, transposed; den = 1 + dt / rho (mu_W + mu_M) / r^2, the 1/r^2 term.
+__global__ void k_axi_coef_u_z(Grid g, MomConst M, const double *__restrict__ ls, const double *__restrict__ H,
+                               const double *__restrict__ dtp, const double *__restrict__ xr, double *lo, double *di,
+                               double *up, double *d, double *den) {
+    const int J = NB + blockIdx.x * TJ + threadIdx.x, I = NB + 1 + blockIdx.y * TI + threadIdx.y;
+    if (J >= g.ny + NB || I >= g.nx + NB) return;
+    const int jj = J - NB, n = g.ny;
     const double dz = g.dy, dt = *dtp;
-    double up_prev = 0.0, x_prev = 0.0;
-    for (int jj = 0; jj < n; jj++) {
-        const int J = jj + NB;
-        const int64_t c = IX(g, I, J), W = IX(g, I - 1, J), S = IX(g, I, J - 1), WS = IX(g, I - 1, J - 1),
-                      Nn = IX(g, I, J + 1), WN = IX(g, I - 1, J + 1);
-        const double lsS = quarter(ls, c, W, WS, S), lsN = quarter(ls, c, W, WN, Nn);
-        const double muS = quarter_mu(M, H, c, W, WS, S), muN = quarter_mu(M, H, c, W, WN, Nn);
-        const double rho = rho_mix(M, heavy_frac(lsS, lsN));
-        Tri t;
-        t.d = xr[c];
-        t.lo = -dt / rho * muS / (dz * dz);
-        t.di = 1.0 + dt / rho * (muS + muN) / (dz * dz);
-        t.up = -dt / rho * muN / (dz * dz);
-        if (jj == 0)
-            end_row(t, true, k_neu3(g.bu[2]), k_dir3(g.bu[2]), g.bu[2] == 0, 2.0, g.cu[2], xr[IX(g, I, n - 1 + NB)]);
-        if (jj == n - 1)
-            end_row(t, false, k_neu3(g.bu[3]), k_dir3(g.bu[3]), g.bu[3] == 0, 2.0, g.cu[3], xr[IX(g, I, NB)]);
-        thomas_fwd(jj, n, t, up_prev, x_prev, upw + c, xz + c);
-    }
+    const int64_t c = IX(g, I, J), W = IX(g, I - 1, J), S = IX(g, I, J - 1), WS = IX(g, I - 1, J - 1),
+                  Nn = IX(g, I, J + 1), WN = IX(g, I - 1, J + 1);
+    const double lsS = quarter(ls, c, W, WS, S), lsN = quarter(ls, c, W, WN, Nn);
+    const double muS = quarter_mu(M, H, c, W, WS, S), muN = quarter_mu(M, H, c, W, WN, Nn);
+    const double rho = rho_mix(M, heavy_frac(lsS, lsN));
+    Tri t;
+    t.d = xr[c];
+    t.lo = -dt / rho * muS / (dz * dz);
+    t.di = 1.0 + dt / rho * (muS + muN) / (dz * dz);
+    t.up = -dt / rho * muN / (dz * dz);
+    if (jj == 0)
+        end_row(t, true, k_neu3(g.bu[2]), k_dir3(g.bu[2]), g.bu[2] == 0, 2.0, g.cu[2], xr[IX(g, I, n - 1 + NB)]);
+    if (jj == n - 1)
+        end_row(t, false, k_neu3(g.bu[3]), k_dir3(g.bu[3]), g.bu[3] == 0, 2.0, g.cu[3], xr[IX(g, I, NB)]);
+    const int64_t a = TX(g, I, J);
+    store_tri(t, a, lo, di, up, d);
     const double rUM = (I - NB) * g.dx;
-    for (int jj = n - 1; jj >= 0; jj--) {
-        const int J = jj + NB;
-        const int64_t c = IX(g, I, J), w = IX(g, I - 1, J);
-        if (jj < n - 1) x_prev = xz[c] - upw[c] * x_prev;
-        const double rho = rho_mix(M, heavy_frac(ls[w], ls[c]));
-        uhat[c] = x_prev / (1.0 + dt / rho * (mu_of(M, H, w) + mu_of(M, H, c)) / (rUM * rUM));
-    }
+    const double rhoWE = rho_mix(M, heavy_frac(ls[W], ls[c]));
+    den[a] = 1.0 + dt / rhoWE * (mu_of(M, H, W) + mu_of(M, H, c)) / (rUM * rUM);
 }
 
 // v, r lines: cells i = 3 .. nx+2 of v-row j (j = 4 .. ny+2).
-__global__ void k_axi_v_rlines(Grid g, MomConst M, const double *__restrict__ ls, const double *__restrict__ rhs,
-                               const double *__restrict__ H, const double *__restrict__ dtp, double *__restrict__ upw,
-                               double *__restrict__ xr) {
-    const int jj = blockIdx.x * blockDim.x + threadIdx.x;
-    if (jj >= g.ny - 1) return;
-    const int J = jj + NB + 1, n = g.nx;
+__global__ void k_axi_coef_v_r(Grid g, MomConst M, const double *__restrict__ ls, const double *__restrict__ rhs,
+                               const double *__restrict__ H, const double *__restrict__ dtp, double *lo, double *di,
+                               double *up, double *d) {
+    const int J = NB + 1 + blockIdx.x * TJ + threadIdx.x, I = NB + blockIdx.y * TI + threadIdx.y;
+    if (J >= g.ny + NB || I >= g.nx + NB) return;
+    const int k = I - NB, n = g.nx;
     const double dr = g.dx, dt = *dtp;
-    double up_prev = 0.0, x_prev = 0.0;
-    for (int k = 0; k < n; k++) {
-        const int I = k + NB;
-        const int64_t c = IX(g, I, J), W = IX(g, I - 1, J), E = IX(g, I + 1, J), S = IX(g, I, J - 1),
-                      WS = IX(g, I - 1, J - 1), ES = IX(g, I + 1, J - 1);
-        const double rVM = (k + 0.5) * dr, rVW = k * dr, rVE = (k + 1.0) * dr;
-        const double lsVW = quarter(ls, c, W, S, WS), lsVE = quarter(ls, c, E, S, ES);
-        const double muVW = quarter_mu(M, H, c, W, S, WS), muVE = quarter_mu(M, H, c, E, S, ES);
-        const double rho = rho_mix(M, heavy_frac(lsVW, lsVE));
-        Tri t;
-        t.d = rhs[c];
-        t.lo = -dt / (rho * rVM) * rVW * muVW / (dr * dr);
-        t.di = 1.0 + dt / (rho * rVM) * (rVW * muVW + rVE * muVE) / (dr * dr);
-        t.up = -dt / (rho * rVM) * rVE * muVE / (dr * dr);
-        if (k == 0)
-            end_row(t, true, k_neu3(g.bv[0]), k_dir3(g.bv[0]), g.bv[0] == 0, 2.0, g.cv[0], rhs[IX(g, n - 1 + NB, J)]);
-        if (k == n - 1)
-            end_row(t, false, k_neu3(g.bv[1]), k_dir3(g.bv[1]), g.bv[1] == 0, 2.0, g.cv[1], rhs[IX(g, NB, J)]);
-        thomas_fwd(k, n, t, up_prev, x_prev, upw + c, xr + c);
-    }
-    for (int k = n - 2; k >= 0; k--) {
-        const int64_t c = IX(g, k + NB, J);
-        x_prev = xr[c] - upw[c] * x_prev;
-        xr[c] = x_prev;
-    }
+    const int64_t c = IX(g, I, J), W = IX(g, I - 1, J), E = IX(g, I + 1, J), S = IX(g, I, J - 1),
+                  WS = IX(g, I - 1, J - 1), ES = IX(g, I + 1, J - 1);
+    const double rVM = (k + 0.5) * dr, rVW = k * dr, rVE = (k + 1.0) * dr;
+    const double lsVW = quarter(ls, c, W, S, WS), lsVE = quarter(ls, c, E, S, ES);
+    const double muVW = quarter_mu(M, H, c, W, S, WS), muVE = quarter_mu(M, H, c, E, S, ES);
+    const double rho = rho_mix(M, heavy_frac(lsVW, lsVE));
+    Tri t;
+    t.d = rhs[c];
+    t.lo = -dt / (rho * rVM) * rVW * muVW / (dr * dr);
+    t.di = 1.0 + dt / (rho * rVM) * (rVW * muVW + rVE * muVE) / (dr * dr);
+    t.up = -dt / (rho * rVM) * rVE * muVE / (dr * dr);
+    if (k == 0)
+        end_row(t, true, k_neu3(g.bv[0]), k_dir3(g.bv[0]), g.bv[0] == 0, 2.0, g.cv[0], rhs[IX(g, n - 1 + NB, J)]);
+    if (k == n - 1)
+        end_row(t, false, k_neu3(g.bv[1]), k_dir3(g.bv[1]), g.bv[1] == 0, 2.0, g.cv[1], rhs[IX(g, NB, J)]);
+    store_tri(t, c, lo, di, up, d);
 }
 
-// v, z lines of column i (v faces j = 4 .. ny+2) into vhat.
-__global__ void k_axi_v_zlines(Grid g, MomConst M, const double *__restrict__ ls, const double *__restrict__ H,
-                               const double *__restrict__ dtp, const double *__restrict__ xr, double *__restrict__ upw,
-                               double *__restrict__ xz, double *__restrict__ vhat) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= g.nx) return;
-    const int I = k + NB, n = g.ny - 1;
+// v, z lines of every column i (v faces j = 4 .. ny+2), transposed.
+__global__ void k_axi_coef_v_z(Grid g, MomConst M, const double *__restrict__ ls, const double *__restrict__ H,
+                               const double *__restrict__ dtp, const double *__restrict__ xr, double *lo, double *di,
+                               double *up, double *d) {
+    const int J = NB + 1 + blockIdx.x * TJ + threadIdx.x, I = NB + blockIdx.y * TI + threadIdx.y;
+    if (J >= g.ny + NB || I >= g.nx + NB) return;
+    const int jj = J - NB - 1, n = g.ny - 1;
     const double dz = g.dy, dt = *dtp;
+    const int64_t c = IX(g, I, J), S = IX(g, I, J - 1);
+    const double muS = mu_of(M, H, S), muM = mu_of(M, H, c);
+    const double rho = rho_mix(M, heavy_frac(ls[S], ls[c]));
+    Tri t;
+    t.d = xr[c];
+    t.lo = -dt / rho * (2.0 * muS) / (dz * dz);
+    t.di = 1.0 + dt / rho * 2.0 * (muS + muM) / (dz * dz);
+    t.up = -dt / rho * (2.0 * muM) / (dz * dz);
+    if (jj == 0)
+        end_row(t, true, k_neu2(g.bv[2]), k_dir4(g.bv[2]), g.bv[2] == 0, 1.0, g.cv[2], xr[IX(g, I, n - 1 + NB + 1)]);
+    if (jj == n - 1)
+        end_row(t, false, k_neu2(g.bv[3]), k_dir4(g.bv[3]), g.bv[3] == 0, 1.0, g.cv[3], xr[IX(g, I, NB + 1)]);
+    store_tri(t, TX(g, I, J), lo, di, up, d);
+}
+
+// Element (line l, row k) of a line-ordered array: base + l * ls + k * ks.
+struct LineMap {
+    int64_t base, ls, ks;
+};
+
+// The recurrence of one line per thread (n >= 2 rows): the forward sweep
+// overwrites up with the scaled upper diagonal and d with the scaled right
+// side, the back substitution leaves the solution in d, or, with out, writes
+// it there through O (divided by den when den is given).  The rows are read
+// TP ahead into a register ring (the loads of row k + TP are issued before row
+// k's divisions), since one row's dependent chain is far shorter than a load
+// from L2 or HBM.
+constexpr int TP = 8;
+
+// Rows further ahead than the register ring are pulled into L1 with a
+// prefetch hint PF rows ahead (the ring alone covers 8 rows of the dependent
+// chain, less than an L2 round trip).
+constexpr int PF = 32;
+__device__ __forceinline__ void pf_l1(const void *p) { asm volatile("prefetch.L1 [%0];" ::"l"(p)); }
+
+// a / b with the IEEE result, taking the quotient of a zero numerator as the
+// product (a signed zero, sign(a) xor sign(b), for finite nonzero b): where
+// the fluid is at rest most right sides are exactly 0, and the division
+// sequence leaves its fast path for a zero quotient.
+__device__ __forceinline__ double qdiv(double a, double b) { return a == 0.0 ? a * b : a / b; }
+
+__global__ void __launch_bounds__(64) k_axi_thomas(int nlines, int n, LineMap A, const double *__restrict__ lo,
+                                                   const double *__restrict__ di, double *__restrict__ up,
+                                                   double *__restrict__ d, LineMap O, double *__restrict__ out,
+                                                   const double *__restrict__ den) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nlines) return;
+    const int64_t a0 = A.base + (int64_t)l * A.ls, ks = A.ks;
+    double rlo[TP], rdi[TP], rup[TP], rd[TP];
+#pragma unroll
+    for (int q = 0; q < TP; q++)
+        if (q < n) {
+            const int64_t a = a0 + (int64_t)q * ks;
+            rlo[q] = lo[a];
+            rdi[q] = di[a];
+            rup[q] = up[a];
+            rd[q] = d[a];
+        }
     double up_prev = 0.0, x_prev = 0.0;
-    for (int jj = 0; jj < n; jj++) {
-        const int J = jj + NB + 1;
-        const int64_t c = IX(g, I, J), S = IX(g, I, J - 1);
-        const double muS = mu_of(M, H, S), muM = mu_of(M, H, c);
-        const double rho = rho_mix(M, heavy_frac(ls[S], ls[c]));
-        Tri t;
-        t.d = xr[c];
-        t.lo = -dt / rho * (2.0 * muS) / (dz * dz);
-        t.di = 1.0 + dt / rho * 2.0 * (muS + muM) / (dz * dz);
-        t.up = -dt / rho * (2.0 * muM) / (dz * dz);
-        if (jj == 0)
-            end_row(t, true, k_neu2(g.bv[2]), k_dir4(g.bv[2]), g.bv[2] == 0, 1.0, g.cv[2], xr[IX(g, I, n - 1 + NB + 1)]);
-        if (jj == n - 1)
-            end_row(t, false, k_neu2(g.bv[3]), k_dir4(g.bv[3]), g.bv[3] == 0, 1.0, g.cv[3], xr[IX(g, I, NB + 1)]);
-        thomas_fwd(jj, n, t, up_prev, x_prev, upw + c, xz + c);
+    for (int k0 = 0; k0 < n; k0 += TP) {
+#pragma unroll
+        for (int q = 0; q < TP; q++) {
+            const int k = k0 + q;
+            if (k < n) {
+                const double clo = rlo[q], cdi = rdi[q], cup = rup[q], cd = rd[q];
+                if (k + TP < n) {
+                    const int64_t a = a0 + (int64_t)(k + TP) * ks;
+                    rlo[q] = lo[a];
+                    rdi[q] = di[a];
+                    rup[q] = up[a];
+                    rd[q] = d[a];
+                }
+                if (k + PF < n) {
+                    const int64_t a = a0 + (int64_t)(k + PF) * ks;
+                    pf_l1(lo + a);
+                    pf_l1(di + a);
+                    pf_l1(up + a);
+                    pf_l1(d + a);
+                }
+                if (k == 0) {
+                    up_prev = qdiv(cup, cdi);
+                    x_prev = qdiv(cd, cdi);
+                } else {
+                    const double piv = cdi - clo * up_prev;
+                    up_prev = (k < n - 1) ? qdiv(cup, piv) : cup;
+                    x_prev = qdiv(cd - clo * x_prev, piv);
+                }
+                const int64_t a = a0 + (int64_t)k * ks;
+                up[a] = up_prev;
+                d[a] = x_prev;
+            }
+        }
     }
-    for (int jj = n - 1; jj >= 0; jj--) {
-        const int64_t c = IX(g, I, jj + NB + 1);
-        if (jj < n - 1) x_prev = xz[c] - upw[c] * x_prev;
-        vhat[c] = x_prev;
+    // back substitution, rows n-2 .. 0, again TP rows ahead
+    const int64_t o0 = out ? O.base + (int64_t)l * O.ls : 0;
+    auto emit = [&](int k, int64_t a, double x) {
+        if (out) out[o0 + (int64_t)k * O.ks] = den ? qdiv(x, den[a]) : x;
+        else d[a] = x;
+    };
+    emit(n - 1, a0 + (int64_t)(n - 1) * ks, x_prev);
+    double bup[TP], bd[TP];
+#pragma unroll
+    for (int q = 0; q < TP; q++) {
+        const int k = n - 2 - q;
+        if (k >= 0) {
+            const int64_t a = a0 + (int64_t)k * ks;
+            bup[q] = up[a];
+            bd[q] = d[a];
+        }
+    }
+    for (int k0 = n - 2; k0 >= 0; k0 -= TP) {
+#pragma unroll
+        for (int q = 0; q < TP; q++) {
+            const int k = k0 - q;
+            if (k >= 0) {
+                const double cup = bup[q], cd = bd[q];
+                if (k - TP >= 0) {
+                    const int64_t a = a0 + (int64_t)(k - TP) * ks;
+                    bup[q] = up[a];
+                    bd[q] = d[a];
+                }
+                if (k - PF >= 0) {
+                    const int64_t a = a0 + (int64_t)(k - PF) * ks;
+                    pf_l1(up + a);
+                    pf_l1(d + a);
+                    if (den) pf_l1(den + a);
+                }
+                x_prev = cd - cup * x_prev;
+                emit(k, a0 + (int64_t)k * ks, x_prev);
+            }
+        }
     }
 }
 
@@ -504,30 +589,48 @@ void launch_axi_kappa(const Grid &g, const double *ls, double *kappa, cudaStream
 static dim3 padded_grid(const Grid &g) { return dim3((g.sy + TJ - 1) / TJ, (g.sx + TI - 1) / TI); }
 
 void launch_axi_rhs_u(const Grid &g, const MomConst &M, const double *ls, const double *u, const double *v,
-                      const double *H, const double *cU, const double *dtp, double *out, cudaStream_t st) {
-    k_axi_rhs_u<<<padded_grid(g), dim3(TJ, TI), 0, st>>>(g, M, ls, u, v, H, cU, dtp, out);
+                      const double *H, const double *cU, const double *dtp, double *out, cudaStream_t st,
+                      int visc_only) {
+    k_axi_rhs_u<<<padded_grid(g), dim3(TJ, TI), 0, st>>>(g, M, ls, u, v, H, cU, dtp, visc_only, out);
 }
 
 void launch_axi_rhs_v(const Grid &g, const MomConst &M, const double *ls, const double *u, const double *uhat,
                       const double *v, const double *H, const double *cV, const double *dtp, double *out,
-                      cudaStream_t st) {
-    k_axi_rhs_v<<<padded_grid(g), dim3(TJ, TI), 0, st>>>(g, M, ls, u, uhat, v, H, cV, dtp, out);
+                      cudaStream_t st, int visc_only) {
+    k_axi_rhs_v<<<padded_grid(g), dim3(TJ, TI), 0, st>>>(g, M, ls, u, uhat, v, H, cV, dtp, visc_only, out);
 }
 
-// The implicit step of one velocity component: r lines (into w0, with w1 the
-// scaled upper diagonals), z lines (w2 their right sides) into out.  out is
-// zeroed first: only its interior faces are written, as in the reference.
+// The implicit step of one velocity component into out (zeroed first: only
+// its interior faces are written, as in the reference).  w[0..5]: six padded
+// scratch arrays (coefficients lo, di, up, the r-line right sides and
+// solution, the z-line right sides, the 1/r^2 denominators).
 void launch_axi_hat(const Grid &g, const MomConst &M, int comp, const double *ls, const double *rhs,
-                    const double *H, const double *dtp, double *out, double *w0, double *w1, double *w2,
-                    cudaStream_t st) {
-    constexpr int T = 128;
-    cudaMemsetAsync(out, 0, sizeof(double) * (size_t)g.sx * g.sy, st);
+                    const double *H, const double *dtp, double *out, double *const w[6], cudaStream_t st) {
+    constexpr int T = 64;
+    double *lo = w[0], *di = w[1], *up = w[2], *dr = w[3], *dz = w[4], *den = w[5];
+    const int64_t sx = g.sx, sy = g.sy;
+    cudaMemsetAsync(out, 0, sizeof(double) * (size_t)sx * sy, st);
+    const dim3 blk(TJ, TI);
     if (comp == 0) {
-        k_axi_u_rlines<<<(g.ny + T - 1) / T, T, 0, st>>>(g, M, ls, rhs, H, dtp, w1, w0);
-        k_axi_u_zlines<<<(g.nx - 1 + T - 1) / T, T, 0, st>>>(g, M, ls, H, dtp, w0, w1, w2, out);
+        const int m = g.nx - 1;
+        k_axi_coef_u_r<<<dim3((g.ny + TJ - 1) / TJ, (m + TI - 1) / TI), blk, 0, st>>>(g, M, ls, rhs, H, dtp, lo, di,
+                                                                                       up, dr);
+        k_axi_thomas<<<(g.ny + T - 1) / T, T, 0, st>>>(g.ny, m, LineMap{NB + sy * (NB + 1), 1, sy}, lo, di, up, dr,
+                                                       LineMap{0, 0, 0}, nullptr, nullptr);
+        k_axi_coef_u_z<<<dim3((g.ny + TJ - 1) / TJ, (m + TI - 1) / TI), blk, 0, st>>>(g, M, ls, H, dtp, dr, lo, di,
+                                                                                       up, dz, den);
+        k_axi_thomas<<<(m + T - 1) / T, T, 0, st>>>(m, g.ny, LineMap{(NB + 1) + sx * NB, 1, sx}, lo, di, up, dz,
+                                                    LineMap{NB + sy * (NB + 1), sy, 1}, out, den);
     } else {
-        k_axi_v_rlines<<<(g.ny - 1 + T - 1) / T, T, 0, st>>>(g, M, ls, rhs, H, dtp, w1, w0);
-        k_axi_v_zlines<<<(g.nx + T - 1) / T, T, 0, st>>>(g, M, ls, H, dtp, w0, w1, w2, out);
+        const int m = g.ny - 1;
+        k_axi_coef_v_r<<<dim3((m + TJ - 1) / TJ, (g.nx + TI - 1) / TI), blk, 0, st>>>(g, M, ls, rhs, H, dtp, lo, di,
+                                                                                        up, dr);
+        k_axi_thomas<<<(m + T - 1) / T, T, 0, st>>>(m, g.nx, LineMap{(NB + 1) + sy * NB, 1, sy}, lo, di, up, dr,
+                                                    LineMap{0, 0, 0}, nullptr, nullptr);
+        k_axi_coef_v_z<<<dim3((m + TJ - 1) / TJ, (g.nx + TI - 1) / TI), blk, 0, st>>>(g, M, ls, H, dtp, dr, lo, di,
+                                                                                        up, dz);
+        k_axi_thomas<<<(g.nx + T - 1) / T, T, 0, st>>>(g.nx, m, LineMap{NB + sx * (NB + 1), 1, sx}, lo, di, up, dz,
+                                                       LineMap{(NB + 1) + sy * NB, sy, 1}, out, nullptr);
     }
 }
 

@@ -39,13 +39,13 @@ void launch_ntk(const Grid &g, const double *ls, const double *absg, double *nxo
 // axisym.cu: the axisymmetric MAC step (MACSolver2DAxisym); x is r, y is z
 void launch_axi_kappa(const Grid &g, const double *ls, double *kappa, cudaStream_t st);
 void launch_axi_rhs_u(const Grid &g, const MomConst &M, const double *ls, const double *u, const double *v,
-                      const double *H, const double *cU, const double *dtp, double *out, cudaStream_t st);
+                      const double *H, const double *cU, const double *dtp, double *out, cudaStream_t st,
+                      int visc_only = 0);
 void launch_axi_rhs_v(const Grid &g, const MomConst &M, const double *ls, const double *u, const double *uhat,
                       const double *v, const double *H, const double *cV, const double *dtp, double *out,
-                      cudaStream_t st);
+                      cudaStream_t st, int visc_only = 0);
 void launch_axi_hat(const Grid &g, const MomConst &M, int comp, const double *ls, const double *rhs,
-                    const double *H, const double *dtp, double *out, double *w0, double *w1, double *w2,
-                    cudaStream_t st);
+                    const double *H, const double *dtp, double *out, double *const w[6], cudaStream_t st);
 void launch_axi_div(const Grid &g, int for_poisson, const double *u, const double *v, double *div, cudaStream_t st);
 void launch_axi_update_dt(const Grid &g, const MomConst &M, const double *u, const double *v, const double *kappa,
                           double *partial, unsigned *counter, double *dt_out, cudaStream_t st);

@@ -11,6 +11,7 @@
 
 using asd2g_dropin::report;
 using asd2g_dropin::SessionCache;
+using asd2g_dropin::write_zone;
 
 MACSolver2D::MACSolver2D(double Re, double We, double Fr, GAXISENUM2D GAxis, double L, double U, double sigma,
                          double densityRatio, double viscosityRatio, double rhoH, double muH, int nx, int ny,
@@ -362,38 +363,6 @@ int MACSolver2D::SetPLTType(PLTTYPE type) {
     return 0;
 }
 
-namespace {
-// One Tecplot ASCII zone (point packing, x fastest) of the cell-centred
-// interior: a zone line, then per cell "x,y,c0,c1,c2" with the values
-// formatted as an ostream's default double output (%g, 6 significant digits).
-bool write_zone(const std::string &path, bool header, const char *title, const char *vars, int iter, double t,
-                int nx, int ny, int nbc, double base_x, double base_y, double dx, double dy,
-                const std::vector<const std::vector<double> *> &cols) {
-    std::FILE *f = std::fopen(path.c_str(), header ? "w" : "a");
-    if (!f) return false;
-    if (header) std::fprintf(f, "TITLE = %s\nVARIABLES = %s \n", title, vars);
-    std::fprintf(f, "ZONE T=\"%d\", I=%d, J=%d, SOLUTIONTIME=%g, STRANDID=%d\n", iter, nx, ny, t, iter + 1);
-    const int64_t stride = ny + 2 * nbc;
-    std::string line;
-    char num[40];
-    for (int j = nbc; j < ny + nbc; j++)
-        for (int i = nbc; i < nx + nbc; i++) {
-            const int64_t k = j + stride * i;
-            line.clear();
-            std::snprintf(num, sizeof num, "%g", base_x + static_cast<double>(i + 0.5 - nbc) * dx);
-            line += num;
-            std::snprintf(num, sizeof num, ",%g", base_y + static_cast<double>(j + 0.5 - nbc) * dy);
-            line += num;
-            for (const std::vector<double> *c : cols) {
-                std::snprintf(num, sizeof num, ",%g", (*c)[k]);
-                line += num;
-            }
-            line += '\n';
-            std::fputs(line.c_str(), f);
-        }
-    return std::fclose(f) == 0;
-}
-}  // namespace
 
 // Tecplot ASCII output (mac2d.cpp:1990-2063): <vel>_ASCII.plt with X, Y, the
 // face velocities averaged to the cell centres, LS and PS; <div>_ASCII.plt

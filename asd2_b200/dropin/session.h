@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "asd2g.h"
@@ -30,6 +31,13 @@ struct SessionCache {
     void up(int field, const std::vector<double> &v);
     void down(int field, std::vector<double> &v);
 };
+
+// One Tecplot ASCII zone of OutRes (mac2d.cpp:1990-2063, mac2dAxisym.cpp:2323-
+// 2397): the cell-centred interior, x fastest, "x,y,c0,c1,..." per cell with
+// an ostream's default double format; header (TITLE / VARIABLES) when asked.
+bool write_zone(const std::string &path, bool header, const char *title, const char *vars, int iter, double t,
+                int nx, int ny, int nbc, double base_x, double base_y, double dx, double dy,
+                const std::vector<const std::vector<double> *> &cols);
 
 // Report a failed call the way the reference reports errors: a message; for
 // a non-finite value, exit(1) as the reference does on NaN/Inf.

@@ -13,6 +13,7 @@
  *   MACSolver2D        include/mac2d.h:31-168
  *   PoissonSolver2D    include/poisson2d.h:31-61
  *   BoundaryCondition2D include/bc2d.h:20-127
+ *   MACSolver2DAxisym  include/mac2dAxisym.h:31-168 (the asd2g_axi_* functions)
  * The C++ classes with those exact signatures live in asd2_b200/dropin/ and
  * are implemented on top of these functions.
  */
@@ -113,7 +114,7 @@ typedef struct asd2g_params {
     int32_t nx, ny;          /* interior cells (>= 4 each) */
     int32_t nbc;             /* ghost layers: must be 3 (WENO5) */
     int32_t precision;       /* ASD2G_PRECISION_FP64 (the drop-in) or ASD2G_PRECISION_MIXED */
-    double base_x, base_y;   /* lower-left corner (only for bookkeeping) */
+    double base_x, base_y;   /* lower-left corner (base_x is kBaseR of the asd2g_axi_* functions) */
     double dx, dy;           /* cell sizes */
     int32_t bc_u[4], bc_v[4], bc_p[4];      /* asd2g_bc per side, order W, E, S, N */
     double bcc_u[4], bcc_v[4], bcc_p[4];    /* Dirichlet constants per side */
@@ -266,6 +267,10 @@ int asd2g_axi_kappa(asd2g_session *s);
 int asd2g_axi_rhs_u(asd2g_session *s, double dt, int ls, int u, int v, int h, int out);
 /* GetRHSV(ls, u, uhat, v, h) -> out (V ghost fill applied), :294. */
 int asd2g_axi_rhs_v(asd2g_session *s, double dt, int ls, int u, int uhat, int v, int h, int out);
+/* AddExternalViscosityFU(u, v, ls, h) -> du and AddExternalViscosityFV(u,
+ * uhat, v, ls, h) -> dv (:590, :755), whole padded arrays (0 off the
+ * interior faces, and everywhere when kRe <= 0). */
+int asd2g_axi_viscosity(asd2g_session *s, int ls, int u, int uhat, int v, int h, int du, int dv);
 /* GetUHat (comp 0, :950) / GetVHat (comp 1, :1231)(ls, rhs, h) with time step
  * dt -> out: the implicit viscous step, one tridiagonal solve per r line and
  * per z line; only the interior faces of out are written (the rest 0, no

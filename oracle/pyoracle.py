@@ -397,13 +397,14 @@ class Oracle:
     def axi_update_dt(self, g, f, u, v, kappa) -> float:
         return self.L.ora_axi_update_dt(C.byref(g.c()), C.byref(f.c()), u, v, kappa)
 
-    def axi_step(self, g, f, st, base_r=0.0, ls_grid=None, tol=1e-10, maxit=200000, reinit_mode=2):
+    def axi_step(self, g, f, st, base_r=0.0, ls_grid=None, tol=1e-10, maxit=200000, reinit_mode=2, pcg_mode=0):
         """One step of the reference's axisymmetric driver
         (tests/LargeTests/test_mac2d_large.cpp:1264-1303): level set advected
         and reinitialised on ``ls_grid`` (the level-set solver's boundary
         kinds; default g), curvature, Heaviside, the implicit viscous uhat and
         vhat, the r-weighted divergence, the assembly solved by the
-        fixed-order FP64 PCG to ``tol``, the projection and the next dt.
+        fixed-order FP64 PCG to ``tol`` (``pcg_mode`` 1: the reference's own CG
+        iteration), the projection and the next dt.
         ``st`` holds ls, u, v, kappa (padded) and dt; updated in place."""
         lg = g if ls_grid is None else ls_grid
         ls, u, v = st["ls"], st["u"], st["v"]
@@ -423,13 +424,17 @@ class Oracle:
         vh = self.axi_vhat(g, f, dt, ls, rhs_v, HS)
         self.bc(g, "v", vh)
         div = self.axi_div4p(g, base_r, uh, vh)
+        self.bc(lg, "p", ls)  # the driver fills the level set again here (:1294)
         sysd = self.axi_assemble(g, f, base_r, dt, ls, st["kappa"], H, div, recompute_kappa=f.sigma != 0.0)
-        x, it, res, tres = self.pcg(g, sysd, tol=tol, maxit=maxit, mode=0)
+        x, it, res, tres = self.pcg(g, sysd, tol=tol, maxit=maxit, mode=pcg_mode)
         ps = g.zeros()
         self.scatter(g, x, ps)
-        self.bc(g, "p", ps)
+        self.bc(g, "p", ps)  # SolvePoisson's own fill
+        self.bc(g, "p", ps)  # and the driver's (:1299); with mixed kinds the corners differ after the second
         st["ps"] = ps
         self.update_vel(g, f, dt, u, v, uh, vh, ps, ls, H, st["kappa"])
+        self.bc(g, "u", u)  # the driver's fills after UpdateVel's own (:1304-1305)
+        self.bc(g, "v", v)
         st["dt_used"] = dt
         st["dt"] = self.axi_update_dt(g, f, u, v, st["kappa"])
         return dict(iters=it, resid=res, true_resid=tres, sys=sysd, div=div, H=H, HS=HS, uhat=uh, vhat=vh,
