@@ -476,8 +476,12 @@ int asd2g_batch_step(asd2g_batch *b, double *dt, int reinit_mode, double tol, in
                      double *rel_resid) {
     NvtxRange nv("asd2g_batch_step");
     if (!b || !dt || !(tol > 0.0) || maxit < 1) return api_fail(ASD2G_E_ARG, "batch_step: bad arguments");
-    if (reinit_mode != ASD2G_REINIT_ORIGINAL && reinit_mode != ASD2G_REINIT_MINRK2)
-        return api_fail(ASD2G_E_UNSUPPORTED, "batch_step implements reinit modes 0 (original) and 2 (MinRK2)");
+    if (reinit_mode < ASD2G_REINIT_ORIGINAL || reinit_mode > ASD2G_REINIT_MINRK2_SUSSMAN ||
+        reinit_mode == ASD2G_REINIT_FIRSTTIME)
+        return api_fail(ASD2G_E_UNSUPPORTED, "batch_step implements reinit modes 0, 1, 2 and 4");
+    const bool sussman = reinit_mode == ASD2G_REINIT_SUSSMAN || reinit_mode == ASD2G_REINIT_MINRK2_SUSSMAN;
+    if (sussman && b->splan.any_mixed)
+        return api_fail(ASD2G_E_UNSUPPORTED, "batch_step: mixed-precision instances implement reinit modes 0 and 2");
     // instances keep their own time order and reinitialisation step count:
     // the phases run up to the largest, instances without a phase skip it
     int steps = 0, omax = 0;
@@ -504,16 +508,21 @@ int asd2g_batch_step(asd2g_batch *b, double *dt, int reinit_mode, double tol, in
     launch_bstep_ls_stage(P, 2, BS_W1, BS_LS, BS_W2, st);
     launch_bstep_ls_stage(P, 3, BS_W2, BS_LS, BS_LS, st);
     // reinitialisation (levelset2d.cpp:264-316, :433-486): lsInit, then the pseudo-steps
-    if (reinit_mode == ASD2G_REINIT_MINRK2) {
+    if (reinit_mode == ASD2G_REINIT_MINRK2 || reinit_mode == ASD2G_REINIT_MINRK2_SUSSMAN) {
         launch_bstep_fill_p(P, BS_LS, false, st);
         cudaMemcpyAsync(slot(BS_LS0), slot(BS_LS), slot_bytes, cudaMemcpyDeviceToDevice, st);
     } else {
         cudaMemcpyAsync(slot(BS_LS0), slot(BS_LS), slot_bytes, cudaMemcpyDeviceToDevice, st);
         launch_bstep_fill_p(P, BS_LS, false, st);
     }
+    // the Sussman modes start from zeroed work arrays (levelset2d.cpp:329-331;
+    // their ghosts and corners stay 0): W1 (Sussman), W2 (both)
+    if (reinit_mode == ASD2G_REINIT_SUSSMAN) cudaMemsetAsync(slot(BS_W1), 0, slot_bytes, st);
+    if (sussman) cudaMemsetAsync(slot(BS_W2), 0, slot_bytes, st);
     for (int k = 0; k < steps; k++) {
-        launch_bstep_reinit_pass(P, reinit_mode, false, k, st);
-        launch_bstep_reinit_pass(P, reinit_mode, true, k, st);
+        launch_bstep_reinit_pass(P, reinit_mode, 0, k, st);
+        launch_bstep_reinit_pass(P, reinit_mode, 1, k, st);
+        if (sussman) launch_bstep_reinit_pass(P, reinit_mode, 2, k, st);
     }
     // mixed instances: the same level-set step in FP32 (a session's
     // launch_ls_step32: LS with its ghosts -> FP32, centred velocities, three

@@ -135,7 +135,8 @@ void launch_bstep_fill_p(const BStepPlan &P, int slot, bool kappa_only_if_flagge
 void launch_bstep_fill_uv(const BStepPlan &P, int su, int sv, cudaStream_t st, int min_order = 0);
 void launch_bstep_ls_stage(const BStepPlan &P, int stage, int in, int n, int out, cudaStream_t st);
 // pass a or b of pseudo-step k (instances with fewer pseudo-steps skip it)
-void launch_bstep_reinit_pass(const BStepPlan &P, int mode, bool pass_b, int k, cudaStream_t st);
+// pass 0: A (LS -> W1), 1: B (-> LS, or W2 for the Sussman modes), 2: C (the Sussman constraint -> LS)
+void launch_bstep_reinit_pass(const BStepPlan &P, int mode, int pass, int k, cudaStream_t st);
 // Mixed instances' FP32 level-set step (levelset32.cu, weno32.cu,
 // reinit32.cu): FP64 LS <-> FP32 phi (interior and ghosts), the FP32
 // centred velocities, one TVD-RK3 stage (arrays 0 phi, 2 a, 3 b), pass a or

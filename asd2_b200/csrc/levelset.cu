@@ -1,6 +1,8 @@
 // Level-set kernels in FP64 (the bit-exact path, built with -fmad=false):
 // the templated stencils of levelset_impl.cuh instantiated for double, the
 // reinitialisation driver and the building-block kernels of the ABI.
+#include <type_traits>
+
 #include "levelset_impl.cuh"
 #include "batch.cuh"
 
@@ -259,14 +261,21 @@ __global__ void __launch_bounds__(TJ *TI) k_bls_stage(const BInst *__restrict__ 
                                  bslot(I, out), I.sc, t.bx, t.by);
 }
 
-// LS1 = LS - adt S (|grad LS| - 1) into W1; LS = 0.5 (LS + LS2(W1)) (both with ghost mirrors)
+// One pseudo-step of every instance, as launch_reinit does for a session:
+// A: LS1 = LS - adt S (|grad LS| - 1) into W1 (the Sussman mode without its
+// ghost mirrors, W1's ghosts stay 0: levelset2d.cpp:336-340);
+// B: 0.5 (LS + LS2(W1)) into LS, or for the Sussman modes into W2 (the
+// session's third work array);
+// C (Sussman modes): LS = base + constraint(W2), base = LS (Sussman) or W2
+// (MinRK2 + Sussman).
 template <int MODE>
 __global__ void __launch_bounds__(TJ *TI) k_breinit_a(const BInst *__restrict__ insts, const BTile *__restrict__ tiles,
                                                       int k) {
     const BTile t = tiles[blockIdx.x];
     const BInst &I = insts[t.inst];
     if (k >= I.nreinit || I.mixed) return;
-    reinit_a_tile<MODE, double>(I.g, I.K, bslot(I, BS_LS), bslot(I, BS_LS0), bslot(I, BS_W1), 1, t.bx, t.by);
+    reinit_a_tile<MODE, double>(I.g, I.K, bslot(I, BS_LS), bslot(I, BS_LS0), bslot(I, BS_W1), MODE == RM_SUSS ? 0 : 1,
+                                t.bx, t.by);
 }
 template <int MODE>
 __global__ void __launch_bounds__(TJ *TI) k_breinit_b(const BInst *__restrict__ insts, const BTile *__restrict__ tiles,
@@ -274,8 +283,18 @@ __global__ void __launch_bounds__(TJ *TI) k_breinit_b(const BInst *__restrict__ 
     const BTile t = tiles[blockIdx.x];
     const BInst &I = insts[t.inst];
     if (k >= I.nreinit || I.mixed) return;
-    reinit_b_tile<MODE, double>(I.g, I.K, bslot(I, BS_W1), bslot(I, BS_LS0), bslot(I, BS_LS), bslot(I, BS_LS), 1,
-                                t.bx, t.by);
+    constexpr bool SUSS = MODE == RM_SUSS || MODE == RM_MINRK2_SUSS;
+    reinit_b_tile<MODE, double>(I.g, I.K, bslot(I, BS_W1), bslot(I, BS_LS0), bslot(I, BS_LS),
+                                bslot(I, SUSS ? BS_W2 : BS_LS), 1, t.bx, t.by);
+}
+template <int MODE>
+__global__ void __launch_bounds__(TJ *TI) k_breinit_c(const BInst *__restrict__ insts, const BTile *__restrict__ tiles,
+                                                      int k) {
+    const BTile t = tiles[blockIdx.x];
+    const BInst &I = insts[t.inst];
+    if (k >= I.nreinit || I.mixed) return;
+    reinit_c_tile<double>(I.g, I.K, bslot(I, BS_W2), bslot(I, BS_LS0), bslot(I, MODE == RM_SUSS ? BS_LS : BS_W2),
+                          bslot(I, BS_LS), 1, t.bx, t.by);
 }
 
 void launch_bstep_center_vel(const BStepPlan &P, cudaStream_t st) {
@@ -289,15 +308,18 @@ void launch_bstep_ls_stage(const BStepPlan &P, int stage, int in, int n, int out
     else k_bls_stage<3><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, in, n, out);
 }
 
-void launch_bstep_reinit_pass(const BStepPlan &P, int mode, bool pass_b, int k, cudaStream_t st) {
+void launch_bstep_reinit_pass(const BStepPlan &P, int mode, int pass, int k, cudaStream_t st) {
     const dim3 blk(TJ, TI);
-    if (mode == RM_ORIG) {
-        if (pass_b) k_breinit_b<RM_ORIG><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, k);
-        else k_breinit_a<RM_ORIG><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, k);
-    } else {
-        if (pass_b) k_breinit_b<RM_MINRK2><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, k);
-        else k_breinit_a<RM_MINRK2><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, k);
-    }
+    auto run = [&](auto m) {
+        constexpr int M = decltype(m)::value;
+        if (pass == 0) k_breinit_a<M><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, k);
+        else if (pass == 1) k_breinit_b<M><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, k);
+        else k_breinit_c<M><<<P.ntiles, blk, 0, st>>>(P.insts, P.tiles, k);
+    };
+    if (mode == RM_ORIG) run(std::integral_constant<int, RM_ORIG>{});
+    else if (mode == RM_SUSS) run(std::integral_constant<int, RM_SUSS>{});
+    else if (mode == RM_MINRK2) run(std::integral_constant<int, RM_MINRK2>{});
+    else run(std::integral_constant<int, RM_MINRK2_SUSS>{});
 }
 
 }  // namespace asd2g

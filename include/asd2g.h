@@ -360,8 +360,9 @@ int asd2g_batch_solve(asd2g_batch *b, double tol, int maxit, int *iters, double 
 int asd2g_batch_sync(asd2g_batch *b);
 /* The full droplet step of every instance (what asd2g_droplet_step does for
  * one session, with the MG-FCG pressure solve), one kernel launch per phase
- * for the whole batch: level-set advection, reinitialisation (reinit_mode 0
- * or 2), curvature, Heaviside, FP64 volume check, intermediate velocity,
+ * for the whole batch: level-set advection, reinitialisation (reinit_mode 0,
+ * 1, 2 or 4; 1 and 4 with FP64 instances only), curvature, Heaviside, FP64
+ * volume check, intermediate velocity,
  * divergence, GFM assembly, batched MG-FCG to tol, projection, next dt.
  * Instances: FP64 or mixed precision (the level-set advection and
  * reinitialisation in FP32, as asd2g_droplet_step of a mixed session does);

@@ -33,7 +33,8 @@ def _rel(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
-@pytest.mark.parametrize("reinit", [api.REINIT_MINRK2, api.REINIT_ORIGINAL])
+@pytest.mark.parametrize("reinit", [api.REINIT_MINRK2, api.REINIT_ORIGINAL, api.REINIT_SUSSMAN,
+                                    api.REINIT_MINRK2_SUSSMAN])
 def test_batch_step_matches_sessions(reinit):
     cases = [_case(k, nx, ny) for k, (nx, ny) in enumerate(SIDES)]
     sessions, init, dts = [], [], []
@@ -175,6 +176,6 @@ def test_batch_step_refusals():
     c, g, f = _case(0, 48, 48)
     with api.Batch([params_for(g, f)]) as b:
         with pytest.raises(api.Asd2gError):
-            b.step([1e-3], reinit_mode=api.REINIT_SUSSMAN)
+            b.step([1e-3], reinit_mode=api.REINIT_FIRSTTIME)
         with pytest.raises(api.Asd2gError):
             b.step([-1.0])
