@@ -78,3 +78,22 @@ def test_batch_refuses_periodic_pressure_before_device_work():
     with pytest.raises(api.Asd2gError) as e:
         api.Batch([ok, bad])
     assert e.value.code == -4
+
+
+def test_axisymmetric_entry_points_check_arguments_first():
+    """The asd2g_axi_* functions refuse a null session or a bad component
+    with ASD2G_E_ARG before any device work."""
+    L = api.load()
+    d = ctypes.c_double(1e-3)
+    assert L.asd2g_axi_kappa(None) == -1
+    assert L.asd2g_axi_rhs_u(None, 1e-3, 0, 1, 2, 7, 13) == -1
+    assert L.asd2g_axi_rhs_v(None, 1e-3, 0, 1, 9, 2, 7, 13) == -1
+    assert L.asd2g_axi_viscosity(None, 0, 1, 9, 2, 7, 13, 14) == -1
+    assert L.asd2g_axi_hat(None, 2, 1e-3, 0, 13, 7, 9) == -1
+    assert L.asd2g_axi_divergence(None, 9, 10, 8, 1) == -1
+    assert L.asd2g_axi_assemble(None, 1e-3, 1) == -1
+    assert L.asd2g_axi_update_dt(None, ctypes.byref(d)) == -1
+    it, res = ctypes.c_int(), ctypes.c_double()
+    assert L.asd2g_axi_step(None, ctypes.byref(d), 2, None, None, 0, 1e-10, 100, ctypes.byref(it),
+                            ctypes.byref(res)) == -1
+    assert b"null" in L.asd2g_last_error()
