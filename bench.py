@@ -61,13 +61,15 @@ MG_BYTES_PER_UNKNOWN_ITER = 180
 MG_ITER_DRAM_BYTES_256 = 913408
 # the same for the one-launch solve (k_mgfcg_persist): DRAM bytes read +
 # written by one launch (2.19008 MB + 13.3 KB, 15 iterations) divided by its
-# iterations, from the ncu capture summarised in profiles/mgfcg_persist_256.md
+# iterations, from one ncu capture of the 256^2 headline solve
 MG_PERSIST_DRAM_BYTES_PER_ITER_256 = 146893
 
 
+METRIC = "GFM Poisson solves/s @resid 1e-8: learned-PC mixed CG vs FP64 CG; LS Mcells/s"
+
+
 def metric_name():
-    with open(os.path.join(ROOT, "BASELINE.json")) as f:
-        return json.load(f)["metric"]
+    return METRIC
 
 
 def headline_config(n, world):
