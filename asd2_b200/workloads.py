@@ -104,6 +104,34 @@ def droplet(n: int = 256, seed: int = 0, rho_ratio: float = 1000.0, mu_ratio: fl
                 meta=dict(seed=seed, radius=r, centre=(cx, cy)))
 
 
+def zalesak(n: int = 100) -> Case:
+    """Zalesak's slotted disk in rigid rotation, the reference's level-set
+    driver (test_levelset2d_large.cpp:1339-1485): 100 x 100 cells of size 1,
+    disk of radius 15 at (50, 75) with a slot 7.5 wide reaching y = 82.5,
+    phi = +2 inside / -2 outside (0 on the circle), sampled at the cell
+    corners x = i, y = j; velocity (pi/314)(50 - y, x - 50) at the cell centres
+    of the whole padded grid; dt = 1 and 629 steps (one revolution takes
+    628); Neumann sides.  The reference reinitialises (Reinit_Original_2D)
+    before the first step and after every step."""
+    if n != 100:
+        raise ValueError("the reference's slotted disk is defined on 100 x 100 unit cells")
+    dx = dy = 1.0
+    I = np.arange(n + 6)[:, None]
+    J = np.arange(n + 6)[None, :]
+    xc, yc = (I + 0.5 - 3) * dx, (J + 0.5 - 3) * dy
+    u = np.ascontiguousarray(np.broadcast_to((np.pi / 314.0) * (50.0 - yc), (n + 6, n + 6)))
+    v = np.ascontiguousarray(np.broadcast_to((np.pi / 314.0) * (xc - 50.0), (n + 6, n + 6)))
+    x, y = (I - 3) * dx + 0.0 * J, (J - 3) * dy + 0.0 * I
+    d = np.sqrt((x - 50.0) ** 2 + (y - 75.0) ** 2) - 15.0
+    ls = np.where(d < 0, 2.0, np.where(d == 0, 0.0, -2.0))
+    ls[(x >= 50 - 0.25 * 15.0) & (x <= 50 + 0.25 * 15.0) & (y <= 75 + 7.5)] = -2.0
+    inner = np.zeros_like(ls, dtype=bool)
+    inner[3:-3, 3:-3] = True
+    ls = np.ascontiguousarray(np.where(inner, ls, -2.0))
+    return Case(n, n, dx, dy, ls, u, v, dt=1.0, steps=629, bc_u=("neumann",) * 4, bc_v=("neumann",) * 4,
+                bc_p=("neumann",) * 4, meta=dict(radius=15.0, centre=(50.0, 75.0), slot=7.5))
+
+
 def axisym_bubble(nr: int = 64, nz: int = 128) -> Case:
     """An air bubble at rest in water on the axisymmetric (r, z) grid, the
     configuration of the reference's stationary-bubble driver

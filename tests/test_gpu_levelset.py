@@ -183,3 +183,38 @@ def test_ls_step_graph_matches_separate_launches(mode):
                     s.reinit(mode)
             outs.append(s.download("ls"))
     assert np.array_equal(outs[0], outs[1])
+
+
+def test_zalesak_full_revolution():
+    """Zalesak's slotted disk (the reference's test_levelset2d_large.cpp:
+    1339-1485): 629 steps of dt = 1 (one revolution and one step), each
+    advection + Reinit_Original_2D, on the GPU against the oracle: the level
+    set bit-identical, so the reference's mass count (cells with phi > 0) and
+    its error norms against the initial field are the oracle's."""
+    from oracle.pyoracle import GridSpec
+    c = W.zalesak()
+    g = GridSpec(c.nx, c.ny, c.dx, c.dy, bc_u=c.bc_u, bc_v=c.bc_v, bc_p=c.bc_p)
+    a = c.ls.copy()
+    O.reinit(g, api.REINIT_ORIGINAL, a)
+    O.bc(g, "p", a)
+    a0 = a.copy()
+    p = api.Params(c.nx, c.ny, c.dx, c.dy, bc_u=c.bc_u, bc_v=c.bc_v, bc_p=c.bc_p)
+    with api.Session(p) as s:
+        s.upload("ls", c.ls)
+        s.upload("u", c.u)
+        s.upload("v", c.v)
+        s.reinit(api.REINIT_ORIGINAL)
+        s.apply_bc("ls", "P")
+        assert_bitexact(s.download("ls"), a0, "initial reinitialisation")
+        for _ in range(c.steps):
+            s.ls_step(c.dt, api.REINIT_ORIGINAL)
+        got = s.download("ls")
+    for _ in range(c.steps):
+        O.ls_advect(g, a, c.u, c.v, c.dt)
+        O.bc(g, "p", a)
+        O.reinit(g, api.REINIT_ORIGINAL, a)
+        O.bc(g, "p", a)
+    assert_bitexact(got[3:-3, 3:-3], a[3:-3, 3:-3], "slotted disk after one revolution")
+    err = np.abs(got - a0)[3:-3, 3:-3]
+    print(f"Zalesak: mass {(a0[3:-3, 3:-3] > 0).sum()} -> {(got[3:-3, 3:-3] > 0).sum()} cells; "
+          f"error norms inf {err.max():.4f}, L1 {err.sum() / err.size:.4f}, L2 {np.sqrt((err ** 2).mean()):.4f}")

@@ -233,3 +233,31 @@ def test_masks():
         for j in range(c.ny):
             if ff[i, j] & 1 and i > 0:
                 assert mm[i, j] or mm[i - 1, j]
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference build (oracle/_ref) not present")
+def test_zalesak_against_live_reference():
+    """Zalesak's slotted disk (test_levelset2d_large.cpp:1339-1485): the
+    initial Reinit_Original_2D and 60 steps of the driver's loop (advect,
+    fill, reinitialise, fill) agree bit for bit with the reference."""
+    from asd2_b200 import workloads as W
+    c = W.zalesak()
+    g = GridSpec(c.nx, c.ny, c.dx, c.dy, bc_u=c.bc_u, bc_v=c.bc_v, bc_p=c.bc_p)
+    R = Reference(g)
+    a, b = c.ls.copy(), c.ls.copy()
+    for arr, reinit, bc in ((a, lambda x: O.reinit(g, 0, x), lambda x: O.bc(g, "p", x)),
+                            (b, lambda x: R.reinit(0, x), lambda x: R.bc("p", x))):
+        reinit(arr)
+        bc(arr)
+    assert_bitexact(a, b, "initial reinitialisation")
+    for _ in range(60):
+        O.ls_advect(g, a, c.u, c.v, c.dt)
+        O.bc(g, "p", a)
+        O.reinit(g, 0, a)
+        O.bc(g, "p", a)
+        R.ls_advect(b, c.u, c.v, c.dt)
+        R.bc("p", b)
+        R.reinit(0, b)
+        R.bc("p", b)
+    assert_bitexact(a, b, "60 steps")
+    R.close()
