@@ -299,3 +299,64 @@ def test_upload_async_then_solve():
             assert r["status"] == 0
             out.append(s.download("ps"))
     assert np.array_equal(out[0], out[1])
+
+
+def test_cavity_flow_driver_matches_oracle():
+    """The reference's lid-driven cavity driver (test_mac2d_large.cpp:3-182):
+    128^2, one fluid (phi = 1, rho 1, mu 0.01, Re 100), no-slip walls with
+    the north lid at u = 1, all-Neumann pressure (the corrected pin), RK3,
+    CFL 0.3.  Each step as the driver writes it: sharp Heaviside, the
+    intermediate velocity with H, U/V fills, divergence, GFM assembly and
+    solve, projection, dt.  20 steps through the per-function ABI against
+    the oracle's same sequence: velocities and pressure within 1e-8 of their
+    maxima (the two solves sum in different orders), dt within 1e-9."""
+    n = 128
+    g = GridSpec(n, n, 1.0 / n, 1.0 / n, bc_u=("dirichlet",) * 4, bc_v=("dirichlet",) * 4, bc_p=("neumann",) * 4,
+                 cu=(0.0, 0.0, 0.0, 1.0))
+    f = FluidSpec(rho_h=1.0, rho_l=1.0, mu_h=0.01, mu_l=0.01, sigma=0.0, g=0.0, g_axis=1, time_order=2, cfl=0.3)
+    ls = np.ones(g.shape)
+    u, v = g.zeros(), g.zeros()
+    O.bc(g, "u", u)
+    O.bc(g, "v", v)
+    O.bc(g, "p", ls)
+    kappa = g.zeros()
+    dt = 0.3 * (1.0 / n) / 1.0
+    p = params_for(g, f)
+    with api.Session(p) as s:
+        for fld, a in (("ls", ls), ("u", u), ("v", v), ("kappa", kappa)):
+            s.upload(fld, a)
+        dt_gpu = dt
+        for k in range(20):
+            s.heaviside()
+            s.intermediate_vel(dt_gpu, h="H")
+            s.apply_bc("uhat", "U")
+            s.apply_bc("vhat", "V")
+            s.divergence()
+            s.assemble_gfm(dt_gpu, recompute_kappa=False)
+            r = s.solve_pressure(api.PCG, tol=1e-12, maxit=100000, dt=dt_gpu)
+            assert r["status"] == 0, r
+            s.update_vel(dt_gpu)
+            dt_gpu_next = s.update_dt()
+            # the oracle's step
+            H = O.heaviside(g, ls)
+            uh, vh = O.intermediate_vel(g, f, dt, ls, u, v, H)
+            O.bc(g, "u", uh)
+            O.bc(g, "v", vh)
+            div = O.divergence(g, uh, vh)
+            sysd = O.gfm_assemble(g, f, dt, ls, kappa, H, div, recompute_kappa=False)
+            x, it, res, tres = O.pcg(g, sysd, tol=1e-12, maxit=100000)
+            ps = g.zeros()
+            O.scatter(g, x, ps)
+            O.bc(g, "p", ps)
+            O.update_vel(g, f, dt, u, v, uh, vh, ps, ls, H, kappa)
+            dt_next = O.update_dt(g, f, u, v)
+            for name, ref in (("u", u), ("v", v), ("ps", ps)):
+                got = s.download(name)
+                assert_close(interior(got), interior(ref), 0.0, 1e-8 * max(np.abs(interior(ref)).max(), 1e-30),
+                             f"cavity {name} step {k}")
+            assert abs(dt_gpu_next - dt_next) <= 1e-9 * dt_next, (k, dt_gpu_next, dt_next)
+            dt = dt_gpu = dt_next
+            # both continue from the oracle's state so the comparison stays step-for-step
+            s.upload("u", u)
+            s.upload("v", v)
+    print(f"cavity: 20 steps, last dt {dt:.4e}, max |u| {np.abs(interior(u)).max():.3f}, PCG iterations {it}")
