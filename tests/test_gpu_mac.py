@@ -360,3 +360,84 @@ def test_cavity_flow_driver_matches_oracle():
             s.upload("u", u)
             s.upload("v", v)
     print(f"cavity: 20 steps, last dt {dt:.4e}, max |u| {np.abs(interior(u)).max():.3f}, PCG iterations {it}")
+
+
+def _driver_2d(name):
+    """Initial state and parameters of three more of the reference's 2D MAC
+    drivers (test_mac2d_large.cpp): the small and the large rising air
+    bubble (:572-762, :764-954) and the Rayleigh-Taylor interface
+    (:956-1143, with gravity on V by fix_gravity), after their initial
+    reinitialisation; (grid, fluid, state, reinitialisation mode)."""
+    import math
+    if name == "small_bubble":
+        nx, ny, bx, by, lx, ly, cfl, order, mode = 80, 120, -0.01, -0.01, 0.02, 0.03, 0.3, 2, 2
+        f = FluidSpec(rho_h=1000.0, rho_l=1.226, mu_h=1.137e-3, mu_l=1.78e-5, sigma=0.0728, g=9.81, g_axis=1,
+                      time_order=order, cfl=cfl)
+        radius, u_scale = 1.0 / 300.0, 1.0
+        bc = ("dirichlet",) * 4
+    elif name == "large_bubble":
+        nx, ny, bx, by, lx, ly, cfl, order, mode = 80, 120, -1.0, -1.0, 2.0, 3.0, 0.5, 1, 1
+        f = FluidSpec(rho_h=1000.0, rho_l=1.226, mu_h=1.137e-3, mu_l=1.78e-5, sigma=0.0728, g=9.81, g_axis=1,
+                      time_order=order, cfl=cfl)
+        radius, u_scale = 1.0 / 3.0, 1.0
+        bc = ("dirichlet",) * 4
+    else:  # Rayleigh-Taylor: the first MACSolver2D constructor's constants
+        nx, ny, bx, by, lx, ly, cfl, order, mode = 128, 512, -0.5, -2.0, 1.0, 4.0, 0.2, 2, 2
+        gc, L = 200.0, 1.0
+        U = L / math.sqrt(L / gc)
+        Re, Fr = 1000.0, U / math.sqrt(gc * L)
+        rho_h, mu_h = 3.0, 3.0 / Re * math.sqrt(L * L * L * 9.8)
+        rho_l, mu_l = 1.0, 1.0 / Re * math.sqrt(L * L * L * 9.8)
+        # as written the driver gets no gravity at all (V takes AddGravityFU, Q5),
+        # and nothing moves; the fix (fix_gravity) applies it to V
+        f = FluidSpec(rho_h=rho_h, rho_l=rho_h * (rho_l / rho_h), mu_h=mu_h, mu_l=mu_h * (mu_l / mu_h), sigma=0.0,
+                      g=Fr * L / (U * U), g_axis=1, fix_gravity=1, time_order=order, cfl=cfl)
+        u_scale = U
+        bc = ("neumann", "neumann", "dirichlet", "dirichlet")
+    dx, dy = lx / nx, ly / ny
+    g = GridSpec(nx, ny, dx, dy, bc_u=bc, bc_v=bc, bc_p=("neumann",) * 4)
+    x = bx + (np.arange(nx + 6)[:, None] - 3 + 0.5) * dx
+    y = by + (np.arange(ny + 6)[None, :] - 3 + 0.5) * dy
+    if name == "taylor":
+        ls = -y - 0.1 * np.cos(2.0 * np.pi * x)
+    else:
+        ls = np.sqrt(x * x + y * y) - radius
+    ls = np.ascontiguousarray(ls + 0.0 * x * y)
+    O.bc(g, "p", ls)
+    O.reinit(g, mode, ls)
+    O.bc(g, "p", ls)
+    st = dict(ls=ls, u=g.zeros(), v=g.zeros(), kappa=g.zeros(), ps=g.zeros(), p=g.zeros(),
+              dt=cfl * min(dx, dy) / u_scale)
+    return g, f, st, mode
+
+
+@pytest.mark.parametrize("name", ["small_bubble", "large_bubble", "taylor"])
+def test_reference_2d_drivers(name):
+    """Three steps of each driver through asd2g_droplet_step against the
+    oracle's droplet step (RK3 / RK2, MinRK2 / Sussman reinitialisation,
+    gravity, Neumann side walls for the Rayleigh-Taylor case), pressure to
+    1e-12: level set bit-identical after the first step except with the
+    Sussman constraint (cos), within 1e-10 of its max otherwise; velocities
+    and pressure within 1e-8 of their maxima; dt within 1e-9."""
+    g, f, st, mode = _driver_2d(name)
+    with api.Session(params_for(g, f)) as s:
+        for fld in ("ls", "u", "v"):
+            s.upload(fld, st[fld])
+        dt = st["dt"]
+        for k in range(3):
+            r = s.droplet_step(dt, reinit_mode=mode, tol=1e-12, maxit=200000)
+            assert r["status"] == 0, r
+            O.droplet_step(g, f, st, tol=1e-12, reinit_mode=mode)
+            gl = s.download("ls")
+            if k == 0 and mode != api.REINIT_SUSSMAN:
+                assert_bitexact(gl, st["ls"], f"{name} level set after step 0")
+            else:
+                assert_close(gl, st["ls"], 0.0, 1e-10 * np.abs(st["ls"]).max(), f"{name} level set step {k}")
+            for fld in ("u", "v"):
+                ref = st[fld]
+                assert_close(s.download(fld), ref, 0.0, 1e-8 * max(np.abs(ref).max(), 1e-30), f"{name} {fld} {k}")
+            ps_ref = st["ps"]
+            assert_close(interior(s.download("ps")), interior(ps_ref), 0.0, 1e-8 * max(np.abs(ps_ref).max(), 1e-30),
+                         f"{name} ps {k}")
+            assert abs(r["dt_next"] - st["dt"]) <= 1e-9 * st["dt"], (name, k, r["dt_next"], st["dt"])
+            dt = st["dt"]
