@@ -78,3 +78,30 @@ def bc_fixture(trial):
     cu, cv, cp = (tuple(float(x) for x in row) for row in G[f"BC{trial}_consts"])
     g = GridSpec(13, 9, 0.1, 0.125, bc_u=bu, bc_v=bv, bc_p=bp, cu=cu, cv=cv, cp=cp)
     return g, (lambda key: G[f"BC{trial}_{key}"])
+
+
+def reinit_driver_case(name):
+    """Initial fields of two of the reference's reinitialisation-only drivers
+    (test_levelset2d_large.cpp), 128^2 on [-2, 2]^2 with Neumann sides:
+    "kinks" (:1042, two overlapping unit circles 1.4 apart, the union's
+    distance with its kinks; max pseudo-time 80) and "minrk2_2" (:882, the
+    unit circle's distance times (x-1)^2 + (y-1)^2 + 0.1, far from a
+    distance function; max pseudo-time 2 max(nx, ny) = 256).  Returns
+    (grid, padded phi with zero ghosts, max pseudo-time)."""
+    n, L, base = 128, 4.0, -2.0
+    dx = L / n
+    g = GridSpec(n, n, dx, dx, bc_p=("neumann",) * 4)
+    i = np.arange(n + 6)[:, None]
+    j = np.arange(n + 6)[None, :]
+    x = base + (i - 3 + 0.5) * dx + 0.0 * j
+    y = base + (j - 3 + 0.5) * dx + 0.0 * i
+    if name == "kinks":
+        r, a = 1.0, 0.7
+        ls = np.minimum(np.sqrt((x + a) ** 2 + y * y) - r, np.sqrt((x - a) ** 2 + y * y) - r)
+        max_atime = 80.0
+    else:
+        ls = ((x - 1.0) ** 2 + (y - 1.0) ** 2 + 0.1) * (np.sqrt(x * x + y * y) - 1.0)
+        max_atime = 256.0
+    inner = np.zeros(ls.shape, dtype=bool)
+    inner[3:-3, 3:-3] = True
+    return g, np.ascontiguousarray(np.where(inner, ls, 0.0)), max_atime

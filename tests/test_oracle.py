@@ -261,3 +261,20 @@ def test_zalesak_against_live_reference():
         R.bc("p", b)
     assert_bitexact(a, b, "60 steps")
     R.close()
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference build (oracle/_ref) not present")
+def test_reinit_with_kinks_against_live_reference():
+    """The reference's kinks driver (test_levelset2d_large.cpp:1042): one
+    Reinit_MinRK2_2D over pseudo-time 80 (5120 pseudo-steps) of the union of
+    two circles, bit for bit."""
+    from tests.helpers import reinit_driver_case
+    g, ls, mt = reinit_driver_case("kinks")
+    a, b = ls.copy(), ls.copy()
+    O.bc(g, "p", a)
+    O.reinit(g, 2, a, mt)
+    R = Reference(g, ls_max_atime=mt)
+    R.bc("p", b)
+    R.reinit(2, b)
+    assert_bitexact(a, b, "kinks after 5120 pseudo-steps")
+    R.close()
