@@ -173,3 +173,62 @@ def test_axisym_step_mg_solver_and_errors():
     with api.Session(params_for(g, f, precision=api.PRECISION_MIXED)) as s:
         with pytest.raises(api.Asd2gError):
             s.axi_step(1e-3)
+
+
+def test_axisym_droplet_collision_driver():
+    """The reference's axisymmetric droplet-collision driver
+    (test_mac2d_large.cpp:1762-1960): 120 x 320 cells, two spheres of radius
+    150 um 3L apart on the axis approaching at +-U/2 (U = 1.4 m/s),
+    density 1000 / 1.226, surface tension, all-Neumann pressure (the
+    corrected pin), U/V axisym-Dirichlet-Neumann-Neumann, the level set's own
+    sides axisym-Neumann; the first MACSolver2DAxisym constructor's
+    constants (kRe, kWe finite, no gravity).  Three steps against the
+    oracle's restatement of the driver: level set within 1e-10, u, v, ps
+    within 1e-7 of their maxima, dt within 1e-10."""
+    L, U = 300 * 10e-6, 1.4
+    rho_h, mu_h, rho_l, mu_l, sigma = 1000.0, 1.137e-3, 1.226, 1.78e-5, 0.0728
+    nr, nz = 120, 320
+    lr, lz = L * 3.0, L * 8.0
+    base_z = -0.5 * lz
+    dr, dz = lr / nr, lz / nz
+    bu = ("axisym", "dirichlet", "neumann", "neumann")
+    g = GridSpec(nr, nz, dr, dz, bc_u=bu, bc_v=bu, bc_p=("neumann",) * 4)
+    lg = GridSpec(nr, nz, dr, dz, bc_u=bu, bc_v=bu, bc_p=("axisym", "neumann", "neumann", "neumann"))
+    f = FluidSpec(rho_h=rho_h, rho_l=rho_h * (rho_l / rho_h), mu_h=mu_h, mu_l=mu_h * (mu_l / mu_h), sigma=sigma,
+                  g=0.0, g_axis=1, cfl=0.1)
+    radius = 150 * 10e-6
+    r = (np.arange(nr + 6)[:, None] - 3 + 0.5) * dr
+    z = base_z + (np.arange(nz + 6)[None, :] - 3 + 0.5) * dz
+    d1 = np.sqrt(r * r + (z - L * 1.5) * (z - L * 1.5)) - radius
+    d2 = np.sqrt(r * r + (z + L * 1.5) * (z + L * 1.5)) - radius
+    inner = np.zeros((nr + 6, nz + 6), dtype=bool)
+    inner[3:-3, 3:-3] = True
+    v = np.where(inner & (d1 < 0), -U * 0.5, 0.0)
+    v = np.ascontiguousarray(np.where(inner & (d2 < 0), U * 0.5, v))
+    ls = np.ascontiguousarray(np.where(inner, np.minimum(d1, d2), 0.0))
+    u = g.zeros()
+    O.bc(lg, "p", ls)
+    O.reinit(lg, 2, ls)
+    O.bc(lg, "p", ls)
+    O.bc(g, "u", u)
+    O.bc(g, "v", v)
+    kappa = g.zeros()
+    st = dict(ls=ls, u=u, v=v, kappa=kappa, dt=O.axi_update_dt(g, f, u, v, kappa))
+    with session(g, f, 0.0) as s:
+        for fld in ("ls", "u", "v", "kappa"):
+            s.upload(fld, st[fld])
+        dt = st["dt"]
+        for k in range(3):
+            r_ = s.axi_step(dt, ls_bc=lg.bc_p, solver=api.PCG, tol=1e-12, maxit=200000)
+            assert r_["status"] == 0, r_
+            info = O.axi_step(g, f, st, ls_grid=lg, tol=1e-12)
+            assert abs(r_["dt_next"] - st["dt"]) <= 1e-10 * st["dt"], (k, r_["dt_next"], st["dt"])
+            for fld in ("ls", "u", "v", "ps"):
+                ref = st[fld]
+                err = np.abs(s.download(fld) - ref)[3:-3, 3:-3].max()
+                scale = max(np.abs(ref[3:-3, 3:-3]).max(), 1e-30)
+                bar = 1e-10 * scale if fld == "ls" else 1e-7 * scale
+                assert err <= bar, (k, fld, err, scale)
+            print(f"collision step {k}: PCG iterations GPU {r_['iters']} / oracle {info['iters']}, "
+                  f"dt {st['dt']:.3e}, max |v| {np.abs(st['v'][3:-3, 3:-3]).max():.3f}")
+            dt = st["dt"]
