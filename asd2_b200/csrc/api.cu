@@ -260,6 +260,13 @@ struct asd2g_session {
     // asd2g_droplet_step's phases before and after the solve, replayed as
     // graphs from the second call on (per reinitialisation mode / one)
     cudaGraphExec_t pre_exec[5] = {}, post_exec = nullptr;
+    // asd2g_axi_step's phases likewise; the pre-solve graphs hold the level
+    // set's boundary kinds of their capture (axi_ls_key) and are dropped
+    // when a call brings others
+    cudaGraphExec_t axi_pre_exec[5] = {}, axi_post_exec = nullptr;
+    int axi_pre_calls[5] = {}, axi_post_calls = 0;
+    int32_t axi_ls_key[4] = {-1, -1, -1, -1};
+    double axi_ls_cst[4] = {0.0, 0.0, 0.0, 0.0};
     int pre_calls[5] = {}, post_calls = 0;
     int run_reinit = -1, run_maxit = -1;
     double run_tol = -1.0;
@@ -487,6 +494,9 @@ int asd2g_destroy(asd2g_session *s) {
     for (auto &e : s->pre_exec)
         if (e) cudaGraphExecDestroy(e);
     if (s->post_exec) cudaGraphExecDestroy(s->post_exec);
+    for (auto &e : s->axi_pre_exec)
+        if (e) cudaGraphExecDestroy(e);
+    if (s->axi_post_exec) cudaGraphExecDestroy(s->axi_post_exec);
     for (cudaStream_t a : s->aux_st)
         if (a) cudaStreamDestroy(a);
     if (s->copy_st) {
@@ -1612,6 +1622,56 @@ int asd2g_axi_update_dt(asd2g_session *s, double *dt) {
     return ASD2G_OK;
 }
 
+// One step of the axisymmetric driver before its pressure solve (test_mac2d_
+// large.cpp:1269-1292): level set with the level set's own P grid gl,
+// curvature, Heaviside, right sides and the implicit viscous step of u and v,
+// the r-weighted divergence, the assembly.
+static int axi_step_pre(asd2g_session *s, const Grid &gl, int reinit_mode) {
+    const Grid &g = s->g;
+    double *ls = s->f[ASD2G_LS], *u = s->f[ASD2G_U], *v = s->f[ASD2G_V];
+    double *uh = s->f[ASD2G_UHAT], *vh = s->f[ASD2G_VHAT], *HS = s->f[ASD2G_HS];
+    cudaMemcpyAsync(s->f[ASD2G_LSB], ls, sizeof(double) * s->G, cudaMemcpyDeviceToDevice, s->st);
+    launch_center_vel(gl, u, v, s->tu, s->tv, s->st);
+    launch_fill_p(gl, ls, s->st);
+    launch_ls_stage(1, gl, ls, s->tu, s->tv, ls, s->w1, s->dsc, s->st);
+    launch_ls_stage(2, gl, s->w1, s->tu, s->tv, ls, s->w2, s->dsc, s->st);
+    launch_ls_stage(3, gl, s->w2, s->tu, s->tv, ls, ls, s->dsc, s->st);
+    launch_fill_p(gl, ls, s->st);
+    launch_reinit(gl, reinit_mode, s->prm.ls_max_atime, ls, s->f[ASD2G_LS0], s->w1, s->w2, s->w3, s->st);
+    launch_fill_p(gl, ls, s->st);
+    launch_axi_kappa(g, ls, s->f[ASD2G_KAPPA], s->st);
+    launch_heaviside(g, ls, s->f[ASD2G_H], HS, s->st);
+    int rc = axi_rhs(s, 0, ASD2G_LS, ASD2G_U, ASD2G_V, -1, ASD2G_HS, ASD2G_W0);
+    if (rc) return rc;
+    double *const w[6] = {s->ua, s->va, s->ub, s->vb, s->w1, s->w2};
+    launch_axi_hat(g, s->M, 0, ls, s->f[ASD2G_W0], HS, s->dsc, uh, w, s->st);
+    launch_fill_uv(g, uh, nullptr, s->st);
+    rc = axi_rhs(s, 1, ASD2G_LS, ASD2G_U, ASD2G_V, ASD2G_UHAT, ASD2G_HS, ASD2G_W0);
+    if (rc) return rc;
+    launch_axi_hat(g, s->M, 1, ls, s->f[ASD2G_W0], HS, s->dsc, vh, w, s->st);
+    launch_fill_uv(g, nullptr, vh, s->st);
+    launch_axi_div(g, 1, uh, vh, s->f[ASD2G_DIV], s->st);
+    launch_fill_p(gl, ls, s->st);  // the driver fills the level set again before the solve (:1294)
+    axi_assemble_enqueue(s, axi_we_finite(s));
+    return cuda_check("axi_step (before the solve)");
+}
+
+// After the solve (:1296-1306): ps and p, the projection, the next dt (dsc[1]).
+// The driver repeats the fills that SolvePoisson and UpdateVel end with
+// (:1299, :1304-1305); with a Neumann side next to a Dirichlet one a second
+// fill changes the corner ghosts, so it is repeated here too.
+static int axi_step_post(asd2g_session *s) {
+    const Grid &g = s->g;
+    double *u = s->f[ASD2G_U], *v = s->f[ASD2G_V];
+    launch_scatter_ps(g, s->x, s->f[ASD2G_PS], s->f[ASD2G_P], s->dsc, s->st);
+    launch_fill_p(g, s->f[ASD2G_PS], s->st);
+    launch_update_vel(g, s->M, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->f[ASD2G_PS], s->f[ASD2G_LS], s->f[ASD2G_H],
+                      s->f[ASD2G_KAPPA], u, v, s->dsc, s->st);
+    launch_fill_uv(g, u, v, s->st);
+    launch_axi_update_dt(g, s->M, u, v, s->f[ASD2G_KAPPA], s->partial, s->counter, s->dsc + 1, s->st);
+    return cuda_check("axi_step (after the solve)");
+}
+
 int asd2g_axi_step(asd2g_session *s, double *dt, int reinit_mode, const int32_t *ls_bc, const double *ls_bcc,
                    int solver, double tol, int maxit, int *iters, double *rel_resid) {
     NvtxRange nv("asd2g_axi_step");
@@ -1624,60 +1684,42 @@ int asd2g_axi_step(asd2g_session *s, double *dt, int reinit_mode, const int32_t 
     if (rc) return rc;
     // the level-set solver's own P-grid boundary (LevelSetSolver2D has its own BoundaryCondition2D)
     Grid gl = s->g;
+    int32_t key[4];
+    double cst[4];
+    for (int k = 0; k < 4; k++) {
+        key[k] = ls_bc ? ls_bc[k] : s->prm.bc_p[k];
+        cst[k] = ls_bc ? (ls_bcc ? ls_bcc[k] : 0.0) : s->prm.bcc_p[k];
+        if (key[k] < 0 || key[k] > 9) return fail(ASD2G_E_ARG, "level-set boundary kind out of range");
+    }
     if (ls_bc) {
         bool mirror = true;
         for (int k = 0; k < 4; k++) {
-            if (ls_bc[k] < 0 || ls_bc[k] > 9) return fail(ASD2G_E_ARG, "level-set boundary kind out of range");
-            gl.kp[k] = kind_p(ls_bc[k]);
-            gl.bp[k] = ls_bc[k];
-            gl.cp[k] = ls_bcc ? ls_bcc[k] : 0.0;
+            gl.kp[k] = kind_p(key[k]);
+            gl.bp[k] = key[k];
+            gl.cp[k] = cst[k];
             mirror &= (gl.kp[k] == K_NEU || gl.kp[k] == K_DIR);
         }
         gl.p_mirror = mirror ? 1 : 0;
     }
+    if (std::memcmp(key, s->axi_ls_key, sizeof key) != 0 || std::memcmp(cst, s->axi_ls_cst, sizeof cst) != 0) {
+        for (int m = 0; m < 5; m++) {  // graphs captured with other level-set kinds
+            if (s->axi_pre_exec[m]) cudaGraphExecDestroy(s->axi_pre_exec[m]);
+            s->axi_pre_exec[m] = nullptr;
+            s->axi_pre_calls[m] = 0;
+        }
+        std::memcpy(s->axi_ls_key, key, sizeof key);
+        std::memcpy(s->axi_ls_cst, cst, sizeof cst);
+    }
     rc = set_dt(s, *dt);
     if (rc) return rc;
-    const Grid &g = s->g;
-    double *ls = s->f[ASD2G_LS], *u = s->f[ASD2G_U], *v = s->f[ASD2G_V];
-    double *uh = s->f[ASD2G_UHAT], *vh = s->f[ASD2G_VHAT], *HS = s->f[ASD2G_HS];
-    // level set (test_mac2d_large.cpp:1269-1274)
-    cudaMemcpyAsync(s->f[ASD2G_LSB], ls, sizeof(double) * s->G, cudaMemcpyDeviceToDevice, s->st);
-    launch_center_vel(gl, u, v, s->tu, s->tv, s->st);
-    launch_fill_p(gl, ls, s->st);
-    launch_ls_stage(1, gl, ls, s->tu, s->tv, ls, s->w1, s->dsc, s->st);
-    launch_ls_stage(2, gl, s->w1, s->tu, s->tv, ls, s->w2, s->dsc, s->st);
-    launch_ls_stage(3, gl, s->w2, s->tu, s->tv, ls, ls, s->dsc, s->st);
-    launch_fill_p(gl, ls, s->st);
-    launch_reinit(gl, reinit_mode, s->prm.ls_max_atime, ls, s->f[ASD2G_LS0], s->w1, s->w2, s->w3, s->st);
-    launch_fill_p(gl, ls, s->st);
-    // momentum (:1276-1292)
-    launch_axi_kappa(g, ls, s->f[ASD2G_KAPPA], s->st);
-    launch_heaviside(g, ls, s->f[ASD2G_H], HS, s->st);
-    rc = axi_rhs(s, 0, ASD2G_LS, ASD2G_U, ASD2G_V, -1, ASD2G_HS, ASD2G_W0);
+    rc = replay_phase(s, &s->axi_pre_exec[reinit_mode], &s->axi_pre_calls[reinit_mode], "axi_step (before the solve)",
+                      [&] { return axi_step_pre(s, gl, reinit_mode); });
     if (rc) return rc;
-    double *const w[6] = {s->ua, s->va, s->ub, s->vb, s->w1, s->w2};
-    launch_axi_hat(g, s->M, 0, ls, s->f[ASD2G_W0], HS, s->dsc, uh, w, s->st);
-    launch_fill_uv(g, uh, nullptr, s->st);
-    rc = axi_rhs(s, 1, ASD2G_LS, ASD2G_U, ASD2G_V, ASD2G_UHAT, ASD2G_HS, ASD2G_W0);
-    if (rc) return rc;
-    launch_axi_hat(g, s->M, 1, ls, s->f[ASD2G_W0], HS, s->dsc, vh, w, s->st);
-    launch_fill_uv(g, nullptr, vh, s->st);
-    launch_axi_div(g, 1, uh, vh, s->f[ASD2G_DIV], s->st);
-    launch_fill_p(gl, ls, s->st);  // the driver fills the level set again before the solve (:1294)
-    axi_assemble_enqueue(s, axi_we_finite(s));
-    rc = cuda_check("axi_step (before the solve)");
-    if (rc) return rc;
-    // pressure, projection, dt (:1294-1306)
     const int st = solve(s, solver, tol, maxit, iters, rel_resid);
     if (st < 0) return st;
-    launch_scatter_ps(g, s->x, s->f[ASD2G_PS], s->f[ASD2G_P], s->dsc, s->st);
-    // The driver repeats the fills that SolvePoisson and UpdateVel end with
-    // (:1299, :1304-1305); with a Neumann side next to a Dirichlet one a
-    // second fill changes the corner ghosts, so it is repeated here too.
-    launch_fill_p(g, s->f[ASD2G_PS], s->st);
-    launch_update_vel(g, s->M, uh, vh, s->f[ASD2G_PS], ls, s->f[ASD2G_H], s->f[ASD2G_KAPPA], u, v, s->dsc, s->st);
-    launch_fill_uv(g, u, v, s->st);
-    launch_axi_update_dt(g, s->M, u, v, s->f[ASD2G_KAPPA], s->partial, s->counter, s->dsc + 1, s->st);
+    rc = replay_phase(s, &s->axi_post_exec, &s->axi_post_calls, "axi_step (after the solve)",
+                      [&] { return axi_step_post(s); });
+    if (rc) return rc;
     cudaMemcpyAsync(s->dsc_host, s->dsc, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
     rc = sync(s);
     if (rc) return rc;
