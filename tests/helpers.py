@@ -82,7 +82,9 @@ def bc_fixture(trial):
 
 def reinit_driver_case(name):
     """Initial fields of two of the reference's reinitialisation-only drivers
-    (test_levelset2d_large.cpp), 128^2 on [-2, 2]^2 with Neumann sides:
+    (test_levelset2d_large.cpp), 128^2 on [-2, 2]^2 with Neumann sides
+    (and "firsttime", :1220, the sign field of the unit circle for the
+    first-time Sussman reinitialisation):
     "kinks" (:1042, two overlapping unit circles 1.4 apart, the union's
     distance with its kinks; max pseudo-time 80) and "minrk2_2" (:882, the
     unit circle's distance times (x-1)^2 + (y-1)^2 + 0.1, far from a
@@ -99,6 +101,10 @@ def reinit_driver_case(name):
         r, a = 1.0, 0.7
         ls = np.minimum(np.sqrt((x + a) ** 2 + y * y) - r, np.sqrt((x - a) ** 2 + y * y) - r)
         max_atime = 80.0
+    elif name == "firsttime":  # :1220, +1 inside / -1 outside the unit circle, FirstTimeOnlyReinit_Sussman_2D
+        d = np.sqrt(x * x + y * y) - 1.0
+        ls = np.where(d < 0, 1.0, np.where(d > 0, -1.0, 0.0))
+        max_atime = 256.0
     else:
         ls = ((x - 1.0) ** 2 + (y - 1.0) ** 2 + 0.1) * (np.sqrt(x * x + y * y) - 1.0)
         max_atime = 256.0

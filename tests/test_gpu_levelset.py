@@ -220,22 +220,26 @@ def test_zalesak_full_revolution():
           f"error norms inf {err.max():.4f}, L1 {err.sum() / err.size:.4f}, L2 {np.sqrt((err ** 2).mean()):.4f}")
 
 
-@pytest.mark.parametrize("name", ["kinks", "minrk2_2"])
+@pytest.mark.parametrize("name", ["kinks", "minrk2_2", "firsttime"])
 def test_reinit_only_drivers(name):
-    """Two of the reference's reinitialisation-only drivers
-    (test_levelset2d_large.cpp:882, :1042), one Reinit_MinRK2_2D over their
-    long pseudo-times (5120 and 16384 pseudo-steps) on the GPU: bit-identical
+    """Three of the reference's reinitialisation-only drivers
+    (test_levelset2d_large.cpp:882, :1042, :1220): one Reinit_MinRK2_2D over
+    their long pseudo-times (5120 and 16384 pseudo-steps), and one
+    FirstTimeOnlyReinit_Sussman_2D of a sign field, on the GPU: bit-identical
     to the oracle."""
     from tests.helpers import reinit_driver_case
     g, ls, mt = reinit_driver_case(name)
+    mode = api.REINIT_FIRSTTIME if name == "firsttime" else api.REINIT_MINRK2
     a = ls.copy()
     O.bc(g, "p", a)
-    O.reinit(g, api.REINIT_MINRK2, a, mt)
+    O.reinit(g, mode, a, mt)
     p = api.Params(g.nx, g.ny, g.dx, g.dy, bc_u=g.bc_u, bc_v=g.bc_v, bc_p=g.bc_p, ls_max_atime=mt)
     with api.Session(p) as s:
         s.upload("ls", ls)
         s.apply_bc("ls", "P")
-        s.reinit(api.REINIT_MINRK2)
+        s.reinit(mode)
         got = s.download("ls")
-    assert_bitexact(got, a, f"{name}: {O.reinit_steps(g, mt)} pseudo-steps")
-    print(f"{name}: {O.reinit_steps(g, mt)} pseudo-steps, cells with phi > 0: {(a[3:-3, 3:-3] > 0).sum()}")
+    # the first-time mode runs over the domain's longer side as pseudo-time
+    steps = O.reinit_steps(g, max(g.nx * g.dx, g.ny * g.dy) if name == "firsttime" else mt)
+    assert_bitexact(got, a, f"{name}: {steps} pseudo-steps")
+    print(f"{name}: {steps} pseudo-steps, cells with phi > 0: {(a[3:-3, 3:-3] > 0).sum()}")

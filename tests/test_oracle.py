@@ -278,3 +278,20 @@ def test_reinit_with_kinks_against_live_reference():
     R.reinit(2, b)
     assert_bitexact(a, b, "kinks after 5120 pseudo-steps")
     R.close()
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference build (oracle/_ref) not present")
+def test_first_time_reinit_against_live_reference():
+    """The reference's first-time reinitialisation driver
+    (test_levelset2d_large.cpp:1220): FirstTimeOnlyReinit_Sussman_2D of the
+    sign field of the unit circle, bit for bit."""
+    from tests.helpers import reinit_driver_case
+    g, ls, mt = reinit_driver_case("firsttime")
+    a, b = ls.copy(), ls.copy()
+    O.bc(g, "p", a)
+    O.reinit(g, 3, a, mt)
+    R = Reference(g, ls_max_atime=mt)
+    R.bc("p", b)
+    R.reinit(3, b)
+    assert_bitexact(a, b, "first-time reinitialisation")
+    R.close()
