@@ -98,3 +98,62 @@ def test_axisym_against_live_reference(name, capfd):
     capfd.readouterr()  # GetUHat prints one debug line per z row (mac2dAxisym.cpp:1122-1123)
     out = oracle_outputs(g, f, base, ls, u, v, ps, dt)
     compare(g, out, lambda k: ref[k], f"live {name}")
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference build (oracle/_ref) not present")
+def test_axisym_driver_steps_against_live_reference(capfd):
+    """Three whole steps of the reference's axisymmetric driver loop
+    (test_mac2d_large.cpp:1264-1306) run through the reference's own objects
+    (LevelSetSolver2D with the level set's boundary, MACSolver2DAxisym with
+    its CG) and through the oracle's restatement of the step with the
+    reference CG iteration: level set, velocities, pressure and dt bit for
+    bit, on a bubble with density ratio 816 and surface tension."""
+    from oracle.pyoracle import FluidSpec, GridSpec, Reference
+    nr, nz = 32, 64
+    bu = ("axisym", "neumann", "dirichlet", "dirichlet")
+    g = GridSpec(nr, nz, 0.5 / nr, 1.0 / nz, bc_u=bu, bc_v=bu, bc_p=("axisym", "pressure", "neumann", "neumann"),
+                 cu=(0.0, 1.0, 1.0, 1.0))
+    lg = GridSpec(nr, nz, g.dx, g.dy, bc_u=bu, bc_v=bu, bc_p=("axisym", "lsfree", "lsfree", "lsfree"))
+    f = FluidSpec(rho_h=1000.0, rho_l=1.226, mu_h=1.137e-3, mu_l=1.78e-5, sigma=0.0728, g=0.0, g_axis=1, cfl=0.3)
+    r = (np.arange(nr + 6)[:, None] - 3 + 0.5) * g.dx
+    z = (np.arange(nz + 6)[None, :] - 3 + 0.5) * g.dy
+    ls = np.ascontiguousarray(np.sqrt(r ** 2 + (z - 0.5) ** 2) - 0.2)
+    O.bc(lg, "p", ls)
+    O.reinit(lg, 2, ls)
+    O.bc(lg, "p", ls)
+    u = np.full(ls.shape, 1.0)
+    v = g.zeros()
+    O.bc(g, "u", u)
+    O.bc(g, "v", v)
+    kappa = g.zeros()
+    dt = O.axi_update_dt(g, f, u, v, kappa)
+    st = dict(ls=ls.copy(), u=u.copy(), v=v.copy(), kappa=kappa.copy(), dt=dt)
+    R2, AR = Reference(lg, f), AxiReference(g, f)
+    ls_r, u_r, v_r, k_r = ls.copy(), u.copy(), v.copy(), kappa.copy()
+    for step in range(3):
+        lsB = ls_r.copy()
+        R2.ls_advect(ls_r, u_r, v_r, dt)
+        R2.bc("p", ls_r)
+        R2.reinit(2, ls_r)
+        R2.bc("p", ls_r)
+        AR.set_state(u_r, v_r, k_r, dt)
+        k_r = AR.kappa(ls_r)
+        H, HS = R2.heaviside(ls_r)
+        uh = AR.bc("u", AR.uhat(ls_r, u_r, AR.rhs_u(ls_r, u_r, v_r, HS), HS))
+        vh = AR.bc("v", AR.vhat(ls_r, v_r, AR.rhs_v(ls_r, u_r, uh, v_r, HS), HS))
+        d4, _ = AR.divergences(uh, vh)
+        R2.bc("p", ls_r)
+        ps, _ = AR.poisson_capture(d4, ls_r, lsB, H, maxiter=10000)
+        AR.bc("p", ps)
+        AR.update_vel(uh, vh, ps, ls_r, lsB, H)
+        got = AR.get_state()
+        u_r, v_r, k_r = AR.bc("u", got["u"]), AR.bc("v", got["v"]), got["kappa"]
+        AR.set_state(u_r, v_r, k_r, dt)
+        dt = AR.update_dt(u_r, v_r)
+        O.axi_step(g, f, st, ls_grid=lg, tol=1e-6, pcg_mode=1)
+        for name, a, b in (("ls", ls_r, st["ls"]), ("u", u_r, st["u"]), ("v", v_r, st["v"]), ("ps", ps, st["ps"])):
+            assert_bitexact(b, a, f"step {step} {name}")
+        assert dt == st["dt"], step
+    R2.close()
+    AR.close()
+    capfd.readouterr()
