@@ -295,3 +295,49 @@ def test_first_time_reinit_against_live_reference():
     R.reinit(3, b)
     assert_bitexact(a, b, "first-time reinitialisation")
     R.close()
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference build (oracle/_ref) not present")
+def test_droplet_steps_against_live_reference(capfd):
+    """Whole droplet steps of the reference's MAC driver loop
+    (test_mac2d_large.cpp:496-552) run through the reference's own objects
+    (LevelSetSolver2D, MACSolver2D with SolvePoisson and its CG) and through
+    the oracle's composed step with the reference CG iteration: level set,
+    velocities, pressure and dt bit for bit for two steps (RK3, MinRK2, GFM
+    jumps with surface tension; a Dirichlet top so that the reference's own
+    operator is well posed, see the all-Neumann pin)."""
+    from asd2_b200 import workloads as W
+    c = W.droplet(48, seed=5)
+    g = GridSpec(c.nx, c.ny, c.dx, c.dy, bc_u=c.bc_u, bc_v=c.bc_v, bc_p=("neumann", "neumann", "neumann", "dirichlet"))
+    fl = c.fluid
+    f = FluidSpec(rho_h=fl["rho_h"], rho_l=fl["rho_l"], mu_h=fl["mu_h"], mu_l=fl["mu_l"], sigma=fl["sigma"],
+                  g=fl["g"], g_axis=fl["g_axis"], fix_gravity=0, time_order=2, cfl=0.5)
+    ls = c.ls.copy()
+    O.bc(g, "p", ls)
+    st = dict(ls=ls.copy(), u=c.u.copy(), v=c.v.copy(), kappa=g.zeros(), ps=g.zeros(), p=g.zeros())
+    st["dt"] = dt = O.update_dt(g, f, st["u"], st["v"])
+    R = Reference(g, f)
+    ls_r, u_r, v_r, ps_r = ls.copy(), c.u.copy(), c.v.copy(), g.zeros()
+    for step in range(2):
+        lsB = ls_r.copy()
+        R.ls_advect(ls_r, u_r, v_r, dt)
+        R.bc("p", ls_r)
+        R.reinit(2, ls_r)
+        R.bc("p", ls_r)
+        R.set_state(u_r, v_r, ps_r, dt)
+        R.kappa(ls_r)
+        H, HS = R.heaviside(ls_r)
+        uh, vh = R.intermediate_vel(ls_r, u_r, v_r, HS)
+        R.bc("u", uh, which=1)
+        R.bc("v", vh, which=1)
+        ps_r, _ = R.poisson_capture(R.divergence(uh, vh), ls_r, lsB, H, maxiter=100000)
+        R.update_vel(uh, vh, ps_r, ls_r, lsB, H)
+        got = R.get_state()
+        u_r, v_r = got["u"], got["v"]
+        dt = R.update_dt(u_r, v_r)
+        O.droplet_step(g, f, st, tol=1e-6, pcg_mode=1)
+        for name, a, b in (("ls", ls_r, st["ls"]), ("u", u_r, st["u"]), ("v", v_r, st["v"]), ("ps", ps_r, st["ps"])):
+            assert_bitexact(b, a, f"step {step} {name}")
+        assert dt == st["dt"], step
+    R.close()
+    capfd.readouterr()
