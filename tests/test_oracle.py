@@ -298,20 +298,23 @@ def test_first_time_reinit_against_live_reference():
 
 
 @pytest.mark.skipif(not have_reference(), reason="reference build (oracle/_ref) not present")
-def test_droplet_steps_against_live_reference(capfd):
+@pytest.mark.parametrize("order, mode", [(2, 2), (0, 0), (1, 1), (2, 4)])
+def test_droplet_steps_against_live_reference(capfd, order, mode):
     """Whole droplet steps of the reference's MAC driver loop
     (test_mac2d_large.cpp:496-552) run through the reference's own objects
     (LevelSetSolver2D, MACSolver2D with SolvePoisson and its CG) and through
     the oracle's composed step with the reference CG iteration: level set,
-    velocities, pressure and dt bit for bit for two steps (RK3, MinRK2, GFM
-    jumps with surface tension; a Dirichlet top so that the reference's own
-    operator is well posed, see the all-Neumann pin)."""
+    velocities, pressure and dt bit for bit for two steps (time orders Euler,
+    RK2, RK3; reinitialisation original, Sussman, MinRK2, MinRK2 with the
+    constraint -- both sides call the same libm cos; GFM jumps with surface
+    tension; a Dirichlet top so that the reference's own operator is well
+    posed, see the all-Neumann pin)."""
     from asd2_b200 import workloads as W
     c = W.droplet(48, seed=5)
     g = GridSpec(c.nx, c.ny, c.dx, c.dy, bc_u=c.bc_u, bc_v=c.bc_v, bc_p=("neumann", "neumann", "neumann", "dirichlet"))
     fl = c.fluid
     f = FluidSpec(rho_h=fl["rho_h"], rho_l=fl["rho_l"], mu_h=fl["mu_h"], mu_l=fl["mu_l"], sigma=fl["sigma"],
-                  g=fl["g"], g_axis=fl["g_axis"], fix_gravity=0, time_order=2, cfl=0.5)
+                  g=fl["g"], g_axis=fl["g_axis"], fix_gravity=0, time_order=order, cfl=0.5)
     ls = c.ls.copy()
     O.bc(g, "p", ls)
     st = dict(ls=ls.copy(), u=c.u.copy(), v=c.v.copy(), kappa=g.zeros(), ps=g.zeros(), p=g.zeros())
@@ -322,7 +325,7 @@ def test_droplet_steps_against_live_reference(capfd):
         lsB = ls_r.copy()
         R.ls_advect(ls_r, u_r, v_r, dt)
         R.bc("p", ls_r)
-        R.reinit(2, ls_r)
+        R.reinit(mode, ls_r)
         R.bc("p", ls_r)
         R.set_state(u_r, v_r, ps_r, dt)
         R.kappa(ls_r)
@@ -335,7 +338,7 @@ def test_droplet_steps_against_live_reference(capfd):
         got = R.get_state()
         u_r, v_r = got["u"], got["v"]
         dt = R.update_dt(u_r, v_r)
-        O.droplet_step(g, f, st, tol=1e-6, pcg_mode=1)
+        O.droplet_step(g, f, st, tol=1e-6, pcg_mode=1, reinit_mode=mode)
         for name, a, b in (("ls", ls_r, st["ls"]), ("u", u_r, st["u"]), ("v", v_r, st["v"]), ("ps", ps_r, st["ps"])):
             assert_bitexact(b, a, f"step {step} {name}")
         assert dt == st["dt"], step
