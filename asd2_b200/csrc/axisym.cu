@@ -319,8 +319,27 @@ constexpr int TP = 8;
 
 // Rows further ahead than the register ring are pulled into L1 with a
 // prefetch hint PF rows ahead (the ring alone covers 8 rows of the dependent
-// chain, less than an L2 round trip).
-constexpr int PF = 32;
+// chain, less than an L2 round trip).  Build-time tunable.
+#ifndef ASD2G_AXI_THOMAS_PF
+#define ASD2G_AXI_THOMAS_PF 32
+#endif
+constexpr int PF = ASD2G_AXI_THOMAS_PF;
+
+// Lines per CTA.  A sweep has one thread per grid line and no more (1023 to
+// 2048 threads at 1024 x 2048), so the CTAs are kept small to spread the
+// lines over all the SMs: each SM's L1 keeps a bounded number of misses in
+// flight, and the rows' loads bound the sweep.  8 adjacent lines read 64
+// contiguous bytes per row and array (two full sectors).  Wider CTAs only
+// once there are lines for several CTAs per SM.  Build-time override:
+// ASD2G_AXI_THOMAS_LINES.
+inline int thomas_lines_per_cta(int nlines) {
+#ifdef ASD2G_AXI_THOMAS_LINES
+    (void)nlines;
+    return ASD2G_AXI_THOMAS_LINES;
+#else
+    return nlines <= 4 * 148 * 8 ? 8 : nlines <= 4 * 148 * 32 ? 32 : 64;
+#endif
+}
 __device__ __forceinline__ void pf_l1(const void *p) { asm volatile("prefetch.L1 [%0];" ::"l"(p)); }
 
 // a / b with the IEEE result, taking the quotient of a zero numerator as the
@@ -606,7 +625,6 @@ void launch_axi_rhs_v(const Grid &g, const MomConst &M, const double *ls, const 
 // solution, the z-line right sides, the 1/r^2 denominators).
 void launch_axi_hat(const Grid &g, const MomConst &M, int comp, const double *ls, const double *rhs,
                     const double *H, const double *dtp, double *out, double *const w[6], cudaStream_t st) {
-    constexpr int T = 64;
     double *lo = w[0], *di = w[1], *up = w[2], *dr = w[3], *dz = w[4], *den = w[5];
     const int64_t sx = g.sx, sy = g.sy;
     cudaMemsetAsync(out, 0, sizeof(double) * (size_t)sx * sy, st);
@@ -615,20 +633,24 @@ void launch_axi_hat(const Grid &g, const MomConst &M, int comp, const double *ls
         const int m = g.nx - 1;
         k_axi_coef_u_r<<<dim3((g.ny + TJ - 1) / TJ, (m + TI - 1) / TI), blk, 0, st>>>(g, M, ls, rhs, H, dtp, lo, di,
                                                                                        up, dr);
+        int T = thomas_lines_per_cta(g.ny);
         k_axi_thomas<<<(g.ny + T - 1) / T, T, 0, st>>>(g.ny, m, LineMap{NB + sy * (NB + 1), 1, sy}, lo, di, up, dr,
                                                        LineMap{0, 0, 0}, nullptr, nullptr);
         k_axi_coef_u_z<<<dim3((g.ny + TJ - 1) / TJ, (m + TI - 1) / TI), blk, 0, st>>>(g, M, ls, H, dtp, dr, lo, di,
                                                                                        up, dz, den);
+        T = thomas_lines_per_cta(m);
         k_axi_thomas<<<(m + T - 1) / T, T, 0, st>>>(m, g.ny, LineMap{(NB + 1) + sx * NB, 1, sx}, lo, di, up, dz,
                                                     LineMap{NB + sy * (NB + 1), sy, 1}, out, den);
     } else {
         const int m = g.ny - 1;
         k_axi_coef_v_r<<<dim3((m + TJ - 1) / TJ, (g.nx + TI - 1) / TI), blk, 0, st>>>(g, M, ls, rhs, H, dtp, lo, di,
                                                                                         up, dr);
+        int T = thomas_lines_per_cta(m);
         k_axi_thomas<<<(m + T - 1) / T, T, 0, st>>>(m, g.nx, LineMap{(NB + 1) + sy * NB, 1, sy}, lo, di, up, dr,
                                                     LineMap{0, 0, 0}, nullptr, nullptr);
         k_axi_coef_v_z<<<dim3((m + TJ - 1) / TJ, (g.nx + TI - 1) / TI), blk, 0, st>>>(g, M, ls, H, dtp, dr, lo, di,
                                                                                         up, dz);
+        T = thomas_lines_per_cta(g.nx);
         k_axi_thomas<<<(g.nx + T - 1) / T, T, 0, st>>>(g.nx, m, LineMap{NB + sx * (NB + 1), 1, sx}, lo, di, up, dz,
                                                        LineMap{(NB + 1) + sy * NB, sy, 1}, out, nullptr);
     }
