@@ -629,14 +629,19 @@ class AxiReference:
     """The reference's MACSolver2DAxisym, compiled unmodified (oracle/_ref).
     Grid x is r, y is z; gravity axis 0 = R, 1 = Z."""
 
-    def __init__(self, g: GridSpec, f: FluidSpec | None = None, base_r=0.0, base_z=0.0, path: str = REF_SO):
+    def __init__(self, g: GridSpec, f: FluidSpec | None = None, base_r=0.0, base_z=0.0, len_r=None, len_z=None,
+                 path: str = REF_SO):
+        """len_r / len_z: the domain lengths the reference divides by nr / nz
+        for its spacings (default dr * nr, dz * nz)."""
         L = self.L = _load(path)
         f = f or FluidSpec()
         self.g = g
         V = C.c_void_p
         L.ref_axi_create.restype = V
         L.ref_axi_create.argtypes = [C.c_int, C.c_int] + [C.c_double] * 9 + [C.c_int, C.c_double, C.c_double]
-        self.h = V(L.ref_axi_create(g.nx, g.ny, base_r, base_z, g.dx * g.nx, g.dy * g.ny, f.rho_h, f.rho_l, f.mu_h,
+        lr = g.dx * g.nx if len_r is None else len_r
+        lz = g.dy * g.ny if len_z is None else len_z
+        self.h = V(L.ref_axi_create(g.nx, g.ny, base_r, base_z, lr, lz, f.rho_h, f.rho_l, f.mu_h,
                                     f.mu_l, f.g, f.g_axis, f.sigma, f.cfl))
         for name, args, res in [
             ("ref_axi_set_bc", [V, C.c_char, C.c_char_p, _dp], None),

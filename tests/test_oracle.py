@@ -315,13 +315,23 @@ def test_droplet_steps_against_live_reference(capfd, order, mode):
     fl = c.fluid
     f = FluidSpec(rho_h=fl["rho_h"], rho_l=fl["rho_l"], mu_h=fl["mu_h"], mu_l=fl["mu_l"], sigma=fl["sigma"],
                   g=fl["g"], g_axis=fl["g_axis"], fix_gravity=0, time_order=order, cfl=0.5)
-    ls = c.ls.copy()
+    live_droplet_steps(g, f, c.ls, c.u, c.v, mode, steps=2)
+    capfd.readouterr()
+
+
+def live_droplet_steps(g, f, ls0, u0, v0, mode, steps=2, equal=assert_bitexact, len_x=None, len_y=None):
+    """`steps` steps of the reference's MAC driver loop through the
+    reference's own objects and through the oracle's composed step (reference
+    CG iteration to 1e-6); level set, u, v, ps and dt compared with `equal`
+    after every step.  len_x / len_y: the domain lengths the reference divides
+    by nx / ny for its spacings (default dx * nx, dy * ny)."""
+    ls = ls0.copy()
     O.bc(g, "p", ls)
-    st = dict(ls=ls.copy(), u=c.u.copy(), v=c.v.copy(), kappa=g.zeros(), ps=g.zeros(), p=g.zeros())
+    st = dict(ls=ls.copy(), u=u0.copy(), v=v0.copy(), kappa=g.zeros(), ps=g.zeros(), p=g.zeros())
     st["dt"] = dt = O.update_dt(g, f, st["u"], st["v"])
-    R = Reference(g, f)
-    ls_r, u_r, v_r, ps_r = ls.copy(), c.u.copy(), c.v.copy(), g.zeros()
-    for step in range(2):
+    R = Reference(g, f, len_x=len_x, len_y=len_y)
+    ls_r, u_r, v_r, ps_r = ls.copy(), u0.copy(), v0.copy(), g.zeros()
+    for step in range(steps):
         lsB = ls_r.copy()
         R.ls_advect(ls_r, u_r, v_r, dt)
         R.bc("p", ls_r)
@@ -340,7 +350,6 @@ def test_droplet_steps_against_live_reference(capfd, order, mode):
         dt = R.update_dt(u_r, v_r)
         O.droplet_step(g, f, st, tol=1e-6, pcg_mode=1, reinit_mode=mode)
         for name, a, b in (("ls", ls_r, st["ls"]), ("u", u_r, st["u"]), ("v", v_r, st["v"]), ("ps", ps_r, st["ps"])):
-            assert_bitexact(b, a, f"step {step} {name}")
-        assert dt == st["dt"], step
+            equal(b, a, f"step {step} {name}")
+        assert dt == st["dt"] or (dt != dt and st["dt"] != st["dt"]), step
     R.close()
-    capfd.readouterr()

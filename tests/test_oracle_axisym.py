@@ -72,12 +72,11 @@ def test_axisym_golden(name):
     compare(g, out, lambda k: GOLD[f"{name}/{k}"], name)
 
 
-@pytest.mark.skipif(not have_reference(), reason="reference build (oracle/_ref) not present")
-@pytest.mark.parametrize("name", list(CASES))
-def test_axisym_against_live_reference(name, capfd):
-    g, f, base, ls, u, v, ps = case_inputs(name, seed=1234)
-    dt = 1.5e-3
-    R = AxiReference(g, f, base_r=base)
+def reference_outputs(g, f, base, ls, u, v, ps, dt, **lengths):
+    """The fixture's pipeline through the reference's own MACSolver2DAxisym
+    (oracle/_ref), in the order the golden script calls it; lengths: len_r /
+    len_z for AxiReference."""
+    R = AxiReference(g, f, base_r=base, **lengths)
     HS = smooth_heaviside(ls, 1.5 * min(g.dx, g.dy))
     H = np.ascontiguousarray((ls >= 0.0).astype(np.float64))
     ref = {"kappa": R.kappa(ls)}
@@ -95,6 +94,15 @@ def test_axisym_against_live_reference(name, capfd):
     ref["u_new"], ref["v_new"] = st["u"], st["v"]
     ref["dt_next"] = np.array([R.update_dt(st["u"], st["v"])])
     R.close()
+    return ref
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("name", list(CASES))
+def test_axisym_against_live_reference(name, capfd):
+    g, f, base, ls, u, v, ps = case_inputs(name, seed=1234)
+    dt = 1.5e-3
+    ref = reference_outputs(g, f, base, ls, u, v, ps, dt)
     capfd.readouterr()  # GetUHat prints one debug line per z row (mac2dAxisym.cpp:1122-1123)
     out = oracle_outputs(g, f, base, ls, u, v, ps, dt)
     compare(g, out, lambda k: ref[k], f"live {name}")
