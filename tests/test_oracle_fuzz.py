@@ -157,3 +157,47 @@ def test_axisym_functions_fuzz(capfd, nr, nz, base, bu, bv, bp, cu, cv, cp, f, s
     capfd.readouterr()  # GetUHat's debug line per z row
     out = oracle_outputs(g, f, base, ls, u, v, ps, dt)
     compare(g, out, lambda k: ref[k], f"axisym {bu, bv, bp} base {base}")
+
+
+@FUZZ
+@given(nx=st.integers(6, 20), ny=st.integers(6, 20), bp=p_sides(), cp=consts, f=fluids(),
+       its=st.sampled_from((1, 2, 5, 12)), seed=st.integers(0, 2 ** 31 - 1))
+def test_gfm_system_and_reference_solvers_fuzz(capfd, nx, ny, bp, cp, f, its, seed):
+    """SolvePoisson's GFM system (src/mac2d.cpp:1300-1660, captured before the
+    solve) equals the oracle's assembly entry by entry, CSR structure
+    included, and the reference's own CG and BiCGStab (src/poisson2d.cpp,
+    BiCGStab with its rho_2 that is never updated) equal the oracle's
+    reference iterations after `its` iterations, on drawn grids, Dirichlet-
+    group pressure boundaries, constants and fluids."""
+    lx, ly = 1.0, 1.0
+    dx, dy = lx / nx, ly / ny
+    g = GridSpec(nx, ny, dx, dy, bc_p=bp, cp=cp)
+    ls, u, v = drop_fields(nx, ny, dx, dy, seed)
+    rng = np.random.Generator(np.random.PCG64(seed + 7))
+    div = np.ascontiguousarray(rng.standard_normal(g.shape))
+    dt = 2.0e-4
+    R = Reference(g, f, len_x=lx, len_y=ly)
+    try:
+        R.bc("P", ls, which=1)
+        H, _ = R.heaviside(ls)
+        k = R.kappa(ls)
+        R.set_state(u, v, g.zeros(), dt)
+        R.set_kappa(k.copy())
+        _, (a, ia, ja, b) = R.poisson_capture(div, ls, ls, H, maxiter=0)
+        kap = k.copy()
+        sysd = O.gfm_assemble(g, f, dt, ls, kap, H, div, recompute_kappa=True)
+        a2, ia2, ja2, b2 = O.gfm_to_csr(g, sysd)
+        assert np.array_equal(ia2, ia) and np.array_equal(ja2, ja), "CSR structure"
+        same(a2, a, "CSR values")
+        same(b2, b, "right-hand side")
+        rhs = g.zeros()
+        rhs[3:-3, 3:-3] = b.reshape(ny, nx).T
+        mdiag = np.array([a[ia[r]:ia[r + 1]][ja[ia[r]:ia[r + 1]] == r][0] for r in range(len(ia) - 1)])
+        x, _, _, _ = O.pcg(g, sysd, tol=1e-6, maxit=its, mode=1)
+        same(O.scatter(g, x)[3:-3, 3:-3], R.cg(rhs, (a, ia, ja), mdiag, its)[3:-3, 3:-3], f"CG, {its} its")
+        x, _, _, _ = O.bicgstab(g, sysd, tol=1e-6, maxit=its, mode=1)
+        same(O.scatter(g, x)[3:-3, 3:-3], R.bicgstab(rhs, (a, ia, ja), mdiag, its)[3:-3, 3:-3],
+             f"BiCGStab, {its} its")
+    finally:
+        R.close()
+    capfd.readouterr()
