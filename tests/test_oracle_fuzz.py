@@ -201,3 +201,35 @@ def test_gfm_system_and_reference_solvers_fuzz(capfd, nx, ny, bp, cp, f, its, se
     finally:
         R.close()
     capfd.readouterr()
+
+
+@FUZZ
+@given(nx=st.integers(6, 28), ny=st.integers(6, 28), bp=st.tuples(*[st.sampled_from(KINDS_P)] * 4),
+       mode=st.sampled_from((0, 1, 2, 3, 4)), atime=st.sampled_from((0.0, 1.0, 5.0)),
+       shape=st.sampled_from(("drop", "sign", "scaled")), seed=st.integers(0, 2 ** 31 - 1))
+def test_reinitialisation_fuzz(nx, ny, bp, mode, atime, shape, seed):
+    """Every reinitialisation of LevelSetSolver2D (src/levelset2d.cpp:
+    Reinit_Original_2D, Reinit_Sussman_2D, Reinit_MinRK2_2D,
+    FirstTimeOnlyReinit_Sussman_2D and MinRK2 with the Sussman constraint)
+    over its pseudo-time (the default or a drawn maximum), from a distance
+    function, a sign field or a distance far from unit gradient, with every
+    P-grid boundary kind on any side, against the reference's own solver."""
+    lx, ly = 1.0, 1.0
+    dx, dy = lx / nx, ly / ny
+    g = GridSpec(nx, ny, dx, dy, bc_p=bp)
+    ls, _, _ = drop_fields(nx, ny, dx, dy, seed)
+    if shape == "sign":
+        ls = np.ascontiguousarray(np.sign(ls))
+    elif shape == "scaled":
+        x = (np.arange(nx + 6)[:, None] - 3 + 0.5) * dx
+        ls = np.ascontiguousarray(ls * ((x - 0.3) ** 2 + 0.1))
+    a, b = ls.copy(), ls.copy()
+    O.bc(g, "p", a)
+    O.reinit(g, mode, a, atime)
+    R = Reference(g, len_x=lx, len_y=ly, ls_max_atime=atime)
+    try:
+        R.bc("p", b)
+        R.reinit(mode, b)
+    finally:
+        R.close()
+    same(a, b, f"reinitialisation mode {mode}, {shape}, {bp}")
