@@ -233,3 +233,38 @@ def test_reinitialisation_fuzz(nx, ny, bp, mode, atime, shape, seed):
     finally:
         R.close()
     same(a, b, f"reinitialisation mode {mode}, {shape}, {bp}")
+
+
+AXI_P_DIRICHLET = ("dirichlet", "inlet", "outlet", "pressure")
+
+
+@st.composite
+def axi_p_sides(draw):
+    """Pressure kinds of the axisymmetric assembly with at least one side of
+    its Dirichlet group (no pinned all-Neumann system)."""
+    k = list(draw(st.tuples(*[st.sampled_from(AXI_P)] * 4)))
+    if not any(x in AXI_P_DIRICHLET for x in k):
+        k[draw(st.integers(0, 3))] = draw(st.sampled_from(AXI_P_DIRICHLET))
+    return tuple(k)
+
+
+@FUZZ
+@given(nr=st.integers(8, 20), nz=st.integers(8, 24), base=st.sampled_from((0.0, 0.05)), bu=sides_uv, bv=sides_uv,
+       bp=axi_p_sides(), bl=st.tuples(*[st.sampled_from(KINDS_P)] * 4), cu=consts, cv=consts, cp=consts,
+       f=fluids(axisym=True), mode=st.sampled_from((0, 2, 4)), seed=st.integers(0, 2 ** 31 - 1))
+def test_axisym_driver_steps_fuzz(capfd, nr, nz, base, bu, bv, bp, bl, cu, cv, cp, f, mode, seed):
+    """Two whole steps of the reference's axisymmetric driver loop (the level
+    set on its own P-grid kinds, MACSolver2DAxisym with SolvePoisson's CG)
+    against the oracle's composed step, bit for bit, on drawn grids, axis
+    offsets, boundary sets of all four grids, fluids and reinitialisations."""
+    from tests.test_oracle_axisym import live_axi_steps
+    lr, lz = 0.5, 1.0
+    dr, dz = lr / nr, lz / nz
+    g = GridSpec(nr, nz, dr, dz, bc_u=bu, bc_v=bv, bc_p=bp, cu=cu, cv=cv, cp=cp)
+    lg = GridSpec(nr, nz, dr, dz, bc_u=bu, bc_v=bv, bc_p=bl)
+    ls, u, v = drop_fields(nr, nz, dr, dz, seed, base_x=base)
+    O.bc(lg, "p", ls)
+    O.bc(g, "u", u)
+    O.bc(g, "v", v)
+    live_axi_steps(g, lg, f, ls, u, v, steps=2, mode=mode, base_r=base, equal=same, len_r=lr, len_z=lz)
+    capfd.readouterr()
