@@ -1120,6 +1120,7 @@ def run_ours(args):
     }
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(snap, c, dt, args)
+        line["cpu_reference_cg"] = cg_blas_baseline(snap, c, dt, line["cpu_baseline"]["pcg_iterations"])
     if rank == 0:
         print(json.dumps(line), flush=True)
     s.close()
@@ -1170,7 +1171,109 @@ def cpu_baseline(snap, case, dt, args, procs=1, budget_s=None):
         it, tres = res[0][2], res[0][3]
     return {"value": total / tmax, "unit": "GFM Poisson solves/s", "cores": procs, "kind": "port",
             "sample": f"{total} solves of the same {case.nx}x{case.ny} GFM system ({it} PCG iterations each, "
-                      f"true rel. residual {tres:.1e}) in {tmax:.1f} s, oracle/asd2_oracle.c built -O2"}
+                      f"true rel. residual {tres:.1e}) in {tmax:.1f} s, oracle/asd2_oracle.c built -O2",
+            "pcg_iterations": it}
+
+
+def _quiet_call(fn):
+    """fn() with the process's stdout (fd 1) sent to a pipe; returns (fn's
+    result, what it printed).  The reference's solvers print one status line
+    per solve, which must not reach the bench's JSON line."""
+    import ctypes
+    sys.stdout.flush()
+    libc = ctypes.CDLL(None)
+    r, w = os.pipe()
+    saved = os.dup(1)
+    try:
+        os.dup2(w, 1)
+        out = fn()
+        libc.fflush(None)
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(w)
+    with os.fdopen(r) as f:
+        text = f.read()
+    return out, text
+
+
+def _cg_worker(payload):
+    """One build of the reference's CG timed in a fresh process (its BLAS and
+    OpenMP thread counts come from the environment it was started with)."""
+    sys.path.insert(0, ROOT)
+    from oracle.pyoracle import FluidSpec, GridSpec, Reference
+    g = GridSpec(**payload["grid"])
+    R = Reference(g, FluidSpec(**payload["fluid"]), path=payload["path"])
+    a, ia, ja = payload["csr"]
+    best, printed = float("inf"), ""
+    for _ in range(payload["reps"]):
+        t0 = time.perf_counter()
+        _, printed = _quiet_call(lambda: R.cg(payload["rhs"], (a, ia, ja), payload["mdiag"], payload["iters"]))
+        best = min(best, time.perf_counter() - t0)
+    R.close()
+    ran = [ln.split() for ln in printed.splitlines() if ln.startswith("CG :")]
+    return best, (int(ran[-1][2]) if ran else None)
+
+
+def cg_blas_baseline(snap, case, dt, its_to_tol, iters=200, reps=3):
+    """The reference's own CG_2FUniformP_2D (poisson2d.cpp:230-401) timed per
+    iteration on the same GFM system, in its two CPU builds: the serial
+    fixed-order BLAS shim (oracle/_ref/libasd2ref.so, one core) and OpenBLAS
+    BLAS-1 with the CSR SpMV split over OpenMP threads (libasd2ref_blas.so) at
+    three splits of the host cores between the two (passive OpenMP waits: with
+    both spinning on every core the two thread pools starve each other).
+    The system is the restatement's correctly pinned CSR (the reference's own
+    pin is mis-indexed and its CG does not converge on it); `iters`
+    iterations per timed call, below the count at which its 1e-6 stop could
+    end the call early.  Solves/s = 1 / (time per iteration x the Jacobi-PCG
+    iterations to the bench's tolerance, its_to_tol)."""
+    import multiprocessing as mp
+    from oracle.pyoracle import REF_SO, FluidSpec, GridSpec, Oracle
+    blas_so = os.path.join(os.path.dirname(REF_SO), "libasd2ref_blas.so")
+    if not os.path.exists(REF_SO):
+        return None
+    grid = dict(nx=case.nx, ny=case.ny, dx=case.dx, dy=case.dy, bc_u=case.bc_u, bc_v=case.bc_v, bc_p=case.bc_p)
+    g, f = GridSpec(**grid), FluidSpec(**case.fluid)
+    O = Oracle()
+    kap = snap["kappa"].copy()
+    sysd = O.gfm_assemble(g, f, dt, snap["ls"], kap, snap["H"], snap["div"], recompute_kappa=True)
+    a, ia, ja, b = O.gfm_to_csr(g, sysd)
+    rows = len(ia) - 1
+    mdiag = np.array([a[ia[r]:ia[r + 1]][ja[ia[r]:ia[r + 1]] == r][0] for r in range(rows)])
+    rhs = g.zeros()
+    nat = np.concatenate([[0.0], b]) if rows == g.nx * g.ny - 1 else b
+    rhs[3:-3, 3:-3] = nat.reshape(g.ny, g.nx).T
+    iters = int(min(iters, max(2, its_to_tol // 2)))
+    out = {"system": f"{case.nx}x{case.ny} GFM, {rows} unknowns", "iterations_per_call": iters,
+           "iterations_to_tol": int(its_to_tol)}
+    cores = os.cpu_count() or 1
+    runs = [("serial_shim", REF_SO, 1, 1)]
+    if os.path.exists(blas_so):
+        half = max(1, cores // 2)
+        runs += [(f"openblas_{bt}_openmp_{ot}", blas_so, bt, ot) for bt, ot in ((1, cores), (half, half), (cores, 1))]
+    ctx = mp.get_context("spawn")
+    saved = {k: os.environ.get(k) for k in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "OMP_WAIT_POLICY")}
+    best_name, best_ms = None, float("inf")
+    try:
+        for name, path, bt, ot in runs:
+            os.environ.update(OPENBLAS_NUM_THREADS=str(bt), OMP_NUM_THREADS=str(ot), OMP_WAIT_POLICY="passive")
+            payload = dict(grid=grid, fluid=dict(case.fluid), path=path, csr=(a, ia, ja), mdiag=mdiag, rhs=rhs,
+                           iters=iters, reps=reps)
+            with ctx.Pool(1) as pool:
+                t, done = pool.apply(_cg_worker, (payload,))
+            ms_it = 1e3 * t / (done or iters)
+            out[name] = {"openblas_threads": bt, "openmp_threads": ot, "ms_per_iteration": ms_it,
+                         "iterations_run": done, "solves_per_s": 1e3 / (ms_it * its_to_tol)}
+            if ms_it < best_ms:
+                best_name, best_ms = name, ms_it
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    out["best"] = best_name
+    return out
 
 
 def learned_cpu_baseline(snaps):

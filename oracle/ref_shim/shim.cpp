@@ -9,6 +9,11 @@
 // operand and the first dcopy records its source vector.  Inside
 // PoissonSolver2D::CG_2FUniform_2D (poisson2d.cpp:320-329) those are exactly
 // the assembled matrix A and the right-hand side b.
+//
+// With ASD2_SHIM_EXTERNAL_CBLAS (the threaded build for the timed CPU
+// baseline, not for parity) the cblas_d* calls go to a real CBLAS linked in
+// (OpenBLAS, its own threads), the SpMV rows are split over OpenMP threads
+// (each row still summed in order) and dcopy captures nothing.
 #include "mkl.h"
 #include <cmath>
 #include <vector>
@@ -23,6 +28,7 @@ struct Capture {
 }  // namespace
 
 extern "C" {
+#ifndef ASD2_SHIM_EXTERNAL_CBLAS
 void cblas_dcopy(const MKL_INT n, const double *x, const MKL_INT incx, double *y, const MKL_INT incy) {
     if (g_cap.armed && g_cap.have_a && !g_cap.have_b) {
         g_cap.b.assign(n, 0.0);
@@ -52,6 +58,7 @@ double cblas_dnrm2(const MKL_INT n, const double *x, const MKL_INT incx) {
 void cblas_dscal(const MKL_INT n, const double a, double *x, const MKL_INT incx) {
     for (MKL_INT i = 0; i < n; i++) x[(int64_t)i * incx] *= a;
 }
+#endif
 
 void mkl_cspblas_dcsrgemv(const char *, const MKL_INT *m, const double *a, const MKL_INT *ia,
                           const MKL_INT *ja, const double *x, double *y) {
@@ -63,6 +70,9 @@ void mkl_cspblas_dcsrgemv(const char *, const MKL_INT *m, const double *a, const
         g_cap.a.assign(a, a + ia[rows]);
         g_cap.have_a = true;
     }
+#ifdef ASD2_SHIM_EXTERNAL_CBLAS
+#pragma omp parallel for schedule(static)
+#endif
     for (MKL_INT r = 0; r < rows; r++) {
         double s = 0.0;
         for (MKL_INT k = ia[r]; k < ia[r + 1]; k++) {
