@@ -645,6 +645,7 @@ class AxiReference:
                                     f.mu_l, f.g, f.g_axis, f.sigma, f.cfl))
         for name, args, res in [
             ("ref_axi_set_bc", [V, C.c_char, C.c_char_p, _dp], None),
+            ("ref_axi_tdma", [V, _dp, _dp, _dp, _dp, C.c_int], C.c_int),
             ("ref_axi_apply_bc", [V, C.c_char, _dp], None),
             ("ref_axi_set_state", [V, _dp, _dp, _dp, C.c_double], None),
             ("ref_axi_get_state", [V, _dp, _dp, _dp, _dp, _dp], None),
@@ -693,6 +694,13 @@ class AxiReference:
         u, v, ps, p, k = (self.z() for _ in range(5))
         self.L.ref_axi_get_state(self.h, u, v, ps, p, k)
         return dict(u=u, v=v, ps=ps, p=p, kappa=k)
+
+    def tdma(self, a, b, c, d):
+        """SolveTDMA on copies; returns (c, d) as the reference leaves them."""
+        f = lambda x: np.array(x, dtype=np.float64)
+        a, b, c, d = f(a), f(b), f(c), f(d)
+        rc = self.L.ref_axi_tdma(self.h, a, b, c, d, len(d))
+        return rc, c, d
 
     def kappa(self, ls):
         out = self.z()

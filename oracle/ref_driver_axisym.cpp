@@ -6,6 +6,7 @@
 // layout idx(i,j) = j + (nz+6)*i, i along r.
 #include <cstring>
 #include <memory>
+#include <algorithm>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -43,6 +44,18 @@ void *ref_axi_create(int nr, int nz, double base_r, double base_z, double len_r,
     return c;
 }
 void ref_axi_destroy(void *h) { delete static_cast<AxiCtx *>(h); }
+
+// MACSolver2DAxisym::SolveTDMA (mac2dAxisym.cpp:2255-2306) on one system of n
+// rows: a, b, c the sub-, main and super-diagonal, d the right side; c and d
+// come back as the solver leaves them (d the solution).
+int ref_axi_tdma(void *h, double *a, double *b, double *c, double *d, int n) {
+    AxiCtx *x = static_cast<AxiCtx *>(h);
+    std::vector<double> A(a, a + n), B(b, b + n), Cv(c, c + n), D(d, d + n);
+    const int rc = x->mac->SolveTDMA(A, B, Cv, D, n);
+    std::copy(Cv.begin(), Cv.end(), c);
+    std::copy(D.begin(), D.end(), d);
+    return rc;
+}
 
 // kind 'U', 'V' or 'P'; spec: four lower-case names "W E S N"; k4: W E S N constants.
 void ref_axi_set_bc(void *h, char kind, const char *spec, const double *k4) {

@@ -16,7 +16,7 @@ import pytest
 
 from asd2_b200 import build as B
 from asd2_b200 import workloads as W
-from oracle.pyoracle import Oracle
+from oracle.pyoracle import Oracle, have_reference
 from tests.helpers import assert_bitexact, assert_close, fluid_from_case, grid_from_case, interior
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -270,3 +270,46 @@ def test_axisym_driver_steps(tmp_path, kind):
         assert_close(interior(ps), interior(st["ps"]), 0.0, 1e-8 * max(np.abs(st["ps"]).max(), 1e-30),
                      f"ps step {k}")
         assert abs(blk[4 * n] - st["dt"]) <= 1e-9 * st["dt"]
+
+
+TDMA_DRIVER = os.path.join(HERE, "dropin", "tdma_driver.cpp")
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("n", [2, 3, 17, 64])
+def test_axisym_solve_tdma_equals_reference(tmp_path, n):
+    """MACSolver2DAxisym::SolveTDMA of the drop-in (host code, no GPU) against
+    the reference's own (mac2dAxisym.cpp:2255-2306) on random diagonally
+    dominant and on non-dominant systems: the overwritten super-diagonal and
+    the solution bit for bit."""
+    from oracle.pyoracle import AxiReference, GridSpec
+    exe = _compile(tmp_path, TDMA_DRIVER)
+    rng = np.random.Generator(np.random.PCG64(n))
+    systems = []
+    for k in range(40):
+        a, c, d = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n), rng.standard_normal(n)
+        b = rng.uniform(2.1, 3.0, n) * rng.choice([-1.0, 1.0], n) if k % 2 else rng.uniform(-1.5, 1.5, n)
+        systems.append((a, b, c, d))
+    inp, out = os.path.join(str(tmp_path), "in.bin"), os.path.join(str(tmp_path), "out.bin")
+    with open(inp, "wb") as fh:
+        np.array([n, len(systems)], dtype=np.int32).tofile(fh)
+        for s in systems:
+            for v in s:
+                np.ascontiguousarray(v, dtype=np.float64).tofile(fh)
+    r = subprocess.run([exe, inp, out], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-2000:]
+    raw = open(out, "rb").read()
+    rec = 4 + 16 * n
+    assert len(raw) == rec * len(systems)
+    R = AxiReference(GridSpec(8, 8, 1 / 8, 1 / 8))
+    try:
+        for k, s in enumerate(systems):
+            blk = raw[k * rec:(k + 1) * rec]
+            rc = int(np.frombuffer(blk[:4], dtype=np.int32)[0])
+            cd = np.frombuffer(blk[4:], dtype=np.float64)
+            rrc, rc_c, rc_d = R.tdma(*s)
+            assert rc == rrc == 0, k
+            np.testing.assert_array_equal(cd[:n], rc_c, err_msg=f"system {k}: c")
+            np.testing.assert_array_equal(cd[n:], rc_d, err_msg=f"system {k}: d")
+    finally:
+        R.close()
