@@ -268,3 +268,50 @@ def test_axisym_driver_steps_fuzz(capfd, nr, nz, base, bu, bv, bp, bl, cu, cv, c
     O.bc(g, "v", v)
     live_axi_steps(g, lg, f, ls, u, v, steps=2, mode=mode, base_r=base, equal=same, len_r=lr, len_z=lz)
     capfd.readouterr()
+
+
+@FUZZ
+@given(nx=st.integers(6, 28), ny=st.integers(6, 28), bp=p_sides(), cp=consts, f=fluids(),
+       seed=st.integers(0, 2 ** 31 - 1))
+def test_gfm_operator_is_symmetric(nx, ny, bp, cp, f, seed):
+    """The 2D GFM operator (whose entries equal the reference's bit for bit,
+    test_gfm_system_and_reference_solvers_fuzz) is exactly symmetric: the
+    west coupling of every cell equals the east coupling of its west
+    neighbour and the south coupling the north one, bit for bit.  The GPU
+    solvers therefore store each face once (east / north) without changing
+    the operator."""
+    g = GridSpec(nx, ny, 1.0 / nx, 1.0 / ny, bc_p=bp, cp=cp)
+    ls, _, _ = drop_fields(nx, ny, g.dx, g.dy, seed)
+    O.bc(g, "p", ls)
+    H, kap = O.heaviside(g, ls), O.kappa(g, ls)
+    div = np.ascontiguousarray(np.random.Generator(np.random.PCG64(seed)).standard_normal(g.shape))
+    s = O.gfm_assemble(g, f, 1.0e-3, ls, kap, H, div, recompute_kappa=True)
+    cw, ce, cs, cn = (s[k].reshape(ny, nx) for k in ("cw", "ce", "cs", "cn"))
+    assert np.array_equal(cw[:, 1:], ce[:, :-1]), "west/east couplings"
+    assert np.array_equal(cs[1:, :], cn[:-1, :]), "south/north couplings"
+
+
+@FUZZ
+@given(nr=st.integers(6, 28), nz=st.integers(6, 28), base=st.sampled_from((0.0, 0.05, 0.1)), bp=axi_p_sides(),
+       cp=consts, sigma=st.sampled_from((0.0, 0.0728, 1.0)), seed=st.integers(0, 2 ** 31 - 1))
+def test_axisym_operator_asymmetry_is_rounding_at_crossing_faces(nr, nz, base, bp, cp, sigma, seed):
+    """The r-weighted GFM operator of MACSolver2DAxisym (entries equal to the
+    reference's, test_axisym_functions_fuzz) is symmetric except at faces the
+    interface crosses, where the two cells interpolate the face radius in
+    different orders: there the two couplings differ by at most a few ulps
+    (relative 1e-15).  That is the whole difference between the reference's
+    operator and the once-per-face storage of the GPU solvers."""
+    g = GridSpec(nr, nz, 0.5 / nr, 1.0 / nz, bc_p=bp, cp=cp)
+    f = FluidSpec(rho_h=1000.0, rho_l=1.226, sigma=sigma)
+    ls, _, _ = drop_fields(nr, nz, g.dx, g.dy, seed, base_x=base)
+    O.bc(g, "p", ls)
+    H = np.ascontiguousarray((ls >= 0.0).astype(np.float64))
+    kap = O.axi_kappa(g, base, ls)
+    div = np.ascontiguousarray(np.random.Generator(np.random.PCG64(seed)).standard_normal(g.shape))
+    s = O.axi_assemble(g, f, base, 1.0e-3, ls, kap, H, div, recompute_kappa=True)
+    cw, ce, cs, cn = (s[k].reshape(nz, nr) for k in ("cw", "ce", "cs", "cn"))
+    heavy = ls[3:-3, 3:-3].T >= 0.0  # (z, r)
+    for d, ref, cross in ((cw[:, 1:] - ce[:, :-1], ce[:, :-1], heavy[:, 1:] != heavy[:, :-1]),
+                          (cs[1:, :] - cn[:-1, :], cn[:-1, :], heavy[1:, :] != heavy[:-1, :])):
+        assert not np.any((d != 0) & ~cross), "asymmetry away from the interface"
+        assert np.all(np.abs(d) <= 1e-15 * np.abs(ref)), float(np.max(np.abs(d) / np.maximum(np.abs(ref), 1e-300)))
