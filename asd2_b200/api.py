@@ -35,7 +35,7 @@ FLAG_NO_CLUSTER_PCG = 1
 FLAG_NO_PERSIST_MG = 2
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "unsupported",
-          -5: "non-finite value", -6: "Krylov breakdown", -7: "checkpoint I/O"}
+          -5: "non-finite value", -6: "Krylov breakdown", -7: "checkpoint I/O", -8: "internal error"}
 
 
 class Asd2gError(RuntimeError):

@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <new>
 #include <vector>
 
@@ -114,6 +115,13 @@ void launch_run_step_end(const KState *ks, RunStats *rs, double tol, double *dsc
 }  // namespace asd2g
 
 using namespace asd2g;
+
+namespace asd2g {
+// The handler of every entry point's function-try-block: a C++ exception
+// (a host allocation that failed, or any other) becomes a status code with
+// its message in asd2g_last_error.  None crosses the C ABI.
+int api_exception(const char *fn);
+}  // namespace asd2g
 
 namespace {
 thread_local char g_err[512] = "";
@@ -382,7 +390,7 @@ extern "C" {
 int asd2g_version(void) { return ASD2G_VERSION; }
 const char *asd2g_last_error(void) { return g_err; }
 
-int asd2g_create(const asd2g_params *p, void *stream, asd2g_session **out) {
+int asd2g_create(const asd2g_params *p, void *stream, asd2g_session **out) try {
     if (!p || !out) return fail(ASD2G_E_ARG, "null argument");
     *out = nullptr;
     Grid g0{};
@@ -480,9 +488,11 @@ int asd2g_create(const asd2g_params *p, void *stream, asd2g_session **out) {
     }
     *out = s;
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_create");
 }
 
-int asd2g_destroy(asd2g_session *s) {
+int asd2g_destroy(asd2g_session *s) try {
     if (s && s->pc_net) asd2g_unet_set_stream(s->pc_net, nullptr);  // it must not keep this session's stream
     if (!s) return ASD2G_OK;
     if (s->st) cudaStreamSynchronize(s->st);
@@ -512,31 +522,41 @@ int asd2g_destroy(asd2g_session *s) {
     if (s->own_stream && s->st) cudaStreamDestroy(s->st);
     delete s;
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_destroy");
 }
 
-int asd2g_sync(asd2g_session *s) {
+int asd2g_sync(asd2g_session *s) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     return sync(s);
+} catch (...) {
+    return asd2g::api_exception("asd2g_sync");
 }
 
-int asd2g_field_ptr(asd2g_session *s, int field, double **dptr) {
+int asd2g_field_ptr(asd2g_session *s, int field, double **dptr) try {
     if (!s || !dptr || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field or null argument");
     *dptr = s->f[field];
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_field_ptr");
 }
 
-int asd2g_upload(asd2g_session *s, int field, const double *host) {
+int asd2g_upload(asd2g_session *s, int field, const double *host) try {
     if (!s || !host || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field or null argument");
     if (cudaMemcpyAsync(s->f[field], host, sizeof(double) * s->G, cudaMemcpyHostToDevice, s->st) != cudaSuccess)
         return cuda_check("upload");
     return sync(s);
+} catch (...) {
+    return asd2g::api_exception("asd2g_upload");
 }
 
-int asd2g_upload_async(asd2g_session *s, int field, const double *host) {
+int asd2g_upload_async(asd2g_session *s, int field, const double *host) try {
     if (!s || !host || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field or null argument");
     if (cudaMemcpyAsync(s->f[field], host, sizeof(double) * s->G, cudaMemcpyHostToDevice, s->st) != cudaSuccess)
         return cuda_check("upload");
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_upload_async");
 }
 
 // Staged copies: the session's copy stream waits for the compute work
@@ -561,47 +581,59 @@ static int staged(asd2g_session *s, int field, void *host, bool up) {
     return cuda_check("staged copy");
 }
 
-int asd2g_upload_staged(asd2g_session *s, int field, const double *host) {
+int asd2g_upload_staged(asd2g_session *s, int field, const double *host) try {
     return staged(s, field, const_cast<double *>(host), true);
+} catch (...) {
+    return asd2g::api_exception("asd2g_upload_staged");
 }
 
 int asd2g_download_staged(asd2g_session *s, int field, double *host) { return staged(s, field, host, false); }
 
-int asd2g_join_copies(asd2g_session *s, int which) {
+int asd2g_join_copies(asd2g_session *s, int which) try {
     if (!s || which < 1 || which > 3) return fail(ASD2G_E_ARG, "which: 1 uploads, 2 downloads, 3 both");
     if (!s->copy_st) return ASD2G_OK;
     if (which & 1) cudaStreamWaitEvent(s->st, s->ev_up, 0);
     if (which & 2) cudaStreamWaitEvent(s->st, s->ev_down, 0);
     return cuda_check("join copies");
+} catch (...) {
+    return asd2g::api_exception("asd2g_join_copies");
 }
 
-int asd2g_sync_copies(asd2g_session *s) {
+int asd2g_sync_copies(asd2g_session *s) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     if (s->copy_st && cudaStreamSynchronize(s->copy_st) != cudaSuccess) return cuda_check("copy stream");
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_sync_copies");
 }
 
-int asd2g_download(asd2g_session *s, int field, double *host) {
+int asd2g_download(asd2g_session *s, int field, double *host) try {
     if (!s || !host || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field or null argument");
     if (cudaMemcpyAsync(host, s->f[field], sizeof(double) * s->G, cudaMemcpyDeviceToHost, s->st) != cudaSuccess)
         return cuda_check("download");
     return sync(s);
+} catch (...) {
+    return asd2g::api_exception("asd2g_download");
 }
 
-int asd2g_copy_field(asd2g_session *s, int dst, int src) {
+int asd2g_copy_field(asd2g_session *s, int dst, int src) try {
     if (!s || !valid_field(dst) || !valid_field(src)) return fail(ASD2G_E_ARG, "bad field");
     if (dst == src) return ASD2G_OK;
     cudaMemcpyAsync(s->f[dst], s->f[src], sizeof(double) * s->G, cudaMemcpyDeviceToDevice, s->st);
     return cuda_check("copy_field");
+} catch (...) {
+    return asd2g::api_exception("asd2g_copy_field");
 }
 
-int asd2g_fill_field(asd2g_session *s, int field, double value) {
+int asd2g_fill_field(asd2g_session *s, int field, double value) try {
     if (!s || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field");
     k_fill<<<(int)((s->G + 255) / 256), 256, 0, s->st>>>(s->f[field], (int64_t)s->G, value);
     return cuda_check("fill_field");
+} catch (...) {
+    return asd2g::api_exception("asd2g_fill_field");
 }
 
-int asd2g_apply_bc_side(asd2g_session *s, int field, char kind, int side, int fill) {
+int asd2g_apply_bc_side(asd2g_session *s, int field, char kind, int side, int fill) try {
     if (!s || !valid_field(field) || side < 0 || side > 3) return fail(ASD2G_E_ARG, "bad field or side");
     int gk;
     if (kind == 'U' || kind == 'u') gk = 0;
@@ -617,15 +649,19 @@ int asd2g_apply_bc_side(asd2g_session *s, int field, char kind, int side, int fi
     else return fail(ASD2G_E_ARG, "fill rule %d not defined for this grid", fill);
     launch_fill_side(s->g, s->f[field], gk, side, k, s->st);
     return cuda_check("apply_bc_side");
+} catch (...) {
+    return asd2g::api_exception("asd2g_apply_bc_side");
 }
 
-int asd2g_apply_bc(asd2g_session *s, int field, char kind) {
+int asd2g_apply_bc(asd2g_session *s, int field, char kind) try {
     if (!s || !valid_field(field)) return fail(ASD2G_E_ARG, "bad field");
     if (kind == 'U' || kind == 'u') launch_fill_uv(s->g, s->f[field], nullptr, s->st);
     else if (kind == 'V' || kind == 'v') launch_fill_uv(s->g, nullptr, s->f[field], s->st);
     else if (kind == 'P' || kind == 'p') launch_fill_p(s->g, s->f[field], s->st);
     else return fail(ASD2G_E_ARG, "grid kind must be U, V or P");
     return cuda_check("apply_bc");
+} catch (...) {
+    return asd2g::api_exception("asd2g_apply_bc");
 }
 
 // ------------------------------------------------------------ level set --
@@ -640,15 +676,17 @@ static void enqueue_ls_advect(asd2g_session *s) {
     launch_ls_stage(3, g, s->w2, s->tu, s->tv, ls, ls, s->dsc, s->st);
 }
 
-int asd2g_ls_advect(asd2g_session *s, double dt) {
+int asd2g_ls_advect(asd2g_session *s, double dt) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     int rc = set_dt(s, dt);
     if (rc) return rc;
     enqueue_ls_advect(s);
     return cuda_check("ls_advect");
+} catch (...) {
+    return asd2g::api_exception("asd2g_ls_advect");
 }
 
-int asd2g_ls_weno_rhs(asd2g_session *s, int ls, int uc, int vc, int out) {
+int asd2g_ls_weno_rhs(asd2g_session *s, int ls, int uc, int vc, int out) try {
     if (!s || !valid_field(ls) || !valid_field(uc) || !valid_field(vc) || !valid_field(out))
         return fail(ASD2G_E_ARG, "bad field");
     if (out == ls || out == uc || out == vc) return fail(ASD2G_E_ARG, "out must differ from the inputs");
@@ -656,47 +694,61 @@ int asd2g_ls_weno_rhs(asd2g_session *s, int ls, int uc, int vc, int out) {
     cudaMemsetAsync(s->f[out], 0, sizeof(double) * s->G, s->st);
     launch_ls_stage(0, s->g, s->f[ls], s->f[uc], s->f[vc], s->f[ls], s->f[out], s->dsc, s->st);
     return cuda_check("ls_weno_rhs");
+} catch (...) {
+    return asd2g::api_exception("asd2g_ls_weno_rhs");
 }
 
-int asd2g_reinit(asd2g_session *s, int mode) {
+int asd2g_reinit(asd2g_session *s, int mode) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     if (mode < 0 || mode > 4) return fail(ASD2G_E_ARG, "reinit mode %d out of range", mode);
     launch_reinit(s->g, mode, s->prm.ls_max_atime, s->f[ASD2G_LS], s->f[ASD2G_LS0], s->w1, s->w2, s->w3, s->st);
     return cuda_check("reinit");
+} catch (...) {
+    return asd2g::api_exception("asd2g_reinit");
 }
 
-int asd2g_subcell_eno(asd2g_session *s, int ls, int ls0, int out) {
+int asd2g_subcell_eno(asd2g_session *s, int ls, int ls0, int out) try {
     if (!s || !valid_field(ls) || !valid_field(ls0) || !valid_field(out) || out == ls || out == ls0)
         return fail(ASD2G_E_ARG, "bad field");
     launch_absgrad(s->g, true, s->f[ls], s->f[ls0], s->f[out], s->st);
     return cuda_check("subcell_eno");
+} catch (...) {
+    return asd2g::api_exception("asd2g_subcell_eno");
 }
 
-int asd2g_eno(asd2g_session *s, int ls, int ls0, int out) {
+int asd2g_eno(asd2g_session *s, int ls, int ls0, int out) try {
     if (!s || !valid_field(ls) || !valid_field(ls0) || !valid_field(out) || out == ls || out == ls0)
         return fail(ASD2G_E_ARG, "bad field");
     launch_absgrad(s->g, false, s->f[ls], s->f[ls0], s->f[out], s->st);
     return cuda_check("eno");
+} catch (...) {
+    return asd2g::api_exception("asd2g_eno");
 }
 
-int asd2g_sussman_constraint(asd2g_session *s, int ls, int ls0, int hd, int out) {
+int asd2g_sussman_constraint(asd2g_session *s, int ls, int ls0, int hd, int out) try {
     if (!s || !valid_field(ls) || !valid_field(ls0) || !valid_field(hd) || !valid_field(out) || out == ls ||
         out == ls0 || out == hd)
         return fail(ASD2G_E_ARG, "bad field");
     launch_sussman_only(s->g, s->f[ls], s->f[ls0], s->f[hd], s->f[out], s->st);
     return cuda_check("sussman_constraint");
+} catch (...) {
+    return asd2g::api_exception("asd2g_sussman_constraint");
 }
 
-int asd2g_heaviside_deriv(asd2g_session *s, int ls, int out) {
+int asd2g_heaviside_deriv(asd2g_session *s, int ls, int out) try {
     if (!s || !valid_field(ls) || !valid_field(out)) return fail(ASD2G_E_ARG, "bad field");
     launch_pointwise_ls(s->g, 0, s->f[ls], s->f[out], s->st);
     return cuda_check("heaviside_deriv");
+} catch (...) {
+    return asd2g::api_exception("asd2g_heaviside_deriv");
 }
 
-int asd2g_smoothed_sign(asd2g_session *s, int ls, int out) {
+int asd2g_smoothed_sign(asd2g_session *s, int ls, int out) try {
     if (!s || !valid_field(ls) || !valid_field(out)) return fail(ASD2G_E_ARG, "bad field");
     launch_pointwise_ls(s->g, 1, s->f[ls], s->f[out], s->st);
     return cuda_check("smoothed_sign");
+} catch (...) {
+    return asd2g::api_exception("asd2g_smoothed_sign");
 }
 
 // Advection + reinitialisation of LS with dt = dsc[0]: the FP32 path for
@@ -718,7 +770,7 @@ static void enqueue_ls_step(asd2g_session *s, int reinit_mode) {
 // kernels take a few microseconds each and launching them one by one from
 // the host is what bounds the step.  Inside a caller's own stream capture
 // they are enqueued directly.
-int asd2g_ls_step(asd2g_session *s, double dt, int reinit_mode) {
+int asd2g_ls_step(asd2g_session *s, double dt, int reinit_mode) try {
     NvtxRange nv("asd2g_ls_step");
     if (!s) return fail(ASD2G_E_ARG, "null session");
     if (reinit_mode < 0 || reinit_mode > 4) return fail(ASD2G_E_ARG, "reinit mode %d out of range", reinit_mode);
@@ -747,16 +799,20 @@ int asd2g_ls_step(asd2g_session *s, double dt, int reinit_mode) {
     }
     if (cudaGraphLaunch(s->ls_exec[reinit_mode], s->st) != cudaSuccess) return cuda_check("ls_step graph launch");
     return cuda_check("ls_step");
+} catch (...) {
+    return asd2g::api_exception("asd2g_ls_step");
 }
 
-int asd2g_last_volume(asd2g_session *s, double *sharp, double *smooth) {
+int asd2g_last_volume(asd2g_session *s, double *sharp, double *smooth) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     if (sharp) *sharp = s->last_volume[0];
     if (smooth) *smooth = s->last_volume[1];
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_last_volume");
 }
 
-int asd2g_volume(asd2g_session *s, double *sharp, double *smooth) {
+int asd2g_volume(asd2g_session *s, double *sharp, double *smooth) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     launch_heaviside(s->g, s->f[ASD2G_LS], s->f[ASD2G_H], s->f[ASD2G_HS], s->st);
     launch_volume(s->g, s->f[ASD2G_H], s->f[ASD2G_HS], s->partial, s->counter + 1, s->dsc + 5, s->st);
@@ -766,9 +822,11 @@ int asd2g_volume(asd2g_session *s, double *sharp, double *smooth) {
     if (sharp) *sharp = s->dsc_host[5];
     if (smooth) *smooth = s->dsc_host[6];
     return cuda_check("volume");
+} catch (...) {
+    return asd2g::api_exception("asd2g_volume");
 }
 
-int asd2g_weno5_line(asd2g_session *s, const double *F, double *FP, double *FM, double d, int n) {
+int asd2g_weno5_line(asd2g_session *s, const double *F, double *FP, double *FM, double d, int n) try {
     if (!s || !F || !FP || !FM || n < 1 || (size_t)(n + 2 * NB) > s->G || !(d > 0.0))
         return fail(ASD2G_E_ARG, "weno5_line: bad arguments");
     const size_t m = (size_t)n + 2 * NB;
@@ -780,26 +838,34 @@ int asd2g_weno5_line(asd2g_session *s, const double *F, double *FP, double *FM, 
     cudaMemcpyAsync(FM, s->f[ASD2G_W2], sizeof(double) * m, cudaMemcpyDeviceToHost, s->st);
     int rc = cuda_check("weno5_line");
     return rc ? rc : sync(s);
+} catch (...) {
+    return asd2g::api_exception("asd2g_weno5_line");
 }
 
-int asd2g_weno_absgrad(asd2g_session *s, int ls, int ls0, int out) {
+int asd2g_weno_absgrad(asd2g_session *s, int ls, int ls0, int out) try {
     if (!s || !valid_field(ls) || !valid_field(ls0) || !valid_field(out) || out == ls || out == ls0)
         return fail(ASD2G_E_ARG, "bad field");
     launch_weno_absgrad(s->g, s->f[ls], s->f[ls0], s->f[out], s->st);
     return cuda_check("weno_absgrad");
+} catch (...) {
+    return asd2g::api_exception("asd2g_weno_absgrad");
 }
 
 // -------------------------------------------------------------- momentum --
-int asd2g_kappa(asd2g_session *s) {
+int asd2g_kappa(asd2g_session *s) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     launch_kappa(s->g, s->f[ASD2G_LS], s->f[ASD2G_KAPPA], s->st);
     return cuda_check("kappa");
+} catch (...) {
+    return asd2g::api_exception("asd2g_kappa");
 }
 
-int asd2g_heaviside(asd2g_session *s) {
+int asd2g_heaviside(asd2g_session *s) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     launch_heaviside(s->g, s->f[ASD2G_LS], s->f[ASD2G_H], s->f[ASD2G_HS], s->st);
     return cuda_check("heaviside");
+} catch (...) {
+    return asd2g::api_exception("asd2g_heaviside");
 }
 
 static int mom_single(asd2g_session *s, int kind, int ls, int u, int v, int h, int fu, int fv) {
@@ -815,11 +881,15 @@ static int mom_single(asd2g_session *s, int kind, int ls, int u, int v, int h, i
 }
 
 int asd2g_convection(asd2g_session *s, int u, int v, int cu, int cv) { return mom_single(s, 5, -1, u, v, -1, cu, cv); }
-int asd2g_viscosity(asd2g_session *s, int u, int v, int ls, int h, int du, int dv) {
+int asd2g_viscosity(asd2g_session *s, int u, int v, int ls, int h, int du, int dv) try {
     return mom_single(s, 6, ls, u, v, h, du, dv);
+} catch (...) {
+    return asd2g::api_exception("asd2g_viscosity");
 }
-int asd2g_momentum_rhs(asd2g_session *s, int ls, int u, int v, int h, int fu, int fv) {
+int asd2g_momentum_rhs(asd2g_session *s, int ls, int u, int v, int h, int fu, int fv) try {
     return mom_single(s, 4, ls, u, v, h, fu, fv);
+} catch (...) {
+    return asd2g::api_exception("asd2g_momentum_rhs");
 }
 
 static int intermediate(asd2g_session *s, int h) {
@@ -844,31 +914,37 @@ static int intermediate(asd2g_session *s, int h) {
     return cuda_check("intermediate_vel");
 }
 
-int asd2g_intermediate_vel(asd2g_session *s, double dt, int h) {
+int asd2g_intermediate_vel(asd2g_session *s, double dt, int h) try {
     if (!s || !valid_field(h)) return fail(ASD2G_E_ARG, "bad field");
     int rc = set_dt(s, dt);
     if (rc) return rc;
     return intermediate(s, h);
+} catch (...) {
+    return asd2g::api_exception("asd2g_intermediate_vel");
 }
 
-int asd2g_divergence(asd2g_session *s, int u, int v, int div) {
+int asd2g_divergence(asd2g_session *s, int u, int v, int div) try {
     if (!s || !valid_field(u) || !valid_field(v) || !valid_field(div) || div == u || div == v)
         return fail(ASD2G_E_ARG, "bad field");
     cudaMemsetAsync(s->f[div], 0, sizeof(double) * s->G, s->st);
     launch_divergence(s->g, s->f[u], s->f[v], s->f[div], s->st);
     return cuda_check("divergence");
+} catch (...) {
+    return asd2g::api_exception("asd2g_divergence");
 }
 
-int asd2g_update_vel(asd2g_session *s, double dt) {
+int asd2g_update_vel(asd2g_session *s, double dt) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     int rc = set_dt(s, dt);
     if (rc) return rc;
     launch_update_vel(s->g, s->M, s->f[ASD2G_UHAT], s->f[ASD2G_VHAT], s->f[ASD2G_PS], s->f[ASD2G_LS], s->f[ASD2G_H],
                       s->f[ASD2G_KAPPA], s->f[ASD2G_U], s->f[ASD2G_V], s->dsc, s->st);
     return cuda_check("update_vel");
+} catch (...) {
+    return asd2g::api_exception("asd2g_update_vel");
 }
 
-int asd2g_update_dt(asd2g_session *s, double *dt) {
+int asd2g_update_dt(asd2g_session *s, double *dt) try {
     if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
     launch_update_dt(s->g, s->M, s->f[ASD2G_U], s->f[ASD2G_V], s->partial, s->counter, s->dsc + 1, s->st);
     cudaMemcpyAsync(s->dsc_host, s->dsc, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
@@ -876,14 +952,18 @@ int asd2g_update_dt(asd2g_session *s, double *dt) {
     if (rc) return rc;
     *dt = s->dsc_host[1];
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_update_dt");
 }
 
-int asd2g_update_ntk(asd2g_session *s, int ls, int nxf, int nyf) {
+int asd2g_update_ntk(asd2g_session *s, int ls, int nxf, int nyf) try {
     if (!s || !valid_field(ls) || !valid_field(nxf) || !valid_field(nyf) || nxf == nyf || nxf == ls || nyf == ls)
         return fail(ASD2G_E_ARG, "bad field");
     launch_absgrad(s->g, false, s->f[ls], s->f[ls], s->w1, s->st);  // ENO_DerivAbsLS_2D(ls, ls)
     launch_ntk(s->g, s->f[ls], s->w1, s->f[nxf], s->f[nyf], s->st);
     return cuda_check("update_ntk");
+} catch (...) {
+    return asd2g::api_exception("asd2g_update_ntk");
 }
 
 // -------------------------------------------------------------- pressure --
@@ -913,15 +993,17 @@ static int assemble(asd2g_session *s, int recompute_kappa) {
     return cuda_check("assemble_gfm");
 }
 
-int asd2g_assemble_gfm(asd2g_session *s, double dt, int recompute_kappa) {
+int asd2g_assemble_gfm(asd2g_session *s, double dt, int recompute_kappa) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     int rc = set_dt(s, dt);
     if (rc) return rc;
     return assemble(s, recompute_kappa);
+} catch (...) {
+    return asd2g::api_exception("asd2g_assemble_gfm");
 }
 
 int asd2g_get_system(asd2g_session *s, double *diag, double *cw, double *ce, double *cs, double *cn, double *rhs,
-                     int *pinned) {
+                     int *pinned) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     if (!s->assembled) return fail(ASD2G_E_ARG, "no system assembled");
     const int nx = s->g.nx, ny = s->g.ny;
@@ -939,6 +1021,8 @@ int asd2g_get_system(asd2g_session *s, double *diag, double *cw, double *ce, dou
     }
     if (pinned) *pinned = s->sys.pinned;
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_get_system");
 }
 
 static int capture_chunk(asd2g_session *s, int solver) {
@@ -1203,7 +1287,7 @@ static int solve_learned(asd2g_session *s, double tol, int maxit, int *iters, do
     return st;
 }
 
-int asd2g_set_preconditioner_net(asd2g_session *s, asd2g_unet *net) {
+int asd2g_set_preconditioner_net(asd2g_session *s, asd2g_unet *net) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     if (net && (s->g.nx % 8 || s->g.ny % 8))
         return fail(ASD2G_E_UNSUPPORTED, "the learned preconditioner needs nx and ny multiples of 8");
@@ -1232,21 +1316,27 @@ int asd2g_set_preconditioner_net(asd2g_session *s, asd2g_unet *net) {
         s->chunk_exec[ASD2G_SOLVER_UNET] = nullptr;
     }
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_set_preconditioner_net");
 }
 
-int asd2g_last_solve_one_launch(asd2g_session *s, int *one_launch) {
+int asd2g_last_solve_one_launch(asd2g_session *s, int *one_launch) try {
     if (!s || !one_launch) return fail(ASD2G_E_ARG, "null argument");
     *one_launch = s->last_one_launch;
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_last_solve_one_launch");
 }
 
-int asd2g_last_fallback(asd2g_session *s, int *used) {
+int asd2g_last_fallback(asd2g_session *s, int *used) try {
     if (!s || !used) return fail(ASD2G_E_ARG, "null argument");
     *used = s->last_fallback;
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_last_fallback");
 }
 
-int asd2g_pc_training_pair_at(asd2g_session *s, int iters, void *feats, void *target) {
+int asd2g_pc_training_pair_at(asd2g_session *s, int iters, void *feats, void *target) try {
     if (!s || !feats || !target) return fail(ASD2G_E_ARG, "null argument");
     if (iters < 0 || iters > 1000) return fail(ASD2G_E_ARG, "iters must be in [0, 1000]");
     if (!s->assembled) return fail(ASD2G_E_ARG, "assemble and solve the system first");
@@ -1281,14 +1371,18 @@ int asd2g_pc_training_pair_at(asd2g_session *s, int iters, void *feats, void *ta
                    (float *)feats, (float *)target, s->st);
     cudaMemcpyAsync(s->x, xs, sizeof(double) * N, cudaMemcpyDeviceToDevice, s->st);
     return cuda_check("training pair");
+} catch (...) {
+    return asd2g::api_exception("asd2g_pc_training_pair_at");
 }
 
-int asd2g_pc_training_pair(asd2g_session *s, void *feats, void *target) {
+int asd2g_pc_training_pair(asd2g_session *s, void *feats, void *target) try {
     return asd2g_pc_training_pair_at(s, 0, feats, target);
+} catch (...) {
+    return asd2g::api_exception("asd2g_pc_training_pair");
 }
 
 int asd2g_solve_pressure(asd2g_session *s, int solver, double tol, int maxit, double dt, int *iters,
-                         double *rel_resid) {
+                         double *rel_resid) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     if (solver < 0 || solver > ASD2G_SOLVER_UNET) return fail(ASD2G_E_ARG, "solver %d out of range", solver);
     if (!s->assembled) return fail(ASD2G_E_ARG, "assemble the system first");
@@ -1301,9 +1395,11 @@ int asd2g_solve_pressure(asd2g_session *s, int solver, double tol, int maxit, do
     launch_scatter_ps(s->g, s->x, s->f[ASD2G_PS], s->f[ASD2G_P], s->dsc, s->st);
     rc = cuda_check("scatter ps");
     return rc ? rc : st;
+} catch (...) {
+    return asd2g::api_exception("asd2g_solve_pressure");
 }
 
-int asd2g_true_residual(asd2g_session *s, double *rel) {
+int asd2g_true_residual(asd2g_session *s, double *rel) try {
     if (!s || !rel) return fail(ASD2G_E_ARG, "null argument");
     if (!s->assembled) return fail(ASD2G_E_ARG, "no system assembled");
     launch_true_residual(s->g, s->sys, s->f[ASD2G_PS], s->partial, s->dsc + 2, s->st);
@@ -1314,11 +1410,13 @@ int asd2g_true_residual(asd2g_session *s, double *rel) {
     if (bb == 0.0) bb = 1.0;
     *rel = std::sqrt(s->dsc_host[2]) / std::sqrt(bb);
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_true_residual");
 }
 
 int asd2g_csr_solve(asd2g_session *s, int solver, int rows, const int *ia, const int *ja, const double *a,
                     const double *diag, const double *b, double *x, double tol, int maxit, int *iters,
-                    double *rel_resid) {
+                    double *rel_resid) try {
     if (!s || !ia || !ja || !a || !diag || !b || !x) return fail(ASD2G_E_ARG, "null argument");
     if (rows < 1 || (size_t)rows > s->N) return fail(ASD2G_E_ARG, "rows must be in [1, nx*ny]");
     if (solver < 0 || solver > 3) return fail(ASD2G_E_ARG, "solver %d not available for CSR input", solver);
@@ -1382,6 +1480,8 @@ int asd2g_csr_solve(asd2g_session *s, int solver, int rows, const int *ia, const
     if (k.status == -6) return fail(ASD2G_E_BREAKDOWN, "Krylov breakdown at iteration %d", k.it);
     const bool conv = solver == 0 ? !(k.res > tol) : (k.res <= tol);
     return conv ? ASD2G_OK : ASD2G_NOT_CONVERGED;
+} catch (...) {
+    return asd2g::api_exception("asd2g_csr_solve");
 }
 
 // ------------------------------------------------------------------ step --
@@ -1469,7 +1569,7 @@ int replay_phase(asd2g_session *s, cudaGraphExec_t *ex, int *calls, const char *
 }  // extern "C++"
 
 int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver, double tol, int maxit, int *iters,
-                       double *rel_resid) {
+                       double *rel_resid) try {
     NvtxRange nv("asd2g_droplet_step");
     if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
     if (reinit_mode < 0 || reinit_mode > 4) return fail(ASD2G_E_ARG, "reinit mode %d out of range", reinit_mode);
@@ -1496,6 +1596,8 @@ int asd2g_droplet_step(asd2g_session *s, double *dt, int reinit_mode, int solver
     s->last_volume[0] = s->dsc_host[5];
     s->last_volume[1] = s->dsc_host[6];
     return st;
+} catch (...) {
+    return asd2g::api_exception("asd2g_droplet_step");
 }
 
 
@@ -1548,29 +1650,35 @@ int axi_we_finite(const asd2g_session *s) {
 }
 }  // namespace
 
-int asd2g_axi_kappa(asd2g_session *s) {
+int asd2g_axi_kappa(asd2g_session *s) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     launch_axi_kappa(s->g, s->f[ASD2G_LS], s->f[ASD2G_KAPPA], s->st);
     return cuda_check("axi_kappa");
+} catch (...) {
+    return asd2g::api_exception("asd2g_axi_kappa");
 }
 
-int asd2g_axi_rhs_u(asd2g_session *s, double dt, int ls, int u, int v, int h, int out) {
+int asd2g_axi_rhs_u(asd2g_session *s, double dt, int ls, int u, int v, int h, int out) try {
     if (!s || !valid_field(ls) || !valid_field(u) || !valid_field(v) || !valid_field(h) || !valid_field(out) ||
         out == ls || out == u || out == v || out == h)
         return fail(ASD2G_E_ARG, "bad field");
     int rc = set_dt(s, dt);
     return rc ? rc : axi_rhs(s, 0, ls, u, v, -1, h, out);
+} catch (...) {
+    return asd2g::api_exception("asd2g_axi_rhs_u");
 }
 
-int asd2g_axi_rhs_v(asd2g_session *s, double dt, int ls, int u, int uhat, int v, int h, int out) {
+int asd2g_axi_rhs_v(asd2g_session *s, double dt, int ls, int u, int uhat, int v, int h, int out) try {
     if (!s || !valid_field(ls) || !valid_field(u) || !valid_field(uhat) || !valid_field(v) || !valid_field(h) ||
         !valid_field(out) || out == ls || out == u || out == uhat || out == v || out == h)
         return fail(ASD2G_E_ARG, "bad field");
     int rc = set_dt(s, dt);
     return rc ? rc : axi_rhs(s, 1, ls, u, v, uhat, h, out);
+} catch (...) {
+    return asd2g::api_exception("asd2g_axi_rhs_v");
 }
 
-int asd2g_axi_viscosity(asd2g_session *s, int ls, int u, int uhat, int v, int h, int du, int dv) {
+int asd2g_axi_viscosity(asd2g_session *s, int ls, int u, int uhat, int v, int h, int du, int dv) try {
     if (!s || !valid_field(ls) || !valid_field(u) || !valid_field(uhat) || !valid_field(v) || !valid_field(h) ||
         !valid_field(du) || !valid_field(dv) || du == dv)
         return fail(ASD2G_E_ARG, "bad field");
@@ -1581,9 +1689,11 @@ int asd2g_axi_viscosity(asd2g_session *s, int ls, int u, int uhat, int v, int h,
     launch_axi_rhs_v(g, s->M, s->f[ls], s->f[u], s->f[uhat], s->f[v], s->f[h], s->f[dv], s->dsc, s->f[dv], s->st,
                      1);
     return cuda_check("axi_viscosity");
+} catch (...) {
+    return asd2g::api_exception("asd2g_axi_viscosity");
 }
 
-int asd2g_axi_hat(asd2g_session *s, int comp, double dt, int ls, int rhs, int h, int out) {
+int asd2g_axi_hat(asd2g_session *s, int comp, double dt, int ls, int rhs, int h, int out) try {
     if (!s || (comp != 0 && comp != 1) || !valid_field(ls) || !valid_field(rhs) || !valid_field(h) ||
         !valid_field(out) || out == ls || out == rhs || out == h)
         return fail(ASD2G_E_ARG, "bad field or component");
@@ -1592,16 +1702,20 @@ int asd2g_axi_hat(asd2g_session *s, int comp, double dt, int ls, int rhs, int h,
     double *const w[6] = {s->ua, s->va, s->ub, s->vb, s->w1, s->w2};
     launch_axi_hat(s->g, s->M, comp, s->f[ls], s->f[rhs], s->f[h], s->dsc, s->f[out], w, s->st);
     return cuda_check("axi_hat");
+} catch (...) {
+    return asd2g::api_exception("asd2g_axi_hat");
 }
 
-int asd2g_axi_divergence(asd2g_session *s, int u, int v, int div, int for_poisson) {
+int asd2g_axi_divergence(asd2g_session *s, int u, int v, int div, int for_poisson) try {
     if (!s || !valid_field(u) || !valid_field(v) || !valid_field(div) || div == u || div == v)
         return fail(ASD2G_E_ARG, "bad field");
     launch_axi_div(s->g, for_poisson ? 1 : 0, s->f[u], s->f[v], s->f[div], s->st);
     return cuda_check("axi_divergence");
+} catch (...) {
+    return asd2g::api_exception("asd2g_axi_divergence");
 }
 
-int asd2g_axi_assemble(asd2g_session *s, double dt, int recompute_kappa) {
+int asd2g_axi_assemble(asd2g_session *s, double dt, int recompute_kappa) try {
     if (!s) return fail(ASD2G_E_ARG, "null session");
     int rc = axi_p_supported(s);
     if (rc) return rc;
@@ -1609,9 +1723,11 @@ int asd2g_axi_assemble(asd2g_session *s, double dt, int recompute_kappa) {
     if (rc) return rc;
     axi_assemble_enqueue(s, recompute_kappa);
     return cuda_check("axi_assemble");
+} catch (...) {
+    return asd2g::api_exception("asd2g_axi_assemble");
 }
 
-int asd2g_axi_update_dt(asd2g_session *s, double *dt) {
+int asd2g_axi_update_dt(asd2g_session *s, double *dt) try {
     if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
     launch_axi_update_dt(s->g, s->M, s->f[ASD2G_U], s->f[ASD2G_V], s->f[ASD2G_KAPPA], s->partial, s->counter,
                          s->dsc + 1, s->st);
@@ -1620,6 +1736,8 @@ int asd2g_axi_update_dt(asd2g_session *s, double *dt) {
     if (rc) return rc;
     *dt = s->dsc_host[1];
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_axi_update_dt");
 }
 
 // One step of the axisymmetric driver before its pressure solve (test_mac2d_
@@ -1673,7 +1791,7 @@ static int axi_step_post(asd2g_session *s) {
 }
 
 int asd2g_axi_step(asd2g_session *s, double *dt, int reinit_mode, const int32_t *ls_bc, const double *ls_bcc,
-                   int solver, double tol, int maxit, int *iters, double *rel_resid) {
+                   int solver, double tol, int maxit, int *iters, double *rel_resid) try {
     NvtxRange nv("asd2g_axi_step");
     if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
     if (reinit_mode < 0 || reinit_mode > 4) return fail(ASD2G_E_ARG, "reinit mode %d out of range", reinit_mode);
@@ -1727,6 +1845,8 @@ int asd2g_axi_step(asd2g_session *s, double *dt, int reinit_mode, const int32_t 
     if (rc) return rc;
     *dt = s->dsc_host[1];
     return st;
+} catch (...) {
+    return asd2g::api_exception("asd2g_axi_step");
 }
 
 // ---- checkpoint / restart ----
@@ -1795,7 +1915,7 @@ int ck_read(const char *path, CkHeader &h, std::vector<double> *payload) {
 }
 }  // namespace
 
-int asd2g_checkpoint_save(asd2g_session *s, const char *path, double t, long long step, double dt) {
+int asd2g_checkpoint_save(asd2g_session *s, const char *path, double t, long long step, double dt) try {
     if (!s || !path) return fail(ASD2G_E_ARG, "null argument");
     const size_t G = s->G;
     std::vector<double> buf(5 * G);
@@ -1823,9 +1943,11 @@ int asd2g_checkpoint_save(asd2g_session *s, const char *path, double t, long lon
     const bool ok = std::fwrite(&h, sizeof h, 1, f) == 1 && std::fwrite(buf.data(), 1, h.payload_bytes, f) == h.payload_bytes;
     const bool closed = std::fclose(f) == 0;
     return ok && closed ? ASD2G_OK : fail(ASD2G_E_IO, "writing checkpoint %s failed", path);
+} catch (...) {
+    return asd2g::api_exception("asd2g_checkpoint_save");
 }
 
-int asd2g_checkpoint_load(asd2g_session *s, const char *path, double *t, long long *step, double *dt) {
+int asd2g_checkpoint_load(asd2g_session *s, const char *path, double *t, long long *step, double *dt) try {
     if (!s || !path) return fail(ASD2G_E_ARG, "null argument");
     CkHeader h{};
     std::vector<double> buf;
@@ -1844,9 +1966,11 @@ int asd2g_checkpoint_load(asd2g_session *s, const char *path, double *t, long lo
     if (step) *step = h.step;
     if (dt) *dt = h.dt;
     return cuda_check("checkpoint load");
+} catch (...) {
+    return asd2g::api_exception("asd2g_checkpoint_load");
 }
 
-int asd2g_checkpoint_info(const char *path, int *nx, int *ny, double *t, long long *step, double *dt) {
+int asd2g_checkpoint_info(const char *path, int *nx, int *ny, double *t, long long *step, double *dt) try {
     if (!path) return fail(ASD2G_E_ARG, "null argument");
     CkHeader h{};
     const int rc = ck_read(path, h, nullptr);
@@ -1857,6 +1981,8 @@ int asd2g_checkpoint_info(const char *path, int *nx, int *ny, double *t, long lo
     if (step) *step = h.step;
     if (dt) *dt = h.dt;
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_checkpoint_info");
 }
 
 // ---- device-resident multi-step run ----
@@ -1985,7 +2111,7 @@ static int capture_run_graph(asd2g_session *s, int reinit_mode, double tol, int 
 }
 
 int asd2g_run_steps(asd2g_session *s, int nsteps, double *dt, int reinit_mode, int solver, double tol, int maxit,
-                    int *steps_done, long long *iters_total, double *max_resid) {
+                    int *steps_done, long long *iters_total, double *max_resid) try {
     NvtxRange nv("asd2g_run_steps");
     if (!s || !dt) return fail(ASD2G_E_ARG, "null argument");
     if (nsteps < 0) return fail(ASD2G_E_ARG, "nsteps must be >= 0");
@@ -2039,6 +2165,8 @@ int asd2g_run_steps(asd2g_session *s, int nsteps, double *dt, int reinit_mode, i
         return ASD2G_NOT_CONVERGED;
     }
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_run_steps");
 }
 
 }  // extern "C"
@@ -2046,5 +2174,16 @@ int asd2g_run_steps(asd2g_session *s, int nsteps, double *dt, int reinit_mode, i
 // Entry points of the ABI layer's helpers for the other host unit (batch.cu).
 namespace asd2g {
 int api_fail(int code, const char *msg) { return fail(code, "%s", msg); }
+int api_exception(const char *fn) {
+    try {
+        throw;
+    } catch (const std::bad_alloc &) {
+        return fail(ASD2G_E_NOMEM, "%s: host allocation failed", fn);
+    } catch (const std::exception &e) {
+        return fail(ASD2G_E_INTERNAL, "%s: %s", fn, e.what());
+    } catch (...) {
+        return fail(ASD2G_E_INTERNAL, "%s: unknown C++ exception", fn);
+    }
+}
 int api_grid_from_params(const asd2g_params *p, Grid &g, MomConst &M) { return grid_from_params(p, g, M); }
 }  // namespace asd2g

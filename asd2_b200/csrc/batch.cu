@@ -17,6 +17,7 @@
 
 namespace asd2g {
 int api_fail(int code, const char *msg);
+int api_exception(const char *fn);  // the entry points' exception handler (api.cu)
 int api_grid_from_params(const asd2g_params *p, Grid &g, MomConst &M);
 LsConst make_lsconst(const Grid &g);              // levelset.cu
 template <typename T> LsConstT<T> make_lsconst_t(const Grid &g);
@@ -363,7 +364,7 @@ int build(asd2g_batch *b) {
 
 extern "C" {
 
-int asd2g_batch_create(const asd2g_params *params, int count, void *stream, asd2g_batch **out) {
+int asd2g_batch_create(const asd2g_params *params, int count, void *stream, asd2g_batch **out) try {
     if (!params || !out || count < 1) return api_fail(ASD2G_E_ARG, "batch_create: bad arguments");
     *out = nullptr;
     for (int i = 0; i < count; i++) {  // validate every instance before any device work
@@ -393,16 +394,20 @@ int asd2g_batch_create(const asd2g_params *params, int count, void *stream, asd2
     }
     *out = b;
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_create");
 }
 
-int asd2g_batch_destroy(asd2g_batch *b) {
+int asd2g_batch_destroy(asd2g_batch *b) try {
     if (!b) return ASD2G_OK;
     cudaStreamSynchronize(b->st);
     release(b);
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_destroy");
 }
 
-int asd2g_batch_upload(asd2g_batch *b, int inst, int field, const double *host) {
+int asd2g_batch_upload(asd2g_batch *b, int inst, int field, const double *host) try {
     const int slot = pad_slot(field);
     if (!b || !host || inst < 0 || inst >= b->count || slot < 0)
         return api_fail(ASD2G_E_ARG, "batch_upload: bad instance or field (LS, KAPPA, H, DIV, PS, P)");
@@ -410,9 +415,11 @@ int asd2g_batch_upload(asd2g_batch *b, int inst, int field, const double *host) 
     double *dst = b->pad + (size_t)slot * b->gtot + b->goff[inst];
     cudaMemcpyAsync(dst, host, sizeof(double) * (size_t)g.sx * g.sy, cudaMemcpyHostToDevice, b->st);
     return check("batch_upload");
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_upload");
 }
 
-int asd2g_batch_download(asd2g_batch *b, int inst, int field, double *host) {
+int asd2g_batch_download(asd2g_batch *b, int inst, int field, double *host) try {
     const int slot = pad_slot(field);
     if (!b || !host || inst < 0 || inst >= b->count || slot < 0)
         return api_fail(ASD2G_E_ARG, "batch_download: bad instance or field (LS, KAPPA, H, DIV, PS, P)");
@@ -421,20 +428,26 @@ int asd2g_batch_download(asd2g_batch *b, int inst, int field, double *host) {
     cudaMemcpyAsync(host, src, sizeof(double) * (size_t)g.sx * g.sy, cudaMemcpyDeviceToHost, b->st);
     if (cudaStreamSynchronize(b->st) != cudaSuccess) return check("batch_download");
     return check("batch_download");
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_download");
 }
 
-int asd2g_batch_field_ptr(asd2g_batch *b, int field, void **dptr, size_t *stride_doubles) {
+int asd2g_batch_field_ptr(asd2g_batch *b, int field, void **dptr, size_t *stride_doubles) try {
     const int slot = pad_slot(field);
     if (!b || !dptr || slot < 0) return api_fail(ASD2G_E_ARG, "batch_field_ptr: bad field");
     *dptr = b->pad + (size_t)slot * b->gtot;
     if (stride_doubles) *stride_doubles = b->gtot;
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_field_ptr");
 }
 
-int asd2g_batch_offset(asd2g_batch *b, int inst, size_t *offset_doubles) {
+int asd2g_batch_offset(asd2g_batch *b, int inst, size_t *offset_doubles) try {
     if (!b || !offset_doubles || inst < 0 || inst >= b->count) return api_fail(ASD2G_E_ARG, "batch_offset: bad instance");
     *offset_doubles = b->goff[inst];
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_offset");
 }
 
 }  // extern "C"
@@ -456,24 +469,28 @@ int solve_impl(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_re
 
 extern "C" {
 
-int asd2g_batch_assemble(asd2g_batch *b, const double *dt) {
+int asd2g_batch_assemble(asd2g_batch *b, const double *dt) try {
     NvtxRange nv("batched GFM assembly");
     if (!b || !dt) return api_fail(ASD2G_E_ARG, "batch_assemble: null argument");
     int rc = set_dts(b, dt);
     if (rc) return rc;
     launch_batch_assemble(b->dinst, b->cell_tiles, b->ncell_tiles, b->st);
     return check("batch_assemble");
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_assemble");
 }
 
-int asd2g_batch_solve(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_resid) {
+int asd2g_batch_solve(asd2g_batch *b, double tol, int maxit, int *iters, double *rel_resid) try {
     if (!b || !(tol > 0.0) || maxit < 1) return api_fail(ASD2G_E_ARG, "batch_solve: bad arguments");
     return solve_impl(b, tol, maxit, iters, rel_resid);
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_solve");
 }
 
 // The full droplet step of every instance (asd2g_droplet_step per instance,
 // MG-FCG pressure solve), one launch per phase for the whole batch.
 int asd2g_batch_step(asd2g_batch *b, double *dt, int reinit_mode, double tol, int maxit, int *iters,
-                     double *rel_resid) {
+                     double *rel_resid) try {
     NvtxRange nv("asd2g_batch_step");
     if (!b || !dt || !(tol > 0.0) || maxit < 1) return api_fail(ASD2G_E_ARG, "batch_step: bad arguments");
     if (reinit_mode < ASD2G_REINIT_ORIGINAL || reinit_mode > ASD2G_REINIT_MINRK2_SUSSMAN ||
@@ -579,9 +596,11 @@ int asd2g_batch_step(asd2g_batch *b, double *dt, int reinit_mode, double tol, in
     if (cudaStreamSynchronize(st) != cudaSuccess) return check("batch_step");
     rc = check("batch_step");
     return rc ? rc : st_solve;
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_step");
 }
 
-int asd2g_batch_volume(asd2g_batch *b, double *sharp, double *smooth) {
+int asd2g_batch_volume(asd2g_batch *b, double *sharp, double *smooth) try {
     if (!b) return api_fail(ASD2G_E_ARG, "null batch");
     if (sharp)
         cudaMemcpy2DAsync(sharp, sizeof(double), b->sc + 2, sizeof(double) * SC_PER_INST, sizeof(double), b->count,
@@ -591,6 +610,8 @@ int asd2g_batch_volume(asd2g_batch *b, double *sharp, double *smooth) {
                           cudaMemcpyDeviceToHost, b->st);
     if (cudaStreamSynchronize(b->st) != cudaSuccess) return check("batch_volume");
     return check("batch_volume");
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_volume");
 }
 
 }  // extern "C"
@@ -850,16 +871,18 @@ int solve_learned_impl(asd2g_batch *b, double tol, int maxit, int *iters, double
 
 extern "C" {
 
-int asd2g_batch_tile_shape(asd2g_batch *b, int *rows, int *cols, float *trial_ms) {
+int asd2g_batch_tile_shape(asd2g_batch *b, int *rows, int *cols, float *trial_ms) try {
     if (!b) return api_fail(ASD2G_E_ARG, "null batch");
     if (rows) *rows = MG_SHAPES[b->plan.shape][0];
     if (cols) *cols = MG_SHAPES[b->plan.shape][1];
     if (trial_ms)
         for (int k = 0; k < MG_NSHAPES; k++) trial_ms[k] = (float)b->shape_ms[k];
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_tile_shape");
 }
 
-int asd2g_batch_set_preconditioner_net(asd2g_batch *b, asd2g_unet *net) {
+int asd2g_batch_set_preconditioner_net(asd2g_batch *b, asd2g_unet *net) try {
     if (!b) return api_fail(ASD2G_E_ARG, "null batch");
     if (b->pc_exec) {  // the captured chunk holds the previous network's launches
         cudaGraphExecDestroy(b->pc_exec);
@@ -888,25 +911,33 @@ int asd2g_batch_set_preconditioner_net(asd2g_batch *b, asd2g_unet *net) {
     rc = asd2g_unet_get_params(net, h.data());
     if (!rc) rc = asd2g_unet_set_params(b->net, h.data());
     return rc;
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_set_preconditioner_net");
 }
 
-int asd2g_batch_solve_with(asd2g_batch *b, int solver, double tol, int maxit, int *iters, double *rel_resid) {
+int asd2g_batch_solve_with(asd2g_batch *b, int solver, double tol, int maxit, int *iters, double *rel_resid) try {
     if (!b || !(tol > 0.0) || maxit < 1) return api_fail(ASD2G_E_ARG, "batch_solve: bad arguments");
     if (solver == ASD2G_SOLVER_MGPCG) return solve_impl(b, tol, maxit, iters, rel_resid);
     if (solver == ASD2G_SOLVER_UNET) return solve_learned_impl(b, tol, maxit, iters, rel_resid);
     return api_fail(ASD2G_E_ARG, "batch solver must be ASD2G_SOLVER_MGPCG or ASD2G_SOLVER_UNET");
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_solve_with");
 }
 
-int asd2g_batch_last_fallback(asd2g_batch *b, int *used) {
+int asd2g_batch_last_fallback(asd2g_batch *b, int *used) try {
     if (!b || !used) return api_fail(ASD2G_E_ARG, "null argument");
     *used = b->last_fallback;
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_last_fallback");
 }
 
-int asd2g_batch_sync(asd2g_batch *b) {
+int asd2g_batch_sync(asd2g_batch *b) try {
     if (!b) return api_fail(ASD2G_E_ARG, "null batch");
     if (cudaStreamSynchronize(b->st) != cudaSuccess) return check("batch sync");
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_batch_sync");
 }
 
 }  // extern "C"

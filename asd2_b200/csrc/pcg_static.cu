@@ -32,6 +32,10 @@
 #include "pressure.cuh"
 
 namespace asd2g {
+int api_exception(const char *fn);  // the entry points' exception handler (api.cu)
+}  // namespace asd2g
+
+namespace asd2g {
 namespace {
 
 constexpr int64_t kMaxUnknowns = ASD2G_STATIC_MAX_UNKNOWNS;
@@ -64,7 +68,7 @@ using namespace asd2g;
 
 extern "C" int asd2g_pcg_solve_static(int nx, int ny, int pinned, const double *diag, const double *ce,
                                       const double *cn, const double *b, double *x, double tol, int maxit,
-                                      void *stream, int *iters, double *rel_resid) {
+                                      void *stream, int *iters, double *rel_resid) try {
     if (nx < 1 || ny < 1) return static_fail(ASD2G_E_ARG, "asd2g_pcg_solve_static: nx and ny must be positive");
     if ((int64_t)nx * ny > kMaxUnknowns)
         return static_fail(ASD2G_E_ARG,
@@ -143,4 +147,6 @@ extern "C" int asd2g_pcg_solve_static(int nx, int ny, int pinned, const double *
     if (hk.status == -5) return static_fail(ASD2G_E_NONFINITE, "asd2g_pcg_solve_static: non-finite residual");
     if (hk.status == -6) return static_fail(ASD2G_E_BREAKDOWN, "asd2g_pcg_solve_static: breakdown (p.Ap = 0)");
     return !(hk.res > tol) ? ASD2G_OK : ASD2G_NOT_CONVERGED;
+} catch (...) {
+    return asd2g::api_exception("asd2g_pcg_solve_static");
 }

@@ -30,6 +30,10 @@
 #include "tc05.cuh"
 
 namespace asd2g {
+int api_exception(const char *fn);  // the entry points' exception handler (api.cu)
+}  // namespace asd2g
+
+namespace asd2g {
 
 bool conv_cout_ok(int c) { return c == 16 || c == 32 || c == 48 || c == 64 || c == 96 || c == 128 || c == 192; }
 
@@ -801,7 +805,7 @@ extern "C" {
 
 size_t asd2g_conv_wpack_bytes(int cout_pad, int cin_pad) { return (size_t)cout_pad * cin_pad * 9 * 2; }
 
-int asd2g_conv_pack_weights(const float *w, int cout, int cin, int cout_pad, int cin_pad, void *wpack, void *stream) {
+int asd2g_conv_pack_weights(const float *w, int cout, int cin, int cout_pad, int cin_pad, void *wpack, void *stream) try {
     if (!w || !wpack || cout < 1 || cin < 1 || cout > cout_pad || cin > cin_pad || cin_pad % 16 ||
         !conv_cout_ok(cout_pad))
         return ASD2G_E_ARG;
@@ -809,13 +813,17 @@ int asd2g_conv_pack_weights(const float *w, int cout, int cin, int cout_pad, int
     k_pack_conv<<<(int)((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184), 256, 0, (cudaStream_t)stream>>>(
         w, cout, cin, cout_pad, cin_pad, (__nv_bfloat16 *)wpack);
     return cudaGetLastError() == cudaSuccess ? ASD2G_OK : ASD2G_E_CUDA;
+} catch (...) {
+    return asd2g::api_exception("asd2g_conv_pack_weights");
 }
 
 int asd2g_conv3x3_bf16(const void *in, int n, int h, int w, int cin, const void *wpack, const float *bias, int cout,
-                       void *out, float *out32, int relu, int *err, void *stream) {
+                       void *out, float *out32, int relu, int *err, void *stream) try {
     if (!in || !wpack || !bias || (!out && !out32) || n < 1 || h < 1 || w < 1 || cin < 16 || cin % 16)
         return ASD2G_E_ARG;
     return conv3x3_tc(in, n, h, w, cin, wpack, bias, cout, out, out32, relu, err, (cudaStream_t)stream, nullptr, 0);
+} catch (...) {
+    return asd2g::api_exception("asd2g_conv3x3_bf16");
 }
 
 }  // extern "C"

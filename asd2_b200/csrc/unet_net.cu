@@ -27,6 +27,7 @@
 
 namespace asd2g {
 int api_fail(int code, const char *msg);
+int api_exception(const char *fn);  // the entry points' exception handler (api.cu)
 bool conv_cout_ok(int c);
 // low != nullptr: the input is concat(nearest-upsampled low with cl channels, in)
 int wgrad_tc(const void *X, const void *G, int B, int H, int W, int CIS, int CI, int COS, int CO, float *dW,
@@ -589,7 +590,7 @@ void release(asd2g_unet *u) {
 
 extern "C" {
 
-int asd2g_unet_create(int max_batch, int max_h, int max_w, void *stream, asd2g_unet **out) {
+int asd2g_unet_create(int max_batch, int max_h, int max_w, void *stream, asd2g_unet **out) try {
     if (!out || max_batch < 1 || max_h < 8 || max_w < 8 || max_h % 8 || max_w % 8)
         return api_fail(ASD2G_E_ARG, "unet_create: sizes must be positive multiples of 8");
     *out = nullptr;
@@ -666,19 +667,23 @@ int asd2g_unet_create(int max_batch, int max_h, int max_w, void *stream, asd2g_u
     cudaMemsetAsync(u->w, 0, sizeof(float) * u->nparam, u->st);
     *out = u;
     return cuda_ok("create");
+} catch (...) {
+    return asd2g::api_exception("asd2g_unet_create");
 }
 
-int asd2g_unet_destroy(asd2g_unet *u) {
+int asd2g_unet_destroy(asd2g_unet *u) try {
     if (!u) return ASD2G_OK;
     cudaStreamSynchronize(u->st);
     release(u);
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_unet_destroy");
 }
 
 size_t asd2g_unet_nparams(asd2g_unet *u) { return u ? u->nparam : 0; }
 
 // He-normal initialisation (std = sqrt(2 / (9 cin))), the last layer scaled by 0.1, zero biases.
-int asd2g_unet_init(asd2g_unet *u, unsigned long long seed) {
+int asd2g_unet_init(asd2g_unet *u, unsigned long long seed) try {
     if (!u) return api_fail(ASD2G_E_ARG, "null network");
     std::vector<float> h(u->nparam, 0.0f);
     std::mt19937_64 rng(seed);
@@ -688,9 +693,11 @@ int asd2g_unet_init(asd2g_unet *u, unsigned long long seed) {
         for (size_t k = 0; k < (size_t)l.cout * l.cin * 9; k++) h[l.woff + k] = nd(rng);
     }
     return asd2g_unet_set_params(u, h.data());
+} catch (...) {
+    return asd2g::api_exception("asd2g_unet_init");
 }
 
-int asd2g_unet_set_params(asd2g_unet *u, const float *host) {
+int asd2g_unet_set_params(asd2g_unet *u, const float *host) try {
     if (!u || !host) return api_fail(ASD2G_E_ARG, "null argument");
     cudaMemcpyAsync(u->w, host, sizeof(float) * u->nparam, cudaMemcpyHostToDevice, u->st);
     cudaMemsetAsync(u->m, 0, sizeof(float) * u->nparam, u->st);
@@ -699,12 +706,16 @@ int asd2g_unet_set_params(asd2g_unet *u, const float *host) {
     const int rc = repack(u);
     if (rc) return rc;
     return cudaStreamSynchronize(u->st) == cudaSuccess ? ASD2G_OK : cuda_ok("set_params");
+} catch (...) {
+    return asd2g::api_exception("asd2g_unet_set_params");
 }
 
-int asd2g_unet_get_params(asd2g_unet *u, float *host) {
+int asd2g_unet_get_params(asd2g_unet *u, float *host) try {
     if (!u || !host) return api_fail(ASD2G_E_ARG, "null argument");
     cudaMemcpyAsync(host, u->w, sizeof(float) * u->nparam, cudaMemcpyDeviceToHost, u->st);
     return cudaStreamSynchronize(u->st) == cudaSuccess ? ASD2G_OK : cuda_ok("get_params");
+} catch (...) {
+    return asd2g::api_exception("asd2g_unet_get_params");
 }
 
 // A forward pass fits when its B * H * W pixels fit the activation buffers
@@ -720,7 +731,7 @@ static int check_shape(asd2g_unet *u, int B, int H, int W, bool training = true)
 }
 
 // feats: device FP32 [B][H][W][4]; out: device FP32 [B][H][W].
-int asd2g_unet_forward(asd2g_unet *u, int B, int H, int W, const float *feats, float *out) {
+int asd2g_unet_forward(asd2g_unet *u, int B, int H, int W, const float *feats, float *out) try {
     NvtxRange nv("U-Net forward");
     int rc = check_shape(u, B, H, W, false);
     if (rc) return rc;
@@ -731,6 +742,8 @@ int asd2g_unet_forward(asd2g_unet *u, int B, int H, int W, const float *feats, f
     if (rc) return rc;
     cudaMemcpyAsync(out, u->out, sizeof(float) * npix, cudaMemcpyDeviceToDevice, u->st);
     return cuda_ok("unet_forward");
+} catch (...) {
+    return asd2g::api_exception("asd2g_unet_forward");
 }
 
 static int train_finish(asd2g_unet *u, int B, int H, int W, float *loss_mean) {
@@ -756,7 +769,7 @@ static int train_finish(asd2g_unet *u, int B, int H, int W, float *loss_mean) {
 
 // One Adam step on a batch: loss = mean over samples of |out - target|^2 / |target|^2.
 int asd2g_unet_train_step(asd2g_unet *u, int B, int H, int W, const float *feats, const float *target, float lr,
-                          float *loss_mean) {
+                          float *loss_mean) try {
     NvtxRange nv("U-Net train step (MSE)");
     int rc = check_shape(u, B, H, W);
     if (rc) return rc;
@@ -768,12 +781,14 @@ int asd2g_unet_train_step(asd2g_unet *u, int B, int H, int W, const float *feats
     k_loss<<<B, 256, 0, u->st>>>(u->out, target, npix, u->gL, u->loss);
     u->lr = lr;
     return train_finish(u, B, H, W, loss_mean);
+} catch (...) {
+    return asd2g::api_exception("asd2g_unet_train_step");
 }
 
 // One Adam step on the energy loss: mean over samples of the relative A-norm
 // error 1 - (out' A t)^2 / ((out' A out)(t' A t)).
 int asd2g_unet_train_step_energy(asd2g_unet *u, int B, int H, int W, const float *feats, const float *target,
-                                 float lr, float *loss_mean) {
+                                 float lr, float *loss_mean) try {
     NvtxRange nv("U-Net train step (energy)");
     int rc = check_shape(u, B, H, W);
     if (rc) return rc;
@@ -785,11 +800,13 @@ int asd2g_unet_train_step_energy(asd2g_unet *u, int B, int H, int W, const float
     k_loss_energy<<<B, 1024, 0, u->st>>>(u->out, feats, target, H, W, u->lscr, u->gL, u->loss);
     u->lr = lr;
     return train_finish(u, B, H, W, loss_mean);
+} catch (...) {
+    return asd2g::api_exception("asd2g_unet_train_step_energy");
 }
 
 // One Adam step on the residual loss: mean over samples of 1 - cos^2(A out, r).
 int asd2g_unet_train_step_residual(asd2g_unet *u, int B, int H, int W, const float *feats, float lr,
-                                   float *loss_mean) {
+                                   float *loss_mean) try {
     NvtxRange nv("U-Net train step (residual)");
     int rc = check_shape(u, B, H, W);
     if (rc) return rc;
@@ -801,25 +818,33 @@ int asd2g_unet_train_step_residual(asd2g_unet *u, int B, int H, int W, const flo
     k_loss_stencil<<<B, 1024, 0, u->st>>>(u->out, feats, H, W, u->lscr, u->gL, u->loss);
     u->lr = lr;
     return train_finish(u, B, H, W, loss_mean);
+} catch (...) {
+    return asd2g::api_exception("asd2g_unet_train_step_residual");
 }
 
 // NULL returns the network to the stream it was created with.
-int asd2g_unet_set_stream(asd2g_unet *u, void *stream) {
+int asd2g_unet_set_stream(asd2g_unet *u, void *stream) try {
     if (!u) return api_fail(ASD2G_E_ARG, "null network");
     u->st = stream ? (cudaStream_t)stream : u->home_st;
     return ASD2G_OK;
+} catch (...) {
+    return asd2g::api_exception("asd2g_unet_set_stream");
 }
 
-int asd2g_unet_get_grads(asd2g_unet *u, float *host) {
+int asd2g_unet_get_grads(asd2g_unet *u, float *host) try {
     if (!u || !host) return api_fail(ASD2G_E_ARG, "null argument");
     cudaMemcpyAsync(host, u->g, sizeof(float) * u->nparam, cudaMemcpyDeviceToHost, u->st);
     return cudaStreamSynchronize(u->st) == cudaSuccess ? ASD2G_OK : cuda_ok("get_grads");
+} catch (...) {
+    return asd2g::api_exception("asd2g_unet_get_grads");
 }
 
-int asd2g_unet_error_flag(asd2g_unet *u, int *flag) {
+int asd2g_unet_error_flag(asd2g_unet *u, int *flag) try {
     if (!u || !flag) return api_fail(ASD2G_E_ARG, "null argument");
     cudaMemcpyAsync(flag, u->err, sizeof(int), cudaMemcpyDeviceToHost, u->st);
     return cudaStreamSynchronize(u->st) == cudaSuccess ? ASD2G_OK : cuda_ok("error flag");
+} catch (...) {
+    return asd2g::api_exception("asd2g_unet_error_flag");
 }
 
 }  // extern "C"

@@ -32,11 +32,12 @@ extern "C" {
 #define ASD2G_NOT_CONVERGED 1     /* iterative solve hit maxit */
 #define ASD2G_E_ARG (-1)          /* invalid argument (size, enum, null) */
 #define ASD2G_E_CUDA (-2)         /* CUDA runtime error */
-#define ASD2G_E_NOMEM (-3)        /* device allocation failed */
+#define ASD2G_E_NOMEM (-3)        /* device (or host) allocation failed */
 #define ASD2G_E_UNSUPPORTED (-4)  /* configuration outside the implemented path */
 #define ASD2G_E_NONFINITE (-5)    /* NaN/Inf detected (the reference exit(1)s) */
 #define ASD2G_E_BREAKDOWN (-6)    /* Krylov breakdown (zero denominator) */
 #define ASD2G_E_IO (-7)           /* checkpoint file: open/read/write failed, or not a valid checkpoint */
+#define ASD2G_E_INTERNAL (-8)     /* a C++ exception inside the library, caught at the entry point */
 
 /* ---- boundary kinds: same values as enum class BC2D (include/common.h:4) ---- */
 enum asd2g_bc {
