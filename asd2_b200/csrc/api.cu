@@ -1865,15 +1865,27 @@ static_assert(sizeof(CkHeader) == 128, "checkpoint header is 128 bytes");
 constexpr char CK_MAGIC[8] = {'A', 'S', 'D', '2', 'G', 'C', 'K', '1'};
 constexpr int CK_FIELDS[5] = {ASD2G_LS, ASD2G_U, ASD2G_V, ASD2G_PS, ASD2G_P};
 
-// Weighted word sum  sum_i w_i (2 i + 1)  mod 2^64 over the payload's 64-bit words.
-uint64_t ck_checksum(const double *data, size_t nwords) {
+// Weighted word sum  sum_i w_i (2 i + 1)  mod 2^64 over 64-bit words w_i,
+// the index i counted from `first` (a sum taken in pieces).
+uint64_t ck_checksum(const void *data, size_t nwords, uint64_t first = 0) {
+    const unsigned char *p = static_cast<const unsigned char *>(data);
     uint64_t h = 0;
     for (size_t i = 0; i < nwords; i++) {
         uint64_t w;
-        std::memcpy(&w, data + i, 8);
-        h += w * (2u * (uint64_t)i + 1u);
+        std::memcpy(&w, p + 8 * i, 8);
+        h += w * (2u * (first + i) + 1u);
     }
     return h;
+}
+
+// The file's checksum: the header with its checksum field zeroed is words
+// 0..15, the payload words 16 on (so t, dt, step and the reserved bytes are
+// covered as well as the fields).
+uint64_t ck_file_checksum(const CkHeader &h, const double *payload, size_t nwords) {
+    CkHeader z = h;
+    z.checksum = 0;
+    constexpr size_t hw = sizeof(CkHeader) / 8;
+    return ck_checksum(&z, hw) + ck_checksum(payload, nwords, hw);
 }
 
 // Reads and checks the header; with payload != nullptr also reads the payload.
@@ -1889,7 +1901,7 @@ int ck_read(const char *path, CkHeader &h, std::vector<double> *payload) {
     if (std::fseek(f, 0, SEEK_END) == 0) file_bytes = std::ftell(f);
     std::rewind(f);
     if (std::fread(&h, sizeof h, 1, f) != 1) rc = fail(ASD2G_E_IO, "%s: short header", path);
-    else if (std::memcmp(h.magic, CK_MAGIC, 8) != 0 || h.version != 1 || h.header_bytes != sizeof(CkHeader))
+    else if (std::memcmp(h.magic, CK_MAGIC, 8) != 0 || h.version != 2 || h.header_bytes != sizeof(CkHeader))
         rc = fail(ASD2G_E_IO, "%s: not an asd2g checkpoint (magic/version)", path);
     else if (h.nx < 1 || h.ny < 1 || h.nx > kMaxSide || h.ny > kMaxSide || h.nbc != 3 || h.nfields != 5 ||
              h.payload_bytes != (uint64_t)h.nfields * (uint64_t)((int64_t)h.nx + 6) *
@@ -1902,7 +1914,7 @@ int ck_read(const char *path, CkHeader &h, std::vector<double> *payload) {
             std::vector<double> buf(h.payload_bytes / 8);
             if (std::fread(buf.data(), 1, h.payload_bytes, f) != h.payload_bytes)
                 rc = fail(ASD2G_E_IO, "%s: short payload", path);
-            else if (ck_checksum(buf.data(), buf.size()) != h.checksum)
+            else if (ck_file_checksum(h, buf.data(), buf.size()) != h.checksum)
                 rc = fail(ASD2G_E_IO, "%s: checksum mismatch", path);
             else if (payload)
                 payload->swap(buf);
@@ -1925,7 +1937,7 @@ int asd2g_checkpoint_save(asd2g_session *s, const char *path, double t, long lon
     if (rc) return rc;
     CkHeader h{};
     std::memcpy(h.magic, CK_MAGIC, 8);
-    h.version = 1;
+    h.version = 2;
     h.header_bytes = sizeof(CkHeader);
     h.nx = s->g.nx;
     h.ny = s->g.ny;
@@ -1937,7 +1949,7 @@ int asd2g_checkpoint_save(asd2g_session *s, const char *path, double t, long lon
     h.nfields = 5;
     for (int k : CK_FIELDS) h.field_bits |= 1u << k;
     h.payload_bytes = sizeof(double) * buf.size();
-    h.checksum = ck_checksum(buf.data(), buf.size());
+    h.checksum = ck_file_checksum(h, buf.data(), buf.size());
     FILE *f = std::fopen(path, "wb");
     if (!f) return fail(ASD2G_E_IO, "cannot create checkpoint %s", path);
     const bool ok = std::fwrite(&h, sizeof h, 1, f) == 1 && std::fwrite(buf.data(), 1, h.payload_bytes, f) == h.payload_bytes;

@@ -510,13 +510,15 @@ int asd2g_run_steps(asd2g_session *s, int nsteps, double *dt, int reinit_mode, i
 /* ---- checkpoint / restart (no reference counterpart: the reference writes
  * Tecplot output only) ----
  * A raw binary file: a 128-byte little-endian header
- *   char magic[8] = "ASD2GCK1"; u32 version = 1; u32 header_bytes = 128;
+ *   char magic[8] = "ASD2GCK1"; u32 version = 2; u32 header_bytes = 128;
  *   i32 nx, ny, nbc (= 3), precision; f64 t, dt; i64 step;
  *   u32 nfields, field_bits (bit f set for each field id stored);
  *   u64 payload_bytes; u64 checksum; zero padding
  * then the fields LS, U, V, PS, P in that order, each the padded
- * (nx+6) x (ny+6) FP64 array of the session layout.  checksum = sum over the
- * payload's little-endian 64-bit words w_i of w_i (2 i + 1), mod 2^64.  Enough to restart a
+ * (nx+6) x (ny+6) FP64 array of the session layout.  checksum = sum of
+ * w_i (2 i + 1) mod 2^64 over the little-endian 64-bit words w_i of the
+ * header (its checksum field read as 0; words 0-15) followed by the payload
+ * (words 16 on): any changed word, header included, changes it.  Enough to restart a
  * run (with t, step and the next dt) and to hand fields between processes.
  * save: writes the session's current fields.  load: checks magic, version,
  * sizes (nx, ny must match the session) and checksum, then replaces the

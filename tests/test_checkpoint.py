@@ -81,3 +81,50 @@ def test_library_refuses_header_claiming_huge_grid(tmp_path, claim):
     with pytest.raises(api.Asd2gError) as e:
         api.checkpoint_info(p)
     assert e.value.code == -7
+
+
+def test_reader_fuzz(tmp_path):
+    """Random damage to a valid checkpoint (a flipped bit anywhere, a random
+    byte run, a cut at any length, trailing bytes): the library's reader and
+    the numpy reader refuse every damaged file (-7 / ValueError; the checksum
+    covers the header too), accept it only where the damage rewrote bytes
+    with their own values, and never crash."""
+    hyp = pytest.importorskip("hypothesis")
+    from hypothesis import HealthCheck, given, settings
+    from hypothesis import strategies as st
+
+    p0 = tmp_path / "base.ck"
+    CK.write(p0, _fields(7, 5, seed=9), t=0.5, step=3, dt=1e-3)
+    base = p0.read_bytes()
+    truth = dict(nx=7, ny=5, t=0.5, step=3, dt=1e-3)
+
+    @settings(max_examples=300, deadline=None, derandomize=True,
+              suppress_health_check=[HealthCheck.function_scoped_fixture])
+    @given(kind=st.sampled_from(("bit", "run", "cut", "extend")), pos=st.integers(0, len(base) - 1),
+           bit=st.integers(0, 7), run=st.binary(min_size=1, max_size=24))
+    def check(kind, pos, bit, run):
+        raw = bytearray(base)
+        if kind == "bit":
+            raw[pos] ^= 1 << bit
+        elif kind == "run":
+            raw[pos:pos + len(run)] = run
+        elif kind == "cut":
+            raw = raw[:pos]
+        else:
+            raw += run
+        p = tmp_path / "fuzz.ck"
+        p.write_bytes(bytes(raw))
+        try:
+            info = api.checkpoint_info(p)
+        except api.Asd2gError as e:
+            assert e.code == -7, e
+            info = None
+        try:
+            CK.read(p)
+            ok_np = True
+        except ValueError:
+            ok_np = False
+        assert (info is not None) == ok_np == (bytes(raw) == base), (kind, pos, bit, run)
+        if info is not None:
+            assert info == truth
+    check()
