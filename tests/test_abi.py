@@ -5,6 +5,7 @@ import glob
 import os
 import re
 
+import numpy as np
 import pytest
 
 from asd2_b200 import api
@@ -97,3 +98,44 @@ def test_axisymmetric_entry_points_check_arguments_first():
     assert L.asd2g_axi_step(None, ctypes.byref(d), 2, None, None, 0, 1e-10, 100, ctypes.byref(it),
                             ctypes.byref(res)) == -1
     assert b"null" in L.asd2g_last_error()
+
+
+# Entry points for which null / zero arguments are a valid call: destroying
+# nothing succeeds (like free(NULL)), sizes of nothing are 0.
+NULL_OK = {"asd2g_version": 1, "asd2g_destroy": 0, "asd2g_batch_destroy": 0, "asd2g_unet_destroy": 0,
+           "asd2g_conv_wpack_bytes": 0, "asd2g_unet_nparams": 0}
+
+
+def _zero_args(fn):
+    args = []
+    for t in fn.argtypes or []:
+        if hasattr(t, "_dtype_"):  # an ndpointer: a one-element array
+            args.append(np.zeros(1, dtype=t._dtype_))
+        elif t in (ctypes.c_int, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint, ctypes.c_longlong, ctypes.c_size_t,
+                   ctypes.c_ulonglong):
+            args.append(0)
+        elif t in (ctypes.c_double, ctypes.c_float):
+            args.append(0.0)
+        elif t is ctypes.c_char:
+            args.append(b"P")
+        else:
+            args.append(None)
+    return args
+
+
+def test_every_entry_point_refuses_null_arguments():
+    """Every exported function called with null pointers, zero sizes and zero
+    scalars returns an error status (or the documented value for a null
+    destroy / an empty size); none dereferences a null pointer or launches
+    device work."""
+    L = api.load()
+    for name in api.EXPORTS:
+        fn = getattr(L, name)
+        if name == "asd2g_last_error":
+            assert isinstance(fn(), bytes)
+            continue
+        r = fn(*_zero_args(fn))
+        if name in NULL_OK:
+            assert r == NULL_OK[name], (name, r)
+        else:
+            assert r < 0, (name, r)
