@@ -1186,6 +1186,14 @@ def _quiet_call(fn):
     sys.stdout.flush()
     libc = ctypes.CDLL(None)
     r, w = os.pipe()
+    chunks = []
+
+    def drain():  # read while fn runs, so that no amount of output fills the pipe
+        with os.fdopen(r, "rb") as f:
+            for block in iter(lambda: f.read1(65536), b""):
+                chunks.append(block)
+    reader = threading.Thread(target=drain, daemon=True)
+    reader.start()
     saved = os.dup(1)
     try:
         os.dup2(w, 1)
@@ -1195,9 +1203,8 @@ def _quiet_call(fn):
         os.dup2(saved, 1)
         os.close(saved)
         os.close(w)
-    with os.fdopen(r) as f:
-        text = f.read()
-    return out, text
+        reader.join()
+    return out, b"".join(chunks).decode(errors="replace")
 
 
 def _cg_worker(payload):

@@ -64,3 +64,17 @@ def test_quiet_call_keeps_stdout_clean(capfd):
     res, text = bench._quiet_call(noisy)
     assert res == 3 and text == "CG : 7 7 Err : 0.5\n"
     assert "CG :" not in capfd.readouterr().out
+
+
+def test_quiet_call_drains_large_output(capfd):
+    """More output than a pipe holds (the reference's GetUHat prints a line
+    per grid row) does not block the guard."""
+    import bench
+
+    def chatty():
+        for _ in range(4096):
+            os.write(1, b"x" * 63 + b"\n")
+        return 1
+    res, text = bench._quiet_call(chatty)
+    assert res == 1 and len(text) == 4096 * 64
+    assert capfd.readouterr().out == ""
