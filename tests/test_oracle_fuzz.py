@@ -315,3 +315,62 @@ def test_axisym_operator_asymmetry_is_rounding_at_crossing_faces(nr, nz, base, b
                           (cs[1:, :] - cn[:-1, :], cn[:-1, :], heavy[1:, :] != heavy[:-1, :])):
         assert not np.any((d != 0) & ~cross), "asymmetry away from the interface"
         assert np.all(np.abs(d) <= 1e-15 * np.abs(ref)), float(np.max(np.abs(d) / np.maximum(np.abs(ref), 1e-300)))
+
+
+@FUZZ
+@given(nx=st.integers(5, 26), ny=st.integers(5, 26), bp=st.tuples(*[st.sampled_from(KINDS_P)] * 4),
+       bu=sides_uv, bv=sides_uv, f=fluids(), shape=st.sampled_from(("drop", "sign", "noise")),
+       seed=st.integers(0, 2 ** 31 - 1))
+def test_building_blocks_fuzz(capfd, nx, ny, bp, bu, bv, f, shape, seed):
+    """The building blocks one by one on drawn grids, boundary sets and fields
+    (a drop, a sign field with its ties, plain noise): the WENO5 right side
+    and its 1D kernel (levelset2d.cpp:88-262), the subcell and plain ENO
+    Godunov gradients (:560-785), the Sussman constraint and the Heaviside
+    derivative (:27-41, :787-893), the smoothed sign (:914-923), the
+    curvature and UpdateNTK (mac2d.cpp:124-252), both Heavisides (:87-122),
+    convection and viscosity (:308-1041), the divergence (:1729-1738) and
+    UpdateDt (:1851-1880), against the reference's own classes."""
+    lx, ly = 1.0, 1.0
+    dx, dy = lx / nx, ly / ny
+    g = GridSpec(nx, ny, dx, dy, bc_u=bu, bc_v=bv, bc_p=bp)
+    ls, u, v = drop_fields(nx, ny, dx, dy, seed)
+    rng = np.random.Generator(np.random.PCG64(seed + 3))
+    if shape == "sign":
+        ls = np.ascontiguousarray(np.sign(ls))
+    elif shape == "noise":
+        ls = np.ascontiguousarray(rng.standard_normal(ls.shape))
+    ls0 = np.ascontiguousarray(ls + 0.01 * rng.standard_normal(ls.shape))
+    R = Reference(g, f, len_x=lx, len_y=ly)
+    try:
+        # every call gets its own copies: the functions fill ghost cells of
+        # their inputs in place, and some fills are not idempotent
+        k = lambda a: a.copy()
+        same(O.ls_weno_rhs(g, k(ls), u, v), R.ls_weno_rhs(k(ls), u, v), "HJWENO5_LS_2D")
+        F = rng.standard_normal(nx + 6)
+        for a, b in zip(O.unit_weno5(F, dx, nx), R.unit_weno5(F, dx, nx)):
+            same(a, b, "UnitHJWENO5")
+        same(O.subcell_eno_absgrad(g, k(ls), k(ls0)), R.subcell_eno_absgrad(k(ls), k(ls0)), "SubcellENO_Min_DerivAbsLS_2D")
+        same(O.eno_absgrad(g, k(ls), k(ls0)), R.eno_absgrad(k(ls), k(ls0)), "ENO_DerivAbsLS_2D")
+        hd = O.heaviside_deriv(g, k(ls0))
+        same(hd, R.heaviside_deriv(k(ls0)), "UpdateHeavisideFuncDeriv")
+        same(O.sussman_constraint(g, k(ls), k(ls0), k(hd)), R.sussman_constraint(k(ls), k(ls0), k(hd)), "GetSussmanReinitConstraint")
+        same(O.smoothed_sign(g, k(ls0)), R.smoothed_sign(k(ls0)), "GetSmoothedSignFunc")
+        same(O.kappa(g, k(ls)), R.kappa(k(ls)), "UpdateKappa")
+        a = O.ntk(g, k(ls), np.full(g.shape, 7.0), np.full(g.shape, -7.0))
+        b = R.ntk(k(ls), np.full(g.shape, 7.0), np.full(g.shape, -7.0))
+        same(a[0], b[0], "UpdateNTK x")
+        same(a[1], b[1], "UpdateNTK y")
+        H, HS = R.heaviside(k(ls))
+        same(O.heaviside(g, k(ls)), H, "UpdateHeavisideFunc")
+        same(O.smooth_heaviside(g, k(ls)), HS, "UpdateSmoothHeavisideFunc")
+        cu, cv = R.conv(k(u), k(v))
+        same(O.conv_u(g, k(u), k(v)), cu, "AddConvectionFU")
+        same(O.conv_v(g, k(u), k(v)), cv, "AddConvectionFV")
+        du, dv = R.visc(k(u), k(v), k(ls), k(HS))
+        same(O.visc_u(g, f, k(u), k(v), k(ls), k(HS)), du, "AddViscosityFU")
+        same(O.visc_v(g, f, k(u), k(v), k(ls), k(HS)), dv, "AddViscosityFV")
+        same(O.divergence(g, k(u), k(v)), R.divergence(k(u), k(v)), "GetDivergence")
+        assert O.update_dt(g, f, k(u), k(v)) == R.update_dt(k(u), k(v)), "UpdateDt"
+    finally:
+        R.close()
+    capfd.readouterr()
