@@ -19,6 +19,7 @@
  */
 #ifndef ASD2G_H_INCLUDED
 #define ASD2G_H_INCLUDED
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
