@@ -47,3 +47,23 @@ def test_c_example_compiles(tmp_path, n):
                         "-Werror=incompatible-pointer-types", "-Werror=int-conversion", "-Werror=return-type",
                         "-I", os.path.join(ROOT, "include"), str(path)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-3000:] + "\n" + block
+
+
+def cpp_blocks():
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    return re.findall(r"```cpp\n(.*?)```", text, re.S)
+
+
+@pytest.mark.parametrize("n", range(len(cpp_blocks())))
+def test_cpp_example_compiles(tmp_path, n):
+    """The C++ example, with its placeholder `...` for the first dt filled in
+    and the caller's std::vector fields declared."""
+    block = cpp_blocks()[n].replace("= ...;", "= 1e-3;")
+    head = "\n".join(ln for ln in block.splitlines() if ln.startswith("#include"))
+    body = "\n".join(ln for ln in block.splitlines() if not ln.startswith("#include"))
+    src = (head + "\n#include <vector>\nvoid example() {\n    std::vector<double> ls, u, v, ps;\n" + body + "\n}\n")
+    path = tmp_path / f"example{n}.cpp"
+    path.write_text(src)
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(path)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:] + "\n" + block
