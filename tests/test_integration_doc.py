@@ -67,3 +67,31 @@ def test_cpp_example_compiles(tmp_path, n):
     r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(path)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-3000:] + "\n" + block
+
+
+def python_blocks():
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    return re.findall(r"```python\n(.*?)```", text, re.S)
+
+
+@pytest.mark.parametrize("n", range(len(python_blocks())))
+def test_python_example_names_real_api(n):
+    """The Python examples parse, and every api.* / workloads.* name and every
+    Session method they call exists, with the keyword arguments they pass."""
+    import ast
+    import inspect
+
+    from asd2_b200 import api
+    from asd2_b200 import workloads as W
+    tree = ast.parse(python_blocks()[n])
+    modules = {"api": api, "W": W}
+    for node in ast.walk(tree):
+        if isinstance(node, ast.Attribute) and isinstance(node.value, ast.Name) and node.value.id in modules:
+            assert hasattr(modules[node.value.id], node.attr), f"{node.value.id}.{node.attr}"
+        if (isinstance(node, ast.Call) and isinstance(node.func, ast.Attribute)
+                and isinstance(node.func.value, ast.Name) and node.func.value.id == "s"):
+            meth = getattr(api.Session, node.func.attr, None)
+            assert meth is not None, f"Session.{node.func.attr}"
+            params = inspect.signature(meth).parameters
+            for kw in node.keywords:
+                assert kw.arg in params, f"Session.{node.func.attr}({kw.arg}=...)"
