@@ -95,3 +95,20 @@ def test_python_example_names_real_api(n):
             params = inspect.signature(meth).parameters
             for kw in node.keywords:
                 assert kw.arg in params, f"Session.{node.func.attr}({kw.arg}=...)"
+
+
+REPO_PREFIXES = ("asd2_b200/", "tests/", "oracle/", "include/", "profiles/")
+
+
+@pytest.mark.parametrize("doc", ["DESIGN.md", "INTEGRATION.md", "README.md"])
+def test_docs_name_existing_repo_files(doc):
+    """Every repository path a document names in backticks exists (paths of
+    the reference's own tree, such as src/mac2d.cpp, are not checked)."""
+    text = open(os.path.join(ROOT, doc)).read()
+    missing = []
+    for m in re.finditer(r"`([A-Za-z0-9_./-]+)`", text):
+        path = m.group(1).rstrip(".").split(":")[0]
+        if path.startswith(REPO_PREFIXES) and "*" not in path and "_ref/" not in path:
+            if not os.path.exists(os.path.join(ROOT, path)):
+                missing.append(path)
+    assert not missing, sorted(set(missing))
