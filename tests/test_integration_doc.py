@@ -1,5 +1,7 @@
-"""CPU: the C examples in INTEGRATION.md compile against include/asd2g.h, so
-every documented call names a real entry point with the right arguments."""
+"""CPU: the examples of the integration guide compile against
+include/asd2g.h (C, C++) or name the binding's real functions (Python), so
+every documented call names a real entry point with the right arguments; the
+repository paths the documents name exist."""
 import os
 import re
 import subprocess
