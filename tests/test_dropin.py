@@ -313,3 +313,18 @@ def test_axisym_solve_tdma_equals_reference(tmp_path, n):
             np.testing.assert_array_equal(cd[n:], rc_d, err_msg=f"system {k}: d")
     finally:
         R.close()
+
+
+@pytest.mark.parametrize("header", sorted(f for f in os.listdir(B.DROPIN) if f.endswith(".h")) + ["asd2g.h"])
+def test_headers_are_self_contained(tmp_path, header):
+    """Each drop-in header (and the C ABI header, in C and C++) compiles when
+    included first and alone, as a user's translation unit includes it."""
+    inc = ["-I", os.path.join(B.ROOT, "include"), "-I", B.DROPIN]
+    langs = [("cpp", [B.gxx(), "-std=c++17"])]
+    if header == "asd2g.h":
+        langs.append(("c", ["gcc", "-std=c11"]))
+    for ext, cc in langs:
+        src = tmp_path / f"only_{header}.{ext}"
+        src.write_text(f'#include "{header}"\nint main(void) {{ return 0; }}\n')
+        r = subprocess.run(cc + ["-fsyntax-only", "-Wall", *inc, str(src)], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr[-2000:]
