@@ -1207,6 +1207,42 @@ def _quiet_call(fn):
     return out, b"".join(chunks).decode(errors="replace")
 
 
+def _isolated_entry(conn, fn, payload):
+    try:
+        conn.send(("ok", fn(payload)))
+    except BaseException as e:  # noqa: BLE001 (reported to the parent)
+        conn.send(("error", f"{type(e).__name__}: {e}"))
+    finally:
+        conn.close()
+
+
+def _run_isolated(fn, payload, timeout):
+    """fn(payload) in a fresh spawned process: its result, or an exception
+    when it raises, dies (an abort in native code) or runs past `timeout`
+    seconds (then it is terminated).  The bench never waits on it for good."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    recv, send = ctx.Pipe(duplex=False)
+    proc = ctx.Process(target=_isolated_entry, args=(send, fn, payload), daemon=True)
+    proc.start()
+    send.close()
+    try:
+        if not recv.poll(timeout):
+            raise TimeoutError(f"worker ran past {timeout} s")
+        status, value = recv.recv()
+    except EOFError:
+        proc.join(5)
+        raise RuntimeError(f"worker died (exit code {proc.exitcode})") from None
+    finally:
+        if proc.is_alive():
+            proc.terminate()
+        proc.join(5)
+        recv.close()
+    if status != "ok":
+        raise RuntimeError(value)
+    return value
+
+
 def _cg_worker(payload):
     """One build of the reference's CG timed in a fresh process (its BLAS and
     OpenMP thread counts come from the environment it was started with)."""
@@ -1237,7 +1273,6 @@ def cg_blas_baseline(snap, case, dt, its_to_tol, iters=200, reps=3):
     iterations per timed call, below the count at which its 1e-6 stop could
     end the call early.  Solves/s = 1 / (time per iteration x the Jacobi-PCG
     iterations to the bench's tolerance, its_to_tol)."""
-    import multiprocessing as mp
     from oracle.pyoracle import REF_SO, FluidSpec, GridSpec, Oracle
     blas_so = os.path.join(os.path.dirname(REF_SO), "libasd2ref_blas.so")
     if not os.path.exists(REF_SO):
@@ -1256,12 +1291,14 @@ def cg_blas_baseline(snap, case, dt, its_to_tol, iters=200, reps=3):
     iters = int(min(iters, max(2, its_to_tol // 2)))
     out = {"system": f"{case.nx}x{case.ny} GFM, {rows} unknowns", "iterations_per_call": iters,
            "iterations_to_tol": int(its_to_tol)}
-    cores = os.cpu_count() or 1
+    # a 65k-row system gains nothing from more threads than this, and an
+    # OpenBLAS asked for more threads than it was built for may abort
+    cores = min(os.cpu_count() or 1, 32)
     runs = [("serial_shim", REF_SO, 1, 1)]
     if os.path.exists(blas_so):
         half = max(1, cores // 2)
         runs += [(f"openblas_{bt}_openmp_{ot}", blas_so, bt, ot) for bt, ot in ((1, cores), (half, half), (cores, 1))]
-    ctx = mp.get_context("spawn")
+
     saved = {k: os.environ.get(k) for k in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "OMP_WAIT_POLICY")}
     best_name, best_ms = None, float("inf")
     try:
@@ -1269,8 +1306,7 @@ def cg_blas_baseline(snap, case, dt, its_to_tol, iters=200, reps=3):
             os.environ.update(OPENBLAS_NUM_THREADS=str(bt), OMP_NUM_THREADS=str(ot), OMP_WAIT_POLICY="passive")
             payload = dict(grid=grid, fluid=dict(case.fluid), path=path, csr=(a, ia, ja), mdiag=mdiag, rhs=rhs,
                            iters=iters, reps=reps)
-            with ctx.Pool(1) as pool:
-                t, done = pool.apply(_cg_worker, (payload,))
+            t, done = _run_isolated(_cg_worker, payload, timeout=300)
             ms_it = 1e3 * t / (done or iters)
             out[name] = {"openblas_threads": bt, "openmp_threads": ot, "ms_per_iteration": ms_it,
                          "iterations_run": done, "solves_per_s": 1e3 / (ms_it * its_to_tol)}

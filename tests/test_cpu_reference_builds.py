@@ -78,3 +78,31 @@ def test_quiet_call_drains_large_output(capfd):
     res, text = bench._quiet_call(chatty)
     assert res == 1 and len(text) == 4096 * 64
     assert capfd.readouterr().out == ""
+
+
+def _raises(payload):
+    raise ValueError("planted")
+
+
+def _dies(payload):
+    os._exit(3)
+
+
+def _sleeps(payload):
+    import time
+    time.sleep(payload)
+    return payload
+
+
+def test_isolated_worker_never_leaves_the_bench_waiting():
+    """The bench's isolated worker returns a result, and turns a raising, a
+    dying and an overrunning worker into exceptions (the overrunning one is
+    terminated)."""
+    import bench
+    assert bench._run_isolated(_sleeps, 0, timeout=60) == 0
+    with pytest.raises(RuntimeError, match="planted"):
+        bench._run_isolated(_raises, None, timeout=60)
+    with pytest.raises(RuntimeError, match="died"):
+        bench._run_isolated(_dies, None, timeout=60)
+    with pytest.raises(TimeoutError):
+        bench._run_isolated(_sleeps, 30, timeout=1)
