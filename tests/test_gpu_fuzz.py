@@ -1,6 +1,7 @@
-"""B200: whole droplet steps of asd2g_droplet_step against the oracle on
-drawn configurations (grid sizes, U / V / P boundary kinds and constants,
-fluids, time orders, reinitialisation modes), with the same strategies the
+"""B200: whole droplet steps of asd2g_droplet_step and axisymmetric steps of
+asd2g_axi_step against the oracle on drawn configurations (grid sizes, U / V
+/ P boundary kinds and constants, axis offsets, fluids, time orders,
+reinitialisation modes), with the same strategies the
 CPU pins of the oracle against the reference use (tests/test_oracle_fuzz.py).
 
 A randomised sweep kept out of the default GPU suite: it runs with
@@ -18,7 +19,7 @@ from hypothesis import strategies as st  # noqa: E402
 from asd2_b200 import api  # noqa: E402
 from oracle.pyoracle import GridSpec, Oracle  # noqa: E402
 from tests.helpers import assert_bitexact, assert_close, interior, params_for  # noqa: E402
-from tests.test_oracle_fuzz import consts, drop_fields, fluids, p_sides, sides_uv  # noqa: E402
+from tests.test_oracle_fuzz import axi_p_sides, consts, drop_fields, fluids, p_sides, sides_uv  # noqa: E402
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(os.environ.get("ASD2G_GPU_FUZZ") != "1", reason="opt-in: ASD2G_GPU_FUZZ=1")]
@@ -65,3 +66,39 @@ def test_droplet_steps_gpu_fuzz(nx, ny, bu, bv, bp, cu, cv, cp, f, mode, seed):
                          1e-8 * max(np.abs(ps_ref).max(), 1e-30), f"ps step {k}")
             assert abs(r["dt_next"] - st_["dt"]) <= 1e-9 * st_["dt"], (k, r["dt_next"], st_["dt"])
             dt = st_["dt"]
+
+
+@settings(max_examples=EXAMPLES, deadline=None, derandomize=True, print_blob=True,
+          suppress_health_check=[HealthCheck.too_slow, HealthCheck.data_too_large])
+@given(nr=st.integers(8, 32), nz=st.integers(8, 40), base=st.sampled_from((0.0, 0.05)), bu=sides_uv, bv=sides_uv,
+       bp=axi_p_sides(), cu=consts, cv=consts, cp=consts, f=fluids(axisym=True), seed=st.integers(0, 2 ** 31 - 1))
+def test_axisym_steps_gpu_fuzz(nr, nz, base, bu, bv, bp, cu, cv, cp, f, seed):
+    """Two axisymmetric driver steps (asd2g_axi_step, level set on the
+    reference driver's own kinds: axisym, lsfree x 3) against the oracle's,
+    pressure to 1e-12: level set within 1e-10 of max(|phi|, 1), u, v and ps
+    within 1e-7 of their maxima, dt within 1e-10."""
+    lr, lz = 0.5, 1.0
+    dr, dz = lr / nr, lz / nz
+    g = GridSpec(nr, nz, dr, dz, bc_u=bu, bc_v=bv, bc_p=bp, cu=cu, cv=cv, cp=cp)
+    lg = GridSpec(nr, nz, dr, dz, bc_u=bu, bc_v=bv, bc_p=("axisym", "lsfree", "lsfree", "lsfree"))
+    ls, u, v = drop_fields(nr, nz, dr, dz, seed, base_x=base)
+    O.bc(lg, "p", ls)
+    O.bc(g, "u", u)
+    O.bc(g, "v", v)
+    st_ = dict(ls=ls, u=u, v=v, kappa=g.zeros())
+    st_["dt"] = dt = O.axi_update_dt(g, f, u, v, st_["kappa"])
+    with api.Session(params_for(g, f, base_x=base)) as s:
+        for fld in ("ls", "u", "v", "kappa"):
+            s.upload(fld, st_[fld])
+        for k in range(2):
+            r = s.axi_step(dt, ls_bc=lg.bc_p, solver=api.PCG, tol=1e-12, maxit=200000)
+            assert r["status"] == 0, r
+            O.axi_step(g, f, st_, base_r=base, ls_grid=lg, tol=1e-12)
+            assert abs(r["dt_next"] - st_["dt"]) <= 1e-10 * st_["dt"], (k, r["dt_next"], st_["dt"])
+            dt = st_["dt"]
+            for fld in ("ls", "u", "v", "ps"):
+                ref = st_[fld]
+                err = np.abs(s.download(fld) - ref)[3:-3, 3:-3].max()
+                scale = max(np.abs(ref[3:-3, 3:-3]).max(), 1e-30)
+                bar = 1e-10 * max(scale, 1.0) if fld == "ls" else 1e-7 * scale
+                assert err <= bar, (k, fld, err, scale, bu, bv, bp)
