@@ -9,10 +9,18 @@ time order and the reinitialisation mode; each drawn case runs through both
 implementations.  The draws are derandomised (the same cases on every run),
 so a failure reproduces; hypothesis prints the failing case.
 
+Properties: ghost fills; the building blocks one by one; all five
+reinitialisations; the captured GFM system with the reference's CG and
+BiCGStab iterates; whole droplet steps; the axisymmetric functions and whole
+axisymmetric driver steps; and two properties of the operators the GPU
+solvers rely on (the 2D GFM operator is symmetric bit for bit, the
+axisymmetric one up to a few ulps at interface-crossing faces).
+
 What the restatement corrects on purpose is kept out of the draws: the
 all-Neumann pressure pin (the reference's CSR is mis-indexed), periodic
 pressure (the product refuses it) and the V-gravity fix (off, as in the
-reference).
+reference).  The spacings are derived as the reference derives them, length
+over cell count.
 """
 import numpy as np
 import pytest
